@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark of the HONEI sparse-solver hot path on B200.
+
+Default workload (the SpMV configuration of the north-star configs): ELL SpMV, FP64, on the
+2-D Q1 Poisson stiffness matrix of a 2049 x 2049 node grid (4,198,401 rows, 37,720,073
+nonzeros, Dirichlet rows identity), x ~ U[-1,1] seeded.  One step = 10 SpMV applications, the
+sample the reference's own ELL benchmark times (benchmark/product_ell_file_BENCHMARK.cc).
+The matrix (453 MB of Ax + Aj) is larger than L2 (126 MB), so every application streams it
+from HBM; x (34 MB) is the gathered, L2-resident operand.
+
+Metric: SpMV GB/s of algorithmic traffic, nnz*(8+4) + 2*n*8 bytes per application (Ax + 32-bit
+Aj once, x read once, y written once), against the measured HBM copy bandwidth.
+Extras on the same line: plain FP64 CG solves/s and p50/p99 latency on the 257^2 system
+(x_true U[-1,1], x0 = 0, relative residual 1e-8), and the FP32 SpMV.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU: replicas only (one independent system per GPU, no collective; weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+M_SPMV = 2049
+M_CG = 257
+SPMV_PER_STEP = 10
+
+
+def spmv_bytes(nnz, n, s):
+    return nnz * (s + 4) + 2 * n * s
+
+
+def q1_nnz(M):
+    return (M - 2) ** 2 * 9 + (4 * M - 4)
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, copy burst)"
+    except Exception:
+        return 6650.0, "fallback (6.65 TB/s earlier pool measurement)"
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch from the committed ncu summary profiles/<name>.md, if present."""
+    import re
+    p = os.path.join(ROOT, "profiles", name + ".md")
+    try:
+        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while the timed region runs."""
+
+    REASONS = {
+        "gpu_idle": 0x1, "applications_clocks_setting": 0x2, "sw_power_cap": 0x4,
+        "hw_slowdown": 0x8, "sync_boost": 0x10, "sw_thermal_slowdown": 0x20,
+        "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80, "display_clock_setting": 0x100,
+    }
+
+    def __init__(self, device_index=0, period=0.005):
+        self.samples, self.reasons = [], set()
+        self.period = period
+        self._stop = threading.Event()
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.max_mhz = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                mask = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for k, bit in self.REASONS.items():
+                    if mask & bit and k != "gpu_idle":
+                        self.reasons.add(k)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples), "source": "nvml" if self.ok else "unavailable"}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------------------------------
+# Reference arm: the reference's own CPU path (oracle/_ref, tags::CPU::MultiCore::SSE on all
+# host cores), else the C restatement (single core).
+# ---------------------------------------------------------------------------------------
+def cpu_spmv_gbs(reps=None, budget_s=10.0):
+    from honei_b200 import problems as P
+    A = P.q1_poisson(M_SPMV)
+    x = P.uniform_vector(A.rows, 1)
+    nbytes = spmv_bytes(A.nnz, A.rows, 8)
+    cores = os.cpu_count() or 1
+    try:
+        from oracle.bindings import REF_SO, Reference
+        if not os.path.exists(REF_SO):
+            raise OSError
+        R = Reference()
+        R.set_threads(cores)
+        _, t1 = R.spmv(A, x, tag="mc-sse", reps=1)
+        if reps is None:
+            reps = int(max(3, min(200, budget_s / max(t1, 1e-4))))
+        _, t = R.spmv(A, x, tag="mc-sse", reps=reps)
+        kind, used_cores = "reference", cores
+        desc = f"tags::CPU::MultiCore::SSE, {reps} SpMVs of the 2049^2 FP64 matrix, median"
+    except OSError:
+        from oracle.bindings import Oracle
+        O = Oracle()
+        t0 = time.perf_counter()
+        O.spmv(A, x)
+        t1 = time.perf_counter() - t0
+        if reps is None:
+            reps = int(max(3, min(100, budget_s / max(t1, 1e-4))))
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            O.spmv(A, x)
+            ts.append(time.perf_counter() - t0)
+        t = statistics.median(ts)
+        kind, used_cores = "port", 1
+        desc = f"C restatement of tags::CPU, {reps} SpMVs of the 2049^2 FP64 matrix, median"
+    return nbytes / t / 1e9, used_cores, kind, desc, reps
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    gbs_list = []
+    for _ in range(args.warmup):
+        cpu_spmv_gbs(reps=SPMV_PER_STEP)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        g, cores, kind, desc, _ = cpu_spmv_gbs(reps=SPMV_PER_STEP)
+        gbs_list.append(g)
+    wall = time.perf_counter() - t0
+    value = statistics.median(gbs_list)
+    line = {
+        "impl": "reference", "metric": "ell_spmv_gbs_q1_2049_f64", "value": round(value, 3), "unit": "GB/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000 * wall / max(args.steps, 1), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "ell_spmv_q1_2049_f64", "rows": M_SPMV ** 2, "nnz": q1_nnz(M_SPMV),
+                   "spmv_per_step": SPMV_PER_STEP},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": cores, "kind": kind,
+                         "sample": desc.replace(f"{SPMV_PER_STEP} SpMVs", f"{SPMV_PER_STEP} SpMVs per step")},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------------
+# Our arm
+# ---------------------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from honei_b200 import la, problems as P
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    ctx = la.Context(local)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- SpMV workload (replica per rank, assembled on the device) ----
+    A = la.SparseMatrixELL.q1_poisson(M_SPMV, ctx=ctx)
+    n = A.rows()
+    nnz = q1_nnz(M_SPMV)
+    x = torch.from_numpy(P.uniform_vector(n, 1 + rank)).cuda()
+    y = torch.empty_like(x)
+    nbytes = spmv_bytes(nnz, n, 8)
+
+    def step():
+        for _ in range(SPMV_PER_STEP):
+            la.Product.value(y, A, x, ctx=ctx)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    barrier()
+    l0 = ctx.launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = ctx.launches() - l0
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    apps = args.steps * SPMV_PER_STEP
+    per_launch_s = ms / 1e3 / apps
+    value = ws * nbytes * apps / (ms_max / 1e3) / 1e9
+    achieved = nbytes / per_launch_s / 1e9
+    peak, peak_src = measured_peak()
+
+    # ---- e2e through the public API with host buffers (pinned), per step: H2D x, 10 SpMVs,
+    # D2H y (the step's result) ----
+    xh = torch.from_numpy(P.uniform_vector(n, 7 + rank)).pin_memory()
+    yh = torch.empty(n, dtype=torch.float64).pin_memory()
+    xd = torch.empty_like(x)
+
+    def e2e_step():
+        xd.copy_(xh, non_blocking=True)
+        for _ in range(SPMV_PER_STEP):
+            la.Product.value(y, A, xd, ctx=ctx)
+        yh.copy_(y, non_blocking=True)
+
+    for _ in range(3):
+        e2e_step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        dist.all_reduce(ems, op=dist.ReduceOp.MAX)
+    e2e_value = ws * nbytes * apps / (float(ems.item()) / 1e3) / 1e9
+
+    # ---- FP32 SpMV on the same matrix (extra) ----
+    A32 = A.to_float(ctx=ctx)
+    x32, y32 = x.float(), torch.empty(n, dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        la.Product.value(y32, A32, x32, ctx=ctx)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(100):
+        la.Product.value(y32, A32, x32, ctx=ctx)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    gbs32 = spmv_bytes(nnz, n, 4) * 100 / (f0.elapsed_time(f1) / 1e3) / 1e9
+    del A32, x32, y32
+
+    # ---- plain FP64 CG on 257^2: solve latency (host b -> device solve -> host x) ----
+    Acg = la.SparseMatrixELL.q1_poisson(M_CG, ctx=ctx)
+    ncg = Acg.rows()
+    xt = torch.from_numpy(P.uniform_vector(ncg, 1)).cuda()
+    bcg = torch.empty_like(xt)
+    la.Product.value(bcg, Acg, xt, ctx=ctx)
+    bh = bcg.cpu().pin_memory()
+    xh_cg = torch.empty(ncg, dtype=torch.float64).pin_memory()
+    bd, xd_cg = torch.empty_like(bcg), torch.empty_like(bcg)
+    lat, iters = [], None
+    n_solves = 30
+    for i in range(n_solves + 3):
+        t0 = time.perf_counter()
+        bd.copy_(bh, non_blocking=True)
+        xd_cg.zero_()
+        iters = la.CGSolver.value(Acg, None, bd, xd_cg, 20000, 1e-8, ctx=ctx)
+        xh_cg.copy_(xd_cg, non_blocking=True)
+        torch.cuda.synchronize()
+        if i >= 3:
+            lat.append(time.perf_counter() - t0)
+    lat_ms = sorted(1e3 * v for v in lat)
+    cg_extra = {"workload": "plain FP64 CG, Q1 257^2, 1e-8 relative, x0 = 0", "iterations": iters,
+                "solves_per_s": round(len(lat) / sum(lat), 2),
+                "p50_ms": round(statistics.median(lat_ms), 3),
+                "p99_ms": round(lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))], 3)}
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if ws == 1 and not args.no_cpu_baseline:
+            g, cores, kind, desc, reps = cpu_spmv_gbs()
+            cpu = {"value": round(g, 3), "unit": "GB/s", "cores": cores, "kind": kind, "sample": desc}
+        line = {
+            "metric": "ell_spmv_gbs_q1_2049_f64", "value": round(value, 2), "unit": "GB/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": round(ms_max / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Q1 Poisson 2049^2, x ~ U[-1,1])",
+            "config": {"workload": "ell_spmv_q1_2049_f64", "rows": n, "nnz": nnz, "spmv_per_step": SPMV_PER_STEP,
+                       "bytes_per_spmv": nbytes, "parallelism": f"replicas{ws}",
+                       "l2": "matrix 453 MB > L2 each application; no flush (x stays L2-resident by design)"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_src,
+                         "traffic": profile_traffic("ell_spmv_q1_2049_f64"),
+                         "kernel": "ell_spmv_kernel<double,9,false>"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": n * 8,
+                    "d2h_bytes_per_step": n * 8, "api": "honei_b200.la.Product.value (C ABI hb_spmv_f64)"},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "extra": {"spmv_f32_gbs": round(gbs32, 2), "cg_257": cg_extra},
+        }
+        print(json.dumps(line), flush=True)
+    barrier()
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,263 @@
+// hb_cg.cu -- CGSolver<Tag, methods::NONE> (honei/math/cg.hh:63-133) as one persistent
+// cooperative kernel.
+//
+// The reference runs 7 launches, 2 device->host scalar round trips and 2 cudaMalloc/cudaFree
+// pairs per iteration (honei/la/*-cuda.cc).  Here the loop, its scalars and its stopping test
+// live on the device; per iteration there are two phases separated by grid barriers:
+//
+//   phase 1  p_i = r_i + beta * p_i  (computed on the fly for every gathered column, so the
+//            separate Scale+Sum passes disappear), v = A p, partial v.p
+//   phase 2  lambda = alpha / v.p;  x += lambda p;  r += (-lambda) v;  partial r.r
+//
+// p is double-buffered (phase 1 gathers the old p of neighbour rows while writing the new p
+// of its own rows).  Every elementwise formula rounds exactly as cg.hh's operator sequence
+// (ScaledSum, Scale, Sum) does on tags::CPU; the two dot products use a fixed-order tree
+// (block partials, then every block sums all partials in the same order), so each block
+// computes bit-identical scalars and takes the same branch at the stopping test.
+#include "hb_spmv_core.cuh"
+
+#include <cfloat>
+
+namespace {
+
+constexpr int CG_THREADS = 512;
+
+template <typename T> struct CGParams {
+    int64_t rows, ld;
+    int K;
+    const int32_t *Aj;
+    const T *Ax;
+    const T *b_user;
+    T *x_user;
+    T *x, *r, *p0, *p1, *v;    // padded work vectors, ld entries each
+    int64_t max_iters;
+    T eps;
+    T *partials;                // 2 * gridDim.x
+    hbd::GridBarrier bar;
+    hb_solve_result *res;
+};
+
+template <typename T> __device__ __forceinline__ T eps_mach();
+template <> __device__ __forceinline__ double eps_mach<double>() { return DBL_EPSILON; }
+template <> __device__ __forceinline__ float eps_mach<float>() { return FLT_EPSILON; }
+__device__ __forceinline__ double dsqrt(double v) { return __dsqrt_rn(v); }
+__device__ __forceinline__ float dsqrt(float v) { return __fsqrt_rn(v); }
+
+// Sum of the gridDim.x block partials in a fixed tree order; identical in every block.
+template <typename T>
+__device__ __forceinline__ T grid_total(const T *part, T *red, T *bcast)
+{
+    T v = T(0);
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) v = hbd::add(v, __ldcg(part + i));
+    v = hbd::block_sum(v, red);
+    if (threadIdx.x == 0) *bcast = v;
+    __syncthreads();
+    return *bcast;
+}
+
+template <typename T, int KT>
+__global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
+{
+    using hbd::add; using hbd::mul; using hbd::sub;
+    __shared__ T red[32];
+    __shared__ T bcast;
+    __shared__ int s_flag;
+    const unsigned G = gridDim.x;
+    const int64_t groups = P.ld / 4;
+    const int64_t gpb = (groups + G - 1) / G;
+    const int64_t g_lo = (int64_t)blockIdx.x * gpb;
+    const int64_t g_hi = min(groups, g_lo + gpb);
+    T *slotA = P.partials, *slotB = P.partials + G;
+    const int64_t rows = P.rows;
+    bool ok = true;
+
+    // x (padded with zeros) from the caller's x0
+    for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+        T xv[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) xv[i] = (4 * g + i < rows) ? P.x_user[4 * g + i] : T(0);
+        hbd::st4(P.x + 4 * g, xv);
+    }
+    ok = P.bar.sync(G, &s_flag);
+
+    // r = b - A x (Defect), alpha = r.r (Norm<l2, false>)
+    T acc = T(0);
+    if (ok) {
+        const T *xw = P.x;
+        for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+            T s[4], rv[4];
+            hbd::ell_rows4<T, KT>(P.Aj, P.Ax, P.ld, P.K, 4 * g, [&](int32_t j) { return __ldcg(xw + j); }, s);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const T bb = (4 * g + i < rows) ? P.b_user[4 * g + i] : T(0);
+                rv[i] = sub(bb, s[i]);
+                acc = add(acc, mul(rv[i], rv[i]));
+            }
+            hbd::st4(P.r + 4 * g, rv);
+        }
+        acc = hbd::block_sum(acc, red);
+        if (threadIdx.x == 0) slotB[blockIdx.x] = acc;
+        ok = P.bar.sync(G, &s_flag);
+    }
+    T alpha = ok ? grid_total(slotB, red, &bcast) : T(0);
+    const T initial_defect = dsqrt(alpha);
+    T current_defect = T(0);
+    T beta = T(0);
+    const T epsm = eps_mach<T>();
+    T *pin = P.p0, *pout = P.p1;
+    int64_t it = 0, used = 0;
+    while (ok && it < P.max_iters) {
+        // ---- phase 1: p = beta p + r (first iteration: p = r), v = A p, v.p
+        const T *rw = P.r, *pw = pin;
+        const bool first = (it == 0);
+        acc = T(0);
+        for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+            T s[4];
+            hbd::ell_rows4<T, KT>(P.Aj, P.Ax, P.ld, P.K, 4 * g, [&](int32_t j) {
+                const T rj = __ldcg(rw + j);
+                return first ? rj : add(mul(__ldcg(pw + j), beta), rj);
+            }, s);
+            T rv[4], pv[4], pn[4];
+            hbd::ld4(P.r + 4 * g, rv);
+            hbd::ld4(pin + 4 * g, pv);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                pn[i] = first ? rv[i] : add(mul(pv[i], beta), rv[i]);
+                acc = add(acc, mul(s[i], pn[i]));
+            }
+            hbd::st4(pout + 4 * g, pn);
+            hbd::st4(P.v + 4 * g, s);
+        }
+        acc = hbd::block_sum(acc, red);
+        if (threadIdx.x == 0) slotA[blockIdx.x] = acc;
+        if (!P.bar.sync(G, &s_flag)) break;
+        const T temp = grid_total(slotA, red, &bcast);
+        const T lambda = alpha / (fabs(temp) > epsm ? temp : epsm);
+        const T mlambda = -lambda;
+
+        // ---- phase 2: x += lambda p; r += (-lambda) v; alpha = r.r
+        acc = T(0);
+        for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+            T xv[4], pv[4], rv[4], vv[4];
+            hbd::ld4(P.x + 4 * g, xv);
+            hbd::ld4(pout + 4 * g, pv);
+            hbd::ld4(P.r + 4 * g, rv);
+            hbd::ld4(P.v + 4 * g, vv);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                xv[i] = add(xv[i], mul(lambda, pv[i]));
+                rv[i] = add(rv[i], mul(mlambda, vv[i]));
+                acc = add(acc, mul(rv[i], rv[i]));
+            }
+            hbd::st4(P.x + 4 * g, xv);
+            hbd::st4(P.r + 4 * g, rv);
+        }
+        acc = hbd::block_sum(acc, red);
+        if (threadIdx.x == 0) slotB[blockIdx.x] = acc;
+        if (!P.bar.sync(G, &s_flag)) break;
+        const T alpha_old = alpha;
+        alpha = grid_total(slotB, red, &bcast);
+        beta = alpha / (fabs(alpha_old) > epsm ? alpha_old : epsm);
+        T *t = pin; pin = pout; pout = t;
+        ++it;
+        current_defect = dsqrt(alpha);
+        if (current_defect < P.eps * initial_defect) { used = it; break; }
+        if (current_defect < P.eps) { used = it; break; }
+        if (it == P.max_iters) used = it;
+    }
+    // x back to the caller (own rows)
+    for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x)
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (4 * g + i < rows) P.x_user[4 * g + i] = P.x[4 * g + i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        P.res->used = used;
+        P.res->defect0 = (double)initial_defect;
+        P.res->defect = (double)current_defect;
+        P.res->status = *(volatile int *)P.bar.status;
+    }
+}
+
+template <typename T, int KT>
+int launch_cg_kt(hb_context *ctx, CGParams<T> &P, int blocks)
+{
+    void *args[] = {&P};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *)cg_kernel<T, KT>, dim3(blocks), dim3(CG_THREADS),
+                                                args, 0, ctx->stream);
+    if (e != cudaSuccess) { hb_note_error(ctx, e, "cudaLaunchCooperativeKernel(cg_kernel)"); return HB_ERR_CUDA; }
+    return hb_check_launch(ctx, "cg_kernel");
+}
+
+template <typename T, int KT>
+int cg_max_blocks(hb_context *ctx)
+{
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, cg_kernel<T, KT>, CG_THREADS, 0);
+    return std::max(1, occ) * ctx->num_sms;
+}
+
+template <typename T>
+int cg_impl(hb_context *ctx, const hb_ell *A, const T *b, T *x, int64_t max_iters, T eps,
+            int64_t *used_iters, T *final_defect, int dtype)
+{
+    if (!ctx || !A || !b || !x || !used_iters || max_iters < 0) return HB_ERR_INVALID;
+    if (A->dtype != dtype || !A->Aj || !A->Ax || A->ld % 64 || A->ld < A->rows) return HB_ERR_INVALID;
+    if (A->rows != A->cols) return HB_ERR_SIZE;
+    if (A->rows > INT32_MAX) return HB_ERR_UNSUPPORTED;
+    const int64_t ld = A->ld;
+    int st = hb_ensure_work(ctx, (size_t)ld * sizeof(T) * 5);
+    if (st) return st;
+    CGParams<T> P;
+    P.rows = A->rows;
+    P.ld = ld;
+    P.K = (int)A->K;
+    P.Aj = A->Aj;
+    P.Ax = (const T *)A->Ax;
+    P.b_user = b;
+    P.x_user = x;
+    T *w = (T *)ctx->work;
+    P.x = w; P.r = w + ld; P.p0 = w + 2 * ld; P.p1 = w + 3 * ld; P.v = w + 4 * ld;
+    P.max_iters = max_iters;
+    P.eps = eps;
+    P.partials = (T *)hb_partials(ctx);
+    unsigned *bar = hb_bar(ctx);
+    P.bar.count = bar;
+    P.bar.gen = bar + 1;
+    P.bar.status = (int *)(bar + 2);
+    P.res = hb_result(ctx);
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), ctx->stream));
+
+    const int64_t groups = ld / 4;
+    const bool k9 = (A->K == 9);
+    const int maxb = k9 ? cg_max_blocks<T, 9>(ctx) : cg_max_blocks<T, 0>(ctx);
+    // about one row group per thread for small systems; all co-resident blocks otherwise
+    int64_t want = (groups + CG_THREADS - 1) / CG_THREADS;
+    int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(maxb, 4096)));
+    st = k9 ? launch_cg_kt<T, 9>(ctx, P, blocks) : launch_cg_kt<T, 0>(ctx, P, blocks);
+    if (st) return st;
+    hb_solve_result *h = (hb_solve_result *)ctx->pinned;
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, P.res, sizeof(hb_solve_result), cudaMemcpyDeviceToHost, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h->status == HB_DEV_TIMEOUT) return HB_ERR_TIMEOUT;
+    *used_iters = h->used;
+    if (final_defect) *final_defect = (T)h->defect;
+    return HB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hb_cg_f64(hb_context *ctx, const hb_ell *A, const double *b, double *x, int64_t max_iters,
+              double eps, int64_t *used_iters, double *final_defect)
+{
+    return cg_impl<double>(ctx, A, b, x, max_iters, eps, used_iters, final_defect, HB_F64);
+}
+
+int hb_cg_f32(hb_context *ctx, const hb_ell *A, const float *b, float *x, int64_t max_iters,
+              float eps, int64_t *used_iters, float *final_defect)
+{
+    return cg_impl<float>(ctx, A, b, x, max_iters, eps, used_iters, final_defect, HB_F32);
+}
+
+}  // extern "C"

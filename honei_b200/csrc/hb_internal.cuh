@@ -1,0 +1,209 @@
+// hb_internal.cuh -- shared device helpers and the context structure of libhonei_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <mutex>
+
+#include "../../include/honei_b200.h"
+
+#define HB_CUDA_TRY(ctx, call)                                                   \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) { hb_note_error((ctx), e_, #call); return HB_ERR_CUDA; } \
+    } while (0)
+
+#define HB_CHECK(cond, code) do { if (!(cond)) return (code); } while (0)
+
+// Device-side status word values (written by bounded waits and input checks).
+enum { HB_DEV_OK = 0, HB_DEV_TIMEOUT = 1, HB_DEV_NONFINITE = 2 };
+
+// Bounded wait: a grid barrier gives up after this many nanoseconds (2 s) and reports
+// HB_ERR_TIMEOUT; no legitimate phase of any kernel here comes close.
+static constexpr uint64_t HB_WAIT_NS = 2000000000ull;
+
+// Scalars a solver kernel reports back (one pinned-host readback per solve).
+struct hb_solve_result {
+    int64_t used;
+    double defect0;
+    double defect;
+    int32_t status;
+    int32_t pad;
+};
+
+struct hb_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 148;
+    // device scratch: reduction partials, barrier words, solver results
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    // device work vectors for solvers (grown on demand, or by hb_reserve)
+    void *work = nullptr;
+    size_t work_bytes = 0;
+    // pinned host slot for scalar readback
+    void *pinned = nullptr;
+    uint64_t launches = 0;
+    std::string last_error;
+};
+
+void hb_note_error(hb_context *ctx, cudaError_t e, const char *what);
+int hb_ensure_work(hb_context *ctx, size_t bytes);
+int hb_check_launch(hb_context *ctx, const char *what);
+
+// Scratch map (bytes from ctx->scratch): partial sums, barrier words, result slots.
+static constexpr size_t HB_PARTIALS = 8192;                    // doubles
+static constexpr size_t HB_OFF_PARTIALS = 0;
+static constexpr size_t HB_OFF_BAR = HB_PARTIALS * 8;          // 64 unsigned words
+static constexpr size_t HB_OFF_RESULT = HB_OFF_BAR + 256;      // hb_solve_result[16]
+static constexpr size_t HB_OFF_SCALAR = HB_OFF_RESULT + 16 * sizeof(hb_solve_result);
+static constexpr size_t HB_SCRATCH_BYTES = HB_OFF_SCALAR + 4096;
+
+inline double *hb_partials(hb_context *c) { return (double *)((char *)c->scratch + HB_OFF_PARTIALS); }
+inline unsigned *hb_bar(hb_context *c) { return (unsigned *)((char *)c->scratch + HB_OFF_BAR); }
+inline hb_solve_result *hb_result(hb_context *c) { return (hb_solve_result *)((char *)c->scratch + HB_OFF_RESULT); }
+inline double *hb_scalars(hb_context *c) { return (double *)((char *)c->scratch + HB_OFF_SCALAR); }
+
+inline int64_t hb_round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+// --------------------------------------------------------------------------------------
+// Device helpers
+// --------------------------------------------------------------------------------------
+namespace hbd {
+
+// One rounding per multiply and per add (no FMA contraction): the reference's CPU order.
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+
+template <typename T> struct vec4;
+template <> struct vec4<double> { double2 a, b; };
+template <> struct vec4<float> { float4 a; };
+
+// Streaming (evict-first) 4-wide loads of matrix data: the matrix is touched once per
+// operator application, the vectors are the reusable part of L2.
+__device__ __forceinline__ void ld4_stream(const double *p, double (&v)[4])
+{
+    double2 a = __ldcs(reinterpret_cast<const double2 *>(p));
+    double2 b = __ldcs(reinterpret_cast<const double2 *>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void ld4_stream(const float *p, float (&v)[4])
+{
+    float4 a = __ldcs(reinterpret_cast<const float4 *>(p));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void ld4_stream(const int32_t *p, int32_t (&v)[4])
+{
+    int4 a = __ldcs(reinterpret_cast<const int4 *>(p));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+// Cached 4-wide loads / stores of padded work vectors (16-byte aligned by construction).
+__device__ __forceinline__ void ld4(const double *p, double (&v)[4])
+{
+    double2 a = *reinterpret_cast<const double2 *>(p);
+    double2 b = *(reinterpret_cast<const double2 *>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void ld4(const float *p, float (&v)[4])
+{
+    float4 a = *reinterpret_cast<const float4 *>(p);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void st4(double *p, const double (&v)[4])
+{
+    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void st4(float *p, const float (&v)[4])
+{
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned *p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t globaltimer()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Warp tree sum in a fixed order (shuffle-down halving): deterministic.
+template <typename T> __device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = add(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block sum in a fixed order; result valid in thread 0.  smem: >= 32 entries.
+template <typename T> __device__ __forceinline__ T block_sum(T v, T *smem)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) smem[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < nwarps ? smem[lane] : T(0);
+        v = warp_sum(v);
+    }
+    return v;
+}
+
+// Grid barrier for cooperative (co-resident) launches: generation counter + arrival count.
+// Every wait is bounded (HB_WAIT_NS); on timeout the status word gets HB_DEV_TIMEOUT and all
+// blocks return false, so the kernel ends instead of hanging.
+struct GridBarrier {
+    unsigned *count;
+    unsigned *gen;
+    int *status;
+
+    __device__ __forceinline__ bool sync(unsigned nblocks, int *s_flag) const
+    {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int ok = 1;
+            const unsigned g = ld_acquire(gen);
+            __threadfence();
+            const unsigned arrived = atomicAdd(count, 1u);
+            if (arrived == nblocks - 1) {
+                atomicExch(count, 0u);
+                __threadfence();
+                st_release(gen, g + 1);
+            } else {
+                const uint64_t t0 = globaltimer();
+                while (ld_acquire(gen) == g) {
+                    if (*(volatile int *)status != HB_DEV_OK) { ok = 0; break; }
+                    if (globaltimer() - t0 > HB_WAIT_NS) {
+                        atomicCAS(status, HB_DEV_OK, HB_DEV_TIMEOUT);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            __threadfence();
+            if (*(volatile int *)status != HB_DEV_OK) ok = 0;
+            *s_flag = ok;
+        }
+        __syncthreads();
+        return *(volatile int *)s_flag != 0;
+    }
+};
+
+}  // namespace hbd

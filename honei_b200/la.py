@@ -1,0 +1,350 @@
+"""Host-side mirror of HONEI's tag-dispatched operator API for the B200 backend.
+
+The C++ plugin (honei_b200/plugin) is the drop-in for HONEI itself; this module offers the
+same operators to Python callers, with the reference's names, argument order and error
+behaviour (size mismatches raise ``VectorSizeDoesNotMatch`` before anything is launched, as
+honei/la/product.hh:154-161 does).  Dense vectors are CUDA ``torch.Tensor`` objects (float64
+or float32, contiguous): torch provides device memory and streams only; every operation runs
+in libhonei_b200.so.
+
+    A = SparseMatrixELL.from_reference(ell)        # problems.EllMatrix, reference layout
+    Product.value(y, A, x)                           # Product<tags::GPU::CUDA>::value
+    r = Defect.value(r, b, A, x)
+    d = DotProduct.value(x, y); n = Norm.value(x, root=True)
+    used = CGSolver.value(A, None, b, x, max_iters=10000, eps_relative=1e-8)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import HbEll, check, lib
+
+
+class VectorSizeDoesNotMatch(ValueError):
+    """honei/la/vector_error.hh: VectorSizeDoesNotMatch(size, expected)."""
+
+    def __init__(self, size, expected):
+        super().__init__(f"Vector size does not match: {size} != {expected}")
+
+
+class MatrixRowsDoNotMatch(ValueError):
+    """honei/la/matrix_error.hh: MatrixRowsDoNotMatch(rows, expected)."""
+
+    def __init__(self, rows, expected):
+        super().__init__(f"Matrix rows do not match: {rows} != {expected}")
+
+
+_DT = {torch.float64: 0, torch.float32: 1}
+_SUF = {torch.float64: "f64", torch.float32: "f32"}
+
+
+class Context:
+    """An hb_context bound to one device and (by default) torch's current stream."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        h = C.c_void_p()
+        check(lib().hb_create(C.byref(h), device), "hb_create")
+        self.handle = h
+        self.bind_stream()
+
+    def bind_stream(self, stream=None):
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        check(lib().hb_set_stream(self.handle, C.c_void_p(s.cuda_stream)), "hb_set_stream", self.handle)
+
+    def launches(self) -> int:
+        return int(lib().hb_launch_count(self.handle))
+
+    def reserve(self, n: int) -> None:
+        check(lib().hb_reserve(self.handle, n), "hb_reserve", self.handle)
+
+    def synchronize(self):
+        check(lib().hb_synchronize(self.handle), "hb_synchronize", self.handle)
+
+    def close(self):
+        if self.handle:
+            lib().hb_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_ctx_lock = threading.Lock()
+_ctx_by_dev: dict[int, Context] = {}
+
+
+def default_context(device: int | None = None) -> Context:
+    dev = torch.cuda.current_device() if device is None else device
+    with _ctx_lock:
+        c = _ctx_by_dev.get(dev)
+        if c is None:
+            c = _ctx_by_dev[dev] = Context(dev)
+        c.bind_stream()
+        return c
+
+
+def _vec(t: torch.Tensor, dtype, name: str) -> int:
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} has dtype {t.dtype}, expected {dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    return t.data_ptr()
+
+
+class SparseMatrixELL:
+    """Device mirror of a HONEI SparseMatrixELL (honei/la/sparse_matrix_ell.hh:44-129)."""
+
+    def __init__(self, rows, cols, K, ld, Aj: torch.Tensor, Ax: torch.Tensor):
+        self._rows, self._cols, self.K, self.ld = int(rows), int(cols), int(K), int(ld)
+        self.Aj, self.Ax = Aj, Ax
+        self.dtype = Ax.dtype
+        self._s = HbEll(self._rows, self._cols, self.K, self.ld, Aj.data_ptr(), Ax.data_ptr(),
+                        _DT[Ax.dtype], 0)
+
+    def rows(self) -> int:
+        return self._rows
+
+    def columns(self) -> int:
+        return self._cols
+
+    @property
+    def struct(self) -> HbEll:
+        return self._s
+
+    @staticmethod
+    def layout(rows, ncpr, threads=1):
+        K, ld = C.c_int64(), C.c_int64()
+        check(lib().hb_ell_layout(rows, ncpr, threads, C.byref(K), C.byref(ld)), "hb_ell_layout")
+        return K.value, ld.value
+
+    @classmethod
+    def from_reference(cls, ell, ctx: Context | None = None, device="cuda") -> "SparseMatrixELL":
+        """Uploads the reference-layout arrays (u64 Aj, Ax, u64 Arl) and imports them."""
+        ctx = ctx or default_context()
+        dt = torch.float64 if ell.Ax.dtype == np.float64 else torch.float32
+        K, ld = cls.layout(ell.rows, ell.ncpr, ell.threads)
+        Aj_ref = torch.from_numpy(ell.Aj.view(np.int64)).to(device)
+        Ax_ref = torch.from_numpy(ell.Ax).to(device)
+        Arl = torch.from_numpy(ell.Arl.view(np.int64)).to(device)
+        Aj = torch.empty(K * ld, dtype=torch.int32, device=device)
+        Ax = torch.empty(K * ld, dtype=dt, device=device)
+        out = HbEll(ell.rows, ell.cols, K, ld, Aj.data_ptr(), Ax.data_ptr(), _DT[dt], 0)
+        fn = lib().hb_ell_import_f64 if dt == torch.float64 else lib().hb_ell_import_f32
+        check(fn(ctx.handle, ell.rows, ell.cols, ell.stride, ell.ncpr, ell.threads, Aj_ref.data_ptr(),
+                 Ax_ref.data_ptr(), Arl.data_ptr(), C.byref(out)), "hb_ell_import", ctx.handle)
+        return cls(ell.rows, ell.cols, K, ld, Aj, Ax)
+
+    @classmethod
+    def q1_poisson(cls, M: int, coef: torch.Tensor | None = None, ctx: Context | None = None,
+                   device="cuda") -> "SparseMatrixELL":
+        """Q1 Poisson (Dirichlet rows identity) assembled on the device, FP64."""
+        ctx = ctx or default_context()
+        N = M * M
+        K, ld = cls.layout(N, 9, 1)
+        Aj = torch.empty(K * ld, dtype=torch.int32, device=device)
+        Ax = torch.empty(K * ld, dtype=torch.float64, device=device)
+        out = HbEll(N, N, K, ld, Aj.data_ptr(), Ax.data_ptr(), 0, 0)
+        cptr = None
+        if coef is not None:
+            cptr = _vec(coef, torch.float64, "coef")
+            if coef.numel() != (M - 1) * (M - 1):
+                raise VectorSizeDoesNotMatch(coef.numel(), (M - 1) * (M - 1))
+        check(lib().hb_q1_assemble_f64(ctx.handle, M, cptr, C.byref(out)), "hb_q1_assemble_f64", ctx.handle)
+        return cls(N, N, K, ld, Aj, Ax)
+
+    def to_float(self, ctx: Context | None = None) -> "SparseMatrixELL":
+        """Same pattern with FP32 values (the reference fills FP32 matrices from FP64 values)."""
+        ctx = ctx or default_context()
+        Ax = torch.empty(self.K * self.ld, dtype=torch.float32, device=self.Ax.device)
+        Aj = torch.empty_like(self.Aj)
+        dst = HbEll(self._rows, self._cols, self.K, self.ld, Aj.data_ptr(), Ax.data_ptr(), 1, 0)
+        check(lib().hb_ell_cast_f64_f32(ctx.handle, C.byref(self._s), C.byref(dst)), "hb_ell_cast", ctx.handle)
+        return SparseMatrixELL(self._rows, self._cols, self.K, self.ld, Aj, Ax)
+
+
+class Product:
+    """Product<tags::GPU::CUDA>::value(y, A, x): y = A x (honei/la/product.hh:1758-1760)."""
+
+    @staticmethod
+    def value(y: torch.Tensor, A: SparseMatrixELL, x: torch.Tensor, ctx: Context | None = None):
+        if x.numel() != A.columns():
+            raise VectorSizeDoesNotMatch(x.numel(), A.columns())
+        if A.rows() != y.numel():
+            raise VectorSizeDoesNotMatch(A.rows(), y.numel())
+        ctx = ctx or default_context()
+        fn = getattr(lib(), f"hb_spmv_{_SUF[A.dtype]}")
+        check(fn(ctx.handle, C.byref(A.struct), _vec(x, A.dtype, "x"), _vec(y, A.dtype, "y")), "Product", ctx.handle)
+        return y
+
+
+class Defect:
+    """Defect<tags::GPU::CUDA>::value(r, b, A, x): r = b - A x (honei/math/defect.hh:660-670)."""
+
+    @staticmethod
+    def value(r: torch.Tensor, b: torch.Tensor, A: SparseMatrixELL, x: torch.Tensor, ctx: Context | None = None):
+        if x.numel() != A.columns():
+            raise VectorSizeDoesNotMatch(x.numel(), A.columns())
+        if b.numel() != A.columns():
+            raise VectorSizeDoesNotMatch(b.numel(), A.columns())
+        if r.numel() != A.rows():
+            raise VectorSizeDoesNotMatch(r.numel(), A.rows())
+        ctx = ctx or default_context()
+        fn = getattr(lib(), f"hb_defect_{_SUF[A.dtype]}")
+        check(fn(ctx.handle, C.byref(A.struct), _vec(b, A.dtype, "b"), _vec(x, A.dtype, "x"),
+                 _vec(r, A.dtype, "r")), "Defect", ctx.handle)
+        return r
+
+
+def _pair(x, y):
+    if x.numel() != y.numel():
+        raise VectorSizeDoesNotMatch(y.numel(), x.numel())
+
+
+class DotProduct:
+    """DotProduct<tags::GPU::CUDA>::value(x, y) -> scalar (honei/la/dot_product.hh:358-360)."""
+
+    @staticmethod
+    def value(x: torch.Tensor, y: torch.Tensor, ctx: Context | None = None) -> float:
+        _pair(x, y)
+        ctx = ctx or default_context()
+        out = C.c_double() if x.dtype == torch.float64 else C.c_float()
+        fn = getattr(lib(), f"hb_dot_{_SUF[x.dtype]}")
+        check(fn(ctx.handle, x.numel(), _vec(x, x.dtype, "x"), _vec(y, x.dtype, "y"), C.byref(out)),
+              "DotProduct", ctx.handle)
+        return out.value
+
+
+class Norm:
+    """Norm<vnt_l_two, root, tags::GPU::CUDA>::value(x); root=False returns the squared norm."""
+
+    @staticmethod
+    def value(x: torch.Tensor, root: bool = False, ctx: Context | None = None) -> float:
+        ctx = ctx or default_context()
+        out = C.c_double() if x.dtype == torch.float64 else C.c_float()
+        fn = getattr(lib(), f"hb_norm_l2_{_SUF[x.dtype]}")
+        check(fn(ctx.handle, x.numel(), _vec(x, x.dtype, "x"), int(root), C.byref(out)), "Norm", ctx.handle)
+        return out.value
+
+
+class ScaledSum:
+    """ScaledSum<tags::GPU::CUDA>::value(x, y, b): x += b y;  value(r, x, y, b): r = x + b y."""
+
+    @staticmethod
+    def value(*args, ctx: Context | None = None):
+        ctx = ctx or default_context()
+        if len(args) == 3:
+            x, y, b = args
+            _pair(x, y)
+            fn = getattr(lib(), f"hb_scaled_sum_{_SUF[x.dtype]}")
+            check(fn(ctx.handle, x.numel(), _vec(x, x.dtype, "x"), _vec(y, x.dtype, "y"), b), "ScaledSum", ctx.handle)
+            return x
+        r, x, y, b = args
+        _pair(x, y)
+        _pair(x, r)
+        fn = getattr(lib(), f"hb_scaled_sum3_{_SUF[x.dtype]}")
+        check(fn(ctx.handle, x.numel(), _vec(r, x.dtype, "r"), _vec(x, x.dtype, "x"), _vec(y, x.dtype, "y"), b),
+              "ScaledSum", ctx.handle)
+        return r
+
+
+class Scale:
+    """Scale<tags::GPU::CUDA>::value(x, a): x *= a (honei/la/scale.hh:263)."""
+
+    @staticmethod
+    def value(x: torch.Tensor, a: float, ctx: Context | None = None):
+        ctx = ctx or default_context()
+        fn = getattr(lib(), f"hb_scale_{_SUF[x.dtype]}")
+        check(fn(ctx.handle, x.numel(), _vec(x, x.dtype, "x"), a), "Scale", ctx.handle)
+        return x
+
+
+class Sum:
+    """Sum<tags::GPU::CUDA>::value(x, y): x += y (honei/la/sum.hh:684)."""
+
+    @staticmethod
+    def value(x: torch.Tensor, y: torch.Tensor, ctx: Context | None = None):
+        _pair(x, y)
+        ctx = ctx or default_context()
+        fn = getattr(lib(), f"hb_sum_{_SUF[x.dtype]}")
+        check(fn(ctx.handle, x.numel(), _vec(x, x.dtype, "x"), _vec(y, x.dtype, "y")), "Sum", ctx.handle)
+        return x
+
+
+class Difference:
+    """Difference: r = x - y."""
+
+    @staticmethod
+    def value(r: torch.Tensor, x: torch.Tensor, y: torch.Tensor, ctx: Context | None = None):
+        _pair(x, y)
+        _pair(x, r)
+        ctx = ctx or default_context()
+        fn = getattr(lib(), f"hb_difference_{_SUF[x.dtype]}")
+        check(fn(ctx.handle, x.numel(), _vec(r, x.dtype, "r"), _vec(x, x.dtype, "x"), _vec(y, x.dtype, "y")),
+              "Difference", ctx.handle)
+        return r
+
+
+class ElementProduct:
+    """ElementProduct: r = x * y elementwise (the Jacobi apply Product(DV, DV, DV))."""
+
+    @staticmethod
+    def value(r: torch.Tensor, x: torch.Tensor, y: torch.Tensor, ctx: Context | None = None):
+        _pair(x, y)
+        _pair(x, r)
+        ctx = ctx or default_context()
+        fn = getattr(lib(), f"hb_element_product_{_SUF[x.dtype]}")
+        check(fn(ctx.handle, x.numel(), _vec(r, x.dtype, "r"), _vec(x, x.dtype, "x"), _vec(y, x.dtype, "y")),
+              "ElementProduct", ctx.handle)
+        return r
+
+
+def convert(dst: torch.Tensor, src: torch.Tensor, ctx: Context | None = None):
+    """convert<Tag>(copy, orig) (honei/la/algorithm.hh:163-198): FP64 <-> FP32."""
+    _pair(dst, src)
+    ctx = ctx or default_context()
+    if src.dtype == torch.float64 and dst.dtype == torch.float32:
+        check(lib().hb_convert_f64_f32(ctx.handle, src.numel(), dst.data_ptr(), _vec(src, src.dtype, "src")),
+              "convert", ctx.handle)
+    elif src.dtype == torch.float32 and dst.dtype == torch.float64:
+        check(lib().hb_convert_f32_f64(ctx.handle, src.numel(), dst.data_ptr(), _vec(src, src.dtype, "src")),
+              "convert", ctx.handle)
+    else:
+        raise TypeError("convert needs one float64 and one float32 vector")
+    return dst
+
+
+class CGSolver:
+    """CGSolver<tags::GPU::CUDA, methods::NONE>::value (honei/math/cg.hh:63-133).
+
+    ``value(A, P, b, x, max_iters, eps_relative=1e-8)`` solves in place into x (x holds x0)
+    and returns used_iters; ``last_defect`` holds sqrt(alpha) at exit.
+    """
+
+    last_defect = None
+
+    @staticmethod
+    def value(A: SparseMatrixELL, P, b: torch.Tensor, x: torch.Tensor, max_iters: int,
+              eps_relative: float = 1e-8, ctx: Context | None = None) -> int:
+        if b.numel() != A.rows():
+            raise VectorSizeDoesNotMatch(b.numel(), A.rows())
+        if x.numel() != A.columns():
+            raise VectorSizeDoesNotMatch(x.numel(), A.columns())
+        ctx = ctx or default_context()
+        used = C.c_int64(0)
+        d = C.c_double() if A.dtype == torch.float64 else C.c_float()
+        fn = getattr(lib(), f"hb_cg_{_SUF[A.dtype]}")
+        check(fn(ctx.handle, C.byref(A.struct), _vec(b, A.dtype, "b"), _vec(x, A.dtype, "x"), int(max_iters),
+                 eps_relative, C.byref(used), C.byref(d)), "CGSolver", ctx.handle)
+        CGSolver.last_defect = d.value
+        return used.value

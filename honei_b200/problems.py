@@ -1,0 +1,288 @@
+"""Seeded problem generators for the HONEI sparse-solver path (host side, numpy).
+
+Every matrix is produced in the reference's SparseMatrixELL layout
+(honei/la/sparse_matrix_ell-impl.hh:75-122): entry k of row r at
+``(k % T) + r*T + (k // T)*stride``, ``stride = 32 * ceil(rows*T / 32)``,
+``Arl[r] = ceil(nnz_r / T)``, 64-bit column indices, columns ascending per row, explicit
+zeros dropped.  These arrays are exactly what HONEI's ``SparseMatrixELL`` holds, so they feed
+both the reference CPU path and the device import (``hb_ell_import_*``).
+
+Q1 Poisson with Dirichlet rows set to identity follows
+``FillMatrix<Tag, POISSON, DIRICHLET_0>`` (honei/math/fill_matrix.hh:37-77): interior rows
+carry the 9-point stencil 8/3 and -1/3 and keep their couplings to boundary nodes.  The
+variable-coefficient form assembles the bilinear element matrix
+``K_e = k_c/6 * [[4,-1,-2,-1],[-1,4,-1,-2],[-2,-1,4,-1],[-1,-2,-1,4]]`` per cell; with
+``k == 1`` it reproduces the constant stencil bit for bit (the sums are formed as
+``4*(k1+k2+k3+k4)/6``, ``-(ka+kb)/6`` and ``-2*kc/6``).
+
+MG transfer matrices follow ``Prolongation<Tag, methods::NONE>`` + ``ApplyDirichletBoundaries``
+(honei/math/prolongation.hh:42-139): bilinear interpolation, fine Dirichlet rows zeroed;
+the restriction is the transpose (``Transposition``, honei/math/transposition.hh:30-50).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+
+def ell_stride(rows: int, threads: int = 1) -> int:
+    """Row stride of the reference ELL layout (sparse_matrix_ell-impl.hh:97-98)."""
+    return 32 * ((rows * threads + 31) // 32)
+
+
+@dataclasses.dataclass
+class EllMatrix:
+    """A sparse matrix in the reference's SparseMatrixELL layout (host arrays)."""
+
+    rows: int
+    cols: int
+    stride: int
+    ncpr: int
+    threads: int
+    Aj: np.ndarray   # uint64[ncpr*stride]
+    Ax: np.ndarray   # float64 or float32 [ncpr*stride]
+    Arl: np.ndarray  # uint64[rows]
+    nnz: int = 0
+
+    @property
+    def dtype(self):
+        return self.Ax.dtype
+
+    def astype(self, dtype) -> "EllMatrix":
+        """Same pattern with values cast (the reference fills FP32 matrices from FP64 values)."""
+        return dataclasses.replace(self, Ax=self.Ax.astype(dtype))
+
+    def info(self) -> list[int]:
+        return [self.rows, self.cols, self.stride, self.ncpr, self.threads]
+
+    def to_csr(self):
+        """(indptr, indices, data) of the stored entries, per-row slot order."""
+        T, stride = self.threads, self.stride
+        counts = self.Arl.astype(np.int64) * T
+        indptr = np.zeros(self.rows + 1, np.int64)
+        np.cumsum(counts, out=indptr[1:])
+        row = np.repeat(np.arange(self.rows, dtype=np.int64), counts)
+        k = np.arange(indptr[-1], dtype=np.int64) - indptr[row]
+        pos = (k % T) + row * T + (k // T) * stride
+        return indptr, self.Aj[pos].astype(np.int64), self.Ax[pos]
+
+
+def ell_from_csr(rows: int, cols: int, indptr, indices, data, threads: int = 1,
+                 dtype=np.float64) -> EllMatrix:
+    """Packs a CSR matrix (ascending columns per row) into the reference ELL layout.
+
+    Zero values are dropped before packing, as the reference constructor does
+    (sparse_matrix_ell-impl.hh:108-119).
+    """
+    indptr = np.asarray(indptr, np.int64)
+    indices = np.asarray(indices, np.int64)
+    data = np.asarray(data)
+    keep = data != 0
+    row_of = np.repeat(np.arange(rows, dtype=np.int64), np.diff(indptr))
+    row_of, indices, data = row_of[keep], indices[keep], data[keep]
+    counts = np.bincount(row_of, minlength=rows).astype(np.int64)
+    T = int(threads)
+    maxc = int(counts.max()) if rows else 0
+    ncpr = max(1, maxc)
+    ncpr = int(math.ceil(ncpr / T))
+    stride = ell_stride(rows, T)
+    start = np.zeros(rows + 1, np.int64)
+    np.cumsum(counts, out=start[1:])
+    k = np.arange(len(indices), dtype=np.int64) - start[row_of]
+    pos = (k % T) + row_of * T + (k // T) * stride
+    Aj = np.zeros(ncpr * stride, np.uint64)
+    Ax = np.zeros(ncpr * stride, dtype)
+    Aj[pos] = indices.astype(np.uint64)
+    Ax[pos] = data.astype(dtype)
+    Arl = ((counts + T - 1) // T).astype(np.uint64)
+    return EllMatrix(rows, cols, stride, ncpr, T, Aj, Ax, Arl, int(len(indices)))
+
+
+def q1_poisson_csr(M: int, coef=None):
+    """CSR of the Q1 Poisson matrix on an M x M node grid, Dirichlet rows = identity.
+
+    ``coef`` is None (unit coefficient) or an (M-1, M-1) array of per-cell coefficients.
+    Node r = i*M + j (lexicographic), as FillMatrix numbers them.
+    """
+    M = int(M)
+    N = M * M
+    if coef is None:
+        coef = np.ones((max(M - 1, 0), max(M - 1, 0)), np.float64)
+    coef = np.asarray(coef, np.float64)
+    ii, jj = np.divmod(np.arange(N, dtype=np.int64), M)
+    bnd = (ii == 0) | (ii == M - 1) | (jj == 0) | (jj == M - 1)
+    inner = np.nonzero(~bnd)[0]
+    counts = np.where(bnd, 1, 9).astype(np.int64)
+    indptr = np.zeros(N + 1, np.int64)
+    np.cumsum(counts, out=indptr[1:])
+    indices = np.empty(indptr[-1], np.int64)
+    data = np.empty(indptr[-1], np.float64)
+    b_rows = np.nonzero(bnd)[0]
+    indices[indptr[b_rows]] = b_rows
+    data[indptr[b_rows]] = 1.0
+    if len(inner):
+        i, j = ii[inner], jj[inner]
+        k_nw, k_ne = coef[i - 1, j - 1], coef[i - 1, j]
+        k_sw, k_se = coef[i, j - 1], coef[i, j]
+        six = 6.0
+        vals = [
+            -(2.0 * k_nw) / six,            # (i-1, j-1)
+            -(k_nw + k_ne) / six,           # (i-1, j)
+            -(2.0 * k_ne) / six,            # (i-1, j+1)
+            -(k_nw + k_sw) / six,           # (i,   j-1)
+            (4.0 * (((k_nw + k_ne) + k_sw) + k_se)) / six,  # diagonal
+            -(k_ne + k_se) / six,           # (i,   j+1)
+            -(2.0 * k_sw) / six,            # (i+1, j-1)
+            -(k_sw + k_se) / six,           # (i+1, j)
+            -(2.0 * k_se) / six,            # (i+1, j+1)
+        ]
+        offs = [-M - 1, -M, -M + 1, -1, 0, 1, M - 1, M, M + 1]
+        base = indptr[inner]
+        for s, (o, v) in enumerate(zip(offs, vals)):
+            indices[base + s] = inner + o
+            data[base + s] = v
+    return indptr, indices, data
+
+
+def q1_poisson(M: int, coef=None, threads: int = 1, dtype=np.float64) -> EllMatrix:
+    """Q1 Poisson ELL matrix (see module docstring); FP32 values are the FP64 values cast."""
+    indptr, indices, data = q1_poisson_csr(M, coef)
+    A = ell_from_csr(M * M, M * M, indptr, indices, data, threads, np.float64)
+    return A if dtype == np.float64 else A.astype(dtype)
+
+
+def log_uniform_coef(M: int, lo: float, hi: float, seed: int) -> np.ndarray:
+    """Per-cell coefficient 10**U(log10 lo, log10 hi) on the (M-1)^2 cells, seeded."""
+    rng = np.random.default_rng(seed)
+    return 10.0 ** rng.uniform(math.log10(lo), math.log10(hi), size=(M - 1, M - 1))
+
+
+def coarsen_coef(coef: np.ndarray) -> np.ndarray:
+    """Cell coefficients of the next coarser grid: mean of the 2x2 children."""
+    c = np.asarray(coef, np.float64)
+    return ((c[0::2, 0::2] + c[0::2, 1::2]) + (c[1::2, 0::2] + c[1::2, 1::2])) / 4.0
+
+
+def uniform_vector(n: int, seed: int, lo: float = -1.0, hi: float = 1.0) -> np.ndarray:
+    """Seeded U[lo, hi] vector (x_true, SpMV inputs)."""
+    return np.random.default_rng(seed).uniform(lo, hi, size=n)
+
+
+def permute_csr(n: int, indptr, indices, data, perm):
+    """A'[perm[i], perm[j]] = A[i, j], columns re-sorted ascending per row."""
+    perm = np.asarray(perm, np.int64)
+    indptr = np.asarray(indptr, np.int64)
+    counts = np.diff(indptr)
+    row = np.repeat(np.arange(n, dtype=np.int64), counts)
+    new_row = perm[row]
+    new_col = perm[np.asarray(indices, np.int64)]
+    order = np.lexsort((new_col, new_row))
+    new_counts = np.bincount(new_row, minlength=n)
+    new_indptr = np.zeros(n + 1, np.int64)
+    np.cumsum(new_counts, out=new_indptr[1:])
+    return new_indptr, new_col[order], np.asarray(data)[order]
+
+
+def random_permutation(n: int, seed: int) -> np.ndarray:
+    """Seeded Fisher-Yates permutation."""
+    return np.random.default_rng(seed).permutation(n)
+
+
+def q1_poisson_permuted(M: int, seed: int, coef=None, threads: int = 1, dtype=np.float64):
+    """(A', perm) with A'[perm[i], perm[j]] = A[i, j]; permute vectors with v'[perm] = v."""
+    indptr, indices, data = q1_poisson_csr(M, coef)
+    perm = random_permutation(M * M, seed)
+    p_indptr, p_indices, p_data = permute_csr(M * M, indptr, indices, data, perm)
+    A = ell_from_csr(M * M, M * M, p_indptr, p_indices, p_data, threads, np.float64)
+    return (A if dtype == np.float64 else A.astype(dtype)), perm
+
+
+def prolongation_csr(Mc: int):
+    """Bilinear Q1 prolongation from an Mc x Mc to a (2Mc-1)^2 grid, fine Dirichlet rows zero."""
+    Mc = int(Mc)
+    Mf = 2 * Mc - 1
+    Nf = Mf * Mf
+    I, J = np.divmod(np.arange(Nf, dtype=np.int64), Mf)
+    bnd = (I == 0) | (I == Mf - 1) | (J == 0) | (J == Mf - 1)
+    rows, cols, vals = [], [], []
+    ie, je = (I % 2 == 0), (J % 2 == 0)
+    ci0, cj0 = I // 2, J // 2
+    ci1, cj1 = (I + 1) // 2, (J + 1) // 2
+
+    def add(mask, ci, cj, w):
+        m = mask & ~bnd
+        r = np.nonzero(m)[0]
+        rows.append(r)
+        cols.append(ci[m] * Mc + cj[m])
+        vals.append(np.full(len(r), w))
+
+    add(ie & je, ci0, cj0, 1.0)
+    add(ie & ~je, ci0, cj0, 0.5)
+    add(ie & ~je, ci0, cj1, 0.5)
+    add(~ie & je, ci0, cj0, 0.5)
+    add(~ie & je, ci1, cj0, 0.5)
+    add(~ie & ~je, ci0, cj0, 0.25)
+    add(~ie & ~je, ci0, cj1, 0.25)
+    add(~ie & ~je, ci1, cj0, 0.25)
+    add(~ie & ~je, ci1, cj1, 0.25)
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    v = np.concatenate(vals)
+    order = np.lexsort((c, r))
+    r, c, v = r[order], c[order], v[order]
+    indptr = np.zeros(Nf + 1, np.int64)
+    np.cumsum(np.bincount(r, minlength=Nf), out=indptr[1:])
+    return Nf, Mc * Mc, indptr, c, v
+
+
+def transpose_csr(rows: int, cols: int, indptr, indices, data):
+    """CSR transpose with ascending columns per row (what Transposition produces)."""
+    indptr = np.asarray(indptr, np.int64)
+    r = np.repeat(np.arange(rows, dtype=np.int64), np.diff(indptr))
+    c = np.asarray(indices, np.int64)
+    order = np.lexsort((r, c))
+    t_indptr = np.zeros(cols + 1, np.int64)
+    np.cumsum(np.bincount(c, minlength=cols), out=t_indptr[1:])
+    return t_indptr, r[order], np.asarray(data)[order]
+
+
+@dataclasses.dataclass
+class MGHierarchy:
+    """Levels coarsest first (HONEI level 1 == index 0), as MGData stores them."""
+
+    A: list      # EllMatrix per level
+    prol: list   # EllMatrix, prol[l]: level l -> l+1
+    res: list    # EllMatrix, res[l] = prol[l]^T
+    sides: list  # grid side per level
+
+    def astype(self, dtype) -> "MGHierarchy":
+        return MGHierarchy([a.astype(dtype) for a in self.A], [p.astype(dtype) for p in self.prol],
+                           [r.astype(dtype) for r in self.res], list(self.sides))
+
+
+def mg_hierarchy(M: int, coarsest: int = 9, coef=None, threads: int = 1) -> MGHierarchy:
+    """Q1 Poisson hierarchy on sides M, (M+1)/2, ..., coarsest (all of the form 2^k + 1).
+
+    Coarser-level coefficients are the 2x2 means of the finer ones (rediscretisation).
+    """
+    sides = [int(M)]
+    while sides[-1] > coarsest:
+        if (sides[-1] - 1) % 2:
+            raise ValueError(f"grid side {sides[-1]} cannot be coarsened (need 2^k + 1)")
+        sides.append((sides[-1] + 1) // 2)
+    sides = sides[::-1]
+    coefs = [None] * len(sides)
+    if coef is not None:
+        coefs[-1] = np.asarray(coef, np.float64)
+        for l in range(len(sides) - 2, -1, -1):
+            coefs[l] = coarsen_coef(coefs[l + 1])
+    A = [q1_poisson(s, coefs[l], threads) for l, s in enumerate(sides)]
+    prol, res = [], []
+    for l in range(len(sides) - 1):
+        nf, nc, ip, ix, dv = prolongation_csr(sides[l])
+        prol.append(ell_from_csr(nf, nc, ip, ix, dv, threads))
+        t_ip, t_ix, t_dv = transpose_csr(nf, nc, ip, ix, dv)
+        res.append(ell_from_csr(nc, nf, t_ip, t_ix, t_dv, threads))
+    return MGHierarchy(A, prol, res, sides)

@@ -1,0 +1,184 @@
+/* honei_b200.h -- C ABI of the B200 (sm_100a) backend for HONEI's sparse iterative-solver path.
+ *
+ * Everything here is plain C: opaque handles, plain pointers, sizes and an int status.  No
+ * CUDA or torch types appear in the signatures (streams are passed as void* = cudaStream_t).
+ * Vectors and matrix arrays are DEVICE pointers unless a parameter says "host".
+ *
+ * Each entry point names the reference interface it replaces (paths within the HONEI tree).
+ * The reference's own GPU ABI is honei/backends/cuda/operations.hh:27-128 (e.g.
+ * cuda_product_smell_dv_double) behind the tag-dispatched operators Product<tags::GPU::CUDA>,
+ * Defect<...>, DotProduct<...>, Norm<...>, ScaledSum<...> and the solver templates CGSolver,
+ * RISmoother, MGSolver and IRSolver.  Results are bit-compatible with tags::CPU wherever the
+ * operation is elementwise or per-row (SpMV, defect, axpy family); reductions use a fixed
+ * tree order (deterministic, run to run and alone vs. batched).
+ *
+ * Errors: every function returns HB_OK (0) or an hb_status code.  HB_ERR_SIZE corresponds to
+ * the reference's VectorSizeDoesNotMatch / MatrixRowsDoNotMatch, raised before any launch.
+ */
+#ifndef HONEI_B200_H
+#define HONEI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef enum {
+    HB_OK = 0,
+    HB_ERR_INVALID = 1,      /* null pointer, bad enum, misaligned device pointer         */
+    HB_ERR_SIZE = 2,         /* vector / matrix sizes do not match (VectorSizeDoesNotMatch) */
+    HB_ERR_CUDA = 3,         /* a CUDA runtime call failed                                  */
+    HB_ERR_ALLOC = 4,        /* device or pinned allocation failed                          */
+    HB_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up                          */
+    HB_ERR_UNSUPPORTED = 6,  /* shape outside what the kernels support (e.g. > 2^31 rows)   */
+    HB_ERR_CAPACITY = 7,     /* admission refused: over the HBM budget or slot count        */
+    HB_ERR_NOT_FOUND = 8,    /* unknown request id                                          */
+    HB_ERR_NONFINITE = 9     /* NaN or Inf found in an input that must be finite            */
+} hb_status;
+
+typedef enum { HB_F64 = 0, HB_F32 = 1 } hb_dtype;
+
+/* ------------------------------------------------------------------------------------------
+ * Context: device, stream, reduction scratch and pinned scalar slots (the role of the
+ * reference's GPUPool + MemoryBackend<tags::GPU::CUDA>, honei/backends/cuda/gpu_pool.hh:53-88,
+ * honei/util/memory_backend.hh:131-165).  One context per host thread / stream.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct hb_context hb_context;
+
+int  hb_create(hb_context **ctx, int device);
+int  hb_destroy(hb_context *ctx);
+int  hb_set_stream(hb_context *ctx, void *stream);      /* cudaStream_t; NULL = legacy stream */
+int  hb_synchronize(hb_context *ctx);
+const char *hb_status_string(int status);
+/* Text of the last CUDA error seen by this context (empty if none). */
+const char *hb_last_error(hb_context *ctx);
+/* Number of kernels this library launched through ctx since creation (instrumentation). */
+uint64_t hb_launch_count(hb_context *ctx);
+/* Pre-size the context workspace for vectors of n entries, so later calls (and stream
+ * captures) need no allocation. */
+int  hb_reserve(hb_context *ctx, int64_t n);
+
+/* ------------------------------------------------------------------------------------------
+ * Device ELL matrix.  Replaces the device copies of SparseMatrixELL's Aj/Ax/Arl arrays
+ * (honei/la/sparse_matrix_ell.hh:44-129) that the reference's MemoryBackend uploads.
+ *
+ * Layout: K slots per row (K = ncpr * threads of the reference), column-major with leading
+ * dimension ld (a multiple of 64): slot k of row r is at k*ld + r.  Slot order within a row
+ * is the reference's summation order.  Padding slots hold Aj = -1 and Ax = 0.  Column indices
+ * are 32-bit.  Aj and Ax must be 16-byte aligned (cudaMalloc / torch allocations are).
+ * ---------------------------------------------------------------------------------------- */
+typedef struct {
+    int64_t rows, cols;
+    int64_t K;        /* slots per row                                         */
+    int64_t ld;       /* leading dimension, multiple of 64, >= rows            */
+    int32_t *Aj;      /* device int32[K*ld]                                    */
+    void *Ax;         /* device double[K*ld] or float[K*ld]                    */
+    int32_t dtype;    /* hb_dtype                                              */
+    int32_t pad_;
+} hb_ell;
+
+/* Device layout for a reference ELL matrix with `rows` rows, `ncpr` columns per row and
+ * `threads` lanes: *K = ncpr*threads, *ld = rows rounded up to 64. */
+int hb_ell_layout(int64_t rows, int64_t ncpr, int64_t threads, int64_t *K, int64_t *ld);
+
+/* Import a reference SparseMatrixELL whose arrays (u64 Aj, Ax, u64 Arl, reference layout
+ * (k%T) + r*T + (k/T)*stride) are already on the device, into the hb_ell layout in `out`
+ * (out->Aj / out->Ax preallocated, out->rows/cols/K/ld set, e.g. from hb_ell_layout).
+ * Replaces the upload half of MemoryBackend<tags::GPU::CUDA>::upload for matrices
+ * (honei/backends/cuda/memory_backend.cc) plus the narrowing of the 64-bit indices. */
+int hb_ell_import_f64(hb_context *ctx, int64_t rows, int64_t cols, int64_t stride, int64_t ncpr,
+                      int64_t threads, const uint64_t *Aj_ref, const double *Ax_ref,
+                      const uint64_t *Arl_ref, hb_ell *out);
+int hb_ell_import_f32(hb_context *ctx, int64_t rows, int64_t cols, int64_t stride, int64_t ncpr,
+                      int64_t threads, const uint64_t *Aj_ref, const float *Ax_ref,
+                      const uint64_t *Arl_ref, hb_ell *out);
+/* Same pattern, values cast to float (for the FP32 inner solves of mixed precision). */
+int hb_ell_cast_f64_f32(hb_context *ctx, const hb_ell *src, hb_ell *dst);
+
+/* Q1 Poisson assembly on the device (the FillMatrix<POISSON, DIRICHLET_0> stencil,
+ * honei/math/fill_matrix.hh:37-77, built straight into hb_ell layout, K = 9): M x M nodes,
+ * Dirichlet rows identity; coef = NULL (unit) or device double[(M-1)^2] cell coefficients
+ * (bilinear element matrix k/6 [[4,-1,-2,-1],...]).  out->Aj/Ax preallocated with K=9,
+ * ld from hb_ell_layout(M*M, 9, 1).  Identical to the host generator bit for bit. */
+int hb_q1_assemble_f64(hb_context *ctx, int64_t M, const double *coef, hb_ell *out);
+
+/* ------------------------------------------------------------------------------------------
+ * Operators (the static value() functions of the tag-dispatched API).
+ * ---------------------------------------------------------------------------------------- */
+/* y = A x.  Product<tags::GPU::CUDA>::value(DenseVector&, const SparseMatrixELL&, const
+ * DenseVector&), honei/la/product.hh:1758-1760; replaces cuda_product_smell_dv_{float,double}
+ * (honei/backends/cuda/operations.hh, honei/backends/cuda/product.cu:356-401).
+ * Per-row sum in the reference order, one rounding per multiply and per add: bit-identical to
+ * Product<tags::CPU> (honei/la/product.hh:148-204). */
+int hb_spmv_f64(hb_context *ctx, const hb_ell *A, const double *x, double *y);
+int hb_spmv_f32(hb_context *ctx, const hb_ell *A, const float *x, float *y);
+
+/* r = b - A x.  Defect<tags::GPU::CUDA>::value, honei/math/defect.hh:660-670; replaces
+ * cuda_defect_smell_dv_{float,double} (honei/backends/cuda/defect.cu:367-416).
+ * Bit-identical to Defect<tags::CPU> (honei/math/defect.hh:357-383). */
+int hb_defect_f64(hb_context *ctx, const hb_ell *A, const double *b, const double *x, double *r);
+int hb_defect_f32(hb_context *ctx, const hb_ell *A, const float *b, const float *x, float *r);
+
+/* Host scalar results (synchronous, like the reference's value-returning operators).
+ * DotProduct<tags::GPU::CUDA>::value, honei/la/dot_product.hh:358-360 (replaces
+ * cuda_dot_product_two_{float,double}, honei/backends/cuda/dot_product.cu:77-155);
+ * Norm<vnt_l_two, root, tags::GPU::CUDA>::value, honei/la/norm.hh:551-574 (root = 0 returns
+ * the squared norm, as Norm<vnt_l_two, false> does). */
+int hb_dot_f64(hb_context *ctx, int64_t n, const double *x, const double *y, double *result_host);
+int hb_dot_f32(hb_context *ctx, int64_t n, const float *x, const float *y, float *result_host);
+int hb_norm_l2_f64(hb_context *ctx, int64_t n, const double *x, int root, double *result_host);
+int hb_norm_l2_f32(hb_context *ctx, int64_t n, const float *x, int root, float *result_host);
+
+/* x += b*y  (ScaledSum(x, y, b), honei/la/scaled_sum.hh:461-466)
+ * r = x + b*y (ScaledSum(r, x, y, b), honei/la/scaled_sum.hh:467-471) */
+int hb_scaled_sum_f64(hb_context *ctx, int64_t n, double *x, const double *y, double b);
+int hb_scaled_sum_f32(hb_context *ctx, int64_t n, float *x, const float *y, float b);
+int hb_scaled_sum3_f64(hb_context *ctx, int64_t n, double *r, const double *x, const double *y, double b);
+int hb_scaled_sum3_f32(hb_context *ctx, int64_t n, float *r, const float *x, const float *y, float b);
+/* x *= a (Scale, honei/la/scale.hh:263); x += y (Sum, honei/la/sum.hh:684);
+ * r = x - y (Difference); r = x * y elementwise (ElementProduct; also the Jacobi apply
+ * Product(DV, DV, DV), honei/la/product.hh:1198-1204). */
+int hb_scale_f64(hb_context *ctx, int64_t n, double *x, double a);
+int hb_scale_f32(hb_context *ctx, int64_t n, float *x, float a);
+int hb_sum_f64(hb_context *ctx, int64_t n, double *x, const double *y);
+int hb_sum_f32(hb_context *ctx, int64_t n, float *x, const float *y);
+int hb_difference_f64(hb_context *ctx, int64_t n, double *r, const double *x, const double *y);
+int hb_difference_f32(hb_context *ctx, int64_t n, float *r, const float *x, const float *y);
+int hb_element_product_f64(hb_context *ctx, int64_t n, double *r, const double *x, const double *y);
+int hb_element_product_f32(hb_context *ctx, int64_t n, float *r, const float *x, const float *y);
+/* copy / fill / precision conversion: copy<Tag>, fill<Tag>, convert<Tag>
+ * (honei/la/algorithm.hh:50-86,163-198; MemoryBackend copy/fill/convert_float_double/
+ * convert_double_float, honei/backends/cuda/transfer.cu:28-46,153-159). */
+int hb_copy(hb_context *ctx, void *dst, const void *src, int64_t bytes);
+int hb_fill_f64(hb_context *ctx, int64_t n, double *x, double value);
+int hb_fill_f32(hb_context *ctx, int64_t n, float *x, float value);
+int hb_convert_f64_f32(hb_context *ctx, int64_t n, float *dst, const double *src);
+int hb_convert_f32_f64(hb_context *ctx, int64_t n, double *dst, const float *src);
+
+/* ------------------------------------------------------------------------------------------
+ * Solvers.
+ * ---------------------------------------------------------------------------------------- */
+/* Plain CG, CGSolver<Tag, methods::NONE>::value(A, P, b, x, max_iters, used_iters, eps),
+ * honei/math/cg.hh:63-133: same update formulas, the same guarded divisions and the same dual
+ * stopping rule (sqrt(alpha) < eps*sqrt(alpha0) or sqrt(alpha) < eps).  The whole loop runs
+ * in ONE persistent cooperative kernel (2 grid barriers per iteration, scalars on the
+ * device); x holds x0 on entry and the solution on exit.  *used_iters (host) receives the
+ * iteration count, *final_defect (host, may be NULL) sqrt(alpha) at exit.
+ * Returns HB_ERR_TIMEOUT if a bounded device-side barrier wait gave up. */
+int hb_cg_f64(hb_context *ctx, const hb_ell *A, const double *b, double *x, int64_t max_iters,
+              double eps, int64_t *used_iters, double *final_defect);
+int hb_cg_f32(hb_context *ctx, const hb_ell *A, const float *b, float *x, int64_t max_iters,
+              float eps, int64_t *used_iters, float *final_defect);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif /* HONEI_B200_H */

@@ -1,0 +1,316 @@
+"""ctypes bindings to the parity oracles.  TEST INFRASTRUCTURE ONLY.
+
+* ``Oracle``    -- oracle/_build/libhonei_oracle.so, the plain-C restatement (honei_oracle.c).
+* ``Reference`` -- oracle/_ref/libhonei_ref.so, the reference's own CPU path compiled from the
+                   unmodified HONEI sources plus ref_shim.cc (present where it was built).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libhonei_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libhonei_ref.so")
+
+_c = ctypes
+_u64 = _c.c_uint64
+_vp = _c.c_void_p
+
+TAGS = {"cpu": 0, "generic": 1, "sse": 2, "mc-generic": 3, "mc-sse": 4}
+
+
+def build_oracle() -> None:
+    """Compiles the C restatement (and the reference shim when the HONEI tree is present)."""
+    subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_vp)
+
+
+class _OraEll(_c.Structure):
+    _fields_ = [("rows", _u64), ("cols", _u64), ("stride", _u64), ("ncpr", _u64),
+                ("threads", _u64), ("Aj", _vp), ("Ax", _vp), ("Arl", _vp)]
+
+
+class _OraMG(_c.Structure):
+    _fields_ = [("nlevels", _c.c_int), ("A", _c.POINTER(_OraEll)), ("prol", _c.POINTER(_OraEll)),
+                ("res", _c.POINTER(_OraEll)), ("max_iters", _u64), ("max_iters_coarse", _u64),
+                ("n_pre", _u64), ("n_post", _u64)]
+
+
+def _ell(A):
+    e = _OraEll(A.rows, A.cols, A.stride, A.ncpr, A.threads, A.Aj.ctypes.data, A.Ax.ctypes.data,
+                A.Arl.ctypes.data)
+    e._keep = A
+    return e
+
+
+class Oracle:
+    """The plain-C restatement of the HONEI path."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            build_oracle()
+        self.lib = _c.CDLL(path)
+        L = self.lib
+        for name, res in [("ora_dot_f64", _c.c_double), ("ora_dot_f32", _c.c_float)]:
+            getattr(L, name).restype = res
+        L.ora_dot_f64.argtypes = [_u64, _vp, _vp]
+        L.ora_dot_f32.argtypes = [_u64, _vp, _vp]
+        L.ora_cg_f64.argtypes = [_vp, _vp, _vp, _u64, _c.c_double, _c.POINTER(_u64), _vp]
+        L.ora_cg_f32.argtypes = [_vp, _vp, _vp, _u64, _c.c_float, _c.POINTER(_u64), _vp]
+        L.ora_mg_f64.argtypes = [_vp, _c.c_double, _vp, _vp, _c.c_double, _c.POINTER(_u64), _vp]
+        L.ora_mg_f32.argtypes = [_vp, _c.c_float, _vp, _vp, _c.c_float, _c.POINTER(_u64), _vp]
+        L.ora_ir_mg.argtypes = [_vp, _vp, _c.c_float, _vp, _vp, _c.c_double, _c.c_float, _u64,
+                                _c.c_int, _c.POINTER(_u64), _vp]
+        L.ora_ir_cg.argtypes = [_vp, _vp, _vp, _vp, _c.c_double, _c.c_float, _u64, _u64,
+                                _c.POINTER(_u64), _c.POINTER(_u64), _vp]
+        for n in ("ora_scaled_sum_f64", "ora_scale_f64"):
+            getattr(L, n).argtypes = [_u64, _vp, _vp, _c.c_double] if n == "ora_scaled_sum_f64" \
+                else [_u64, _vp, _c.c_double]
+        L.ora_scaled_sum3_f64.argtypes = [_u64, _vp, _vp, _vp, _c.c_double]
+
+    @staticmethod
+    def _suffix(dtype):
+        return "f64" if np.dtype(dtype) == np.float64 else "f32"
+
+    def spmv(self, A, x):
+        s = self._suffix(A.dtype)
+        x = np.ascontiguousarray(x, A.dtype)
+        y = np.zeros(A.rows, A.dtype)
+        e = _ell(A)
+        getattr(self.lib, f"ora_spmv_{s}")(_c.byref(e), _ptr(x), _ptr(y))
+        return y
+
+    def defect(self, A, b, x):
+        s = self._suffix(A.dtype)
+        b = np.ascontiguousarray(b, A.dtype)
+        x = np.ascontiguousarray(x, A.dtype)
+        r = np.zeros(A.rows, A.dtype)
+        e = _ell(A)
+        getattr(self.lib, f"ora_defect_{s}")(_c.byref(e), _ptr(b), _ptr(x), _ptr(r))
+        return r
+
+    def dot(self, x, y):
+        x = np.ascontiguousarray(x)
+        y = np.ascontiguousarray(y, x.dtype)
+        f = self.lib.ora_dot_f64 if x.dtype == np.float64 else self.lib.ora_dot_f32
+        return f(len(x), _ptr(x), _ptr(y))
+
+    def cg(self, A, b, x0=None, max_iters=10000, eps=1e-8, history=False):
+        """Returns (x, used_iters[, sqrt(alpha) history])."""
+        s = self._suffix(A.dtype)
+        b = np.ascontiguousarray(b, A.dtype)
+        x = np.zeros(A.rows, A.dtype) if x0 is None else np.array(x0, A.dtype)
+        used = _u64(0)
+        hist = np.zeros(max_iters + 1, A.dtype)
+        e = _ell(A)
+        getattr(self.lib, f"ora_cg_{s}")(_c.byref(e), _ptr(b), _ptr(x), max_iters, eps,
+                                         _c.byref(used), _ptr(hist))
+        if history:
+            return x, used.value, hist[: used.value + 1]
+        return x, used.value
+
+    def _mg_struct(self, H, max_iters, max_iters_coarse, n_pre, n_post):
+        L = len(H.A)
+        A = (_OraEll * L)(*[_ell(a) for a in H.A])
+        P = (_OraEll * max(L - 1, 1))(*[_ell(a) for a in H.prol])
+        R = (_OraEll * max(L - 1, 1))(*[_ell(a) for a in H.res])
+        mg = _OraMG(L, A, P, R, max_iters, max_iters_coarse, n_pre, n_post)
+        mg._keep = (A, P, R, H)
+        return mg
+
+    def mg(self, H, b, x0=None, damping=0.7, eps=1e-8, max_iters=100, max_iters_coarse=1000,
+           n_pre=2, n_post=2, history=False):
+        """V(n_pre, n_post) MG, Jacobi smoother, PROLMAT transfers, CG coarse solve."""
+        dt = H.A[-1].dtype
+        s = self._suffix(dt)
+        b = np.ascontiguousarray(b, dt)
+        x = np.zeros(H.A[-1].rows, dt) if x0 is None else np.array(x0, dt)
+        mg = self._mg_struct(H, max_iters, max_iters_coarse, n_pre, n_post)
+        used = _u64(0)
+        hist = np.zeros(max_iters + 1, dt)
+        getattr(self.lib, f"ora_mg_{s}")(_c.byref(mg), damping, _ptr(b), _ptr(x), eps,
+                                         _c.byref(used), _ptr(hist))
+        if history:
+            return x, used.value, hist[: used.value + 1]
+        return x, used.value
+
+    def ir_mg(self, A64, H32, b, x0=None, damping=0.7, eps=1e-10, inner_eps=1e-3, max_iters=100,
+              inner_max_iters=100, max_iters_coarse=1000, n_pre=2, n_post=2, warm_start=True):
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(A64.rows) if x0 is None else np.array(x0, np.float64)
+        mg = self._mg_struct(H32, inner_max_iters, max_iters_coarse, n_pre, n_post)
+        used = _u64(0)
+        hist = np.zeros(max_iters + 1)
+        e = _ell(A64)
+        self.lib.ora_ir_mg(_c.byref(e), _c.byref(mg), damping, _ptr(b), _ptr(x), eps, inner_eps,
+                           max_iters, int(warm_start), _c.byref(used), _ptr(hist))
+        return x, used.value, hist[: used.value + 1]
+
+    def ir_cg(self, A64, A32, b, x0=None, eps=1e-10, inner_eps=1e-3, inner_max_iters=100000,
+              max_iters=100):
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(A64.rows) if x0 is None else np.array(x0, np.float64)
+        used, inner = _u64(0), _u64(0)
+        hist = np.zeros(max_iters + 1)
+        e64, e32 = _ell(A64), _ell(A32)
+        self.lib.ora_ir_cg(_c.byref(e64), _c.byref(e32), _ptr(b), _ptr(x), eps, inner_eps,
+                           inner_max_iters, max_iters, _c.byref(used), _c.byref(inner), _ptr(hist))
+        return x, used.value, inner.value, hist[: used.value + 1]
+
+
+class Reference:
+    """The reference's own CPU path (unmodified HONEI sources + ref_shim.cc)."""
+
+    def __init__(self, path: str = REF_SO):
+        self.lib = _c.CDLL(path)
+        L = self.lib
+        L.ref_last_error.restype = _c.c_char_p
+        ul = _c.c_ulong
+        ell_args = [ul] * 5 + [_vp, _vp]
+        L.ref_spmv_f64.argtypes = [_c.c_int] + ell_args + [_vp, _vp, _c.c_int, _c.POINTER(_c.c_double)]
+        L.ref_spmv_f32.argtypes = L.ref_spmv_f64.argtypes
+        L.ref_defect_f64.argtypes = [_c.c_int] + ell_args + [_vp, _vp, _vp]
+        L.ref_defect_f32.argtypes = L.ref_defect_f64.argtypes
+        L.ref_dot_f64.argtypes = [_c.c_int, ul, _vp, _vp, _vp]
+        L.ref_dot_f32.argtypes = L.ref_dot_f64.argtypes
+        L.ref_cg_f64.argtypes = [_c.c_int] + ell_args + [_vp, _vp, ul, _c.c_double,
+                                                         _c.POINTER(ul), _c.POINTER(_c.c_double)]
+        L.ref_cg_f32.argtypes = [_c.c_int] + ell_args + [_vp, _vp, ul, _c.c_float,
+                                                         _c.POINTER(ul), _c.POINTER(_c.c_double)]
+        L.ref_q1_poisson_f64.argtypes = [ul, _vp, _vp, _vp, _vp]
+        L.ref_read_ell_f64.argtypes = [_c.c_char_p, _vp, _vp, _vp, _vp]
+        L.ref_read_exp_f64.argtypes = [_c.c_char_p, _c.POINTER(ul), _vp]
+        L.ref_set_threads.argtypes = [_c.c_int]
+        mg_args = [_c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+        L.ref_mg_f64.argtypes = mg_args + [_c.c_double, ul, ul, ul, ul, _c.c_double,
+                                           _c.POINTER(ul), _c.POINTER(_c.c_double)]
+        L.ref_mg_f32.argtypes = mg_args + [_c.c_float, ul, ul, ul, ul, _c.c_float,
+                                           _c.POINTER(ul), _c.POINTER(_c.c_double)]
+        L.ref_ir_mg.argtypes = [_c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                _c.c_float, ul, ul, ul, ul, _c.c_float, _c.c_double, ul,
+                                _c.POINTER(ul), _c.POINTER(_c.c_double)]
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError("reference: " + self.lib.ref_last_error().decode())
+
+    def set_threads(self, n: int):
+        self._check(self.lib.ref_set_threads(n))
+
+    @staticmethod
+    def _args(A):
+        return [A.rows, A.cols, A.stride, A.ncpr, A.threads, _ptr(A.Aj), _ptr(A.Ax)]
+
+    def q1_poisson(self, M):
+        from honei_b200.problems import EllMatrix
+        info = (_c.c_ulong * 6)()
+        self._check(self.lib.ref_q1_poisson_f64(M, info, None, None, None))
+        rows, cols, stride, ncpr, T, nnz = list(info)
+        Aj = np.zeros(ncpr * stride, np.uint64)
+        Ax = np.zeros(ncpr * stride)
+        Arl = np.zeros(rows, np.uint64)
+        self._check(self.lib.ref_q1_poisson_f64(M, info, _ptr(Aj), _ptr(Ax), _ptr(Arl)))
+        return EllMatrix(rows, cols, stride, ncpr, T, Aj, Ax, Arl, nnz)
+
+    def read_ell(self, path):
+        from honei_b200.problems import EllMatrix
+        info = (_c.c_ulong * 6)()
+        p = path.encode()
+        self._check(self.lib.ref_read_ell_f64(p, info, None, None, None))
+        rows, cols, stride, ncpr, T, nnz = list(info)
+        Aj = np.zeros(ncpr * stride, np.uint64)
+        Ax = np.zeros(ncpr * stride)
+        Arl = np.zeros(rows, np.uint64)
+        self._check(self.lib.ref_read_ell_f64(p, info, _ptr(Aj), _ptr(Ax), _ptr(Arl)))
+        return EllMatrix(rows, cols, stride, ncpr, T, Aj, Ax, Arl, nnz)
+
+    def read_exp(self, path):
+        n = _c.c_ulong(0)
+        self._check(self.lib.ref_read_exp_f64(path.encode(), _c.byref(n), None))
+        out = np.zeros(n.value)
+        self._check(self.lib.ref_read_exp_f64(path.encode(), _c.byref(n), _ptr(out)))
+        return out
+
+    def spmv(self, A, x, tag="cpu", reps=0):
+        """Returns (y, median seconds of `reps` timed calls after one warm-up)."""
+        s = "f64" if A.dtype == np.float64 else "f32"
+        x = np.ascontiguousarray(x, A.dtype)
+        y = np.zeros(A.rows, A.dtype)
+        sec = _c.c_double(0)
+        self._check(getattr(self.lib, f"ref_spmv_{s}")(TAGS[tag], *self._args(A), _ptr(x), _ptr(y),
+                                                        reps, _c.byref(sec)))
+        return y, sec.value
+
+    def defect(self, A, b, x, tag="cpu"):
+        s = "f64" if A.dtype == np.float64 else "f32"
+        b = np.ascontiguousarray(b, A.dtype)
+        x = np.ascontiguousarray(x, A.dtype)
+        r = np.zeros(A.rows, A.dtype)
+        self._check(getattr(self.lib, f"ref_defect_{s}")(TAGS[tag], *self._args(A), _ptr(b), _ptr(x), _ptr(r)))
+        return r
+
+    def dot(self, x, y, tag="cpu"):
+        x = np.ascontiguousarray(x)
+        y = np.ascontiguousarray(y, x.dtype)
+        out = np.zeros(1, x.dtype)
+        f = self.lib.ref_dot_f64 if x.dtype == np.float64 else self.lib.ref_dot_f32
+        self._check(f(TAGS[tag], len(x), _ptr(x), _ptr(y), _ptr(out)))
+        return out[0]
+
+    def cg(self, A, b, x0=None, max_iters=10000, eps=1e-8, tag="cpu"):
+        """Returns (x, used_iters, seconds)."""
+        s = "f64" if A.dtype == np.float64 else "f32"
+        b = np.ascontiguousarray(b, A.dtype)
+        x = np.zeros(A.rows, A.dtype) if x0 is None else np.array(x0, A.dtype)
+        used = _c.c_ulong(0)
+        sec = _c.c_double(0)
+        self._check(getattr(self.lib, f"ref_cg_{s}")(TAGS[tag], *self._args(A), _ptr(b), _ptr(x),
+                                                      max_iters, eps, _c.byref(used), _c.byref(sec)))
+        return x, used.value, sec.value
+
+    def _mg_arrays(self, H):
+        L = len(H.A)
+        ainfo = np.array([a.info() for a in H.A], np.uint64).ravel()
+        pinfo = np.array([p.info() for p in H.prol] or [[0] * 5], np.uint64).ravel()
+        Aj = (_vp * L)(*[a.Aj.ctypes.data for a in H.A])
+        Ax = (_vp * L)(*[a.Ax.ctypes.data for a in H.A])
+        Pj = (_vp * max(L - 1, 1))(*[p.Aj.ctypes.data for p in H.prol])
+        Px = (_vp * max(L - 1, 1))(*[p.Ax.ctypes.data for p in H.prol])
+        return L, ainfo, pinfo, Aj, Ax, Pj, Px
+
+    def mg(self, H, b, x0=None, damping=0.7, eps=1e-8, max_iters=100, max_iters_coarse=1000,
+           n_pre=2, n_post=2, tag="cpu"):
+        dt = H.A[-1].dtype
+        s = "f64" if dt == np.float64 else "f32"
+        L, ainfo, pinfo, Aj, Ax, Pj, Px = self._mg_arrays(H)
+        b = np.ascontiguousarray(b, dt)
+        x = np.zeros(H.A[-1].rows, dt) if x0 is None else np.array(x0, dt)
+        used = _c.c_ulong(0)
+        sec = _c.c_double(0)
+        self._check(getattr(self.lib, f"ref_mg_{s}")(TAGS[tag], L, _ptr(ainfo), Aj, Ax, _ptr(pinfo), Pj, Px,
+                                                      _ptr(b), _ptr(x), damping, max_iters, max_iters_coarse,
+                                                      n_pre, n_post, eps, _c.byref(used), _c.byref(sec)))
+        return x, used.value, sec.value
+
+    def ir_mg(self, H64, H32, b, x0=None, damping=0.7, eps=1e-10, inner_eps=1e-3, max_iters=100,
+              inner_max_iters=100, max_iters_coarse=1000, n_pre=2, n_post=2):
+        L, ainfo, pinfo, Aj, Ax64, Pj, _ = self._mg_arrays(H64)
+        Ax32 = (_vp * L)(*[a.Ax.ctypes.data for a in H32.A])
+        Px32 = (_vp * max(L - 1, 1))(*[p.Ax.ctypes.data for p in H32.prol])
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(H64.A[-1].rows) if x0 is None else np.array(x0, np.float64)
+        used = _c.c_ulong(0)
+        sec = _c.c_double(0)
+        self._check(self.lib.ref_ir_mg(L, _ptr(ainfo), Aj, Ax64, Ax32, _ptr(pinfo), Pj, Px32, _ptr(b),
+                                       _ptr(x), damping, inner_max_iters, max_iters_coarse, n_pre, n_post,
+                                       inner_eps, eps, max_iters, _c.byref(used), _c.byref(sec)))
+        return x, used.value, sec.value

@@ -1,0 +1,291 @@
+/* honei_oracle.c -- plain-C restatement of the HONEI sparse-solver path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker, never the thing measured or shipped.  Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
+ *
+ * Pinned against the reference itself: tests/test_oracle_pin.py compares every routine
+ * bit-for-bit with oracle/_ref/libhonei_ref.so (the unmodified HONEI CPU path) and with the
+ * committed fixtures under tests/golden/.
+ *
+ * Each routine cites the reference source it restates (paths within the HONEI tree).
+ * Build with -ffp-contract=off: the reference rounds once per multiply and once per add.
+ */
+#include "honei_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ---------------------------------------------------------------------------------------
+ * ELL SpMV -- honei/la/product.hh:148-204 (Product<tags::CPU>, SparseMatrixELL x DenseVector)
+ *   for row: sum = 0; for col < Arl[row]: for thread < T: sum += Ax[j+thread] * x[Aj[j+thread]]
+ *   with j = row*T + col*stride.
+ * Defect -- honei/math/defect.hh:357-383: temp = A x, then r[i] = b[i] - temp[i].
+ * ------------------------------------------------------------------------------------- */
+#define ORA_SPMV(SUF, DT)                                                                   \
+void ora_spmv_##SUF(const ora_ell *A, const DT *x, DT *y)                                   \
+{                                                                                           \
+    const DT *ax = (const DT *)A->Ax;                                                       \
+    for (uint64_t row = 0; row < A->rows; ++row) {                                          \
+        DT sum = 0;                                                                         \
+        uint64_t j = row * A->threads;                                                      \
+        for (uint64_t col = 0; col < A->Arl[row]; ++col, j += A->stride)                    \
+            for (uint64_t t = 0; t < A->threads; ++t)                                       \
+                sum += ax[j + t] * x[A->Aj[j + t]];                                         \
+        y[row] = sum;                                                                       \
+    }                                                                                       \
+}                                                                                           \
+void ora_defect_##SUF(const ora_ell *A, const DT *b, const DT *x, DT *r)                    \
+{                                                                                           \
+    DT *temp = (DT *)malloc(sizeof(DT) * (A->rows ? A->rows : 1));                          \
+    ora_spmv_##SUF(A, x, temp);                                                             \
+    for (uint64_t i = 0; i < A->rows; ++i) r[i] = b[i] - temp[i];                           \
+    free(temp);                                                                             \
+}
+ORA_SPMV(f64, double)
+ORA_SPMV(f32, float)
+
+/* DotProduct<tags::CPU> -- honei/la/dot_product.hh:72-88: sequential, left to right.
+ * Norm<vnt_l_two, false> == DotProduct(x, x) (honei/la/norm.hh:290-306). */
+#define ORA_DOT(SUF, DT)                                                                    \
+DT ora_dot_##SUF(uint64_t n, const DT *x, const DT *y)                                      \
+{                                                                                           \
+    DT result = 0;                                                                          \
+    for (uint64_t i = 0; i < n; ++i) result += x[i] * y[i];                                 \
+    return result;                                                                          \
+}
+ORA_DOT(f64, double)
+ORA_DOT(f32, float)
+
+/* ScaledSum -- honei/la/scaled_sum.hh:73-110: x[i] += b * y[i];  r[i] = b * y[i] + x[i]. */
+void ora_scaled_sum_f64(uint64_t n, double *x, const double *y, double b)
+{ for (uint64_t i = 0; i < n; ++i) x[i] += b * y[i]; }
+void ora_scaled_sum_f32(uint64_t n, float *x, const float *y, float b)
+{ for (uint64_t i = 0; i < n; ++i) x[i] += b * y[i]; }
+void ora_scaled_sum3_f64(uint64_t n, double *r, const double *x, const double *y, double b)
+{ for (uint64_t i = 0; i < n; ++i) r[i] = b * y[i] + x[i]; }
+/* Scale -- honei/la/scale.hh:77 (x *= a); Sum -- honei/la/sum.hh:98 (x += y);
+ * Difference (r = x - y); ElementProduct -- honei/la/element_product.hh:76-140 (r = x * y). */
+void ora_scale_f64(uint64_t n, double *x, double a)
+{ for (uint64_t i = 0; i < n; ++i) x[i] *= a; }
+void ora_sum_f64(uint64_t n, double *x, const double *y)
+{ for (uint64_t i = 0; i < n; ++i) x[i] += y[i]; }
+void ora_difference_f64(uint64_t n, double *r, const double *x, const double *y)
+{ for (uint64_t i = 0; i < n; ++i) r[i] = x[i] - y[i]; }
+void ora_element_product_f64(uint64_t n, double *r, const double *x, const double *y)
+{ for (uint64_t i = 0; i < n; ++i) r[i] = x[i] * y[i]; }
+
+/* ---------------------------------------------------------------------------------------
+ * CGSolver<Tag, methods::NONE> -- honei/math/cg.hh:63-133.
+ *   r = b - A x; p = r; alpha = r.r; d0 = sqrt(alpha)
+ *   loop: v = A p; temp = v.p; lambda = alpha / (|temp| > eps_mach ? temp : eps_mach)
+ *         x += lambda p; r += (-lambda) v; alpha_old = alpha; alpha = r.r
+ *         beta = alpha / (|alpha_old| > eps_mach ? alpha_old : eps_mach); p *= beta; p += r
+ *         stop if sqrt(alpha) < eps * d0 or sqrt(alpha) < eps (used_iters set only on stop
+ *         or when max_iters is reached).
+ * ------------------------------------------------------------------------------------- */
+#define ORA_CG(SUF, DT, EPSM, SQRT, FABS)                                                   \
+int ora_cg_##SUF(const ora_ell *A, const DT *b, DT *x, uint64_t max_iters, DT eps,          \
+                 uint64_t *used, DT *hist)                                                  \
+{                                                                                           \
+    const uint64_t n = A->rows;                                                             \
+    DT *p = (DT *)malloc(sizeof(DT) * (n ? n : 1));                                         \
+    DT *r = (DT *)malloc(sizeof(DT) * (n ? n : 1));                                         \
+    DT *v = (DT *)malloc(sizeof(DT) * (n ? n : 1));                                         \
+    if (!p || !r || !v) { free(p); free(r); free(v); return 1; }                            \
+    ora_defect_##SUF(A, b, x, r);                                                           \
+    memcpy(p, r, sizeof(DT) * n);                                                           \
+    DT alpha = ora_dot_##SUF(n, r, r), alpha_old, lambda, temp;                             \
+    DT initial_defect = SQRT(alpha), current_defect = 0;                                    \
+    if (hist) hist[0] = initial_defect;                                                     \
+    uint64_t it = 0;                                                                        \
+    while (it < max_iters) {                                                                \
+        ora_spmv_##SUF(A, p, v);                                                            \
+        temp = ora_dot_##SUF(n, v, p);                                                      \
+        lambda = alpha / (FABS(temp) > EPSM ? temp : EPSM);                                 \
+        for (uint64_t i = 0; i < n; ++i) x[i] += lambda * p[i];                             \
+        DT mlambda = -lambda;                                                               \
+        for (uint64_t i = 0; i < n; ++i) r[i] += mlambda * v[i];                            \
+        alpha_old = alpha;                                                                  \
+        alpha = ora_dot_##SUF(n, r, r);                                                     \
+        DT talpha = alpha / (FABS(alpha_old) > EPSM ? alpha_old : EPSM);                    \
+        for (uint64_t i = 0; i < n; ++i) p[i] *= talpha;                                    \
+        for (uint64_t i = 0; i < n; ++i) p[i] += r[i];                                      \
+        ++it;                                                                               \
+        current_defect = SQRT(alpha);                                                       \
+        if (hist) hist[it] = current_defect;                                                \
+        if (current_defect < eps * initial_defect) { *used = it; break; }                   \
+        if (current_defect < eps) { *used = it; break; }                                    \
+        if (it == max_iters) *used = it;                                                    \
+    }                                                                                       \
+    free(p); free(r); free(v);                                                              \
+    return 0;                                                                               \
+}
+ORA_CG(f64, double, DBL_EPSILON, sqrt, fabs)
+ORA_CG(f32, float, FLT_EPSILON, sqrtf, fabsf)
+
+/* ---------------------------------------------------------------------------------------
+ * Multigrid V-cycle -- honei/math/mg.hh:567-662 (MGCycleCreation<V::STATIC>) and
+ * honei/math/mg.hh:1093-1127 (MGSolver), with
+ *   smoother RISmoother -- honei/math/ri.hh:97-133: n x { t0 = b - A x; t1 = P * t0; x += t1 }
+ *   P = damping / diag(A)  -- PreconFill "jac", honei/math/mg.hh:255-286
+ *   restriction  d_{l-1} = Res_l store_l  -- honei/math/restriction.hh:175-185
+ *   prolongation store_l = Prol_l c_{l-1}; x_l += store_l -- honei/math/prolongation.hh:142-155
+ *   coarse solve CGSolver<NONE>(A_1, b_1, x_1, max_iters_coarse, eps) at min_level = 1.
+ * Top level works on (x, b); every lower level on (c, d), c zero-filled before recursion.
+ * ------------------------------------------------------------------------------------- */
+#define ORA_MG(SUF, DT, SQRT)                                                               \
+typedef struct {                                                                            \
+    const ora_mg *mg;                                                                       \
+    DT **P, **d, **c, **store, **t0, **t1;                                                  \
+    DT eps;                                                                                 \
+    uint64_t used_coarse;                                                                   \
+} mgws_##SUF;                                                                               \
+/* A(row, row) as SparseMatrixELL::operator() finds it (sparse_matrix_ell-impl.hh:326-338) */ \
+static DT ora_diag_##SUF(const ora_ell *A, uint64_t row)                                    \
+{                                                                                           \
+    const DT *ax = (const DT *)A->Ax;                                                       \
+    uint64_t j = row * A->threads;                                                          \
+    for (uint64_t col = 0; col < A->Arl[row] && A->Aj[j] <= row; ++col, j += A->stride)     \
+        for (uint64_t t = 0; t < A->threads; ++t)                                           \
+            if (A->Aj[j + t] == row) return ax[j + t];                                      \
+    return 0;                                                                               \
+}                                                                                           \
+static void ora_smooth_##SUF(mgws_##SUF *w, int l, const DT *b, DT *x, uint64_t n_sweeps)   \
+{                                                                                           \
+    const ora_ell *A = &w->mg->A[l];                                                        \
+    for (uint64_t s = 0; s < n_sweeps; ++s) {                                               \
+        ora_defect_##SUF(A, b, x, w->t0[l]);                                                \
+        for (uint64_t i = 0; i < A->rows; ++i) w->t1[l][i] = w->P[l][i] * w->t0[l][i];      \
+        for (uint64_t i = 0; i < A->rows; ++i) x[i] += w->t1[l][i];                         \
+    }                                                                                       \
+}                                                                                           \
+static void ora_vcycle_##SUF(mgws_##SUF *w, int l, DT *x, const DT *b)                      \
+{                                                                                           \
+    const ora_mg *mg = w->mg;                                                               \
+    if (l == 0) {                                                                           \
+        uint64_t u = w->used_coarse;                                                        \
+        ora_cg_##SUF(&mg->A[0], b, x, mg->max_iters_coarse, w->eps, &u, NULL);              \
+        w->used_coarse = u;                                                                 \
+        return;                                                                             \
+    }                                                                                       \
+    ora_smooth_##SUF(w, l, b, x, mg->n_pre);                                                \
+    ora_defect_##SUF(&mg->A[l], b, x, w->store[l]);                                         \
+    ora_spmv_##SUF(&mg->res[l - 1], w->store[l], w->d[l - 1]);                              \
+    memset(w->c[l - 1], 0, sizeof(DT) * mg->A[l - 1].rows);                                 \
+    ora_vcycle_##SUF(w, l - 1, w->c[l - 1], w->d[l - 1]);                                   \
+    ora_spmv_##SUF(&mg->prol[l - 1], w->c[l - 1], w->store[l]);                             \
+    for (uint64_t i = 0; i < mg->A[l].rows; ++i) x[i] += w->store[l][i];                    \
+    ora_smooth_##SUF(w, l, b, x, mg->n_post);                                               \
+}                                                                                           \
+int ora_mg_##SUF(const ora_mg *mg, DT damping, const DT *b, DT *x, DT eps, uint64_t *used,  \
+                 DT *rnorm_hist)                                                            \
+{                                                                                           \
+    const int L = mg->nlevels;                                                              \
+    mgws_##SUF w;                                                                           \
+    w.mg = mg; w.eps = eps; w.used_coarse = 0;                                              \
+    DT ***arrs[] = { &w.P, &w.d, &w.c, &w.store, &w.t0, &w.t1 };                            \
+    for (int a = 0; a < 6; ++a) {                                                           \
+        *arrs[a] = (DT **)calloc(L, sizeof(DT *));                                          \
+        for (int l = 0; l < L; ++l)                                                         \
+            (*arrs[a])[l] = (DT *)calloc(mg->A[l].rows ? mg->A[l].rows : 1, sizeof(DT));    \
+    }                                                                                       \
+    for (int l = 0; l < L; ++l)                                                             \
+        for (uint64_t i = 0; i < mg->A[l].rows; ++i) {                                      \
+            DT p = damping;                                                                 \
+            p /= ora_diag_##SUF(&mg->A[l], i);                                              \
+            w.P[l][i] = p;                                                                  \
+        }                                                                                   \
+    const uint64_t n = mg->A[L - 1].rows;                                                   \
+    DT *r = (DT *)calloc(n ? n : 1, sizeof(DT));                                            \
+    ora_defect_##SUF(&mg->A[L - 1], b, x, r);                                               \
+    DT rnorm_initial = SQRT(ora_dot_##SUF(n, r, r));                                        \
+    DT rnorm_current = (DT)1e16;                                                            \
+    if (rnorm_hist) rnorm_hist[0] = rnorm_initial;                                          \
+    for (uint64_t i = 0; i < mg->max_iters; ++i) {                                          \
+        ora_vcycle_##SUF(&w, L - 1, x, b);                                                  \
+        ora_defect_##SUF(&mg->A[L - 1], b, x, r);                                           \
+        rnorm_current = SQRT(ora_dot_##SUF(n, r, r));                                       \
+        if (rnorm_hist) rnorm_hist[i + 1] = rnorm_current;                                  \
+        *used = i + 1;                                                                      \
+        if (rnorm_current < eps * rnorm_initial) break;                                     \
+    }                                                                                       \
+    free(r);                                                                                \
+    for (int a = 0; a < 6; ++a) {                                                           \
+        for (int l = 0; l < L; ++l) free((*arrs[a])[l]);                                    \
+        free(*arrs[a]);                                                                     \
+    }                                                                                       \
+    return 0;                                                                               \
+}
+ORA_MG(f64, double, sqrt)
+ORA_MG(f32, float, sqrtf)
+
+/* ---------------------------------------------------------------------------------------
+ * IRSolver<Outer=double, Inner=float> -- honei/math/ir.hh:30-78.
+ *   for i < max_iters: r = b - A x (FP64); i == 0 ? rnorm0 = |r| : (used = i; stop if
+ *   |r| < eps * rnorm0); b_inner = (float) r; inner MG; c = (double) x_inner; x += c.
+ * The reference leaves x_inner as it was (warm start); warm_start == 0 zeroes it instead.
+ * ------------------------------------------------------------------------------------- */
+int ora_ir_mg(const ora_ell *A64, const ora_mg *mg32, float damping, const double *b, double *x,
+              double eps, float inner_eps, uint64_t max_iters, int warm_start, uint64_t *used,
+              double *rnorm_hist)
+{
+    const uint64_t n = A64->rows;
+    double *r = (double *)calloc(n ? n : 1, sizeof(double));
+    float *bi = (float *)calloc(n ? n : 1, sizeof(float));
+    float *xi = (float *)calloc(n ? n : 1, sizeof(float));
+    double rnorm_initial = 1e16, rnorm_current = 1e16;
+    for (uint64_t i = 0; i < max_iters; ++i) {
+        ora_defect_f64(A64, b, x, r);
+        if (i == 0) {
+            rnorm_initial = sqrt(ora_dot_f64(n, r, r));
+            if (rnorm_hist) rnorm_hist[0] = rnorm_initial;
+        } else {
+            rnorm_current = sqrt(ora_dot_f64(n, r, r));
+            if (rnorm_hist) rnorm_hist[i] = rnorm_current;
+            *used = i;
+            if (rnorm_current < eps * rnorm_initial) break;
+        }
+        for (uint64_t k = 0; k < n; ++k) bi[k] = (float)r[k];
+        if (!warm_start) memset(xi, 0, sizeof(float) * n);
+        uint64_t inner_used = 0;
+        ora_mg_f32(mg32, damping, bi, xi, inner_eps, &inner_used, NULL);
+        for (uint64_t k = 0; k < n; ++k) x[k] += (double)xi[k];
+    }
+    free(r); free(bi); free(xi);
+    return 0;
+}
+
+int ora_ir_cg(const ora_ell *A64, const ora_ell *A32, const double *b, double *x, double eps,
+              float inner_eps, uint64_t inner_max_iters, uint64_t max_iters, uint64_t *used,
+              uint64_t *inner_total, double *rnorm_hist)
+{
+    const uint64_t n = A64->rows;
+    double *r = (double *)calloc(n ? n : 1, sizeof(double));
+    float *bi = (float *)calloc(n ? n : 1, sizeof(float));
+    float *xi = (float *)calloc(n ? n : 1, sizeof(float));
+    double rnorm_initial = 1e16, rnorm_current = 1e16;
+    uint64_t total = 0;
+    for (uint64_t i = 0; i < max_iters; ++i) {
+        ora_defect_f64(A64, b, x, r);
+        if (i == 0) {
+            rnorm_initial = sqrt(ora_dot_f64(n, r, r));
+            if (rnorm_hist) rnorm_hist[0] = rnorm_initial;
+        } else {
+            rnorm_current = sqrt(ora_dot_f64(n, r, r));
+            if (rnorm_hist) rnorm_hist[i] = rnorm_current;
+            *used = i;
+            if (rnorm_current < eps * rnorm_initial) break;
+        }
+        for (uint64_t k = 0; k < n; ++k) bi[k] = (float)r[k];
+        memset(xi, 0, sizeof(float) * n);
+        uint64_t inner_used = 0;
+        ora_cg_f32(A32, bi, xi, inner_max_iters, inner_eps, &inner_used, NULL);
+        total += inner_used;
+        for (uint64_t k = 0; k < n; ++k) x[k] += (double)xi[k];
+    }
+    if (inner_total) *inner_total = total;
+    free(r); free(bi); free(xi);
+    return 0;
+}

@@ -1,0 +1,83 @@
+/* honei_oracle.h -- plain-C restatement of the HONEI sparse-solver path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg may load this; the product never does.
+ *
+ * Parity pin: every routine is checked bit-for-bit against the reference's own CPU path
+ * (oracle/_ref/libhonei_ref.so, compiled from the unmodified HONEI sources) and against the
+ * FEATFLOW2 fixtures the reference's tests use (tests/golden, tests/test_oracle_pin.py).
+ *
+ * Matrices use the reference ELL layout (honei/la/sparse_matrix_ell-impl.hh:75-122):
+ * entry k of row r lives at (k % T) + r*T + (k / T)*stride, Arl[r] = ceil(nnz_r / T),
+ * Aj are 64-bit column indices.  All arithmetic is one IEEE rounding per operation, in the
+ * order the reference source states it (build with -ffp-contract=off).
+ */
+#ifndef HONEI_ORACLE_H
+#define HONEI_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    uint64_t rows, cols, stride, ncpr, threads;
+    const uint64_t *Aj;
+    const void *Ax;       /* double* or float* */
+    const uint64_t *Arl;
+} ora_ell;
+
+/* ---- BLAS-1 and SpMV (f64 / f32) ---- */
+void   ora_spmv_f64(const ora_ell *A, const double *x, double *y);
+void   ora_spmv_f32(const ora_ell *A, const float *x, float *y);
+void   ora_defect_f64(const ora_ell *A, const double *b, const double *x, double *r);
+void   ora_defect_f32(const ora_ell *A, const float *b, const float *x, float *r);
+double ora_dot_f64(uint64_t n, const double *x, const double *y);
+float  ora_dot_f32(uint64_t n, const float *x, const float *y);
+void   ora_scaled_sum_f64(uint64_t n, double *x, const double *y, double b);
+void   ora_scaled_sum_f32(uint64_t n, float *x, const float *y, float b);
+void   ora_scaled_sum3_f64(uint64_t n, double *r, const double *x, const double *y, double b);
+void   ora_scale_f64(uint64_t n, double *x, double a);
+void   ora_sum_f64(uint64_t n, double *x, const double *y);
+void   ora_difference_f64(uint64_t n, double *r, const double *x, const double *y);
+void   ora_element_product_f64(uint64_t n, double *r, const double *x, const double *y);
+
+/* ---- Solvers ----
+ * CG returns the number of iterations in *used; hist (optional, max_iters+1 entries) gets
+ * sqrt(alpha) after every iteration, hist[0] = initial defect. */
+int ora_cg_f64(const ora_ell *A, const double *b, double *x, uint64_t max_iters, double eps,
+               uint64_t *used, double *hist);
+int ora_cg_f32(const ora_ell *A, const float *b, float *x, uint64_t max_iters, float eps,
+               uint64_t *used, float *hist);
+
+/* MG hierarchy, coarsest level first (level index 0 == HONEI level 1).  prol[l] maps level l
+ * to level l+1 (rows = n_{l+1}); res[l] = prol[l]^T.  P[l] = damping / diag(A[l]). */
+typedef struct {
+    int nlevels;
+    const ora_ell *A;
+    const ora_ell *prol;
+    const ora_ell *res;
+    uint64_t max_iters, max_iters_coarse, n_pre, n_post;
+} ora_mg;
+
+int ora_mg_f64(const ora_mg *mg, double damping, const double *b, double *x, double eps,
+               uint64_t *used, double *rnorm_hist);
+int ora_mg_f32(const ora_mg *mg, float damping, const float *b, float *x, float eps,
+               uint64_t *used, float *rnorm_hist);
+
+/* IR (honei/math/ir.hh:30-78): FP64 outer defect + update around the FP32 MG above.
+ * A64 is the finest FP64 matrix; mg32 the FP32 hierarchy. warm_start != 0 keeps the inner
+ * x between outer steps (the reference behaviour); 0 restarts it at zero. */
+int ora_ir_mg(const ora_ell *A64, const ora_mg *mg32, float damping, const double *b, double *x,
+              double eps, float inner_eps, uint64_t max_iters, int warm_start, uint64_t *used,
+              double *rnorm_hist);
+
+/* IR with an FP32 CG inner solver (same outer loop; inner CG from x = 0 every step). */
+int ora_ir_cg(const ora_ell *A64, const ora_ell *A32, const double *b, double *x, double eps,
+              float inner_eps, uint64_t inner_max_iters, uint64_t max_iters, uint64_t *used,
+              uint64_t *inner_total, double *rnorm_hist);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

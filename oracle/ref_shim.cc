@@ -1,0 +1,450 @@
+// ref_shim.cc -- C entry points into the reference HONEI CPU path (test infrastructure only).
+//
+// This file is compiled together with the unmodified HONEI sources (oracle/Makefile) into
+// oracle/_ref/libhonei_ref.so.  Every function builds the reference's own containers from
+// plain arrays and calls the reference's own operators, so the numbers it returns ARE the
+// reference's: it is the parity pin for the plain-C restatement in honei_oracle.c and the
+// timed CPU baseline.  Nothing in the product links it.
+//
+// Tag selector (int tag):
+//   0 tags::CPU                      (sequential; the parity oracle)
+//   1 tags::CPU::Generic
+//   2 tags::CPU::SSE                 (best single core)
+//   3 tags::CPU::MultiCore::Generic
+//   4 tags::CPU::MultiCore::SSE      (all cores)
+//
+// Reference functions called (paths within the HONEI tree):
+//   Product<Tag>::value(DV, SparseMatrixELL, DV)            honei/la/product.hh:148-204
+//   Defect<Tag>::value(DV, DV, SparseMatrixELL, DV)         honei/math/defect.hh:357-383
+//   DotProduct<Tag>, Norm<vnt_l_two, false/true, Tag>       honei/la/dot_product.hh:72-88, honei/la/norm.hh:290-397
+//   CGSolver<Tag, methods::NONE>                            honei/math/cg.hh:63-133
+//   MGUtil / MGCycleCreation<V::STATIC> / MGSolver          honei/math/mg.hh:423-662, 1093-1127
+//   IRSolver<Outer, Inner, Norm>                            honei/math/ir.hh:30-78
+//   FillMatrix<POISSON, DIRICHLET_0> + SparseMatrix -> ELL  honei/math/fill_matrix.hh:37-77, honei/la/sparse_matrix_ell-impl.hh:75-122
+//   Transposition<Tag>                                      honei/math/transposition.hh:30-50
+
+#include <honei/la/dense_vector.hh>
+#include <honei/la/sparse_matrix.hh>
+#include <honei/la/sparse_matrix_ell.hh>
+#include <honei/la/banded_matrix_qx.hh>
+#include <honei/la/product.hh>
+#include <honei/la/dot_product.hh>
+#include <honei/la/norm.hh>
+#include <honei/la/scaled_sum.hh>
+#include <honei/la/sum.hh>
+#include <honei/la/algorithm.hh>
+#include <honei/math/defect.hh>
+#include <honei/math/cg.hh>
+#include <honei/math/ri.hh>
+#include <honei/math/mg.hh>
+#include <honei/math/ir.hh>
+#include <honei/math/operator.hh>
+#include <honei/math/restriction.hh>
+#include <honei/math/prolongation.hh>
+#include <honei/math/transposition.hh>
+#include <honei/math/fill_matrix.hh>
+#include <honei/math/matrix_io.hh>
+#include <honei/math/vector_io.hh>
+#include <honei/util/configuration.hh>
+
+#include <cstdint>
+#include <cstring>
+#include <ctime>
+#include <vector>
+#include <string>
+#include <exception>
+#include <iostream>
+#include <sstream>
+#include <algorithm>
+
+using namespace honei;
+
+namespace
+{
+    double now_s()
+    {
+        timespec ts;
+        clock_gettime(CLOCK_MONOTONIC, &ts);
+        return ts.tv_sec + 1e-9 * ts.tv_nsec;
+    }
+
+    template <typename DT_> DenseVector<DT_> dv_from(const DT_ * p, unsigned long n)
+    {
+        DenseVector<DT_> v(n);
+        if (n) std::memcpy(v.elements(), p, n * sizeof(DT_));
+        return v;
+    }
+
+    template <typename DT_> void dv_to(const DenseVector<DT_> & v, DT_ * p)
+    {
+        if (v.size()) std::memcpy(p, v.elements(), v.size() * sizeof(DT_));
+    }
+
+    // Builds the reference container from the raw ELL arrays; the raw constructor recomputes
+    // Arl from the first zero value of every row (sparse_matrix_ell-impl.hh:186-208).
+    template <typename DT_> SparseMatrixELL<DT_> ell_from(unsigned long rows, unsigned long cols,
+            unsigned long stride, unsigned long ncpr, unsigned long threads,
+            const uint64_t * Aj, const DT_ * Ax)
+    {
+        const unsigned long size(ncpr * stride);
+        DenseVector<unsigned long> aj(size);
+        for (unsigned long i(0) ; i < size ; ++i) aj[i] = Aj[i];
+        DenseVector<DT_> ax(dv_from(Ax, size));
+        return SparseMatrixELL<DT_>(rows, cols, stride, ncpr, aj, ax, threads);
+    }
+
+    template <typename DT_> void ell_export(const SparseMatrixELL<DT_> & A, unsigned long * info,
+            uint64_t * Aj, DT_ * Ax, uint64_t * Arl)
+    {
+        info[0] = A.rows(); info[1] = A.columns(); info[2] = A.stride();
+        info[3] = A.num_cols_per_row(); info[4] = A.threads(); info[5] = A.used_elements();
+        if (Aj)  for (unsigned long i(0) ; i < A.Aj().size() ; ++i) Aj[i] = A.Aj()[i];
+        if (Ax)  dv_to(A.Ax(), Ax);
+        if (Arl) for (unsigned long i(0) ; i < A.Arl().size() ; ++i) Arl[i] = A.Arl()[i];
+    }
+
+    std::string g_last_error;
+
+    template <typename F_> int guarded(F_ f)
+    {
+        try { f(); return 0; }
+        catch (honei::Exception & e) { g_last_error = e.message(); return 1; }
+        catch (std::exception & e) { g_last_error = e.what(); return 1; }
+        catch (...) { g_last_error = "unknown exception"; return 1; }
+    }
+
+#define REF_DISPATCH(tag, CALL)                                               \
+    switch (tag) {                                                            \
+        case 0: { typedef tags::CPU T_; CALL; } break;                        \
+        case 1: { typedef tags::CPU::Generic T_; CALL; } break;               \
+        case 2: { typedef tags::CPU::SSE T_; CALL; } break;                   \
+        case 3: { typedef tags::CPU::MultiCore::Generic T_; CALL; } break;    \
+        case 4: { typedef tags::CPU::MultiCore::SSE T_; CALL; } break;        \
+        default: throw InternalError("ref_shim: unknown tag selector");       \
+    }
+
+    template <typename T_, typename DT_> void spmv_reps(SparseMatrixELL<DT_> & A, DenseVector<DT_> & y,
+            const DenseVector<DT_> & x, int reps, double * seconds)
+    {
+        Product<T_>::value(y, A, x);                      // warm-up
+        std::vector<double> t;
+        for (int r(0) ; r < reps ; ++r)
+        {
+            double t0(now_s());
+            Product<T_>::value(y, A, x);
+            t.push_back(now_s() - t0);
+        }
+        if (seconds)
+        {
+            std::sort(t.begin(), t.end());
+            *seconds = t.empty() ? 0. : t[t.size() / 2];
+        }
+    }
+
+    template <typename DT_> int spmv_impl(int tag, unsigned long rows, unsigned long cols, unsigned long stride,
+            unsigned long ncpr, unsigned long threads, const uint64_t * Aj, const DT_ * Ax,
+            const DT_ * x, DT_ * y, int reps, double * seconds)
+    {
+        return guarded([&]() {
+            SparseMatrixELL<DT_> A(ell_from(rows, cols, stride, ncpr, threads, Aj, Ax));
+            DenseVector<DT_> xv(dv_from(x, cols));
+            DenseVector<DT_> yv(rows, DT_(0));
+            REF_DISPATCH(tag, (spmv_reps<T_, DT_>(A, yv, xv, reps, seconds)));
+            dv_to(yv, y);
+        });
+    }
+
+    template <typename DT_> int defect_impl(int tag, unsigned long rows, unsigned long cols, unsigned long stride,
+            unsigned long ncpr, unsigned long threads, const uint64_t * Aj, const DT_ * Ax,
+            const DT_ * b, const DT_ * x, DT_ * r)
+    {
+        return guarded([&]() {
+            SparseMatrixELL<DT_> A(ell_from(rows, cols, stride, ncpr, threads, Aj, Ax));
+            DenseVector<DT_> xv(dv_from(x, cols)), bv(dv_from(b, rows)), rv(rows, DT_(0));
+            REF_DISPATCH(tag, (Defect<T_>::value(rv, bv, A, xv)));
+            dv_to(rv, r);
+        });
+    }
+
+    template <typename DT_> int cg_impl(int tag, unsigned long rows, unsigned long cols, unsigned long stride,
+            unsigned long ncpr, unsigned long threads, const uint64_t * Aj, const DT_ * Ax,
+            const DT_ * b, DT_ * x, unsigned long max_iters, DT_ eps, unsigned long * used, double * seconds)
+    {
+        return guarded([&]() {
+            SparseMatrixELL<DT_> A(ell_from(rows, cols, stride, ncpr, threads, Aj, Ax));
+            DenseVector<DT_> xv(dv_from(x, cols)), bv(dv_from(b, rows));
+            unsigned long u(0);
+            double t0(now_s());
+            REF_DISPATCH(tag, (CGSolver<T_, methods::NONE>::value(A, A, bv, xv, max_iters, u, eps)));
+            if (seconds) *seconds = now_s() - t0;
+            *used = u;
+            dv_to(xv, x);
+        });
+    }
+
+    // Levels are given finest-last (level 1 = coarsest), as MGData stores them (mg.hh:35-54).
+    template <typename DT_> struct MGLevels
+    {
+        std::vector<SparseMatrixELL<DT_> > A, prol, res;
+        std::vector<DenseVector<DT_> > P, b, x, d, c, store;
+        std::vector<std::vector<DenseVector<DT_> > > smoother_temp;
+    };
+
+    // Builds MGData exactly as MGUtil::load_data (mg.hh:442-547) does from files, but from
+    // arrays: A_l, Prol_l from the caller; P_l = PreconFill "jac" = damping / diag(A_l)
+    // (mg.hh:255-286); Res_l = Transposition(Prol_l) (mg.hh:496).
+    template <typename DT_> MGData<SparseMatrixELL<DT_>, DenseVector<DT_>, SparseMatrixELL<DT_>, DenseVector<DT_>, DT_>
+    mg_data_from(int nlevels, const unsigned long * ainfo, const uint64_t * const * Aj, const DT_ * const * Ax,
+            const unsigned long * pinfo, const uint64_t * const * Pj, const DT_ * const * Px,
+            const DT_ * b, const DT_ * x0, DT_ damping)
+    {
+        MGLevels<DT_> L;
+        for (int i(0) ; i < nlevels ; ++i)
+        {
+            const unsigned long * ai(ainfo + 5 * i);
+            SparseMatrixELL<DT_> a(ell_from(ai[0], ai[1], ai[2], ai[3], ai[4], Aj[i], Ax[i]));
+            L.A.push_back(a);
+            PreconFill<DenseVector<DT_>, SparseMatrixELL<DT_>, DT_>::value(i, L.P, "", "jac", a, damping);
+            if (i < nlevels - 1)
+            {
+                const unsigned long * pi(pinfo + 5 * i);
+                SparseMatrixELL<DT_> p(ell_from(pi[0], pi[1], pi[2], pi[3], pi[4], Pj[i], Px[i]));
+                L.prol.push_back(p);
+                L.res.push_back(Transposition<tags::CPU>::value(p.copy()));
+            }
+            const unsigned long n(ai[0]);
+            DenseVector<DT_> zero(n, DT_(0));
+            if (i == nlevels - 1)
+            {
+                L.b.push_back(dv_from(b, n));
+                L.x.push_back(dv_from(x0, n));
+            }
+            else
+            {
+                L.b.push_back(zero.copy());
+                L.x.push_back(zero.copy());
+            }
+            L.d.push_back(zero.copy());
+            L.c.push_back(zero.copy());
+            L.store.push_back(zero.copy());
+            L.smoother_temp.push_back(std::vector<DenseVector<DT_> >());
+        }
+        return MGData<SparseMatrixELL<DT_>, DenseVector<DT_>, SparseMatrixELL<DT_>, DenseVector<DT_>, DT_>(
+                L.A, L.res, L.prol, L.P, L.b, L.x, L.d, L.c, L.store, L.smoother_temp, 0, 0, 0, 0, 0, DT_(0));
+    }
+
+    template <typename T_, typename DT_> void mg_run(
+            MGData<SparseMatrixELL<DT_>, DenseVector<DT_>, SparseMatrixELL<DT_>, DenseVector<DT_>, DT_> & data)
+    {
+        OperatorList cycle(MGCycleCreation<T_, methods::CYCLE::V::STATIC, CGSolver<T_, methods::NONE>, RISmoother<T_>,
+                Restriction<T_, methods::PROLMAT>, Prolongation<T_, methods::PROLMAT>, DT_>::value(data));
+        MGSolver<T_, Norm<vnt_l_two, true, T_> >::value(data, cycle);
+    }
+
+    // MGSolver prints its initial and final norm to stdout (mg.hh:1107,1125); keep the
+    // caller's stdout clean.
+    struct MuteCout
+    {
+        std::streambuf * old;
+        std::ostringstream sink;
+        MuteCout() : old(std::cout.rdbuf(sink.rdbuf())) {}
+        ~MuteCout() { std::cout.rdbuf(old); }
+    };
+}
+
+extern "C"
+{
+    const char * ref_last_error() { return g_last_error.c_str(); }
+
+    // Threads used by the MultiCore tags: mc::num_threads and every max_count key on the path.
+    int ref_set_threads(int n)
+    {
+        return guarded([&]() {
+            Configuration * c(Configuration::instance());
+            c->set_value("mc::num_threads", n);
+            const char * keys[] = { "mc::Product(DV,SMELL,DV)::max_count", "mc::dot_product(DVCB,DVCB)::max_count",
+                "mc::ScaledSum(DVB,DVB,DT)::max_count", "mc::ScaledSum(DVCB,DVCB,DT)::max_count",
+                "mc::Sum(DVCB,DVCB)::max_count", "mc::Scale(DVCB,DT)::max_count",
+                "mc::Difference(DVCB,DVCB)::max_count", "mc::ElementProduct(DVCB,DVCB)::max_count",
+                "mc::Defect(DV,DV,SMELL,DV)::max_count" };
+            for (const char * k : keys) c->set_value(k, n);
+        });
+    }
+
+    // Q1 Poisson (Dirichlet rows = identity) on an M x M node grid through the reference's own
+    // construction path: FillMatrix -> BandedMatrixQx -> SparseMatrix -> SparseMatrixELL.
+    // Call with Aj == NULL to receive info = {rows, cols, stride, ncpr, threads, nnz} only.
+    int ref_q1_poisson_f64(unsigned long M, unsigned long * info, uint64_t * Aj, double * Ax, uint64_t * Arl)
+    {
+        return guarded([&]() {
+            const unsigned long N(M * M);
+            DenseVector<double> z(N, 0.);
+            BandedMatrixQx<Q1Type, double> q1(N, z.copy(), z.copy(), z.copy(), z.copy(), z.copy(), z.copy(),
+                    z.copy(), z.copy(), z.copy());
+            FillMatrix<tags::CPU, applications::POISSON, boundary_types::DIRICHLET::DIRICHLET_0>::value(q1);
+            SparseMatrix<double> sm(q1);
+            SparseMatrixELL<double> A(sm);
+            ell_export(A, info, Aj, Ax, Arl);
+        });
+    }
+
+    // Reads a HONEI .ell file with the reference reader (matrix_io.hh:433-582).
+    int ref_read_ell_f64(const char * path, unsigned long * info, uint64_t * Aj, double * Ax, uint64_t * Arl)
+    {
+        return guarded([&]() {
+            SparseMatrixELL<double> A(MatrixIO<io_formats::ELL>::read_matrix(std::string(path), double(0)));
+            ell_export(A, info, Aj, Ax, Arl);
+        });
+    }
+
+    // Reads an EXP vector with the reference reader (vector_io.hh:52-115). n receives the size.
+    int ref_read_exp_f64(const char * path, unsigned long * n, double * out)
+    {
+        return guarded([&]() {
+            DenseVector<double> v(VectorIO<io_formats::EXP>::read_vector(std::string(path), double(0)));
+            *n = v.size();
+            if (out) dv_to(v, out);
+        });
+    }
+
+    // Transposition of an ELL matrix (the MG restriction matrix), raw arrays in, ELL arrays out.
+    int ref_transpose_f64(const unsigned long * ainfo, const uint64_t * Aj, const double * Ax,
+            unsigned long * info, uint64_t * Tj, double * Tx, uint64_t * Trl)
+    {
+        return guarded([&]() {
+            SparseMatrixELL<double> A(ell_from(ainfo[0], ainfo[1], ainfo[2], ainfo[3], ainfo[4], Aj, Ax));
+            SparseMatrixELL<double> T(Transposition<tags::CPU>::value(A));
+            ell_export(T, info, Tj, Tx, Trl);
+        });
+    }
+
+    int ref_spmv_f64(int tag, unsigned long rows, unsigned long cols, unsigned long stride, unsigned long ncpr,
+            unsigned long threads, const uint64_t * Aj, const double * Ax, const double * x, double * y,
+            int reps, double * seconds)
+    { return spmv_impl<double>(tag, rows, cols, stride, ncpr, threads, Aj, Ax, x, y, reps, seconds); }
+
+    int ref_spmv_f32(int tag, unsigned long rows, unsigned long cols, unsigned long stride, unsigned long ncpr,
+            unsigned long threads, const uint64_t * Aj, const float * Ax, const float * x, float * y,
+            int reps, double * seconds)
+    { return spmv_impl<float>(tag, rows, cols, stride, ncpr, threads, Aj, Ax, x, y, reps, seconds); }
+
+    int ref_defect_f64(int tag, unsigned long rows, unsigned long cols, unsigned long stride, unsigned long ncpr,
+            unsigned long threads, const uint64_t * Aj, const double * Ax, const double * b, const double * x, double * r)
+    { return defect_impl<double>(tag, rows, cols, stride, ncpr, threads, Aj, Ax, b, x, r); }
+
+    int ref_defect_f32(int tag, unsigned long rows, unsigned long cols, unsigned long stride, unsigned long ncpr,
+            unsigned long threads, const uint64_t * Aj, const float * Ax, const float * b, const float * x, float * r)
+    { return defect_impl<float>(tag, rows, cols, stride, ncpr, threads, Aj, Ax, b, x, r); }
+
+    int ref_dot_f64(int tag, unsigned long n, const double * x, const double * y, double * out)
+    {
+        return guarded([&]() {
+            DenseVector<double> xv(dv_from(x, n)), yv(dv_from(y, n));
+            REF_DISPATCH(tag, (*out = DotProduct<T_>::value(xv, yv)));
+        });
+    }
+
+    int ref_dot_f32(int tag, unsigned long n, const float * x, const float * y, float * out)
+    {
+        return guarded([&]() {
+            DenseVector<float> xv(dv_from(x, n)), yv(dv_from(y, n));
+            REF_DISPATCH(tag, (*out = DotProduct<T_>::value(xv, yv)));
+        });
+    }
+
+    int ref_norm2sq_f64(int tag, unsigned long n, const double * x, double * out)
+    {
+        return guarded([&]() {
+            DenseVector<double> xv(dv_from(x, n));
+            REF_DISPATCH(tag, (*out = Norm<vnt_l_two, false, T_>::value(xv)));
+        });
+    }
+
+    int ref_cg_f64(int tag, unsigned long rows, unsigned long cols, unsigned long stride, unsigned long ncpr,
+            unsigned long threads, const uint64_t * Aj, const double * Ax, const double * b, double * x,
+            unsigned long max_iters, double eps, unsigned long * used, double * seconds)
+    { return cg_impl<double>(tag, rows, cols, stride, ncpr, threads, Aj, Ax, b, x, max_iters, eps, used, seconds); }
+
+    int ref_cg_f32(int tag, unsigned long rows, unsigned long cols, unsigned long stride, unsigned long ncpr,
+            unsigned long threads, const uint64_t * Aj, const float * Ax, const float * b, float * x,
+            unsigned long max_iters, float eps, unsigned long * used, double * seconds)
+    { return cg_impl<float>(tag, rows, cols, stride, ncpr, threads, Aj, Ax, b, x, max_iters, eps, used, seconds); }
+
+    // V(n_pre, n_post) MG with damped Jacobi ("jac") smoothing, PROLMAT transfers and a CG
+    // coarse solver at level 1.  ainfo/pinfo hold {rows, cols, stride, ncpr, threads} per level,
+    // coarsest first; x holds x0 on entry and the solution on exit.
+    int ref_mg_f64(int tag, int nlevels, const unsigned long * ainfo, const uint64_t * const * Aj,
+            const double * const * Ax, const unsigned long * pinfo, const uint64_t * const * Pj,
+            const double * const * Px, const double * b, double * x, double damping,
+            unsigned long max_iters, unsigned long max_iters_coarse, unsigned long n_pre, unsigned long n_post,
+            double eps, unsigned long * used, double * seconds)
+    {
+        return guarded([&]() {
+            MuteCout mute;
+            MGData<SparseMatrixELL<double>, DenseVector<double>, SparseMatrixELL<double>, DenseVector<double>, double>
+                data(mg_data_from<double>(nlevels, ainfo, Aj, Ax, pinfo, Pj, Px, b, x, damping));
+            MGUtil<tags::CPU, SparseMatrixELL<double>, DenseVector<double>, SparseMatrixELL<double>, DenseVector<double>,
+                MatrixIO<io_formats::ELL>, VectorIO<io_formats::EXP>, double>::configure(
+                        data, max_iters, max_iters_coarse, n_pre, n_post, 1, eps);
+            double t0(now_s());
+            REF_DISPATCH(tag, (mg_run<T_, double>(data)));
+            if (seconds) *seconds = now_s() - t0;
+            *used = data.used_iters;
+            dv_to(data.x.back(), x);
+        });
+    }
+
+    int ref_mg_f32(int tag, int nlevels, const unsigned long * ainfo, const uint64_t * const * Aj,
+            const float * const * Ax, const unsigned long * pinfo, const uint64_t * const * Pj,
+            const float * const * Px, const float * b, float * x, float damping,
+            unsigned long max_iters, unsigned long max_iters_coarse, unsigned long n_pre, unsigned long n_post,
+            float eps, unsigned long * used, double * seconds)
+    {
+        return guarded([&]() {
+            MuteCout mute;
+            MGData<SparseMatrixELL<float>, DenseVector<float>, SparseMatrixELL<float>, DenseVector<float>, float>
+                data(mg_data_from<float>(nlevels, ainfo, Aj, Ax, pinfo, Pj, Px, b, x, damping));
+            MGUtil<tags::CPU, SparseMatrixELL<float>, DenseVector<float>, SparseMatrixELL<float>, DenseVector<float>,
+                MatrixIO<io_formats::ELL>, VectorIO<io_formats::EXP>, float>::configure(
+                        data, max_iters, max_iters_coarse, n_pre, n_post, 1, eps);
+            double t0(now_s());
+            REF_DISPATCH(tag, (mg_run<T_, float>(data)));
+            if (seconds) *seconds = now_s() - t0;
+            *used = data.used_iters;
+            dv_to(data.x.back(), x);
+        });
+    }
+
+    // IRSolver<tags::CPU, tags::CPU, Norm<l2, true>> (ir.hh:30-78): FP64 outer defect/update
+    // around the FP32 MG above.  The inner data keeps its x between outer steps, as ir.hh does.
+    int ref_ir_mg(int nlevels, const unsigned long * ainfo, const uint64_t * const * Aj,
+            const double * const * Ax64, const float * const * Ax32, const unsigned long * pinfo,
+            const uint64_t * const * Pj, const float * const * Px32, const double * b, double * x,
+            float damping, unsigned long inner_max_iters, unsigned long max_iters_coarse,
+            unsigned long n_pre, unsigned long n_post, float inner_eps, double eps,
+            unsigned long max_iters, unsigned long * used, double * seconds)
+    {
+        return guarded([&]() {
+            MuteCout mute;
+            const unsigned long n(ainfo[5 * (nlevels - 1)]);
+            std::vector<float> zero(n, 0.f);
+            MGData<SparseMatrixELL<float>, DenseVector<float>, SparseMatrixELL<float>, DenseVector<float>, float>
+                data(mg_data_from<float>(nlevels, ainfo, Aj, Ax32, pinfo, Pj, Px32, zero.data(), zero.data(), damping));
+            MGUtil<tags::CPU, SparseMatrixELL<float>, DenseVector<float>, SparseMatrixELL<float>, DenseVector<float>,
+                MatrixIO<io_formats::ELL>, VectorIO<io_formats::EXP>, float>::configure(
+                        data, inner_max_iters, max_iters_coarse, n_pre, n_post, 1, inner_eps);
+            OperatorList cycle(MGCycleCreation<tags::CPU, methods::CYCLE::V::STATIC, CGSolver<tags::CPU, methods::NONE>,
+                    RISmoother<tags::CPU>, Restriction<tags::CPU, methods::PROLMAT>, Prolongation<tags::CPU, methods::PROLMAT>,
+                    float>::value(data));
+            const unsigned long * ai(ainfo + 5 * (nlevels - 1));
+            SparseMatrixELL<double> A(ell_from(ai[0], ai[1], ai[2], ai[3], ai[4], Aj[nlevels - 1], Ax64[nlevels - 1]));
+            DenseVector<double> bv(dv_from(b, n)), xv(dv_from(x, n));
+            unsigned long u(0);
+            double t0(now_s());
+            IRSolver<tags::CPU, tags::CPU, Norm<vnt_l_two, true, tags::CPU> >::value(A, bv, xv, data, cycle, eps, max_iters, u);
+            if (seconds) *seconds = now_s() - t0;
+            *used = u;
+            dv_to(xv, x);
+        });
+    }
+}

@@ -1,0 +1,56 @@
+"""Test configuration: the `gpu` marker and shared fixtures.
+
+`-m "not gpu"` runs the oracle pins, host logic and ABI checks on any machine; `-m gpu` runs
+the parity tests that call libhonei_b200.so on a B200.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and libhonei_b200.so")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle.bindings import Oracle
+    return Oracle()
+
+
+@pytest.fixture(scope="session")
+def reference():
+    """The reference's own CPU path, where it was built (not on machines without it)."""
+    from oracle.bindings import REF_SO, Reference
+    if not os.path.exists(REF_SO):
+        pytest.skip("oracle/_ref/libhonei_ref.so not built here")
+    return Reference()
+
+
+def load_golden(name):
+    return np.load(os.path.join(GOLDEN, name + ".npz"))
+
+
+def golden_matrix(d, name, dtype=np.float64):
+    """EllMatrix (reference layout, T = 1) from a CSR stored in a golden npz."""
+    from honei_b200 import problems as P
+    rows, cols = (int(v) for v in d[f"{name}_shape"])
+    return P.ell_from_csr(rows, cols, d[f"{name}_indptr"], d[f"{name}_indices"], d[f"{name}_data"], 1, dtype)
+
+
+@pytest.fixture(scope="session")
+def featflow():
+    """The MGSolverTest fixture (poisson_advanced4, levels 1..4) as a hierarchy + vectors."""
+    from honei_b200 import problems as P
+    d = load_golden("featflow_pa4")
+    A = [golden_matrix(d, f"A_{l}") for l in range(1, 5)]
+    prol = [golden_matrix(d, f"prol_{l}") for l in range(2, 5)]
+    res = [P.ell_from_csr(p.cols, p.rows, *P.transpose_csr(p.rows, p.cols, *p.to_csr())) for p in prol]
+    return P.MGHierarchy(A, prol, res, [0] * 4), d

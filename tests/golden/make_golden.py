@@ -1,0 +1,141 @@
+"""Generates the committed golden fixtures from the reference itself.
+
+Run where the HONEI tree and oracle/_ref/libhonei_ref.so exist (``make -C oracle ref``):
+
+    python tests/golden/make_golden.py [/path/to/honei-tree]
+
+Outputs (all numbers come from the reference's own CPU path, tags::CPU, through
+oracle/ref_shim.cc; the FEATFLOW2 matrices and vectors are read with the reference's own
+readers, honei/math/matrix_io.hh and honei/math/vector_io.hh):
+
+* featflow_pa4.npz -- the MGSolverTest fixture (honei/math/mg_TEST.cc:224-365, data
+  honei/math/testdata/poisson_advanced4/sort_0): A_1..A_4, prol_2..prol_4, rhs_4, init_4,
+  sol_4, stored as CSR; plus the reference's results on them: V(2,2) MG with the "jac"
+  smoother (damping 0.7) and a CG coarse solver, CG on A_4, SpMV and defect of A_4.
+* defect_5pt.npz -- honei/math/testdata/5pt_10x10.ell (defect_TEST.cc) with a seeded
+  SpMV/defect evaluated by the reference.
+* q1_small.npz -- the reference's own Q1 Poisson construction (FillMatrix -> SparseMatrix ->
+  SparseMatrixELL) at 33^2, with SpMV/CG/MG/IR results, FP64 and FP32, natural, permuted and
+  variable-coefficient variants, plus CG iteration counts at 257^2.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from honei_b200 import problems as P  # noqa: E402
+from oracle.bindings import Reference  # noqa: E402
+
+
+def csr_of(A):
+    ip, ix, dv = A.to_csr()
+    return ip.astype(np.int64), ix.astype(np.int32), dv.astype(np.float64)
+
+
+def put_matrix(out, name, A):
+    ip, ix, dv = csr_of(A)
+    out[f"{name}_shape"] = np.array([A.rows, A.cols], np.int64)
+    out[f"{name}_indptr"] = ip
+    out[f"{name}_indices"] = ix
+    out[f"{name}_data"] = dv
+
+
+def main(tree: str) -> None:
+    R = Reference()
+    td = os.path.join(tree, "honei", "math", "testdata")
+
+    # ---- FEATFLOW2 MG fixture --------------------------------------------------------
+    base = os.path.join(td, "poisson_advanced4", "sort_0") + "/"
+    out = {}
+    A = [R.read_ell(base + f"A_{l}.ell") for l in range(1, 5)]
+    prol = [R.read_ell(base + f"prol_{l}.ell") for l in range(2, 5)]
+    for l, a in enumerate(A, 1):
+        put_matrix(out, f"A_{l}", a)
+    for l, p in enumerate(prol, 2):
+        put_matrix(out, f"prol_{l}", p)
+    for v in ("rhs_4", "init_4", "sol_4"):
+        out[v] = R.read_exp(base + v)
+    res = [P.ell_from_csr(p.cols, p.rows, *P.transpose_csr(p.rows, p.cols, *p.to_csr())) for p in prol]
+    H = P.MGHierarchy(A, prol, res, [0] * 4)
+    x, used, _ = R.mg(H, out["rhs_4"], out["init_4"], damping=0.7, eps=1e-8, max_iters=100,
+                      max_iters_coarse=1000, n_pre=2, n_post=2)
+    out["mg_x"], out["mg_used"] = x, np.array(used)
+    x, used, _ = R.cg(A[3], out["rhs_4"], out["init_4"], max_iters=10000, eps=1e-8)
+    out["cg_x"], out["cg_used"] = x, np.array(used)
+    xs = P.uniform_vector(A[3].rows, 11)
+    out["spmv_x"] = xs
+    out["spmv_y"], _ = R.spmv(A[3], xs)
+    out["defect_r"] = R.defect(A[3], out["rhs_4"], xs)
+    np.savez_compressed(os.path.join(HERE, "featflow_pa4.npz"), **out)
+
+    # ---- 5pt defect fixture -----------------------------------------------------------
+    out = {}
+    A5 = R.read_ell(os.path.join(td, "5pt_10x10.ell"))
+    put_matrix(out, "A", A5)
+    x = P.uniform_vector(A5.cols, 3)
+    b = P.uniform_vector(A5.rows, 4)
+    out["x"], out["b"] = x, b
+    out["y"], _ = R.spmv(A5, x)
+    out["r"] = R.defect(A5, b, x)
+    np.savez_compressed(os.path.join(HERE, "defect_5pt.npz"), **out)
+
+    # ---- Q1 Poisson (reference construction) -----------------------------------------
+    out = {}
+    M = 33
+    Aq = R.q1_poisson(M)
+    out["q1_Aj"], out["q1_Ax"], out["q1_Arl"] = Aq.Aj, Aq.Ax, Aq.Arl
+    out["q1_info"] = np.array(Aq.info() + [Aq.nnz], np.int64)
+    x = P.uniform_vector(Aq.rows, 2)
+    out["spmv_x"] = x
+    out["spmv_y64"], _ = R.spmv(Aq, x)
+    A32 = Aq.astype(np.float32)
+    out["spmv_y32"], _ = R.spmv(A32, x.astype(np.float32))
+    xt = P.uniform_vector(Aq.rows, 1)
+    b, _ = R.spmv(Aq, xt)
+    out["b"] = b
+    x64, u64, _ = R.cg(Aq, b, eps=1e-8)
+    out["cg_x64"], out["cg_used64"] = x64, np.array(u64)
+    x32, u32, _ = R.cg(A32, b.astype(np.float32), eps=1e-5)
+    out["cg_x32"], out["cg_used32"] = x32, np.array(u32)
+    H = P.mg_hierarchy(M)
+    xm, um, _ = R.mg(H, b, eps=1e-8)
+    out["mg_x64"], out["mg_used64"] = xm, np.array(um)
+    H32 = H.astype(np.float32)
+    xm, um, _ = R.mg(H32, b.astype(np.float32), eps=1e-5)
+    out["mg_x32"], out["mg_used32"] = xm, np.array(um)
+    xi, ui, _ = R.ir_mg(H, H32, b, eps=1e-10, inner_eps=1e-3)
+    out["ir_x"], out["ir_used"] = xi, np.array(ui)
+    # permuted variant (seed 7) and variable coefficient (seed 5, log-uniform [1e-2, 1e2])
+    Ap, perm = P.q1_poisson_permuted(M, 7)
+    bp = np.empty_like(b)
+    bp[perm] = b
+    out["perm"] = perm
+    out["perm_spmv_y"], _ = R.spmv(Ap, x)
+    xp, up, _ = R.cg(Ap, bp, eps=1e-8)
+    out["perm_cg_x"], out["perm_cg_used"] = xp, np.array(up)
+    coef = P.log_uniform_coef(M, 1e-2, 1e2, 5)
+    Av = P.q1_poisson(M, coef)
+    bv, _ = R.spmv(Av, xt)
+    out["var_b"] = bv
+    xv, uv, _ = R.cg(Av, bv, eps=1e-8)
+    out["var_cg_x"], out["var_cg_used"] = xv, np.array(uv)
+    # 257^2, plain FP64 CG (the CG-latency workload); iteration count and checksums only
+    A257 = R.q1_poisson(257)
+    xt257 = P.uniform_vector(A257.rows, 1)
+    b257, _ = R.spmv(A257, xt257)
+    x257, u257, _ = R.cg(A257, b257, eps=1e-8)
+    out["cg257_used"] = np.array(u257)
+    out["cg257_x_sample"] = x257[::97].copy()
+    out["cg257_x_sum"] = np.array(x257.sum())
+    np.savez_compressed(os.path.join(HERE, "q1_small.npz"), **out)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

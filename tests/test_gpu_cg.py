@@ -1,0 +1,147 @@
+"""GPU parity of CGSolver<GPU, NONE> against the oracle (honei/math/cg.hh:63-133).
+
+Tolerance (the solver bar): the iteration count within +-1 of the oracle's, the final true
+relative residual ||b - A x|| / ||b|| within 1e-10 of the oracle's (both ~1e-8), and the
+solutions equal to within the accuracy the stopping rule guarantees.  FP32 solves use the
+FP32 bar: iterations within 2% + 1, residual matching to 1e-5 relative of ||b||.
+The dot products are fixed-order trees on the GPU and sequential sums on tags::CPU, so the
+iterates differ at round-off level; everything elementwise is bit-identical.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from honei_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def hb():
+    from honei_b200 import la
+    assert torch.cuda.is_available()
+    return la
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def relres(oracle, A, b, x):
+    r = oracle.defect(A, b, x)
+    return np.linalg.norm(r) / np.linalg.norm(b)
+
+
+def run_cg(hb, A, b, eps, max_iters=20000, x0=None):
+    Ad = hb.SparseMatrixELL.from_reference(A)
+    x = dev(np.zeros(A.rows, A.dtype) if x0 is None else x0.astype(A.dtype))
+    used = hb.CGSolver.value(Ad, None, dev(b.astype(A.dtype)), x, max_iters, eps)
+    torch.cuda.synchronize()
+    return x.cpu().numpy(), used
+
+
+CASES64 = [
+    ("q1_33", lambda: P.q1_poisson(33)),
+    ("q1_257", lambda: P.q1_poisson(257)),
+    ("q1_129_varcoef", lambda: P.q1_poisson(129, P.log_uniform_coef(129, 1e-2, 1e2, 5))),
+    ("q1_129_permuted", lambda: P.q1_poisson_permuted(129, 3)[0]),
+    ("q1_65_threads4", lambda: P.ell_from_csr(4225, 4225, *P.q1_poisson_csr(65), threads=4)),
+]
+
+
+@pytest.mark.parametrize("name,make", CASES64, ids=[c[0] for c in CASES64])
+def test_cg_f64_parity(hb, oracle, name, make):
+    A = make()
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 1))
+    x_o, u_o = oracle.cg(A, b, eps=1e-8, max_iters=20000)
+    x_g, u_g = run_cg(hb, A, b, 1e-8)
+    assert abs(u_g - u_o) <= 1, (u_g, u_o)
+    rg, ro = relres(oracle, A, b, x_g), relres(oracle, A, b, x_o)
+    assert abs(rg - ro) <= 1e-10, (rg, ro)
+    assert np.linalg.norm(x_g - x_o) <= 1e-6 * np.linalg.norm(x_o)
+
+
+def test_cg_257_matches_reference_fixture(hb, oracle):
+    """The plain FP64 CG workload (257^2 Q1, x_true U[-1,1], x0 = 0, 1e-8): the reference's
+    own iteration count from the golden fixture."""
+    d = load_golden("q1_small")
+    A = P.q1_poisson(257)
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 1))
+    x_g, u_g = run_cg(hb, A, b, 1e-8)
+    assert abs(u_g - int(d["cg257_used"])) <= 1
+    assert relres(oracle, A, b, x_g) < 1.2e-8
+
+
+def test_cg_f32_parity(hb, oracle):
+    for M in (33, 129):
+        A = P.q1_poisson(M).astype(np.float32)
+        b = oracle.spmv(A, P.uniform_vector(A.rows, 1).astype(np.float32))
+        x_o, u_o = oracle.cg(A, b, eps=1e-5, max_iters=20000)
+        x_g, u_g = run_cg(hb, A, b, 1e-5)
+        assert abs(u_g - u_o) <= 0.02 * u_o + 1, (u_g, u_o)
+        r_o = relres(oracle, A.astype(np.float64), b.astype(np.float64), x_o.astype(np.float64))
+        r_g = relres(oracle, A.astype(np.float64), b.astype(np.float64), x_g.astype(np.float64))
+        assert abs(r_g - r_o) <= 1e-5, (r_g, r_o)
+
+
+def test_cg_edge_cases(hb, oracle):
+    A = P.q1_poisson(17)
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 2))
+    # max_iters bounds the loop and is reported as used
+    x_g, u_g = run_cg(hb, A, b, 1e-12, max_iters=7)
+    x_o, u_o = oracle.cg(A, b, eps=1e-12, max_iters=7)
+    assert u_g == u_o == 7
+    assert np.linalg.norm(x_g - x_o) <= 1e-12 * np.linalg.norm(x_o)
+    # zero right-hand side: the absolute test fires after one iteration, x stays 0
+    x_g, u_g = run_cg(hb, A, np.zeros(A.rows), 1e-8)
+    x_o, u_o = oracle.cg(A, np.zeros(A.rows), eps=1e-8)
+    assert u_g == u_o and np.array_equal(x_g, x_o)
+    # max_iters = 0: no iteration, x unchanged
+    x0 = P.uniform_vector(A.rows, 3)
+    x_g, u_g = run_cg(hb, A, b, 1e-8, max_iters=0, x0=x0)
+    assert u_g == 0 and np.array_equal(x_g, x0)
+    # non-zero start vector
+    x_g, u_g = run_cg(hb, A, b, 1e-8, x0=x0)
+    x_o, u_o = oracle.cg(A, b, x0=x0, eps=1e-8)
+    assert abs(u_g - u_o) <= 1
+    # tiny systems (one block, ragged row count)
+    for M in (2, 3, 5):
+        A = P.q1_poisson(M)
+        b = P.uniform_vector(A.rows, M)
+        x_g, u_g = run_cg(hb, A, b, 1e-8)
+        x_o, u_o = oracle.cg(A, b, eps=1e-8)
+        assert u_g == u_o and np.allclose(x_g, x_o, rtol=0, atol=1e-14)
+
+
+def test_cg_deterministic(hb, oracle):
+    A = P.q1_poisson(129)
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 1))
+    xs = [run_cg(hb, A, b, 1e-8) for _ in range(3)]
+    assert all(np.array_equal(xs[0][0], x) and xs[0][1] == u for x, u in xs)
+
+
+def test_cg_size_mismatch_raises(hb):
+    A = hb.SparseMatrixELL.q1_poisson(9)
+    with pytest.raises(hb.VectorSizeDoesNotMatch):
+        hb.CGSolver.value(A, None, torch.zeros(80, dtype=torch.float64, device="cuda"),
+                          torch.zeros(81, dtype=torch.float64, device="cuda"), 10)
+
+
+def test_cg_full_size_1025_property(hb):
+    """At 1025^2 (configs' CG size) the oracle takes minutes: check size-independent properties
+    instead -- convergence to the stated relative residual, measured with the GPU's own
+    (bit-exact) defect, and reproducibility."""
+    M = 1025
+    Ad = hb.SparseMatrixELL.q1_poisson(M)
+    xt = dev(P.uniform_vector(M * M, 1))
+    b = torch.empty_like(xt)
+    hb.Product.value(b, Ad, xt)
+    x = torch.zeros_like(xt)
+    used = hb.CGSolver.value(Ad, None, b, x, 20000, 1e-8)
+    r = torch.empty_like(xt)
+    hb.Defect.value(r, b, Ad, x)
+    rel = hb.Norm.value(r, root=True) / hb.Norm.value(b, root=True)
+    assert used < 20000 and rel < 1.5e-8
+    x2 = torch.zeros_like(xt)
+    assert hb.CGSolver.value(Ad, None, b, x2, 20000, 1e-8) == used and torch.equal(x, x2)

@@ -1,0 +1,142 @@
+"""Pins the plain-C oracle and the problem generators to the reference.
+
+* Always (no HONEI tree needed): against the committed golden fixtures, which hold the
+  reference's own outputs (tests/golden/make_golden.py).
+* Where oracle/_ref/libhonei_ref.so exists: live, against the reference's CPU path.
+Bit-exact comparisons throughout: the oracle restates tags::CPU's arithmetic order.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_matrix, load_golden
+from honei_b200 import problems as P
+
+
+def test_q1_generator_matches_reference_construction():
+    d = load_golden("q1_small")
+    A = P.q1_poisson(33)
+    rows, cols, stride, ncpr, T, nnz = (int(v) for v in d["q1_info"])
+    assert (A.rows, A.cols, A.stride, A.ncpr, A.threads, A.nnz) == (rows, cols, stride, ncpr, T, nnz)
+    assert np.array_equal(A.Aj, d["q1_Aj"])
+    assert np.array_equal(A.Ax, d["q1_Ax"])
+    assert np.array_equal(A.Arl, d["q1_Arl"])
+
+
+def test_oracle_spmv_cg_mg_ir_match_reference_q1():
+    from oracle.bindings import Oracle
+    O = Oracle()
+    d = load_golden("q1_small")
+    A = P.q1_poisson(33)
+    assert np.array_equal(O.spmv(A, d["spmv_x"]), d["spmv_y64"])
+    A32 = A.astype(np.float32)
+    assert np.array_equal(O.spmv(A32, d["spmv_x"].astype(np.float32)), d["spmv_y32"])
+    b = d["b"]
+    x, used = O.cg(A, b, eps=1e-8)
+    assert used == int(d["cg_used64"]) and np.array_equal(x, d["cg_x64"])
+    x, used = O.cg(A32, b.astype(np.float32), eps=1e-5)
+    assert used == int(d["cg_used32"]) and np.array_equal(x, d["cg_x32"])
+    H = P.mg_hierarchy(33)
+    x, used = O.mg(H, b, eps=1e-8)
+    assert used == int(d["mg_used64"]) and np.array_equal(x, d["mg_x64"])
+    H32 = H.astype(np.float32)
+    x, used = O.mg(H32, b.astype(np.float32), eps=1e-5)
+    assert used == int(d["mg_used32"]) and np.array_equal(x, d["mg_x32"])
+    x, used, _ = O.ir_mg(H.A[-1], H32, b, eps=1e-10, inner_eps=1e-3, warm_start=True)
+    assert used == int(d["ir_used"]) and np.array_equal(x, d["ir_x"])
+
+
+def test_oracle_matches_reference_permuted_and_variable_coefficient():
+    from oracle.bindings import Oracle
+    O = Oracle()
+    d = load_golden("q1_small")
+    Ap, perm = P.q1_poisson_permuted(33, 7)
+    assert np.array_equal(perm, d["perm"])
+    assert np.array_equal(O.spmv(Ap, d["spmv_x"]), d["perm_spmv_y"])
+    bp = np.empty_like(d["b"])
+    bp[perm] = d["b"]
+    x, used = O.cg(Ap, bp, eps=1e-8)
+    assert used == int(d["perm_cg_used"]) and np.array_equal(x, d["perm_cg_x"])
+    Av = P.q1_poisson(33, P.log_uniform_coef(33, 1e-2, 1e2, 5))
+    x, used = O.cg(Av, d["var_b"], eps=1e-8)
+    assert used == int(d["var_cg_used"]) and np.array_equal(x, d["var_cg_x"])
+
+
+def test_oracle_cg_257_iteration_count_and_solution():
+    """The plain FP64 CG workload on 257^2 (566-578 iterations with the reference)."""
+    from oracle.bindings import Oracle
+    O = Oracle()
+    d = load_golden("q1_small")
+    A = P.q1_poisson(257)
+    b = O.spmv(A, P.uniform_vector(A.rows, 1))
+    x, used = O.cg(A, b, eps=1e-8)
+    assert used == int(d["cg257_used"])
+    assert np.array_equal(x[::97], d["cg257_x_sample"])
+    assert x.sum() == float(d["cg257_x_sum"])
+
+
+def test_oracle_featflow_fixture(featflow):
+    """MGSolverTest data (poisson_advanced4): reference MG/CG/SpMV/defect results, and the
+    FEATFLOW2 solution sol_4 within the reference test's own tolerance (8e-3, mg_TEST.cc)."""
+    from oracle.bindings import Oracle
+    O = Oracle()
+    H, d = featflow
+    A4 = H.A[-1]
+    assert np.array_equal(O.spmv(A4, d["spmv_x"]), d["spmv_y"])
+    assert np.array_equal(O.defect(A4, d["rhs_4"], d["spmv_x"]), d["defect_r"])
+    x, used = O.cg(A4, d["rhs_4"], d["init_4"], eps=1e-8)
+    assert used == int(d["cg_used"]) and np.array_equal(x, d["cg_x"])
+    x, used = O.mg(H, d["rhs_4"], d["init_4"], damping=0.7, eps=1e-8, max_iters=100)
+    assert used == int(d["mg_used"]) and np.array_equal(x, d["mg_x"])
+    assert np.max(np.abs(x - d["sol_4"])) < 8e-3
+
+
+def test_oracle_defect_fixture():
+    from oracle.bindings import Oracle
+    O = Oracle()
+    d = load_golden("defect_5pt")
+    A = golden_matrix(d, "A")
+    assert np.array_equal(O.spmv(A, d["x"]), d["y"])
+    assert np.array_equal(O.defect(A, d["b"], d["x"]), d["r"])
+
+
+def test_oracle_threads_layout_matches_reference(reference):
+    """T > 1 lanes per row (ell::threads): the oracle's SpMV follows the reference order."""
+    from oracle.bindings import Oracle
+    O = Oracle()
+    ip, ix, dv = P.q1_poisson_csr(17)
+    for T in (1, 2, 3, 4, 16):
+        A = P.ell_from_csr(289, 289, ip, ix, dv, T)
+        x = P.uniform_vector(289, T)
+        y_ref, _ = reference.spmv(A, x)
+        assert np.array_equal(O.spmv(A, x), y_ref)
+
+
+def test_oracle_live_against_reference(reference):
+    from oracle.bindings import Oracle
+    O = Oracle()
+    for M in (3, 9, 65):
+        Ar = reference.q1_poisson(M)
+        A = P.q1_poisson(M)
+        assert np.array_equal(A.Aj, Ar.Aj) and np.array_equal(A.Ax, Ar.Ax) and np.array_equal(A.Arl, Ar.Arl)
+    A = P.q1_poisson(65, P.log_uniform_coef(65, 1e-1, 1e1, 3))
+    b = O.spmv(A, P.uniform_vector(A.rows, 9))
+    for dt, eps in ((np.float64, 1e-8), (np.float32, 1e-5)):
+        Ad = A.astype(dt)
+        bd = b.astype(dt)
+        x1, u1 = O.cg(Ad, bd, eps=eps)
+        x2, u2, _ = reference.cg(Ad, bd, eps=eps)
+        assert u1 == u2 and np.array_equal(x1, x2)
+        assert O.dot(bd, bd) == reference.dot(bd, bd)
+    H = P.mg_hierarchy(65, coef=P.log_uniform_coef(65, 1e-1, 1e1, 3))
+    x1, u1 = O.mg(H, b)
+    x2, u2, _ = reference.mg(H, b)
+    assert u1 == u2 and np.array_equal(x1, x2)
+
+
+def test_oracle_multicore_tags_agree_on_iterations(reference):
+    """The reference's own tags agree with tags::CPU on the CG iteration count (orientation
+    for the +-1 iteration tolerance used against the GPU)."""
+    A = P.q1_poisson(65)
+    b, _ = reference.spmv(A, P.uniform_vector(A.rows, 1))
+    counts = {tag: reference.cg(A, b, tag=tag)[1] for tag in ("cpu", "generic", "sse", "mc-sse")}
+    assert max(counts.values()) - min(counts.values()) <= 1, counts
