@@ -60,16 +60,22 @@ dot_kernel(int64_t n, const T *__restrict__ x, const T *__restrict__ y, double *
 }
 
 template <typename T, bool SQUARE>
+int dot_launch(hb_context *ctx, int64_t n, const T *x, const T *y, T *out)
+{
+    const int blocks = red_blocks(ctx, n);
+    unsigned *ticket = hb_bar(ctx) + 8;
+    dot_kernel<T, SQUARE><<<blocks, RED_THREADS, 0, ctx->stream>>>(n, x, y, hb_partials(ctx), ticket, out);
+    return hb_check_launch(ctx, "dot_kernel");
+}
+
+template <typename T, bool SQUARE>
 int dot_impl(hb_context *ctx, int64_t n, const T *x, const T *y, T *result_host)
 {
     if (!ctx || !result_host || n < 0) return HB_ERR_INVALID;
     if (n == 0) { *result_host = T(0); return HB_OK; }
     if (!x || (!SQUARE && !y)) return HB_ERR_INVALID;
-    const int blocks = red_blocks(ctx, n);
     T *out = reinterpret_cast<T *>(hb_scalars(ctx) + 8);
-    unsigned *ticket = hb_bar(ctx) + 8;
-    dot_kernel<T, SQUARE><<<blocks, RED_THREADS, 0, ctx->stream>>>(n, x, y, hb_partials(ctx), ticket, out);
-    int st = hb_check_launch(ctx, "dot_kernel");
+    int st = dot_launch<T, SQUARE>(ctx, n, x, y, out);
     if (st) return st;
     HB_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->pinned, out, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
     HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
@@ -135,6 +141,17 @@ int convert_impl(hb_context *ctx, int64_t n, D *dst, const S *src)
 }
 
 }  // namespace
+
+template <typename T> int hb_launch_dot(hb_context *ctx, int64_t n, const T *x, const T *y, T *out_dev)
+{
+    if (n == 0) {
+        HB_CUDA_TRY(ctx, cudaMemsetAsync(out_dev, 0, sizeof(T), ctx->stream));
+        return HB_OK;
+    }
+    return (x == y) ? dot_launch<T, true>(ctx, n, x, x, out_dev) : dot_launch<T, false>(ctx, n, x, y, out_dev);
+}
+template int hb_launch_dot<double>(hb_context *, int64_t, const double *, const double *, double *);
+template int hb_launch_dot<float>(hb_context *, int64_t, const float *, const float *, float *);
 
 extern "C" {
 

@@ -196,17 +196,13 @@ int cg_max_blocks(hb_context *ctx)
     return std::max(1, occ) * ctx->num_sms;
 }
 
+}  // namespace
+
 template <typename T>
-int cg_impl(hb_context *ctx, const hb_ell *A, const T *b, T *x, int64_t max_iters, T eps,
-            int64_t *used_iters, T *final_defect, int dtype)
+int hb_launch_cg(hb_context *ctx, const hb_ell *A, const T *b, T *x, int64_t max_iters, T eps, T *work,
+                 hb_solve_result *res)
 {
-    if (!ctx || !A || !b || !x || !used_iters || max_iters < 0) return HB_ERR_INVALID;
-    if (A->dtype != dtype || !A->Aj || !A->Ax || A->ld % 64 || A->ld < A->rows) return HB_ERR_INVALID;
-    if (A->rows != A->cols) return HB_ERR_SIZE;
-    if (A->rows > INT32_MAX) return HB_ERR_UNSUPPORTED;
     const int64_t ld = A->ld;
-    int st = hb_ensure_work(ctx, (size_t)ld * sizeof(T) * 5);
-    if (st) return st;
     CGParams<T> P;
     P.rows = A->rows;
     P.ld = ld;
@@ -215,8 +211,7 @@ int cg_impl(hb_context *ctx, const hb_ell *A, const T *b, T *x, int64_t max_iter
     P.Ax = (const T *)A->Ax;
     P.b_user = b;
     P.x_user = x;
-    T *w = (T *)ctx->work;
-    P.x = w; P.r = w + ld; P.p0 = w + 2 * ld; P.p1 = w + 3 * ld; P.v = w + 4 * ld;
+    P.x = work; P.r = work + ld; P.p0 = work + 2 * ld; P.p1 = work + 3 * ld; P.v = work + 4 * ld;
     P.max_iters = max_iters;
     P.eps = eps;
     P.partials = (T *)hb_partials(ctx);
@@ -224,19 +219,38 @@ int cg_impl(hb_context *ctx, const hb_ell *A, const T *b, T *x, int64_t max_iter
     P.bar.count = bar;
     P.bar.gen = bar + 1;
     P.bar.status = (int *)(bar + 2);
-    P.res = hb_result(ctx);
+    P.res = res;
     HB_CUDA_TRY(ctx, cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), ctx->stream));
-
     const int64_t groups = ld / 4;
     const bool k9 = (A->K == 9);
     const int maxb = k9 ? cg_max_blocks<T, 9>(ctx) : cg_max_blocks<T, 0>(ctx);
     // about one row group per thread for small systems; all co-resident blocks otherwise
-    int64_t want = (groups + CG_THREADS - 1) / CG_THREADS;
-    int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(maxb, 4096)));
-    st = k9 ? launch_cg_kt<T, 9>(ctx, P, blocks) : launch_cg_kt<T, 0>(ctx, P, blocks);
+    const int64_t want = (groups + CG_THREADS - 1) / CG_THREADS;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(maxb, 4096)));
+    return k9 ? launch_cg_kt<T, 9>(ctx, P, blocks) : launch_cg_kt<T, 0>(ctx, P, blocks);
+}
+template int hb_launch_cg<double>(hb_context *, const hb_ell *, const double *, double *, int64_t, double,
+                                  double *, hb_solve_result *);
+template int hb_launch_cg<float>(hb_context *, const hb_ell *, const float *, float *, int64_t, float, float *,
+                                 hb_solve_result *);
+
+namespace {
+
+template <typename T>
+int cg_impl(hb_context *ctx, const hb_ell *A, const T *b, T *x, int64_t max_iters, T eps,
+            int64_t *used_iters, T *final_defect, int dtype)
+{
+    if (!ctx || !A || !b || !x || !used_iters || max_iters < 0) return HB_ERR_INVALID;
+    int st = hb_check_ell(A, dtype);
+    if (st) return st;
+    if (A->rows != A->cols) return HB_ERR_SIZE;
+    st = hb_ensure_work(ctx, (size_t)A->ld * sizeof(T) * 5);
+    if (st) return st;
+    st = hb_launch_cg<T>(ctx, A, b, x, max_iters, eps, (T *)ctx->work, hb_result(ctx));
     if (st) return st;
     hb_solve_result *h = (hb_solve_result *)ctx->pinned;
-    HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, P.res, sizeof(hb_solve_result), cudaMemcpyDeviceToHost, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, hb_result(ctx), sizeof(hb_solve_result), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
     HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     if (h->status == HB_DEV_TIMEOUT) return HB_ERR_TIMEOUT;
     *used_iters = h->used;

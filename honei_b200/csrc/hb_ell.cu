@@ -8,7 +8,7 @@
 // evict-first loads).  Per row the sum runs over the slots in the reference order with one
 // rounding per multiply and add, so y is bit-identical to Product<tags::CPU>
 // (honei/la/product.hh:148-204).
-#include "hb_internal.cuh"
+#include "hb_spmv_core.cuh"
 
 namespace {
 
@@ -108,95 +108,126 @@ __global__ void q1_assemble_kernel(int64_t M, const double *__restrict__ coef, i
 }
 
 // ---------------------------------------------------------------------------------------
-// SpMV / defect.  KT > 0: K known at compile time (all slot loads issued up front);
-// KT == 0: runtime K in chunks of 4 slots.
+// SpMV family, one kernel template per output mode:
+//   SPMV    y = A x                                   (Product)
+//   DEFECT  y = b - A x                               (Defect: temp = A x; r = b - temp)
+//   ADD     y = y + A x                               (Prolongation<PROLMAT> + Sum: store = P c; x += store)
+//   JACOBI  y = x + P * (b - A x)                     (one RISmoother sweep: t0 = b - A x; t1 = P t0; x += t1)
+// Each rounds exactly as the reference's operator sequence does, so the results are
+// bit-identical to tags::CPU.  x is read-only for the whole launch (gathered through L1).
 // ---------------------------------------------------------------------------------------
-template <typename T, int KT, bool DEFECT>
+template <typename T, int KT, int MODE>
 __global__ void __launch_bounds__(SPMV_THREADS)
 ell_spmv_kernel(int64_t rows, int64_t ld, int K, const int32_t *__restrict__ Aj,
                 const T *__restrict__ Ax, const T *__restrict__ x, const T *__restrict__ b,
-                T *__restrict__ y, int vec_io)
+                const T *__restrict__ P, T *__restrict__ y, int vec_io)
 {
-    using hbd::add; using hbd::mul;
+    using hbd::add; using hbd::mul; using hbd::sub;
     const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t r0 = g * 4;
     if (r0 >= rows) return;
-    T sum[4] = {T(0), T(0), T(0), T(0)};
-    if (KT > 0) {
-        int32_t j[KT > 0 ? KT : 1][4];
-        T a[KT > 0 ? KT : 1][4];
-#pragma unroll
-        for (int k = 0; k < KT; ++k) {
-            hbd::ld4_stream(Aj + k * ld + r0, j[k]);
-            hbd::ld4_stream(Ax + k * ld + r0, a[k]);
-        }
-#pragma unroll
-        for (int k = 0; k < KT; ++k)
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-                if (j[k][i] >= 0) sum[i] = add(sum[i], mul(a[k][i], __ldg(x + j[k][i])));
-    } else {
-        for (int k0 = 0; k0 < K; k0 += 4) {
-            int32_t j[4][4];
-            T a[4][4];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                if (k0 + c < K) {
-                    hbd::ld4_stream(Aj + (k0 + c) * ld + r0, j[c]);
-                    hbd::ld4_stream(Ax + (k0 + c) * ld + r0, a[c]);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) { j[c][i] = -1; a[c][i] = T(0); }
-                }
-            }
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    if (j[c][i] >= 0) sum[i] = add(sum[i], mul(a[c][i], __ldg(x + j[c][i])));
-        }
-    }
+    T sum[4];
+    hbd::ell_rows4<T, KT>(Aj, Ax, ld, K, r0, [&](int32_t j) { return __ldg(x + j); }, sum);
+    T out[4];
     if (vec_io && r0 + 3 < rows) {
-        if (DEFECT) {
-            T bb[4];
-            hbd::ld4(b + r0, bb);
+        T bb[4], xx[4], pp[4], yy[4];
+        if (MODE == HB_MODE_DEFECT || MODE == HB_MODE_JACOBI) hbd::ld4(b + r0, bb);
+        if (MODE == HB_MODE_JACOBI) { hbd::ld4(x + r0, xx); hbd::ld4(P + r0, pp); }
+        if (MODE == HB_MODE_ADD) hbd::ld4(y + r0, yy);
 #pragma unroll
-            for (int i = 0; i < 4; ++i) sum[i] = hbd::sub(bb[i], sum[i]);
+        for (int i = 0; i < 4; ++i) {
+            if (MODE == HB_MODE_SPMV) out[i] = sum[i];
+            if (MODE == HB_MODE_DEFECT) out[i] = sub(bb[i], sum[i]);
+            if (MODE == HB_MODE_ADD) out[i] = add(yy[i], sum[i]);
+            if (MODE == HB_MODE_JACOBI) out[i] = add(xx[i], mul(pp[i], sub(bb[i], sum[i])));
         }
-        hbd::st4(y + r0, sum);
+        hbd::st4(y + r0, out);
     } else {
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-            if (r0 + i < rows) y[r0 + i] = DEFECT ? hbd::sub(b[r0 + i], sum[i]) : sum[i];
+        for (int i = 0; i < 4; ++i) {
+            const int64_t r = r0 + i;
+            if (r >= rows) break;
+            T o = sum[i];
+            if (MODE == HB_MODE_DEFECT) o = sub(b[r], sum[i]);
+            if (MODE == HB_MODE_ADD) o = add(y[r], sum[i]);
+            if (MODE == HB_MODE_JACOBI) o = add(x[r], mul(P[r], sub(b[r], sum[i])));
+            y[r] = o;
+        }
     }
 }
 
-template <typename T, bool DEFECT>
-int launch_spmv(hb_context *ctx, const hb_ell *A, const T *x, const T *b, T *y)
+// P[i] = damping / A(i, i), A(i, i) = the first slot of row i holding column i
+// (SparseMatrixELL::operator(), honei/la/sparse_matrix_ell-impl.hh:326-338; PreconFill "jac",
+// honei/math/mg.hh:255-286).
+template <typename T>
+__global__ void jacobi_diag_kernel(int64_t rows, int64_t ld, int K, const int32_t *__restrict__ Aj,
+                                   const T *__restrict__ Ax, T damping, T *__restrict__ P)
+{
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        T d = T(0);
+        for (int k = 0; k < K; ++k) {
+            if (Aj[k * ld + r] == (int32_t)r) { d = Ax[k * ld + r]; break; }
+        }
+        P[r] = damping / d;
+    }
+}
+
+}  // namespace
+
+template <typename T>
+int hb_launch_spmv_mode(hb_context *ctx, const hb_ell *A, int mode, const T *x, const T *b, const T *P, T *y)
 {
     if (!ctx || !A) return HB_ERR_INVALID;
     if (A->rows == 0) return HB_OK;
-    if (!x || !y || (DEFECT && !b)) return HB_ERR_INVALID;
+    if (!x || !y) return HB_ERR_INVALID;
+    if ((mode == HB_MODE_DEFECT || mode == HB_MODE_JACOBI) && !b) return HB_ERR_INVALID;
+    if (mode == HB_MODE_JACOBI && !P) return HB_ERR_INVALID;
     const int64_t groups = (A->rows + 3) / 4;
     const int64_t blocks = (groups + SPMV_THREADS - 1) / SPMV_THREADS;
-    const int vec = (((uintptr_t)y | (DEFECT ? (uintptr_t)b : 0)) % 16) == 0;
+    const int vec = (((uintptr_t)y | (uintptr_t)b | (uintptr_t)P |
+                      (mode == HB_MODE_JACOBI ? (uintptr_t)x : 0)) % 16) == 0;
     const int K = (int)A->K;
     const int32_t *Aj = A->Aj;
     const T *Ax = (const T *)A->Ax;
-#define HB_SPMV_CASE(KC)                                                                       \
-    ell_spmv_kernel<T, KC, DEFECT><<<(unsigned)blocks, SPMV_THREADS, 0, ctx->stream>>>(         \
-        A->rows, A->ld, K, Aj, Ax, x, b, y, vec)
-    switch (K) {
-        case 1: HB_SPMV_CASE(1); break;
-        case 4: HB_SPMV_CASE(4); break;
-        case 9: HB_SPMV_CASE(9); break;
-        default: HB_SPMV_CASE(0); break;
+#define HB_SPMV_CASE(KC, MD)                                                                    \
+    ell_spmv_kernel<T, KC, MD><<<(unsigned)blocks, SPMV_THREADS, 0, ctx->stream>>>(              \
+        A->rows, A->ld, K, Aj, Ax, x, b, P, y, vec)
+#define HB_SPMV_K(MD)                                                                           \
+    switch (K) {                                                                                \
+        case 4: HB_SPMV_CASE(4, MD); break;                                                     \
+        case 9: HB_SPMV_CASE(9, MD); break;                                                     \
+        default: HB_SPMV_CASE(0, MD); break;                                                    \
     }
+    switch (mode) {
+        case HB_MODE_SPMV: HB_SPMV_K(HB_MODE_SPMV); break;
+        case HB_MODE_DEFECT: HB_SPMV_K(HB_MODE_DEFECT); break;
+        case HB_MODE_ADD: HB_SPMV_K(HB_MODE_ADD); break;
+        case HB_MODE_JACOBI: HB_SPMV_K(HB_MODE_JACOBI); break;
+        default: return HB_ERR_INVALID;
+    }
+#undef HB_SPMV_K
 #undef HB_SPMV_CASE
-    return hb_check_launch(ctx, DEFECT ? "ell_defect_kernel" : "ell_spmv_kernel");
+    return hb_check_launch(ctx, "ell_spmv_kernel");
 }
+template int hb_launch_spmv_mode<double>(hb_context *, const hb_ell *, int, const double *, const double *,
+                                         const double *, double *);
+template int hb_launch_spmv_mode<float>(hb_context *, const hb_ell *, int, const float *, const float *,
+                                        const float *, float *);
 
-int check_ell(const hb_ell *A, int dtype)
+template <typename T>
+int hb_launch_jacobi_diag(hb_context *ctx, const hb_ell *A, T damping, T *P)
+{
+    if (A->rows == 0) return HB_OK;
+    const unsigned blocks = (unsigned)std::min<int64_t>((A->rows + 255) / 256, (int64_t)ctx->num_sms * 16);
+    jacobi_diag_kernel<T><<<blocks, 256, 0, ctx->stream>>>(A->rows, A->ld, (int)A->K, A->Aj, (const T *)A->Ax,
+                                                           damping, P);
+    return hb_check_launch(ctx, "jacobi_diag_kernel");
+}
+template int hb_launch_jacobi_diag<double>(hb_context *, const hb_ell *, double, double *);
+template int hb_launch_jacobi_diag<float>(hb_context *, const hb_ell *, float, float *);
+
+int hb_check_ell(const hb_ell *A, int dtype)
 {
     if (!A || !A->Aj || !A->Ax) return HB_ERR_INVALID;
     if (A->dtype != dtype) return HB_ERR_INVALID;
@@ -205,6 +236,8 @@ int check_ell(const hb_ell *A, int dtype)
     if (((uintptr_t)A->Aj | (uintptr_t)A->Ax) % 16) return HB_ERR_INVALID;
     return HB_OK;
 }
+
+namespace {
 
 template <typename T>
 int import_impl(hb_context *ctx, int64_t rows, int64_t cols, int64_t stride, int64_t ncpr,
@@ -220,7 +253,7 @@ int import_impl(hb_context *ctx, int64_t rows, int64_t cols, int64_t stride, int
     int64_t K, ld;
     hb_ell_layout(rows, ncpr, threads, &K, &ld);
     if (out->K != K || out->ld != ld) return HB_ERR_SIZE;
-    int st = check_ell(out, dtype);
+    int st = hb_check_ell(out, dtype);
     if (st) return st;
     int *bad = (int *)hb_scalars(ctx);
     HB_CUDA_TRY(ctx, cudaMemsetAsync(bad, 0, sizeof(int), ctx->stream));
@@ -265,13 +298,13 @@ int hb_ell_import_f32(hb_context *ctx, int64_t rows, int64_t cols, int64_t strid
 int hb_ell_cast_f64_f32(hb_context *ctx, const hb_ell *src, hb_ell *dst)
 {
     if (!ctx) return HB_ERR_INVALID;
-    int st = check_ell(src, HB_F64);
+    int st = hb_check_ell(src, HB_F64);
     if (st) return st;
     if (!dst || dst->K != src->K || dst->ld != src->ld) return HB_ERR_SIZE;
     dst->rows = src->rows;
     dst->cols = src->cols;
     dst->dtype = HB_F32;
-    st = check_ell(dst, HB_F32);
+    st = hb_check_ell(dst, HB_F32);
     if (st) return st;
     const int64_t total = src->K * src->ld;
     HB_CUDA_TRY(ctx, cudaMemcpyAsync(dst->Aj, src->Aj, total * sizeof(int32_t), cudaMemcpyDeviceToDevice,
@@ -291,7 +324,7 @@ int hb_q1_assemble_f64(hb_context *ctx, int64_t M, const double *coef, hb_ell *o
     out->rows = N;
     out->cols = N;
     out->dtype = HB_F64;
-    int st = check_ell(out, HB_F64);
+    int st = hb_check_ell(out, HB_F64);
     if (st) return st;
     const unsigned blocks = (unsigned)std::min<int64_t>((ld + 255) / 256, (int64_t)ctx->num_sms * 32);
     q1_assemble_kernel<<<blocks, 256, 0, ctx->stream>>>(M, coef, ld, out->Aj, (double *)out->Ax);
@@ -300,32 +333,32 @@ int hb_q1_assemble_f64(hb_context *ctx, int64_t M, const double *coef, hb_ell *o
 
 int hb_spmv_f64(hb_context *ctx, const hb_ell *A, const double *x, double *y)
 {
-    int st = check_ell(A, HB_F64);
+    int st = hb_check_ell(A, HB_F64);
     if (st) return st;
-    return launch_spmv<double, false>(ctx, A, x, nullptr, y);
+    return hb_launch_spmv_mode<double>(ctx, A, HB_MODE_SPMV, x, nullptr, nullptr, y);
 }
 
 int hb_spmv_f32(hb_context *ctx, const hb_ell *A, const float *x, float *y)
 {
-    int st = check_ell(A, HB_F32);
+    int st = hb_check_ell(A, HB_F32);
     if (st) return st;
-    return launch_spmv<float, false>(ctx, A, x, nullptr, y);
+    return hb_launch_spmv_mode<float>(ctx, A, HB_MODE_SPMV, x, nullptr, nullptr, y);
 }
 
 int hb_defect_f64(hb_context *ctx, const hb_ell *A, const double *b, const double *x, double *r)
 {
-    int st = check_ell(A, HB_F64);
+    int st = hb_check_ell(A, HB_F64);
     if (st) return st;
     if (A->rows != A->cols) return HB_ERR_SIZE;
-    return launch_spmv<double, true>(ctx, A, x, b, r);
+    return hb_launch_spmv_mode<double>(ctx, A, HB_MODE_DEFECT, x, b, nullptr, r);
 }
 
 int hb_defect_f32(hb_context *ctx, const hb_ell *A, const float *b, const float *x, float *r)
 {
-    int st = check_ell(A, HB_F32);
+    int st = hb_check_ell(A, HB_F32);
     if (st) return st;
     if (A->rows != A->cols) return HB_ERR_SIZE;
-    return launch_spmv<float, true>(ctx, A, x, b, r);
+    return hb_launch_spmv_mode<float>(ctx, A, HB_MODE_DEFECT, x, b, nullptr, r);
 }
 
 }  // extern "C"

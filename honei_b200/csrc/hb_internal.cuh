@@ -67,6 +67,23 @@ inline double *hb_scalars(hb_context *c) { return (double *)((char *)c->scratch 
 
 inline int64_t hb_round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
+// Output modes of the SpMV family (hb_ell.cu).
+enum { HB_MODE_SPMV = 0, HB_MODE_DEFECT = 1, HB_MODE_ADD = 2, HB_MODE_JACOBI = 3 };
+
+int hb_check_ell(const hb_ell *A, int dtype);
+// y = A x | b - A x | y + A x | x + P (b - A x), asynchronous on ctx->stream.
+template <typename T>
+int hb_launch_spmv_mode(hb_context *ctx, const hb_ell *A, int mode, const T *x, const T *b, const T *P, T *y);
+// P[i] = damping / A(i, i)
+template <typename T> int hb_launch_jacobi_diag(hb_context *ctx, const hb_ell *A, T damping, T *P);
+// Sum of squares / dot product into a device scalar (no host sync).
+template <typename T> int hb_launch_dot(hb_context *ctx, int64_t n, const T *x, const T *y, T *out_dev);
+// Plain CG (cg.hh semantics) as one persistent kernel, asynchronous: work = 5 * ld entries,
+// result written to *res on the device.
+template <typename T>
+int hb_launch_cg(hb_context *ctx, const hb_ell *A, const T *b, T *x, int64_t max_iters, T eps, T *work,
+                 hb_solve_result *res);
+
 // --------------------------------------------------------------------------------------
 // Device helpers
 // --------------------------------------------------------------------------------------
