@@ -17,6 +17,7 @@
 #include "hb_spmv_core.cuh"
 
 #include <cfloat>
+#include <mutex>
 
 namespace {
 
@@ -275,3 +276,135 @@ int hb_cg_f32(hb_context *ctx, const hb_ell *A, const float *b, float *x, int64_
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free CG: hb_cg_f64_noalloc.
+//
+// For callers that cannot allocate device memory at solve time: code that runs while a
+// stream is being captured into a CUDA graph (cudaMalloc is not allowed there), real-time
+// or embedded hosts that forbid allocation after start-up, and processes whose device memory
+// is entirely reserved by another framework's caching allocator.  The work vectors, the
+// reduction partials, the barrier words and the result record live in one file-scope
+// __device__ array instead of a context's cudaMalloc'd workspace.  Every GPU that loads this
+// library holds the array (NOALLOC_BYTES, about 5.3 MB) until the process exits.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t NOALLOC_MAX_ROWS = 131072;       // rows (= ld bound, a multiple of 64)
+constexpr int NOALLOC_MAX_BLOCKS = 1024;
+constexpr size_t NOALLOC_WORK_BYTES = 5 * (size_t)NOALLOC_MAX_ROWS * sizeof(double);
+constexpr size_t NOALLOC_PART_BYTES = 2 * (size_t)NOALLOC_MAX_BLOCKS * sizeof(double);
+constexpr size_t NOALLOC_BAR_BYTES = 256;
+constexpr size_t NOALLOC_RES_BYTES = 256;
+constexpr size_t NOALLOC_BYTES = NOALLOC_WORK_BYTES + NOALLOC_PART_BYTES + NOALLOC_BAR_BYTES + NOALLOC_RES_BYTES;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char hb_cg_noalloc_scratch[NOALLOC_BYTES];
+
+namespace {
+
+// The symbol's device address, looked up once per device with that device current.  The
+// name hb_cg_noalloc_scratch is only a host-side stand-in in host code; kernels must be given
+// this address.
+struct NoAllocDevice {
+    std::once_flag once;
+    void *base = nullptr;
+    int num_sms = 0;
+    int status = HB_OK;
+};
+NoAllocDevice g_noalloc[NOALLOC_MAX_DEVICES];
+
+int noalloc_setup(int device, NoAllocDevice **out)
+{
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) return HB_ERR_UNSUPPORTED;
+    NoAllocDevice &d = g_noalloc[device];
+    std::call_once(d.once, [&d, device]() {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, hb_cg_noalloc_scratch);
+        if (e != cudaSuccess) { cudaGetLastError(); d.status = HB_ERR_CUDA; return; }
+        int sms = 0;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e != cudaSuccess) { cudaGetLastError(); d.status = HB_ERR_CUDA; return; }
+        d.base = p;
+        d.num_sms = sms;
+    });
+    *out = &d;
+    return d.status;
+}
+
+template <int KT>
+int noalloc_launch(cudaStream_t stream, int num_sms, CGParams<double> &P, int64_t groups)
+{
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, cg_kernel<double, KT>, CG_THREADS, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return HB_ERR_CUDA;
+    }
+    const int64_t maxb = (int64_t)std::max(1, occ) * num_sms;
+    const int64_t want = (groups + CG_THREADS - 1) / CG_THREADS;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(maxb, NOALLOC_MAX_BLOCKS)));
+    void *args[] = {&P};
+    if (cudaLaunchCooperativeKernel((const void *)cg_kernel<double, KT>, dim3(blocks), dim3(CG_THREADS), args, 0,
+                                    stream) != cudaSuccess) {
+        cudaGetLastError();
+        return HB_ERR_CUDA;
+    }
+    return HB_OK;
+}
+
+}  // namespace
+
+extern "C" int hb_cg_f64_noalloc(const hb_ell *A, const double *b, double *x, int64_t max_iters, double eps,
+                                 int64_t *used_iters, double *final_defect, void *stream_)
+{
+    if (!A || !b || !x || !used_iters || max_iters < 0) return HB_ERR_INVALID;
+    int st = hb_check_ell(A, HB_F64);
+    if (st) return st;
+    if (A->rows != A->cols) return HB_ERR_SIZE;
+    if (A->rows > NOALLOC_MAX_ROWS || A->ld > NOALLOC_MAX_ROWS) return HB_ERR_UNSUPPORTED;
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return HB_ERR_CUDA; }
+    NoAllocDevice *d = nullptr;
+    st = noalloc_setup(device, &d);
+    if (st) return st;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    char *base = (char *)d->base;
+    double *work = (double *)base;
+    double *partials = (double *)(base + NOALLOC_WORK_BYTES);
+    unsigned *bar = (unsigned *)(base + NOALLOC_WORK_BYTES + NOALLOC_PART_BYTES);
+    hb_solve_result *res = (hb_solve_result *)(base + NOALLOC_WORK_BYTES + NOALLOC_PART_BYTES + NOALLOC_BAR_BYTES);
+    // the barrier words must start at zero; everything else is written before it is read
+    if (cudaMemsetAsync(bar, 0, NOALLOC_BAR_BYTES, stream) != cudaSuccess) { cudaGetLastError(); return HB_ERR_CUDA; }
+    const int64_t ld = A->ld;
+    CGParams<double> P;
+    P.rows = A->rows;
+    P.ld = ld;
+    P.K = (int)A->K;
+    P.Aj = A->Aj;
+    P.Ax = (const double *)A->Ax;
+    P.b_user = b;
+    P.x_user = x;
+    P.x = work; P.r = work + ld; P.p0 = work + 2 * ld; P.p1 = work + 3 * ld; P.v = work + 4 * ld;
+    P.max_iters = max_iters;
+    P.eps = eps;
+    P.partials = partials;
+    P.bar.count = bar;
+    P.bar.gen = bar + 1;
+    P.bar.status = (int *)(bar + 2);
+    P.res = res;
+    const int64_t groups = ld / 4;
+    st = (A->K == 9) ? noalloc_launch<9>(stream, d->num_sms, P, groups) : noalloc_launch<0>(stream, d->num_sms, P, groups);
+    if (st) return st;
+    hb_solve_result h;
+    if (cudaMemcpyAsync(&h, res, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess) {
+        cudaGetLastError();
+        return HB_ERR_CUDA;
+    }
+    if (h.status == HB_DEV_TIMEOUT) return HB_ERR_TIMEOUT;
+    *used_iters = h.used;
+    if (final_defect) *final_defect = h.defect;
+    return HB_OK;
+}

@@ -175,6 +175,24 @@ int hb_cg_f64(hb_context *ctx, const hb_ell *A, const double *b, double *x, int6
 int hb_cg_f32(hb_context *ctx, const hb_ell *A, const float *b, float *x, int64_t max_iters,
               float eps, int64_t *used_iters, float *final_defect);
 
+/* Allocation-free variant of hb_cg_f64.  This entry point has no counterpart in the reference.
+ * It is for callers that cannot allocate device memory when they solve: code issuing work
+ * while a stream is captured into a CUDA graph (cudaMalloc is not allowed there), real-time
+ * or embedded hosts that forbid allocation after start-up, and processes whose device memory
+ * is held entirely by another framework's caching allocator.  It needs no hb_context: its
+ * work vectors, reduction partials, barrier words and result record live in one static
+ * __device__ array of about 5.3 MB that every GPU loading this library keeps until exit.
+ * Limit: A->rows <= 131072 (FP64; e.g. the 257 x 257 Q1 grid); larger systems return
+ * HB_ERR_UNSUPPORTED without launching.  The caller passes A, b, x (device) and the stream
+ * (cudaStream_t, NULL = legacy stream); results as for hb_cg_f64.  It calls no cudaMalloc,
+ * cudaFree or other allocating routine.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current: make that first call
+ * before any stream capture.  All calls on a device share the one array, so calls that
+ * overlap on the GPU (different streams, threads or processes' streams at once) race and
+ * must be serialised by the caller; the barrier words are re-zeroed by every call. */
+int hb_cg_f64_noalloc(const hb_ell *A, const double *b, double *x, int64_t max_iters, double eps,
+                      int64_t *used_iters, double *final_defect, void *stream);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -1,0 +1,87 @@
+"""hb_cg_f64_noalloc: the allocation-free CG entry point, checked against hb_cg_f64.
+
+The entry point exists for callers that cannot allocate device memory when they solve (work
+issued during CUDA-graph stream capture, real-time hosts that forbid allocation after
+start-up, processes whose device memory is held by another framework's caching allocator).
+It keeps its scratch in a static device array, so it must give the same answer as the
+context-based hb_cg_f64 -- call after call, since the array keeps the previous call's
+contents.  This file is collected last; it passes alone in a fresh process and after the
+other tests.  Both calls go straight through the C ABI.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from honei_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _ell(t_aj, t_ax, rows, K, ld):
+    from honei_b200._lib import HbEll
+    return HbEll(rows, rows, K, ld, t_aj.data_ptr(), t_ax.data_ptr(), 0, 0)
+
+
+def _solve_noalloc(lib, A, b, x, max_iters, eps):
+    used, d = C.c_int64(0), C.c_double(0)
+    st = lib.hb_cg_f64_noalloc(C.byref(A), b.data_ptr(), x.data_ptr(), max_iters, eps, C.byref(used),
+                               C.byref(d), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    return st, used.value, d.value
+
+
+def _solve_ctx(lib, ctx, A, b, x, max_iters, eps):
+    used, d = C.c_int64(0), C.c_double(0)
+    st = lib.hb_cg_f64(ctx, C.byref(A), b.data_ptr(), x.data_ptr(), max_iters, eps, C.byref(used), C.byref(d))
+    return st, used.value, d.value
+
+
+def test_noalloc_cg_matches_context_cg_twice_in_a_row():
+    from honei_b200._lib import lib
+    from honei_b200.la import SparseMatrixELL
+    L = lib()
+    assert torch.cuda.is_available()
+    ctx = C.c_void_p()
+    assert L.hb_create(C.byref(ctx), torch.cuda.current_device()) == 0
+    assert L.hb_set_stream(ctx, C.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
+    try:
+        # two different systems back to back, so the second call starts from the first
+        # call's leftovers in the static array
+        for M, seed in ((257, 1), (65, 2)):
+            Ad = SparseMatrixELL.from_reference(P.q1_poisson(M, P.log_uniform_coef(M, 1e-1, 1e1, seed)))
+            A = _ell(Ad.Aj, Ad.Ax, Ad.rows(), Ad.K, Ad.ld)
+            xt = torch.from_numpy(P.uniform_vector(M * M, seed)).cuda()
+            b = torch.empty_like(xt)
+            from honei_b200 import la
+            la.Product.value(b, Ad, xt)
+            x_ref = torch.zeros_like(xt)
+            st, u_ref, d_ref = _solve_ctx(L, ctx, A, b, x_ref, 20000, 1e-8)
+            assert st == 0
+            for _ in range(2):
+                x = torch.zeros_like(xt)
+                st, u, d = _solve_noalloc(L, A, b, x, 20000, 1e-8)
+                assert st == 0
+                # same kernel, same launch shape: identical, which is inside the CG tolerance
+                # (+-1 iteration, residual to 1e-10) the other tests use
+                assert abs(u - u_ref) <= 1 and u == u_ref
+                assert abs(d - d_ref) <= 1e-10 * max(d_ref, 1e-300) or d == d_ref
+                assert torch.equal(x, x_ref)
+                rel = (x - xt).norm().item() / xt.norm().item()
+                assert rel < 1e-4
+    finally:
+        L.hb_destroy(ctx)
+
+
+def test_noalloc_cg_rejects_systems_over_the_limit():
+    from honei_b200._lib import lib
+    from honei_b200.la import SparseMatrixELL
+    L = lib()
+    M = 363                                  # 131769 rows > 131072
+    Ad = SparseMatrixELL.q1_poisson(M)
+    A = _ell(Ad.Aj, Ad.Ax, Ad.rows(), Ad.K, Ad.ld)
+    b = torch.ones(M * M, dtype=torch.float64, device="cuda")
+    x = torch.zeros_like(b)
+    st, _, _ = _solve_noalloc(L, A, b, x, 10, 1e-8)
+    assert st == 6                           # HB_ERR_UNSUPPORTED, nothing launched
+    assert torch.count_nonzero(x).item() == 0
