@@ -1,0 +1,394 @@
+// hb_mg.cu -- multigrid (MGSolver with a V(n_pre, n_post) cycle) and mixed-precision
+// iterative refinement (IRSolver) on the device.
+//
+// Reference: MGData / MGCycleCreation<V::STATIC, CGSolver<NONE>, RISmoother, Restriction
+// <PROLMAT>, Prolongation<PROLMAT>> / MGSolver<Norm<l2, true>> (honei/math/mg.hh:57-243,
+// 567-662, 1093-1127), RISmoother (honei/math/ri.hh:97-133), IRSolver (honei/math/ir.hh:30-78).
+//
+// The reference executes its cycle as a list of Operator objects, one tag-dispatched call
+// each (honei/math/operator_list.hh:48-90).  Here every level is a short, fixed sequence of
+// fused kernels on one stream:
+//   n_pre  x  Jacobi sweep   x' = x + P (b - A x)          (defect + ElementProduct + Sum)
+//   defect + restriction     d_c = R (b - A x)              (Defect into store, Product)
+//   zero c_c, recurse / coarse CG (persistent kernel)
+//   prolongation + sum       x += P_l c_c                    (Product into store, Sum)
+//   n_post x  Jacobi sweep
+// Every fused formula rounds as the reference's operator sequence does; the only
+// difference from tags::CPU is the summation order of the norms and of the coarse CG's
+// dot products.
+#include "hb_internal.cuh"
+
+#include <cmath>
+#include <vector>
+
+struct hb_mg {
+    hb_context *ctx = nullptr;
+    int L = 0;
+    int dtype = HB_F64;
+    std::vector<hb_ell> A, prol, res;
+    hb_mg_params prm{};
+    void *mem = nullptr;
+    std::vector<void *> P, d, c, store, xt;   // per level
+    void *r = nullptr;                          // finest defect (dtype)
+    void *cgwork = nullptr;                     // 5 * ld(level 0), dtype
+    hb_solve_result *cgres = nullptr;
+    void *norm = nullptr;                       // device scalar
+    // mixed precision (dtype == F32): FP64 defect, FP32 inner right-hand side and solution
+    double *ir_r = nullptr;
+    float *ir_b = nullptr, *ir_x = nullptr;
+    int64_t used_coarse_total = 0;
+};
+
+namespace {
+
+__global__ void add_f32_to_f64_kernel(int64_t n, double *__restrict__ x, const float *__restrict__ c)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = __dadd_rn(x[i], (double)c[i]);
+}
+
+__global__ void f64_to_f32_kernel(int64_t n, float *__restrict__ dst, const double *__restrict__ src)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
+}
+
+// Scaled mode: b32 = (float)(r * s) with s = 1/|r|, and x += |r| * (double)c.
+__global__ void f64_to_f32_scaled_kernel(int64_t n, float *__restrict__ dst, const double *__restrict__ src, double s)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = (float)__dmul_rn(src[i], s);
+}
+
+__global__ void add_scaled_f32_to_f64_kernel(int64_t n, double *__restrict__ x, const float *__restrict__ c, double a)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = __dadd_rn(x[i], __dmul_rn(a, (double)c[i]));
+}
+
+inline unsigned ew_blocks(hb_context *ctx, int64_t n)
+{
+    return (unsigned)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 16);
+}
+
+int launch_add_f32_to_f64(hb_context *ctx, int64_t n, double *x, const float *c)
+{
+    if (n == 0) return HB_OK;
+    add_f32_to_f64_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, x, c);
+    return hb_check_launch(ctx, "add_f32_to_f64_kernel");
+}
+
+int launch_f64_to_f32(hb_context *ctx, int64_t n, float *dst, const double *src)
+{
+    if (n == 0) return HB_OK;
+    f64_to_f32_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, dst, src);
+    return hb_check_launch(ctx, "f64_to_f32_kernel");
+}
+
+int launch_f64_to_f32_scaled(hb_context *ctx, int64_t n, float *dst, const double *src, double s)
+{
+    if (n == 0) return HB_OK;
+    f64_to_f32_scaled_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, dst, src, s);
+    return hb_check_launch(ctx, "f64_to_f32_scaled_kernel");
+}
+
+int launch_add_scaled_f32_to_f64(hb_context *ctx, int64_t n, double *x, const float *c, double a)
+{
+    if (n == 0) return HB_OK;
+    add_scaled_f32_to_f64_kernel<<<ew_blocks(ctx, n), 256, 0, ctx->stream>>>(n, x, c, a);
+    return hb_check_launch(ctx, "add_scaled_f32_to_f64_kernel");
+}
+
+#define HB_TRY(expr) do { int s_ = (expr); if (s_) return s_; } while (0)
+
+template <typename T> inline T *tp(void *p) { return static_cast<T *>(p); }
+
+// Device norm: sqrt of the fixed-order sum of squares, read back (one sync).
+template <typename T> int norm_host(hb_mg *mg, const T *v, int64_t n, T *out)
+{
+    hb_context *ctx = mg->ctx;
+    HB_TRY(hb_launch_dot<T>(ctx, n, v, v, tp<T>(mg->norm)));
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->pinned, mg->norm, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    *out = std::sqrt(*static_cast<T *>(ctx->pinned));
+    return HB_OK;
+}
+
+template <typename T> int smooth(hb_mg *mg, int l, T *X, const T *B, int64_t sweeps)
+{
+    hb_context *ctx = mg->ctx;
+    T *cur = X, *other = tp<T>(mg->xt[l]);
+    for (int64_t s = 0; s < sweeps; ++s) {
+        HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->A[l], HB_MODE_JACOBI, cur, B, tp<T>(mg->P[l]), other));
+        T *t = cur; cur = other; other = t;
+    }
+    if (cur != X)
+        HB_CUDA_TRY(ctx, cudaMemcpyAsync(X, cur, sizeof(T) * mg->A[l].rows, cudaMemcpyDeviceToDevice, ctx->stream));
+    return HB_OK;
+}
+
+template <typename T> int vcycle(hb_mg *mg, int l, T *X, const T *B)
+{
+    hb_context *ctx = mg->ctx;
+    if (l == 0)
+        return hb_launch_cg<T>(ctx, &mg->A[0], B, X, mg->prm.max_iters_coarse, (T)mg->prm.eps, tp<T>(mg->cgwork),
+                               mg->cgres);
+    HB_TRY(smooth<T>(mg, l, X, B, mg->prm.n_pre));
+    HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->A[l], HB_MODE_DEFECT, X, B, nullptr, tp<T>(mg->store[l])));
+    HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->res[l - 1], HB_MODE_SPMV, tp<T>(mg->store[l]), nullptr, nullptr,
+                                  tp<T>(mg->d[l - 1])));
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(mg->c[l - 1], 0, sizeof(T) * mg->A[l - 1].rows, ctx->stream));
+    HB_TRY(vcycle<T>(mg, l - 1, tp<T>(mg->c[l - 1]), tp<T>(mg->d[l - 1])));
+    HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->prol[l - 1], HB_MODE_ADD, tp<T>(mg->c[l - 1]), nullptr, nullptr, X));
+    return smooth<T>(mg, l, X, B, mg->prm.n_post);
+}
+
+// MGSolver::value (mg.hh:1098-1126): r = b - A x; rnorm0 = |r|; cycles until |r| < eps rnorm0.
+template <typename T> int mg_solve(hb_mg *mg, const T *b, T *x, int64_t *used, T *rnorm)
+{
+    hb_context *ctx = mg->ctx;
+    const int top = mg->L - 1;
+    const int64_t n = mg->A[top].rows;
+    T *r = tp<T>(mg->r);
+    HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->A[top], HB_MODE_DEFECT, x, b, nullptr, r));
+    T r0, rc = T(1e16);
+    HB_TRY(norm_host<T>(mg, r, n, &r0));
+    int64_t u = 0;
+    for (int64_t i = 0; i < mg->prm.max_iters; ++i) {
+        HB_TRY(vcycle<T>(mg, top, x, b));
+        HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->A[top], HB_MODE_DEFECT, x, b, nullptr, r));
+        HB_TRY(norm_host<T>(mg, r, n, &rc));
+        u = i + 1;
+        if (rc < (T)mg->prm.eps * r0) break;
+    }
+    hb_solve_result h;
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(&h, mg->cgres, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h.status == HB_DEV_TIMEOUT) return HB_ERR_TIMEOUT;
+    if (used) *used = u;
+    if (rnorm) { rnorm[0] = r0; rnorm[1] = rc; }
+    return HB_OK;
+}
+
+inline size_t pad_entries(int64_t n) { return (size_t)hb_round_up(n > 0 ? n : 1, 64); }
+
+template <typename T> int jacobi_init(hb_mg *mg)
+{
+    for (int l = 0; l < mg->L; ++l)
+        HB_TRY(hb_launch_jacobi_diag<T>(mg->ctx, &mg->A[l], (T)mg->prm.damping, tp<T>(mg->P[l])));
+    return HB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hb_mg_create(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *prol, const hb_ell *res,
+                 const hb_mg_params *params, hb_mg **out)
+{
+    if (!ctx || !A || !params || !out || nlevels < 1) return HB_ERR_INVALID;
+    if (nlevels > 1 && (!prol || !res)) return HB_ERR_INVALID;
+    *out = nullptr;
+    const int dt = A[0].dtype;
+    for (int l = 0; l < nlevels; ++l) {
+        HB_TRY(hb_check_ell(&A[l], dt));
+        if (A[l].rows != A[l].cols) return HB_ERR_SIZE;
+        if (l + 1 < nlevels) {
+            HB_TRY(hb_check_ell(&prol[l], dt));
+            HB_TRY(hb_check_ell(&res[l], dt));
+            if (prol[l].rows != A[l + 1].rows || prol[l].cols != A[l].rows) return HB_ERR_SIZE;
+            if (res[l].rows != A[l].rows || res[l].cols != A[l + 1].rows) return HB_ERR_SIZE;
+        }
+    }
+    if (params->max_iters < 0 || params->max_iters_coarse < 0 || params->n_pre < 0 || params->n_post < 0)
+        return HB_ERR_INVALID;
+    hb_mg *mg = new hb_mg();
+    mg->ctx = ctx;
+    mg->L = nlevels;
+    mg->dtype = dt;
+    mg->A.assign(A, A + nlevels);
+    if (nlevels > 1) {
+        mg->prol.assign(prol, prol + nlevels - 1);
+        mg->res.assign(res, res + nlevels - 1);
+    }
+    mg->prm = *params;
+    const size_t es = dt == HB_F64 ? 8 : 4;
+    const int64_t nf = A[nlevels - 1].rows;
+    size_t entries = 0;
+    for (int l = 0; l < nlevels; ++l) entries += 5 * pad_entries(A[l].rows);
+    entries += pad_entries(nf);                        // r
+    entries += 5 * pad_entries(A[0].ld);               // coarse CG work
+    entries += 64;                                     // norm scalar
+    size_t bytes = entries * es + 256 /* cg result */;
+    if (dt == HB_F32) bytes += pad_entries(nf) * (8 + 4 + 4);   // IR: r64, b32, x32
+    if (cudaMalloc(&mg->mem, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        delete mg;
+        return HB_ERR_ALLOC;
+    }
+    char *p = (char *)mg->mem;
+    auto take = [&](size_t n_entries, size_t esz) { void *q = p; p += n_entries * esz; return q; };
+    mg->cgres = (hb_solve_result *)take(256, 1);
+    for (int l = 0; l < nlevels; ++l) {
+        const size_t n = pad_entries(A[l].rows);
+        mg->P.push_back(take(n, es));
+        mg->d.push_back(take(n, es));
+        mg->c.push_back(take(n, es));
+        mg->store.push_back(take(n, es));
+        mg->xt.push_back(take(n, es));
+    }
+    mg->r = take(pad_entries(nf), es);
+    mg->cgwork = take(5 * pad_entries(A[0].ld), es);
+    mg->norm = take(64, es);
+    if (dt == HB_F32) {
+        mg->ir_r = (double *)take(pad_entries(nf), 8);
+        mg->ir_b = (float *)take(pad_entries(nf), 4);
+        mg->ir_x = (float *)take(pad_entries(nf), 4);
+    }
+    int st = cudaMemsetAsync(mg->mem, 0, bytes, ctx->stream) == cudaSuccess ? HB_OK : HB_ERR_CUDA;
+    if (!st) st = dt == HB_F64 ? jacobi_init<double>(mg) : jacobi_init<float>(mg);
+    if (st) {
+        cudaFree(mg->mem);
+        delete mg;
+        return st;
+    }
+    *out = mg;
+    return HB_OK;
+}
+
+int hb_mg_destroy(hb_mg *mg)
+{
+    if (!mg) return HB_ERR_INVALID;
+    cudaStreamSynchronize(mg->ctx->stream);
+    cudaFree(mg->mem);
+    delete mg;
+    return HB_OK;
+}
+
+int hb_mg_set_params(hb_mg *mg, const hb_mg_params *params)
+{
+    if (!mg || !params) return HB_ERR_INVALID;
+    if (params->max_iters < 0 || params->max_iters_coarse < 0 || params->n_pre < 0 || params->n_post < 0)
+        return HB_ERR_INVALID;
+    const bool redo = params->damping != mg->prm.damping;
+    mg->prm = *params;
+    if (redo) return mg->dtype == HB_F64 ? jacobi_init<double>(mg) : jacobi_init<float>(mg);
+    return HB_OK;
+}
+
+int hb_mg_solve_f64(hb_mg *mg, const double *b, double *x, int64_t *used_cycles, double *rnorm_host)
+{
+    if (!mg || !b || !x) return HB_ERR_INVALID;
+    if (mg->dtype != HB_F64) return HB_ERR_INVALID;
+    return mg_solve<double>(mg, b, x, used_cycles, rnorm_host);
+}
+
+int hb_mg_solve_f32(hb_mg *mg, const float *b, float *x, int64_t *used_cycles, float *rnorm_host)
+{
+    if (!mg || !b || !x) return HB_ERR_INVALID;
+    if (mg->dtype != HB_F32) return HB_ERR_INVALID;
+    return mg_solve<float>(mg, b, x, used_cycles, rnorm_host);
+}
+
+// IRSolver<double outer, float inner, Norm<l2, true>> (honei/math/ir.hh:30-78).
+int hb_ir_mg_solve(hb_context *ctx, const hb_ell *A64, hb_mg *mg32, const double *b, double *x, double eps,
+                   int64_t max_iters, int warm_start, int64_t *used_outer, double *rnorm_host)
+{
+    if (!ctx || !A64 || !mg32 || !b || !x || max_iters < 0) return HB_ERR_INVALID;
+    HB_TRY(hb_check_ell(A64, HB_F64));
+    if (mg32->dtype != HB_F32) return HB_ERR_INVALID;
+    const int64_t n = A64->rows;
+    if (A64->cols != n || mg32->A[mg32->L - 1].rows != n) return HB_ERR_SIZE;
+    hb_context *saved = mg32->ctx;
+    mg32->ctx = ctx;
+    double r0 = 1e16, rc = 1e16;
+    int64_t u = 0;
+    int st = HB_OK;
+    for (int64_t i = 0; i < max_iters && !st; ++i) {
+        st = hb_launch_spmv_mode<double>(ctx, A64, HB_MODE_DEFECT, x, b, nullptr, mg32->ir_r);
+        if (st) break;
+        double nrm;
+        st = hb_launch_dot<double>(ctx, n, mg32->ir_r, mg32->ir_r, (double *)hb_scalars(ctx) + 16);
+        if (st) break;
+        if (cudaMemcpyAsync(ctx->pinned, (double *)hb_scalars(ctx) + 16, 8, cudaMemcpyDeviceToHost, ctx->stream) ||
+            cudaStreamSynchronize(ctx->stream)) { st = HB_ERR_CUDA; break; }
+        nrm = std::sqrt(*(double *)ctx->pinned);
+        if (i == 0) {
+            r0 = nrm;
+        } else {
+            rc = nrm;
+            u = i;
+            if (rc < eps * r0) break;
+        }
+        if (warm_start) {
+            st = launch_f64_to_f32(ctx, n, mg32->ir_b, mg32->ir_r);
+        } else {
+            st = launch_f64_to_f32_scaled(ctx, n, mg32->ir_b, mg32->ir_r, 1.0 / nrm);
+            if (!st && cudaMemsetAsync(mg32->ir_x, 0, sizeof(float) * n, ctx->stream)) st = HB_ERR_CUDA;
+        }
+        if (st) break;
+        st = mg_solve<float>(mg32, mg32->ir_b, mg32->ir_x, nullptr, nullptr);
+        if (st) break;
+        st = warm_start ? launch_add_f32_to_f64(ctx, n, x, mg32->ir_x)
+                        : launch_add_scaled_f32_to_f64(ctx, n, x, mg32->ir_x, nrm);
+    }
+    mg32->ctx = saved;
+    if (st) return st;
+    if (used_outer) *used_outer = u;
+    if (rnorm_host) { rnorm_host[0] = r0; rnorm_host[1] = rc; }
+    return HB_OK;
+}
+
+// The same outer loop around an FP32 CG inner solve that restarts from zero each step.
+int hb_ir_cg_solve(hb_context *ctx, const hb_ell *A64, const hb_ell *A32, const double *b, double *x, double eps,
+                   float inner_eps, int64_t inner_max_iters, int64_t max_iters, int64_t *used_outer,
+                   int64_t *inner_total, double *rnorm_host)
+{
+    if (!ctx || !A64 || !A32 || !b || !x || max_iters < 0 || inner_max_iters < 0) return HB_ERR_INVALID;
+    HB_TRY(hb_check_ell(A64, HB_F64));
+    HB_TRY(hb_check_ell(A32, HB_F32));
+    const int64_t n = A64->rows;
+    if (A64->cols != n || A32->rows != n || A32->cols != n) return HB_ERR_SIZE;
+    const int64_t ld = A64->ld;
+    // work: CG (5 ld floats) | r64 (ld doubles) | b32 | x32 (ld floats)
+    HB_TRY(hb_ensure_work(ctx, (size_t)ld * (5 * 4 + 8 + 4 + 4)));
+    float *cgw = (float *)ctx->work;
+    double *r64 = (double *)(cgw + 5 * ld);
+    float *b32 = (float *)(r64 + ld);
+    float *x32 = b32 + ld;
+    double r0 = 1e16, rc = 1e16, *dnorm = (double *)hb_scalars(ctx) + 16;
+    int64_t u = 0, total = 0;
+    hb_solve_result *res = hb_result(ctx) + 1;
+    for (int64_t i = 0; i < max_iters; ++i) {
+        HB_TRY(hb_launch_spmv_mode<double>(ctx, A64, HB_MODE_DEFECT, x, b, nullptr, r64));
+        HB_TRY(hb_launch_dot<double>(ctx, n, r64, r64, dnorm));
+        HB_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->pinned, dnorm, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        if (i > 0) {
+            hb_solve_result *h = (hb_solve_result *)((char *)ctx->pinned + 64);
+            HB_CUDA_TRY(ctx, cudaMemcpy(h, res, sizeof(*h), cudaMemcpyDeviceToHost));
+            if (h->status == HB_DEV_TIMEOUT) return HB_ERR_TIMEOUT;
+            total += h->used;
+        }
+        const double nrm = std::sqrt(*(double *)ctx->pinned);
+        if (i == 0) {
+            r0 = nrm;
+        } else {
+            rc = nrm;
+            u = i;
+            if (rc < eps * r0) break;
+        }
+        // normalised defect: the inner CG's absolute stopping test (cg.hh:118) then means
+        // "relative to this step's defect" and cannot end the inner solve early
+        HB_TRY(launch_f64_to_f32_scaled(ctx, n, b32, r64, 1.0 / nrm));
+        HB_CUDA_TRY(ctx, cudaMemsetAsync(x32, 0, sizeof(float) * n, ctx->stream));
+        HB_TRY(hb_launch_cg<float>(ctx, A32, b32, x32, inner_max_iters, inner_eps, cgw, res));
+        HB_TRY(launch_add_scaled_f32_to_f64(ctx, n, x, x32, nrm));
+    }
+    if (used_outer) *used_outer = u;
+    if (inner_total) *inner_total = total;
+    if (rnorm_host) { rnorm_host[0] = r0; rnorm_host[1] = rc; }
+    return HB_OK;
+}
+
+}  // extern "C"

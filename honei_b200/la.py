@@ -348,3 +348,122 @@ class CGSolver:
                  eps_relative, C.byref(used), C.byref(d)), "CGSolver", ctx.handle)
         CGSolver.last_defect = d.value
         return used.value
+
+
+class MGData:
+    """Device MG hierarchy (MGData + the V(n_pre, n_post) cycle; honei/math/mg.hh:57-243, 567-662).
+
+    Levels are coarsest first (HONEI level 1 first); ``prol[l]`` maps level l to l+1 and
+    ``res[l] = prol[l]^T``.  Smoother: damped Jacobi (RISmoother with the "jac"
+    preconditioner); coarse solver: CG on level 1 with the MG eps.
+    """
+
+    def __init__(self, A, prol, res, max_iters=100, max_iters_coarse=1000, n_pre=2, n_post=2,
+                 damping=0.7, eps=1e-8, ctx: Context | None = None):
+        from ._lib import HbMGParams
+        self.ctx = ctx or default_context()
+        self.A, self.prol, self.res = list(A), list(prol), list(res)
+        self.dtype = self.A[0].dtype
+        L = len(self.A)
+        self._A = (HbEll * L)(*[a.struct for a in self.A])
+        self._P = (HbEll * max(L - 1, 1))(*[p.struct for p in self.prol])
+        self._R = (HbEll * max(L - 1, 1))(*[r.struct for r in self.res])
+        self.params = HbMGParams(max_iters, max_iters_coarse, n_pre, n_post, damping, eps)
+        h = C.c_void_p()
+        check(lib().hb_mg_create(self.ctx.handle, L, self._A, self._P, self._R, C.byref(self.params), C.byref(h)),
+              "hb_mg_create", self.ctx.handle)
+        self.handle = h
+        self.used_iters = 0
+
+    @classmethod
+    def from_hierarchy(cls, H, dtype=np.float64, ctx: Context | None = None, **kw) -> "MGData":
+        """From a host problems.MGHierarchy (reference-layout matrices)."""
+        ctx = ctx or default_context()
+        Hd = H if dtype == np.float64 else H.astype(dtype)
+        up = lambda m: SparseMatrixELL.from_reference(m, ctx)  # noqa: E731
+        return cls([up(a) for a in Hd.A], [up(p) for p in Hd.prol], [up(r) for r in Hd.res], ctx=ctx, **kw)
+
+    def configure(self, **kw):
+        """MGUtil::configure (honei/math/mg.hh:426-439)."""
+        for k, v in kw.items():
+            setattr(self.params, k, v)
+        check(lib().hb_mg_set_params(self.handle, C.byref(self.params)), "hb_mg_set_params", self.ctx.handle)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().hb_mg_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MGSolver:
+    """MGSolver<tags::GPU::CUDA, Norm<vnt_l_two, true>>::value(data, x, b) (honei/math/mg.hh:1093-1127).
+
+    Returns (used_cycles, initial_norm, final_norm); x holds x0 on entry.
+    """
+
+    @staticmethod
+    def value(data: MGData, b: torch.Tensor, x: torch.Tensor):
+        n = data.A[-1].rows()
+        if b.numel() != n:
+            raise VectorSizeDoesNotMatch(b.numel(), n)
+        if x.numel() != n:
+            raise VectorSizeDoesNotMatch(x.numel(), n)
+        data.ctx.bind_stream()
+        used = C.c_int64(0)
+        if data.dtype == torch.float64:
+            rn = (C.c_double * 2)()
+            st = lib().hb_mg_solve_f64(data.handle, _vec(b, data.dtype, "b"), _vec(x, data.dtype, "x"),
+                                       C.byref(used), rn)
+        else:
+            rn = (C.c_float * 2)()
+            st = lib().hb_mg_solve_f32(data.handle, _vec(b, data.dtype, "b"), _vec(x, data.dtype, "x"),
+                                       C.byref(used), rn)
+        check(st, "MGSolver", data.ctx.handle)
+        data.used_iters = used.value
+        return used.value, rn[0], rn[1]
+
+
+class IRSolver:
+    """IRSolver<Outer=double, Inner=float, Norm<l2, true>> (honei/math/ir.hh:30-78).
+
+    ``value(A64, b, x, mg32, eps, max_iters, warm_start=True)`` with an FP32 MG inner solve, or
+    ``value_cg(A64, A32, b, x, eps, inner_eps, inner_max_iters, max_iters)`` with FP32 CG.
+    Both return (used_outer, initial_norm, final_norm[, inner_iterations]).
+    """
+
+    @staticmethod
+    def value(A64: SparseMatrixELL, b: torch.Tensor, x: torch.Tensor, mg32: MGData, eps: float = 1e-10,
+              max_iters: int = 100, warm_start: bool = True, ctx: Context | None = None):
+        if b.numel() != A64.rows():
+            raise VectorSizeDoesNotMatch(b.numel(), A64.rows())
+        if x.numel() != A64.columns():
+            raise VectorSizeDoesNotMatch(x.numel(), A64.columns())
+        ctx = ctx or default_context()
+        used = C.c_int64(0)
+        rn = (C.c_double * 2)()
+        check(lib().hb_ir_mg_solve(ctx.handle, C.byref(A64.struct), mg32.handle, _vec(b, torch.float64, "b"),
+                                   _vec(x, torch.float64, "x"), eps, max_iters, int(warm_start), C.byref(used), rn),
+              "IRSolver", ctx.handle)
+        return used.value, rn[0], rn[1]
+
+    @staticmethod
+    def value_cg(A64: SparseMatrixELL, A32: SparseMatrixELL, b: torch.Tensor, x: torch.Tensor, eps: float = 1e-10,
+                 inner_eps: float = 1e-3, inner_max_iters: int = 100000, max_iters: int = 100,
+                 ctx: Context | None = None):
+        if b.numel() != A64.rows():
+            raise VectorSizeDoesNotMatch(b.numel(), A64.rows())
+        if x.numel() != A64.columns():
+            raise VectorSizeDoesNotMatch(x.numel(), A64.columns())
+        ctx = ctx or default_context()
+        used, inner = C.c_int64(0), C.c_int64(0)
+        rn = (C.c_double * 2)()
+        check(lib().hb_ir_cg_solve(ctx.handle, C.byref(A64.struct), C.byref(A32.struct), _vec(b, torch.float64, "b"),
+                                   _vec(x, torch.float64, "x"), eps, inner_eps, inner_max_iters, max_iters,
+                                   C.byref(used), C.byref(inner), rn), "IRSolver", ctx.handle)
+        return used.value, rn[0], rn[1], inner.value

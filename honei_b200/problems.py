@@ -262,11 +262,32 @@ class MGHierarchy:
                            [r.astype(dtype) for r in self.res], list(self.sides))
 
 
-def mg_hierarchy(M: int, coarsest: int = 9, coef=None, threads: int = 1) -> MGHierarchy:
+def galerkin_csr(A: EllMatrix, prol: EllMatrix, res: EllMatrix):
+    """CSR of the Galerkin coarse operator R A P (columns ascending, zeros dropped)."""
+    import scipy.sparse as sp
+
+    def csr(m):
+        ip, ix, dv = m.to_csr()
+        return sp.csr_matrix((dv, ix, ip), shape=(m.rows, m.cols))
+
+    Ac = (csr(res) @ csr(A) @ csr(prol)).tocsr()
+    Ac.eliminate_zeros()
+    Ac.sort_indices()
+    return Ac.shape[0], Ac.indptr.astype(np.int64), Ac.indices.astype(np.int64), Ac.data
+
+
+def mg_hierarchy(M: int, coarsest: int = 9, coef=None, threads: int = 1, coarse: str = "auto") -> MGHierarchy:
     """Q1 Poisson hierarchy on sides M, (M+1)/2, ..., coarsest (all of the form 2^k + 1).
 
-    Coarser-level coefficients are the 2x2 means of the finer ones (rediscretisation).
+    coarse = "rediscretize": every level is the Q1 matrix of its own grid (coarser cell
+    coefficients = 2x2 means).  coarse = "galerkin": A_{l-1} = R_l A_l P_l from the finest
+    matrix down (robust for jumping coefficients, where rediscretisation diverges).
+    "auto" = rediscretize for the unit coefficient, galerkin for a coefficient field.
     """
+    if coarse == "auto":
+        coarse = "rediscretize" if coef is None else "galerkin"
+    if coarse not in ("rediscretize", "galerkin"):
+        raise ValueError(coarse)
     sides = [int(M)]
     while sides[-1] > coarsest:
         if (sides[-1] - 1) % 2:
@@ -278,11 +299,18 @@ def mg_hierarchy(M: int, coarsest: int = 9, coef=None, threads: int = 1) -> MGHi
         coefs[-1] = np.asarray(coef, np.float64)
         for l in range(len(sides) - 2, -1, -1):
             coefs[l] = coarsen_coef(coefs[l + 1])
-    A = [q1_poisson(s, coefs[l], threads) for l, s in enumerate(sides)]
     prol, res = [], []
     for l in range(len(sides) - 1):
         nf, nc, ip, ix, dv = prolongation_csr(sides[l])
         prol.append(ell_from_csr(nf, nc, ip, ix, dv, threads))
         t_ip, t_ix, t_dv = transpose_csr(nf, nc, ip, ix, dv)
         res.append(ell_from_csr(nc, nf, t_ip, t_ix, t_dv, threads))
+    if coarse == "rediscretize":
+        A = [q1_poisson(s, coefs[l], threads) for l, s in enumerate(sides)]
+    else:
+        A = [None] * len(sides)
+        A[-1] = q1_poisson(sides[-1], coefs[-1], threads)
+        for l in range(len(sides) - 1, 0, -1):
+            n, ip, ix, dv = galerkin_csr(A[l], prol[l - 1], res[l - 1])
+            A[l - 1] = ell_from_csr(n, n, ip, ix, dv, threads)
     return MGHierarchy(A, prol, res, sides)

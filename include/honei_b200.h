@@ -193,6 +193,48 @@ int hb_cg_f32(hb_context *ctx, const hb_ell *A, const float *b, float *x, int64_
 int hb_cg_f64_noalloc(const hb_ell *A, const double *b, double *x, int64_t max_iters, double eps,
                       int64_t *used_iters, double *final_defect, void *stream);
 
+/* Multigrid (MGData + MGCycleCreation<V::STATIC, CGSolver<NONE>, RISmoother, Restriction
+ * <PROLMAT>, Prolongation<PROLMAT>> + MGSolver<Norm<l2, true>>, honei/math/mg.hh:57-243,
+ * 567-662, 1093-1127; RISmoother honei/math/ri.hh:97-133 with the "jac" preconditioner
+ * damping/diag(A), honei/math/mg.hh:255-286).  Levels are given coarsest first (HONEI level
+ * 1 first); prol[l] maps level l to l+1, res[l] = prol[l]^T.  All matrices share one dtype.
+ * The hierarchy object owns its per-level work vectors. */
+typedef struct hb_mg hb_mg;
+typedef struct {
+    int64_t max_iters;         /* V-cycles                                        */
+    int64_t max_iters_coarse;  /* CG iterations on level 1                        */
+    int64_t n_pre, n_post;     /* smoothing sweeps                                */
+    double damping;            /* Jacobi damping (0.7 in the north-star configs)  */
+    double eps;                /* relative stop on ||r||_2; also the coarse CG eps */
+} hb_mg_params;
+
+int hb_mg_create(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *prol,
+                 const hb_ell *res, const hb_mg_params *params, hb_mg **out);
+int hb_mg_destroy(hb_mg *mg);
+int hb_mg_set_params(hb_mg *mg, const hb_mg_params *params);
+/* Solve on the finest level: x holds x0 on entry.  *used_cycles (host) and
+ * rnorm_host[2] = {initial, final} defect norms (may be NULL). */
+int hb_mg_solve_f64(hb_mg *mg, const double *b, double *x, int64_t *used_cycles, double *rnorm_host);
+int hb_mg_solve_f32(hb_mg *mg, const float *b, float *x, int64_t *used_cycles, float *rnorm_host);
+
+/* Mixed precision iterative refinement, IRSolver<Outer=double, Inner=float>,
+ * honei/math/ir.hh:30-78: FP64 defect b - A x, convergence norm and solution update on the
+ * device; FP32 inner MG (mg32, eps and cycle count from its params) on the cast defect.
+ * warm_start != 0 is the reference's loop: the cast defect is the inner right-hand side and
+ * the inner x is kept between outer steps (ir.hh:69-73).  warm_start = 0 is the scaled mode:
+ * the defect is normalised to unit norm before the cast, the inner solve starts from zero and
+ * x += |r| * c, so the inner eps is relative to each step's defect.
+ * *used_outer (host) gets the outer step count; rnorm_host[2] = {initial, final}. */
+int hb_ir_mg_solve(hb_context *ctx, const hb_ell *A64, hb_mg *mg32, const double *b, double *x,
+                   double eps, int64_t max_iters, int warm_start, int64_t *used_outer,
+                   double *rnorm_host);
+/* The same outer loop, scaled mode, with an FP32 CG inner solver (A32 = A64 cast) from zero:
+ * the normalised defect keeps CGSolver's absolute stopping test (cg.hh:118) from ending the
+ * inner solve early, so inner_eps is relative.  *inner_total = summed inner CG iterations. */
+int hb_ir_cg_solve(hb_context *ctx, const hb_ell *A64, const hb_ell *A32, const double *b, double *x,
+                   double eps, float inner_eps, int64_t inner_max_iters, int64_t max_iters,
+                   int64_t *used_outer, int64_t *inner_total, double *rnorm_host);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -225,7 +225,9 @@ ORA_MG(f32, float, sqrtf)
  * IRSolver<Outer=double, Inner=float> -- honei/math/ir.hh:30-78.
  *   for i < max_iters: r = b - A x (FP64); i == 0 ? rnorm0 = |r| : (used = i; stop if
  *   |r| < eps * rnorm0); b_inner = (float) r; inner MG; c = (double) x_inner; x += c.
- * The reference leaves x_inner as it was (warm start); warm_start == 0 zeroes it instead.
+ * The reference leaves x_inner as it was (warm start, warm_start != 0).  warm_start == 0 is
+ * the scaled mode: the defect is normalised to unit norm before the cast, the inner solve starts
+ * from zero and the correction is scaled back (x += |r| * c), so the inner eps is relative.
  * ------------------------------------------------------------------------------------- */
 int ora_ir_mg(const ora_ell *A64, const ora_mg *mg32, float damping, const double *b, double *x,
               double eps, float inner_eps, uint64_t max_iters, int warm_start, uint64_t *used,
@@ -247,11 +249,22 @@ int ora_ir_mg(const ora_ell *A64, const ora_mg *mg32, float damping, const doubl
             *used = i;
             if (rnorm_current < eps * rnorm_initial) break;
         }
-        for (uint64_t k = 0; k < n; ++k) bi[k] = (float)r[k];
-        if (!warm_start) memset(xi, 0, sizeof(float) * n);
+        if (warm_start) {
+            for (uint64_t k = 0; k < n; ++k) bi[k] = (float)r[k];
+        } else {
+            /* scaled mode: normalised defect, inner solve from zero, correction scaled back */
+            const double s = 1.0 / (i == 0 ? rnorm_initial : rnorm_current);
+            for (uint64_t k = 0; k < n; ++k) bi[k] = (float)(r[k] * s);
+            memset(xi, 0, sizeof(float) * n);
+        }
         uint64_t inner_used = 0;
         ora_mg_f32(mg32, damping, bi, xi, inner_eps, &inner_used, NULL);
-        for (uint64_t k = 0; k < n; ++k) x[k] += (double)xi[k];
+        if (warm_start) {
+            for (uint64_t k = 0; k < n; ++k) x[k] += (double)xi[k];
+        } else {
+            const double nr = (i == 0 ? rnorm_initial : rnorm_current);
+            for (uint64_t k = 0; k < n; ++k) x[k] += nr * (double)xi[k];
+        }
     }
     free(r); free(bi); free(xi);
     return 0;
@@ -278,12 +291,14 @@ int ora_ir_cg(const ora_ell *A64, const ora_ell *A32, const double *b, double *x
             *used = i;
             if (rnorm_current < eps * rnorm_initial) break;
         }
-        for (uint64_t k = 0; k < n; ++k) bi[k] = (float)r[k];
+        /* normalised defect, so the inner CG's absolute test (cg.hh:118) cannot stop it early */
+        const double nr = (i == 0 ? rnorm_initial : rnorm_current), s = 1.0 / nr;
+        for (uint64_t k = 0; k < n; ++k) bi[k] = (float)(r[k] * s);
         memset(xi, 0, sizeof(float) * n);
         uint64_t inner_used = 0;
         ora_cg_f32(A32, bi, xi, inner_max_iters, inner_eps, &inner_used, NULL);
         total += inner_used;
-        for (uint64_t k = 0; k < n; ++k) x[k] += (double)xi[k];
+        for (uint64_t k = 0; k < n; ++k) x[k] += nr * (double)xi[k];
     }
     if (inner_total) *inner_total = total;
     free(r); free(bi); free(xi);

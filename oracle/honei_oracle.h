@@ -67,12 +67,13 @@ int ora_mg_f32(const ora_mg *mg, float damping, const float *b, float *x, float 
 
 /* IR (honei/math/ir.hh:30-78): FP64 outer defect + update around the FP32 MG above.
  * A64 is the finest FP64 matrix; mg32 the FP32 hierarchy. warm_start != 0 keeps the inner
- * x between outer steps (the reference behaviour); 0 restarts it at zero. */
+ * x between outer steps (the reference behaviour); 0 = scaled mode (normalised defect, inner
+ * x from zero, correction scaled back by |r|). */
 int ora_ir_mg(const ora_ell *A64, const ora_mg *mg32, float damping, const double *b, double *x,
               double eps, float inner_eps, uint64_t max_iters, int warm_start, uint64_t *used,
               double *rnorm_hist);
 
-/* IR with an FP32 CG inner solver (same outer loop; inner CG from x = 0 every step). */
+/* IR with an FP32 CG inner solver in the scaled mode (normalised defect, inner CG from 0). */
 int ora_ir_cg(const ora_ell *A64, const ora_ell *A32, const double *b, double *x, double eps,
               float inner_eps, uint64_t inner_max_iters, uint64_t max_iters, uint64_t *used,
               uint64_t *inner_total, double *rnorm_hist);
