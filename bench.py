@@ -129,10 +129,15 @@ def dist_setup():
 # Reference arm: the reference's own CPU path (oracle/_ref, tags::CPU::MultiCore::SSE on all
 # host cores), else the C restatement (single core).
 # ---------------------------------------------------------------------------------------
+_CPU_CASE = {}
+
+
 def cpu_spmv_gbs(reps=None, budget_s=10.0):
     from honei_b200 import problems as P
-    A = P.q1_poisson(M_SPMV)
-    x = P.uniform_vector(A.rows, 1)
+    if not _CPU_CASE:
+        _CPU_CASE["A"] = P.q1_poisson(M_SPMV)
+        _CPU_CASE["x"] = P.uniform_vector(_CPU_CASE["A"].rows, 1)
+    A, x = _CPU_CASE["A"], _CPU_CASE["x"]
     nbytes = spmv_bytes(A.nnz, A.rows, 8)
     cores = os.cpu_count() or 1
     try:
@@ -197,6 +202,86 @@ def run_reference_arm(args):
 # ---------------------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------------------
+def bench_batch(la, ctx, n_systems=512, seed=2024):
+    """512 independent SPD Q1 systems, side ~ U{17..257}, cell coefficient 10^U(-1,1), b = A x_true:
+    one persistent batched launch (FP64 CG, and FP32-inner IR to a 1e-8 FP64 residual) against
+    plain FP64 CG solved one system at a time (hb_cg_f64, the whole GPU per solve)."""
+    import torch
+    from honei_b200 import batch as B
+
+    rng = np.random.default_rng(seed)
+    sides = rng.integers(17, 258, size=n_systems)
+    out = {"workload": f"{n_systems} SPD Q1 systems, side U{{17..257}}, coef 10^U(-1,1), CG to 1e-8",
+           "rows_total": int(sum(int(m) * int(m) for m in sides))}
+    for mode in ("cg64", "ir32"):
+        systems = B.q1_batch(sides, coef_range=(1e-1, 1e1), seed=seed, mode=mode, eps=1e-8, inner_eps=1e-3)
+        solver = B.BatchSolver(systems, ctx=ctx)
+        cfg = solver.tune(use_cache=False)
+        for sys_ in systems:
+            sys_.x.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        solver.run(cfg)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        res = solver.results()
+        out[mode] = {"ms": round(ms, 2), "systems_per_s": round(n_systems / (ms / 1e3), 1),
+                     "config": {"cluster": cfg.cluster, "threads": cfg.threads},
+                     "iterations_mean": round(float(np.mean([r["iterations"] for r in res])), 1),
+                     "max_true_relres": float(max(r["true_relres"] for r in res)),
+                     "tune_ms": getattr(solver, "tune_times", None)}
+        if mode == "cg64":
+            # baseline: the same systems, plain FP64 CG one at a time (grid-wide persistent kernel)
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            for sys_ in systems:
+                sys_.x.zero_()
+            torch.cuda.synchronize()
+            t0.record()
+            iters = []
+            for sys_ in systems:
+                iters.append(la.CGSolver.value(sys_.A64, None, sys_.b, sys_.x, 100000, 1e-8, ctx=ctx))
+            t1.record()
+            torch.cuda.synchronize()
+            bms = t0.elapsed_time(t1)
+            out["sequential_cg64"] = {"ms": round(bms, 2), "systems_per_s": round(n_systems / (bms / 1e3), 1),
+                                      "iterations_mean": round(float(np.mean(iters)), 1)}
+        del solver, systems
+        torch.cuda.empty_cache()
+    out["speedup_batched_ir32_vs_sequential_cg64"] = round(out["sequential_cg64"]["ms"] / out["ir32"]["ms"], 2)
+    out["speedup_batched_cg64_vs_sequential_cg64"] = round(out["sequential_cg64"]["ms"] / out["cg64"]["ms"], 2)
+    return out
+
+
+def bench_cg_cluster(ctx, M=M_CG, n_solves=30):
+    """The 257^2 plain FP64 CG solve on one thread-block cluster (batched kernel, batch of 1)."""
+    import torch
+    from honei_b200 import batch as B
+
+    best = None
+    for cluster in (8, 16):
+        for threads in (512, 256):
+            s = B.q1_batch([M], coef_range=None, seed=1, mode="cg64", symmetric=False, eps=1e-8)
+            solver = B.BatchSolver(s, ctx=ctx)
+            cfg = B.HbBatchConfig(cluster, threads)
+            lat = []
+            for i in range(n_solves + 3):
+                s[0].x.zero_()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                r = solver.solve(cfg)
+                lat.append(time.perf_counter() - t0)
+            lat = sorted(1e3 * v for v in lat[3:])
+            cand = {"cluster": cluster, "threads": threads, "iterations": r[0]["iterations"],
+                    "solves_per_s": round(len(lat) / (sum(lat) / 1e3), 2),
+                    "p50_ms": round(statistics.median(lat), 3), "p99_ms": round(lat[-1], 3)}
+            if best is None or cand["p50_ms"] < best["p50_ms"]:
+                best = cand
+    return best
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -317,6 +402,9 @@ def run_ours(args):
                 "p50_ms": round(statistics.median(lat_ms), 3),
                 "p99_ms": round(lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))], 3)}
 
+    cg_cluster = bench_cg_cluster(ctx)
+    batch_extra = None if args.no_batch else bench_batch(la, ctx)
+
     line = None
     if rank == 0:
         cpu = None
@@ -340,7 +428,8 @@ def run_ours(args):
                     "d2h_bytes_per_step": n * 8, "api": "honei_b200.la.Product.value (C ABI hb_spmv_f64)"},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
-            "extra": {"spmv_f32_gbs": round(gbs32, 2), "cg_257": cg_extra},
+            "extra": {"spmv_f32_gbs": round(gbs32, 2), "cg_257": cg_extra, "cg_257_cluster": cg_cluster,
+                      "batch_512": batch_extra},
         }
         print(json.dumps(line), flush=True)
     barrier()
@@ -356,6 +445,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 512-system batched workload")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

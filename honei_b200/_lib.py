@@ -51,7 +51,7 @@ SIGNATURES = {
     "hb_ell_import_f64": (i32, [vp, i64, i64, i64, i64, i64, vp, vp, vp, P_ell]),
     "hb_ell_import_f32": (i32, [vp, i64, i64, i64, i64, i64, vp, vp, vp, P_ell]),
     "hb_ell_cast_f64_f32": (i32, [vp, P_ell, P_ell]),
-    "hb_q1_assemble_f64": (i32, [vp, i64, vp, P_ell]),
+    "hb_q1_assemble_f64": (i32, [vp, i64, vp, i32, P_ell]),
     "hb_spmv_f64": (i32, [vp, P_ell, vp, vp]),
     "hb_spmv_f32": (i32, [vp, P_ell, vp, vp]),
     "hb_defect_f64": (i32, [vp, P_ell, vp, vp, vp]),
@@ -87,6 +87,13 @@ SIGNATURES = {
     "hb_mg_solve_f32": (i32, [vp, vp, vp, P_i64, C.POINTER(f32)]),
     "hb_ir_mg_solve": (i32, [vp, P_ell, vp, vp, vp, f64, i64, i32, P_i64, C.POINTER(f64)]),
     "hb_ir_cg_solve": (i32, [vp, P_ell, P_ell, vp, vp, f64, f32, i64, i64, P_i64, P_i64, C.POINTER(f64)]),
+    # batched solves (struct pointers passed as void*; honei_b200.batch declares the structs)
+    "hb_batch_workspace_bytes": (i32, [vp, i64, C.POINTER(C.c_size_t)]),
+    "hb_batch_solve": (i32, [vp, vp, i64, vp, vp, vp]),
+    "hb_batch_prepare": (i32, [vp, vp, i64, vp]),
+    "hb_batch_run": (i32, [vp, i64, vp, vp]),
+    "hb_batch_results": (i32, [vp, i64, vp, vp]),
+    "hb_batch_tune": (i32, [vp, vp, i64, vp, vp, vp]),
 }
 
 

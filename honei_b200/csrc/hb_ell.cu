@@ -59,7 +59,7 @@ __global__ void ell_cast_kernel(int64_t total, const double *__restrict__ src, f
 // Q1 Poisson assembly, one thread per row (FillMatrix<POISSON, DIRICHLET_0> stencil, or the
 // bilinear element matrix k/6 [[4,-1,-2,-1],...] summed per node for a cell coefficient).
 // ---------------------------------------------------------------------------------------
-__global__ void q1_assemble_kernel(int64_t M, const double *__restrict__ coef, int64_t ld,
+__global__ void q1_assemble_kernel(int64_t M, const double *__restrict__ coef, int64_t ld, int symmetric,
                                    int32_t *__restrict__ Aj, double *__restrict__ Ax)
 {
     const int64_t N = M * M;
@@ -97,6 +97,21 @@ __global__ void q1_assemble_kernel(int64_t M, const double *__restrict__ coef, i
                 const int64_t offs[9] = {-M - 1, -M, -M + 1, -1, 0, 1, M - 1, M, M + 1};
 #pragma unroll
                 for (int s = 0; s < 9; ++s) jj[s] = (int32_t)(r + offs[s]);
+                if (symmetric) {
+                    // drop couplings to boundary nodes, keep the slot order compact
+                    int k = 0;
+#pragma unroll
+                    for (int s = 0; s < 9; ++s) {
+                        const int64_t c = r + offs[s];
+                        const int64_t ci = c / M, cj = c - ci * M;
+                        const bool cb = ci == 0 || ci == M - 1 || cj == 0 || cj == M - 1;
+                        const int32_t jv = jj[s];
+                        const double av = vv[s];
+                        jj[s] = -1;
+                        vv[s] = 0.0;
+                        if (!cb) { jj[k] = jv; vv[k] = av; ++k; }
+                    }
+                }
             }
         }
 #pragma unroll
@@ -307,14 +322,15 @@ int hb_ell_cast_f64_f32(hb_context *ctx, const hb_ell *src, hb_ell *dst)
     st = hb_check_ell(dst, HB_F32);
     if (st) return st;
     const int64_t total = src->K * src->ld;
-    HB_CUDA_TRY(ctx, cudaMemcpyAsync(dst->Aj, src->Aj, total * sizeof(int32_t), cudaMemcpyDeviceToDevice,
-                                     ctx->stream));
+    if (dst->Aj != src->Aj)   // the FP32 copy may share the index array
+        HB_CUDA_TRY(ctx, cudaMemcpyAsync(dst->Aj, src->Aj, total * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
     const unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 32);
     ell_cast_kernel<<<blocks, 256, 0, ctx->stream>>>(total, (const double *)src->Ax, (float *)dst->Ax);
     return hb_check_launch(ctx, "ell_cast_kernel");
 }
 
-int hb_q1_assemble_f64(hb_context *ctx, int64_t M, const double *coef, hb_ell *out)
+int hb_q1_assemble_f64(hb_context *ctx, int64_t M, const double *coef, int symmetric, hb_ell *out)
 {
     if (!ctx || !out || M < 1) return HB_ERR_INVALID;
     const int64_t N = M * M;
@@ -327,7 +343,7 @@ int hb_q1_assemble_f64(hb_context *ctx, int64_t M, const double *coef, hb_ell *o
     int st = hb_check_ell(out, HB_F64);
     if (st) return st;
     const unsigned blocks = (unsigned)std::min<int64_t>((ld + 255) / 256, (int64_t)ctx->num_sms * 32);
-    q1_assemble_kernel<<<blocks, 256, 0, ctx->stream>>>(M, coef, ld, out->Aj, (double *)out->Ax);
+    q1_assemble_kernel<<<blocks, 256, 0, ctx->stream>>>(M, coef, ld, symmetric, out->Aj, (double *)out->Ax);
     return hb_check_launch(ctx, "q1_assemble_kernel");
 }
 

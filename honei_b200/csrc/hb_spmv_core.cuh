@@ -10,13 +10,15 @@ namespace hbd {
 // accumulated left to right with one rounding per multiply and add.
 // KT > 0: K is a compile-time constant, all slot loads first; KT == 0: runtime K, 4 slots per
 // chunk.
-template <typename T, int KT, typename Gather>
+// CH = slots whose loads are in flight together (register budget); CH >= KT loads every slot
+// before the first gather.
+template <typename T, int KT, int CH = (KT > 0 ? KT : 4), typename Gather>
 __device__ __forceinline__ void ell_rows4(const int32_t *__restrict__ Aj, const T *__restrict__ Ax,
                                           int64_t ld, int K, int64_t r0, Gather gather, T (&sum)[4])
 {
 #pragma unroll
     for (int i = 0; i < 4; ++i) sum[i] = T(0);
-    if (KT > 0) {
+    if (KT > 0 && CH >= KT) {
         // every slot's Aj/Ax load issued before the first gather: one memory round trip
         int32_t j[KT > 0 ? KT : 1][4];
         T a[KT > 0 ? KT : 1][4];
@@ -32,7 +34,6 @@ __device__ __forceinline__ void ell_rows4(const int32_t *__restrict__ Aj, const 
                 if (j[k][i] >= 0) sum[i] = add(sum[i], mul(a[k][i], gather(j[k][i])));
         return;
     }
-    constexpr int CH = 4;
     const int kend = KT > 0 ? KT : K;
 #pragma unroll
     for (int k0 = 0; k0 < kend; k0 += CH) {

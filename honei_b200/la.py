@@ -147,8 +147,9 @@ class SparseMatrixELL:
 
     @classmethod
     def q1_poisson(cls, M: int, coef: torch.Tensor | None = None, ctx: Context | None = None,
-                   device="cuda") -> "SparseMatrixELL":
-        """Q1 Poisson (Dirichlet rows identity) assembled on the device, FP64."""
+                   device="cuda", symmetric: bool = False) -> "SparseMatrixELL":
+        """Q1 Poisson (Dirichlet rows identity) assembled on the device, FP64; symmetric=True
+        drops the interior rows' boundary couplings (SPD form)."""
         ctx = ctx or default_context()
         N = M * M
         K, ld = cls.layout(N, 9, 1)
@@ -160,7 +161,8 @@ class SparseMatrixELL:
             cptr = _vec(coef, torch.float64, "coef")
             if coef.numel() != (M - 1) * (M - 1):
                 raise VectorSizeDoesNotMatch(coef.numel(), (M - 1) * (M - 1))
-        check(lib().hb_q1_assemble_f64(ctx.handle, M, cptr, C.byref(out)), "hb_q1_assemble_f64", ctx.handle)
+        check(lib().hb_q1_assemble_f64(ctx.handle, M, cptr, int(symmetric), C.byref(out)), "hb_q1_assemble_f64",
+              ctx.handle)
         return cls(N, N, K, ld, Aj, Ax)
 
     def to_float(self, ctx: Context | None = None) -> "SparseMatrixELL":

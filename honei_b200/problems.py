@@ -100,11 +100,13 @@ def ell_from_csr(rows: int, cols: int, indptr, indices, data, threads: int = 1,
     return EllMatrix(rows, cols, stride, ncpr, T, Aj, Ax, Arl, int(len(indices)))
 
 
-def q1_poisson_csr(M: int, coef=None):
+def q1_poisson_csr(M: int, coef=None, symmetric: bool = False):
     """CSR of the Q1 Poisson matrix on an M x M node grid, Dirichlet rows = identity.
 
     ``coef`` is None (unit coefficient) or an (M-1, M-1) array of per-cell coefficients.
-    Node r = i*M + j (lexicographic), as FillMatrix numbers them.
+    Node r = i*M + j (lexicographic), as FillMatrix numbers them.  ``symmetric`` drops the
+    interior rows' couplings to boundary nodes (Dirichlet values eliminated into the right-hand
+    side), which makes the matrix SPD; the default keeps them, as FillMatrix does.
     """
     M = int(M)
     N = M * M
@@ -143,12 +145,20 @@ def q1_poisson_csr(M: int, coef=None):
         for s, (o, v) in enumerate(zip(offs, vals)):
             indices[base + s] = inner + o
             data[base + s] = v
+        if symmetric:
+            keep = np.ones(len(indices), bool)
+            row_of = np.repeat(np.arange(N, dtype=np.int64), counts)
+            keep[(~bnd[row_of]) & bnd[indices]] = False
+            new_counts = np.bincount(row_of[keep], minlength=N).astype(np.int64)
+            indptr = np.zeros(N + 1, np.int64)
+            np.cumsum(new_counts, out=indptr[1:])
+            indices, data = indices[keep], data[keep]
     return indptr, indices, data
 
 
-def q1_poisson(M: int, coef=None, threads: int = 1, dtype=np.float64) -> EllMatrix:
+def q1_poisson(M: int, coef=None, threads: int = 1, dtype=np.float64, symmetric: bool = False) -> EllMatrix:
     """Q1 Poisson ELL matrix (see module docstring); FP32 values are the FP64 values cast."""
-    indptr, indices, data = q1_poisson_csr(M, coef)
+    indptr, indices, data = q1_poisson_csr(M, coef, symmetric)
     A = ell_from_csr(M * M, M * M, indptr, indices, data, threads, np.float64)
     return A if dtype == np.float64 else A.astype(dtype)
 

@@ -103,9 +103,12 @@ int hb_ell_cast_f64_f32(hb_context *ctx, const hb_ell *src, hb_ell *dst);
 /* Q1 Poisson assembly on the device (the FillMatrix<POISSON, DIRICHLET_0> stencil,
  * honei/math/fill_matrix.hh:37-77, built straight into hb_ell layout, K = 9): M x M nodes,
  * Dirichlet rows identity; coef = NULL (unit) or device double[(M-1)^2] cell coefficients
- * (bilinear element matrix k/6 [[4,-1,-2,-1],...]).  out->Aj/Ax preallocated with K=9,
- * ld from hb_ell_layout(M*M, 9, 1).  Identical to the host generator bit for bit. */
-int hb_q1_assemble_f64(hb_context *ctx, int64_t M, const double *coef, hb_ell *out);
+ * (bilinear element matrix k/6 [[4,-1,-2,-1],...]).  symmetric = 0 keeps the interior rows'
+ * couplings to boundary nodes, as FillMatrix does (non-symmetric); symmetric = 1 drops them
+ * (Dirichlet values eliminated into the right-hand side), which makes the matrix SPD.
+ * out->Aj/Ax preallocated with K=9, ld from hb_ell_layout(M*M, 9, 1).  Identical to the host
+ * generator (honei_b200/problems.py) bit for bit. */
+int hb_q1_assemble_f64(hb_context *ctx, int64_t M, const double *coef, int symmetric, hb_ell *out);
 
 /* ------------------------------------------------------------------------------------------
  * Operators (the static value() functions of the tag-dispatched API).
@@ -234,6 +237,70 @@ int hb_ir_mg_solve(hb_context *ctx, const hb_ell *A64, hb_mg *mg32, const double
 int hb_ir_cg_solve(hb_context *ctx, const hb_ell *A64, const hb_ell *A32, const double *b, double *x,
                    double eps, float inner_eps, int64_t inner_max_iters, int64_t max_iters,
                    int64_t *used_outer, int64_t *inner_total, double *rnorm_host);
+
+/* ------------------------------------------------------------------------------------------
+ * Batched solves (no reference counterpart: HONEI solves one system per CGSolver call).
+ * Many independent systems of uneven size in ONE persistent launch: each system is solved by
+ * one thread-block cluster (hardware cluster barriers, DSMEM reductions), clusters pull
+ * systems largest-first from a device work counter.  A system's result depends only on the
+ * system and the launch shape, never on what else is in the batch (same answer alone and in
+ * the mix, bit for bit).
+ *   HB_BATCH_CG64: plain FP64 CG with CGSolver<NONE>'s update formulas and dual stopping rule.
+ *   HB_BATCH_IR32: FP64 outer refinement (defect, norm, update in FP64) around FP32 CG with
+ *                  FP32 accumulation on the normalised defect to inner_eps per outer step,
+ *                  until ||b - A x|| < eps ||b - A x0||.
+ * A64 is always required (FP64 values); A32 (same pattern, FP32 values) for HB_BATCH_IR32.
+ * ---------------------------------------------------------------------------------------- */
+enum { HB_BATCH_CG64 = 0, HB_BATCH_IR32 = 1 };
+
+typedef struct {
+    hb_ell A64;                /* device matrix, FP64 values                              */
+    hb_ell A32;                /* same pattern, FP32 values (HB_BATCH_IR32), else zeroed   */
+    const double *b;           /* device, n entries                                       */
+    double *x;                 /* device, n entries: x0 in, solution out                  */
+    int32_t mode;              /* HB_BATCH_CG64 / HB_BATCH_IR32                           */
+    int32_t pad_;
+    int64_t max_iters;         /* CG iterations (CG64) / inner CG iterations per step (IR) */
+    int64_t max_outer;         /* outer refinement steps (IR)                             */
+    double eps;                /* CG64: CGSolver eps; IR: target relative FP64 residual   */
+    double inner_eps;          /* IR: inner relative eps (FP32 CG)                        */
+} hb_batch_system;
+
+typedef struct {
+    int64_t iterations;        /* CG iterations (IR: summed inner iterations)             */
+    int64_t outer;             /* outer steps (IR), 0 for CG64                            */
+    double defect0;            /* initial defect norm (CG64: sqrt(alpha0))                 */
+    double defect;             /* final defect norm (CG64: sqrt(alpha), IR: true FP64)     */
+    double true_relres;        /* ||b - A x|| / ||b|| in FP64 after the solve             */
+    int32_t status;            /* hb_status                                               */
+    int32_t pad_;
+} hb_batch_result;
+
+typedef struct {
+    int32_t cluster;           /* CTAs per system: 1, 2, 4, 8 or 16                        */
+    int32_t threads;           /* threads per CTA: 256 or 512                              */
+} hb_batch_config;
+
+/* Device workspace bytes for these systems (work vectors, descriptors, results, counter). */
+int hb_batch_workspace_bytes(const hb_batch_system *sys, int64_t count, size_t *bytes);
+/* Solve all systems in one launch (workspace: device, hb_batch_workspace_bytes long, 256-byte
+ * aligned).  results_host receives one record per system.  cfg = NULL picks the default
+ * (cluster 4, 512 threads).  Synchronous. */
+int hb_batch_solve(hb_context *ctx, const hb_batch_system *sys, int64_t count, void *workspace,
+                   const hb_batch_config *cfg, hb_batch_result *results_host);
+/* Two-step form for CUDA graphs: prepare writes the device descriptors into the workspace
+ * (synchronous, once per batch); run only resets the work counter and launches, so it can be
+ * captured into a graph and replayed.  Results land in the workspace; hb_batch_results copies
+ * them to the host. */
+int hb_batch_prepare(hb_context *ctx, const hb_batch_system *sys, int64_t count, void *workspace);
+int hb_batch_run(hb_context *ctx, int64_t count, void *workspace, const hb_batch_config *cfg);
+int hb_batch_results(hb_context *ctx, int64_t count, void *workspace, hb_batch_result *results_host);
+/* Autotuner core: times every (cluster, threads) candidate on this batch (each run once after a
+ * warm-up) and returns the fastest in *best; times_ms (may be NULL) receives one time per
+ * candidate in the order cluster {1,2,4,8,16} x threads {256,512} (-1 = shape not launchable).
+ * Every run starts from x = 0 (the systems' x are zeroed and overwritten). */
+int hb_batch_tune(hb_context *ctx, const hb_batch_system *sys, int64_t count, void *workspace,
+                  hb_batch_config *best, double *times_ms);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

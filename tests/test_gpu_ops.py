@@ -123,12 +123,17 @@ def test_import_rejects_out_of_range_columns(hb):
     assert getattr(ei.value, "status", None) == 1
 
 
-def test_device_q1_assembly_matches_host_generator(hb, oracle):
+@pytest.mark.parametrize("symmetric", [False, True])
+def test_device_q1_assembly_matches_host_generator(hb, oracle, symmetric):
     for M, coef in ((3, None), (33, None), (257, P.log_uniform_coef(257, 1e-2, 1e2, 9))):
-        Ah = P.q1_poisson(M, coef)
-        Ad = hb.SparseMatrixELL.q1_poisson(M, None if coef is None else dev(coef.ravel()))
+        Ah = P.q1_poisson(M, coef, symmetric=symmetric)
+        Ad = hb.SparseMatrixELL.q1_poisson(M, None if coef is None else dev(coef.ravel()), symmetric=symmetric)
         Ai = hb.SparseMatrixELL.from_reference(Ah)
-        assert torch.equal(Ad.Aj, Ai.Aj) and torch.equal(Ad.Ax, Ai.Ax)
+        # the device kernel always lays out K = 9 slots; the host packing may need fewer
+        K = Ai.K
+        assert Ad.ld == Ai.ld and K <= Ad.K
+        assert torch.equal(Ad.Aj[: K * Ad.ld], Ai.Aj) and torch.equal(Ad.Ax[: K * Ad.ld], Ai.Ax)
+        assert bool((Ad.Aj[K * Ad.ld:] == -1).all()) and bool((Ad.Ax[K * Ad.ld:] == 0).all())
         x = P.uniform_vector(M * M, 2)
         y = torch.empty(M * M, dtype=torch.float64, device="cuda")
         hb.Product.value(y, Ad, dev(x))

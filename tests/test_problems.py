@@ -79,3 +79,20 @@ def test_mg_hierarchy_sides():
     assert H.sides == [9, 17, 33, 65]
     assert [a.rows for a in H.A] == [81, 289, 1089, 4225]
     assert [(p.rows, p.cols) for p in H.prol] == [(289, 81), (1089, 289), (4225, 1089)]
+
+
+def test_symmetric_form_is_spd_and_consistent():
+    import scipy.sparse as sp
+    M = 9
+    A = P.q1_poisson(M, P.log_uniform_coef(M, 1e-2, 1e2, 2), symmetric=True)
+    ip, ix, dv = A.to_csr()
+    S = sp.csr_matrix((dv, ix, ip), shape=(A.rows, A.cols)).toarray()
+    assert np.array_equal(S, S.T)
+    assert np.linalg.eigvalsh(S).min() > 0
+    full = P.q1_poisson(M, P.log_uniform_coef(M, 1e-2, 1e2, 2))
+    fi, fx, fd = full.to_csr()
+    F = sp.csr_matrix((fd, fx, fi), shape=(A.rows, A.cols)).toarray()
+    ii, jj = np.divmod(np.arange(M * M), M)
+    bnd = (ii == 0) | (ii == M - 1) | (jj == 0) | (jj == M - 1)
+    assert np.array_equal(S[np.ix_(~bnd, ~bnd)], F[np.ix_(~bnd, ~bnd)])
+    assert np.array_equal(S[bnd], F[bnd])
