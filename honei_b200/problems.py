@@ -286,7 +286,8 @@ def galerkin_csr(A: EllMatrix, prol: EllMatrix, res: EllMatrix):
     return Ac.shape[0], Ac.indptr.astype(np.int64), Ac.indices.astype(np.int64), Ac.data
 
 
-def mg_hierarchy(M: int, coarsest: int = 9, coef=None, threads: int = 1, coarse: str = "auto") -> MGHierarchy:
+def mg_hierarchy(M: int, coarsest: int = 9, coef=None, threads: int = 1, coarse: str = "auto",
+                 symmetric: bool = False) -> MGHierarchy:
     """Q1 Poisson hierarchy on sides M, (M+1)/2, ..., coarsest (all of the form 2^k + 1).
 
     coarse = "rediscretize": every level is the Q1 matrix of its own grid (coarser cell
@@ -316,11 +317,48 @@ def mg_hierarchy(M: int, coarsest: int = 9, coef=None, threads: int = 1, coarse:
         t_ip, t_ix, t_dv = transpose_csr(nf, nc, ip, ix, dv)
         res.append(ell_from_csr(nc, nf, t_ip, t_ix, t_dv, threads))
     if coarse == "rediscretize":
-        A = [q1_poisson(s, coefs[l], threads) for l, s in enumerate(sides)]
+        A = [q1_poisson(s, coefs[l], threads, symmetric=symmetric) for l, s in enumerate(sides)]
     else:
         A = [None] * len(sides)
-        A[-1] = q1_poisson(sides[-1], coefs[-1], threads)
+        A[-1] = q1_poisson(sides[-1], coefs[-1], threads, symmetric=symmetric)
         for l in range(len(sides) - 1, 0, -1):
             n, ip, ix, dv = galerkin_csr(A[l], prol[l - 1], res[l - 1])
             A[l - 1] = ell_from_csr(n, n, ip, ix, dv, threads)
     return MGHierarchy(A, prol, res, sides)
+
+
+# ---------------------------------------------------------------------------------------------
+# HONEI file formats (honei/math/matrix_io.hh:433-582, honei/math/vector_io.hh:52-115)
+# ---------------------------------------------------------------------------------------------
+def write_ell(path: str, A: EllMatrix) -> None:
+    """Binary ELL file: u64 {size, rows, cols, stride, ncpr}, u64 Aj[size], f64 Ax[size]
+    (MatrixIO<io_formats::ELL>::write_matrix; FP64, one lane per row)."""
+    if A.threads != 1:
+        raise ValueError("the ELL file format stores one-lane layouts only")
+    size = A.ncpr * A.stride
+    with open(path, "wb") as f:
+        np.array([size, A.rows, A.cols, A.stride, A.ncpr], np.uint64).tofile(f)
+        np.asarray(A.Aj, np.uint64).tofile(f)
+        np.asarray(A.Ax, np.float64).tofile(f)
+
+
+def read_ell(path: str) -> EllMatrix:
+    """Reads a binary ELL file (MatrixIO<io_formats::ELL>::read_matrix); Arl is recomputed from
+    the first zero value of every row, as the reference's raw-array constructor does."""
+    with open(path, "rb") as f:
+        size, rows, cols, stride, ncpr = (int(v) for v in np.fromfile(f, np.uint64, 5))
+        Aj = np.fromfile(f, np.uint64, size)
+        Ax = np.fromfile(f, np.float64, size)
+    nz = (Ax.reshape(ncpr, stride)[:, :rows] != 0)
+    # row length = number of leading non-zero slots
+    first_zero = np.where(nz.all(axis=0), ncpr, np.argmin(nz, axis=0))
+    Arl = first_zero.astype(np.uint64)
+    return EllMatrix(rows, cols, stride, ncpr, 1, Aj, Ax, Arl, int(Arl.sum()))
+
+
+def write_exp(path: str, v) -> None:
+    """EXP vector file: a '#' header line, then one value per line (VectorIO<io_formats::EXP>)."""
+    with open(path, "w") as f:
+        f.write("# honei_b200 vector\n")
+        for x in np.asarray(v, np.float64):
+            f.write(repr(float(x)) + "\n")

@@ -1,0 +1,196 @@
+// HONEI's own operators and generic solver templates on tags::GPU::CUDA, provided by the B200
+// plugin (honei_b200/plugin), checked against tags::CPU on the same inputs.
+//   plugin_ops_test [mg_dir]
+// mg_dir holds A_1..A_L.ell, prol_2..prol_L.ell, rhs_L, init_L (HONEI file formats); it is
+// loaded with MGUtil::load_data exactly as honei/math/mg_TEST.cc loads FEATFLOW data.
+// This translation unit does NOT include solvers_b200.hh: CGSolver<tags::GPU::CUDA, NONE> here
+// is HONEI's generic template (honei/math/cg.hh:63-133) running on the plugin's operators.
+#include "plugin_common.hh"
+
+#include <honei/la/difference.hh>
+#include <honei/la/dot_product.hh>
+#include <honei/la/element_product.hh>
+#include <honei/la/norm.hh>
+#include <honei/la/product.hh>
+#include <honei/la/scale.hh>
+#include <honei/la/scaled_sum.hh>
+#include <honei/la/sum.hh>
+#include <honei/math/cg.hh>
+#include <honei/math/defect.hh>
+#include <honei/math/matrix_io.hh>
+#include <honei/math/mg.hh>
+#include <honei/math/operator.hh>
+#include <honei/math/prolongation.hh>
+#include <honei/math/restriction.hh>
+#include <honei/math/ri.hh>
+#include <honei/math/vector_io.hh>
+
+#include <iostream>
+#include <sstream>
+
+using namespace honei;
+using namespace plugin_test;
+
+template <typename DT_> bool equal(const DenseVector<DT_> & a, const DenseVector<DT_> & b)
+{
+    a.lock(lm_read_only);
+    b.lock(lm_read_only);
+    bool ok(a.size() == b.size());
+    for (unsigned long i(0) ; ok && i < a.size() ; ++i)
+        ok = (a[i] == b[i]);
+    a.unlock(lm_read_only);
+    b.unlock(lm_read_only);
+    return ok;
+}
+
+template <typename DT_> void operators(unsigned long M, const std::string & tag)
+{
+    SparseMatrixELL<DT_> A(q1<DT_>(M));
+    const unsigned long n(A.rows());
+    DenseVector<DT_> x(seeded<DT_>(n, 1)), y(seeded<DT_>(n, 2)), b(seeded<DT_>(n, 3));
+
+    DenseVector<DT_> ycpu(n), ygpu(n);
+    Product<tags::CPU>::value(ycpu, A, x);
+    Product<tags::GPU::CUDA>::value(ygpu, A, x);
+    report(equal(ycpu, ygpu), "Product<GPU::CUDA> ELL bit-exact " + tag);
+
+    DenseVector<DT_> rcpu(n), rgpu(n);
+    Defect<tags::CPU>::value(rcpu, b, A, x);
+    Defect<tags::GPU::CUDA>::value(rgpu, b, A, x);
+    report(equal(rcpu, rgpu), "Defect<GPU::CUDA> ELL bit-exact " + tag);
+
+    const DT_ dc(DotProduct<tags::CPU>::value(x, y)), dg(DotProduct<tags::GPU::CUDA>::value(x, y));
+    DT_ scale(0);
+    for (unsigned long i(0) ; i < n ; ++i) scale += std::abs(x[i] * y[i]);
+    const double tol(sizeof(DT_) == 8 ? 1e-13 : 1e-5);
+    report(std::abs(dc - dg) <= tol * scale, "DotProduct<GPU::CUDA> " + tag);
+    const DT_ nc(Norm<vnt_l_two, true, tags::CPU>::value(x)), ng(Norm<vnt_l_two, true, tags::GPU::CUDA>::value(x));
+    report(std::abs(nc - ng) <= tol * nc, "Norm<l2, true, GPU::CUDA> " + tag);
+    const DT_ nsc(Norm<vnt_l_two, false, tags::CPU>::value(x)), nsg(Norm<vnt_l_two, false, tags::GPU::CUDA>::value(x));
+    report(std::abs(nsc - nsg) <= tol * nsc, "Norm<l2, false, GPU::CUDA> " + tag);
+
+    DenseVector<DT_> a1(x.copy()), a2(x.copy());
+    ScaledSum<tags::CPU>::value(a1, y, DT_(0.37));
+    ScaledSum<tags::GPU::CUDA>::value(a2, y, DT_(0.37));
+    report(equal(a1, a2), "ScaledSum<GPU::CUDA>(x, y, b) bit-exact " + tag);
+    DenseVector<DT_> s1(n), s2(n);
+    ScaledSum<tags::CPU>::value(s1, x, y, DT_(-1.25));
+    ScaledSum<tags::GPU::CUDA>::value(s2, x, y, DT_(-1.25));
+    report(equal(s1, s2), "ScaledSum<GPU::CUDA>(r, x, y, b) bit-exact " + tag);
+    DenseVector<DT_> c1(x.copy()), c2(x.copy());
+    Scale<tags::CPU>::value(c1, DT_(3.1));
+    Scale<tags::GPU::CUDA>::value(c2, DT_(3.1));
+    report(equal(c1, c2), "Scale<GPU::CUDA> bit-exact " + tag);
+    DenseVector<DT_> u1(x.copy()), u2(x.copy());
+    Sum<tags::CPU>::value(u1, y);
+    Sum<tags::GPU::CUDA>::value(u2, y);
+    report(equal(u1, u2), "Sum<GPU::CUDA> bit-exact " + tag);
+    DenseVector<DT_> d1(x.copy()), d2(x.copy());
+    Difference<tags::CPU>::value(d1, y);
+    Difference<tags::GPU::CUDA>::value(d2, y);
+    report(equal(d1, d2), "Difference<GPU::CUDA> bit-exact " + tag);
+    DenseVector<DT_> e1(x.copy()), e2(x.copy());
+    ElementProduct<tags::CPU>::value(e1, y);
+    ElementProduct<tags::GPU::CUDA>::value(e2, y);
+    report(equal(e1, e2), "ElementProduct<GPU::CUDA> bit-exact " + tag);
+
+    // coherence: change x on the host after a GPU use; the next GPU product must see it
+    x.lock(lm_read_and_write);
+    x[n / 2] += DT_(1);
+    x.unlock(lm_read_and_write);
+    Product<tags::CPU>::value(ycpu, A, x);
+    Product<tags::GPU::CUDA>::value(ygpu, A, x);
+    report(equal(ycpu, ygpu), "host write of x is seen by the next GPU product " + tag);
+
+    // a host change of the matrix values invalidates the device mirror
+    A.Ax().lock(lm_read_and_write);
+    A.Ax()[A.stride() * 4 + M + 1] *= DT_(2);
+    A.Ax().unlock(lm_read_and_write);
+    Product<tags::CPU>::value(ycpu, A, x);
+    Product<tags::GPU::CUDA>::value(ygpu, A, x);
+    report(equal(ycpu, ygpu), "host write of A is seen by the next GPU product " + tag);
+
+    bool threw(false);
+    try
+    {
+        DenseVector<DT_> wrong(n + 1);
+        Product<tags::GPU::CUDA>::value(wrong, A, x);
+    }
+    catch (VectorSizeDoesNotMatch &)
+    {
+        threw = true;
+    }
+    report(threw, "VectorSizeDoesNotMatch before launch " + tag);
+}
+
+void generic_cg()
+{
+    // HONEI's generic CGSolver template on the GPU tag (operator by operator)
+    SparseMatrixELL<double> A(q1<double>(65));
+    const unsigned long n(A.rows());
+    DenseVector<double> xt(seeded<double>(n, 7)), b(n);
+    Product<tags::CPU>::value(b, A, xt);
+    DenseVector<double> xc(n, 0.), xg(n, 0.);
+    unsigned long uc(0), ug(0);
+    CGSolver<tags::CPU, methods::NONE>::value(A, A, b, xc, 10000ul, uc, 1e-8);
+    CGSolver<tags::GPU::CUDA, methods::NONE>::value(A, A, b, xg, 10000ul, ug, 1e-8);
+    std::ostringstream d;
+    d << "iterations cpu " << uc << " gpu " << ug;
+    // tags::CPU's product reads elements() without locking: bring the GPU result home first
+    xg.lock(lm_read_only);
+    xg.unlock(lm_read_only);
+    DenseVector<double> r(n);
+    Defect<tags::CPU>::value(r, b, A, xg);
+    const double rel(Norm<vnt_l_two, true, tags::CPU>::value(r) / Norm<vnt_l_two, true, tags::CPU>::value(b));
+    d << ", relres " << rel;
+    report((uc > ug ? uc - ug : ug - uc) <= 1 && rel < 1.5e-8, "generic CGSolver<GPU::CUDA, NONE> vs tags::CPU", d.str());
+}
+
+template <typename Tag_> void run_mg(const std::string & dir, unsigned long L, DenseVector<double> & x_out,
+        unsigned long & cycles)
+{
+    typedef MGUtil<Tag_, SparseMatrixELL<double>, DenseVector<double>, SparseMatrixELL<double>, DenseVector<double>,
+            MatrixIO<io_formats::ELL>, VectorIO<io_formats::EXP>, double> Util;
+    MGData<SparseMatrixELL<double>, DenseVector<double>, SparseMatrixELL<double>, DenseVector<double>, double>
+        data(Util::load_data(dir + "/", L, 0.7, "jac"));
+    Util::configure(data, 100, 1000, 2, 2, 1, 1e-8);
+    OperatorList ol(MGCycleCreation<Tag_, methods::CYCLE::V::STATIC, CGSolver<Tag_, methods::NONE>, RISmoother<Tag_>,
+            Restriction<Tag_, methods::PROLMAT>, Prolongation<Tag_, methods::PROLMAT>, double>::value(data));
+    MGSolver<Tag_, Norm<vnt_l_two, true, Tag_> >::value(data, ol);
+    cycles = data.used_iters;
+    x_out = data.x.back().copy();
+}
+
+void generic_mg(const std::string & dir, unsigned long L)
+{
+    DenseVector<double> xc(1), xg(1);
+    unsigned long cc(0), cg(0);
+    run_mg<tags::CPU>(dir, L, xc, cc);
+    run_mg<tags::GPU::CUDA>(dir, L, xg, cg);
+    double err(0), nrm(0);
+    xc.lock(lm_read_only);
+    xg.lock(lm_read_only);
+    for (unsigned long i(0) ; i < xc.size() ; ++i)
+    {
+        err = std::max(err, std::abs(xc[i] - xg[i]));
+        nrm = std::max(nrm, std::abs(xc[i]));
+    }
+    xc.unlock(lm_read_only);
+    xg.unlock(lm_read_only);
+    std::ostringstream d;
+    d << "cycles cpu " << cc << " gpu " << cg << ", max |x_gpu - x_cpu| / max |x| = " << err / nrm;
+    report((cc > cg ? cc - cg : cg - cc) <= 1 && err <= 1e-6 * nrm, "MGSolver<GPU::CUDA> (MGUtil::load_data, V(2,2), jac)",
+            d.str());
+}
+
+int main(int argc, char ** argv)
+{
+    operators<double>(33, "f64 33^2");
+    operators<double>(129, "f64 129^2");
+    operators<float>(65, "f32 65^2");
+    generic_cg();
+    if (argc > 2)
+        generic_mg(argv[1], std::stoul(argv[2]));
+    std::printf("%d failure(s)\n", failures());
+    return failures() ? 1 : 0;
+}

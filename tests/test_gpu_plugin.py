@@ -1,0 +1,50 @@
+"""HONEI's own operators and solver templates on tags::GPU::CUDA through the B200 plugin
+(honei_b200/plugin): the C++ programs in tests/plugin link HONEI's CPU library and the plugin,
+and compare every GPU-tag result with tags::CPU on the same inputs.  The MG case loads its
+hierarchy with HONEI's MGUtil::load_data from files written in HONEI's formats."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from honei_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+BUILD = os.path.join(ROOT, "tests", "plugin", "_build")
+
+
+def _run(name, *args):
+    exe = os.path.join(BUILD, name)
+    if not os.path.exists(exe):
+        pytest.skip(f"{exe} not built (make -C tests/plugin needs the HONEI headers)")
+    p = subprocess.run([exe, *args], capture_output=True, text=True, timeout=600)
+    print(p.stdout)
+    print(p.stderr[-2000:])
+    fails = [l for l in p.stdout.splitlines() if l.startswith("FAIL")]
+    assert p.returncode == 0 and not fails, fails or p.stderr[-2000:]
+    return p.stdout
+
+
+def test_plugin_operators_and_generic_solvers(tmp_path):
+    H = P.mg_hierarchy(65)
+    L = len(H.A)
+    for l, A in enumerate(H.A, 1):
+        P.write_ell(str(tmp_path / f"A_{l}.ell"), A)
+    for l, Pm in enumerate(H.prol, 2):
+        P.write_ell(str(tmp_path / f"prol_{l}.ell"), Pm)
+    A = H.A[-1]
+    xt = P.uniform_vector(A.rows, 4)
+    ip, ix, dv = A.to_csr()
+    b = np.add.reduceat(dv * xt[ix], ip[:-1])
+    P.write_exp(str(tmp_path / f"rhs_{L}"), b)
+    P.write_exp(str(tmp_path / f"init_{L}"), np.zeros(A.rows))
+    out = _run("plugin_ops_test", str(tmp_path), str(L))
+    assert "PASS MGSolver<GPU::CUDA>" in out
+    assert out.count("PASS") >= 40
+
+
+def test_plugin_cg_specialisation():
+    out = _run("plugin_cg_test")
+    assert out.count("PASS") == 4
