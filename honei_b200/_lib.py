@@ -94,6 +94,15 @@ SIGNATURES = {
     "hb_batch_run": (i32, [vp, i64, vp, vp]),
     "hb_batch_results": (i32, [vp, i64, vp, vp]),
     "hb_batch_tune": (i32, [vp, vp, i64, vp, vp, vp]),
+    # served Q1 systems (device-built multigrid)
+    "hb_q1_coarse_side": (i32, [i64]),
+    "hb_q1_transfers": (i32, [vp, i64, P_ell, P_ell]),
+    "hb_q1_galerkin": (i32, [vp, i64, P_ell, P_ell]),
+    "hb_q1_create": (i32, [vp, i64, vp, C.POINTER(vp)]),
+    "hb_q1_destroy": (i32, [vp]),
+    "hb_q1_levels": (i32, [vp, C.POINTER(i32), P_i64]),
+    "hb_q1_level": (i32, [vp, i32, P_ell, P_ell, P_ell, P_ell]),
+    "hb_q1_solve": (i32, [vp, vp, vp, f64, f64, i64, i64, vp]),
 }
 
 

@@ -70,6 +70,14 @@ int hb_create(hb_context **out, int device)
         return HB_ERR_ALLOC;
     }
     std::memset(ctx->pinned, 0, 4096);
+    // keep freed stream-ordered allocations in the device pool (no release to the driver
+    // between requests)
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
     *out = ctx;
     return HB_OK;
 }

@@ -84,6 +84,14 @@ template <typename T>
 int hb_launch_cg(hb_context *ctx, const hb_ell *A, const T *b, T *x, int64_t max_iters, T eps, T *work,
                  hb_solve_result *res);
 
+// MG-preconditioned CG in FP32 on the finest level of an FP32 hierarchy (hb_mg.cu).
+struct hb_mg;
+int hb_mg_pcg_f32(hb_mg *mg, const float *b, float *x, float eps, int64_t max_iters, float *work, int64_t *used);
+int hb_mg_finest(hb_mg *mg, hb_ell *A);
+int hb_mg_set_dense_coarse(hb_mg *mg, void *inv);
+int hb_mg_pcg_f32_graph(hb_mg *mg, cudaStream_t capture_stream, const float *b, float *x, float eps, int64_t max_iters,
+                        float *work, cudaGraphExec_t *graph, int check_every, int64_t *used);
+
 // --------------------------------------------------------------------------------------
 // Device helpers
 // --------------------------------------------------------------------------------------

@@ -37,6 +37,8 @@ struct hb_mg {
     double *ir_r = nullptr;
     float *ir_b = nullptr, *ir_x = nullptr;
     int64_t used_coarse_total = 0;
+    // optional exact coarse solve: dense inverse of A[0] (row-major, dtype), replacing the CG
+    void *coarse_inv = nullptr;
 };
 
 namespace {
@@ -127,9 +129,24 @@ template <typename T> int smooth(hb_mg *mg, int l, T *X, const T *B, int64_t swe
     return HB_OK;
 }
 
+// x = Ainv b on the coarsest level (one block, one thread per row, fixed summation order).
+template <typename T>
+__global__ void dense_solve_kernel(int64_t n, const T *__restrict__ inv, const T *__restrict__ b, T *__restrict__ x)
+{
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        T acc = T(0);
+        for (int64_t j = 0; j < n; ++j) acc = hbd::add(acc, hbd::mul(inv[i * n + j], b[j]));
+        x[i] = acc;
+    }
+}
+
 template <typename T> int vcycle(hb_mg *mg, int l, T *X, const T *B)
 {
     hb_context *ctx = mg->ctx;
+    if (l == 0 && mg->coarse_inv) {
+        dense_solve_kernel<T><<<1, 128, 0, ctx->stream>>>(mg->A[0].rows, tp<T>(mg->coarse_inv), B, X);
+        return hb_check_launch(ctx, "dense_solve_kernel");
+    }
     if (l == 0)
         return hb_launch_cg<T>(ctx, &mg->A[0], B, X, mg->prm.max_iters_coarse, (T)mg->prm.eps, tp<T>(mg->cgwork),
                                mg->cgres);
@@ -171,6 +188,236 @@ template <typename T> int mg_solve(hb_mg *mg, const T *b, T *x, int64_t *used, T
 }
 
 inline size_t pad_entries(int64_t n) { return (size_t)hb_round_up(n > 0 ? n : 1, 64); }
+
+// Device dot product read back to the host (one sync).
+template <typename T> int dot_host(hb_context *ctx, int64_t n, const T *x, const T *y, T *dev_slot, T *out)
+{
+    HB_TRY(hb_launch_dot<T>(ctx, n, x, y, dev_slot));
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->pinned, dev_slot, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    *out = *static_cast<T *>(ctx->pinned);
+    return HB_OK;
+}
+
+}  // namespace
+
+// Preconditioned CG in FP32 with one V-cycle from a zero start as the preconditioner (damped
+// Jacobi pre/post smoothing, R = P^T, coarse CG): a symmetric positive definite preconditioner
+// for SPD systems with Galerkin coarse levels.  Solves A x = b on the finest level of mg from
+// x = 0 until ||r|| < eps ||b||.  work: 4 vectors of the finest size (r, z, p, v).
+int hb_mg_pcg_f32(hb_mg *mg, const float *b, float *x, float eps, int64_t max_iters, float *work, int64_t *used)
+{
+    hb_context *ctx = mg->ctx;
+    const int top = mg->L - 1;
+    const hb_ell *A = &mg->A[top];
+    const int64_t n = A->rows;
+    const int64_t ldn = (int64_t)pad_entries(n);
+    float *r = work, *z = work + ldn, *p = work + 2 * ldn, *v = work + 3 * ldn;
+    float *slot = tp<float>(mg->norm);
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(x, 0, sizeof(float) * n, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(r, b, sizeof(float) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    float rr;
+    HB_TRY(dot_host<float>(ctx, n, r, r, slot, &rr));
+    const float r0 = std::sqrt(rr);
+    int64_t it = 0;
+    if (r0 > 0.f && max_iters > 0) {
+        HB_CUDA_TRY(ctx, cudaMemsetAsync(z, 0, sizeof(float) * n, ctx->stream));
+        HB_TRY(vcycle<float>(mg, top, z, r));
+        HB_CUDA_TRY(ctx, cudaMemcpyAsync(p, z, sizeof(float) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+        float rz;
+        HB_TRY(dot_host<float>(ctx, n, r, z, slot, &rz));
+        while (it < max_iters) {
+            HB_TRY(hb_launch_spmv_mode<float>(ctx, A, HB_MODE_SPMV, p, nullptr, nullptr, v));
+            float pv;
+            HB_TRY(dot_host<float>(ctx, n, p, v, slot, &pv));
+            if (!(pv > 0.f)) break;                      // breakdown (not SPD / converged to 0)
+            const float a = rz / pv;
+            HB_TRY(hb_scaled_sum_f32(ctx, n, x, p, a));
+            HB_TRY(hb_scaled_sum_f32(ctx, n, r, v, -a));
+            ++it;
+            HB_TRY(dot_host<float>(ctx, n, r, r, slot, &rr));
+            if (std::sqrt(rr) < eps * r0) break;
+            HB_CUDA_TRY(ctx, cudaMemsetAsync(z, 0, sizeof(float) * n, ctx->stream));
+            HB_TRY(vcycle<float>(mg, top, z, r));
+            float rz_new;
+            HB_TRY(dot_host<float>(ctx, n, r, z, slot, &rz_new));
+            const float beta = rz_new / rz;
+            rz = rz_new;
+            HB_TRY(hb_scaled_sum3_f32(ctx, n, p, z, p, beta));   // p = beta p + z
+        }
+    }
+    hb_solve_result h;
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(&h, mg->cgres, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h.status == HB_DEV_TIMEOUT) return HB_ERR_TIMEOUT;
+    if (used) *used = it;
+    return HB_OK;
+}
+
+int hb_mg_finest(hb_mg *mg, hb_ell *A)
+{
+    *A = mg->A[mg->L - 1];
+    return HB_OK;
+}
+
+int hb_mg_set_dense_coarse(hb_mg *mg, void *inv)
+{
+    mg->coarse_inv = inv;
+    return HB_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Device-scalar PCG: every scalar of the iteration (r.z, p.v, alpha, beta, |r|) lives in device
+// memory, so one iteration is a fixed sequence of launches with no host round trip.  It is
+// captured once into a CUDA graph and replayed; the host reads the done flag every few
+// iterations.  After convergence the guarded updates are no-ops, so replays past the stop
+// leave x unchanged.
+// ---------------------------------------------------------------------------------------
+struct PcgScalars {
+    float rz, rz_new, pv, rr, r0, eps;
+    int done, it;
+};
+
+namespace {
+
+__global__ void pcg_start_kernel(PcgScalars *s, float eps)
+{
+    s->r0 = sqrtf(s->rr);
+    s->eps = eps;
+    s->done = !(s->r0 > 0.f);
+    s->it = 0;
+}
+
+// x += alpha p; r -= alpha v with alpha = rz / pv (skipped once converged or on breakdown)
+__global__ void pcg_xr_kernel(int64_t n, PcgScalars *s, float *__restrict__ x, float *__restrict__ r,
+                              const float *__restrict__ p, const float *__restrict__ v)
+{
+    if (s->done || !(s->pv > 0.f)) return;
+    const float a = s->rz / s->pv, ma = -a;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] = hbd::add(x[i], hbd::mul(a, p[i]));
+        r[i] = hbd::add(r[i], hbd::mul(ma, v[i]));
+    }
+}
+
+__global__ void pcg_check_kernel(PcgScalars *s)
+{
+    if (s->done) return;
+    if (!(s->pv > 0.f)) { s->done = 1; return; }
+    s->it += 1;
+    if (sqrtf(s->rr) < s->eps * s->r0) s->done = 1;
+}
+
+// p = beta p + z with beta = rz_new / rz; rz = rz_new (one thread finalises the scalars after
+// every block has used the old rz: a second tiny kernel does it)
+__global__ void pcg_p_kernel(int64_t n, const PcgScalars *s, float *__restrict__ p, const float *__restrict__ z)
+{
+    if (s->done) return;
+    const float beta = s->rz_new / s->rz;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = hbd::add(hbd::mul(beta, p[i]), z[i]);
+}
+
+__global__ void pcg_roll_kernel(PcgScalars *s)
+{
+    if (!s->done) s->rz = s->rz_new;
+}
+
+inline unsigned ewb(hb_context *ctx, int64_t n)
+{
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 8));
+}
+
+// One PCG iteration: v = A p; pv = p.v; x, r update; rr = r.r; check; z = M(r); rz_new = r.z;
+// p = beta p + z; rz = rz_new.
+int pcg_iteration(hb_mg *mg, float *x, float *r, float *z, float *p, float *v, PcgScalars *s)
+{
+    hb_context *ctx = mg->ctx;
+    const hb_ell *A = &mg->A[mg->L - 1];
+    const int64_t n = A->rows;
+    HB_TRY(hb_launch_spmv_mode<float>(ctx, A, HB_MODE_SPMV, p, nullptr, nullptr, v));
+    HB_TRY(hb_launch_dot<float>(ctx, n, p, v, &s->pv));
+    pcg_xr_kernel<<<ewb(ctx, n), 256, 0, ctx->stream>>>(n, s, x, r, p, v);
+    HB_TRY(hb_check_launch(ctx, "pcg_xr_kernel"));
+    HB_TRY(hb_launch_dot<float>(ctx, n, r, r, &s->rr));
+    pcg_check_kernel<<<1, 1, 0, ctx->stream>>>(s);
+    HB_TRY(hb_check_launch(ctx, "pcg_check_kernel"));
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(z, 0, sizeof(float) * n, ctx->stream));
+    HB_TRY(vcycle<float>(mg, mg->L - 1, z, r));
+    HB_TRY(hb_launch_dot<float>(ctx, n, r, z, &s->rz_new));
+    pcg_p_kernel<<<ewb(ctx, n), 256, 0, ctx->stream>>>(n, s, p, z);
+    HB_TRY(hb_check_launch(ctx, "pcg_p_kernel"));
+    pcg_roll_kernel<<<1, 1, 0, ctx->stream>>>(s);
+    return hb_check_launch(ctx, "pcg_roll_kernel");
+}
+
+}  // namespace
+
+// PCG on the finest level of an FP32 hierarchy with device scalars.  work: 4 padded vectors
+// (r, z, p, v) + one PcgScalars slot (16 floats).  graph (optional, in/out): a captured
+// iteration for this (mg, work, x) triple, reused across calls.  check_every: iterations per
+// host check of the done flag.
+int hb_mg_pcg_f32_graph(hb_mg *mg, cudaStream_t capture_stream, const float *b, float *x, float eps, int64_t max_iters,
+                        float *work, cudaGraphExec_t *graph, int check_every, int64_t *used)
+{
+    hb_context *ctx = mg->ctx;
+    const int top = mg->L - 1;
+    const int64_t n = mg->A[top].rows;
+    const int64_t ldn = (int64_t)pad_entries(n);
+    float *r = work, *z = work + ldn, *p = work + 2 * ldn, *v = work + 3 * ldn;
+    PcgScalars *s = reinterpret_cast<PcgScalars *>(work + 4 * ldn);
+    // start: x = 0, r = b, rr = r.r, z = M(r), p = z, rz = r.z
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(x, 0, sizeof(float) * n, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(r, b, sizeof(float) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    HB_TRY(hb_launch_dot<float>(ctx, n, r, r, &s->rr));
+    pcg_start_kernel<<<1, 1, 0, ctx->stream>>>(s, eps);
+    HB_TRY(hb_check_launch(ctx, "pcg_start_kernel"));
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(z, 0, sizeof(float) * n, ctx->stream));
+    HB_TRY(vcycle<float>(mg, top, z, r));
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(p, z, sizeof(float) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    HB_TRY(hb_launch_dot<float>(ctx, n, r, z, &s->rz));
+    if (graph && !*graph && capture_stream) {
+        // capture one iteration on the capture stream (ordered after the start work)
+        cudaEvent_t ev;
+        HB_CUDA_TRY(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        cudaStream_t saved = ctx->stream;
+        cudaEventRecord(ev, saved);
+        cudaStreamWaitEvent(capture_stream, ev, 0);
+        cudaEventDestroy(ev);
+        ctx->stream = capture_stream;
+        cudaGraph_t g = nullptr;
+        int st = HB_OK;
+        if (cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) st = HB_ERR_CUDA;
+        if (!st) st = pcg_iteration(mg, x, r, z, p, v, s);
+        cudaError_t e = cudaStreamEndCapture(capture_stream, &g);
+        if (!st && e != cudaSuccess) st = HB_ERR_CUDA;
+        ctx->stream = saved;
+        if (!st && cudaGraphInstantiate(graph, g, 0) != cudaSuccess) st = HB_ERR_CUDA;
+        if (g) cudaGraphDestroy(g);
+        if (st) { cudaGetLastError(); *graph = nullptr; return st; }
+    }
+    PcgScalars *h = static_cast<PcgScalars *>(ctx->pinned);
+    int64_t launched = 0;
+    const int every = std::max(1, check_every);
+    while (launched < max_iters) {
+        const int64_t k = std::min<int64_t>(every, max_iters - launched);
+        for (int64_t i = 0; i < k; ++i) {
+            if (graph && *graph) {
+                HB_CUDA_TRY(ctx, cudaGraphLaunch(*graph, ctx->stream));
+            } else {
+                HB_TRY(pcg_iteration(mg, x, r, z, p, v, s));
+            }
+        }
+        launched += k;
+        HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, ctx->stream));
+        HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        if (h->done) break;
+    }
+    if (used) *used = h->it;
+    return HB_OK;
+}
+
+namespace {
 
 template <typename T> int jacobi_init(hb_mg *mg)
 {
@@ -221,7 +468,7 @@ int hb_mg_create(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *pr
     entries += 64;                                     // norm scalar
     size_t bytes = entries * es + 256 /* cg result */;
     if (dt == HB_F32) bytes += pad_entries(nf) * (8 + 4 + 4);   // IR: r64, b32, x32
-    if (cudaMalloc(&mg->mem, bytes) != cudaSuccess) {
+    if (cudaMallocAsync(&mg->mem, bytes, ctx->stream) != cudaSuccess) {
         cudaGetLastError();
         delete mg;
         return HB_ERR_ALLOC;
@@ -248,7 +495,7 @@ int hb_mg_create(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *pr
     int st = cudaMemsetAsync(mg->mem, 0, bytes, ctx->stream) == cudaSuccess ? HB_OK : HB_ERR_CUDA;
     if (!st) st = dt == HB_F64 ? jacobi_init<double>(mg) : jacobi_init<float>(mg);
     if (st) {
-        cudaFree(mg->mem);
+        cudaFreeAsync(mg->mem, ctx->stream);
         delete mg;
         return st;
     }
@@ -259,8 +506,8 @@ int hb_mg_create(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *pr
 int hb_mg_destroy(hb_mg *mg)
 {
     if (!mg) return HB_ERR_INVALID;
-    cudaStreamSynchronize(mg->ctx->stream);
-    cudaFree(mg->mem);
+    // stream-ordered: the memory returns to the pool once the stream's queued work is done
+    cudaFreeAsync(mg->mem, mg->ctx->stream);
     delete mg;
     return HB_OK;
 }

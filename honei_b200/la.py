@@ -102,6 +102,23 @@ def _vec(t: torch.Tensor, dtype, name: str) -> int:
     return t.data_ptr()
 
 
+class _DeviceArray:
+    """__cuda_array_interface__ view of device memory owned elsewhere (zero copy)."""
+
+    _TYPESTR = {torch.float64: "<f8", torch.float32: "<f4", torch.int32: "<i4"}
+
+    def __init__(self, ptr, n, dtype):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": self._TYPESTR[dtype],
+                                         "data": (int(ptr), False), "version": 2, "strides": None}
+
+
+def _wrap_device(ptr, n, dtype):
+    """A torch view of n elements of device memory owned elsewhere (the owner keeps it alive)."""
+    if n == 0 or not ptr:
+        return torch.empty(0, dtype=dtype, device="cuda")
+    return torch.as_tensor(_DeviceArray(ptr, n, dtype), device="cuda")
+
+
 class SparseMatrixELL:
     """Device mirror of a HONEI SparseMatrixELL (honei/la/sparse_matrix_ell.hh:44-129)."""
 
@@ -164,6 +181,29 @@ class SparseMatrixELL:
         check(lib().hb_q1_assemble_f64(ctx.handle, M, cptr, int(symmetric), C.byref(out)), "hb_q1_assemble_f64",
               ctx.handle)
         return cls(N, N, K, ld, Aj, Ax)
+
+    @classmethod
+    def from_struct(cls, e: HbEll) -> "SparseMatrixELL":
+        """Wraps device arrays described by an hb_ell (no copy; the owner keeps them alive)."""
+        n = int(e.K * e.ld)
+        dt = torch.float64 if e.dtype == 0 else torch.float32
+        Aj = _wrap_device(e.Aj, n, torch.int32)
+        Ax = _wrap_device(e.Ax, n, dt)
+        return cls(e.rows, e.cols, e.K, e.ld, Aj, Ax)
+
+    def to_host(self):
+        """The matrix in the reference layout (problems.EllMatrix, one lane per row): the
+        valid slots of every row in slot order."""
+        from . import problems as P
+        torch.cuda.synchronize()
+        Aj = self.Aj.cpu().numpy().reshape(self.K, self.ld)[:, : self._rows]
+        Ax = self.Ax.cpu().numpy().reshape(self.K, self.ld)[:, : self._rows]
+        valid = Aj.T >= 0
+        counts = valid.sum(axis=1)
+        indptr = np.zeros(self._rows + 1, np.int64)
+        np.cumsum(counts, out=indptr[1:])
+        dtype = np.float64 if self.dtype == torch.float64 else np.float32
+        return P.ell_from_csr(self._rows, self._cols, indptr, Aj.T[valid].astype(np.int64), Ax.T[valid], 1, dtype)
 
     def to_float(self, ctx: Context | None = None) -> "SparseMatrixELL":
         """Same pattern with FP32 values (the reference fills FP32 matrices from FP64 values)."""
@@ -469,3 +509,66 @@ class IRSolver:
                                    _vec(x, torch.float64, "x"), eps, inner_eps, inner_max_iters, max_iters,
                                    C.byref(used), C.byref(inner), rn), "IRSolver", ctx.handle)
         return used.value, rn[0], rn[1], inner.value
+
+
+class Q1System:
+    """A served SPD Q1 system (hb_q1): FP64 matrix, FP32 copy and the device-built FP32 MG
+    hierarchy (bilinear transfers, Galerkin levels) for a grid of any side.
+
+        q = Q1System(M, coef)                        # coef: CUDA float64 (M-1)^2 or None
+        info = q.solve(b, x, eps=1e-8)               # IR + FP32 MG-preconditioned CG
+    """
+
+    def __init__(self, M: int, coef: torch.Tensor | None = None, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self.M = int(M)
+        cptr = None
+        if coef is not None:
+            if coef.numel() != (M - 1) * (M - 1):
+                raise VectorSizeDoesNotMatch(coef.numel(), (M - 1) * (M - 1))
+            cptr = _vec(coef, torch.float64, "coef")
+        h = C.c_void_p()
+        check(lib().hb_q1_create(self.ctx.handle, self.M, cptr, C.byref(h)), "hb_q1_create", self.ctx.handle)
+        self.handle = h
+        nl = C.c_int(0)
+        sides = (C.c_int64 * 64)()
+        check(lib().hb_q1_levels(h, C.byref(nl), sides), "hb_q1_levels")
+        self.sides = [sides[i] for i in range(nl.value)]
+
+    def level(self, l: int):
+        """(A64, A32, P32, R32) device views of level l (P/R None on the finest level)."""
+        e = [HbEll() for _ in range(4)]
+        check(lib().hb_q1_level(self.handle, l, *[C.byref(x) for x in e]), "hb_q1_level")
+        A64, A32 = SparseMatrixELL.from_struct(e[0]), SparseMatrixELL.from_struct(e[1])
+        if l + 1 < len(self.sides):
+            return A64, A32, SparseMatrixELL.from_struct(e[2]), SparseMatrixELL.from_struct(e[3])
+        return A64, A32, None, None
+
+    @property
+    def A(self) -> SparseMatrixELL:
+        return self.level(len(self.sides) - 1)[0]
+
+    def solve(self, b: torch.Tensor, x: torch.Tensor, eps=1e-8, inner_eps=1e-3, max_outer=50, max_inner=1000):
+        n = self.M * self.M
+        if b.numel() != n:
+            raise VectorSizeDoesNotMatch(b.numel(), n)
+        if x.numel() != n:
+            raise VectorSizeDoesNotMatch(x.numel(), n)
+        from .batch import HbBatchResult
+        info = HbBatchResult()
+        self.ctx.bind_stream()
+        check(lib().hb_q1_solve(self.handle, _vec(b, torch.float64, "b"), _vec(x, torch.float64, "x"), eps,
+                                inner_eps, max_outer, max_inner, C.byref(info)), "hb_q1_solve", self.ctx.handle)
+        return dict(iterations=info.iterations, outer=info.outer, defect0=info.defect0, defect=info.defect,
+                    true_relres=info.true_relres, status=info.status)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().hb_q1_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass

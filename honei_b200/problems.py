@@ -209,42 +209,47 @@ def q1_poisson_permuted(M: int, seed: int, coef=None, threads: int = 1, dtype=np
     return (A if dtype == np.float64 else A.astype(dtype)), perm
 
 
-def prolongation_csr(Mc: int):
-    """Bilinear Q1 prolongation from an Mc x Mc to a (2Mc-1)^2 grid, fine Dirichlet rows zero."""
-    Mc = int(Mc)
-    Mf = 2 * Mc - 1
-    Nf = Mf * Mf
-    I, J = np.divmod(np.arange(Nf, dtype=np.int64), Mf)
-    bnd = (I == 0) | (I == Mf - 1) | (J == 0) | (J == Mf - 1)
+def coarse_side(M: int) -> int:
+    """Side of the next coarser grid: the fine nodes with even index, plus the last node when
+    M is even (then the last coarse interval spans one fine interval)."""
+    return int(M) // 2 + 1
+
+
+def _interp_1d(i: int, Mf: int):
+    """1-D bilinear interpolation of fine coordinate i: list of (coarse index, weight)."""
+    Mc = coarse_side(Mf)
+    ci = lambda k: Mc - 1 if k == Mf - 1 else k // 2  # noqa: E731
+    if i % 2 == 0 or i == Mf - 1:
+        return [(ci(i), 1.0)]
+    return [(ci(i - 1), 0.5), (ci(i + 1), 0.5)]
+
+
+def prolongation_csr(Mc: int = None, Mf: int = None):
+    """Bilinear Q1 prolongation to an Mf x Mf grid from its coarse grid (coarse_side(Mf)), fine
+    Dirichlet rows zero.  Pass Mc (odd grids, Mf = 2 Mc - 1) or Mf (any side >= 3)."""
+    if Mf is None:
+        Mf = 2 * int(Mc) - 1
+    Mf = int(Mf)
+    Mc = coarse_side(Mf)
+    tab = [_interp_1d(i, Mf) for i in range(Mf)]
     rows, cols, vals = [], [], []
-    ie, je = (I % 2 == 0), (J % 2 == 0)
-    ci0, cj0 = I // 2, J // 2
-    ci1, cj1 = (I + 1) // 2, (J + 1) // 2
-
-    def add(mask, ci, cj, w):
-        m = mask & ~bnd
-        r = np.nonzero(m)[0]
-        rows.append(r)
-        cols.append(ci[m] * Mc + cj[m])
-        vals.append(np.full(len(r), w))
-
-    add(ie & je, ci0, cj0, 1.0)
-    add(ie & ~je, ci0, cj0, 0.5)
-    add(ie & ~je, ci0, cj1, 0.5)
-    add(~ie & je, ci0, cj0, 0.5)
-    add(~ie & je, ci1, cj0, 0.5)
-    add(~ie & ~je, ci0, cj0, 0.25)
-    add(~ie & ~je, ci0, cj1, 0.25)
-    add(~ie & ~je, ci1, cj0, 0.25)
-    add(~ie & ~je, ci1, cj1, 0.25)
-    r = np.concatenate(rows)
-    c = np.concatenate(cols)
-    v = np.concatenate(vals)
+    for I in range(1, Mf - 1):
+        for J in range(1, Mf - 1):
+            f = I * Mf + J
+            for ca, wa in tab[I]:
+                for cb, wb in tab[J]:
+                    rows.append(f)
+                    cols.append(ca * Mc + cb)
+                    vals.append(wa * wb)
+    Nf, Nc = Mf * Mf, Mc * Mc
+    r = np.asarray(rows, np.int64)
+    c = np.asarray(cols, np.int64)
+    v = np.asarray(vals, np.float64)
     order = np.lexsort((c, r))
     r, c, v = r[order], c[order], v[order]
     indptr = np.zeros(Nf + 1, np.int64)
     np.cumsum(np.bincount(r, minlength=Nf), out=indptr[1:])
-    return Nf, Mc * Mc, indptr, c, v
+    return Nf, Nc, indptr, c, v
 
 
 def transpose_csr(rows: int, cols: int, indptr, indices, data):
@@ -282,6 +287,11 @@ def galerkin_csr(A: EllMatrix, prol: EllMatrix, res: EllMatrix):
 
     Ac = (csr(res) @ csr(A) @ csr(prol)).tocsr()
     Ac.eliminate_zeros()
+    # coarse nodes no fine interior node interpolates from (the last line of an even-sided
+    # grid) have empty rows and columns: they get identity rows (their correction is zero)
+    dead = np.nonzero(np.diff(Ac.indptr) == 0)[0]
+    if len(dead):
+        Ac = (Ac + sp.csr_matrix((np.ones(len(dead)), (dead, dead)), shape=Ac.shape)).tocsr()
     Ac.sort_indices()
     return Ac.shape[0], Ac.indptr.astype(np.int64), Ac.indices.astype(np.int64), Ac.data
 
@@ -301,18 +311,18 @@ def mg_hierarchy(M: int, coarsest: int = 9, coef=None, threads: int = 1, coarse:
         raise ValueError(coarse)
     sides = [int(M)]
     while sides[-1] > coarsest:
-        if (sides[-1] - 1) % 2:
-            raise ValueError(f"grid side {sides[-1]} cannot be coarsened (need 2^k + 1)")
-        sides.append((sides[-1] + 1) // 2)
+        sides.append(coarse_side(sides[-1]))
     sides = sides[::-1]
     coefs = [None] * len(sides)
     if coef is not None:
+        if coarse == "rediscretize" and any((s - 1) % 2 for s in sides[1:]):
+            raise ValueError("rediscretised coefficient levels need sides 2^k + 1")
         coefs[-1] = np.asarray(coef, np.float64)
         for l in range(len(sides) - 2, -1, -1):
-            coefs[l] = coarsen_coef(coefs[l + 1])
+            coefs[l] = coarsen_coef(coefs[l + 1]) if coarse == "rediscretize" else None
     prol, res = [], []
     for l in range(len(sides) - 1):
-        nf, nc, ip, ix, dv = prolongation_csr(sides[l])
+        nf, nc, ip, ix, dv = prolongation_csr(Mf=sides[l + 1])
         prol.append(ell_from_csr(nf, nc, ip, ix, dv, threads))
         t_ip, t_ix, t_dv = transpose_csr(nf, nc, ip, ix, dv)
         res.append(ell_from_csr(nc, nf, t_ip, t_ix, t_dv, threads))

@@ -302,6 +302,38 @@ int hb_batch_results(hb_context *ctx, int64_t count, void *workspace, hb_batch_r
 int hb_batch_tune(hb_context *ctx, const hb_batch_system *sys, int64_t count, void *workspace,
                   hb_batch_config *best, double *times_ms);
 
+/* ------------------------------------------------------------------------------------------
+ * Served Q1 systems: device-built multigrid for grids of ANY side (no reference counterpart;
+ * the reference's MG needs pre-built files per level, honei/math/mg.hh:442-547).
+ * Coarsening keeps the even-indexed fine nodes plus the last one (coarse side Mf/2 + 1);
+ * transfers are Prolongation<methods::NONE>'s bilinear interpolation with fine Dirichlet rows
+ * zeroed (honei/math/prolongation.hh:42-139) and its transpose; coarse operators are Galerkin
+ * R A P (robust for jumping coefficients), coarse nodes without fine support get identity rows.
+ * ---------------------------------------------------------------------------------------- */
+/* Coarse side of an Mf x Mf grid. */
+int hb_q1_coarse_side(int64_t Mf);
+/* P (Nf x Nc, K = 4) and R = P^T (Nc x Nf, K = 9) for an Mf grid, FP64 or FP32 (P->dtype),
+ * preallocated with hb_ell_layout. */
+int hb_q1_transfers(hb_context *ctx, int64_t Mf, hb_ell *P, hb_ell *R);
+/* Galerkin coarse operator Ac = R Af P (FP64, K = 9) of a Q1-structured fine matrix. */
+int hb_q1_galerkin(hb_context *ctx, int64_t Mf, const hb_ell *Af, hb_ell *Ac);
+
+typedef struct hb_q1 hb_q1;
+/* Builds the SPD Q1 system of an M x M grid (coef: device (M-1)^2 cell coefficients or NULL)
+ * with its FP32 MG hierarchy, all device-resident (stream-ordered memory on ctx's stream). */
+int hb_q1_create(hb_context *ctx, int64_t M, const double *coef, hb_q1 **out);
+int hb_q1_destroy(hb_q1 *q);
+int hb_q1_levels(const hb_q1 *q, int *nlevels, int64_t *sides);
+/* Level matrices (level 0 = coarsest): FP64 A, FP32 A (shares A64's index array), and the
+ * FP32 transfers from this level to the next finer one (levels below the finest only). */
+int hb_q1_level(const hb_q1 *q, int level, hb_ell *A64, hb_ell *A32, hb_ell *P32, hb_ell *R32);
+/* Mixed-precision solve: FP64 defect, norm and update around FP32 CG preconditioned by one
+ * V(2,2) cycle (damped Jacobi 0.7, coarse CG), on the normalised defect to inner_eps, until
+ * ||b - A x|| < eps ||b - A x0||.  info: iterations = summed inner PCG iterations, outer,
+ * defect0/defect = FP64 defect norms, true_relres = ||b - A x|| / ||b||. */
+int hb_q1_solve(hb_q1 *q, const double *b, double *x, double eps, double inner_eps, int64_t max_outer,
+                int64_t max_inner, hb_batch_result *info);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -72,6 +72,8 @@ class Oracle:
                                 _c.c_int, _c.POINTER(_u64), _vp]
         L.ora_ir_cg.argtypes = [_vp, _vp, _vp, _vp, _c.c_double, _c.c_float, _u64, _u64,
                                 _c.POINTER(_u64), _c.POINTER(_u64), _vp]
+        L.ora_ir_pcg.argtypes = [_vp, _vp, _c.c_float, _vp, _vp, _c.c_double, _c.c_float, _u64, _u64,
+                                 _c.POINTER(_u64), _c.POINTER(_u64), _vp]
         for n in ("ora_scaled_sum_f64", "ora_scale_f64"):
             getattr(L, n).argtypes = [_u64, _vp, _vp, _c.c_double] if n == "ora_scaled_sum_f64" \
                 else [_u64, _vp, _c.c_double]
@@ -154,6 +156,19 @@ class Oracle:
         self.lib.ora_ir_mg(_c.byref(e), _c.byref(mg), damping, _ptr(b), _ptr(x), eps, inner_eps,
                            max_iters, int(warm_start), _c.byref(used), _ptr(hist))
         return x, used.value, hist[: used.value + 1]
+
+    def ir_pcg(self, A64, H32, b, x0=None, eps=1e-8, inner_eps=1e-3, max_outer=50, max_inner=1000,
+               damping=0.7):
+        """IR + FP32 MG-preconditioned CG (V(2,2), coarse CG 200 iterations, eps 1e-6)."""
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(A64.rows) if x0 is None else np.array(x0, np.float64)
+        mg = self._mg_struct(H32, 1, 200, 2, 2)
+        outer, inner = _u64(0), _u64(0)
+        hist = np.zeros(max_outer + 2)
+        e = _ell(A64)
+        self.lib.ora_ir_pcg(_c.byref(e), _c.byref(mg), damping, _ptr(b), _ptr(x), eps, inner_eps, max_outer,
+                            max_inner, _c.byref(outer), _c.byref(inner), _ptr(hist))
+        return x, outer.value, inner.value, hist[: outer.value + 1]
 
     def ir_cg(self, A64, A32, b, x0=None, eps=1e-10, inner_eps=1e-3, inner_max_iters=100000,
               max_iters=100):

@@ -304,3 +304,100 @@ int ora_ir_cg(const ora_ell *A64, const ora_ell *A32, const double *b, double *x
     free(r); free(bi); free(xi);
     return 0;
 }
+
+/* ---------------------------------------------------------------------------------------
+ * IR around an FP32 CG preconditioned by one V-cycle (the served mixed-precision solve of
+ * hb_q1_solve; no reference counterpart).  Outer loop as ora_ir_mg's scaled mode; inner PCG
+ * from x = 0 on the normalised defect until |r| < inner_eps |r0|:
+ *   z = M(r); p = z; rz = r.z; loop { v = A p; a = rz / p.v; x += a p; r -= a v;
+ *   stop if |r| < eps |r0|; z = M(r); beta = r.z_new / rz; p = beta p + z }
+ * M = one V-cycle of ora_vcycle_f32 from z = 0.
+ * ------------------------------------------------------------------------------------- */
+static int ora_pcg_f32(mgws_f32 *w, const float *b, float *x, float eps, uint64_t max_iters, uint64_t *used)
+{
+    const ora_mg *mg = w->mg;
+    const int top = mg->nlevels - 1;
+    const ora_ell *A = &mg->A[top];
+    const uint64_t n = A->rows;
+    float *r = (float *)calloc(n ? n : 1, 4), *z = (float *)calloc(n ? n : 1, 4);
+    float *p = (float *)calloc(n ? n : 1, 4), *v = (float *)calloc(n ? n : 1, 4);
+    memset(x, 0, sizeof(float) * n);
+    memcpy(r, b, sizeof(float) * n);
+    const float r0 = sqrtf(ora_dot_f32(n, r, r));
+    uint64_t it = 0;
+    if (r0 > 0.f && max_iters > 0) {
+        memset(z, 0, sizeof(float) * n);
+        ora_vcycle_f32(w, top, z, r);
+        memcpy(p, z, sizeof(float) * n);
+        float rz = ora_dot_f32(n, r, z);
+        while (it < max_iters) {
+            ora_spmv_f32(A, p, v);
+            const float pv = ora_dot_f32(n, p, v);
+            if (!(pv > 0.f)) break;
+            const float a = rz / pv;
+            for (uint64_t i = 0; i < n; ++i) x[i] += a * p[i];
+            const float ma = -a;
+            for (uint64_t i = 0; i < n; ++i) r[i] += ma * v[i];
+            ++it;
+            if (sqrtf(ora_dot_f32(n, r, r)) < eps * r0) break;
+            memset(z, 0, sizeof(float) * n);
+            ora_vcycle_f32(w, top, z, r);
+            const float rz_new = ora_dot_f32(n, r, z);
+            const float beta = rz_new / rz;
+            rz = rz_new;
+            for (uint64_t i = 0; i < n; ++i) p[i] = beta * p[i] + z[i];
+        }
+    }
+    *used = it;
+    free(r); free(z); free(p); free(v);
+    return 0;
+}
+
+int ora_ir_pcg(const ora_ell *A64, const ora_mg *mg32, float damping, const double *b, double *x, double eps,
+               float inner_eps, uint64_t max_outer, uint64_t max_inner, uint64_t *outer_out, uint64_t *inner_total,
+               double *rnorm_hist)
+{
+    const int L = mg32->nlevels;
+    mgws_f32 w;
+    w.mg = mg32; w.eps = (float)1e-6; w.used_coarse = 0;
+    float ***arrs[] = { &w.P, &w.d, &w.c, &w.store, &w.t0, &w.t1 };
+    for (int a = 0; a < 6; ++a) {
+        *arrs[a] = (float **)calloc(L, sizeof(float *));
+        for (int l = 0; l < L; ++l)
+            (*arrs[a])[l] = (float *)calloc(mg32->A[l].rows ? mg32->A[l].rows : 1, sizeof(float));
+    }
+    for (int l = 0; l < L; ++l)
+        for (uint64_t i = 0; i < mg32->A[l].rows; ++i) {
+            float pv = damping;
+            pv /= ora_diag_f32(&mg32->A[l], i);
+            w.P[l][i] = pv;
+        }
+    const uint64_t n = A64->rows;
+    double *r = (double *)calloc(n ? n : 1, 8);
+    float *bi = (float *)calloc(n ? n : 1, 4), *xi = (float *)calloc(n ? n : 1, 4);
+    double nrm0 = 0.0, nrm = 0.0;
+    uint64_t outer = 0, total = 0;
+    for (;;) {
+        ora_defect_f64(A64, b, x, r);
+        nrm = sqrt(ora_dot_f64(n, r, r));
+        if (rnorm_hist) rnorm_hist[outer] = nrm;
+        if (outer == 0) nrm0 = nrm;
+        else if (nrm < eps * nrm0) break;
+        if (nrm == 0.0 || outer >= max_outer) break;
+        const double s = 1.0 / nrm;
+        for (uint64_t k = 0; k < n; ++k) bi[k] = (float)(r[k] * s);
+        uint64_t used = 0;
+        ora_pcg_f32(&w, bi, xi, inner_eps, max_inner, &used);
+        total += used;
+        for (uint64_t k = 0; k < n; ++k) x[k] += nrm * (double)xi[k];
+        ++outer;
+    }
+    *outer_out = outer;
+    if (inner_total) *inner_total = total;
+    free(r); free(bi); free(xi);
+    for (int a = 0; a < 6; ++a) {
+        for (int l = 0; l < L; ++l) free((*arrs[a])[l]);
+        free(*arrs[a]);
+    }
+    return 0;
+}

@@ -78,6 +78,13 @@ int ora_ir_cg(const ora_ell *A64, const ora_ell *A32, const double *b, double *x
               float inner_eps, uint64_t inner_max_iters, uint64_t max_iters, uint64_t *used,
               uint64_t *inner_total, double *rnorm_hist);
 
+/* IR (scaled mode) around FP32 CG preconditioned by one V-cycle of mg32 from zero (coarse CG
+ * eps 1e-6): the served mixed-precision solve.  *outer_out = outer steps, *inner_total = summed
+ * PCG iterations, rnorm_hist[k] = FP64 defect norm before outer step k. */
+int ora_ir_pcg(const ora_ell *A64, const ora_mg *mg32, float damping, const double *b, double *x, double eps,
+               float inner_eps, uint64_t max_outer, uint64_t max_inner, uint64_t *outer_out, uint64_t *inner_total,
+               double *rnorm_hist);
+
 #ifdef __cplusplus
 }
 #endif
