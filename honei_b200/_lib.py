@@ -103,6 +103,14 @@ SIGNATURES = {
     "hb_q1_levels": (i32, [vp, C.POINTER(i32), P_i64]),
     "hb_q1_level": (i32, [vp, i32, P_ell, P_ell, P_ell, P_ell]),
     "hb_q1_solve": (i32, [vp, vp, vp, f64, f64, i64, i64, vp]),
+    # serving loop
+    "hb_server_create": (i32, [vp, C.POINTER(vp)]),
+    "hb_server_submit": (i32, [vp, vp]),
+    "hb_server_poll": (i32, [vp, vp, i32, C.POINTER(i32), i32]),
+    "hb_server_drain": (i32, [vp]),
+    "hb_server_clock": (f64, [vp]),
+    "hb_server_stats": (i32, [vp, P_i64, P_i64, P_i64, P_i64]),
+    "hb_server_destroy": (i32, [vp]),
 }
 
 

@@ -40,7 +40,7 @@ class HbBatchResult(C.Structure):
 
 
 class HbBatchConfig(C.Structure):
-    _fields_ = [("cluster", C.c_int32), ("threads", C.c_int32)]
+    _fields_ = [("cluster", C.c_int32), ("threads", C.c_int32), ("max_clusters", C.c_int32)]
 
 
 def _register():

@@ -330,7 +330,7 @@ int check_system(const hb_batch_system &s)
     return HB_OK;
 }
 
-template <int THREADS> int launch_batch(hb_context *ctx, int cluster, int64_t count, void *ws)
+template <int THREADS> int launch_batch(hb_context *ctx, int cluster, int max_clusters, int64_t count, void *ws)
 {
     auto kern = batch_kernel<THREADS>;
     if (cluster > 8) {
@@ -349,13 +349,14 @@ template <int THREADS> int launch_batch(hb_context *ctx, int cluster, int64_t co
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cfg.gridDim = dim3(cluster);
-    int max_clusters = 0;
-    cudaError_t e = cudaOccupancyMaxActiveClusters(&max_clusters, kern, &cfg);
-    if (e != cudaSuccess || max_clusters < 1) {
+    int max_active = 0;
+    cudaError_t e = cudaOccupancyMaxActiveClusters(&max_active, kern, &cfg);
+    if (e != cudaSuccess || max_active < 1) {
         hb_note_error(ctx, e == cudaSuccess ? cudaErrorInvalidConfiguration : e, "cudaOccupancyMaxActiveClusters");
         return HB_ERR_UNSUPPORTED;
     }
-    const int64_t clusters = std::max<int64_t>(1, std::min<int64_t>(max_clusters, count));
+    if (max_clusters > 0) max_active = std::min(max_active, max_clusters);
+    const int64_t clusters = std::max<int64_t>(1, std::min<int64_t>(max_active, count));
     cfg.gridDim = dim3((unsigned)(clusters * cluster));
     const BatchDesc *descs = (const BatchDesc *)((char *)ws + 256);
     unsigned long long *counter = (unsigned long long *)ws;
@@ -435,10 +436,11 @@ int hb_batch_run(hb_context *ctx, int64_t count, void *ws, const hb_batch_config
     if (count == 0) return HB_OK;
     const int cluster = cfg ? cfg->cluster : 4;
     const int threads = cfg ? cfg->threads : 512;
+    const int max_clusters = cfg ? cfg->max_clusters : 0;
     if (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8 && cluster != 16) return HB_ERR_INVALID;
     HB_CUDA_TRY(ctx, cudaMemsetAsync(ws, 0, 256, ctx->stream));
-    if (threads == 256) return launch_batch<256>(ctx, cluster, count, ws);
-    if (threads == 512) return launch_batch<512>(ctx, cluster, count, ws);
+    if (threads == 256) return launch_batch<256>(ctx, cluster, max_clusters, count, ws);
+    if (threads == 512) return launch_batch<512>(ctx, cluster, max_clusters, count, ws);
     return HB_ERR_INVALID;
 }
 
@@ -478,7 +480,7 @@ int hb_batch_tune(hb_context *ctx, const hb_batch_system *sys, int64_t count, vo
     int k = 0;
     for (int c : clusters)
         for (int t : threads) {
-            hb_batch_config cfg{c, t};
+            hb_batch_config cfg{c, t, 0};
             float ms = -1.f;
             // warm-up then one timed run, every run from x = 0
             st = zero_x(ctx, sys, count);

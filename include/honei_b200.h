@@ -279,6 +279,8 @@ typedef struct {
 typedef struct {
     int32_t cluster;           /* CTAs per system: 1, 2, 4, 8 or 16                        */
     int32_t threads;           /* threads per CTA: 256 or 512                              */
+    int32_t max_clusters;      /* cap on resident clusters (0 = all that fit): leaves SMs
+                                  to concurrent work on other streams                      */
 } hb_batch_config;
 
 /* Device workspace bytes for these systems (work vectors, descriptors, results, counter). */
@@ -333,6 +335,66 @@ int hb_q1_level(const hb_q1 *q, int level, hb_ell *A64, hb_ell *A32, hb_ell *P32
  * defect0/defect = FP64 defect norms, true_relres = ||b - A x|| / ||b||. */
 int hb_q1_solve(hb_q1 *q, const double *b, double *x, double eps, double inner_eps, int64_t max_outer,
                 int64_t max_inner, hb_batch_result *info);
+
+/* ------------------------------------------------------------------------------------------
+ * Serving (no reference counterpart): a request loop that admits Q1 solve requests by an HBM
+ * budget, keeps each admitted request's matrix, hierarchy and Krylov state on the device, and
+ * serves them concurrently -- small grids in batched cluster launches (HB_BATCH_IR32), large
+ * grids on MG-preconditioned mixed-precision workers (hb_q1_solve), each on its own stream --
+ * while new requests keep arriving (continuous batching).  A request's result does not depend
+ * on what it was served with.  HB_SERVE_PLAIN_CG64 is the baseline on the same queue: one
+ * request at a time, plain FP64 CG (hb_cg_f64) on the whole GPU.
+ * ---------------------------------------------------------------------------------------- */
+enum { HB_SERVE_MIXED = 0, HB_SERVE_PLAIN_CG64 = 1 };
+enum { HB_PATH_BATCH = 0, HB_PATH_MGPCG = 1, HB_PATH_CG64 = 2 };
+
+typedef struct {
+    int32_t mode;               /* HB_SERVE_MIXED or HB_SERVE_PLAIN_CG64                      */
+    int32_t device;
+    int64_t hbm_budget_bytes;   /* admission limit for resident request state                  */
+    int32_t large_workers;      /* concurrent MG-PCG solves (one stream each)                  */
+    int32_t small_workers;      /* concurrent batched launches (one stream each)               */
+    int64_t small_max_side;     /* grid sides <= this take the batched path                    */
+    int32_t max_batch;          /* systems per batched launch                                  */
+    int32_t pad_;
+    hb_batch_config batch_cfg;  /* cluster shape of the batched launches                       */
+    double eps;                 /* target relative FP64 residual ||b - A x|| / ||b||           */
+    double inner_eps;           /* FP32 inner tolerance per refinement step                    */
+} hb_server_params;
+
+typedef struct {
+    int64_t M;                  /* grid side: an M x M node Q1 system (SPD form)              */
+    const double *coef;         /* host, (M-1)^2 cell coefficients, or NULL for 1              */
+    const double *b;            /* host, M^2 right-hand side, or NULL: b = A x_true            */
+    const double *x_true;       /* host, M^2, used when b == NULL                              */
+    double *x;                  /* host, M^2: receives the solution (kept alive by the caller) */
+    uint64_t tag;               /* returned in the completion                                  */
+} hb_request;
+
+typedef struct {
+    uint64_t tag;
+    int32_t status;             /* hb_status                                                   */
+    int32_t path;               /* HB_PATH_*                                                   */
+    int64_t iterations;         /* CG / inner PCG iterations                                   */
+    int64_t outer;              /* refinement steps                                            */
+    double true_relres;         /* ||b - A x|| / ||b|| in FP64                                  */
+    double t_submit, t_admit, t_done;   /* seconds on the server clock                       */
+    int64_t bytes;              /* HBM charged to the request while resident                   */
+} hb_completion;
+
+typedef struct hb_server hb_server;
+int hb_server_create(const hb_server_params *params, hb_server **out);
+/* Queues a request (non-blocking); the host arrays must stay valid until its completion. */
+int hb_server_submit(hb_server *s, const hb_request *req);
+/* Up to max completions (oldest first) into out; waits up to wait_ms for at least one. */
+int hb_server_poll(hb_server *s, hb_completion *out, int max, int *n, int wait_ms);
+/* Blocks until every submitted request has completed. */
+int hb_server_drain(hb_server *s);
+/* Seconds since the server started (the clock of the completion records). */
+double hb_server_clock(hb_server *s);
+/* in_use / peak resident bytes, requests submitted / completed. */
+int hb_server_stats(hb_server *s, int64_t *bytes_in_use, int64_t *bytes_peak, int64_t *submitted, int64_t *completed);
+int hb_server_destroy(hb_server *s);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -1,0 +1,95 @@
+"""The serving loop (hb_server_*): every request of a mixed-size stream reaches the FP64 target,
+a request's solution is the same served alone as served in the mix (bitwise), the plain-FP64-CG
+baseline does what CGSolver does, and admission keeps the resident bytes within the budget."""
+import numpy as np
+import pytest
+
+from honei_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def S():
+    from honei_b200 import serve
+    assert torch.cuda.is_available()
+    return serve
+
+
+def host_relres(oracle, req, x):
+    A = P.q1_poisson(req.M, req.coef.reshape(req.M - 1, req.M - 1), symmetric=True)
+    b = oracle.spmv(A, req.x_true)
+    return np.linalg.norm(oracle.defect(A, b, x)) / np.linalg.norm(b)
+
+
+def test_mixed_stream_reaches_target(S, oracle):
+    trace = S.poisson_trace(24, rate=400.0, side_range=(17, 300), seed=5)
+    with S.Server(mode="mixed", small_max_side=96, large_workers=2) as srv:
+        rep = S.replay(srv, trace)
+    assert rep["completed"] == rep["ok"] == 24
+    assert set(rep["paths"]) == {"batch", "mgpcg"}
+    by_tag = {c.tag: c for c in rep["records"]}
+    for req in trace.requests:
+        c = by_tag[req.tag]
+        rel = host_relres(oracle, req, c.x)
+        assert c.true_relres < 1e-8 and rel < 1e-8, (req.M, c)
+        assert abs(rel - c.true_relres) <= 1e-6 * rel + 1e-14
+        assert np.linalg.norm(c.x - req.x_true) <= 1e-4 * np.linalg.norm(req.x_true)
+
+
+def test_alone_equals_in_the_mix(S):
+    trace = S.poisson_trace(16, rate=0.0, side_range=(17, 200), seed=9)
+    with S.Server(mode="mixed", small_max_side=64, large_workers=3) as srv:
+        mix = {c.tag: c for c in S.replay(srv, trace, realtime=False)["records"]}
+    with S.Server(mode="mixed", small_max_side=64, large_workers=3) as srv:
+        for req in trace.requests:
+            srv.submit(req)
+            (c,) = srv.drain()
+            m = mix[req.tag]
+            assert c.status == m.status == 0 and c.path == m.path
+            assert (c.iterations, c.outer) == (m.iterations, m.outer)
+            assert np.array_equal(c.x, m.x), (req.M, c.path)
+
+
+def test_plain_cg64_matches_cgsolver(S):
+    from honei_b200 import la
+    trace = S.poisson_trace(4, rate=0.0, side_range=(33, 129), seed=2)
+    with S.Server(mode="plain") as srv:
+        rec = {c.tag: c for c in S.replay(srv, trace, realtime=False)["records"]}
+    for req in trace.requests:
+        c = rec[req.tag]
+        assert c.path == "cg64" and c.status == 0 and c.true_relres < 1e-8
+        A = la.SparseMatrixELL.q1_poisson(req.M, torch.from_numpy(req.coef).cuda(), symmetric=True)
+        xt = torch.from_numpy(req.x_true).cuda()
+        b = torch.empty_like(xt)
+        la.Product.value(b, A, xt)
+        x = torch.zeros_like(b)
+        used = la.CGSolver.value(A, None, b, x, 1000000, 1e-8)
+        assert used == c.iterations
+        assert np.array_equal(x.cpu().numpy(), c.x)
+
+
+def test_admission_budget(S):
+    trace = S.poisson_trace(10, rate=0.0, side_range=(150, 260), seed=3)
+    biggest = max((1 << 20) + 320 * r.M * r.M for r in trace.requests)
+    budget = biggest + biggest // 2          # at most one large request resident at a time
+    with S.Server(mode="mixed", budget_bytes=budget, small_max_side=0, large_workers=4) as srv:
+        rep = S.replay(srv, trace, realtime=False)
+        st = srv.stats()
+        with pytest.raises(Exception):
+            srv.submit(S.Request(M=2 * int(np.sqrt(budget / 320)) + 1, x_true=np.zeros(4)))
+    assert rep["ok"] == 10 and st["bytes_in_use"] == 0 and st["bytes_peak"] <= budget
+    # admission kept FIFO order
+    recs = sorted(rep["records"], key=lambda c: c.tag)
+    assert all(a.t_admit <= b.t_admit for a, b in zip(recs, recs[1:]))
+
+
+def test_empty_and_single_node_requests(S):
+    with S.Server(mode="mixed", small_max_side=64) as srv:
+        for tag, M in enumerate((1, 2, 3)):
+            srv.submit(S.Request(M=M, x_true=np.ones(M * M), tag=tag))
+        out = {c.tag: c for c in srv.drain()}
+    for tag, M in enumerate((1, 2, 3)):
+        assert out[tag].status == 0, out[tag]
+        assert np.allclose(out[tag].x, 1.0, rtol=1e-8)
