@@ -11,7 +11,9 @@ from HBM; x (34 MB) is the gathered, L2-resident operand.
 Metric: SpMV GB/s of algorithmic traffic, nnz*(8+4) + 2*n*8 bytes per application (Ax + 32-bit
 Aj once, x read once, y written once), against the measured HBM copy bandwidth.
 Extras on the same line: plain FP64 CG solves/s and p50/p99 latency on the 257^2 system
-(x_true U[-1,1], x0 = 0, relative residual 1e-8), and the FP32 SpMV.
+(x_true U[-1,1], x0 = 0, relative residual 1e-8), the FP32 SpMV, the batched solve of 512
+uneven SPD systems, and a bounded sample of the serving stream (mixed-precision server against
+plain FP64 CG on the same requests: solves/s, p50/p99 latency).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -282,6 +284,161 @@ def bench_cg_cluster(ctx, M=M_CG, n_solves=30):
     return best
 
 
+def _ref_cpu():
+    """The compiled reference (tags::CPU::MultiCore::SSE on every host core), or None."""
+    try:
+        from oracle.bindings import REF_SO, Reference
+        if not os.path.exists(REF_SO):
+            return None
+        R = Reference()
+        R.set_threads(os.cpu_count() or 1)
+        return R
+    except OSError:
+        return None
+
+
+def bench_mg(la, ctx, M=2049, seed=5, cpu=True):
+    """Q1 Poisson M^2 (unit coefficient, the reference's rediscretised hierarchy down to 9^2):
+    MGSolver V(2,2), damped Jacobi 0.7, PROLMAT transfers, coarse CG, x0 = 0, b = A x_true.
+    FP64 to 1e-8 relative; FP32 to 1e-6 (FP32 stagnates near 1e-7).  Plus the FP64 SpMV on the
+    permuted matrix (seeded symmetric row/column permutation) and, when the compiled reference
+    is present, its MultiCore::SSE MG solve of the same FP64 system on the host cores."""
+    import torch
+    from honei_b200 import problems as P
+
+    H = P.mg_hierarchy(M)
+    xt = P.uniform_vector(M * M, seed)
+    out = {"workload": f"MG V(2,2) on Q1 {M}^2, {len(H.sides)} levels, coarse CG on 9^2"}
+    bref = None
+    for name, npdt, tdt, eps in (("f64", np.float64, torch.float64, 1e-8), ("f32", np.float32, torch.float32, 1e-6)):
+        data = la.MGData.from_hierarchy(H, npdt, ctx=ctx, eps=eps, max_iters=100)
+        A = data.A[-1]
+        xtd = torch.from_numpy(xt.astype(npdt)).cuda()
+        b = torch.empty_like(xtd)
+        la.Product.value(b, A, xtd, ctx=ctx)
+        if name == "f64":
+            bref = b.cpu().numpy()
+        x = torch.zeros_like(b)
+        la.MGSolver.value(data, b, x)  # warm-up
+        x.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        cycles, r0, r1 = la.MGSolver.value(data, b, x)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        err = float(torch.linalg.norm((x - xtd).double()) / torch.linalg.norm(xtd.double()))
+        out[name] = {"ms": round(ms, 2), "cycles": cycles, "ms_per_cycle": round(ms / max(cycles, 1), 3),
+                     "relres": r1 / r0 if r0 else 0.0, "eps": eps, "err_vs_x_true": err}
+        data.close()
+        del data, A, b, x, xtd
+        torch.cuda.empty_cache()
+    if cpu:
+        R = _ref_cpu()
+        if R is not None:
+            _, used, sec = R.mg(H, bref, eps=1e-8, tag="mc-sse")
+            out["cpu_reference_f64"] = {"s": round(sec, 3), "cycles": used, "cores": os.cpu_count(),
+                                        "tag": "tags::CPU::MultiCore::SSE"}
+            out["speedup_f64_vs_cpu"] = round(sec * 1e3 / out["f64"]["ms"], 1)
+    # permuted SpMV (stresses the gathers of x)
+    Ap, _ = P.q1_poisson_permuted(M, seed=seed)
+    Ad = la.SparseMatrixELL.from_reference(Ap, ctx)
+    x = torch.from_numpy(P.uniform_vector(M * M, seed + 1)).cuda()
+    y = torch.empty_like(x)
+    for _ in range(3):
+        la.Product.value(y, Ad, x, ctx=ctx)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(50):
+        la.Product.value(y, Ad, x, ctx=ctx)
+    e1.record()
+    torch.cuda.synchronize()
+    out["spmv_permuted_f64_gbs"] = round(spmv_bytes(Ap.nnz, Ap.rows, 8) * 50 / (e0.elapsed_time(e1) / 1e3) / 1e9, 1)
+    return out
+
+
+def bench_ir(la, ctx, M=2049, seed=3):
+    """Mixed precision on Q1 M^2 (SPD form) with a cellwise coefficient 10^U(-2,2): FP64
+    refinement to 1e-10 relative around FP32 inner solves to 1e-3 -- MG-preconditioned CG on the
+    device-built Galerkin hierarchy (hb_q1_solve), and plain FP32 CG (hb_ir_cg_solve) -- each
+    with ||x - x_CG64|| / ||x_CG64|| against plain FP64 CG on the same system run to 1e-12."""
+    import torch
+    from honei_b200 import problems as P
+
+    coef = torch.from_numpy(P.log_uniform_coef(M, 1e-2, 1e2, seed).ravel()).cuda()
+    q = la.Q1System(M, coef, ctx=ctx)
+    A = q.A
+    xt = torch.from_numpy(P.uniform_vector(M * M, seed + 1)).cuda()
+    b = torch.empty_like(xt)
+    la.Product.value(b, A, xt, ctx=ctx)
+    bn = la.Norm.value(b, root=True, ctx=ctx)
+    r = torch.empty_like(b)
+
+    def relres(x):
+        la.Defect.value(r, b, A, x, ctx=ctx)
+        return la.Norm.value(r, root=True, ctx=ctx) / bn
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return res, e0.elapsed_time(e1)
+
+    x64 = torch.zeros_like(b)
+    it64, ms64 = timed(lambda: la.CGSolver.value(A, None, b, x64, 1000000, 1e-12, ctx=ctx))
+    ref_norm = float(torch.linalg.norm(x64))
+    out = {"workload": f"Q1 {M}^2 SPD, coef 10^U(-2,2), FP64 target 1e-10, inner FP32 to 1e-3",
+           "cg64": {"ms": round(ms64, 1), "iterations": it64, "relres": relres(x64)}}
+    x = torch.zeros_like(b)
+    q.solve(b, x, eps=1e-10)  # warm-up (graph instantiation)
+    x.zero_()
+    info, ms = timed(lambda: q.solve(b, x, eps=1e-10))
+    out["ir_mgpcg32"] = {"ms": round(ms, 2), "outer": info["outer"], "inner_iterations": info["iterations"],
+                         "relres": relres(x), "err_vs_cg64": float(torch.linalg.norm(x - x64)) / ref_norm}
+    A32 = A.to_float(ctx=ctx)
+    x.zero_()
+    (outer, _, _, inner), ms = timed(lambda: la.IRSolver.value_cg(A, A32, b, x, eps=1e-10, inner_eps=1e-3, ctx=ctx))
+    out["ir_cg32"] = {"ms": round(ms, 1), "outer": outer, "inner_iterations": inner, "relres": relres(x),
+                      "err_vs_cg64": float(torch.linalg.norm(x - x64)) / ref_norm}
+    out["speedup_ir_mgpcg32_vs_cg64"] = round(ms64 / out["ir_mgpcg32"]["ms"], 1)
+    q.close()
+    return out
+
+
+def bench_serve(n_requests=120, rate=150.0, seed=11):
+    """The serving stream: Q1 requests with grid side log-uniform in [33, 1025], cellwise
+    coefficient log-uniform in [1e-2, 1e2], b = A x_true, each solved to 1e-8 relative FP64
+    residual, submitted from host buffers and returned to host buffers.  The mixed server
+    (batched small grids + concurrent MG-PCG workers) against plain FP64 CG one request at a
+    time, on the same trace: once as a burst (every request queued at t = 0: capacity in
+    solves/s) and once with Poisson arrivals at ``rate`` per second (latency under load)."""
+    from honei_b200 import serve as S
+
+    burst = S.poisson_trace(n_requests, rate=0.0, seed=seed)
+    timed = S.poisson_trace(n_requests, rate=rate, seed=seed)
+    out = {"workload": f"{n_requests} requests of the serving stream (side log-U[33,1025], coef log-U[1e-2,1e2], "
+                       f"1e-8 FP64), burst and Poisson {rate:g}/s", "rows_total": burst.rows}
+    with S.Server(mode="mixed") as srv:  # warm-up: module load, memory pool
+        S.replay(srv, S.poisson_trace(8, 0.0, seed=seed + 1000), realtime=False)
+    for mode in ("mixed", "plain"):
+        res = {}
+        for name, tr, rt in (("burst", burst, False), ("poisson", timed, True)):
+            with S.Server(mode=mode) as srv:
+                rep = S.replay(srv, tr, realtime=rt)
+                peak = srv.stats()["bytes_peak"]
+            res[name] = {"solves_per_s": round(rep["solves_per_s"], 2), "p50_ms": round(rep["p50_ms"], 2),
+                         "p99_ms": round(rep["p99_ms"], 2), "ok": rep["ok"], "paths": rep["paths"],
+                         "max_true_relres": rep["max_true_relres"], "hbm_peak_bytes": peak}
+        out[mode] = res
+    out["speedup_solves_per_s"] = round(out["mixed"]["burst"]["solves_per_s"] / out["plain"]["burst"]["solves_per_s"], 2)
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -404,6 +561,9 @@ def run_ours(args):
 
     cg_cluster = bench_cg_cluster(ctx)
     batch_extra = None if args.no_batch else bench_batch(la, ctx)
+    mg_extra = None if args.no_mg else bench_mg(la, ctx, cpu=(ws == 1 and not args.no_cpu_baseline))
+    ir_extra = None if args.no_mg else bench_ir(la, ctx)
+    serve_extra = None if (args.no_serve or rank != 0 and ws > 1) else bench_serve(args.serve_requests)
 
     line = None
     if rank == 0:
@@ -429,7 +589,7 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "extra": {"spmv_f32_gbs": round(gbs32, 2), "cg_257": cg_extra, "cg_257_cluster": cg_cluster,
-                      "batch_512": batch_extra},
+                      "mg_2049": mg_extra, "ir_2049": ir_extra, "batch_512": batch_extra, "serve": serve_extra},
         }
         print(json.dumps(line), flush=True)
     barrier()
@@ -446,6 +606,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-system batched workload")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream workload")
+    ap.add_argument("--no-mg", action="store_true", help="skip the 2049^2 MG and mixed-precision workloads")
+    ap.add_argument("--serve-requests", type=int, default=120, help="requests in the serving sample")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -156,8 +156,8 @@ class Server:
     device bytes of the admitted requests; a request above the budget alone is refused at
     submit with HB_ERR_CAPACITY."""
 
-    def __init__(self, mode: str = "mixed", budget_bytes: int = 64 << 30, large_workers: int = 2,
-                 small_workers: int = 1, small_max_side: int = 160, max_batch: int = 256, cluster: int = 2,
+    def __init__(self, mode: str = "mixed", budget_bytes: int = 64 << 30, large_workers: int = 8,
+                 small_workers: int = 1, small_max_side: int = 96, max_batch: int = 256, cluster: int = 2,
                  threads: int = 512, max_clusters: int = 0, eps: float = 1e-8, inner_eps: float = 1e-3,
                  device: int = 0, pinned: bool = True):
         self._lib = _register()
@@ -182,8 +182,9 @@ class Server:
         self.handle = h
         self._live = {}
 
-    def submit(self, req: Request) -> int:
-        """Queues ``req``; returns its tag.  The host arrays stay referenced until it completes."""
+    def stage(self, req: Request):
+        """The request's host buffers (page-locked when the server is) and its C record: the
+        input data as it sits in host memory before the request arrives."""
         n = req.M * req.M
         coef = _as_host(req.coef, self.pinned)
         b = _as_host(req.b, self.pinned)
@@ -192,7 +193,13 @@ class Server:
         r = HbRequest(req.M, coef.ctypes.data if coef is not None else None,
                       b.ctypes.data if b is not None else None, xt.ctypes.data if xt is not None else None,
                       x.ctypes.data, req.tag)
-        self._live[req.tag] = (coef, b, xt, x)
+        return r, (coef, b, xt, x)
+
+    def submit(self, req: Request, staged=None) -> int:
+        """Queues ``req`` (staged by ``stage`` or now); returns its tag.  The host arrays stay
+        referenced until it completes."""
+        r, held = staged if staged is not None else self.stage(req)
+        self._live[req.tag] = held
         st = self._lib.hb_server_submit(self.handle, C.byref(r))
         if st:
             del self._live[req.tag]
@@ -247,13 +254,15 @@ class Server:
 
 
 def replay(server: Server, trace: Trace, realtime: bool = True) -> dict:
-    """Submits the trace's requests at their arrival times (on the server clock; all at once when
-    ``realtime`` is false), collects every completion and summarises them: solves/s over the
+    """Stages every request's host buffers, then submits the requests at their arrival times (on
+    the server clock; all at once when ``realtime`` is false), collects every completion and
+    summarises them: solves/s over the
     makespan (first submit to last completion), latency percentiles (submit to completion, so
     queueing included) and service times (admission to completion)."""
     done = []
+    staged = [server.stage(req) for req in trace.requests]
     t_base = server.clock()
-    for req in trace.requests:
+    for req, st in zip(trace.requests, staged):
         if realtime:
             while True:
                 lag = t_base + req.arrival - server.clock()
@@ -264,7 +273,7 @@ def replay(server: Server, trace: Trace, realtime: bool = True) -> dict:
                     while server.clock() < t_base + req.arrival:
                         pass
                     break
-        server.submit(req)
+        server.submit(req, st)
     done += server.drain()
     return summarise(done)
 
