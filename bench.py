@@ -297,6 +297,42 @@ def _ref_cpu():
         return None
 
 
+def bench_q1band(la, ctx, x, ell_s, M=M_SPMV, reps=100, cpu=True):
+    """Product on BandedMatrixQx<Q1Type> (nine bands of n values, no index array) for the same
+    2049^2 Poisson matrix and x as the headline: algorithmic bytes 11*n*8 per product (nine
+    bands, x once, y once).  ``ell_s`` is the ELL product's measured time, for the ratio."""
+    import torch
+    B = la.BandedMatrixQ1.poisson(M, ctx=ctx)
+    n = B.rows()
+    y = torch.empty_like(x)
+    for _ in range(3):
+        la.Product.value(y, B, x, ctx=ctx)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        la.Product.value(y, B, x, ctx=ctx)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    nbytes = 11 * n * 8
+    peak, _ = measured_peak()
+    out = {"workload": f"BandedMatrixQx<Q1Type> product, Poisson {M}^2, FP64", "bytes_per_product": nbytes,
+           "us_per_product": round(t * 1e6, 2), "gbs": round(nbytes / t / 1e9, 1),
+           "frac_of_peak": round(nbytes / t / 1e9 / peak, 4),
+           "speedup_vs_ell_product": round(ell_s / t, 2)}
+    if cpu:
+        R = _ref_cpu()
+        if R is not None:
+            bands = R.q1band_poisson(M)
+            _, sec = R.q1band_spmv(bands, x.cpu().numpy(), tag="mc-sse", reps=20)
+            out["cpu_reference_gbs"] = round(nbytes / sec / 1e9, 2)
+            out["cpu_reference"] = f"tags::CPU::MultiCore::SSE, {os.cpu_count()} cores, median of 20"
+    del B
+    torch.cuda.empty_cache()
+    return out
+
+
 def bench_mg(la, ctx, M=2049, seed=5, cpu=True):
     """Q1 Poisson M^2 (unit coefficient, the reference's rediscretised hierarchy down to 9^2):
     MGSolver V(2,2), damped Jacobi 0.7, PROLMAT transfers, coarse CG, x0 = 0, b = A x_true.
@@ -533,6 +569,9 @@ def run_ours(args):
     gbs32 = spmv_bytes(nnz, n, 4) * 100 / (f0.elapsed_time(f1) / 1e3) / 1e9
     del A32, x32, y32
 
+    # ---- banded Q1 product (BandedMatrixQx<Q1Type>) of the same grid (extra) ----
+    band_extra = bench_q1band(la, ctx, x, per_launch_s, cpu=(ws == 1 and not args.no_cpu_baseline))
+
     # ---- plain FP64 CG on 257^2: solve latency (host b -> device solve -> host x) ----
     Acg = la.SparseMatrixELL.q1_poisson(M_CG, ctx=ctx)
     ncg = Acg.rows()
@@ -588,7 +627,8 @@ def run_ours(args):
                     "d2h_bytes_per_step": n * 8, "api": "honei_b200.la.Product.value (C ABI hb_spmv_f64)"},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
-            "extra": {"spmv_f32_gbs": round(gbs32, 2), "cg_257": cg_extra, "cg_257_cluster": cg_cluster,
+            "extra": {"spmv_f32_gbs": round(gbs32, 2), "q1band_2049": band_extra, "cg_257": cg_extra,
+                      "cg_257_cluster": cg_cluster,
                       "mg_2049": mg_extra, "ir_2049": ir_extra, "batch_512": batch_extra, "serve": serve_extra},
         }
         print(json.dumps(line), flush=True)

@@ -28,6 +28,11 @@ class HbEll(C.Structure):
                 ("Aj", C.c_void_p), ("Ax", C.c_void_p), ("dtype", C.c_int32), ("pad_", C.c_int32)]
 
 
+class HbQ1Band(C.Structure):
+    _fields_ = [("n", C.c_int64), ("root", C.c_int64), ("band", C.c_void_p * 9), ("dtype", C.c_int32),
+                ("pad_", C.c_int32)]
+
+
 class HbMGParams(C.Structure):
     _fields_ = [("max_iters", C.c_int64), ("max_iters_coarse", C.c_int64), ("n_pre", C.c_int64),
                 ("n_post", C.c_int64), ("damping", C.c_double), ("eps", C.c_double)]
@@ -36,6 +41,7 @@ class HbMGParams(C.Structure):
 i64, vp, f64, f32, i32 = C.c_int64, C.c_void_p, C.c_double, C.c_float, C.c_int
 P_i64 = C.POINTER(C.c_int64)
 P_ell = C.POINTER(HbEll)
+P_band = C.POINTER(HbQ1Band)
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -103,6 +109,14 @@ SIGNATURES = {
     "hb_q1_levels": (i32, [vp, C.POINTER(i32), P_i64]),
     "hb_q1_level": (i32, [vp, i32, P_ell, P_ell, P_ell, P_ell]),
     "hb_q1_solve": (i32, [vp, vp, vp, f64, f64, i64, i64, vp]),
+    # banded Q1 matrices
+    "hb_q1band_root": (i64, [i64]),
+    "hb_q1band_spmv_f64": (i32, [vp, P_band, vp, vp]),
+    "hb_q1band_spmv_f32": (i32, [vp, P_band, vp, vp]),
+    "hb_q1band_defect_f64": (i32, [vp, P_band, vp, vp, vp]),
+    "hb_q1band_defect_f32": (i32, [vp, P_band, vp, vp, vp]),
+    "hb_q1band_fill_poisson": (i32, [vp, i64, P_band]),
+    "hb_q1band_from_ell": (i32, [vp, P_ell, P_band]),
     # serving loop
     "hb_server_create": (i32, [vp, C.POINTER(vp)]),
     "hb_server_submit": (i32, [vp, vp]),

@@ -179,6 +179,147 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Small systems (at most SMALL_GROUPS row groups, e.g. the coarsest MG level): the same
+// iteration in one block, thread t owning row group t, p exchanged through shared memory and
+// the matrix slots held in registers, so an iteration is two block reductions and no global
+// round trip or grid barrier.  For these sizes the cooperative kernel runs as a single block
+// with the same thread-to-group mapping and the same reduction tree (threads without rows add
+// exact zeros), so both kernels produce bit-identical iterates.
+// ---------------------------------------------------------------------------------------
+constexpr int SMALL_GROUPS = 256;
+
+template <typename T>
+__device__ __forceinline__ T block_total(T v, T *red, T *bcast)
+{
+    v = hbd::block_sum(v, red);
+    if (threadIdx.x == 0) *bcast = v;
+    __syncthreads();
+    return *bcast;
+}
+
+template <typename T, int KT>
+__global__ void __launch_bounds__(SMALL_GROUPS) cg_small_kernel(CGParams<T> P)
+{
+    using hbd::add; using hbd::mul; using hbd::sub;
+    constexpr int KR = KT > 0 ? KT : 1;
+    __shared__ __align__(16) T sp[4 * SMALL_GROUPS];
+    __shared__ T red[32];
+    __shared__ T bcast;
+    const int64_t rows = P.rows;
+    const int64_t groups = P.ld / 4;
+    const int64_t g = threadIdx.x;
+    const bool own = g < groups;
+    const int64_t r0 = 4 * g;
+
+    int32_t aj[KR][4];
+    T ax[KR][4];
+    if (KT > 0) {
+#pragma unroll
+        for (int k = 0; k < KR; ++k) {
+            if (own) {
+                hbd::ld4_stream(P.Aj + (int64_t)k * P.ld + r0, aj[k]);
+                hbd::ld4_stream(P.Ax + (int64_t)k * P.ld + r0, ax[k]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) { aj[k][i] = -1; ax[k][i] = T(0); }
+            }
+        }
+    }
+    // s = A sp on the thread's own rows, slots in the reference order
+    auto product = [&](T (&s)[4]) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) s[i] = T(0);
+        if (!own) return;
+        if (KT > 0) {
+#pragma unroll
+            for (int k = 0; k < KR; ++k)
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (aj[k][i] >= 0) s[i] = add(s[i], mul(ax[k][i], sp[aj[k][i]]));
+        } else {
+            for (int k = 0; k < P.K; ++k)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int32_t j = __ldg(P.Aj + (int64_t)k * P.ld + r0 + i);
+                    if (j >= 0) s[i] = add(s[i], mul(__ldg(P.Ax + (int64_t)k * P.ld + r0 + i), sp[j]));
+                }
+        }
+    };
+
+    T x[4], r[4], p[4], v[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        x[i] = (own && r0 + i < rows) ? P.x_user[r0 + i] : T(0);
+        if (own) sp[r0 + i] = x[i];
+    }
+    __syncthreads();
+    // r = b - A x, alpha = r.r
+    T acc = T(0);
+    product(v);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const T bb = (own && r0 + i < rows) ? P.b_user[r0 + i] : T(0);
+        r[i] = sub(bb, v[i]);
+        acc = add(acc, mul(r[i], r[i]));
+        p[i] = T(0);
+    }
+    T alpha = block_total(acc, red, &bcast);
+    const T initial_defect = dsqrt(alpha);
+    T current_defect = T(0);
+    T beta = T(0);
+    const T epsm = eps_mach<T>();
+    int64_t it = 0, used = 0;
+    while (it < P.max_iters) {
+        const bool first = (it == 0);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            p[i] = first ? r[i] : add(mul(p[i], beta), r[i]);
+            if (own) sp[r0 + i] = p[i];
+        }
+        __syncthreads();
+        product(v);
+        acc = T(0);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc = add(acc, mul(v[i], p[i]));
+        const T temp = block_total(acc, red, &bcast);
+        const T lambda = alpha / (fabs(temp) > epsm ? temp : epsm);
+        const T mlambda = -lambda;
+        acc = T(0);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            x[i] = add(x[i], mul(lambda, p[i]));
+            r[i] = add(r[i], mul(mlambda, v[i]));
+            acc = add(acc, mul(r[i], r[i]));
+        }
+        const T alpha_old = alpha;
+        alpha = block_total(acc, red, &bcast);
+        beta = alpha / (fabs(alpha_old) > epsm ? alpha_old : epsm);
+        ++it;
+        current_defect = dsqrt(alpha);
+        if (current_defect < P.eps * initial_defect) { used = it; break; }
+        if (current_defect < P.eps) { used = it; break; }
+        if (it == P.max_iters) used = it;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        if (own && r0 + i < rows) P.x_user[r0 + i] = x[i];
+    if (threadIdx.x == 0) {
+        P.res->used = used;
+        P.res->defect0 = (double)initial_defect;
+        P.res->defect = (double)current_defect;
+        P.res->status = 0;
+    }
+}
+
+template <typename T, int KT>
+int launch_cg_small(hb_context *ctx, const CGParams<T> &P, int64_t groups)
+{
+    const int threads = (int)std::max<int64_t>(32, (groups + 31) / 32 * 32);
+    cg_small_kernel<T, KT><<<1, threads, 0, ctx->stream>>>(P);
+    return hb_check_launch(ctx, "cg_small_kernel");
+}
+
 template <typename T, int KT>
 int launch_cg_kt(hb_context *ctx, CGParams<T> &P, int blocks)
 {
@@ -221,9 +362,11 @@ int hb_launch_cg(hb_context *ctx, const hb_ell *A, const T *b, T *x, int64_t max
     P.bar.gen = bar + 1;
     P.bar.status = (int *)(bar + 2);
     P.res = res;
-    HB_CUDA_TRY(ctx, cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), ctx->stream));
     const int64_t groups = ld / 4;
     const bool k9 = (A->K == 9);
+    if (groups <= SMALL_GROUPS)
+        return k9 ? launch_cg_small<T, 9>(ctx, P, groups) : launch_cg_small<T, 0>(ctx, P, groups);
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), ctx->stream));
     const int maxb = k9 ? cg_max_blocks<T, 9>(ctx) : cg_max_blocks<T, 0>(ctx);
     // about one row group per thread for small systems; all co-resident blocks otherwise
     const int64_t want = (groups + CG_THREADS - 1) / CG_THREADS;

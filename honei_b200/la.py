@@ -215,26 +215,106 @@ class SparseMatrixELL:
         return SparseMatrixELL(self._rows, self._cols, self.K, self.ld, Aj, Ax)
 
 
-class Product:
-    """Product<tags::GPU::CUDA>::value(y, A, x): y = A x (honei/la/product.hh:1758-1760)."""
+class BandedMatrixQ1:
+    """BandedMatrixQx<Q1Type, DT> (honei/la/banded_matrix_qx.hh): nine bands of n values in the
+    order LL, LD, LU, DL, DD, DU, UL, UD, UU, on the device.  ``bands`` is a (9, ldb) tensor,
+    ldb = n rounded up to 4 so that every band starts 16-byte aligned.
+
+        A = BandedMatrixQ1.poisson(M)                   # FillMatrix<POISSON, DIRICHLET_0>
+        A = BandedMatrixQ1.from_ell(E)                  # BandedMatrixQx(SparseMatrixELL &)
+        A = BandedMatrixQ1.from_bands([ll, ld, ...])    # nine host or device arrays
+    """
+
+    LL, LD, LU, DL, DD, DU, UL, UD, UU = range(9)
+
+    def __init__(self, n: int, bands: torch.Tensor, root: int | None = None):
+        from ._lib import HbQ1Band
+        self.n = int(n)
+        self.bands = bands
+        self.dtype = bands.dtype
+        self.root = int(root if root is not None else lib().hb_q1band_root(self.n))
+        self._s = HbQ1Band()
+        self._s.n = self.n
+        self._s.root = self.root
+        for k in range(9):
+            self._s.band[k] = bands[k].data_ptr()
+        self._s.dtype = 0 if self.dtype == torch.float64 else 1
 
     @staticmethod
-    def value(y: torch.Tensor, A: SparseMatrixELL, x: torch.Tensor, ctx: Context | None = None):
+    def _empty(n: int, dtype, device="cuda") -> torch.Tensor:
+        ldb = max(4, (n + 3) // 4 * 4)
+        return torch.zeros((9, ldb), dtype=dtype, device=device)
+
+    @classmethod
+    def poisson(cls, M: int, dtype=torch.float64, ctx: Context | None = None) -> "BandedMatrixQ1":
+        ctx = ctx or default_context()
+        A = cls(M * M, cls._empty(M * M, dtype))
+        check(lib().hb_q1band_fill_poisson(ctx.handle, M, C.byref(A._s)), "hb_q1band_fill_poisson", ctx.handle)
+        A.root = A._s.root
+        return A
+
+    @classmethod
+    def from_ell(cls, E: SparseMatrixELL, ctx: Context | None = None) -> "BandedMatrixQ1":
+        ctx = ctx or default_context()
+        A = cls(E.rows(), cls._empty(E.rows(), E.dtype))
+        check(lib().hb_q1band_from_ell(ctx.handle, C.byref(E.struct), C.byref(A._s)), "hb_q1band_from_ell",
+              ctx.handle)
+        A.root = A._s.root
+        return A
+
+    @classmethod
+    def from_bands(cls, bands, dtype=torch.float64) -> "BandedMatrixQ1":
+        bands = [torch.as_tensor(b, dtype=dtype) for b in bands]
+        if len(bands) != 9 or len({b.numel() for b in bands}) != 1:
+            raise ValueError("nine bands of equal size expected")
+        n = bands[0].numel()
+        t = cls._empty(n, dtype)
+        for k, b in enumerate(bands):
+            t[k, :n].copy_(b.reshape(-1))
+        return cls(n, t)
+
+    @property
+    def struct(self):
+        return self._s
+
+    def rows(self) -> int:
+        return self.n
+
+    def columns(self) -> int:
+        return self.n
+
+    def band(self, k: int) -> torch.Tensor:
+        return self.bands[k, : self.n]
+
+
+def _spmv_fn(A, kind: str):
+    if isinstance(A, BandedMatrixQ1):
+        return getattr(lib(), f"hb_q1band_{kind}_{_SUF[A.dtype]}")
+    return getattr(lib(), f"hb_{kind}_{_SUF[A.dtype]}")
+
+
+class Product:
+    """Product<tags::GPU::CUDA>::value(y, A, x): y = A x, for a SparseMatrixELL
+    (honei/la/product.hh:1758-1760) or a BandedMatrixQ1 (honei/la/product.hh:1750-1756)."""
+
+    @staticmethod
+    def value(y: torch.Tensor, A, x: torch.Tensor, ctx: Context | None = None):
         if x.numel() != A.columns():
             raise VectorSizeDoesNotMatch(x.numel(), A.columns())
         if A.rows() != y.numel():
             raise VectorSizeDoesNotMatch(A.rows(), y.numel())
         ctx = ctx or default_context()
-        fn = getattr(lib(), f"hb_spmv_{_SUF[A.dtype]}")
+        fn = _spmv_fn(A, "spmv")
         check(fn(ctx.handle, C.byref(A.struct), _vec(x, A.dtype, "x"), _vec(y, A.dtype, "y")), "Product", ctx.handle)
         return y
 
 
 class Defect:
-    """Defect<tags::GPU::CUDA>::value(r, b, A, x): r = b - A x (honei/math/defect.hh:660-670)."""
+    """Defect<tags::GPU::CUDA>::value(r, b, A, x): r = b - A x for a SparseMatrixELL
+    (honei/math/defect.hh:660-670) or a BandedMatrixQ1 (honei/math/defect.hh:645-658)."""
 
     @staticmethod
-    def value(r: torch.Tensor, b: torch.Tensor, A: SparseMatrixELL, x: torch.Tensor, ctx: Context | None = None):
+    def value(r: torch.Tensor, b: torch.Tensor, A, x: torch.Tensor, ctx: Context | None = None):
         if x.numel() != A.columns():
             raise VectorSizeDoesNotMatch(x.numel(), A.columns())
         if b.numel() != A.columns():
@@ -242,7 +322,7 @@ class Defect:
         if r.numel() != A.rows():
             raise VectorSizeDoesNotMatch(r.numel(), A.rows())
         ctx = ctx or default_context()
-        fn = getattr(lib(), f"hb_defect_{_SUF[A.dtype]}")
+        fn = _spmv_fn(A, "defect")
         check(fn(ctx.handle, C.byref(A.struct), _vec(b, A.dtype, "b"), _vec(x, A.dtype, "x"),
                  _vec(r, A.dtype, "r")), "Defect", ctx.handle)
         return r

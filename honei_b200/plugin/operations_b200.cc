@@ -1,8 +1,9 @@
 /* operations_b200.cc -- HONEI's tags::GPU::CUDA operators on the B200 backend.
  *
  * Defines the static members HONEI declares unconditionally for the GPU tag:
- *   Product<tags::GPU::CUDA>         honei/la/product.hh:1728-1794   (ELL SpMV, Jacobi apply)
- *   Defect<tags::GPU::CUDA>          honei/math/defect.hh:645-692    (ELL defect)
+ *   Product<tags::GPU::CUDA>         honei/la/product.hh:1728-1794   (ELL SpMV, banded Q1
+ *                                                                     product, Jacobi apply)
+ *   Defect<tags::GPU::CUDA>          honei/math/defect.hh:645-692    (ELL and banded Q1 defect)
  *   DotProduct<tags::GPU::CUDA>      honei/la/dot_product.hh:343-368
  *   Norm<vnt_l_two, {false,true}, tags::GPU::CUDA>  honei/la/norm.hh:538-580
  *   ScaledSum<tags::GPU::CUDA>       honei/la/scaled_sum.hh:444-488
@@ -192,6 +193,66 @@ namespace honei
         int eprod(int64_t n, double * r, const double * x, const double * y) { return hb_element_product_f64(context(), n, r, x, y); }
         int eprod(int64_t n, float * r, const float * x, const float * y) { return hb_element_product_f32(context(), n, r, x, y); }
 
+        int q1_spmv(const hb_q1band & A, const double * x, double * y) { return hb_q1band_spmv_f64(context(), &A, x, y); }
+        int q1_spmv(const hb_q1band & A, const float * x, float * y) { return hb_q1band_spmv_f32(context(), &A, x, y); }
+        int q1_defect(const hb_q1band & A, const double * b, const double * x, double * r)
+        { return hb_q1band_defect_f64(context(), &A, b, x, r); }
+        int q1_defect(const hb_q1band & A, const float * b, const float * x, float * r)
+        { return hb_q1band_defect_f32(context(), &A, b, x, r); }
+
+        /// The nine bands of a BandedMatrixQx locked for the GPU tag (the MemoryArbiter uploads
+        /// them on first use and keeps them resident), as an hb_q1band.
+        template <typename DT_> struct BandLocks
+        {
+            const BandedMatrixQx<Q1Type, DT_> & a;
+            hb_q1band s;
+            BandLocks(const BandedMatrixQx<Q1Type, DT_> & aa) : a(aa)
+            {
+                s.n = (int64_t)a.size();
+                s.root = hb_q1band_root(s.n);
+                s.dtype = sizeof(DT_) == 8 ? HB_F64 : HB_F32;
+                s.pad_ = 0;
+                for (unsigned long k(0) ; k < 9 ; ++k)
+                    s.band[k] = a.band(k).lock(lm_read_only, tags::GPU::CUDA::memory_value);
+            }
+            ~BandLocks()
+            {
+                for (unsigned long k(0) ; k < 9 ; ++k) a.band(k).unlock(lm_read_only);
+            }
+        };
+
+        template <typename DT_>
+        void product(DenseVectorContinuousBase<DT_> & result, const BandedMatrixQx<Q1Type, DT_> & a,
+                const DenseVectorContinuousBase<DT_> & b)
+        {
+            if (b.size() != a.columns())
+                throw VectorSizeDoesNotMatch(b.size(), a.columns());
+            if (a.rows() != result.size())
+                throw VectorSizeDoesNotMatch(a.rows(), result.size());
+            BandLocks<DT_> A(a);
+            DeviceLock<DenseVectorContinuousBase<DT_> > x(b, lm_read_only);
+            DeviceLock<DenseVectorContinuousBase<DT_> > y(result, lm_write_only);
+            check(q1_spmv(A.s, (const DT_ *)x.ptr, (DT_ *)y.ptr), "Product<GPU::CUDA> (BandedMatrixQx)");
+        }
+
+        template <typename DT_>
+        void defect(DenseVectorContinuousBase<DT_> & result, const DenseVectorContinuousBase<DT_> & rhs,
+                const BandedMatrixQx<Q1Type, DT_> & a, const DenseVectorContinuousBase<DT_> & x)
+        {
+            if (x.size() != a.columns())
+                throw VectorSizeDoesNotMatch(x.size(), a.columns());
+            if (rhs.size() != a.columns())
+                throw VectorSizeDoesNotMatch(rhs.size(), a.columns());
+            if (result.size() != a.rows())
+                throw VectorSizeDoesNotMatch(result.size(), a.rows());
+            BandLocks<DT_> A(a);
+            DeviceLock<DenseVectorContinuousBase<DT_> > xl(x, lm_read_only);
+            DeviceLock<DenseVectorContinuousBase<DT_> > bl(rhs, lm_read_only);
+            DeviceLock<DenseVectorContinuousBase<DT_> > rl(result, lm_write_only);
+            check(q1_defect(A.s, (const DT_ *)bl.ptr, (const DT_ *)xl.ptr, (DT_ *)rl.ptr),
+                    "Defect<GPU::CUDA> (BandedMatrixQx)");
+        }
+
         template <typename DT_>
         void product(DenseVectorContinuousBase<DT_> & result, const SparseMatrixELL<DT_> & a, const DenseVectorContinuousBase<DT_> & b)
         {
@@ -242,7 +303,73 @@ namespace honei
         return result;
     }
 
+    DenseVector<float> Product<tags::GPU::CUDA>::value(const BandedMatrixQx<Q1Type, float> & a,
+            const DenseVectorContinuousBase<float> & b)
+    {
+        CONTEXT("When multiplying BandedMatrixQx<Q1Type, float> with DenseVector<float> (B200):");
+        DenseVector<float> result(a.rows());
+        b200::product<float>(result, a, b);
+        return result;
+    }
+
+    DenseVector<double> Product<tags::GPU::CUDA>::value(const BandedMatrixQx<Q1Type, double> & a,
+            const DenseVectorContinuousBase<double> & b)
+    {
+        CONTEXT("When multiplying BandedMatrixQx<Q1Type, double> with DenseVector<double> (B200):");
+        DenseVector<double> result(a.rows());
+        b200::product<double>(result, a, b);
+        return result;
+    }
+
+    DenseVector<float> & Product<tags::GPU::CUDA>::value(DenseVector<float> & result,
+            const BandedMatrixQx<Q1Type, float> & a, const DenseVectorContinuousBase<float> & b)
+    {
+        CONTEXT("When multiplying BandedMatrixQx<Q1Type, float> with DenseVector<float> (B200):");
+        b200::product<float>(result, a, b);
+        return result;
+    }
+
+    DenseVector<double> & Product<tags::GPU::CUDA>::value(DenseVector<double> & result,
+            const BandedMatrixQx<Q1Type, double> & a, const DenseVectorContinuousBase<double> & b)
+    {
+        CONTEXT("When multiplying BandedMatrixQx<Q1Type, double> with DenseVector<double> (B200):");
+        b200::product<double>(result, a, b);
+        return result;
+    }
+
     // ---- Defect -------------------------------------------------------------------------
+    DenseVector<float> Defect<tags::GPU::CUDA>::value(const DenseVectorContinuousBase<float> & rhs,
+            const BandedMatrixQx<Q1Type, float> & system, const DenseVectorContinuousBase<float> & x)
+    {
+        DenseVector<float> result(system.rows());
+        b200::defect<float>(result, rhs, system, x);
+        return result;
+    }
+
+    DenseVector<double> Defect<tags::GPU::CUDA>::value(const DenseVectorContinuousBase<double> & rhs,
+            const BandedMatrixQx<Q1Type, double> & system, const DenseVectorContinuousBase<double> & x)
+    {
+        DenseVector<double> result(system.rows());
+        b200::defect<double>(result, rhs, system, x);
+        return result;
+    }
+
+    DenseVector<float> & Defect<tags::GPU::CUDA>::value(DenseVector<float> & result,
+            const DenseVectorContinuousBase<float> & rhs, const BandedMatrixQx<Q1Type, float> & system,
+            const DenseVectorContinuousBase<float> & x)
+    {
+        b200::defect<float>(result, rhs, system, x);
+        return result;
+    }
+
+    DenseVector<double> & Defect<tags::GPU::CUDA>::value(DenseVector<double> & result,
+            const DenseVectorContinuousBase<double> & rhs, const BandedMatrixQx<Q1Type, double> & system,
+            const DenseVectorContinuousBase<double> & x)
+    {
+        b200::defect<double>(result, rhs, system, x);
+        return result;
+    }
+
     DenseVector<float> Defect<tags::GPU::CUDA>::value(const DenseVectorContinuousBase<float> & rhs,
             const SparseMatrixELL<float> & system, const DenseVectorContinuousBase<float> & x)
     {

@@ -127,6 +127,37 @@ int hb_spmv_f32(hb_context *ctx, const hb_ell *A, const float *x, float *y);
 int hb_defect_f64(hb_context *ctx, const hb_ell *A, const double *b, const double *x, double *r);
 int hb_defect_f32(hb_context *ctx, const hb_ell *A, const float *b, const float *x, float *r);
 
+/* BandedMatrixQx<Q1Type, DT> (honei/la/banded_matrix_qx.hh:44-129): the nine-band matrix of a
+ * square Q1 grid, one device array of n values per band, in the Q1BandIndex order LL, LD, LU,
+ * DL, DD, DU, UL, UD, UU (honei/la/band_type.hh); band k of row i multiplies x at i + offset_k,
+ * offsets -root-1, -root, -root+1, -1, 0, 1, root-1, root, root+1, root = floor(sqrt(n)). */
+typedef struct {
+    int64_t n;          /* rows = columns */
+    int64_t root;       /* floor(sqrt(n)); set by hb_q1band_fill_poisson / hb_q1band_from_ell */
+    void *band[9];      /* device pointers, n values each (16-byte aligned for vector loads) */
+    int32_t dtype;      /* hb_dtype */
+    int32_t pad_;
+} hb_q1band;
+int64_t hb_q1band_root(int64_t n);
+/* y = A x.  Product<tags::GPU::CUDA>::value(DenseVector&, const BandedMatrixQx<Q1Type>&, const
+ * DenseVectorContinuousBase&), honei/la/product.hh:1750-1756; replaces
+ * cuda_product_bmdv_q1_{float,double} (honei/backends/cuda/product.cu:30-145).  Bit-identical
+ * to Product<tags::CPU> (honei/la/product.hh:371-404): DD x[i] first, then the eight other
+ * bands in index order, each only where its column lies in [0, n). */
+int hb_q1band_spmv_f64(hb_context *ctx, const hb_q1band *A, const double *x, double *y);
+int hb_q1band_spmv_f32(hb_context *ctx, const hb_q1band *A, const float *x, float *y);
+/* r = b - A x.  Defect<tags::GPU::CUDA>::value on BandedMatrixQx, honei/math/defect.hh:
+ * 645-658; bit-identical to Defect<tags::CPU> (honei/math/defect.hh:194-199). */
+int hb_q1band_defect_f64(hb_context *ctx, const hb_q1band *A, const double *b, const double *x, double *r);
+int hb_q1band_defect_f32(hb_context *ctx, const hb_q1band *A, const float *b, const float *x, float *r);
+/* FillMatrix<Tag, POISSON, DIRICHLET_0>::value(BandedMatrixQx&), honei/math/fill_matrix.hh:
+ * 41-77, on an M x M grid (A->n = M^2, A->dtype and A->band[] set by the caller). */
+int hb_q1band_fill_poisson(hb_context *ctx, int64_t M, hb_q1band *A);
+/* BandedMatrixQx(SparseMatrixELL&), honei/la/banded_matrix_qx-impl.hh:111-167: band k of row
+ * i = A(i, i + offset_k) where that column exists, 0 elsewhere.  n must be a square
+ * (HB_ERR_UNSUPPORTED otherwise); E->dtype == A->dtype. */
+int hb_q1band_from_ell(hb_context *ctx, const hb_ell *E, hb_q1band *A);
+
 /* Host scalar results (synchronous, like the reference's value-returning operators).
  * DotProduct<tags::GPU::CUDA>::value, honei/la/dot_product.hh:358-360 (replaces
  * cuda_dot_product_two_{float,double}, honei/backends/cuda/dot_product.cu:77-155);

@@ -100,6 +100,35 @@ class Oracle:
         getattr(self.lib, f"ora_defect_{s}")(_c.byref(e), _ptr(b), _ptr(x), _ptr(r))
         return r
 
+    @staticmethod
+    def _bands(bands, dtype):
+        bands = [np.ascontiguousarray(b, dtype) for b in bands]
+        return bands, (_vp * 9)(*[b.ctypes.data for b in bands])
+
+    def q1band_spmv(self, bands, x):
+        """Product<tags::CPU> on BandedMatrixQx<Q1Type> (bands: 9 arrays, LL..UU)."""
+        dt = np.asarray(bands[0]).dtype
+        keep, bp = self._bands(bands, dt)
+        x = np.ascontiguousarray(x, dt)
+        y = np.zeros(len(x), dt)
+        getattr(self.lib, f"ora_q1band_spmv_{self._suffix(dt)}")(_u64(len(x)), bp, _ptr(x), _ptr(y))
+        return y
+
+    def q1band_defect(self, bands, b, x):
+        dt = np.asarray(bands[0]).dtype
+        keep, bp = self._bands(bands, dt)
+        b = np.ascontiguousarray(b, dt)
+        x = np.ascontiguousarray(x, dt)
+        r = np.zeros(len(x), dt)
+        getattr(self.lib, f"ora_q1band_defect_{self._suffix(dt)}")(_u64(len(x)), bp, _ptr(b), _ptr(x), _ptr(r))
+        return r
+
+    def q1band_poisson(self, M):
+        out = [np.zeros(M * M) for _ in range(9)]
+        bp = (_vp * 9)(*[b.ctypes.data for b in out])
+        self.lib.ora_q1band_poisson_f64(_u64(M * M), bp)
+        return out
+
     def dot(self, x, y):
         x = np.ascontiguousarray(x)
         y = np.ascontiguousarray(y, x.dtype)
@@ -187,6 +216,11 @@ class Reference:
 
     def __init__(self, path: str = REF_SO):
         self.lib = _c.CDLL(path)
+        # The reference's MultiCore thread pool pins the calling thread to one core when it
+        # starts (honei/backends/multicore/thread_pool.cc:395-399, mc::affinity defaults to
+        # true); every thread this process creates afterwards would inherit that mask.
+        # _check() puts the caller's mask back after each call.
+        self._mask = os.sched_getaffinity(0) if hasattr(os, "sched_getaffinity") else None
         L = self.lib
         L.ref_last_error.restype = _c.c_char_p
         ul = _c.c_ulong
@@ -210,11 +244,18 @@ class Reference:
                                            _c.POINTER(ul), _c.POINTER(_c.c_double)]
         L.ref_mg_f32.argtypes = mg_args + [_c.c_float, ul, ul, ul, ul, _c.c_float,
                                            _c.POINTER(ul), _c.POINTER(_c.c_double)]
+        L.ref_q1band_spmv_f64.argtypes = [_c.c_int, ul, _vp, _vp, _vp, _c.c_int, _c.POINTER(_c.c_double)]
+        L.ref_q1band_spmv_f32.argtypes = L.ref_q1band_spmv_f64.argtypes
+        L.ref_q1band_defect_f64.argtypes = [ul, _vp, _vp, _vp, _vp]
+        L.ref_q1band_poisson_f64.argtypes = [ul, _vp]
+        L.ref_q1band_from_ell_f64.argtypes = [_vp, _vp, _vp, _vp]
         L.ref_ir_mg.argtypes = [_c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                 _c.c_float, ul, ul, ul, ul, _c.c_float, _c.c_double, ul,
                                 _c.POINTER(ul), _c.POINTER(_c.c_double)]
 
     def _check(self, rc):
+        if self._mask is not None:
+            os.sched_setaffinity(0, self._mask)
         if rc != 0:
             raise RuntimeError("reference: " + self.lib.ref_last_error().decode())
 
@@ -235,6 +276,43 @@ class Reference:
         Arl = np.zeros(rows, np.uint64)
         self._check(self.lib.ref_q1_poisson_f64(M, info, _ptr(Aj), _ptr(Ax), _ptr(Arl)))
         return EllMatrix(rows, cols, stride, ncpr, T, Aj, Ax, Arl, nnz)
+
+    def q1band_spmv(self, bands, x, tag="cpu", reps=0):
+        """Product<tag> on BandedMatrixQx<Q1Type>: (y, median seconds of `reps` timed calls);
+        tags "cpu", "sse", "mc-sse"."""
+        dt = np.asarray(bands[0]).dtype
+        bands = [np.ascontiguousarray(b, dt) for b in bands]
+        bp = (_vp * 9)(*[b.ctypes.data for b in bands])
+        x = np.ascontiguousarray(x, dt)
+        y = np.zeros(len(x), dt)
+        sec = _c.c_double(0)
+        s = "f64" if dt == np.float64 else "f32"
+        self._check(getattr(self.lib, f"ref_q1band_spmv_{s}")(TAGS[tag], len(x), bp, _ptr(x), _ptr(y), reps,
+                                                               _c.byref(sec)))
+        return y, sec.value
+
+    def q1band_defect(self, bands, b, x):
+        bands = [np.ascontiguousarray(v, np.float64) for v in bands]
+        bp = (_vp * 9)(*[v.ctypes.data for v in bands])
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.ascontiguousarray(x, np.float64)
+        r = np.zeros(len(x))
+        self._check(self.lib.ref_q1band_defect_f64(len(x), bp, _ptr(b), _ptr(x), _ptr(r)))
+        return r
+
+    def q1band_poisson(self, M):
+        out = [np.zeros(M * M) for _ in range(9)]
+        bp = (_vp * 9)(*[b.ctypes.data for b in out])
+        self._check(self.lib.ref_q1band_poisson_f64(M, bp))
+        return out
+
+    def q1band_from_ell(self, A):
+        """BandedMatrixQx(SparseMatrixELL &) of an FP64 reference-layout matrix: 9 bands."""
+        info = np.array([A.rows, A.cols, A.stride, A.ncpr, A.threads], np.uint64)
+        out = [np.zeros(A.rows) for _ in range(9)]
+        bp = (_vp * 9)(*[b.ctypes.data for b in out])
+        self._check(self.lib.ref_q1band_from_ell_f64(_ptr(info), _ptr(A.Aj), _ptr(A.Ax), bp))
+        return out
 
     def read_ell(self, path):
         from honei_b200.problems import EllMatrix

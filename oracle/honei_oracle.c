@@ -401,3 +401,62 @@ int ora_ir_pcg(const ora_ell *A64, const ora_mg *mg32, float damping, const doub
     }
     return 0;
 }
+
+/* ---- BandedMatrixQx<Q1Type> ------------------------------------------------------------
+ * Product<tags::CPU>::value(result, BandedMatrixQx, x) (honei/la/product.hh:371-404): the
+ * diagonal product first, then the eight off-diagonal bands in the order LL, LD, LU, DL, DU,
+ * UL, UD, UU, each only where its column index lies in [0, n) (a bound on the linear index,
+ * not on the grid line). */
+#define ORA_Q1BAND_ROW(T, i)                                                                  \
+    do {                                                                                      \
+        const long r_ = (long)root, n_ = (long)n, k_ = (long)(i);                             \
+        T s_ = band[4][k_] * x[k_];                                                           \
+        if (k_ - r_ - 1 >= 0) s_ += band[0][k_] * x[k_ - r_ - 1];                             \
+        if (k_ - r_ >= 0)     s_ += band[1][k_] * x[k_ - r_];                                 \
+        if (k_ - r_ + 1 >= 0) s_ += band[2][k_] * x[k_ - r_ + 1];                             \
+        if (k_ - 1 >= 0)      s_ += band[3][k_] * x[k_ - 1];                                  \
+        if (k_ + 1 < n_)      s_ += band[5][k_] * x[k_ + 1];                                  \
+        if (k_ + r_ - 1 < n_) s_ += band[6][k_] * x[k_ + r_ - 1];                             \
+        if (k_ + r_ < n_)     s_ += band[7][k_] * x[k_ + r_];                                 \
+        if (k_ + r_ + 1 < n_) s_ += band[8][k_] * x[k_ + r_ + 1];                             \
+        out_ = s_;                                                                            \
+    } while (0)
+
+static uint64_t q1band_root(uint64_t n) { return (uint64_t)sqrt((double)n); }
+
+void ora_q1band_spmv_f64(uint64_t n, const double *const *band, const double *x, double *y)
+{
+    const uint64_t root = q1band_root(n);
+    for (uint64_t i = 0; i < n; ++i) { double out_; ORA_Q1BAND_ROW(double, i); y[i] = out_; }
+}
+
+void ora_q1band_spmv_f32(uint64_t n, const float *const *band, const float *x, float *y)
+{
+    const uint64_t root = q1band_root(n);
+    for (uint64_t i = 0; i < n; ++i) { float out_; ORA_Q1BAND_ROW(float, i); y[i] = out_; }
+}
+
+void ora_q1band_defect_f64(uint64_t n, const double *const *band, const double *b, const double *x, double *r)
+{
+    const uint64_t root = q1band_root(n);
+    for (uint64_t i = 0; i < n; ++i) { double out_; ORA_Q1BAND_ROW(double, i); r[i] = b[i] - out_; }
+}
+
+void ora_q1band_defect_f32(uint64_t n, const float *const *band, const float *b, const float *x, float *r)
+{
+    const uint64_t root = q1band_root(n);
+    for (uint64_t i = 0; i < n; ++i) { float out_; ORA_Q1BAND_ROW(float, i); r[i] = b[i] - out_; }
+}
+
+/* FillMatrix<Tag, POISSON, DIRICHLET_0> on BandedMatrixQx (honei/math/fill_matrix.hh:41-77):
+ * with 1-based i, rows i <= M, i > N - M, i % M == 1 or i % M == 0 are unit rows; the others
+ * hold 8/3 on the diagonal and -1/3 on all eight off-diagonal bands. */
+void ora_q1band_poisson_f64(uint64_t n, double *const *band)
+{
+    const uint64_t M = q1band_root(n);
+    for (uint64_t i = 1; i <= n; ++i) {
+        const int unit = i <= M || i > n - M || (i % M) == 1 || (i % M) == 0;
+        for (int k = 0; k < 9; ++k) band[k][i - 1] = unit ? 0.0 : -1.0 / 3.0;
+        band[4][i - 1] = unit ? 1.0 : 8.0 / 3.0;
+    }
+}

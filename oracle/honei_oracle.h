@@ -32,6 +32,16 @@ void   ora_spmv_f64(const ora_ell *A, const double *x, double *y);
 void   ora_spmv_f32(const ora_ell *A, const float *x, float *y);
 void   ora_defect_f64(const ora_ell *A, const double *b, const double *x, double *r);
 void   ora_defect_f32(const ora_ell *A, const float *b, const float *x, float *r);
+/* BandedMatrixQx<Q1Type> (honei/la/banded_matrix_qx.hh): nine bands of n values in the
+ * Q1BandIndex order LL, LD, LU, DL, DD, DU, UL, UD, UU (honei/la/band_type.hh); root =
+ * floor(sqrt(n)).  y = A x as Product<tags::CPU> (honei/la/product.hh:371-404); r = b - A x as
+ * Defect<tags::CPU> (honei/math/defect.hh:194-199: the product, then Difference). */
+void   ora_q1band_spmv_f64(uint64_t n, const double *const *band, const double *x, double *y);
+void   ora_q1band_spmv_f32(uint64_t n, const float *const *band, const float *x, float *y);
+void   ora_q1band_defect_f64(uint64_t n, const double *const *band, const double *b, const double *x, double *r);
+void   ora_q1band_defect_f32(uint64_t n, const float *const *band, const float *b, const float *x, float *r);
+/* FillMatrix<POISSON, DIRICHLET_0> on the banded form (honei/math/fill_matrix.hh:41-77). */
+void   ora_q1band_poisson_f64(uint64_t n, double *const *band);
 double ora_dot_f64(uint64_t n, const double *x, const double *y);
 float  ora_dot_f32(uint64_t n, const float *x, const float *y);
 void   ora_scaled_sum_f64(uint64_t n, double *x, const double *y, double b);

@@ -250,11 +250,109 @@ namespace
         MuteCout() : old(std::cout.rdbuf(sink.rdbuf())) {}
         ~MuteCout() { std::cout.rdbuf(old); }
     };
+
+    // Product on BandedMatrixQx<Q1Type> for tags::CPU (product.hh:333-366), tags::CPU::SSE
+    // (product-sse.cc:217-253) and tags::CPU::MultiCore::SSE (product.hh:1970-2020; the
+    // MultiCore::Generic instantiation does not compile in the reference).  reps > 0 times that many products (median into *seconds).
+    template <typename T_, typename DT_> void q1band_product(const BandedMatrixQx<Q1Type, DT_> & A,
+            const DenseVector<DT_> & x, DT_ * y, int reps, double * seconds)
+    {
+        DenseVector<DT_> r(Product<T_>::value(A, x));
+        std::vector<double> t;
+        for (int k(0) ; k < reps ; ++k)
+        {
+            double t0(now_s());
+            DenseVector<DT_> rr(Product<T_>::value(A, x));
+            t.push_back(now_s() - t0);
+        }
+        if (seconds)
+        {
+            std::sort(t.begin(), t.end());
+            *seconds = t.empty() ? 0. : t[t.size() / 2];
+        }
+        dv_to(r, y);
+    }
+
+    template <typename DT_> BandedMatrixQx<Q1Type, DT_> q1band_from(unsigned long n, const DT_ * const * band)
+    {
+        std::vector<DenseVector<DT_> > b;
+        for (int k(0) ; k < 9 ; ++k)
+        {
+            DenseVector<DT_> v(n);
+            for (unsigned long i(0) ; i < n ; ++i) v[i] = band[k][i];
+            b.push_back(v);
+        }
+        return BandedMatrixQx<Q1Type, DT_>(n, b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8]);
+    }
+
+    template <typename DT_> int q1band_spmv_impl(int tag, unsigned long n, const DT_ * const * band, const DT_ * x,
+            DT_ * y, int reps, double * seconds)
+    {
+        return guarded([&]() {
+            BandedMatrixQx<Q1Type, DT_> A(q1band_from<DT_>(n, band));
+            DenseVector<DT_> xv(n);
+            for (unsigned long i(0) ; i < n ; ++i) xv[i] = x[i];
+            switch (tag)
+            {
+                case 0: q1band_product<tags::CPU>(A, xv, y, reps, seconds); break;
+                case 2: q1band_product<tags::CPU::SSE>(A, xv, y, reps, seconds); break;
+                case 4: q1band_product<tags::CPU::MultiCore::SSE>(A, xv, y, reps, seconds); break;
+                default: throw InternalError("ref_shim: no banded Q1 product for this tag");
+            }
+        });
+    }
 }
 
 extern "C"
 {
     const char * ref_last_error() { return g_last_error.c_str(); }
+
+    int ref_q1band_spmv_f64(int tag, unsigned long n, const double * const * band, const double * x, double * y,
+            int reps, double * seconds)
+    { return q1band_spmv_impl<double>(tag, n, band, x, y, reps, seconds); }
+
+    int ref_q1band_spmv_f32(int tag, unsigned long n, const float * const * band, const float * x, float * y,
+            int reps, double * seconds)
+    { return q1band_spmv_impl<float>(tag, n, band, x, y, reps, seconds); }
+
+    // Defect<tags::CPU> on BandedMatrixQx (defect.hh:194-199).
+    int ref_q1band_defect_f64(unsigned long n, const double * const * band, const double * b, const double * x,
+            double * r)
+    {
+        return guarded([&]() {
+            BandedMatrixQx<Q1Type, double> A(q1band_from<double>(n, band));
+            DenseVector<double> bv(n), xv(n), rv(n);
+            for (unsigned long i(0) ; i < n ; ++i) { bv[i] = b[i]; xv[i] = x[i]; }
+            Defect<tags::CPU>::value(rv, bv, A, xv);
+            dv_to(rv, r);
+        });
+    }
+
+    // FillMatrix<POISSON, DIRICHLET_0> on BandedMatrixQx (fill_matrix.hh:41-77), bands out.
+    int ref_q1band_poisson_f64(unsigned long M, double * const * band)
+    {
+        return guarded([&]() {
+            const unsigned long N(M * M);
+            DenseVector<double> z(N, 0.);
+            BandedMatrixQx<Q1Type, double> q1(N, z.copy(), z.copy(), z.copy(), z.copy(), z.copy(), z.copy(),
+                    z.copy(), z.copy(), z.copy());
+            FillMatrix<tags::CPU, applications::POISSON, boundary_types::DIRICHLET::DIRICHLET_0>::value(q1);
+            const Q1BandIndex idx[9] = { LL, LD, LU, DL, DD, DU, UL, UD, UU };
+            for (int k(0) ; k < 9 ; ++k) dv_to(q1.band(idx[k]), band[k]);
+        });
+    }
+
+    // BandedMatrixQx(SparseMatrixELL&) conversion (banded_matrix_qx-impl.hh:111-167): n must be
+    // (2^L + 1)^2.  ELL arrays in, bands out.
+    int ref_q1band_from_ell_f64(const unsigned long * ainfo, const uint64_t * Aj, const double * Ax, double * const * band)
+    {
+        return guarded([&]() {
+            SparseMatrixELL<double> A(ell_from(ainfo[0], ainfo[1], ainfo[2], ainfo[3], ainfo[4], Aj, Ax));
+            BandedMatrixQx<Q1Type, double> q1(A);
+            const Q1BandIndex idx[9] = { LL, LD, LU, DL, DD, DU, UL, UD, UU };
+            for (int k(0) ; k < 9 ; ++k) dv_to(q1.band(idx[k]), band[k]);
+        });
+    }
 
     // Threads used by the MultiCore tags: mc::num_threads and every max_count key on the path.
     int ref_set_threads(int n)

@@ -54,3 +54,19 @@ def featflow():
     prol = [golden_matrix(d, f"prol_{l}") for l in range(2, 5)]
     res = [P.ell_from_csr(p.cols, p.rows, *P.transpose_csr(p.rows, p.cols, *p.to_csr())) for p in prol]
     return P.MGHierarchy(A, prol, res, [0] * 4), d
+
+
+def q1band_test_data(size, dtype):
+    """The vectors of the reference's banded product test (honei/la/product_TEST.cc:196-219):
+    bands (dv3, dv2, dv4, dv2, dv3, dv4, dv4, dv3, dv2) and x = dv1, v[i] = (i + k) % 311."""
+    i = np.arange(size)
+    dv1, dv2, dv3, dv4 = [((i + k) % 311).astype(dtype) for k in (2, 1, 25, 7)]
+    return [dv3, dv2, dv4, dv2, dv3, dv4, dv4, dv3, dv2], dv1
+
+
+def q1band_used_mask(n):
+    """(9, n) mask of the band entries the banded product reads (column inside [0, n))."""
+    root = int(np.sqrt(n))
+    offs = [-root - 1, -root, -root + 1, -1, 0, 1, root - 1, root, root + 1]
+    r = np.arange(n)
+    return np.stack([(r + o >= 0) & (r + o < n) for o in offs])

@@ -17,6 +17,14 @@ readers, honei/math/matrix_io.hh and honei/math/vector_io.hh):
 * q1_small.npz -- the reference's own Q1 Poisson construction (FillMatrix -> SparseMatrix ->
   SparseMatrixELL) at 33^2, with SpMV/CG/MG/IR results, FP64 and FP32, natural, permuted and
   variable-coefficient variants, plus CG iteration counts at 257^2.
+* q1band.npz -- BandedMatrixQx<Q1Type>: the data of the reference's banded product test
+  (honei/la/product_TEST.cc:189-244, bands (i + k) % 311) at levels 2 and 5, FP32 and FP64,
+  with Product<tags::CPU> results; the banded Poisson fill at 33^2
+  (honei/math/fill_matrix.hh:41-77); the banded form of a variable-coefficient Q1 ELL matrix
+  by the reference's conversion (banded_matrix_qx-impl.hh:111-167) with a seeded product and
+  defect.
+
+    python tests/golden/make_golden.py [/path/to/honei-tree] [--only q1band]
 """
 from __future__ import annotations
 
@@ -46,8 +54,52 @@ def put_matrix(out, name, A):
     out[f"{name}_data"] = dv
 
 
-def main(tree: str) -> None:
+def product_test_bands(size: int, dtype):
+    """The vectors of Q1MatrixDenseVectorProductTest (honei/la/product_TEST.cc:196-219): x and
+    the bands (dv3, dv2, dv4, dv2, dv3, dv4, dv4, dv3, dv2), v_k[i] = (i + k) % 311."""
+    i = np.arange(size)
+    dv = {k: ((i + k) % 311).astype(dtype) for k in (1, 2, 7, 25)}
+    dv1, dv2, dv3, dv4 = dv[2], dv[1], dv[25], dv[7]
+    return [dv3, dv2, dv4, dv2, dv3, dv4, dv4, dv3, dv2], dv1
+
+
+def banded(R) -> None:
+    out = {}
+    for level in (2, 5):
+        size = (2 ** level + 1) ** 2
+        for name, dt in (("f64", np.float64), ("f32", np.float32)):
+            bands, x = product_test_bands(size, dt)
+            y, _ = R.q1band_spmv(bands, x, tag="cpu")
+            out[f"test_L{level}_{name}_y"] = y
+    M = 33
+    out["poisson_bands"] = np.stack(R.q1band_poisson(M))
+    coef = P.log_uniform_coef(M, 1e-2, 1e2, 4)
+    A = P.q1_poisson(M, coef)
+    out["var_coef"] = coef
+    bands = R.q1band_from_ell(A)
+    # the conversion leaves band entries whose column lies outside [0, n) as allocated
+    # (uninitialised); the product never reads them.  Zero them for a stable fixture.
+    n, root = M * M, M
+    offs = [-root - 1, -root, -root + 1, -1, 0, 1, root - 1, root, root + 1]
+    r = np.arange(n)
+    for k, o in enumerate(offs):
+        bands[k][(r + o < 0) | (r + o >= n)] = 0.0
+    out["var_bands"] = np.stack(bands)
+    x = P.uniform_vector(M * M, 6)
+    b = P.uniform_vector(M * M, 8)
+    out["var_x"], out["var_b"] = x, b
+    out["var_y64"], _ = R.q1band_spmv(bands, x, tag="cpu")
+    out["var_y32"], _ = R.q1band_spmv([v.astype(np.float32) for v in bands], x.astype(np.float32), tag="cpu")
+    out["var_r64"] = R.q1band_defect(bands, b, x)
+    np.savez_compressed(os.path.join(HERE, "q1band.npz"), **out)
+
+
+def main(tree: str, only: str | None = None) -> None:
     R = Reference()
+    if only is not None:
+        {"q1band": banded}[only](R)
+        print("golden fixture", only, "written to", HERE)
+        return
     td = os.path.join(tree, "honei", "math", "testdata")
 
     # ---- FEATFLOW2 MG fixture --------------------------------------------------------
@@ -134,8 +186,14 @@ def main(tree: str) -> None:
     out["cg257_x_sample"] = x257[::97].copy()
     out["cg257_x_sum"] = np.array(x257.sum())
     np.savez_compressed(os.path.join(HERE, "q1_small.npz"), **out)
+    banded(R)
     print("golden fixtures written to", HERE)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--only")]
+    only = None
+    if "--only" in sys.argv:
+        only = sys.argv[sys.argv.index("--only") + 1]
+        args = [a for a in args if a != only]
+    main(args[0] if args else "/root/reference", only)

@@ -183,8 +183,50 @@ void generic_mg(const std::string & dir, unsigned long L)
             d.str());
 }
 
+// BandedMatrixQx<Q1Type>: the reference's own banded Poisson fill, plus a banded matrix with
+// seeded values on every band; product and defect on tags::GPU::CUDA against tags::CPU.
+template <typename DT_> void banded(unsigned long M, const std::string & tag)
+{
+    const unsigned long n(M * M);
+    DenseVector<DT_> z(n, DT_(0));
+    BandedMatrixQx<Q1Type, DT_> P(n, z.copy(), z.copy(), z.copy(), z.copy(), z.copy(), z.copy(), z.copy(),
+            z.copy(), z.copy());
+    FillMatrix<tags::CPU, applications::POISSON, boundary_types::DIRICHLET::DIRICHLET_0>::value(P);
+    BandedMatrixQx<Q1Type, DT_> R(n, seeded<DT_>(n, 11), seeded<DT_>(n, 12), seeded<DT_>(n, 13), seeded<DT_>(n, 14),
+            seeded<DT_>(n, 15), seeded<DT_>(n, 16), seeded<DT_>(n, 17), seeded<DT_>(n, 18), seeded<DT_>(n, 19));
+    DenseVector<DT_> x(seeded<DT_>(n, 4)), b(seeded<DT_>(n, 5));
+    for (int k(0) ; k < 2 ; ++k)
+    {
+        const BandedMatrixQx<Q1Type, DT_> & A(k == 0 ? P : R);
+        const std::string what(k == 0 ? " Poisson " : " seeded ");
+        DenseVector<DT_> ycpu(n), ygpu(n);
+        Product<tags::CPU>::value(ycpu, A, x);
+        Product<tags::GPU::CUDA>::value(ygpu, A, x);
+        report(equal(ycpu, ygpu), "Product<GPU::CUDA> BandedMatrixQx bit-exact" + what + tag);
+        DenseVector<DT_> yret(Product<tags::GPU::CUDA>::value(A, x));
+        report(equal(ycpu, yret), "Product<GPU::CUDA> BandedMatrixQx (value-returning) bit-exact" + what + tag);
+        DenseVector<DT_> rcpu(n), rgpu(n);
+        Defect<tags::CPU>::value(rcpu, b, A, x);
+        Defect<tags::GPU::CUDA>::value(rgpu, b, A, x);
+        report(equal(rcpu, rgpu), "Defect<GPU::CUDA> BandedMatrixQx bit-exact" + what + tag);
+    }
+    bool threw(false);
+    try
+    {
+        DenseVector<DT_> wrong(n + 1);
+        Product<tags::GPU::CUDA>::value(P, wrong);
+    }
+    catch (VectorSizeDoesNotMatch &)
+    {
+        threw = true;
+    }
+    report(threw, "BandedMatrixQx VectorSizeDoesNotMatch before launch " + tag);
+}
+
 int main(int argc, char ** argv)
 {
+    banded<double>(33, "f64 33^2");
+    banded<float>(129, "f32 129^2");
     operators<double>(33, "f64 33^2");
     operators<double>(129, "f64 129^2");
     operators<float>(65, "f32 65^2");

@@ -150,3 +150,27 @@ def test_cg_full_size_1025_property(hb):
     assert used < 20000 and rel < 1.5e-8
     x2 = torch.zeros_like(xt)
     assert hb.CGSolver.value(Ad, None, b, x2, 20000, 1e-8) == used and torch.equal(x, x2)
+
+
+@pytest.mark.parametrize("M,coef", [(3, False), (9, False), (17, True), (31, True)])
+def test_cg_small_systems_bitwise_equal_to_cooperative_kernel(hb, oracle, M, coef):
+    """Systems of at most 1024 rows run in the one-block kernel; the cooperative kernel (the
+    allocation-free entry point always uses it) must give the same iterates bit for bit,
+    also on the non-symmetric 9^2 coarse matrix whose CG runs to the iteration cap."""
+    import ctypes as C
+    from honei_b200._lib import lib
+    A = P.q1_poisson(M, P.log_uniform_coef(M, 1e-1, 1e1, M) if coef else None)
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 2))
+    Ad = hb.SparseMatrixELL.from_reference(A)
+    bd = dev(b)
+    x1, x2 = torch.zeros_like(bd), torch.zeros_like(bd)
+    u1 = hb.CGSolver.value(Ad, None, bd, x1, 1000, 1e-8)
+    d1 = hb.CGSolver.last_defect
+    u2, d2 = C.c_int64(0), C.c_double(0)
+    st = lib().hb_cg_f64_noalloc(C.byref(Ad.struct), bd.data_ptr(), x2.data_ptr(), 1000, 1e-8, C.byref(u2),
+                                 C.byref(d2), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    assert st == 0 and u1 == u2.value and d1 == d2.value
+    assert torch.equal(x1, x2)
+    x_o, u_o = oracle.cg(A, b, eps=1e-8, max_iters=1000)
+    assert abs(u1 - u_o) <= 1

@@ -140,3 +140,48 @@ def test_oracle_multicore_tags_agree_on_iterations(reference):
     b, _ = reference.spmv(A, P.uniform_vector(A.rows, 1))
     counts = {tag: reference.cg(A, b, tag=tag)[1] for tag in ("cpu", "generic", "sse", "mc-sse")}
     assert max(counts.values()) - min(counts.values()) <= 1, counts
+
+
+# ---- BandedMatrixQx<Q1Type> ----------------------------------------------------------------
+def test_oracle_q1band_matches_reference_fixture(oracle):
+    from conftest import q1band_test_data
+    g = load_golden("q1band")
+    for level in (2, 5):
+        size = (2 ** level + 1) ** 2
+        for name, dt in (("f64", np.float64), ("f32", np.float32)):
+            bands, x = q1band_test_data(size, dt)
+            assert np.array_equal(oracle.q1band_spmv(bands, x), g[f"test_L{level}_{name}_y"]), (level, name)
+    assert np.array_equal(np.stack(oracle.q1band_poisson(33)), g["poisson_bands"])
+    vb = list(g["var_bands"])
+    assert np.array_equal(oracle.q1band_spmv(vb, g["var_x"]), g["var_y64"])
+    assert np.array_equal(oracle.q1band_spmv([v.astype(np.float32) for v in vb], g["var_x"].astype(np.float32)),
+                          g["var_y32"])
+    assert np.array_equal(oracle.q1band_defect(vb, g["var_b"], g["var_x"]), g["var_r64"])
+
+
+def test_oracle_q1band_live_against_reference(oracle, reference):
+    """Random bands on square and non-square sizes: tags::CPU bit for bit; on the sizes the
+    reference's own tests use, (2^L + 1)^2, its SSE and MultiCore::SSE tags agree to rounding
+    (the SSE kernel does not handle a single row)."""
+    from conftest import q1band_used_mask
+    rng = np.random.default_rng(3)
+    for n in (1, 2, 5, 9, 50, 289, 1000, 4225):
+        for dt in (np.float64, np.float32):
+            bands = [rng.uniform(-1, 1, n).astype(dt) for _ in range(9)]
+            x = rng.uniform(-1, 1, n).astype(dt)
+            y_o = oracle.q1band_spmv(bands, x)
+            y_r, _ = reference.q1band_spmv(bands, x, tag="cpu")
+            assert np.array_equal(y_o, y_r), (n, dt)
+            tol = 1e-13 if dt == np.float64 else 1e-5
+            for tag in (("sse", "mc-sse") if n in (9, 289, 4225) else ()):
+                y_t, _ = reference.q1band_spmv(bands, x, tag=tag)
+                assert np.allclose(y_t, y_r, rtol=tol, atol=tol), (n, dt, tag)
+        b = rng.uniform(-1, 1, n)
+        bands64 = [rng.uniform(-1, 1, n) for _ in range(9)]
+        assert np.array_equal(oracle.q1band_defect(bands64, b, x.astype(np.float64)),
+                              reference.q1band_defect(bands64, b, x.astype(np.float64)))
+    # the conversion from ELL reproduces the banded Poisson fill on every entry the product reads
+    conv = np.stack(reference.q1band_from_ell(P.q1_poisson(33)))
+    fill = np.stack(oracle.q1band_poisson(33))
+    mask = q1band_used_mask(33 * 33)
+    assert np.array_equal(conv[mask], fill[mask])
