@@ -472,6 +472,43 @@ class CGSolver:
         return used.value
 
 
+class CGSolverVAR:
+    """CGSolver<tags::GPU::CUDA, methods::VAR>::value (honei/math/cg.hh:140-219): CG with the
+    preconditioner container P -- a CUDA vector (z = P r elementwise, e.g. Jacobi
+    0.7 / diag(A)) or a SparseMatrixELL (z = P r, e.g. SPAI / SAINV).
+
+    ``value(A, P, b, x, max_iters, eps_relative=1e-8)`` solves in place into x (x holds x0) and
+    returns used_iters; ``last_defect`` holds ||r|| at exit.
+    """
+
+    last_defect = None
+
+    @staticmethod
+    def value(A: SparseMatrixELL, P, b: torch.Tensor, x: torch.Tensor, max_iters: int,
+              eps_relative: float = 1e-8, ctx: Context | None = None) -> int:
+        if b.numel() != A.rows():
+            raise VectorSizeDoesNotMatch(b.numel(), A.rows())
+        if x.numel() != A.columns():
+            raise VectorSizeDoesNotMatch(x.numel(), A.columns())
+        ctx = ctx or default_context()
+        used = C.c_int64(0)
+        d = C.c_double() if A.dtype == torch.float64 else C.c_float()
+        if isinstance(P, SparseMatrixELL):
+            if P.rows() != A.rows() or P.columns() != A.columns():
+                raise VectorSizeDoesNotMatch(P.rows(), A.rows())
+            fn = getattr(lib(), f"hb_cg_var_ell_{_SUF[A.dtype]}")
+            pa = C.byref(P.struct)
+        else:
+            if P.numel() != A.rows():
+                raise VectorSizeDoesNotMatch(P.numel(), A.rows())
+            fn = getattr(lib(), f"hb_cg_var_diag_{_SUF[A.dtype]}")
+            pa = _vec(P, A.dtype, "P")
+        check(fn(ctx.handle, C.byref(A.struct), pa, _vec(b, A.dtype, "b"), _vec(x, A.dtype, "x"), int(max_iters),
+                 eps_relative, C.byref(used), C.byref(d)), "CGSolver<VAR>", ctx.handle)
+        CGSolverVAR.last_defect = d.value
+        return used.value
+
+
 class MGData:
     """Device MG hierarchy (MGData + the V(n_pre, n_post) cycle; honei/math/mg.hh:57-243, 567-662).
 

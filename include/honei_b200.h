@@ -209,6 +209,22 @@ int hb_cg_f64(hb_context *ctx, const hb_ell *A, const double *b, double *x, int6
 int hb_cg_f32(hb_context *ctx, const hb_ell *A, const float *b, float *x, int64_t max_iters,
               float eps, int64_t *used_iters, float *final_defect);
 
+/* Preconditioned CG, CGSolver<Tag, methods::VAR>::value(A, P, b, x, max_iters, used_iters,
+ * eps), honei/math/cg.hh:140-219, with the preconditioner container P either a vector (the
+ * _diag entry points: z = P r elementwise, e.g. Jacobi P = damping / diag(A)) or an ELL matrix
+ * of A's size (the _ell entry points: z = P r, e.g. SPAI / SAINV approximate inverses).  Same
+ * update order, sign-keeping division guards and stopping tests (||r|| < eps ||r0||,
+ * ||r|| < eps, max_iters) as the reference; one persistent kernel per solve.  *final_defect
+ * (may be NULL) = ||r|| at exit. */
+int hb_cg_var_diag_f64(hb_context *ctx, const hb_ell *A, const double *P, const double *b, double *x,
+                       int64_t max_iters, double eps, int64_t *used_iters, double *final_defect);
+int hb_cg_var_diag_f32(hb_context *ctx, const hb_ell *A, const float *P, const float *b, float *x,
+                       int64_t max_iters, float eps, int64_t *used_iters, float *final_defect);
+int hb_cg_var_ell_f64(hb_context *ctx, const hb_ell *A, const hb_ell *P, const double *b, double *x,
+                      int64_t max_iters, double eps, int64_t *used_iters, double *final_defect);
+int hb_cg_var_ell_f32(hb_context *ctx, const hb_ell *A, const hb_ell *P, const float *b, float *x,
+                      int64_t max_iters, float eps, int64_t *used_iters, float *final_defect);
+
 /* Allocation-free variant of hb_cg_f64.  This entry point has no counterpart in the reference.
  * It is for callers that cannot allocate device memory when they solve: code issuing work
  * while a stream is captured into a CUDA graph (cudaMalloc is not allowed there), real-time

@@ -149,6 +149,23 @@ class Oracle:
             return x, used.value, hist[: used.value + 1]
         return x, used.value
 
+    def cg_var(self, A, P, b, x0=None, max_iters=10000, eps=1e-8):
+        """CGSolver<VAR>: P a vector (element product) or an EllMatrix.  (x, used_iters)."""
+        s = self._suffix(A.dtype)
+        b = np.ascontiguousarray(b, A.dtype)
+        x = np.zeros(A.rows, A.dtype) if x0 is None else np.array(x0, A.dtype)
+        used = _u64(0)
+        e = _ell(A)
+        f = getattr(self.lib, f"ora_cg_var_{s}")
+        f.argtypes = [_vp, _vp, _vp, _vp, _vp, _u64, _c.c_double if s == "f64" else _c.c_float, _c.POINTER(_u64)]
+        if isinstance(P, np.ndarray):
+            Pd = np.ascontiguousarray(P, A.dtype)
+            f(_c.byref(e), _ptr(Pd), None, _ptr(b), _ptr(x), max_iters, eps, _c.byref(used))
+        else:
+            pe = _ell(P)
+            f(_c.byref(e), None, _c.byref(pe), _ptr(b), _ptr(x), max_iters, eps, _c.byref(used))
+        return x, used.value
+
     def _mg_struct(self, H, max_iters, max_iters_coarse, n_pre, n_post):
         L = len(H.A)
         A = (_OraEll * L)(*[_ell(a) for a in H.A])
@@ -276,6 +293,27 @@ class Reference:
         Arl = np.zeros(rows, np.uint64)
         self._check(self.lib.ref_q1_poisson_f64(M, info, _ptr(Aj), _ptr(Ax), _ptr(Arl)))
         return EllMatrix(rows, cols, stride, ncpr, T, Aj, Ax, Arl, nnz)
+
+    def cg_var(self, A, P, b, x0=None, max_iters=10000, eps=1e-8, tag="cpu"):
+        """CGSolver<tag, methods::VAR>: P a vector or an EllMatrix.  (x, used_iters, seconds)."""
+        s = "f64" if A.dtype == np.float64 else "f32"
+        b = np.ascontiguousarray(b, A.dtype)
+        x = np.zeros(A.rows, A.dtype) if x0 is None else np.array(x0, A.dtype)
+        ainfo = np.array([A.rows, A.cols, A.stride, A.ncpr, A.threads], np.uint64)
+        used, sec = _c.c_ulong(0), _c.c_double(0)
+        f = getattr(self.lib, f"ref_cg_var_{s}")
+        f.argtypes = [_c.c_int] + [_vp] * 9 + [_c.c_ulong, _c.c_double if s == "f64" else _c.c_float,
+                                               _c.POINTER(_c.c_ulong), _c.POINTER(_c.c_double)]
+        if isinstance(P, np.ndarray):
+            Pd = np.ascontiguousarray(P, A.dtype)
+            rc = f(TAGS[tag], _ptr(ainfo), _ptr(A.Aj), _ptr(A.Ax), _ptr(Pd), None, None, None, _ptr(b), _ptr(x),
+                   max_iters, eps, _c.byref(used), _c.byref(sec))
+        else:
+            pinfo = np.array([P.rows, P.cols, P.stride, P.ncpr, P.threads], np.uint64)
+            rc = f(TAGS[tag], _ptr(ainfo), _ptr(A.Aj), _ptr(A.Ax), None, _ptr(pinfo), _ptr(P.Aj), _ptr(P.Ax),
+                   _ptr(b), _ptr(x), max_iters, eps, _c.byref(used), _c.byref(sec))
+        self._check(rc)
+        return x, used.value, sec.value
 
     def q1band_spmv(self, bands, x, tag="cpu", reps=0):
         """Product<tag> on BandedMatrixQx<Q1Type>: (y, median seconds of `reps` timed calls);

@@ -126,6 +126,57 @@ ORA_CG(f64, double, DBL_EPSILON, sqrt, fabs)
 ORA_CG(f32, float, FLT_EPSILON, sqrtf, fabsf)
 
 /* ---------------------------------------------------------------------------------------
+ * CGSolver<Tag, methods::VAR> -- honei/math/cg.hh:140-219.  Product(z, P, r) is the element
+ * product for a vector P (Product(DV, DV, DV), honei/la/product.hh:1198-1204) and the ELL
+ * product for a matrix P.  Norm<l2, true> = sqrt(r.r); divisions guarded by
+ * |t| > eps_mach ? t : eps_mach * (t / |t|) (cg.hh:172, 206).
+ * ------------------------------------------------------------------------------------- */
+#define ORA_CG_VAR(SUF, DT, EPSM, SQRT, FABS)                                               \
+static void precon_##SUF(const DT *Pd, const ora_ell *Pm, uint64_t n, const DT *r, DT *z)    \
+{                                                                                           \
+    if (Pm) ora_spmv_##SUF(Pm, r, z);                                                       \
+    else for (uint64_t i = 0; i < n; ++i) z[i] = Pd[i] * r[i];                              \
+}                                                                                           \
+int ora_cg_var_##SUF(const ora_ell *A, const DT *Pd, const ora_ell *Pm, const DT *b, DT *x,  \
+                     uint64_t max_iters, DT eps, uint64_t *used)                            \
+{                                                                                           \
+    const uint64_t n = A->rows;                                                             \
+    DT *p = (DT *)malloc(sizeof(DT) * (n ? n : 1));                                         \
+    DT *r = (DT *)malloc(sizeof(DT) * (n ? n : 1));                                         \
+    DT *v = (DT *)malloc(sizeof(DT) * (n ? n : 1));                                         \
+    DT *z = (DT *)malloc(sizeof(DT) * (n ? n : 1));                                         \
+    if (!p || !r || !v || !z) { free(p); free(r); free(v); free(z); return 1; }             \
+    ora_defect_##SUF(A, b, x, r);                                                           \
+    precon_##SUF(Pd, Pm, n, r, p);                                                          \
+    const DT initial_defect = SQRT(ora_dot_##SUF(n, r, r));                                 \
+    DT alpha_new = ora_dot_##SUF(n, r, p), alpha, temp, lambda;                             \
+    uint64_t it = 0;                                                                        \
+    while (it < max_iters) {                                                                \
+        ora_spmv_##SUF(A, p, v);                                                            \
+        temp = ora_dot_##SUF(n, v, p);                                                      \
+        lambda = alpha_new / (FABS(temp) > EPSM ? temp : EPSM * (temp / FABS(temp)));       \
+        ++it;                                                                               \
+        for (uint64_t i = 0; i < n; ++i) x[i] += p[i] * lambda;                             \
+        DT mlambda = -lambda;                                                               \
+        for (uint64_t i = 0; i < n; ++i) r[i] += v[i] * mlambda;                            \
+        DT current_defect = SQRT(ora_dot_##SUF(n, r, r));                                   \
+        if (current_defect < eps * initial_defect) { *used = it; break; }                   \
+        if (current_defect < eps) { *used = it; break; }                                    \
+        if (it == max_iters) { *used = it; break; }                                         \
+        precon_##SUF(Pd, Pm, n, r, z);                                                      \
+        alpha = alpha_new;                                                                  \
+        alpha_new = ora_dot_##SUF(n, r, z);                                                 \
+        DT talpha = alpha_new / (FABS(alpha) > EPSM ? alpha : EPSM * (alpha / FABS(alpha))); \
+        for (uint64_t i = 0; i < n; ++i) p[i] *= talpha;                                    \
+        for (uint64_t i = 0; i < n; ++i) p[i] += z[i];                                      \
+    }                                                                                       \
+    free(p); free(r); free(v); free(z);                                                     \
+    return 0;                                                                               \
+}
+ORA_CG_VAR(f64, double, DBL_EPSILON, sqrt, fabs)
+ORA_CG_VAR(f32, float, FLT_EPSILON, sqrtf, fabsf)
+
+/* ---------------------------------------------------------------------------------------
  * Multigrid V-cycle -- honei/math/mg.hh:567-662 (MGCycleCreation<V::STATIC>) and
  * honei/math/mg.hh:1093-1127 (MGSolver), with
  *   smoother RISmoother -- honei/math/ri.hh:97-133: n x { t0 = b - A x; t1 = P * t0; x += t1 }

@@ -60,6 +60,13 @@ int ora_cg_f64(const ora_ell *A, const double *b, double *x, uint64_t max_iters,
 int ora_cg_f32(const ora_ell *A, const float *b, float *x, uint64_t max_iters, float eps,
                uint64_t *used, float *hist);
 
+/* CGSolver<Tag, methods::VAR> (honei/math/cg.hh:140-219): CG with preconditioner P, either a
+ * vector (Pd, the element product z = P r; Pm == NULL) or an ELL matrix (Pm, z = P r). */
+int ora_cg_var_f64(const ora_ell *A, const double *Pd, const ora_ell *Pm, const double *b, double *x,
+                   uint64_t max_iters, double eps, uint64_t *used);
+int ora_cg_var_f32(const ora_ell *A, const float *Pd, const ora_ell *Pm, const float *b, float *x,
+                   uint64_t max_iters, float eps, uint64_t *used);
+
 /* MG hierarchy, coarsest level first (level index 0 == HONEI level 1).  prol[l] maps level l
  * to level l+1 (rows = n_{l+1}); res[l] = prol[l]^T.  P[l] = damping / diag(A[l]). */
 typedef struct {

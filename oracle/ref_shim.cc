@@ -301,11 +301,60 @@ namespace
             }
         });
     }
+    // CGSolver<T_, methods::VAR>::value(A, P, b, x, max_iters, used, eps) (cg.hh:140-219) with a
+    // vector P (Pd != NULL) or an ELL matrix P (pinfo/Pj/Px).
+    template <typename DT_> int cg_var_impl(int tag, const unsigned long * ainfo, const uint64_t * Aj, const DT_ * Ax,
+            const DT_ * Pd, const unsigned long * pinfo, const uint64_t * Pj, const DT_ * Px, const DT_ * b, DT_ * x,
+            unsigned long max_iters, DT_ eps, unsigned long * used, double * seconds)
+    {
+        return guarded([&]() {
+            SparseMatrixELL<DT_> A(ell_from(ainfo[0], ainfo[1], ainfo[2], ainfo[3], ainfo[4], Aj, Ax));
+            DenseVector<DT_> bv(A.rows()), xv(A.rows());
+            for (unsigned long i(0) ; i < A.rows() ; ++i) { bv[i] = b[i]; xv[i] = x[i]; }
+            unsigned long u(0);
+            double t0(now_s());
+            if (Pd)
+            {
+                DenseVector<DT_> P(A.rows());
+                for (unsigned long i(0) ; i < A.rows() ; ++i) P[i] = Pd[i];
+                switch (tag)
+                {
+                    case 0: CGSolver<tags::CPU, methods::VAR>::value(A, P, bv, xv, max_iters, u, eps); break;
+                    case 4: CGSolver<tags::CPU::MultiCore::SSE, methods::VAR>::value(A, P, bv, xv, max_iters, u, eps); break;
+                    default: throw InternalError("ref_shim: CGSolver<VAR> tag not available");
+                }
+            }
+            else
+            {
+                SparseMatrixELL<DT_> P(ell_from(pinfo[0], pinfo[1], pinfo[2], pinfo[3], pinfo[4], Pj, Px));
+                switch (tag)
+                {
+                    case 0: CGSolver<tags::CPU, methods::VAR>::value(A, P, bv, xv, max_iters, u, eps); break;
+                    case 4: CGSolver<tags::CPU::MultiCore::SSE, methods::VAR>::value(A, P, bv, xv, max_iters, u, eps); break;
+                    default: throw InternalError("ref_shim: CGSolver<VAR> tag not available");
+                }
+            }
+            if (seconds) *seconds = now_s() - t0;
+            *used = u;
+            dv_to(xv, x);
+        });
+    }
+
 }
 
 extern "C"
 {
     const char * ref_last_error() { return g_last_error.c_str(); }
+
+    int ref_cg_var_f64(int tag, const unsigned long * ainfo, const uint64_t * Aj, const double * Ax, const double * Pd,
+            const unsigned long * pinfo, const uint64_t * Pj, const double * Px, const double * b, double * x,
+            unsigned long max_iters, double eps, unsigned long * used, double * seconds)
+    { return cg_var_impl<double>(tag, ainfo, Aj, Ax, Pd, pinfo, Pj, Px, b, x, max_iters, eps, used, seconds); }
+
+    int ref_cg_var_f32(int tag, const unsigned long * ainfo, const uint64_t * Aj, const float * Ax, const float * Pd,
+            const unsigned long * pinfo, const uint64_t * Pj, const float * Px, const float * b, float * x,
+            unsigned long max_iters, float eps, unsigned long * used, double * seconds)
+    { return cg_var_impl<float>(tag, ainfo, Aj, Ax, Pd, pinfo, Pj, Px, b, x, max_iters, eps, used, seconds); }
 
     int ref_q1band_spmv_f64(int tag, unsigned long n, const double * const * band, const double * x, double * y,
             int reps, double * seconds)

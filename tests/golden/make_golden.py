@@ -24,7 +24,13 @@ readers, honei/math/matrix_io.hh and honei/math/vector_io.hh):
   by the reference's conversion (banded_matrix_qx-impl.hh:111-167) with a seeded product and
   defect.
 
-    python tests/golden/make_golden.py [/path/to/honei-tree] [--only q1band]
+* pcg.npz -- CGSolver<tags::CPU, methods::VAR>: the Jacobi-preconditioned test of
+  honei/math/cg_TEST.cc:359-440 (testdata/poisson A_6, rhs_6, init_6, P = 0.7 / diag(A),
+  700 iterations, eps 1e-8) with FEATFLOW's sol_6, and the SAINV / SPAI preconditioned solves of
+  poisson_advanced4/sort_0 A_4 (A_4_sainv.ell, A_4_spai.ell; rhs_4, init_4), each with the
+  reference's solution and iteration count (A_4, rhs_4, init_4 live in featflow_pa4.npz).
+
+    python tests/golden/make_golden.py [/path/to/honei-tree] [--only q1band|pcg]
 """
 from __future__ import annotations
 
@@ -94,10 +100,35 @@ def banded(R) -> None:
     np.savez_compressed(os.path.join(HERE, "q1band.npz"), **out)
 
 
+def pcg(R, tree: str) -> None:
+    td = os.path.join(tree, "honei", "math", "testdata")
+    out = {}
+    base = os.path.join(td, "poisson") + "/"
+    A = R.read_ell(base + "A_6.ell")
+    put_matrix(out, "q_A", A)
+    rhs, init, sol = (R.read_exp(base + f"{v}_6") for v in ("rhs", "init", "sol"))
+    out["q_rhs"], out["q_init"], out["q_sol"] = rhs, init, sol
+    ip, ix, dv = A.to_csr()
+    diag = np.array([dv[ip[i]:ip[i + 1]][ix[ip[i]:ip[i + 1]] == i][0] for i in range(A.rows)])
+    out["q_P"] = 0.7 / diag
+    x, used, _ = R.cg_var(A, out["q_P"], rhs, x0=init, max_iters=700, eps=1e-8)
+    out["q_x"], out["q_used"] = x, np.array(used)
+    base = os.path.join(td, "poisson_advanced4", "sort_0") + "/"
+    # A_4, rhs_4 and init_4 are in featflow_pa4.npz already
+    A4 = R.read_ell(base + "A_4.ell")
+    rhs4, init4 = R.read_exp(base + "rhs_4"), R.read_exp(base + "init_4")
+    for kind in ("sainv", "spai"):
+        Pm = R.read_ell(base + f"A_4_{kind}.ell")
+        put_matrix(out, f"a4_{kind}", Pm)
+        x, used, _ = R.cg_var(A4, Pm, rhs4, x0=init4, max_iters=700, eps=1e-8)
+        out[f"a4_{kind}_x"], out[f"a4_{kind}_used"] = x, np.array(used)
+    np.savez_compressed(os.path.join(HERE, "pcg.npz"), **out)
+
+
 def main(tree: str, only: str | None = None) -> None:
     R = Reference()
     if only is not None:
-        {"q1band": banded}[only](R)
+        {"q1band": lambda R: banded(R), "pcg": lambda R: pcg(R, tree)}[only](R)
         print("golden fixture", only, "written to", HERE)
         return
     td = os.path.join(tree, "honei", "math", "testdata")
@@ -187,6 +218,7 @@ def main(tree: str, only: str | None = None) -> None:
     out["cg257_x_sum"] = np.array(x257.sum())
     np.savez_compressed(os.path.join(HERE, "q1_small.npz"), **out)
     banded(R)
+    pcg(R, tree)
     print("golden fixtures written to", HERE)
 
 

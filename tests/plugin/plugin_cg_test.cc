@@ -1,11 +1,13 @@
-// CGSolver<tags::GPU::CUDA, methods::NONE> with the plugin's full specialisation
-// (honei_b200/plugin/solvers_b200.hh: one persistent kernel per solve) against tags::CPU.
+// CGSolver<tags::GPU::CUDA, methods::NONE> and <.., methods::VAR> with the plugin's full
+// specialisations (honei_b200/plugin/solvers_b200.hh: one persistent kernel per solve) against
+// tags::CPU.
 #include "plugin_common.hh"
 
 #include <honei_b200/plugin/solvers_b200.hh>
 
 #include <honei/la/norm.hh>
 #include <honei/la/product.hh>
+#include <honei/la/sparse_matrix.hh>
 #include <honei/math/cg.hh>
 #include <honei/math/defect.hh>
 
@@ -38,8 +40,52 @@ template <typename DT_> void check_cg(unsigned long M, double eps, const std::st
             "CGSolver<GPU::CUDA, NONE> specialisation " + tag, d.str());
 }
 
+// CGSolver<VAR> with a Jacobi vector (0.7 / diag, as honei/math/cg_TEST.cc builds it) and the
+// same preconditioner as a diagonal SparseMatrixELL.
+template <typename DT_> void check_cg_var(unsigned long M, double eps, const std::string & tag)
+{
+    SparseMatrixELL<DT_> A(q1<DT_>(M));
+    const unsigned long n(A.rows());
+    DenseVector<DT_> xt(seeded<DT_>(n, 12)), b(n), P(n);
+    Product<tags::CPU>::value(b, A, xt);
+    for (unsigned long i(0) ; i < n ; ++i) P[i] = DT_(0.7) / A(i, i);
+    SparseMatrix<DT_> Ps(n, n);
+    for (unsigned long i(0) ; i < n ; ++i) Ps(i, i) = P[i];
+    SparseMatrixELL<DT_> Pm(Ps);
+    for (int k(0) ; k < 2 ; ++k)
+    {
+        DenseVector<DT_> xc(n, DT_(0)), xg(n, DT_(0));
+        unsigned long uc(0), ug(0);
+        if (k == 0)
+        {
+            CGSolver<tags::CPU, methods::VAR>::value(A, P, b, xc, 5000ul, uc, DT_(eps));
+            CGSolver<tags::GPU::CUDA, methods::VAR>::value(A, P, b, xg, 5000ul, ug, DT_(eps));
+        }
+        else
+        {
+            CGSolver<tags::CPU, methods::VAR>::value(A, Pm, b, xc, 5000ul, uc, DT_(eps));
+            CGSolver<tags::GPU::CUDA, methods::VAR>::value(A, Pm, b, xg, 5000ul, ug, DT_(eps));
+        }
+        xg.lock(lm_read_only);
+        double err(0), nrm(0);
+        for (unsigned long i(0) ; i < n ; ++i)
+        {
+            err = std::max(err, std::abs(double(xg[i]) - double(xc[i])));
+            nrm = std::max(nrm, std::abs(double(xc[i])));
+        }
+        xg.unlock(lm_read_only);
+        std::ostringstream d;
+        d << "iterations cpu " << uc << " gpu " << ug << ", max |x_gpu - x_cpu| / |x| " << err / nrm;
+        const unsigned long slack(sizeof(DT_) == 8 ? 1 : 1 + uc / 50);
+        report((uc > ug ? uc - ug : ug - uc) <= slack && err <= (sizeof(DT_) == 8 ? 1e-7 : 1e-3) * nrm,
+                std::string("CGSolver<GPU::CUDA, VAR> ") + (k == 0 ? "vector P " : "matrix P ") + tag, d.str());
+    }
+}
+
 int main()
 {
+    check_cg_var<double>(65, 1e-8, "f64 65^2");
+    check_cg_var<float>(33, 1e-5, "f32 33^2");
     check_cg<double>(33, 1e-8, "f64 33^2");
     check_cg<double>(257, 1e-8, "f64 257^2");
     check_cg<float>(65, 1e-5, "f32 65^2");

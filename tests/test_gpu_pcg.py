@@ -1,0 +1,111 @@
+"""CGSolver<methods::VAR> on the device (hb_cg_var_*): Jacobi-vector and ELL-matrix
+preconditioners against the oracle (pinned to the reference's CGSolver<tags::CPU, VAR>) and the
+reference's own fixtures (the Jacobi test of honei/math/cg_TEST.cc on FEATFLOW's poisson A_6, the
+SAINV / SPAI approximate inverses of poisson_advanced4 A_4)."""
+import numpy as np
+import pytest
+
+from conftest import golden_matrix, load_golden
+from honei_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def hb():
+    from honei_b200 import la
+    assert torch.cuda.is_available()
+    return la
+
+
+def dev(a, dt=None):
+    return torch.from_numpy(np.ascontiguousarray(a if dt is None else np.asarray(a).astype(dt))).cuda()
+
+
+def jacobi(A, dt=np.float64):
+    ip, ix, dv = A.to_csr()
+    diag = np.array([dv[ip[i]:ip[i + 1]][ix[ip[i]:ip[i + 1]] == i][0] for i in range(A.rows)])
+    return (dt(0.7) / diag.astype(dt)).astype(dt)
+
+
+def relres(oracle, A, b, x):
+    return np.linalg.norm(oracle.defect(A, b, x)) / np.linalg.norm(b)
+
+
+def solve(hb, A, Pc, b, x0, max_iters, eps):
+    Ad = hb.SparseMatrixELL.from_reference(A)
+    Pd = hb.SparseMatrixELL.from_reference(Pc) if not isinstance(Pc, np.ndarray) else dev(Pc)
+    x = dev(x0)
+    used = hb.CGSolverVAR.value(Ad, Pd, dev(b), x, max_iters, eps)
+    return x.cpu().numpy(), used
+
+
+def test_jacobi_featflow_fixture(hb, oracle):
+    """CGSolverTestSparseELLQuadPrecon: A_6, 0.7/diag, 700 iterations, eps 1e-8, FEATFLOW sol_6
+    within the test's 3e-5; iterations within one of the reference's."""
+    g = load_golden("pcg")
+    A = golden_matrix(g, "q_A")
+    x, used = solve(hb, A, g["q_P"], g["q_rhs"], g["q_init"], 700, 1e-8)
+    assert abs(used - int(g["q_used"])) <= 1, (used, int(g["q_used"]))
+    assert np.abs(x - g["q_sol"]).max() <= 3e-5
+    assert np.abs(x - g["q_x"]).max() <= 1e-7 * np.abs(g["q_x"]).max()
+
+
+@pytest.mark.parametrize("kind", ["spai", "sainv"])
+def test_matrix_preconditioners_fixture(hb, oracle, kind):
+    g = load_golden("pcg")
+    f = load_golden("featflow_pa4")
+    A4 = golden_matrix(f, "A_4")
+    Pm = golden_matrix(g, f"a4_{kind}")
+    x, used = solve(hb, A4, Pm, f["rhs_4"], f["init_4"], 700, 1e-8)
+    ref_used = int(g[f"a4_{kind}_used"])
+    if ref_used < 700:
+        assert abs(used - ref_used) <= 1
+        assert np.abs(x - g[f"a4_{kind}_x"]).max() <= 1e-7 * np.abs(g[f"a4_{kind}_x"]).max()
+    else:
+        # the reference runs to the cap without converging; so must we
+        assert used == 700 and np.isfinite(x).all()
+
+
+@pytest.mark.parametrize("M,dt,eps", [(33, np.float64, 1e-8), (129, np.float64, 1e-8), (65, np.float32, 1e-5),
+                                      (300, np.float64, 1e-8)])
+def test_jacobi_random_q1_parity(hb, oracle, M, dt, eps):
+    A = P.q1_poisson(M, P.log_uniform_coef(M, 1e-1, 1e1, M)).astype(dt)
+    Pd = jacobi(A, dt)
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 2).astype(dt))
+    x_o, u_o = oracle.cg_var(A, Pd, b, max_iters=5000, eps=eps)
+    x_g, u_g = solve(hb, A, Pd, b, np.zeros(A.rows, dt), 5000, eps)
+    tol = 1 if dt == np.float64 else 0.02 * u_o + 1
+    assert abs(u_g - u_o) <= tol, (u_g, u_o)
+    if dt == np.float64:
+        assert abs(relres(oracle, A, b, x_g) - relres(oracle, A, b, x_o)) <= 1e-10
+
+
+def test_vector_and_diagonal_matrix_preconditioner_agree_bitwise(hb, oracle):
+    """The same Jacobi preconditioner as a vector and as a diagonal ELL matrix: z = P r rounds
+    identically (0 + P r), so both kernels produce the same iterates bit for bit."""
+    M = 65
+    A = P.q1_poisson(M, P.log_uniform_coef(M, 1e-2, 1e2, 3))
+    Pd = jacobi(A)
+    Pm = P.ell_from_csr(A.rows, A.rows, np.arange(A.rows + 1), np.arange(A.rows), Pd)
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 4))
+    x1, u1 = solve(hb, A, Pd, b, np.zeros(A.rows), 3000, 1e-8)
+    x2, u2 = solve(hb, A, Pm, b, np.zeros(A.rows), 3000, 1e-8)
+    assert u1 == u2 and np.array_equal(x1, x2)
+
+
+def test_edge_cases(hb, oracle):
+    A = P.q1_poisson(9)
+    Pd = jacobi(A)
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 1))
+    x0 = P.uniform_vector(A.rows, 5)
+    x, used = solve(hb, A, Pd, b, x0, 0, 1e-8)
+    assert used == 0 and np.array_equal(x, x0)
+    Ad = hb.SparseMatrixELL.from_reference(A)
+    with pytest.raises(hb.VectorSizeDoesNotMatch):
+        hb.CGSolverVAR.value(Ad, dev(Pd[:-1]), dev(b), dev(x0), 10, 1e-8)
+    # already solved: stops after one iteration on the absolute test
+    xs, _ = oracle.cg_var(A, Pd, b, max_iters=1000, eps=1e-14)
+    x, used = solve(hb, A, Pd, b, xs, 1000, 1e-8)
+    assert used <= 1

@@ -42,9 +42,12 @@ def test_plugin_operators_and_generic_solvers(tmp_path):
     P.write_exp(str(tmp_path / f"init_{L}"), np.zeros(A.rows))
     out = _run("plugin_ops_test", str(tmp_path), str(L))
     assert "PASS MGSolver<GPU::CUDA>" in out
-    assert out.count("PASS") >= 40
+    assert "FAIL" not in out
+    assert out.count("PASS") >= 54
+    assert out.count("BandedMatrixQx") == 14
 
 
 def test_plugin_cg_specialisation():
     out = _run("plugin_cg_test")
-    assert out.count("PASS") == 4
+    assert out.count("PASS") == 8 and "FAIL" not in out
+    assert out.count("PASS CGSolver<GPU::CUDA, VAR>") == 4

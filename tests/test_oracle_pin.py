@@ -185,3 +185,42 @@ def test_oracle_q1band_live_against_reference(oracle, reference):
     fill = np.stack(oracle.q1band_poisson(33))
     mask = q1band_used_mask(33 * 33)
     assert np.array_equal(conv[mask], fill[mask])
+
+
+# ---- CGSolver<methods::VAR> --------------------------------------------------------------
+def _featflow_eps(digits=3, add=2, size=8):
+    """The FEATFLOW comparison tolerance of honei/math/cg_TEST.cc:200-210 (3e-5 for double)."""
+    base = 1 / 10 ** digits
+    m = (base / 10 ** add - base) / 4
+    return 3 * (m * size + base - 4 * m)
+
+
+def test_oracle_cg_var_matches_reference_fixture(oracle):
+    g = load_golden("pcg")
+    A = golden_matrix(g, "q_A")
+    x, used = oracle.cg_var(A, g["q_P"], g["q_rhs"], x0=g["q_init"], max_iters=700, eps=1e-8)
+    assert used == int(g["q_used"]) and np.array_equal(x, g["q_x"])
+    assert np.abs(x - g["q_sol"]).max() <= _featflow_eps()
+    f = load_golden("featflow_pa4")
+    A4 = golden_matrix(f, "A_4")
+    for kind in ("sainv", "spai"):
+        Pm = golden_matrix(g, f"a4_{kind}")
+        x, used = oracle.cg_var(A4, Pm, f["rhs_4"], x0=f["init_4"], max_iters=700, eps=1e-8)
+        assert used == int(g[f"a4_{kind}_used"]), kind
+        assert np.array_equal(x, g[f"a4_{kind}_x"]), kind
+
+
+def test_oracle_cg_var_live_against_reference(oracle, reference):
+    for M, dt, eps in ((17, np.float64, 1e-8), (33, np.float64, 1e-8), (33, np.float32, 1e-5)):
+        A = P.q1_poisson(M, P.log_uniform_coef(M, 1e-1, 1e1, M)).astype(dt)
+        ip, ix, dv = A.to_csr()
+        diag = np.array([dv[ip[i]:ip[i + 1]][ix[ip[i]:ip[i + 1]] == i][0] for i in range(A.rows)])
+        Pd = (dt(0.7) / diag).astype(dt)
+        b = oracle.spmv(A, P.uniform_vector(A.rows, 2).astype(dt))
+        xo, uo = oracle.cg_var(A, Pd, b, max_iters=700, eps=eps)
+        xr, ur, _ = reference.cg_var(A, Pd, b, max_iters=700, eps=eps)
+        assert uo == ur and np.array_equal(xo, xr), (M, dt)
+        Pm = P.ell_from_csr(A.rows, A.rows, np.arange(A.rows + 1), np.arange(A.rows), Pd, 1, dt)
+        xo2, uo2 = oracle.cg_var(A, Pm, b, max_iters=700, eps=eps)
+        xr2, ur2, _ = reference.cg_var(A, Pm, b, max_iters=700, eps=eps)
+        assert uo2 == ur2 and np.array_equal(xo2, xr2) and np.array_equal(xo2, xo)
