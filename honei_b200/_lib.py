@@ -113,6 +113,11 @@ SIGNATURES = {
     "hb_q1_levels": (i32, [vp, C.POINTER(i32), P_i64]),
     "hb_q1_level": (i32, [vp, i32, P_ell, P_ell, P_ell, P_ell]),
     "hb_q1_solve": (i32, [vp, vp, vp, f64, f64, i64, i64, vp]),
+    # ELL files
+    "hb_ell_file_info": (i32, [C.c_char_p, P_i64]),
+    "hb_ell_read_file_f64": (i32, [vp, C.c_char_p, P_ell]),
+    "hb_ell_read_file_f32": (i32, [vp, C.c_char_p, P_ell]),
+    "hb_ell_write_file": (i32, [vp, P_ell, C.c_char_p]),
     # banded Q1 matrices
     "hb_q1band_root": (i64, [i64]),
     "hb_q1band_spmv_f64": (i32, [vp, P_band, vp, vp]),

@@ -205,6 +205,27 @@ class SparseMatrixELL:
         dtype = np.float64 if self.dtype == torch.float64 else np.float32
         return P.ell_from_csr(self._rows, self._cols, indptr, Aj.T[valid].astype(np.int64), Ax.T[valid], 1, dtype)
 
+    @classmethod
+    def read_file(cls, path: str, dtype=torch.float64, ctx: Context | None = None) -> "SparseMatrixELL":
+        """MatrixIO<io_formats::ELL>::read_matrix straight to the device (hb_ell_read_file_*)."""
+        ctx = ctx or default_context()
+        info = (C.c_int64 * 5)()
+        check(lib().hb_ell_file_info(str(path).encode(), info), f"hb_ell_file_info({path})")
+        size, rows, cols, stride, ncpr = list(info)
+        K, ld = cls.layout(rows, ncpr, 1)
+        Aj = torch.empty(K * ld, dtype=torch.int32, device="cuda")
+        Ax = torch.empty(K * ld, dtype=dtype, device="cuda")
+        s = HbEll(rows, cols, K, ld, Aj.data_ptr(), Ax.data_ptr(), 0 if dtype == torch.float64 else 1, 0)
+        fn = lib().hb_ell_read_file_f64 if dtype == torch.float64 else lib().hb_ell_read_file_f32
+        check(fn(ctx.handle, str(path).encode(), C.byref(s)), f"hb_ell_read_file({path})", ctx.handle)
+        return cls(rows, cols, K, ld, Aj, Ax)
+
+    def write_file(self, path: str, ctx: Context | None = None) -> None:
+        """MatrixIO<io_formats::ELL>::write_matrix of an FP64 matrix (hb_ell_write_file)."""
+        ctx = ctx or default_context()
+        check(lib().hb_ell_write_file(ctx.handle, C.byref(self._s), str(path).encode()), f"hb_ell_write_file({path})",
+              ctx.handle)
+
     def to_float(self, ctx: Context | None = None) -> "SparseMatrixELL":
         """Same pattern with FP32 values (the reference fills FP32 matrices from FP64 values)."""
         ctx = ctx or default_context()

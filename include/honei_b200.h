@@ -110,6 +110,21 @@ int hb_ell_cast_f64_f32(hb_context *ctx, const hb_ell *src, hb_ell *dst);
  * generator (honei_b200/problems.py) bit for bit. */
 int hb_q1_assemble_f64(hb_context *ctx, int64_t M, const double *coef, int symmetric, hb_ell *out);
 
+/* HONEI's binary ELL files (MatrixIO<io_formats::ELL>, honei/math/matrix_io.hh:433-582): five
+ * uint64 {size, rows, columns, stride, num_cols_per_row}, uint64 Aj[size], double Ax[size].
+ * hb_ell_file_info fills info[5] with that header.  hb_ell_read_file_* streams the file into
+ * the caller's hb_ell (Aj/Ax allocated for hb_ell_layout(rows, num_cols_per_row, 1)), keeping
+ * each row's slots up to its first zero value as the reference's raw-array constructor does
+ * (honei/la/sparse_matrix_ell-impl.hh:184-206); _f32 rounds the values as read_matrix's
+ * convert does.  hb_ell_write_file writes an FP64 hb_ell in the reference's one-lane layout
+ * (zero values dropped, num_cols_per_row = longest row, stride = rows rounded up to 32).
+ * HB_ERR_NOT_FOUND: the file cannot be opened; HB_ERR_INVALID: a short or inconsistent file, or
+ * a column index out of range. */
+int hb_ell_file_info(const char *path, int64_t *info);
+int hb_ell_read_file_f64(hb_context *ctx, const char *path, hb_ell *out);
+int hb_ell_read_file_f32(hb_context *ctx, const char *path, hb_ell *out);
+int hb_ell_write_file(hb_context *ctx, const hb_ell *A, const char *path);
+
 /* ------------------------------------------------------------------------------------------
  * Operators (the static value() functions of the tag-dispatched API).
  * ---------------------------------------------------------------------------------------- */

@@ -364,6 +364,21 @@ class Reference:
         self._check(self.lib.ref_read_ell_f64(p, info, _ptr(Aj), _ptr(Ax), _ptr(Arl)))
         return EllMatrix(rows, cols, stride, ncpr, T, Aj, Ax, Arl, nnz)
 
+    def read_mtx(self, path):
+        """MatrixIO<io_formats::MTX>::read_matrix -> SparseMatrixELL (the mtxtoell client)."""
+        from honei_b200.problems import EllMatrix
+        f = self.lib.ref_read_mtx_f64
+        f.argtypes = [_c.c_char_p, _vp, _vp, _vp, _vp]
+        info = (_c.c_ulong * 6)()
+        p = path.encode()
+        self._check(f(p, info, None, None, None))
+        rows, cols, stride, ncpr, T, nnz = list(info)
+        Aj = np.zeros(ncpr * stride, np.uint64)
+        Ax = np.zeros(ncpr * stride)
+        Arl = np.zeros(rows, np.uint64)
+        self._check(f(p, info, _ptr(Aj), _ptr(Ax), _ptr(Arl)))
+        return EllMatrix(rows, cols, stride, ncpr, T, Aj, Ax, Arl, nnz)
+
     def read_exp(self, path):
         n = _c.c_ulong(0)
         self._check(self.lib.ref_read_exp_f64(path.encode(), _c.byref(n), None))

@@ -444,6 +444,16 @@ extern "C"
         });
     }
 
+    // MatrixMarket file -> SparseMatrix -> SparseMatrixELL through the reference (mtxtoell.cc).
+    int ref_read_mtx_f64(const char * path, unsigned long * info, uint64_t * Aj, double * Ax, uint64_t * Arl)
+    {
+        return guarded([&]() {
+            SparseMatrix<double> sm(MatrixIO<io_formats::MTX>::read_matrix(std::string(path), double(0)));
+            SparseMatrixELL<double> A(sm);
+            ell_export(A, info, Aj, Ax, Arl);
+        });
+    }
+
     // Reads an EXP vector with the reference reader (vector_io.hh:52-115). n receives the size.
     int ref_read_exp_f64(const char * path, unsigned long * n, double * out)
     {
