@@ -349,6 +349,50 @@ class Defect:
         return r
 
 
+def _mask8(mask):
+    m = (C.c_uint64 * 8)(*[int(v) for v in mask])
+    if len(mask) != 8:
+        raise ValueError("the Dirichlet mask has 8 entries")
+    return m
+
+
+def _coarse_size(n_fine: int) -> int:
+    side = int(round(n_fine ** 0.5))
+    return ((side - 1) // 2 + 1) ** 2
+
+
+class Prolongation:
+    """Prolongation<tags::GPU::CUDA, methods::NONE>::value(fine, coarse, mask) -- the matrix-free
+    bilinear prolongation of a (2^k + 1)^2 grid (honei/math/prolongation.hh:42-139) followed by
+    ApplyDirichletBoundaries with the 8-entry mask."""
+
+    @staticmethod
+    def value(fine: torch.Tensor, coarse: torch.Tensor, mask, ctx: Context | None = None):
+        if coarse.numel() != _coarse_size(fine.numel()):
+            raise VectorSizeDoesNotMatch(coarse.numel(), _coarse_size(fine.numel()))
+        ctx = ctx or default_context()
+        fn = getattr(lib(), f"hb_prolongate_{_SUF[fine.dtype]}")
+        check(fn(ctx.handle, fine.numel(), _vec(fine, fine.dtype, "fine"), _vec(coarse, fine.dtype, "coarse"),
+                 _mask8(mask)), "Prolongation<NONE>", ctx.handle)
+        return fine
+
+
+class Restriction:
+    """Restriction<tags::GPU::CUDA, methods::NONE>::value(coarse, fine, mask) -- the matrix-free
+    full-weighting restriction (honei/math/restriction.hh:41-170) followed by
+    ApplyDirichletBoundaries with the 8-entry mask."""
+
+    @staticmethod
+    def value(coarse: torch.Tensor, fine: torch.Tensor, mask, ctx: Context | None = None):
+        if coarse.numel() != _coarse_size(fine.numel()):
+            raise VectorSizeDoesNotMatch(coarse.numel(), _coarse_size(fine.numel()))
+        ctx = ctx or default_context()
+        fn = getattr(lib(), f"hb_restrict_{_SUF[fine.dtype]}")
+        check(fn(ctx.handle, fine.numel(), _vec(coarse, fine.dtype, "coarse"), _vec(fine, fine.dtype, "fine"),
+                 _mask8(mask)), "Restriction<NONE>", ctx.handle)
+        return coarse
+
+
 def _pair(x, y):
     if x.numel() != y.numel():
         raise VectorSizeDoesNotMatch(y.numel(), x.numel())

@@ -173,6 +173,19 @@ int hb_q1band_fill_poisson(hb_context *ctx, int64_t M, hb_q1band *A);
  * (HB_ERR_UNSUPPORTED otherwise); E->dtype == A->dtype. */
 int hb_q1band_from_ell(hb_context *ctx, const hb_ell *E, hb_q1band *A);
 
+/* Matrix-free geometric transfers of (2^k + 1)^2 grids: Prolongation<Tag, methods::NONE>
+ * ::value(fine, coarse, mask, prolmat) (honei/math/prolongation.hh:42-139) and
+ * Restriction<Tag, methods::NONE>::value(coarse, fine, mask, resmat) (honei/math/
+ * restriction.hh:41-170), each followed by ApplyDirichletBoundaries with the host array
+ * mask[8] (corners bottom-left, bottom-right, top-right, top-left, edges bottom, right, top,
+ * left; 2 = zero those nodes).  n_fine = Mf^2 with Mf odd (HB_ERR_UNSUPPORTED otherwise); the
+ * coarse vector has ((Mf - 1) / 2 + 1)^2 entries.  Bit-identical to tags::CPU: every node
+ * replays the reference's sequence of += updates, evaluated in double and stored as T. */
+int hb_prolongate_f64(hb_context *ctx, int64_t n_fine, double *fine, const double *coarse, const uint64_t *mask);
+int hb_prolongate_f32(hb_context *ctx, int64_t n_fine, float *fine, const float *coarse, const uint64_t *mask);
+int hb_restrict_f64(hb_context *ctx, int64_t n_fine, double *coarse, const double *fine, const uint64_t *mask);
+int hb_restrict_f32(hb_context *ctx, int64_t n_fine, float *coarse, const float *fine, const uint64_t *mask);
+
 /* Host scalar results (synchronous, like the reference's value-returning operators).
  * DotProduct<tags::GPU::CUDA>::value, honei/la/dot_product.hh:358-360 (replaces
  * cuda_dot_product_two_{float,double}, honei/backends/cuda/dot_product.cu:77-155);

@@ -129,6 +129,26 @@ class Oracle:
         self.lib.ora_q1band_poisson_f64(_u64(M * M), bp)
         return out
 
+    def prolongate(self, coarse, mask, n_fine):
+        """Prolongation<methods::NONE>: the fine vector (n_fine entries) from `coarse`."""
+        coarse = np.ascontiguousarray(coarse)
+        fine = np.zeros(n_fine, coarse.dtype)
+        m = np.ascontiguousarray(mask, np.uint64)
+        getattr(self.lib, f"ora_prolongate_{self._suffix(coarse.dtype)}")(_u64(n_fine), _ptr(fine), _ptr(coarse),
+                                                                          _ptr(m))
+        return fine
+
+    def restrict(self, fine, mask):
+        """Restriction<methods::NONE>: the coarse vector of `fine`."""
+        fine = np.ascontiguousarray(fine)
+        side = int(round(np.sqrt(len(fine))))
+        nc = ((side - 1) // 2 + 1) ** 2
+        coarse = np.zeros(nc, fine.dtype)
+        m = np.ascontiguousarray(mask, np.uint64)
+        getattr(self.lib, f"ora_restrict_{self._suffix(fine.dtype)}")(_u64(len(fine)), _ptr(coarse), _ptr(fine),
+                                                                       _ptr(m))
+        return coarse
+
     def dot(self, x, y):
         x = np.ascontiguousarray(x)
         y = np.ascontiguousarray(y, x.dtype)
@@ -363,6 +383,28 @@ class Reference:
         Arl = np.zeros(rows, np.uint64)
         self._check(self.lib.ref_read_ell_f64(p, info, _ptr(Aj), _ptr(Ax), _ptr(Arl)))
         return EllMatrix(rows, cols, stride, ncpr, T, Aj, Ax, Arl, nnz)
+
+    def prolongate(self, coarse, mask, n_fine):
+        coarse = np.ascontiguousarray(coarse)
+        s = "f64" if coarse.dtype == np.float64 else "f32"
+        fine = np.zeros(n_fine, coarse.dtype)
+        m = np.ascontiguousarray(mask, np.uint64)
+        f = getattr(self.lib, f"ref_prolongate_{s}")
+        f.argtypes = [_c.c_ulong, _vp, _vp, _c.c_ulong, _vp]
+        self._check(f(n_fine, _ptr(fine), _ptr(coarse), len(coarse), _ptr(m)))
+        return fine
+
+    def restrict(self, fine, mask):
+        fine = np.ascontiguousarray(fine)
+        s = "f64" if fine.dtype == np.float64 else "f32"
+        side = int(round(np.sqrt(len(fine))))
+        nc = ((side - 1) // 2 + 1) ** 2
+        coarse = np.zeros(nc, fine.dtype)
+        m = np.ascontiguousarray(mask, np.uint64)
+        f = getattr(self.lib, f"ref_restrict_{s}")
+        f.argtypes = [_c.c_ulong, _vp, _vp, _c.c_ulong, _vp]
+        self._check(f(len(fine), _ptr(coarse), _ptr(fine), nc, _ptr(m)))
+        return coarse
 
     def read_mtx(self, path):
         """MatrixIO<io_formats::MTX>::read_matrix -> SparseMatrixELL (the mtxtoell client)."""

@@ -511,3 +511,89 @@ void ora_q1band_poisson_f64(uint64_t n, double *const *band)
         band[4][i - 1] = unit ? 1.0 : 8.0 / 3.0;
     }
 }
+
+/* ---- Geometric transfers ------------------------------------------------------------------
+ * A literal restatement of the reference loops (prolongation.hh:46-139, restriction.hh:45-170,
+ * apply_dirichlet_boundaries.hh): same visiting order, every += evaluated in double (the
+ * literals 0.5 / 0.25 are double) and stored back as DT. */
+#define ORA_DIRICHLET(SUF, DT)                                                                  \
+static void dirichlet_##SUF(uint64_t N, DT *g, const uint64_t *mask)                            \
+{                                                                                               \
+    const uint64_t M = (uint64_t)sqrt((double)N);                                               \
+    if (mask[0] == 2) g[0] = 0;                                                                 \
+    if (mask[1] == 2) g[M - 1] = 0;                                                             \
+    if (mask[2] == 2) g[N - 1] = 0;                                                             \
+    if (mask[3] == 2) g[N - M] = 0;                                                             \
+    if (mask[4] == 2) for (uint64_t i = 1; i < M - 1; ++i) g[i] = 0;                            \
+    if (mask[5] == 2) for (uint64_t i = 2 * M - 1; i < N - M; i += M) g[i] = 0;                 \
+    if (mask[6] == 2) for (uint64_t i = N - M + 1; i < N - 1; ++i) g[i] = 0;                    \
+    if (mask[7] == 2) for (uint64_t i = M; i < N - M; i += M) g[i] = 0;                         \
+}
+ORA_DIRICHLET(f64, double)
+ORA_DIRICHLET(f32, float)
+
+#define ORA_TRANSFER(SUF, DT)                                                                   \
+void ora_prolongate_##SUF(uint64_t n_fine, DT *fine, const DT *coarse, const uint64_t *mask)   \
+{                                                                                               \
+    const uint64_t nxf = (uint64_t)sqrt((double)n_fine) - 1, nxc = nxf / 2, nyf = nxf + 1,     \
+                   nyc = nxc + 1, istep = 2 * nyf;                                              \
+    for (uint64_t i = 0; i < n_fine; ++i) fine[i] = 0;                                          \
+    for (uint64_t i = 1; i <= nyc; ++i)                                                         \
+        for (uint64_t j = 0, k = 0; j < nyc; ++j, k += 2)                                       \
+            fine[istep * (i - 1) + k] = coarse[i + nxc * (i - 1) - 1 + j];                      \
+    for (uint64_t i = 1; i <= nxc; ++i) {                                                       \
+        uint64_t a = 2 * i;                                                                     \
+        for (uint64_t j = 0; j < nyc; ++j) {                                                    \
+            fine[a - 1 + j * istep] = (DT)((double)fine[a - 1 + j * istep] + (double)coarse[i - 1 + j * nyc] * 0.5); \
+            fine[a - 1 + j * istep] = (DT)((double)fine[a - 1 + j * istep] + (double)coarse[i + j * nyc] * 0.5);     \
+        }                                                                                       \
+        a = nyf + 1 + (i - 1) * istep;                                                          \
+        for (uint64_t j = 0; j < nyc; ++j) {                                                    \
+            fine[a - 1 + j * 2] = (DT)((double)fine[a - 1 + j * 2] + (double)fine[a - nyf - 1 + j * 2] * 0.5);     \
+            fine[a - 1 + j * 2] = (DT)((double)fine[a - 1 + j * 2] + (double)fine[a + nyf - 1 + j * 2] * 0.5);     \
+        }                                                                                       \
+    }                                                                                           \
+    for (uint64_t i = 1; i <= nxc; ++i) {                                                       \
+        const uint64_t a = nxf + 3 + (i - 1) * istep;                                           \
+        for (uint64_t j = 0; j < nxc; ++j) {                                                    \
+            DT *f = &fine[a - 1 + j * 2];                                                       \
+            *f = (DT)((double)*f + (double)fine[a - nxf - 3 + j * 2] * 0.25);                   \
+            *f = (DT)((double)*f + (double)fine[a - nxf - 1 + j * 2] * 0.25);                   \
+            *f = (DT)((double)*f + (double)fine[a + nxf - 1 + j * 2] * 0.25);                   \
+            *f = (DT)((double)*f + (double)fine[a + nxf + 1 + j * 2] * 0.25);                   \
+        }                                                                                       \
+    }                                                                                           \
+    dirichlet_##SUF(n_fine, fine, mask);                                                        \
+}                                                                                               \
+void ora_restrict_##SUF(uint64_t n_fine, DT *coarse, const DT *fine, const uint64_t *mask)     \
+{                                                                                               \
+    const uint64_t nxf = (uint64_t)sqrt((double)n_fine) - 1, nxc = nxf / 2, nyf = nxf + 1,     \
+                   nyc = nxc + 1, istep = 2 * nyf;                                              \
+    for (uint64_t i = 1; i <= nyc; ++i)                                                         \
+        for (uint64_t j = 0, k = 0; j < nyc; ++j, k += 2)                                       \
+            coarse[1 + nyc * (i - 1) - 1 + j] = fine[2 * nyf * (i - 1) + k];                    \
+    for (uint64_t i = 1; i <= nxc; ++i) {                                                       \
+        uint64_t ia = 1 + nyf + 2 * nyf * (i - 1), ia1 = 1 + nyc * i;                           \
+        for (uint64_t j = 0; j < nyc; ++j)                                                      \
+            coarse[ia1 - 1 + j] = (DT)((double)coarse[ia1 - 1 + j] + 0.5 * (double)fine[ia - 1 + j * 2]);          \
+        ia1 -= nyc;                                                                             \
+        for (uint64_t j = 0; j < nyc; ++j)                                                      \
+            coarse[ia1 - 1 + j] = (DT)((double)coarse[ia1 - 1 + j] + 0.5 * (double)fine[ia - 1 + j * 2]);          \
+        for (uint64_t j = 0; j < nyc; ++j)                                                      \
+            coarse[i - 1 + j * nyc] = (DT)((double)coarse[i - 1 + j * nyc] + 0.5 * (double)fine[2 * i - 1 + j * istep]); \
+        for (uint64_t j = 0; j < nyc; ++j)                                                      \
+            coarse[i + j * nyc] = (DT)((double)coarse[i + j * nyc] + 0.5 * (double)fine[2 * i - 1 + j * istep]);   \
+        ++ia;                                                                                   \
+        for (uint64_t j = 0; j < nxc; ++j)                                                      \
+            coarse[ia1 - 1 + j] = (DT)((double)coarse[ia1 - 1 + j] + 0.25 * (double)fine[ia - 1 + j * 2]);         \
+        for (uint64_t j = 0; j < nxc; ++j)                                                      \
+            coarse[ia1 + j] = (DT)((double)coarse[ia1 + j] + 0.25 * (double)fine[ia - 1 + j * 2]);                 \
+        for (uint64_t j = 0; j < nxc; ++j)                                                      \
+            coarse[nyc * i + j] = (DT)((double)coarse[nyc * i + j] + 0.25 * (double)fine[ia - 1 + j * 2]);         \
+        for (uint64_t j = 0; j < nxc; ++j)                                                      \
+            coarse[1 + nyc * i + j] = (DT)((double)coarse[1 + nyc * i + j] + 0.25 * (double)fine[ia - 1 + j * 2]); \
+    }                                                                                           \
+    dirichlet_##SUF(nyc * nyc, coarse, mask);                                                   \
+}
+ORA_TRANSFER(f64, double)
+ORA_TRANSFER(f32, float)

@@ -40,6 +40,16 @@ void   ora_q1band_spmv_f64(uint64_t n, const double *const *band, const double *
 void   ora_q1band_spmv_f32(uint64_t n, const float *const *band, const float *x, float *y);
 void   ora_q1band_defect_f64(uint64_t n, const double *const *band, const double *b, const double *x, double *r);
 void   ora_q1band_defect_f32(uint64_t n, const float *const *band, const float *b, const float *x, float *r);
+/* Geometric transfers of (2^k + 1)^2 grids: Prolongation<Tag, methods::NONE>
+ * (honei/math/prolongation.hh:42-139) and Restriction<Tag, methods::NONE>
+ * (honei/math/restriction.hh:41-170), each followed by ApplyDirichletBoundaries
+ * (honei/math/apply_dirichlet_boundaries.hh) with the 8-entry mask (2 = Dirichlet: zero the
+ * corner / edge).  n_fine = fine nodes; the coarse grid has (sqrt(n_fine) - 1) / 2 + 1 nodes per
+ * side.  Arithmetic in double, stored as DT (the reference's 0.5 / 0.25 literals are double). */
+void   ora_prolongate_f64(uint64_t n_fine, double *fine, const double *coarse, const uint64_t *mask);
+void   ora_prolongate_f32(uint64_t n_fine, float *fine, const float *coarse, const uint64_t *mask);
+void   ora_restrict_f64(uint64_t n_fine, double *coarse, const double *fine, const uint64_t *mask);
+void   ora_restrict_f32(uint64_t n_fine, float *coarse, const float *fine, const uint64_t *mask);
 /* FillMatrix<POISSON, DIRICHLET_0> on the banded form (honei/math/fill_matrix.hh:41-77). */
 void   ora_q1band_poisson_f64(uint64_t n, double *const *band);
 double ora_dot_f64(uint64_t n, const double *x, const double *y);

@@ -444,6 +444,64 @@ extern "C"
         });
     }
 
+    // Prolongation / Restriction<tags::CPU, methods::NONE> (prolongation.hh:42-139,
+    // restriction.hh:41-170) on plain arrays; the unused matrix argument is a dummy.
+    int ref_prolongate_f64(unsigned long n_fine, double * fine, const double * coarse, unsigned long n_coarse,
+            const uint64_t * mask)
+    {
+        return guarded([&]() {
+            DenseVector<double> f(n_fine, 0.), c(n_coarse);
+            DenseVector<unsigned long> m(8);
+            for (unsigned long i(0) ; i < n_coarse ; ++i) c[i] = coarse[i];
+            for (int i(0) ; i < 8 ; ++i) m[i] = mask[i];
+            int unused(0);
+            Prolongation<tags::CPU, methods::NONE>::value(f, c, m, unused);
+            dv_to(f, fine);
+        });
+    }
+
+    int ref_restrict_f64(unsigned long n_fine, double * coarse, const double * fine, unsigned long n_coarse,
+            const uint64_t * mask)
+    {
+        return guarded([&]() {
+            DenseVector<double> f(n_fine), c(n_coarse, 0.);
+            DenseVector<unsigned long> m(8);
+            for (unsigned long i(0) ; i < n_fine ; ++i) f[i] = fine[i];
+            for (int i(0) ; i < 8 ; ++i) m[i] = mask[i];
+            int unused(0);
+            Restriction<tags::CPU, methods::NONE>::value(c, f, m, unused);
+            dv_to(c, coarse);
+        });
+    }
+
+    int ref_prolongate_f32(unsigned long n_fine, float * fine, const float * coarse, unsigned long n_coarse,
+            const uint64_t * mask)
+    {
+        return guarded([&]() {
+            DenseVector<float> f(n_fine, 0.f), c(n_coarse);
+            DenseVector<unsigned long> m(8);
+            for (unsigned long i(0) ; i < n_coarse ; ++i) c[i] = coarse[i];
+            for (int i(0) ; i < 8 ; ++i) m[i] = mask[i];
+            int unused(0);
+            Prolongation<tags::CPU, methods::NONE>::value(f, c, m, unused);
+            dv_to(f, fine);
+        });
+    }
+
+    int ref_restrict_f32(unsigned long n_fine, float * coarse, const float * fine, unsigned long n_coarse,
+            const uint64_t * mask)
+    {
+        return guarded([&]() {
+            DenseVector<float> f(n_fine), c(n_coarse, 0.f);
+            DenseVector<unsigned long> m(8);
+            for (unsigned long i(0) ; i < n_fine ; ++i) f[i] = fine[i];
+            for (int i(0) ; i < 8 ; ++i) m[i] = mask[i];
+            int unused(0);
+            Restriction<tags::CPU, methods::NONE>::value(c, f, m, unused);
+            dv_to(c, coarse);
+        });
+    }
+
     // MatrixMarket file -> SparseMatrix -> SparseMatrixELL through the reference (mtxtoell.cc).
     int ref_read_mtx_f64(const char * path, unsigned long * info, uint64_t * Aj, double * Ax, uint64_t * Arl)
     {

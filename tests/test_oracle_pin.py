@@ -224,3 +224,44 @@ def test_oracle_cg_var_live_against_reference(oracle, reference):
         xo2, uo2 = oracle.cg_var(A, Pm, b, max_iters=700, eps=eps)
         xr2, ur2, _ = reference.cg_var(A, Pm, b, max_iters=700, eps=eps)
         assert uo2 == ur2 and np.array_equal(xo2, xr2) and np.array_equal(xo2, xo)
+
+
+# ---- geometric transfers (Prolongation / Restriction<methods::NONE>) ---------------------
+MASKS = [[2] * 8, [0] * 8, [2, 0, 2, 0, 2, 2, 0, 0], [0, 2, 0, 2, 0, 0, 2, 2]]
+
+
+def test_oracle_geometric_transfers_match_reference(oracle, reference):
+    rng = np.random.default_rng(8)
+    for side in (3, 5, 9, 17, 33, 65):
+        nf, nc = side * side, ((side - 1) // 2 + 1) ** 2
+        for dt in (np.float64, np.float32):
+            for mask in MASKS:
+                c = rng.uniform(-1, 1, nc).astype(dt)
+                f = rng.uniform(-1, 1, nf).astype(dt)
+                assert np.array_equal(oracle.prolongate(c, mask, nf), reference.prolongate(c, mask, nf)), (side, dt)
+                assert np.array_equal(oracle.restrict(f, mask), reference.restrict(f, mask)), (side, dt)
+
+
+def test_geometric_transfers_are_the_bilinear_pair():
+    """Away from the masked boundary the geometric prolongation is the bilinear interpolation of
+    the PROLMAT matrices, and the restriction is its transpose."""
+    from oracle.bindings import Oracle
+    O = Oracle()
+    side = 17
+    nf, ncs = side * side, (side - 1) // 2 + 1
+    nfp, ncp, ip, ix, dv = P.prolongation_csr(Mf=side)
+    Pm = np.zeros((nfp, ncp))
+    for r in range(nfp):
+        Pm[r, ix[ip[r]:ip[r + 1]]] = dv[ip[r]:ip[r + 1]]
+    c = P.uniform_vector(ncs * ncs, 1)
+    f = P.uniform_vector(nf, 2)
+    mask = [2] * 8
+    assert np.allclose(O.prolongate(c, mask, nf), Pm @ c, rtol=0, atol=1e-15)
+    interior = np.ones(ncs * ncs, bool)
+    for k in range(ncs * ncs):
+        i, j = divmod(k, ncs)
+        interior[k] = 0 < i < ncs - 1 and 0 < j < ncs - 1
+    fi = f.copy()
+    fr = np.arange(nf)
+    fi[(fr // side == 0) | (fr // side == side - 1) | (fr % side == 0) | (fr % side == side - 1)] = 0
+    assert np.allclose(O.restrict(fi, mask)[interior], (Pm.T @ fi)[interior], rtol=0, atol=1e-14)
