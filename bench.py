@@ -599,7 +599,7 @@ def run_ours(args):
                 "p99_ms": round(lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))], 3)}
 
     cg_cluster = bench_cg_cluster(ctx)
-    batch_extra = None if args.no_batch else bench_batch(la, ctx)
+    batch_extra = None if args.no_batch else bench_batch(la, ctx, n_systems=args.batch_systems)
     mg_extra = None if args.no_mg else bench_mg(la, ctx, cpu=(ws == 1 and not args.no_cpu_baseline))
     ir_extra = None if args.no_mg else bench_ir(la, ctx)
     serve_extra = None if (args.no_serve or rank != 0 and ws > 1) else bench_serve(args.serve_requests)
@@ -647,6 +647,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-system batched workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream workload")
+    ap.add_argument("--batch-systems", type=int, default=512, help="systems in the batched workload")
     ap.add_argument("--no-mg", action="store_true", help="skip the 2049^2 MG and mixed-precision workloads")
     ap.add_argument("--serve-requests", type=int, default=120, help="requests in the serving sample")
     args = ap.parse_args()
