@@ -189,13 +189,26 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
 // ---------------------------------------------------------------------------------------
 constexpr int SMALL_GROUPS = 256;
 
+// Block-wide fixed-order total, identical in every thread.  A single-warp block (systems of at
+// most 128 rows, e.g. the 9^2 coarse grid) reduces with shuffles only: the block tree of one warp
+// is the warp tree plus exact zeros, so both paths give the same value.
 template <typename T>
 __device__ __forceinline__ T block_total(T v, T *red, T *bcast)
 {
+    if (blockDim.x == 32) {
+        v = hbd::warp_sum(v);
+        return __shfl_sync(0xffffffffu, v, 0);
+    }
     v = hbd::block_sum(v, red);
     if (threadIdx.x == 0) *bcast = v;
     __syncthreads();
     return *bcast;
+}
+
+__device__ __forceinline__ void block_sync()
+{
+    if (blockDim.x == 32) __syncwarp();
+    else __syncthreads();
 }
 
 template <typename T, int KT>
@@ -253,7 +266,7 @@ __global__ void __launch_bounds__(SMALL_GROUPS) cg_small_kernel(CGParams<T> P)
         x[i] = (own && r0 + i < rows) ? P.x_user[r0 + i] : T(0);
         if (own) sp[r0 + i] = x[i];
     }
-    __syncthreads();
+    block_sync();
     // r = b - A x, alpha = r.r
     T acc = T(0);
     product(v);
@@ -272,12 +285,15 @@ __global__ void __launch_bounds__(SMALL_GROUPS) cg_small_kernel(CGParams<T> P)
     int64_t it = 0, used = 0;
     while (it < P.max_iters) {
         const bool first = (it == 0);
+        // every lane's gathers of the previous p are done before p is rewritten (the block
+        // path's reductions end in __syncthreads; shuffles do not order shared memory)
+        if (blockDim.x == 32) __syncwarp();
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             p[i] = first ? r[i] : add(mul(p[i], beta), r[i]);
             if (own) sp[r0 + i] = p[i];
         }
-        __syncthreads();
+        block_sync();
         product(v);
         acc = T(0);
 #pragma unroll
