@@ -121,10 +121,8 @@ class ClockSampler:
 
 
 def dist_setup():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from honei_b200 import replicas
+    return replicas.env()
 
 
 # ---------------------------------------------------------------------------------------
@@ -477,20 +475,17 @@ def bench_serve(n_requests=120, rate=150.0, seed=11):
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
     from honei_b200 import la, problems as P
+    from honei_b200 import replicas
 
-    ws, rank, local = dist_setup()
+    _, _, local = dist_setup()
     torch.cuda.set_device(local)
-    if ws > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    ws, rank, local = replicas.init("nccl", timeout_s=120, device=torch.device("cuda", local))
     ctx = la.Context(local)
     stream = torch.cuda.current_stream()
 
     def barrier():
-        if ws > 1:
-            dist.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
 
     # ---- SpMV workload (replica per rank, assembled on the device) ----
@@ -518,10 +513,7 @@ def run_ours(args):
         torch.cuda.synchronize()
     launches = ctx.launches() - l0
     ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = replicas.max_over_ranks(ms)
     apps = args.steps * SPMV_PER_STEP
     per_launch_s = ms / 1e3 / apps
     value = ws * nbytes * apps / (ms_max / 1e3) / 1e9
@@ -549,10 +541,8 @@ def run_ours(args):
         e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    ems = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(ems, op=dist.ReduceOp.MAX)
-    e2e_value = ws * nbytes * apps / (float(ems.item()) / 1e3) / 1e9
+    ems = replicas.max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = ws * nbytes * apps / (ems / 1e3) / 1e9
 
     # ---- FP32 SpMV on the same matrix (extra) ----
     A32 = A.to_float(ctx=ctx)
@@ -633,8 +623,7 @@ def run_ours(args):
         }
         print(json.dumps(line), flush=True)
     barrier()
-    if ws > 1:
-        dist.destroy_process_group()
+    replicas.finish()
     return 0
 
 
