@@ -92,6 +92,26 @@ int hb_mg_set_dense_coarse(hb_mg *mg, void *inv);
 int hb_mg_pcg_f32_graph(hb_mg *mg, cudaStream_t capture_stream, const float *b, float *x, float eps, int64_t max_iters,
                         float *work, cudaGraphExec_t *graph, int check_every, int64_t *used);
 
+// Device pointers of a served system (hb_q1) for kernels that run its solve themselves (the
+// batched served solve): levels coarsest first, P32[l] / R32[l] transfer between levels l and
+// l + 1, per-level FP32 vectors of the MG hierarchy (Jacobi diagonal, coarse solution c and
+// right-hand side d, smoother ping-pong xt, defect store), the finest FP64 matrix and the
+// refinement / PCG vectors.
+constexpr int HB_Q1_MAXL = 16;
+struct hb_q1_view {
+    int L = 0;
+    hb_ell A64{};
+    hb_ell A32[HB_Q1_MAXL], P32[HB_Q1_MAXL], R32[HB_Q1_MAXL];
+    float *jac[HB_Q1_MAXL], *c[HB_Q1_MAXL], *d[HB_Q1_MAXL], *store[HB_Q1_MAXL], *xt[HB_Q1_MAXL];
+    const float *coarse_inv = nullptr;
+    double *r64 = nullptr;
+    float *b32 = nullptr, *x32 = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *v = nullptr;
+    int n_pre = 2, n_post = 2;
+    hb_context *ctx = nullptr;
+};
+int hb_mg_view(const hb_mg *mg, hb_q1_view *out);
+int hb_q1_view_of(const hb_q1 *q, hb_q1_view *out);
+
 // --------------------------------------------------------------------------------------
 // Device helpers
 // --------------------------------------------------------------------------------------

@@ -254,6 +254,22 @@ int hb_mg_pcg_f32(hb_mg *mg, const float *b, float *x, float eps, int64_t max_it
     return HB_OK;
 }
 
+int hb_mg_view(const hb_mg *mg, hb_q1_view *out)
+{
+    if (!mg || !out || mg->L > HB_Q1_MAXL || mg->dtype != HB_F32) return HB_ERR_INVALID;
+    for (int l = 0; l < mg->L; ++l) {
+        out->jac[l] = tp<float>(mg->P[l]);
+        out->c[l] = tp<float>(mg->c[l]);
+        out->d[l] = tp<float>(mg->d[l]);
+        out->store[l] = tp<float>(mg->store[l]);
+        out->xt[l] = tp<float>(mg->xt[l]);
+    }
+    out->n_pre = (int)mg->prm.n_pre;
+    out->n_post = (int)mg->prm.n_post;
+    out->coarse_inv = tp<const float>(mg->coarse_inv);
+    return HB_OK;
+}
+
 int hb_mg_finest(hb_mg *mg, hb_ell *A)
 {
     *A = mg->A[mg->L - 1];

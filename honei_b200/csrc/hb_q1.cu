@@ -503,6 +503,37 @@ int hb_q1_level(const hb_q1 *q, int level, hb_ell *A64, hb_ell *A32, hb_ell *P32
     return HB_OK;
 }
 
+}  // extern "C"
+
+int hb_q1_view_of(const hb_q1 *q, hb_q1_view *out)
+{
+    if (!q || !out || q->L < 1 || q->L > HB_Q1_MAXL) return HB_ERR_INVALID;
+    out->L = q->L;
+    out->ctx = q->ctx;
+    out->A64 = q->A64[q->L - 1];
+    for (int l = 0; l < q->L; ++l) {
+        out->A32[l] = q->A32[l];
+        if (l + 1 < q->L) {
+            out->P32[l] = q->P32[l];
+            out->R32[l] = q->R32[l];
+        }
+    }
+    int st = hb_mg_view(q->mg, out);
+    if (st) return st;
+    if (!out->coarse_inv) return HB_ERR_INVALID;
+    const int64_t ldn = q->A64[q->L - 1].ld;
+    out->r64 = q->r64;
+    out->b32 = q->b32;
+    out->x32 = q->x32;
+    out->r = q->pcg_work;
+    out->z = q->pcg_work + ldn;
+    out->p = q->pcg_work + 2 * ldn;
+    out->v = q->pcg_work + 3 * ldn;
+    return HB_OK;
+}
+
+extern "C" {
+
 int hb_q1_solve(hb_q1 *q, const double *b, double *x, double eps, double inner_eps, int64_t max_outer,
                 int64_t max_inner, hb_batch_result *info)
 {

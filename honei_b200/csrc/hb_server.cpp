@@ -49,7 +49,7 @@ struct hb_server {
     std::chrono::steady_clock::time_point t0;
     std::mutex mu;
     std::condition_variable cv_pending, cv_work, cv_mem, cv_done;
-    std::deque<Item *> pending, small_q, large_q;
+    std::deque<Item *> pending, small_q, mid_q, large_q;
     std::vector<hb_completion> done;
     int64_t in_use = 0, peak = 0, submitted = 0, completed = 0;
     bool stop = false;
@@ -210,6 +210,9 @@ void admit_loop(hb_server *s)
         } else if (it->r.M <= s->p.small_max_side) {
             it->path = HB_PATH_BATCH;
             s->small_q.push_back(it);
+        } else if (it->r.M <= s->p.mid_max_side) {
+            it->path = HB_PATH_MGBATCH;
+            s->mid_q.push_back(it);
         } else {
             it->path = HB_PATH_MGPCG;
             s->large_q.push_back(it);
@@ -370,6 +373,91 @@ void small_loop(hb_server *s)
     }
 }
 
+// Mid-size grids: every waiting request (up to max_batch) gets its hb_q1 (device-built
+// hierarchy) and all of them are solved in one batched MG-PCG cluster launch.
+void mid_loop(hb_server *s)
+{
+    Worker w;
+    const int init = w.init(s->p.device);
+    while (true) {
+        std::vector<Item *> batch;
+        {
+            std::unique_lock<std::mutex> l(s->mu);
+            s->cv_work.wait(l, [&] { return s->stop || !s->mid_q.empty(); });
+            if (s->stop && s->mid_q.empty()) return;
+            while (!s->mid_q.empty() && (int)batch.size() < std::max(1, s->p.max_batch)) {
+                batch.push_back(s->mid_q.front());
+                s->mid_q.pop_front();
+            }
+        }
+        if (init) {
+            for (Item *it : batch) s->fail(it, init);
+            continue;
+        }
+        const int64_t count = (int64_t)batch.size();
+        std::vector<DeviceSystem> ds(count, DeviceSystem{w.ctx});
+        std::vector<hb_q1 *> qs(count, nullptr);
+        std::vector<int> st(count, HB_OK);
+        for (int64_t i = 0; i < count; ++i) {
+            const hb_request &r = batch[i]->r;
+            st[i] = ds[i].inputs(r, false, false);
+            if (!st[i]) st[i] = hb_q1_create(w.ctx, r.M, ds[i].coef, &qs[i]);
+            hb_ell A{};
+            if (!st[i]) {
+                int nl = 0;
+                hb_q1_levels(qs[i], &nl, nullptr);
+                st[i] = hb_q1_level(qs[i], nl - 1, &A, nullptr, nullptr, nullptr);
+            }
+            if (!st[i]) st[i] = ds[i].rhs(r, A);
+            if (!st[i] && cudaMemsetAsync(ds[i].x, 0, r.M * r.M * 8, w.stream) != cudaSuccess) st[i] = HB_ERR_CUDA;
+        }
+        std::vector<int64_t> live;
+        std::vector<hb_q1 *> lq;
+        std::vector<const double *> lb;
+        std::vector<double *> lx;
+        for (int64_t i = 0; i < count; ++i)
+            if (!st[i]) { live.push_back(i); lq.push_back(qs[i]); lb.push_back(ds[i].b); lx.push_back(ds[i].x); }
+        std::vector<hb_batch_result> res(live.size());
+        int bst = HB_OK;
+        if (!live.empty())
+            bst = hb_q1_batch_solve(w.ctx, lq.data(), lb.data(), lx.data(), (int64_t)live.size(), s->p.eps,
+                                    s->p.inner_eps, 50, 2000, &s->p.mid_cfg, res.data());
+        for (size_t k = 0; k < live.size(); ++k) {
+            const int64_t i = live[k];
+            if (bst) { st[i] = bst; continue; }
+            const hb_request &r = batch[i]->r;
+            if (cudaMemcpyAsync(r.x, ds[i].x, r.M * r.M * 8, cudaMemcpyDeviceToHost, w.stream) != cudaSuccess)
+                st[i] = HB_ERR_CUDA;
+        }
+        for (hb_q1 *q : qs)
+            if (q) hb_q1_destroy(q);
+        for (auto &d : ds) d.release();
+        if (cudaStreamSynchronize(w.stream) != cudaSuccess) cudaGetLastError();
+        const double t = s->now();
+        size_t k = 0;
+        for (int64_t i = 0; i < count; ++i) {
+            hb_completion c{};
+            c.tag = batch[i]->r.tag;
+            c.path = HB_PATH_MGBATCH;
+            c.t_submit = batch[i]->t_submit;
+            c.t_admit = batch[i]->t_admit;
+            c.bytes = batch[i]->bytes;
+            c.t_done = t;
+            c.status = st[i];
+            if (k < live.size() && live[k] == i) {
+                if (!st[i]) {
+                    c.iterations = res[k].iterations;
+                    c.outer = res[k].outer;
+                    c.true_relres = res[k].true_relres;
+                    c.status = res[k].status;
+                }
+                ++k;
+            }
+            s->complete(batch[i], c);
+        }
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -386,6 +474,7 @@ int hb_server_create(const hb_server_params *params, hb_server **out)
     if (s->p.small_workers < 1) s->p.small_workers = 1;
     if (s->p.max_batch < 1) s->p.max_batch = 256;
     if (s->p.batch_cfg.cluster == 0) s->p.batch_cfg = hb_batch_config{2, 512, 0};
+    if (s->p.mid_cfg.cluster == 0) s->p.mid_cfg = hb_batch_config{16, 512, 0};
     s->t0 = std::chrono::steady_clock::now();
     s->admitter = std::thread(admit_loop, s);
     if (s->p.mode == HB_SERVE_PLAIN_CG64) {
@@ -393,6 +482,8 @@ int hb_server_create(const hb_server_params *params, hb_server **out)
     } else {
         for (int i = 0; i < s->p.large_workers; ++i) s->workers.emplace_back(large_loop, s);
         for (int i = 0; i < s->p.small_workers; ++i) s->workers.emplace_back(small_loop, s);
+        if (s->p.mid_max_side > s->p.small_max_side)
+            for (int i = 0; i < std::max(1, s->p.mid_workers); ++i) s->workers.emplace_back(mid_loop, s);
     }
     *out = s;
     return HB_OK;

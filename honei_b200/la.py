@@ -717,6 +717,33 @@ class Q1System:
         check(lib().hb_q1_levels(h, C.byref(nl), sides), "hb_q1_levels")
         self.sides = [sides[i] for i in range(nl.value)]
 
+    @staticmethod
+    def solve_batch(systems, bs, xs, eps=1e-8, inner_eps=1e-3, max_outer=50, max_inner=1000, cluster=8,
+                    threads=256, max_clusters=0, ctx: Context | None = None):
+        """hb_q1_batch_solve: every system (distinct Q1System objects) solved in one launch, one
+        thread-block cluster per system at a time; xs hold the initial guesses.  Returns one info
+        dict per system."""
+        from .batch import HbBatchConfig, HbBatchResult
+        ctx = ctx or default_context()
+        n = len(systems)
+        if not (n == len(bs) == len(xs)):
+            raise ValueError("one b and one x per system")
+        for q, b, x in zip(systems, bs, xs):
+            if b.numel() != q.M * q.M:
+                raise VectorSizeDoesNotMatch(b.numel(), q.M * q.M)
+            if x.numel() != q.M * q.M:
+                raise VectorSizeDoesNotMatch(x.numel(), q.M * q.M)
+        hs = (C.c_void_p * max(n, 1))(*[q.handle.value for q in systems])
+        bp = (C.c_void_p * max(n, 1))(*[_vec(b, torch.float64, "b") for b in bs])
+        xp = (C.c_void_p * max(n, 1))(*[_vec(x, torch.float64, "x") for x in xs])
+        res = (HbBatchResult * max(n, 1))()
+        cfg = HbBatchConfig(cluster, threads, max_clusters)
+        ctx.bind_stream()
+        check(lib().hb_q1_batch_solve(ctx.handle, hs, bp, xp, n, eps, inner_eps, max_outer, max_inner, C.byref(cfg),
+                                      res), "hb_q1_batch_solve", ctx.handle)
+        return [{"iterations": r.iterations, "outer": r.outer, "defect0": r.defect0, "defect": r.defect,
+                 "true_relres": r.true_relres, "status": r.status} for r in res[:n]]
+
     def level(self, l: int):
         """(A64, A32, P32, R32) device views of level l (P/R None on the finest level)."""
         e = [HbEll() for _ in range(4)]

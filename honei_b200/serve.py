@@ -25,14 +25,15 @@ from ._lib import HBError, lib, status_string
 from .batch import HbBatchConfig
 
 HB_SERVE_MIXED, HB_SERVE_PLAIN_CG64 = 0, 1
-PATHS = {0: "batch", 1: "mgpcg", 2: "cg64"}
+PATHS = {0: "batch", 1: "mgpcg", 2: "cg64", 3: "mgbatch"}
 
 
 class HbServerParams(C.Structure):
     _fields_ = [("mode", C.c_int32), ("device", C.c_int32), ("hbm_budget_bytes", C.c_int64),
                 ("large_workers", C.c_int32), ("small_workers", C.c_int32), ("small_max_side", C.c_int64),
                 ("max_batch", C.c_int32), ("pad_", C.c_int32), ("batch_cfg", HbBatchConfig),
-                ("eps", C.c_double), ("inner_eps", C.c_double)]
+                ("eps", C.c_double), ("inner_eps", C.c_double), ("mid_max_side", C.c_int64),
+                ("mid_workers", C.c_int32), ("pad2_", C.c_int32), ("mid_cfg", HbBatchConfig), ("pad3_", C.c_int32)]
 
 
 class HbRequest(C.Structure):
@@ -151,15 +152,17 @@ class Completion:
 
 
 class Server:
-    """Owns an ``hb_server``.  ``mode``: "mixed" (batched small grids + MG-PCG workers for large
-    ones) or "plain" (FP64 CG one request at a time).  ``budget_bytes`` bounds the estimated
+    """Owns an ``hb_server``.  ``mode``: "mixed" (batched small grids, optionally batched MG-PCG
+    cluster launches for grids up to ``mid_max_side``, MG-PCG workers for the large ones) or
+    "plain" (FP64 CG one request at a time).  ``budget_bytes`` bounds the estimated
     device bytes of the admitted requests; a request above the budget alone is refused at
     submit with HB_ERR_CAPACITY."""
 
     def __init__(self, mode: str = "mixed", budget_bytes: int = 64 << 30, large_workers: int = 8,
                  small_workers: int = 1, small_max_side: int = 96, max_batch: int = 256, cluster: int = 2,
                  threads: int = 512, max_clusters: int = 0, eps: float = 1e-8, inner_eps: float = 1e-3,
-                 device: int = 0, pinned: bool = True):
+                 device: int = 0, pinned: bool = True, mid_max_side: int = 300, mid_workers: int = 1,
+                 mid_cluster: int = 16, mid_threads: int = 512, mid_max_clusters: int = 0):
         self._lib = _register()
         prm = HbServerParams()
         prm.mode = {"mixed": HB_SERVE_MIXED, "plain": HB_SERVE_PLAIN_CG64}[mode]
@@ -172,6 +175,9 @@ class Server:
         prm.batch_cfg = HbBatchConfig(cluster, threads, max_clusters)
         prm.eps = eps
         prm.inner_eps = inner_eps
+        prm.mid_max_side = mid_max_side
+        prm.mid_workers = mid_workers
+        prm.mid_cfg = HbBatchConfig(mid_cluster, mid_threads, mid_max_clusters)
         self.mode = mode
         self.params = prm
         self.pinned = pinned

@@ -411,17 +411,28 @@ int hb_q1_level(const hb_q1 *q, int level, hb_ell *A64, hb_ell *A32, hb_ell *P32
 int hb_q1_solve(hb_q1 *q, const double *b, double *x, double eps, double inner_eps, int64_t max_outer,
                 int64_t max_inner, hb_batch_result *info);
 
+/* Batched served solves (no reference counterpart): count distinct hb_q1 systems, each with its
+ * own b[i] and x[i] (device, x holds x0), solved in one persistent launch with the algorithm of
+ * hb_q1_solve; one thread-block cluster (cfg->cluster CTAs of cfg->threads threads; NULL = 8 x
+ * 256) solves one system at a time, largest first, with cluster barriers between phases and
+ * DSMEM reductions.  The systems must be ready on ctx's stream (created on it, or synchronised).
+ * A system's result does not depend on the rest of the batch.  results[i] as hb_q1_solve's info. */
+int hb_q1_batch_solve(hb_context *ctx, hb_q1 *const *systems, const double *const *b, double *const *x, int64_t count,
+                      double eps, double inner_eps, int64_t max_outer, int64_t max_inner, const hb_batch_config *cfg,
+                      hb_batch_result *results);
+
 /* ------------------------------------------------------------------------------------------
  * Serving (no reference counterpart): a request loop that admits Q1 solve requests by an HBM
  * budget, keeps each admitted request's matrix, hierarchy and Krylov state on the device, and
- * serves them concurrently -- small grids in batched cluster launches (HB_BATCH_IR32), large
- * grids on MG-preconditioned mixed-precision workers (hb_q1_solve), each on its own stream --
+ * serves them concurrently -- small grids in batched cluster launches (HB_BATCH_IR32), mid-size
+ * grids in batched MG-preconditioned cluster launches (hb_q1_batch_solve), large grids on
+ * MG-preconditioned mixed-precision workers (hb_q1_solve), each on its own stream --
  * while new requests keep arriving (continuous batching).  A request's result does not depend
  * on what it was served with.  HB_SERVE_PLAIN_CG64 is the baseline on the same queue: one
  * request at a time, plain FP64 CG (hb_cg_f64) on the whole GPU.
  * ---------------------------------------------------------------------------------------- */
 enum { HB_SERVE_MIXED = 0, HB_SERVE_PLAIN_CG64 = 1 };
-enum { HB_PATH_BATCH = 0, HB_PATH_MGPCG = 1, HB_PATH_CG64 = 2 };
+enum { HB_PATH_BATCH = 0, HB_PATH_MGPCG = 1, HB_PATH_CG64 = 2, HB_PATH_MGBATCH = 3 };
 
 typedef struct {
     int32_t mode;               /* HB_SERVE_MIXED or HB_SERVE_PLAIN_CG64                      */
@@ -435,6 +446,12 @@ typedef struct {
     hb_batch_config batch_cfg;  /* cluster shape of the batched launches                       */
     double eps;                 /* target relative FP64 residual ||b - A x|| / ||b||           */
     double inner_eps;           /* FP32 inner tolerance per refinement step                    */
+    int64_t mid_max_side;       /* sides in (small_max_side, mid_max_side] take the batched
+                                   MG-PCG path (hb_q1_batch_solve); 0 = no such path           */
+    int32_t mid_workers;        /* concurrent batched MG-PCG launches (one stream each)        */
+    int32_t pad2_;
+    hb_batch_config mid_cfg;    /* cluster shape of the batched MG-PCG launches                */
+    int32_t pad3_;
 } hb_server_params;
 
 typedef struct {

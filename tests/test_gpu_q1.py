@@ -105,3 +105,74 @@ def test_served_solve_large_high_contrast(hb):
     rel = hb.Norm.value(r, root=True) / hb.Norm.value(b, root=True)
     assert rel < 1e-8 and info["outer"] <= 6 and info["iterations"] < 400, info
     q.close()
+
+
+def _batch_case(hb, sides, seed0=0):
+    systems, bs, xts = [], [], []
+    for k, M in enumerate(sides):
+        coef = torch.from_numpy(P.log_uniform_coef(M, 1e-2, 1e2, seed0 + k).ravel()).cuda()
+        q = hb.Q1System(M, coef)
+        xt = torch.from_numpy(P.uniform_vector(M * M, seed0 + k + 100)).cuda()
+        b = torch.empty_like(xt)
+        hb.Product.value(b, q.A, xt)
+        systems.append(q)
+        bs.append(b)
+        xts.append(xt)
+    return systems, bs, xts
+
+
+@pytest.mark.parametrize("cluster,threads", [(8, 256), (4, 512), (1, 256), (16, 256)])
+def test_batched_served_solve_matches_single(hb, cluster, threads):
+    """hb_q1_batch_solve runs hb_q1_solve's algorithm per cluster: same outer steps, inner
+    iterations within a few (only the dot products' summation order differs), FP64 target met."""
+    sides = [17, 33, 40, 64, 100, 129, 257]
+    systems, bs, xts = _batch_case(hb, sides)
+    xs = [torch.zeros_like(b) for b in bs]
+    infos = hb.Q1System.solve_batch(systems, bs, xs, eps=1e-8, cluster=cluster, threads=threads)
+    for q, b, x, xt, info in zip(systems, bs, xs, xts, infos):
+        x1 = torch.zeros_like(b)
+        ref = q.solve(b, x1, eps=1e-8)
+        r = torch.empty_like(b)
+        hb.Defect.value(r, b, q.A, x)
+        rel = hb.Norm.value(r, root=True) / hb.Norm.value(b, root=True)
+        assert info["status"] == 0 and rel < 1e-8 and abs(info["true_relres"] - rel) <= 1e-6 * rel + 1e-15, (q.M, info)
+        assert abs(info["outer"] - ref["outer"]) <= 1, (q.M, info, ref)
+        assert abs(info["iterations"] - ref["iterations"]) <= 0.1 * ref["iterations"] + 3, (q.M, info, ref)
+        assert float(torch.linalg.norm(x - x1) / torch.linalg.norm(x1)) < 1e-6
+    for q in systems:
+        q.close()
+
+
+def test_batched_served_solve_matches_oracle(hb, oracle):
+    M = 64
+    systems, bs, _ = _batch_case(hb, [M], seed0=7)
+    q = systems[0]
+    L = len(q.sides)
+    levels = [q.level(l) for l in range(L)]
+    H32 = P.MGHierarchy([lv[1].to_host() for lv in levels], [lv[2].to_host() for lv in levels[:-1]],
+                        [lv[3].to_host() for lv in levels[:-1]], list(q.sides))
+    A64 = levels[-1][0].to_host()
+    b = bs[0].cpu().numpy()
+    x_o, outer_o, inner_o, hist = oracle.ir_pcg(A64, H32, b, eps=1e-8, inner_eps=1e-3)
+    x = torch.zeros_like(bs[0])
+    (info,) = hb.Q1System.solve_batch(systems, bs, [x], eps=1e-8)
+    assert abs(info["outer"] - outer_o) <= 1 and abs(info["iterations"] - inner_o) <= 0.2 * inner_o + 2, (info, inner_o)
+    assert np.linalg.norm(x.cpu().numpy() - x_o) <= 1e-6 * np.linalg.norm(x_o)
+    q.close()
+
+
+def test_batched_served_solve_alone_equals_in_the_mix(hb):
+    sides = [33, 65, 129, 200]
+    systems, bs, _ = _batch_case(hb, sides, seed0=3)
+    mix = [torch.zeros_like(b) for b in bs]
+    infos = hb.Q1System.solve_batch(systems, bs, mix, eps=1e-8, cluster=8, threads=256)
+    for q, b, xm, im in zip(systems, bs, mix, infos):
+        xa = torch.zeros_like(b)
+        (ia,) = hb.Q1System.solve_batch([q], [b], [xa], eps=1e-8, cluster=8, threads=256)
+        assert ia == im and torch.equal(xa, xm), q.M
+    # the same handle twice in one batch is refused
+    from honei_b200._lib import HBError
+    with pytest.raises(HBError):
+        hb.Q1System.solve_batch([systems[0], systems[0]], [bs[0], bs[0]], [mix[0], mix[0]])
+    for q in systems:
+        q.close()

@@ -23,12 +23,13 @@ def host_relres(oracle, req, x):
     return np.linalg.norm(oracle.defect(A, b, x)) / np.linalg.norm(b)
 
 
-def test_mixed_stream_reaches_target(S, oracle):
+@pytest.mark.parametrize("mid", [0, 200])
+def test_mixed_stream_reaches_target(S, oracle, mid):
     trace = S.poisson_trace(24, rate=400.0, side_range=(17, 300), seed=5)
-    with S.Server(mode="mixed", small_max_side=96, large_workers=2) as srv:
+    with S.Server(mode="mixed", small_max_side=96, large_workers=2, mid_max_side=mid) as srv:
         rep = S.replay(srv, trace)
     assert rep["completed"] == rep["ok"] == 24
-    assert set(rep["paths"]) == {"batch", "mgpcg"}
+    assert set(rep["paths"]) == ({"batch", "mgpcg"} if mid == 0 else {"batch", "mgbatch", "mgpcg"})
     by_tag = {c.tag: c for c in rep["records"]}
     for req in trace.requests:
         c = by_tag[req.tag]
@@ -38,11 +39,12 @@ def test_mixed_stream_reaches_target(S, oracle):
         assert np.linalg.norm(c.x - req.x_true) <= 1e-4 * np.linalg.norm(req.x_true)
 
 
-def test_alone_equals_in_the_mix(S):
+@pytest.mark.parametrize("mid", [0, 150])
+def test_alone_equals_in_the_mix(S, mid):
     trace = S.poisson_trace(16, rate=0.0, side_range=(17, 200), seed=9)
-    with S.Server(mode="mixed", small_max_side=64, large_workers=3) as srv:
+    with S.Server(mode="mixed", small_max_side=64, large_workers=3, mid_max_side=mid) as srv:
         mix = {c.tag: c for c in S.replay(srv, trace, realtime=False)["records"]}
-    with S.Server(mode="mixed", small_max_side=64, large_workers=3) as srv:
+    with S.Server(mode="mixed", small_max_side=64, large_workers=3, mid_max_side=mid) as srv:
         for req in trace.requests:
             srv.submit(req)
             (c,) = srv.drain()
@@ -74,7 +76,7 @@ def test_admission_budget(S):
     trace = S.poisson_trace(10, rate=0.0, side_range=(150, 260), seed=3)
     biggest = max((1 << 20) + 320 * r.M * r.M for r in trace.requests)
     budget = biggest + biggest // 2          # at most one large request resident at a time
-    with S.Server(mode="mixed", budget_bytes=budget, small_max_side=0, large_workers=4) as srv:
+    with S.Server(mode="mixed", budget_bytes=budget, small_max_side=0, large_workers=4, mid_max_side=0) as srv:
         rep = S.replay(srv, trace, realtime=False)
         st = srv.stats()
         with pytest.raises(Exception):
