@@ -444,7 +444,7 @@ def bench_ir(la, ctx, M=2049, seed=3):
     return out
 
 
-def bench_serve(n_requests=120, rate=150.0, seed=11):
+def bench_serve(n_requests=120, rate=150.0, seed=11, device=0):
     """The serving stream: Q1 requests with grid side log-uniform in [33, 1025], cellwise
     coefficient log-uniform in [1e-2, 1e2], b = A x_true, each solved to 1e-8 relative FP64
     residual, submitted from host buffers and returned to host buffers.  The mixed server
@@ -462,12 +462,13 @@ def bench_serve(n_requests=120, rate=150.0, seed=11):
     for mode in ("mixed", "plain"):
         res = {}
         for name, tr, rt in (("burst", burst, False), ("poisson", timed, True)):
-            with S.Server(mode=mode) as srv:
+            with S.Server(mode=mode) as srv, ClockSampler(device) as clk:
                 rep = S.replay(srv, tr, realtime=rt)
                 peak = srv.stats()["bytes_peak"]
             res[name] = {"solves_per_s": round(rep["solves_per_s"], 2), "p50_ms": round(rep["p50_ms"], 2),
                          "p99_ms": round(rep["p99_ms"], 2), "ok": rep["ok"], "paths": rep["paths"],
-                         "max_true_relres": rep["max_true_relres"], "hbm_peak_bytes": peak}
+                         "max_true_relres": rep["max_true_relres"], "hbm_peak_bytes": peak,
+                         "clocks": clk.summary()}
         out[mode] = res
     out["speedup_solves_per_s"] = round(out["mixed"]["burst"]["solves_per_s"] / out["plain"]["burst"]["solves_per_s"], 2)
     return out
@@ -590,9 +591,10 @@ def run_ours(args):
 
     cg_cluster = bench_cg_cluster(ctx)
     batch_extra = None if args.no_batch else bench_batch(la, ctx, n_systems=args.batch_systems)
+    # the serving sample before the multi-second 2049^2 solves (their heat lowers the clocks)
+    serve_extra = None if (args.no_serve or rank != 0 and ws > 1) else bench_serve(args.serve_requests, device=local)
     mg_extra = None if args.no_mg else bench_mg(la, ctx, cpu=(ws == 1 and not args.no_cpu_baseline))
     ir_extra = None if args.no_mg else bench_ir(la, ctx)
-    serve_extra = None if (args.no_serve or rank != 0 and ws > 1) else bench_serve(args.serve_requests)
 
     line = None
     if rank == 0:
