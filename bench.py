@@ -342,10 +342,15 @@ def bench_mg(la, ctx, M=2049, seed=5, cpu=True):
 
     H = P.mg_hierarchy(M)
     xt = P.uniform_vector(M * M, seed)
-    out = {"workload": f"MG V(2,2) on Q1 {M}^2, {len(H.sides)} levels, coarse CG on 9^2"}
+    out = {"workload": f"MG V(2,2) on Q1 {M}^2, {len(H.sides)} levels, coarse CG on 9^2; *_banded: banded "
+                       "levels and matrix-free transfers, the same cycle"}
     bref = None
-    for name, npdt, tdt, eps in (("f64", np.float64, torch.float64, 1e-8), ("f32", np.float32, torch.float32, 1e-6)):
-        data = la.MGData.from_hierarchy(H, npdt, ctx=ctx, eps=eps, max_iters=100)
+    xs_ell = {}
+    for name, npdt, tdt, eps, banded in (("f64", np.float64, torch.float64, 1e-8, False),
+                                          ("f32", np.float32, torch.float32, 1e-6, False),
+                                          ("f64_banded", np.float64, torch.float64, 1e-8, True),
+                                          ("f32_banded", np.float32, torch.float32, 1e-6, True)):
+        data = la.MGData.from_hierarchy(H, npdt, ctx=ctx, eps=eps, max_iters=100, banded=banded)
         A = data.A[-1]
         xtd = torch.from_numpy(xt.astype(npdt)).cuda()
         b = torch.empty_like(xtd)
@@ -365,8 +370,13 @@ def bench_mg(la, ctx, M=2049, seed=5, cpu=True):
         err = float(torch.linalg.norm((x - xtd).double()) / torch.linalg.norm(xtd.double()))
         out[name] = {"ms": round(ms, 2), "cycles": cycles, "ms_per_cycle": round(ms / max(cycles, 1), 3),
                      "relres": r1 / r0 if r0 else 0.0, "eps": eps, "err_vs_x_true": err}
+        if banded:
+            # the banded cycle rounds as the ELL cycle: same iterate
+            out[name]["same_x_as_ell"] = bool(torch.equal(x, xs_ell[name.split("_")[0]]))
+        else:
+            xs_ell[name] = x.clone()
         data.close()
-        del data, A, b, x, xtd
+        del data, A, b, xtd
         torch.cuda.empty_cache()
     if cpu:
         R = _ref_cpu()

@@ -91,6 +91,7 @@ SIGNATURES = {
     "hb_cg_var_ell_f32": (i32, [vp, P_ell, P_ell, vp, vp, i64, f32, P_i64, C.POINTER(f32)]),
     "hb_cg_f64_noalloc": (i32, [P_ell, vp, vp, i64, f64, P_i64, C.POINTER(f64), vp]),
     "hb_mg_create": (i32, [vp, i32, P_ell, P_ell, P_ell, C.POINTER(HbMGParams), C.POINTER(vp)]),
+    "hb_mg_create_banded": (i32, [vp, i32, P_ell, P_band, C.POINTER(HbMGParams), C.POINTER(vp)]),
     "hb_mg_destroy": (i32, [vp]),
     "hb_mg_set_params": (i32, [vp, C.POINTER(HbMGParams)]),
     "hb_mg_solve_f64": (i32, [vp, vp, vp, P_i64, C.POINTER(f64)]),

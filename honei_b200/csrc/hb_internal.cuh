@@ -76,6 +76,13 @@ template <typename T>
 int hb_launch_spmv_mode(hb_context *ctx, const hb_ell *A, int mode, const T *x, const T *b, const T *P, T *y);
 // P[i] = damping / A(i, i)
 template <typename T> int hb_launch_jacobi_diag(hb_context *ctx, const hb_ell *A, T damping, T *P);
+// Banded Q1 level operator in the fused ELL modes (SPMV / DEFECT / JACOBI), summed in the ELL
+// row's column order, and the matrix-free PROLMAT-order transfers of a (2^k + 1)^2 grid of
+// fine side Mf (y += P c; d = P^T f), all bit-identical to the ELL kernels on the same matrices.
+template <typename T>
+int hb_launch_band_mode(hb_context *ctx, const hb_q1band *A, int mode, const T *x, const T *b, const T *P, T *y);
+template <typename T> int hb_launch_prolong_add(hb_context *ctx, int64_t Mf, T *y, const T *c);
+template <typename T> int hb_launch_restrict_pt(hb_context *ctx, int64_t Mf, T *d, const T *f);
 // Sum of squares / dot product into a device scalar (no host sync).
 template <typename T> int hb_launch_dot(hb_context *ctx, int64_t n, const T *x, const T *y, T *out_dev);
 // Plain CG (cg.hh semantics) as one persistent kernel, asynchronous: work = 5 * ld entries,

@@ -39,6 +39,9 @@ struct hb_mg {
     int64_t used_coarse_total = 0;
     // optional exact coarse solve: dense inverse of A[0] (row-major, dtype), replacing the CG
     void *coarse_inv = nullptr;
+    // optional banded levels (hb_mg_create_banded): levels >= 1 smooth and take defects with the
+    // banded operator and transfer matrix-free; level 0 keeps its ELL matrix for the coarse CG
+    std::vector<hb_q1band> B;
 };
 
 namespace {
@@ -116,12 +119,19 @@ template <typename T> int norm_host(hb_mg *mg, const T *v, int64_t n, T *out)
     return HB_OK;
 }
 
+// The level operator in a fused mode: banded levels (l >= 1 of a banded hierarchy) or ELL.
+template <typename T> int level_mode(hb_mg *mg, int l, int mode, const T *x, const T *b, const T *P, T *y)
+{
+    if (!mg->B.empty() && l >= 1) return hb_launch_band_mode<T>(mg->ctx, &mg->B[l], mode, x, b, P, y);
+    return hb_launch_spmv_mode<T>(mg->ctx, &mg->A[l], mode, x, b, P, y);
+}
+
 template <typename T> int smooth(hb_mg *mg, int l, T *X, const T *B, int64_t sweeps)
 {
     hb_context *ctx = mg->ctx;
     T *cur = X, *other = tp<T>(mg->xt[l]);
     for (int64_t s = 0; s < sweeps; ++s) {
-        HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->A[l], HB_MODE_JACOBI, cur, B, tp<T>(mg->P[l]), other));
+        HB_TRY(level_mode<T>(mg, l, HB_MODE_JACOBI, cur, B, tp<T>(mg->P[l]), other));
         T *t = cur; cur = other; other = t;
     }
     if (cur != X)
@@ -151,12 +161,18 @@ template <typename T> int vcycle(hb_mg *mg, int l, T *X, const T *B)
         return hb_launch_cg<T>(ctx, &mg->A[0], B, X, mg->prm.max_iters_coarse, (T)mg->prm.eps, tp<T>(mg->cgwork),
                                mg->cgres);
     HB_TRY(smooth<T>(mg, l, X, B, mg->prm.n_pre));
-    HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->A[l], HB_MODE_DEFECT, X, B, nullptr, tp<T>(mg->store[l])));
-    HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->res[l - 1], HB_MODE_SPMV, tp<T>(mg->store[l]), nullptr, nullptr,
-                                  tp<T>(mg->d[l - 1])));
+    HB_TRY(level_mode<T>(mg, l, HB_MODE_DEFECT, X, B, nullptr, tp<T>(mg->store[l])));
+    if (!mg->B.empty())
+        HB_TRY(hb_launch_restrict_pt<T>(ctx, mg->B[l].root, tp<T>(mg->d[l - 1]), tp<T>(mg->store[l])));
+    else
+        HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->res[l - 1], HB_MODE_SPMV, tp<T>(mg->store[l]), nullptr, nullptr,
+                                      tp<T>(mg->d[l - 1])));
     HB_CUDA_TRY(ctx, cudaMemsetAsync(mg->c[l - 1], 0, sizeof(T) * mg->A[l - 1].rows, ctx->stream));
     HB_TRY(vcycle<T>(mg, l - 1, tp<T>(mg->c[l - 1]), tp<T>(mg->d[l - 1])));
-    HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->prol[l - 1], HB_MODE_ADD, tp<T>(mg->c[l - 1]), nullptr, nullptr, X));
+    if (!mg->B.empty())
+        HB_TRY(hb_launch_prolong_add<T>(ctx, mg->B[l].root, X, tp<T>(mg->c[l - 1])));
+    else
+        HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->prol[l - 1], HB_MODE_ADD, tp<T>(mg->c[l - 1]), nullptr, nullptr, X));
     return smooth<T>(mg, l, X, B, mg->prm.n_post);
 }
 
@@ -167,13 +183,13 @@ template <typename T> int mg_solve(hb_mg *mg, const T *b, T *x, int64_t *used, T
     const int top = mg->L - 1;
     const int64_t n = mg->A[top].rows;
     T *r = tp<T>(mg->r);
-    HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->A[top], HB_MODE_DEFECT, x, b, nullptr, r));
+    HB_TRY(level_mode<T>(mg, top, HB_MODE_DEFECT, x, b, nullptr, r));
     T r0, rc = T(1e16);
     HB_TRY(norm_host<T>(mg, r, n, &r0));
     int64_t u = 0;
     for (int64_t i = 0; i < mg->prm.max_iters; ++i) {
         HB_TRY(vcycle<T>(mg, top, x, b));
-        HB_TRY(hb_launch_spmv_mode<T>(ctx, &mg->A[top], HB_MODE_DEFECT, x, b, nullptr, r));
+        HB_TRY(level_mode<T>(mg, top, HB_MODE_DEFECT, x, b, nullptr, r));
         HB_TRY(norm_host<T>(mg, r, n, &rc));
         u = i + 1;
         if (rc < (T)mg->prm.eps * r0) break;
@@ -442,21 +458,27 @@ template <typename T> int jacobi_init(hb_mg *mg)
     return HB_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int hb_mg_create(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *prol, const hb_ell *res,
-                 const hb_mg_params *params, hb_mg **out)
+int mg_create_impl(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *prol, const hb_ell *res,
+                   const hb_q1band *B, const hb_mg_params *params, hb_mg **out)
 {
     if (!ctx || !A || !params || !out || nlevels < 1) return HB_ERR_INVALID;
-    if (nlevels > 1 && (!prol || !res)) return HB_ERR_INVALID;
+    if (nlevels > 1 && !B && (!prol || !res)) return HB_ERR_INVALID;
     *out = nullptr;
     const int dt = A[0].dtype;
+    if (B) {
+        // (2^k + 1)^2 grids, each side 2 * (coarser side) - 1, bands of the level's own size
+        for (int l = 0; l < nlevels; ++l) {
+            const int64_t m = B[l].root;
+            if (B[l].dtype != dt || B[l].n != A[l].rows || m * m != B[l].n || !(m & 1)) return HB_ERR_SIZE;
+            if (l > 0 && m != 2 * B[l - 1].root - 1) return HB_ERR_SIZE;
+            for (int k = 0; k < 9; ++k)
+                if (!B[l].band[k]) return HB_ERR_INVALID;
+        }
+    }
     for (int l = 0; l < nlevels; ++l) {
         HB_TRY(hb_check_ell(&A[l], dt));
         if (A[l].rows != A[l].cols) return HB_ERR_SIZE;
-        if (l + 1 < nlevels) {
+        if (l + 1 < nlevels && !B) {
             HB_TRY(hb_check_ell(&prol[l], dt));
             HB_TRY(hb_check_ell(&res[l], dt));
             if (prol[l].rows != A[l + 1].rows || prol[l].cols != A[l].rows) return HB_ERR_SIZE;
@@ -470,10 +492,11 @@ int hb_mg_create(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *pr
     mg->L = nlevels;
     mg->dtype = dt;
     mg->A.assign(A, A + nlevels);
-    if (nlevels > 1) {
+    if (nlevels > 1 && !B) {
         mg->prol.assign(prol, prol + nlevels - 1);
         mg->res.assign(res, res + nlevels - 1);
     }
+    if (B) mg->B.assign(B, B + nlevels);
     mg->prm = *params;
     const size_t es = dt == HB_F64 ? 8 : 4;
     const int64_t nf = A[nlevels - 1].rows;
@@ -517,6 +540,23 @@ int hb_mg_create(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *pr
     }
     *out = mg;
     return HB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hb_mg_create(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *prol, const hb_ell *res,
+                 const hb_mg_params *params, hb_mg **out)
+{
+    return mg_create_impl(ctx, nlevels, A, prol, res, nullptr, params, out);
+}
+
+int hb_mg_create_banded(hb_context *ctx, int nlevels, const hb_ell *A, const hb_q1band *B, const hb_mg_params *params,
+                        hb_mg **out)
+{
+    if (!B) return HB_ERR_INVALID;
+    return mg_create_impl(ctx, nlevels, A, nullptr, nullptr, B, params, out);
 }
 
 int hb_mg_destroy(hb_mg *mg)

@@ -56,10 +56,14 @@ template <> __device__ __forceinline__ void st_vec<float, 4>(float *p, const flo
     *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
 
-// MODE 0: y = A x;  MODE 1: y = b - A x.  VEC: every band, b and y 16-byte aligned.
-template <typename T, int MODE, bool VEC>
+// MODE 0: y = A x;  MODE 1: y = b - A x;  MODE 2: y = x + P (b - A x) (damped Jacobi sweep).
+// VEC: every band, b, P and y 16-byte aligned.  ELL: sum the bands in ascending column order
+// (LL, LD, LU, DL, DD, DU, UL, UD, UU: the order of the same matrix's ELL row) instead of the
+// reference's banded order (DD first).
+template <typename T, int MODE, bool VEC, bool ELL = false>
 __global__ void __launch_bounds__(256) q1band_kernel(int64_t n, int64_t root, Bands<T> B, const T *__restrict__ x,
-                                                     const T *__restrict__ b, T *__restrict__ y)
+                                                     const T *__restrict__ b, T *__restrict__ y,
+                                                     const T *__restrict__ P = nullptr)
 {
     using hbd::add; using hbd::mul; using hbd::sub;
     constexpr int R = Rows<T>::R;
@@ -92,18 +96,28 @@ __global__ void __launch_bounds__(256) q1band_kernel(int64_t n, int64_t root, Ba
 #pragma unroll
         for (int i = 0; i < R; ++i) {
             const int64_t r = r0 + i;
-            T s = mul(a[4][i], mid[i + 1]);
-            if (r - root - 1 >= 0) s = add(s, mul(a[0][i], lo[i]));
-            if (r - root >= 0) s = add(s, mul(a[1][i], lo[i + 1]));
-            if (r - root + 1 >= 0) s = add(s, mul(a[2][i], lo[i + 2]));
-            if (r - 1 >= 0) s = add(s, mul(a[3][i], mid[i]));
+            T s;
+            if (ELL) {
+                s = T(0);
+                if (r - root - 1 >= 0) s = add(s, mul(a[0][i], lo[i]));
+                if (r - root >= 0) s = add(s, mul(a[1][i], lo[i + 1]));
+                if (r - root + 1 >= 0) s = add(s, mul(a[2][i], lo[i + 2]));
+                if (r - 1 >= 0) s = add(s, mul(a[3][i], mid[i]));
+                s = add(s, mul(a[4][i], mid[i + 1]));
+            } else {
+                s = mul(a[4][i], mid[i + 1]);
+                if (r - root - 1 >= 0) s = add(s, mul(a[0][i], lo[i]));
+                if (r - root >= 0) s = add(s, mul(a[1][i], lo[i + 1]));
+                if (r - root + 1 >= 0) s = add(s, mul(a[2][i], lo[i + 2]));
+                if (r - 1 >= 0) s = add(s, mul(a[3][i], mid[i]));
+            }
             if (r + 1 < n) s = add(s, mul(a[5][i], mid[i + 2]));
             if (r + root - 1 < n) s = add(s, mul(a[6][i], hi[i]));
             if (r + root < n) s = add(s, mul(a[7][i], hi[i + 1]));
             if (r + root + 1 < n) s = add(s, mul(a[8][i], hi[i + 2]));
             out[i] = s;
         }
-        if (MODE == 1) {
+        if (MODE >= 1) {
             T bv[R];
             if (VEC && full) {
                 ld_vec<T, R>(b + r0, bv);
@@ -111,8 +125,21 @@ __global__ void __launch_bounds__(256) q1band_kernel(int64_t n, int64_t root, Ba
 #pragma unroll
                 for (int i = 0; i < R; ++i) bv[i] = (r0 + i < n) ? __ldcs(b + r0 + i) : T(0);
             }
+            if (MODE == 1) {
 #pragma unroll
-            for (int i = 0; i < R; ++i) out[i] = sub(bv[i], out[i]);
+                for (int i = 0; i < R; ++i) out[i] = sub(bv[i], out[i]);
+            } else {
+                // x + P (b - s); the own x values are mid[1..R]
+                T pv[R];
+                if (VEC && full) {
+                    ld_vec<T, R>(P + r0, pv);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < R; ++i) pv[i] = (r0 + i < n) ? __ldcs(P + r0 + i) : T(0);
+                }
+#pragma unroll
+                for (int i = 0; i < R; ++i) out[i] = add(mid[i + 1], mul(pv[i], sub(bv[i], out[i])));
+            }
         }
         if (VEC && full) {
             st_vec<T, R>(y + r0, out);
@@ -144,7 +171,7 @@ __global__ void q1band_poisson_kernel(int64_t N, int64_t M, Bands<T> B)
 // are 0 here.
 template <typename T>
 __global__ void q1band_from_ell_kernel(int64_t n, int64_t root, int64_t ld, int K, const int32_t *__restrict__ Aj,
-                                       const T *__restrict__ Ax, Bands<T> B)
+                                       const T *__restrict__ Ax, Bands<T> B, int *off_band)
 {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
         const int64_t off[9] = {-root - 1, -root, -root + 1, -1, 0, 1, root - 1, root, root + 1};
@@ -155,9 +182,11 @@ __global__ void q1band_from_ell_kernel(int64_t n, int64_t root, int64_t ld, int 
             const int32_t j = Aj[(int64_t)s * ld + r];
             if (j < 0) continue;
             const int64_t d = (int64_t)j - r;
+            bool hit = false;
 #pragma unroll
             for (int k = 0; k < 9; ++k)
-                if (d == off[k]) v[k] = Ax[(int64_t)s * ld + r];
+                if (d == off[k]) { v[k] = Ax[(int64_t)s * ld + r]; hit = true; }
+            if (!hit && Ax[(int64_t)s * ld + r] != T(0)) atomicExch(off_band, 1);   // not a Q1 band
         }
 #pragma unroll
         for (int k = 0; k < 9; ++k) const_cast<T *>(B.p[k])[r] = v[k];
@@ -214,6 +243,32 @@ int q1band_apply(hb_context *ctx, const hb_q1band *A, const T *b, const T *x, T 
 
 }  // namespace
 
+template <typename T>
+int hb_launch_band_mode(hb_context *ctx, const hb_q1band *A, int mode, const T *x, const T *b, const T *P, T *y)
+{
+    const int64_t n = A->n;
+    if (n == 0) return HB_OK;
+    bool vec = aligned16(y) && (mode == HB_MODE_SPMV || aligned16(b)) && (mode != HB_MODE_JACOBI || aligned16(P));
+    for (int k = 0; k < 9; ++k) vec = vec && aligned16(A->band[k]);
+    const Bands<T> B = bands_of<T>(A);
+    const int grid = grid_for(ctx, (n + Rows<T>::R - 1) / Rows<T>::R);
+#define HB_BAND_LAUNCH(MD)                                                                                     \
+    if (vec) q1band_kernel<T, MD, true, true><<<grid, 256, 0, ctx->stream>>>(n, A->root, B, x, b, y, P);       \
+    else q1band_kernel<T, MD, false, true><<<grid, 256, 0, ctx->stream>>>(n, A->root, B, x, b, y, P)
+    switch (mode) {
+        case HB_MODE_SPMV: HB_BAND_LAUNCH(0); break;
+        case HB_MODE_DEFECT: HB_BAND_LAUNCH(1); break;
+        case HB_MODE_JACOBI: HB_BAND_LAUNCH(2); break;
+        default: return HB_ERR_INVALID;
+    }
+#undef HB_BAND_LAUNCH
+    return hb_check_launch(ctx, "q1band_kernel (ELL order)");
+}
+template int hb_launch_band_mode<double>(hb_context *, const hb_q1band *, int, const double *, const double *,
+                                         const double *, double *);
+template int hb_launch_band_mode<float>(hb_context *, const hb_q1band *, int, const float *, const float *,
+                                        const float *, float *);
+
 extern "C" {
 
 int64_t hb_q1band_root(int64_t n) { return n > 0 ? q1band_root(n) : 0; }
@@ -265,13 +320,20 @@ int hb_q1band_from_ell(hb_context *ctx, const hb_ell *E, hb_q1band *A)
         if (!A->band[k]) return HB_ERR_INVALID;
     if (!E->Aj || !E->Ax) return HB_ERR_INVALID;
     const int grid = grid_for(ctx, n);
+    int *flag = (int *)hb_scalars(ctx);
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream));
     if (A->dtype == HB_F64)
         q1band_from_ell_kernel<double><<<grid, 256, 0, ctx->stream>>>(n, A->root, E->ld, (int)E->K, E->Aj,
-                                                                      (const double *)E->Ax, bands_of<double>(A));
+                                                                      (const double *)E->Ax, bands_of<double>(A), flag);
     else
         q1band_from_ell_kernel<float><<<grid, 256, 0, ctx->stream>>>(n, A->root, E->ld, (int)E->K, E->Aj,
-                                                                     (const float *)E->Ax, bands_of<float>(A));
-    return hb_check_launch(ctx, "q1band_from_ell_kernel");
+                                                                     (const float *)E->Ax, bands_of<float>(A), flag);
+    int st = hb_check_launch(ctx, "q1band_from_ell_kernel");
+    if (st) return st;
+    int *h = (int *)ctx->pinned;
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return *h ? HB_ERR_UNSUPPORTED : HB_OK;
 }
 
 }  // extern "C"

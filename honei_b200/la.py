@@ -583,8 +583,8 @@ class MGData:
     """
 
     def __init__(self, A, prol, res, max_iters=100, max_iters_coarse=1000, n_pre=2, n_post=2,
-                 damping=0.7, eps=1e-8, ctx: Context | None = None):
-        from ._lib import HbMGParams
+                 damping=0.7, eps=1e-8, ctx: Context | None = None, banded: bool = False):
+        from ._lib import HbMGParams, HbQ1Band
         self.ctx = ctx or default_context()
         self.A, self.prol, self.res = list(A), list(prol), list(res)
         self.dtype = self.A[0].dtype
@@ -594,8 +594,15 @@ class MGData:
         self._R = (HbEll * max(L - 1, 1))(*[r.struct for r in self.res])
         self.params = HbMGParams(max_iters, max_iters_coarse, n_pre, n_post, damping, eps)
         h = C.c_void_p()
-        check(lib().hb_mg_create(self.ctx.handle, L, self._A, self._P, self._R, C.byref(self.params), C.byref(h)),
-              "hb_mg_create", self.ctx.handle)
+        if banded:
+            # banded copies of the levels; transfers become matrix-free (prol / res unused)
+            self.bands = [BandedMatrixQ1.from_ell(a, ctx=self.ctx) for a in self.A]
+            self._B = (HbQ1Band * L)(*[b.struct for b in self.bands])
+            check(lib().hb_mg_create_banded(self.ctx.handle, L, self._A, self._B, C.byref(self.params), C.byref(h)),
+                  "hb_mg_create_banded", self.ctx.handle)
+        else:
+            check(lib().hb_mg_create(self.ctx.handle, L, self._A, self._P, self._R, C.byref(self.params),
+                                     C.byref(h)), "hb_mg_create", self.ctx.handle)
         self.handle = h
         self.used_iters = 0
 

@@ -169,8 +169,9 @@ int hb_q1band_defect_f32(hb_context *ctx, const hb_q1band *A, const float *b, co
  * 41-77, on an M x M grid (A->n = M^2, A->dtype and A->band[] set by the caller). */
 int hb_q1band_fill_poisson(hb_context *ctx, int64_t M, hb_q1band *A);
 /* BandedMatrixQx(SparseMatrixELL&), honei/la/banded_matrix_qx-impl.hh:111-167: band k of row
- * i = A(i, i + offset_k) where that column exists, 0 elsewhere.  n must be a square
- * (HB_ERR_UNSUPPORTED otherwise); E->dtype == A->dtype. */
+ * i = A(i, i + offset_k) where that column exists, 0 elsewhere.  n must be a square and every
+ * non-zero entry of E must lie on one of the nine bands (HB_ERR_UNSUPPORTED otherwise: the
+ * conversion would drop it); E->dtype == A->dtype. */
 int hb_q1band_from_ell(hb_context *ctx, const hb_ell *E, hb_q1band *A);
 
 /* Matrix-free geometric transfers of (2^k + 1)^2 grids: Prolongation<Tag, methods::NONE>
@@ -288,6 +289,14 @@ typedef struct {
 
 int hb_mg_create(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *prol,
                  const hb_ell *res, const hb_mg_params *params, hb_mg **out);
+/* The same multigrid on (2^k + 1)^2 Q1 grids with banded level matrices B[l] (hb_q1band; side
+ * 2 * (coarser side) - 1) and matrix-free bilinear transfers with Dirichlet fine rows zero (the
+ * PROLMAT matrices of the rediscretised hierarchy, never stored).  Levels >= 1 smooth and take
+ * defects with B[l]; level 0 keeps A[0] for its coarse CG; A[l] also gives the Jacobi diagonals.
+ * Every operation rounds as the ELL cycle on the same matrices (bit-identical iterates); per fine
+ * row the cycle reads no column indices and no transfer matrix. */
+int hb_mg_create_banded(hb_context *ctx, int nlevels, const hb_ell *A, const hb_q1band *B, const hb_mg_params *params,
+                        hb_mg **out);
 int hb_mg_destroy(hb_mg *mg);
 int hb_mg_set_params(hb_mg *mg, const hb_mg_params *params);
 /* Solve on the finest level: x holds x0 on entry.  *used_cycles (host) and

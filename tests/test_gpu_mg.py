@@ -159,3 +159,44 @@ def test_mg_full_size_2049_property(hb):
     u, s0, s1 = hb.IRSolver.value(A, b, x2, mg32, eps=1e-10, max_iters=50, warm_start=False)
     assert s1 < 1e-10 * s0
     assert ((x2 - xt).norm() / xt.norm()).item() < 1e-6
+
+
+@pytest.mark.parametrize("M,coarse,coef", [(33, "rediscretize", False), (129, "rediscretize", False),
+                                           (65, "rediscretize", True), (65, "galerkin", True), (257, "galerkin", True)])
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_banded_matrix_free_mg_bitwise_equal_to_ell_mg(hb, M, coarse, coef, dt):
+    """The banded cycle (banded smoother / defect, matrix-free PROLMAT-order transfers) rounds
+    exactly as the ELL cycle on the same matrices: same cycles, same x bit for bit."""
+    c = P.log_uniform_coef(M, 1e-1, 1e1, M) if coef else None
+    H = P.mg_hierarchy(M, coef=c, coarse=coarse)
+    eps = 1e-8 if dt == np.float64 else 1e-5
+    tdt = torch.float64 if dt == np.float64 else torch.float32
+    b = torch.from_numpy(P.uniform_vector(M * M, 4).astype(dt)).cuda()
+    out = []
+    for banded in (False, True):
+        data = hb.MGData.from_hierarchy(H, dt, eps=eps, max_iters=50, banded=banded)
+        x = torch.zeros(M * M, dtype=tdt, device="cuda")
+        used, r0, r1 = hb.MGSolver.value(data, b, x)
+        out.append((used, r0, r1, x.cpu().numpy()))
+        data.close()
+    assert out[0][:3] == out[1][:3]
+    assert np.array_equal(out[0][3], out[1][3])
+
+
+def test_banded_conversion_refuses_off_band_entries(hb):
+    from honei_b200._lib import HBError
+    A = P.q1_poisson(9)
+    ip, ix, dv = A.to_csr()
+    # add an entry two columns right of the diagonal in row 40 (not a Q1 band)
+    rows = []
+    for r in range(A.rows):
+        cols, vals = list(ix[ip[r]:ip[r + 1]]), list(dv[ip[r]:ip[r + 1]])
+        if r == 40:
+            cols.append(42); vals.append(-0.125)
+            order = np.argsort(cols); cols = list(np.array(cols)[order]); vals = list(np.array(vals)[order])
+        rows.append((cols, vals))
+    ip2 = np.cumsum([0] + [len(c) for c, _ in rows])
+    B = P.ell_from_csr(A.rows, A.cols, ip2, np.concatenate([c for c, _ in rows]), np.concatenate([v for _, v in rows]))
+    with pytest.raises(HBError) as e:
+        hb.BandedMatrixQ1.from_ell(hb.SparseMatrixELL.from_reference(B))
+    assert e.value.status == 6
