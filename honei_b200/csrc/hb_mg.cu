@@ -367,7 +367,7 @@ int pcg_iteration(hb_mg *mg, float *x, float *r, float *z, float *p, float *v, P
     hb_context *ctx = mg->ctx;
     const hb_ell *A = &mg->A[mg->L - 1];
     const int64_t n = A->rows;
-    HB_TRY(hb_launch_spmv_mode<float>(ctx, A, HB_MODE_SPMV, p, nullptr, nullptr, v));
+    HB_TRY(level_mode<float>(mg, mg->L - 1, HB_MODE_SPMV, p, nullptr, nullptr, v));
     HB_TRY(hb_launch_dot<float>(ctx, n, p, v, &s->pv));
     pcg_xr_kernel<<<ewb(ctx, n), 256, 0, ctx->stream>>>(n, s, x, r, p, v);
     HB_TRY(hb_check_launch(ctx, "pcg_xr_kernel"));
@@ -466,11 +466,11 @@ int mg_create_impl(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *
     *out = nullptr;
     const int dt = A[0].dtype;
     if (B) {
-        // (2^k + 1)^2 grids, each side 2 * (coarser side) - 1, bands of the level's own size
+        // square grids, each coarse side = (finer side) / 2 + 1, bands of the level's own size
         for (int l = 0; l < nlevels; ++l) {
             const int64_t m = B[l].root;
-            if (B[l].dtype != dt || B[l].n != A[l].rows || m * m != B[l].n || !(m & 1)) return HB_ERR_SIZE;
-            if (l > 0 && m != 2 * B[l - 1].root - 1) return HB_ERR_SIZE;
+            if (B[l].dtype != dt || B[l].n != A[l].rows || m * m != B[l].n) return HB_ERR_SIZE;
+            if (l > 0 && B[l - 1].root != m / 2 + 1) return HB_ERR_SIZE;
             for (int k = 0; k < 9; ++k)
                 if (!B[l].band[k]) return HB_ERR_INVALID;
         }

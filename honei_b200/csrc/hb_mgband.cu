@@ -1,5 +1,7 @@
-// hb_mgband.cu -- matrix-free pieces of the multigrid cycle on (2^k + 1)^2 Q1 grids whose level
-// matrices are banded (BandedMatrixQx<Q1Type> layout, hb_q1band):
+// hb_mgband.cu -- matrix-free pieces of the multigrid cycle on Q1 grids whose level matrices are
+// banded (BandedMatrixQx<Q1Type> layout, hb_q1band).  A fine grid of side Mf has the coarse side
+// Mf / 2 + 1 (2:1 for odd sides; for even sides the last coarse line has no fine support): on
+// interior fine nodes the bilinear interpolation is the same for both.
 //
 //   (the level operator in the fused ELL modes is q1band_kernel's ELL-order variant,
 //   hb_q1band.cu: the nine bands summed in ascending column order, LL, LD, LU, DL, DD, DU, UL,
@@ -22,7 +24,7 @@ __device__ __forceinline__ bool fine_boundary(int64_t R, int64_t C, int64_t Mf)
     return R == 0 || C == 0 || R == Mf - 1 || C == Mf - 1;
 }
 
-// y += P c (fine side Mf, coarse side Mc = (Mf - 1) / 2 + 1)
+// y += P c (fine side Mf, coarse side Mc = Mf / 2 + 1)
 template <typename T>
 __global__ void prolong_add_kernel(int64_t Mf, int64_t Mc, T *__restrict__ y, const T *__restrict__ c)
 {
@@ -78,7 +80,7 @@ unsigned grid_of(hb_context *ctx, int64_t work)
 
 template <typename T> int hb_launch_prolong_add(hb_context *ctx, int64_t Mf, T *y, const T *c)
 {
-    prolong_add_kernel<T><<<grid_of(ctx, Mf * Mf), 256, 0, ctx->stream>>>(Mf, (Mf - 1) / 2 + 1, y, c);
+    prolong_add_kernel<T><<<grid_of(ctx, Mf * Mf), 256, 0, ctx->stream>>>(Mf, Mf / 2 + 1, y, c);
     return hb_check_launch(ctx, "prolong_add_kernel");
 }
 template int hb_launch_prolong_add<double>(hb_context *, int64_t, double *, const double *);
@@ -86,7 +88,7 @@ template int hb_launch_prolong_add<float>(hb_context *, int64_t, float *, const 
 
 template <typename T> int hb_launch_restrict_pt(hb_context *ctx, int64_t Mf, T *d, const T *f)
 {
-    const int64_t Mc = (Mf - 1) / 2 + 1;
+    const int64_t Mc = Mf / 2 + 1;
     restrict_kernel<T><<<grid_of(ctx, Mc * Mc), 256, 0, ctx->stream>>>(Mf, Mc, d, f);
     return hb_check_launch(ctx, "restrict_kernel");
 }

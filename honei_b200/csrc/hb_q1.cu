@@ -250,6 +250,7 @@ struct hb_q1 {
     int L = 0;
     std::vector<int64_t> sides;
     std::vector<hb_ell> A64, A32, P32, R32;
+    std::vector<hb_q1band> B32;     // banded copies of the FP32 levels (the cycle's operator)
     std::vector<void *> blocks;
     hb_mg *mg = nullptr;
     double *r64 = nullptr;
@@ -335,7 +336,21 @@ int q1_build(hb_q1 *q, const double *coef)
     for (int l = 0; l + 1 < L; ++l)
         if ((st = hb_q1_transfers(ctx, q->sides[l + 1], &q->P32[l], &q->R32[l]))) return st;
     hb_mg_params prm{1, 200, 2, 2, 0.7, 1e-6};
-    if ((st = hb_mg_create(ctx, L, q->A32.data(), q->P32.data(), q->R32.data(), &prm, &q->mg))) return st;
+    // banded copies of the FP32 levels: the cycle reads no column indices and, with matrix-free
+    // transfers, no P / R matrix (hb_mg_create_banded; the same iterates as the ELL cycle)
+    q->B32.resize(L);
+    for (int l = 0; l < L; ++l) {
+        const int64_t nl = q->A32[l].rows, ldb = hb_round_up(nl > 0 ? nl : 1, 4);
+        void *bp;
+        if ((st = q1_alloc(q, &bp, (size_t)ldb * 9 * 4))) return st;
+        hb_q1band &bb = q->B32[l];
+        bb = hb_q1band{};
+        bb.n = nl;
+        bb.dtype = HB_F32;
+        for (int k = 0; k < 9; ++k) bb.band[k] = (float *)bp + k * ldb;
+        if ((st = hb_q1band_from_ell(ctx, &q->A32[l], &bb))) return st;
+    }
+    if ((st = hb_mg_create_banded(ctx, L, q->A32.data(), q->B32.data(), &prm, &q->mg))) return st;
     // exact coarse solve: invert the coarsest FP64 Galerkin matrix (at most 81 x 81)
     const int64_t nc = q->A64[0].rows;
     void *p;

@@ -200,3 +200,22 @@ def test_banded_conversion_refuses_off_band_entries(hb):
     with pytest.raises(HBError) as e:
         hb.BandedMatrixQ1.from_ell(hb.SparseMatrixELL.from_reference(B))
     assert e.value.status == 6
+
+
+@pytest.mark.parametrize("M", [64, 100, 130])
+def test_banded_mg_general_sides_bitwise(hb, M):
+    """Even and other non-(2^k + 1) sides (coarse side = side / 2 + 1, the served systems'
+    coarsening): the banded, matrix-free cycle equals the ELL cycle bit for bit (FP32, SPD
+    Galerkin hierarchy, dense coarse solve replaced by the coarse CG here)."""
+    c = P.log_uniform_coef(M, 1e-2, 1e2, M)
+    H = P.mg_hierarchy(M, coef=c, coarse="galerkin", symmetric=True).astype(np.float32)
+    b = torch.from_numpy(P.uniform_vector(M * M, 2).astype(np.float32)).cuda()
+    out = []
+    for banded in (False, True):
+        data = hb.MGData.from_hierarchy(H, np.float32, eps=1e-5, max_iters=30, banded=banded)
+        x = torch.zeros(M * M, dtype=torch.float32, device="cuda")
+        used, r0, r1 = hb.MGSolver.value(data, b, x)
+        out.append((used, r0, r1, x.cpu().numpy()))
+        data.close()
+    assert out[0][:3] == out[1][:3]
+    assert np.array_equal(out[0][3], out[1][3])
