@@ -109,6 +109,7 @@ struct hb_q1_view {
     int L = 0;
     hb_ell A64{};
     hb_ell A32[HB_Q1_MAXL], P32[HB_Q1_MAXL], R32[HB_Q1_MAXL];
+    hb_q1band B32[HB_Q1_MAXL];   // banded copies of the FP32 levels
     float *jac[HB_Q1_MAXL], *c[HB_Q1_MAXL], *d[HB_Q1_MAXL], *store[HB_Q1_MAXL], *xt[HB_Q1_MAXL];
     const float *coarse_inv = nullptr;
     double *r64 = nullptr;

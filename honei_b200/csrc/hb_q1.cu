@@ -526,8 +526,10 @@ int hb_q1_view_of(const hb_q1 *q, hb_q1_view *out)
     out->L = q->L;
     out->ctx = q->ctx;
     out->A64 = q->A64[q->L - 1];
+    if ((int)q->B32.size() != q->L) return HB_ERR_INVALID;
     for (int l = 0; l < q->L; ++l) {
         out->A32[l] = q->A32[l];
+        out->B32[l] = q->B32[l];
         if (l + 1 < q->L) {
             out->P32[l] = q->P32[l];
             out->R32[l] = q->R32[l];

@@ -5,7 +5,8 @@
 // (defect, norm, scaled FP32 right-hand side, update) around FP32 CG preconditioned by one
 // V(n_pre, n_post) cycle -- damped Jacobi sweeps x' = x + P (b - A x), defect, restriction R,
 // zero coarse start, the exact dense solve on the coarsest level, prolongation added with P,
-// post-smoothing -- with every kernel of the served solve replaced by a phase of the cluster:
+// post-smoothing; the levels are the system's banded FP32 copies and the transfers are
+// matrix-free, as in the served solve -- with every kernel replaced by a phase of the cluster:
 // the rows of each level are split over the cluster's CTAs (4 consecutive rows per thread), a
 // hardware cluster barrier separates phases that read other CTAs' rows, and the dot products are
 // fixed-order reductions through each CTA's shared memory and distributed shared memory.  Every
@@ -28,18 +29,15 @@ namespace cgx = cooperative_groups;
 
 namespace {
 
-struct QMat {
-    int64_t rows, ld;
-    int K;
-    const int32_t *Aj;
-    const float *Ax;
+// A level's banded FP32 matrix (nine bands LL .. UU, root = grid side).
+struct QBand {
+    int64_t n, root;
+    const float *b[9];
 };
 
 struct QLevel {
-    int64_t n, ld;
-    QMat A;        // level matrix (FP32)
-    QMat P;        // prolongation from level l-1 into this level (rows n)
-    QMat R;        // restriction from this level to level l-1 (rows n_{l-1})
+    int64_t n, ld, side;   // rows, padded vector length, grid side (coarser side = side / 2 + 1)
+    QBand A;
     const float *jac;
     float *c, *d, *store, *xt;
 };
@@ -128,10 +126,90 @@ __device__ __forceinline__ Range range_of(int64_t ld)
     return Range{rank * per, min(groups, (rank + 1) * per)};
 }
 
-template <typename T, typename G>
-__device__ __forceinline__ void rows4(const QMat &M, int64_t g, G gather, T (&s)[4])
+// s = A x on rows r0..r0+3 of a banded level, the nine bands summed in ascending column order
+// (the ELL row's order: bit-identical to the ELL product of the same matrix); rows >= n give 0.
+__device__ __forceinline__ void band_rows4(const QBand &B, int64_t r0, const float *x, float (&s)[4])
 {
-    hbd::ell_rows4<T, 0, 4>(M.Aj, (const T *)M.Ax, M.ld, M.K, 4 * g, gather, s);
+    using hbd::add; using hbd::mul;
+    const int64_t n = B.n, root = B.root;
+    float a[9][4];
+    if (r0 + 4 <= n) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) hbd::ld4_stream(B.b[k] + r0, a[k]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[k][i] = (r0 + i < n) ? B.b[k][r0 + i] : 0.f;
+    }
+    float lo[6], mid[6], hi[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+        const int64_t jl = r0 - root - 1 + t, jm = r0 - 1 + t, jh = r0 + root - 1 + t;
+        lo[t] = (jl >= 0 && jl < n) ? __ldcg(x + jl) : 0.f;
+        mid[t] = (jm >= 0 && jm < n) ? __ldcg(x + jm) : 0.f;
+        hi[t] = (jh >= 0 && jh < n) ? __ldcg(x + jh) : 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int64_t r = r0 + i;
+        float v = 0.f;
+        if (r < n) {
+            if (r - root - 1 >= 0) v = add(v, mul(a[0][i], lo[i]));
+            if (r - root >= 0) v = add(v, mul(a[1][i], lo[i + 1]));
+            if (r - root + 1 >= 0) v = add(v, mul(a[2][i], lo[i + 2]));
+            if (r - 1 >= 0) v = add(v, mul(a[3][i], mid[i]));
+            v = add(v, mul(a[4][i], mid[i + 1]));
+            if (r + 1 < n) v = add(v, mul(a[5][i], mid[i + 2]));
+            if (r + root - 1 < n) v = add(v, mul(a[6][i], hi[i]));
+            if (r + root < n) v = add(v, mul(a[7][i], hi[i + 1]));
+            if (r + root + 1 < n) v = add(v, mul(a[8][i], hi[i + 2]));
+        }
+        s[i] = v;
+    }
+}
+
+__device__ __forceinline__ bool fine_boundary(int64_t R, int64_t C, int64_t Mf)
+{
+    return R == 0 || C == 0 || R == Mf - 1 || C == Mf - 1;
+}
+
+// (P c)[k] for fine node k of a grid of side Mf (coarse side Mc): the bilinear interpolation with
+// Dirichlet fine rows zero, summed over coarse nodes in ascending order (the PROLMAT row).
+__device__ __forceinline__ float prolong_row(int64_t k, int64_t Mf, int64_t Mc, const float *c)
+{
+    using hbd::add; using hbd::mul;
+    const int64_t R = k / Mf, C = k - R * Mf;
+    float s = 0.f;
+    if (fine_boundary(R, C, Mf)) return s;
+    int64_t ri[2], ci[2];
+    float wr[2], wc[2];
+    int nr, nc;
+    if (R & 1) { ri[0] = (R - 1) / 2; ri[1] = (R + 1) / 2; wr[0] = wr[1] = 0.5f; nr = 2; }
+    else { ri[0] = R / 2; wr[0] = 1.f; nr = 1; }
+    if (C & 1) { ci[0] = (C - 1) / 2; ci[1] = (C + 1) / 2; wc[0] = wc[1] = 0.5f; nc = 2; }
+    else { ci[0] = C / 2; wc[0] = 1.f; nc = 1; }
+    for (int a = 0; a < nr; ++a)
+        for (int q = 0; q < nc; ++q) s = add(s, mul(wr[a] * wc[q], __ldcg(c + ri[a] * Mc + ci[q])));
+    return s;
+}
+
+// (P^T f)[k] for coarse node k: fine nodes in ascending order (the transposed PROLMAT row).
+__device__ __forceinline__ float restrict_row(int64_t k, int64_t Mf, int64_t Mc, const float *f)
+{
+    using hbd::add; using hbd::mul;
+    const int64_t r = k / Mc, c = k - r * Mc;
+    float s = 0.f;
+    for (int64_t R = 2 * r - 1; R <= 2 * r + 1; ++R) {
+        if (R < 0 || R >= Mf) continue;
+        const float wr = (R == 2 * r) ? 1.f : 0.5f;
+        for (int64_t C = 2 * c - 1; C <= 2 * c + 1; ++C) {
+            if (C < 0 || C >= Mf || fine_boundary(R, C, Mf)) continue;
+            const float wc = (C == 2 * c) ? 1.f : 0.5f;
+            s = add(s, mul(wr * wc, __ldcg(f + R * Mf + C)));
+        }
+    }
+    return s;
 }
 
 // One damped Jacobi sweep out = x + jac (b - A x) on a level (ell_spmv_kernel, HB_MODE_JACOBI).
@@ -140,7 +218,7 @@ __device__ __forceinline__ void jacobi(const QLevel &lv, const float *x, const f
     const Range rg = range_of(lv.ld);
     for (int64_t g = rg.lo + threadIdx.x; g < rg.hi; g += blockDim.x) {
         float s[4], xx[4], bb[4], pp[4], o[4];
-        rows4<float>(lv.A, g, [&](int32_t j) { return __ldcg(x + j); }, s);
+        band_rows4(lv.A, 4 * g, x, s);
         ldcg4(x + 4 * g, xx);
         ldcg4(b + 4 * g, bb);
         ldcg4(lv.jac + 4 * g, pp);
@@ -184,7 +262,7 @@ __device__ __forceinline__ void vcycle(const QSys &S, float *z, const float *r)
             const float *x = X(l), *b = B(l);
             for (int64_t g = rg.lo + threadIdx.x; g < rg.hi; g += blockDim.x) {
                 float s[4], bb[4], o[4];
-                rows4<float>(lv.A, g, [&](int32_t j) { return __ldcg(x + j); }, s);
+                band_rows4(lv.A, 4 * g, x, s);
                 ldcg4(b + 4 * g, bb);
 #pragma unroll
                 for (int i = 0; i < 4; ++i) o[i] = hbd::sub(bb[i], s[i]);
@@ -198,7 +276,9 @@ __device__ __forceinline__ void vcycle(const QSys &S, float *z, const float *r)
             const float *st = lv.store;
             for (int64_t g = rg.lo + threadIdx.x; g < rg.hi; g += blockDim.x) {
                 float s[4], zero[4] = {0.f, 0.f, 0.f, 0.f};
-                rows4<float>(lv.R, g, [&](int32_t j) { return __ldcg(st + j); }, s);
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    s[i] = (4 * g + i < cv.n) ? restrict_row(4 * g + i, lv.side, cv.side, st) : 0.f;
                 hbd::st4(cv.d + 4 * g, s);
                 hbd::st4(cv.c + 4 * g, zero);
             }
@@ -225,9 +305,11 @@ __device__ __forceinline__ void vcycle(const QSys &S, float *z, const float *r)
             const Range rg = range_of(lv.ld);
             const float *c = X(l - 1);
             float *x = X(l);
+            const int64_t Mc = S.lv[l - 1].side;
             for (int64_t g = rg.lo + threadIdx.x; g < rg.hi; g += blockDim.x) {
                 float s[4], xx[4];
-                rows4<float>(lv.P, g, [&](int32_t j) { return __ldcg(c + j); }, s);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) s[i] = (4 * g + i < lv.n) ? prolong_row(4 * g + i, lv.side, Mc, c) : 0.f;
                 ldcg4(x + 4 * g, xx);
 #pragma unroll
                 for (int i = 0; i < 4; ++i) xx[i] = hbd::add(xx[i], s[i]);
@@ -278,7 +360,7 @@ __device__ __forceinline__ int64_t pcg(const QSys &S, QSmem &sm, int &phase)
         acc = 0.f;
         for (int64_t g = rg.lo + threadIdx.x; g < rg.hi; g += blockDim.x) {
             float s[4], pp[4];
-            rows4<float>(top.A, g, [&](int32_t j) { return __ldcg(p + j); }, s);
+            band_rows4(top.A, 4 * g, p, s);
             ldcg4(p + 4 * g, pp);
             hbd::st4(v + 4 * g, s);
 #pragma unroll
@@ -429,7 +511,6 @@ __global__ void __launch_bounds__(THREADS, 1) q1batch_kernel(const QSys *__restr
     }
 }
 
-QMat mat_of(const hb_ell &e) { return QMat{e.rows, e.ld, (int)e.K, e.Aj, (const float *)e.Ax}; }
 
 int build(const hb_q1_view &v, const double *b, double *x, double eps, double inner_eps, int64_t max_outer,
           int64_t max_inner, hb_batch_result *res, QSys &S)
@@ -440,13 +521,17 @@ int build(const hb_q1_view &v, const double *b, double *x, double eps, double in
     S.n_post = v.n_post;
     for (int l = 0; l < v.L; ++l) {
         QLevel &q = S.lv[l];
+        const hb_q1band &bb = v.B32[l];
         q.n = v.A32[l].rows;
         q.ld = v.A32[l].ld;
-        q.A = mat_of(v.A32[l]);
-        if (l > 0) {
-            q.P = mat_of(v.P32[l - 1]);
-            q.R = mat_of(v.R32[l - 1]);
-            if (q.P.rows != q.n || q.R.rows != v.A32[l - 1].rows) return HB_ERR_SIZE;
+        q.side = bb.root;
+        if (bb.n != q.n || bb.root * bb.root != q.n || bb.dtype != HB_F32) return HB_ERR_SIZE;
+        if (l > 0 && S.lv[l - 1].side != q.side / 2 + 1) return HB_ERR_SIZE;
+        q.A.n = bb.n;
+        q.A.root = bb.root;
+        for (int k = 0; k < 9; ++k) {
+            q.A.b[k] = (const float *)bb.band[k];
+            if (!q.A.b[k] || ((uintptr_t)q.A.b[k] & 15)) return HB_ERR_INVALID;
         }
         q.jac = v.jac[l];
         q.c = v.c[l];
