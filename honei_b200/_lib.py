@@ -114,6 +114,7 @@ SIGNATURES = {
     "hb_q1_levels": (i32, [vp, C.POINTER(i32), P_i64]),
     "hb_q1_level": (i32, [vp, i32, P_ell, P_ell, P_ell, P_ell]),
     "hb_q1_solve": (i32, [vp, vp, vp, f64, f64, i64, i64, vp]),
+    "hb_q1_set_fused_tail": (i32, [vp, i64]),
     "hb_q1_batch_solve": (i32, [vp, vp, vp, vp, i64, f64, f64, i64, i64, vp, vp]),
     # geometric transfers
     "hb_prolongate_f64": (i32, [vp, i64, vp, vp, vp]),

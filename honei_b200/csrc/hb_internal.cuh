@@ -119,6 +119,17 @@ struct hb_q1_view {
 };
 int hb_mg_view(const hb_mg *mg, hb_q1_view *out);
 int hb_q1_view_of(const hb_q1 *q, hb_q1_view *out);
+// The fused coarse cycle: levels 0..top of a served system's banded FP32 hierarchy as one
+// single-cluster launch (a device descriptor built once; hb_tail_launch runs the V-cycle of
+// those levels on X = z, zero on entry, and B = r, with the same arithmetic as the per-level
+// kernels).  hb_mg_enable_tail switches an hb_mg's cycle to it for the levels of at most max_rows
+// rows (0: per-level kernels only).
+// Off by default: measured on B200, graph-replayed per-level kernels (about 1.5 us each) beat one
+// 16-CTA cluster with a barrier per phase for single solves (65^2 .. 2049^2).
+constexpr int64_t HB_TAIL_DEFAULT_ROWS = 0;
+int hb_tail_create(hb_context *ctx, const hb_q1_view &v, int top, void **desc);
+int hb_tail_launch(hb_context *ctx, const void *desc, float *z, const float *r);
+int hb_mg_enable_tail(hb_mg *mg, int64_t max_rows);
 
 // --------------------------------------------------------------------------------------
 // Device helpers

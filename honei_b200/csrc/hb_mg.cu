@@ -42,6 +42,10 @@ struct hb_mg {
     // optional banded levels (hb_mg_create_banded): levels >= 1 smooth and take defects with the
     // banded operator and transfer matrix-free; level 0 keeps its ELL matrix for the coarse CG
     std::vector<hb_q1band> B;
+    // fused coarse cycle (FP32 banded hierarchies with a dense coarse solve): levels <= tail_level
+    // run as one single-cluster launch; tail_desc is its device descriptor
+    int tail_level = -1, tail_top = -1;
+    void *tail_desc = nullptr;
 };
 
 namespace {
@@ -150,9 +154,20 @@ __global__ void dense_solve_kernel(int64_t n, const T *__restrict__ inv, const T
     }
 }
 
+// The fused coarse cycle applies to FP32 hierarchies only.
+inline bool run_tail(hb_mg *mg, int l, float *X, const float *B, int *st)
+{
+    if (l != mg->tail_level || !mg->tail_desc) return false;
+    *st = hb_tail_launch(mg->ctx, mg->tail_desc, X, B);
+    return true;
+}
+inline bool run_tail(hb_mg *, int, double *, const double *, int *) { return false; }
+
 template <typename T> int vcycle(hb_mg *mg, int l, T *X, const T *B)
 {
     hb_context *ctx = mg->ctx;
+    int tst = HB_OK;
+    if (run_tail(mg, l, X, B, &tst)) return tst;
     if (l == 0 && mg->coarse_inv) {
         dense_solve_kernel<T><<<1, 128, 0, ctx->stream>>>(mg->A[0].rows, tp<T>(mg->coarse_inv), B, X);
         return hb_check_launch(ctx, "dense_solve_kernel");
@@ -295,6 +310,35 @@ int hb_mg_finest(hb_mg *mg, hb_ell *A)
 int hb_mg_set_dense_coarse(hb_mg *mg, void *inv)
 {
     mg->coarse_inv = inv;
+    return HB_OK;
+}
+
+int hb_mg_enable_tail(hb_mg *mg, int64_t max_rows)
+{
+    if (!mg || max_rows < 0) return HB_ERR_INVALID;
+    mg->tail_level = -1;
+    if (max_rows == 0) return HB_OK;
+    if (mg->dtype != HB_F32 || mg->B.empty() || !mg->coarse_inv) return HB_ERR_UNSUPPORTED;
+    int top = -1;
+    for (int l = 0; l < mg->L; ++l)
+        if (mg->A[l].rows <= max_rows) top = l;
+    if (top < 1) return HB_OK;   // nothing to fuse above the dense coarse solve
+    if (mg->tail_desc && mg->tail_top != top) {
+        cudaFreeAsync(mg->tail_desc, mg->ctx->stream);
+        mg->tail_desc = nullptr;
+    }
+    if (!mg->tail_desc) {
+        hb_q1_view v;
+        HB_TRY(hb_mg_view(mg, &v));
+        v.L = mg->L;
+        for (int l = 0; l < mg->L; ++l) {
+            v.A32[l] = mg->A[l];
+            v.B32[l] = mg->B[l];
+        }
+        HB_TRY(hb_tail_create(mg->ctx, v, top, &mg->tail_desc));
+        mg->tail_top = top;
+    }
+    mg->tail_level = top;
     return HB_OK;
 }
 
@@ -563,6 +607,7 @@ int hb_mg_destroy(hb_mg *mg)
 {
     if (!mg) return HB_ERR_INVALID;
     // stream-ordered: the memory returns to the pool once the stream's queued work is done
+    if (mg->tail_desc) cudaFreeAsync(mg->tail_desc, mg->ctx->stream);
     cudaFreeAsync(mg->mem, mg->ctx->stream);
     delete mg;
     return HB_OK;

@@ -364,6 +364,8 @@ int q1_build(hb_q1 *q, const double *coef)
                                                      (int)q->A64[0].K, q->gj, q->coarse_inv, singular);
     if ((st = hb_check_launch(ctx, "dense_inverse_kernel"))) return st;
     hb_mg_set_dense_coarse(q->mg, q->coarse_inv);
+    // the coarse levels of the cycle as one single-cluster launch (same arithmetic)
+    if ((st = hb_mg_enable_tail(q->mg, HB_TAIL_DEFAULT_ROWS))) return st;
     const int64_t n = q->M * q->M, ldn = hb_round_up(n, 64);
     if ((st = q1_alloc(q, &p, (size_t)ldn * 8))) return st;
     q->r64 = (double *)p;
@@ -550,6 +552,20 @@ int hb_q1_view_of(const hb_q1 *q, hb_q1_view *out)
 }
 
 extern "C" {
+
+int hb_q1_set_fused_tail(hb_q1 *q, int64_t max_rows)
+{
+    if (!q) return HB_ERR_INVALID;
+    int st = hb_mg_enable_tail(q->mg, max_rows);
+    if (st) return st;
+    // the captured PCG iteration holds the old cycle: capture again on the next solve
+    if (q->graph) {
+        cudaStreamSynchronize(q->ctx->stream);
+        cudaGraphExecDestroy(q->graph);
+        q->graph = nullptr;
+    }
+    return HB_OK;
+}
 
 int hb_q1_solve(hb_q1 *q, const double *b, double *x, double eps, double inner_eps, int64_t max_outer,
                 int64_t max_inner, hb_batch_result *info)

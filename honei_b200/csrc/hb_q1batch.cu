@@ -512,34 +512,14 @@ __global__ void __launch_bounds__(THREADS, 1) q1batch_kernel(const QSys *__restr
 }
 
 
+int build_levels(const hb_q1_view &v, int L, QSys &S);
+
 int build(const hb_q1_view &v, const double *b, double *x, double eps, double inner_eps, int64_t max_outer,
           int64_t max_inner, hb_batch_result *res, QSys &S)
 {
     S = QSys{};
-    S.L = v.L;
-    S.n_pre = v.n_pre;
-    S.n_post = v.n_post;
-    for (int l = 0; l < v.L; ++l) {
-        QLevel &q = S.lv[l];
-        const hb_q1band &bb = v.B32[l];
-        q.n = v.A32[l].rows;
-        q.ld = v.A32[l].ld;
-        q.side = bb.root;
-        if (bb.n != q.n || bb.root * bb.root != q.n || bb.dtype != HB_F32) return HB_ERR_SIZE;
-        if (l > 0 && S.lv[l - 1].side != q.side / 2 + 1) return HB_ERR_SIZE;
-        q.A.n = bb.n;
-        q.A.root = bb.root;
-        for (int k = 0; k < 9; ++k) {
-            q.A.b[k] = (const float *)bb.band[k];
-            if (!q.A.b[k] || ((uintptr_t)q.A.b[k] & 15)) return HB_ERR_INVALID;
-        }
-        q.jac = v.jac[l];
-        q.c = v.c[l];
-        q.d = v.d[l];
-        q.store = v.store[l];
-        q.xt = v.xt[l];
-    }
-    S.inv = v.coarse_inv;
+    int st = build_levels(v, v.L, S);
+    if (st) return st;
     S.n = v.A64.rows;
     S.ld = v.A64.ld;
     S.K = (int)v.A64.K;
@@ -562,6 +542,47 @@ int build(const hb_q1_view &v, const double *b, double *x, double eps, double in
     if (S.ld != S.lv[v.L - 1].ld) return HB_ERR_SIZE;
     return HB_OK;
 }
+
+// Levels 0..L-1 of a view into S (banded FP32 levels, Jacobi diagonals, vectors, coarse inverse).
+int build_levels(const hb_q1_view &v, int L, QSys &S)
+{
+    S.L = L;
+    S.n_pre = v.n_pre;
+    S.n_post = v.n_post;
+    for (int l = 0; l < L; ++l) {
+        QLevel &q = S.lv[l];
+        const hb_q1band &bb = v.B32[l];
+        q.n = v.A32[l].rows;
+        q.ld = v.A32[l].ld;
+        q.side = bb.root;
+        if (bb.n != q.n || bb.root * bb.root != q.n || bb.dtype != HB_F32) return HB_ERR_SIZE;
+        if (l > 0 && S.lv[l - 1].side != q.side / 2 + 1) return HB_ERR_SIZE;
+        q.A.n = bb.n;
+        q.A.root = bb.root;
+        for (int k = 0; k < 9; ++k) {
+            q.A.b[k] = (const float *)bb.band[k];
+            if (!q.A.b[k] || ((uintptr_t)q.A.b[k] & 15)) return HB_ERR_INVALID;
+        }
+        q.jac = v.jac[l];
+        q.c = v.c[l];
+        q.d = v.d[l];
+        q.store = v.store[l];
+        q.xt = v.xt[l];
+    }
+    S.inv = v.coarse_inv;
+    if (!S.inv) return HB_ERR_INVALID;
+    return HB_OK;
+}
+
+// The coarse part of a served system's cycle in one launch: one cluster runs the V-cycle of
+// levels 0..S.L-1 (S.L - 1 = the fused top level) on X = z (zero on entry) and B = r.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1) q1_tail_kernel(const QSys *__restrict__ S, float *z, const float *r)
+{
+    vcycle(*S, z, r);
+}
+
+constexpr int TAIL_CLUSTER = 16, TAIL_THREADS = 256;
 
 template <int THREADS> int launch(hb_context *ctx, int cluster, int max_clusters, const QSys *sys, int64_t count,
                                   unsigned long long *counter)
@@ -597,6 +618,54 @@ template <int THREADS> int launch(hb_context *ctx, int cluster, int max_clusters
 }
 
 }  // namespace
+
+int hb_tail_create(hb_context *ctx, const hb_q1_view &v, int top, void **desc)
+{
+    if (!ctx || !desc || top < 1 || top >= v.L) return HB_ERR_INVALID;
+    QSys S{};
+    int st = build_levels(v, top + 1, S);
+    if (st) return st;
+    S.n_pre = v.n_pre;
+    S.n_post = v.n_post;
+    void *d = nullptr;
+    if (cudaMallocAsync(&d, sizeof(QSys), ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return HB_ERR_ALLOC;
+    }
+    if (cudaMemcpyAsync(d, &S, sizeof(QSys), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFreeAsync(d, ctx->stream);
+        return HB_ERR_CUDA;
+    }
+    if (TAIL_CLUSTER > 8 &&
+        cudaFuncSetAttribute(q1_tail_kernel<TAIL_THREADS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        cudaFreeAsync(d, ctx->stream);
+        return HB_ERR_UNSUPPORTED;
+    }
+    *desc = d;
+    return HB_OK;
+}
+
+int hb_tail_launch(hb_context *ctx, const void *desc, float *z, const float *r)
+{
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = TAIL_CLUSTER;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(TAIL_CLUSTER);
+    cfg.blockDim = dim3(TAIL_THREADS);
+    cfg.stream = ctx->stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, q1_tail_kernel<TAIL_THREADS>, (const QSys *)desc, z, r);
+    if (e != cudaSuccess) { hb_note_error(ctx, e, "cudaLaunchKernelEx(q1_tail_kernel)"); return HB_ERR_CUDA; }
+    return hb_check_launch(ctx, "q1_tail_kernel");
+}
 
 extern "C" {
 

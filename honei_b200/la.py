@@ -724,6 +724,10 @@ class Q1System:
         check(lib().hb_q1_levels(h, C.byref(nl), sides), "hb_q1_levels")
         self.sides = [sides[i] for i in range(nl.value)]
 
+    def set_fused_tail(self, max_rows: int):
+        """hb_q1_set_fused_tail: the levels of at most max_rows rows in one launch (0: per level)."""
+        check(lib().hb_q1_set_fused_tail(self.handle, int(max_rows)), "hb_q1_set_fused_tail", self.ctx.handle)
+
     @staticmethod
     def solve_batch(systems, bs, xs, eps=1e-8, inner_eps=1e-3, max_outer=50, max_inner=1000, cluster=8,
                     threads=256, max_clusters=0, ctx: Context | None = None):

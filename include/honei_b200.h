@@ -289,9 +289,9 @@ typedef struct {
 
 int hb_mg_create(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *prol,
                  const hb_ell *res, const hb_mg_params *params, hb_mg **out);
-/* The same multigrid on (2^k + 1)^2 Q1 grids with banded level matrices B[l] (hb_q1band; side
- * 2 * (coarser side) - 1) and matrix-free bilinear transfers with Dirichlet fine rows zero (the
- * PROLMAT matrices of the rediscretised hierarchy, never stored).  Levels >= 1 smooth and take
+/* The same multigrid on square Q1 grids with banded level matrices B[l] (hb_q1band; coarse side
+ * = finer side / 2 + 1, the 2:1 coarsening for (2^k + 1) sides) and matrix-free bilinear
+ * transfers with Dirichlet fine rows zero (the PROLMAT matrices, never stored).  Levels >= 1 smooth and take
  * defects with B[l]; level 0 keeps A[0] for its coarse CG; A[l] also gives the Jacobi diagonals.
  * Every operation rounds as the ELL cycle on the same matrices (bit-identical iterates); per fine
  * row the cycle reads no column indices and no transfer matrix. */
@@ -419,6 +419,12 @@ int hb_q1_level(const hb_q1 *q, int level, hb_ell *A64, hb_ell *A32, hb_ell *P32
  * defect0/defect = FP64 defect norms, true_relres = ||b - A x|| / ||b||. */
 int hb_q1_solve(hb_q1 *q, const double *b, double *x, double eps, double inner_eps, int64_t max_outer,
                 int64_t max_inner, hb_batch_result *info);
+
+/* Runs the coarse levels of the served solve's cycle -- those of at most max_rows rows -- as one
+ * single-cluster launch: the same arithmetic as the per-level kernels, so the same iterates, in
+ * one launch instead of about eight per level.  max_rows = 0 (the default) runs every level with
+ * its own kernels, which measured faster for single solves on B200. */
+int hb_q1_set_fused_tail(hb_q1 *q, int64_t max_rows);
 
 /* Batched served solves (no reference counterpart): count distinct hb_q1 systems, each with its
  * own b[i] and x[i] (device, x holds x0), solved in one persistent launch with the algorithm of

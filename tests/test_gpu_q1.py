@@ -176,3 +176,26 @@ def test_batched_served_solve_alone_equals_in_the_mix(hb):
         hb.Q1System.solve_batch([systems[0], systems[0]], [bs[0], bs[0]], [mix[0], mix[0]])
     for q in systems:
         q.close()
+
+
+@pytest.mark.parametrize("M", [9, 17, 100, 257, 300, 700])
+def test_fused_coarse_cycle_same_iterates(hb, M):
+    """The coarse levels of the served cycle in one single-cluster launch compute exactly what the
+    per-level kernels compute: the same solve, bit for bit."""
+    coef = torch.from_numpy(P.log_uniform_coef(M, 1e-2, 1e2, 3 + M).ravel()).cuda()
+    q = hb.Q1System(M, coef)
+    xt = torch.from_numpy(P.uniform_vector(M * M, 9)).cuda()
+    b = torch.empty_like(xt)
+    hb.Product.value(b, q.A, xt)
+    x1 = torch.zeros_like(b)
+    i1 = q.solve(b, x1, eps=1e-8)
+    q.set_fused_tail(0)
+    x0 = torch.zeros_like(b)
+    i0 = q.solve(b, x0, eps=1e-8)
+    assert i0 == i1 and torch.equal(x0, x1), (i0, i1)
+    for rows in (289, 17000, 70000):
+        q.set_fused_tail(rows)
+        x2 = torch.zeros_like(b)
+        i2 = q.solve(b, x2, eps=1e-8)
+        assert i2 == i1 and torch.equal(x2, x1), (rows, i2, i1)
+    q.close()
