@@ -598,6 +598,18 @@ def run_ours(args):
                 "solves_per_s": round(len(lat) / sum(lat), 2),
                 "p50_ms": round(statistics.median(lat_ms), 3),
                 "p99_ms": round(lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))], 3)}
+    if ws == 1 and not args.no_cpu_baseline:
+        # the reference's own CGSolver<MultiCore::SSE> on the host cores, same system
+        R = _ref_cpu()
+        if R is not None:
+            Ah = P.q1_poisson(M_CG)
+            secs = []
+            for _ in range(3):
+                _, used_ref, sec = R.cg(Ah, bh.numpy(), eps=1e-8, max_iters=20000, tag="mc-sse")
+                secs.append(sec)
+            cg_extra["cpu_reference"] = {"ms": round(1e3 * statistics.median(secs), 2), "iterations": used_ref,
+                                         "cores": os.cpu_count(), "tag": "tags::CPU::MultiCore::SSE"}
+            cg_extra["speedup_vs_cpu_reference"] = round(1e3 * statistics.median(secs) / cg_extra["p50_ms"], 1)
 
     cg_cluster = bench_cg_cluster(ctx)
     batch_extra = None if args.no_batch else bench_batch(la, ctx, n_systems=args.batch_systems)
