@@ -85,6 +85,7 @@ SIGNATURES = {
     "hb_convert_f32_f64": (i32, [vp, i64, vp, vp]),
     "hb_cg_f64": (i32, [vp, P_ell, vp, vp, i64, f64, P_i64, C.POINTER(f64)]),
     "hb_cg_f32": (i32, [vp, P_ell, vp, vp, i64, f32, P_i64, C.POINTER(f32)]),
+    "hb_selftest_wait_timeout": (i32, [vp]),
     "hb_cg_var_diag_f64": (i32, [vp, P_ell, vp, vp, vp, i64, f64, P_i64, C.POINTER(f64)]),
     "hb_cg_var_diag_f32": (i32, [vp, P_ell, vp, vp, vp, i64, f32, P_i64, C.POINTER(f32)]),
     "hb_cg_var_ell_f64": (i32, [vp, P_ell, P_ell, vp, vp, i64, f64, P_i64, C.POINTER(f64)]),

@@ -420,7 +420,43 @@ int cg_impl(hb_context *ctx, const hb_ell *A, const T *b, T *x, int64_t max_iter
 
 }  // namespace
 
+namespace {
+
+// One block waits at a grid barrier sized for two: the second arrival never comes, so the wait
+// runs to its limit (HB_WAIT_NS), records HB_DEV_TIMEOUT and the kernel returns.
+__global__ void wait_timeout_kernel(hbd::GridBarrier bar, hb_solve_result *res)
+{
+    __shared__ int s_flag;
+    const bool ok = bar.sync(2, &s_flag);
+    if (threadIdx.x == 0) {
+        res->used = ok ? 1 : 0;
+        res->status = *(volatile int *)bar.status;
+    }
+}
+
+}  // namespace
+
 extern "C" {
+
+int hb_selftest_wait_timeout(hb_context *ctx)
+{
+    if (!ctx) return HB_ERR_INVALID;
+    unsigned *w = hb_bar(ctx);
+    hbd::GridBarrier bar;
+    bar.count = w;
+    bar.gen = w + 1;
+    bar.status = (int *)(w + 2);
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(w, 0, 4 * sizeof(unsigned), ctx->stream));
+    wait_timeout_kernel<<<1, 32, 0, ctx->stream>>>(bar, hb_result(ctx));
+    int st = hb_check_launch(ctx, "wait_timeout_kernel");
+    if (st) return st;
+    hb_solve_result *h = (hb_solve_result *)ctx->pinned;
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, hb_result(ctx), sizeof(hb_solve_result), cudaMemcpyDeviceToHost, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    // leave the barrier words clean for the next cooperative launch
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(w, 0, 4 * sizeof(unsigned), ctx->stream));
+    return (h->status == HB_DEV_TIMEOUT && h->used == 0) ? HB_ERR_TIMEOUT : HB_ERR_CUDA;
+}
 
 int hb_cg_f64(hb_context *ctx, const hb_ell *A, const double *b, double *x, int64_t max_iters,
               double eps, int64_t *used_iters, double *final_defect)

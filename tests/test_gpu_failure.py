@@ -1,0 +1,55 @@
+"""Failure handling on the device without a GPU fault: a bounded wait that runs out reports
+HB_ERR_TIMEOUT to the host and leaves the context usable; errors from bad inputs are refused
+before any launch."""
+import time
+
+import numpy as np
+import pytest
+
+from honei_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def hb():
+    from honei_b200 import la
+    assert torch.cuda.is_available()
+    return la
+
+
+def test_bounded_wait_times_out_and_the_context_stays_usable(hb, oracle):
+    from honei_b200._lib import lib
+    ctx = hb.default_context()
+    t0 = time.perf_counter()
+    st = lib().hb_selftest_wait_timeout(ctx.handle)
+    dt = time.perf_counter() - t0
+    assert st == 5, st                    # HB_ERR_TIMEOUT
+    assert 1.5 < dt < 30.0
+    # the same context solves normally afterwards (the barrier words were reset)
+    A = P.q1_poisson(65)
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 1))
+    Ad = hb.SparseMatrixELL.from_reference(A)
+    x = torch.zeros(A.rows, dtype=torch.float64, device="cuda")
+    used = hb.CGSolver.value(Ad, None, torch.from_numpy(b).cuda(), x, 5000, 1e-8)
+    x_o, u_o = oracle.cg(A, b, eps=1e-8, max_iters=5000)
+    assert abs(used - u_o) <= 1
+
+
+def test_invalid_inputs_are_refused_before_launch(hb):
+    from honei_b200._lib import HBError, lib
+    ctx = hb.default_context()
+    A = hb.SparseMatrixELL.from_reference(P.q1_poisson(9))
+    torch.cuda.synchronize()
+    launches = ctx.launches()
+    with pytest.raises(hb.VectorSizeDoesNotMatch):
+        hb.Product.value(torch.empty(80, dtype=torch.float64, device="cuda"), A,
+                         torch.empty(81, dtype=torch.float64, device="cuda"))
+    # a misaligned matrix array is refused by the C ABI itself
+    import ctypes as C
+    from honei_b200._lib import HbEll
+    bad = HbEll(81, 81, A.K, A.ld, A.Aj.data_ptr() + 4, A.Ax.data_ptr(), 0, 0)
+    x = torch.zeros(81, dtype=torch.float64, device="cuda")
+    assert lib().hb_spmv_f64(ctx.handle, C.byref(bad), x.data_ptr(), x.data_ptr()) == 1
+    assert ctx.launches() == launches
