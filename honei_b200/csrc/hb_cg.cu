@@ -336,6 +336,265 @@ int launch_cg_small(hb_context *ctx, const CGParams<T> &P, int64_t groups)
     return hb_check_launch(ctx, "cg_small_kernel");
 }
 
+// ---------------------------------------------------------------------------------------
+// Resident-operator form, for systems whose rows fit the shared memory of one block per SM:
+// each block owns a contiguous row range, keeps its ELL rows (Ax, and Aj as window offsets),
+// x and v of its rows, and r and p on its column window (its own rows plus the columns its rows
+// reach) in shared memory for the whole solve.  p on the window is formed redundantly by every
+// block that holds it (the same p = beta p + r, bit for bit), so only r crosses blocks: each
+// block stores its rows of r, and after the second exchange of an iteration reads the window's
+// other rows (the halo) from L2 together with the partials.  Both reductions per iteration go
+// through the arrival-counter exchange.  A column outside the window (a block whose rows reach
+// further than the window capacity) is gathered from the global r and p, which every block also
+// stores for its rows; the arithmetic is the same either way.  Per row the product sums the
+// slots in slot order skipping padding, as the ELL product does; the dot products are sums per
+// thread over its rows, a block tree and a tree over the block partials -- deterministic, the
+// same in every block.
+// ---------------------------------------------------------------------------------------
+constexpr int RES_THREADS = 512;
+
+template <typename T> struct ResParams {
+    CGParams<T> c;
+    int64_t rpb;     // rows per block
+    int64_t wcap;    // window capacity: entries of r and of p held in shared memory
+    hbd::CountExchange X;
+};
+
+template <typename T>
+__device__ __forceinline__ T res_total(const T *slots, unsigned e, unsigned G, T *red, T *bcast)
+{
+    T v = threadIdx.x < G ? __ldcg(slots + (e & 1u) * G + threadIdx.x) : T(0);
+    v = hbd::block_sum(v, red);
+    if (threadIdx.x == 0) *bcast = v;
+    __syncthreads();
+    return *bcast;
+}
+
+template <typename T, int KT>
+__global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<T> Q)
+{
+    using hbd::add; using hbd::mul; using hbd::sub;
+    extern __shared__ __align__(16) unsigned char res_smem[];
+    __shared__ T red[32];
+    __shared__ T bcast;
+    __shared__ int s_flag, s_min, s_max;
+    const CGParams<T> &P = Q.c;
+    const int K = KT > 0 ? KT : P.K;
+    const int64_t rpb = Q.rpb, wcap = Q.wcap;
+    const unsigned G = gridDim.x;
+    const int64_t lo = (int64_t)blockIdx.x * rpb;
+    const int64_t hi = min(P.rows, lo + rpb);
+    const int nr = hi > lo ? (int)(hi - lo) : 0;
+    T *Ax_s = (T *)res_smem;                    // [K][rpb]
+    T *r_w = Ax_s + (int64_t)K * rpb;           // [wcap]
+    T *p_w = r_w + wcap;                        // [wcap]
+    T *x_s = p_w + wcap;                        // [rpb]
+    T *v_s = x_s + rpb;                         // [rpb]
+    int32_t *Aj_s = (int32_t *)(v_s + rpb);     // [K][rpb]: window offset, -1 padding, -(j + 2) outside
+
+    // column span of the block's rows (own rows included)
+    if (threadIdx.x == 0) { s_min = INT_MAX; s_max = -1; }
+    __syncthreads();
+    {
+        int cmin = INT_MAX, cmax = -1;
+        for (int64_t q = threadIdx.x; q < (int64_t)K * nr; q += blockDim.x) {
+            const int k = (int)(q / nr), il = (int)(q - (int64_t)k * nr);
+            const int32_t j = P.Aj[(int64_t)k * P.ld + lo + il];
+            if (j >= 0) { cmin = min(cmin, (int)j); cmax = max(cmax, (int)j); }
+        }
+        if (nr > 0) { cmin = min(cmin, (int)lo); cmax = max(cmax, (int)(hi - 1)); }
+        atomicMin(&s_min, cmin);
+        atomicMax(&s_max, cmax);
+    }
+    __syncthreads();
+    int64_t wlo = 0, W = 0;
+    if (nr > 0) {
+        if ((int64_t)s_max - s_min + 1 <= wcap) { wlo = s_min; W = (int64_t)s_max - s_min + 1; }
+        else {
+            wlo = lo - (wcap - nr) / 2;
+            if (wlo < 0) wlo = 0;
+            W = wcap < P.rows - wlo ? wcap : P.rows - wlo;
+        }
+    }
+    const int64_t own = lo - wlo;    // window offset of the block's first row
+    for (int64_t q = threadIdx.x; q < (int64_t)K * nr; q += blockDim.x) {
+        const int k = (int)(q / nr), il = (int)(q - (int64_t)k * nr);
+        const int64_t gi = (int64_t)k * P.ld + lo + il;
+        const int32_t j = P.Aj[gi];
+        Ax_s[(int64_t)k * rpb + il] = P.Ax[gi];
+        Aj_s[(int64_t)k * rpb + il] = j < 0 ? -1 : ((j >= wlo && j < wlo + W) ? (int32_t)(j - wlo) : -(j + 2));
+    }
+    __syncthreads();
+
+    // r = b - A x (Defect), alpha = r.r
+    T acc = T(0);
+    for (int il = threadIdx.x; il < nr; il += blockDim.x) {
+        T s = T(0);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int32_t c = Aj_s[(int64_t)k * rpb + il];
+            if (c == -1) continue;
+            const int64_t j = c >= 0 ? (int64_t)c + wlo : -(int64_t)c - 2;
+            s = add(s, mul(Ax_s[(int64_t)k * rpb + il], P.x_user[j]));
+        }
+        const T r = sub(P.b_user[lo + il], s);
+        r_w[own + il] = r;
+        x_s[il] = P.x_user[lo + il];
+        __stcg(P.r + lo + il, r);
+        acc = add(acc, mul(r, r));
+    }
+    acc = hbd::block_sum(acc, red);
+    unsigned e = 0;
+    bool ok = Q.X.arrive_wait(acc, P.partials, e, G, &s_flag);
+    // the window's other rows of r (halo), loaded beside the partials
+    const int64_t n_left = nr > 0 ? own : 0, n_halo = nr > 0 ? own + (wlo + W - hi) : 0;
+    auto halo = [&]() {
+        for (int64_t q = threadIdx.x; q < n_halo; q += 2 * (int64_t)blockDim.x) {
+            const int64_t q2 = q + blockDim.x;
+            const int64_t w1 = q < n_left ? q : q - n_left + (hi - wlo);
+            const int64_t w2 = q2 < n_left ? q2 : q2 - n_left + (hi - wlo);
+            const T a = __ldcg(P.r + wlo + w1);
+            const T b = q2 < n_halo ? __ldcg(P.r + wlo + w2) : T(0);
+            r_w[w1] = a;
+            if (q2 < n_halo) r_w[w2] = b;
+        }
+    };
+    T alpha = T(0);
+    if (ok) {
+        halo();
+        alpha = res_total(P.partials, e, G, red, &bcast);
+    }
+    const T initial_defect = dsqrt(alpha);
+    T current_defect = T(0);
+    T beta = T(0);
+    const T epsm = eps_mach<T>();
+    T *pin = P.p0, *pout = P.p1;
+    int64_t it = 0, used = 0;
+    while (ok && it < P.max_iters) {
+        // ---- phase 1: p = beta p + r on the window (first iteration: p = r), v = A p, v.p
+        const bool first = (it == 0);
+        for (int64_t w = threadIdx.x; w < W; w += blockDim.x) p_w[w] = first ? r_w[w] : add(mul(p_w[w], beta), r_w[w]);
+        __syncthreads();
+        acc = T(0);
+        for (int il = threadIdx.x; il < nr; il += blockDim.x) {
+            T s = T(0);
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const int32_t c = Aj_s[(int64_t)k * rpb + il];
+                if (c == -1) continue;
+                T pj;
+                if (c >= 0) {
+                    pj = p_w[c];
+                } else {
+                    const int64_t j = -(int64_t)c - 2;
+                    const T rj = __ldcg(P.r + j);
+                    pj = first ? rj : add(mul(__ldcg(pin + j), beta), rj);
+                }
+                s = add(s, mul(Ax_s[(int64_t)k * rpb + il], pj));
+            }
+            v_s[il] = s;
+            const T pi = p_w[own + il];
+            __stcg(pout + lo + il, pi);
+            acc = add(acc, mul(s, pi));
+        }
+        acc = hbd::block_sum(acc, red);
+        if (!Q.X.arrive_wait(acc, P.partials, ++e, G, &s_flag)) break;
+        const T temp = res_total(P.partials, e, G, red, &bcast);
+        const T lambda = alpha / (fabs(temp) > epsm ? temp : epsm);
+        const T mlambda = -lambda;
+
+        // ---- phase 2: x += lambda p; r += (-lambda) v; alpha = r.r
+        acc = T(0);
+        for (int il = threadIdx.x; il < nr; il += blockDim.x) {
+            x_s[il] = add(x_s[il], mul(lambda, p_w[own + il]));
+            const T r = add(r_w[own + il], mul(mlambda, v_s[il]));
+            r_w[own + il] = r;
+            __stcg(P.r + lo + il, r);
+            acc = add(acc, mul(r, r));
+        }
+        acc = hbd::block_sum(acc, red);
+        if (!Q.X.arrive_wait(acc, P.partials, ++e, G, &s_flag)) break;
+        halo();
+        const T alpha_old = alpha;
+        alpha = res_total(P.partials, e, G, red, &bcast);
+        beta = alpha / (fabs(alpha_old) > epsm ? alpha_old : epsm);
+        T *t = pin; pin = pout; pout = t;
+        ++it;
+        current_defect = dsqrt(alpha);
+        if (current_defect < P.eps * initial_defect) { used = it; break; }
+        if (current_defect < P.eps) { used = it; break; }
+        if (it == P.max_iters) used = it;
+    }
+    for (int il = threadIdx.x; il < nr; il += blockDim.x) P.x_user[lo + il] = x_s[il];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        P.res->used = used;
+        P.res->defect0 = (double)initial_defect;
+        P.res->defect = (double)current_defect;
+        P.res->status = *(volatile int *)Q.X.status;
+    }
+}
+
+// Shared memory of cg_res_kernel for rpb rows per block and a window of wcap entries.
+template <typename T> size_t res_smem_bytes(int K, int64_t rpb, int64_t wcap)
+{
+    return (size_t)((int64_t)K * rpb + 2 * wcap + 2 * rpb) * sizeof(T) + (size_t)K * rpb * sizeof(int32_t);
+}
+
+// Plans the resident form: one block per SM (fewer for small systems, about 128 rows each),
+// the window as large as the shared memory left over allows.  Returns false when the rows of a
+// block do not fit.
+template <typename T, int KT>
+bool res_plan(hb_context *ctx, int64_t rows, int K, int *blocks, int64_t *rpb, int64_t *wcap, size_t *smem)
+{
+    int dev = 0, optin = 0, occ = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const size_t avail = (size_t)optin - 1024;    // static shared memory of the kernel
+    const int64_t G = std::max<int64_t>(1, std::min<int64_t>(ctx->num_sms, (rows + 127) / 128));
+    const int64_t r = (rows + G - 1) / G;
+    const size_t fixed = res_smem_bytes<T>(K, r, 0);
+    if (fixed + 2 * (size_t)r * sizeof(T) > avail) return false;
+    const int64_t w = std::min<int64_t>(rows, (int64_t)((avail - fixed) / (2 * sizeof(T))));
+    const size_t bytes = res_smem_bytes<T>(K, r, w);
+    if (cudaFuncSetAttribute((const void *)cg_res_kernel<T, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)bytes) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, cg_res_kernel<T, KT>, RES_THREADS, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if ((int64_t)occ * ctx->num_sms < G) return false;
+    *blocks = (int)G;
+    *rpb = r;
+    *wcap = w;
+    *smem = bytes;
+    return true;
+}
+
+template <typename T, int KT>
+int launch_cg_res(hb_context *ctx, CGParams<T> &P, bool *launched)
+{
+    *launched = false;
+    int blocks = 0;
+    int64_t rpb = 0, wcap = 0;
+    size_t smem = 0;
+    if (!res_plan<T, KT>(ctx, P.rows, P.K, &blocks, &rpb, &wcap, &smem)) return HB_OK;
+    ResParams<T> Q;
+    Q.c = P;
+    Q.rpb = rpb;
+    Q.wcap = wcap;
+    Q.X.count = P.bar.count;
+    Q.X.status = P.bar.status;
+    void *args[] = {&Q};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *)cg_res_kernel<T, KT>, dim3(blocks), dim3(RES_THREADS),
+                                                args, smem, ctx->stream);
+    if (e != cudaSuccess) { hb_note_error(ctx, e, "cudaLaunchCooperativeKernel(cg_res_kernel)"); return HB_ERR_CUDA; }
+    *launched = true;
+    return hb_check_launch(ctx, "cg_res_kernel");
+}
+
 template <typename T, int KT>
 int launch_cg_kt(hb_context *ctx, CGParams<T> &P, int blocks)
 {
@@ -387,6 +646,11 @@ int hb_launch_cg(hb_context *ctx, const hb_ell *A, const T *b, T *x, int64_t max
     // about one row group per thread for small systems; all co-resident blocks otherwise
     const int64_t want = (groups + CG_THREADS - 1) / CG_THREADS;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(maxb, 4096)));
+    if (ctx->cg_resident) {
+        bool launched = false;
+        const int st = k9 ? launch_cg_res<T, 9>(ctx, P, &launched) : launch_cg_res<T, 0>(ctx, P, &launched);
+        if (st || launched) return st;
+    }
     return k9 ? launch_cg_kt<T, 9>(ctx, P, blocks) : launch_cg_kt<T, 0>(ctx, P, blocks);
 }
 template int hb_launch_cg<double>(hb_context *, const hb_ell *, const double *, double *, int64_t, double,

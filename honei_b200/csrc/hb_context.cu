@@ -135,6 +135,14 @@ uint64_t hb_launch_count(hb_context *ctx)
     return ctx ? ctx->launches : 0;
 }
 
+int hb_cg_set_resident(hb_context *ctx, int enable)
+{
+    if (!ctx) return HB_ERR_INVALID;
+    const int prev = ctx->cg_resident;
+    ctx->cg_resident = enable != 0;
+    return prev;
+}
+
 int hb_reserve(hb_context *ctx, int64_t n)
 {
     if (!ctx || n < 0) return HB_ERR_INVALID;

@@ -45,6 +45,8 @@ struct hb_context {
     // pinned host slot for scalar readback
     void *pinned = nullptr;
     uint64_t launches = 0;
+    // CG on systems that fit: the resident-operator kernel (hb_cg_set_resident)
+    int cg_resident = 1;
     std::string last_error;
 };
 
@@ -205,6 +207,11 @@ __device__ __forceinline__ uint64_t globaltimer()
     return t;
 }
 
+__device__ __forceinline__ void red_release_add(unsigned *p, unsigned v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Warp tree sum in a fixed order (shuffle-down halving): deterministic.
 template <typename T> __device__ __forceinline__ T warp_sum(T v)
 {
@@ -263,6 +270,46 @@ struct GridBarrier {
             }
             __threadfence();
             if (*(volatile int *)status != HB_DEV_OK) ok = 0;
+            *s_flag = ok;
+        }
+        __syncthreads();
+        return *(volatile int *)s_flag != 0;
+    }
+};
+
+// Grid-wide exchange of one partial per block, for cooperative launches, on a monotonic
+// arrival counter (zero before the launch).  Exchange e: thread 0 stores the block's partial in
+// slot array e & 1, adds 1 to the counter with release semantics (fire and forget) and waits
+// until the counter reaches (e + 1) * blocks; every block may then read all partials of e, and
+// everything the other blocks wrote before arriving.  Two slot arrays suffice: a block reaches
+// exchange e + 2 only after every block arrived at e + 1, i.e. after every block read e.
+// Waits are bounded like GridBarrier's (HB_WAIT_NS, HB_DEV_TIMEOUT in the status word; a block
+// that sees another block's failure leaves too).
+struct CountExchange {
+    unsigned *count;
+    int *status;
+
+    template <typename T>
+    __device__ __forceinline__ bool arrive_wait(T partial, T *slots, unsigned e, unsigned nblocks, int *s_flag) const
+    {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int ok = 1;
+            __stcg(slots + (e & 1u) * nblocks + blockIdx.x, partial);
+            red_release_add(count, 1u);
+            const unsigned target = (e + 1u) * nblocks;
+            if ((int)(ld_acquire(count) - target) < 0) {
+                const uint64_t t0 = globaltimer();
+                unsigned n = 0;
+                while ((int)(ld_acquire(count) - target) < 0) {
+                    if ((++n & 31u) == 0 && *(volatile int *)status != HB_DEV_OK) { ok = 0; break; }
+                    if (globaltimer() - t0 > HB_WAIT_NS) {
+                        atomicCAS(status, HB_DEV_OK, HB_DEV_TIMEOUT);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
             *s_flag = ok;
         }
         __syncthreads();

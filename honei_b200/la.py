@@ -536,6 +536,13 @@ class CGSolver:
         CGSolver.last_defect = d.value
         return used.value
 
+    @staticmethod
+    def set_resident(enable: bool, ctx: Context | None = None) -> bool:
+        """Whether CG on ctx uses the resident-operator kernel where the system fits (the
+        default) or always the streaming kernel; returns the previous setting."""
+        ctx = ctx or default_context()
+        return bool(lib().hb_cg_set_resident(ctx.handle, 1 if enable else 0))
+
 
 class CGSolverVAR:
     """CGSolver<tags::GPU::CUDA, methods::VAR>::value (honei/math/cg.hh:140-219): CG with the

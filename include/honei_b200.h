@@ -229,14 +229,22 @@ int hb_convert_f32_f64(hb_context *ctx, int64_t n, double *dst, const float *src
 /* Plain CG, CGSolver<Tag, methods::NONE>::value(A, P, b, x, max_iters, used_iters, eps),
  * honei/math/cg.hh:63-133: same update formulas, the same guarded divisions and the same dual
  * stopping rule (sqrt(alpha) < eps*sqrt(alpha0) or sqrt(alpha) < eps).  The whole loop runs
- * in ONE persistent cooperative kernel (2 grid barriers per iteration, scalars on the
+ * in ONE persistent cooperative kernel (2 grid-wide reductions per iteration, scalars on the
  * device); x holds x0 on entry and the solution on exit.  *used_iters (host) receives the
- * iteration count, *final_defect (host, may be NULL) sqrt(alpha) at exit.
- * Returns HB_ERR_TIMEOUT if a bounded device-side barrier wait gave up. */
+ * iteration count, *final_defect (host, may be NULL) sqrt(alpha) at exit.  Systems whose rows
+ * fit the shared memory of one block per SM run in the resident-operator kernel (matrix rows
+ * and vector windows kept on chip for the whole solve); larger ones stream the matrix each
+ * iteration.  Returns HB_ERR_TIMEOUT if a bounded device-side wait gave up. */
 int hb_cg_f64(hb_context *ctx, const hb_ell *A, const double *b, double *x, int64_t max_iters,
               double eps, int64_t *used_iters, double *final_defect);
 int hb_cg_f32(hb_context *ctx, const hb_ell *A, const float *b, float *x, int64_t max_iters,
               float eps, int64_t *used_iters, float *final_defect);
+
+/* Selects whether hb_cg_f64 / hb_cg_f32 on this context use the resident-operator kernel
+ * where it applies (enable != 0, the default) or always the streaming kernel.  Both give
+ * results within rounding of each other (their dot products use different summation trees);
+ * each is deterministic.  Returns the previous setting. */
+int hb_cg_set_resident(hb_context *ctx, int enable);
 
 /* Preconditioned CG, CGSolver<Tag, methods::VAR>::value(A, P, b, x, max_iters, used_iters,
  * eps), honei/math/cg.hh:140-219, with the preconditioner container P either a vector (the

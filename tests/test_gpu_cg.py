@@ -174,3 +174,60 @@ def test_cg_small_systems_bitwise_equal_to_cooperative_kernel(hb, oracle, M, coe
     assert torch.equal(x1, x2)
     x_o, u_o = oracle.cg(A, b, eps=1e-8, max_iters=1000)
     assert abs(u1 - u_o) <= 1
+
+
+RESIDENT_CASES = [
+    ("q1_257", lambda: P.q1_poisson(257)),
+    ("q1_129_varcoef", lambda: P.q1_poisson(129, P.log_uniform_coef(129, 1e-2, 1e2, 5))),
+    # a random permutation spreads each block's columns past its window: the out-of-window path
+    ("q1_257_permuted", lambda: P.q1_poisson_permuted(257, 4)[0]),
+    ("q1_65_threads4", lambda: P.ell_from_csr(4225, 4225, *P.q1_poisson_csr(65), threads=4)),
+]
+
+
+@pytest.mark.parametrize("name,make", RESIDENT_CASES, ids=[c[0] for c in RESIDENT_CASES])
+def test_cg_resident_kernel_matches_streaming_kernel(hb, oracle, name, make):
+    """Systems that fit run in the resident-operator kernel by default; the streaming kernel
+    solves the same system to the same bar (iterations within 1, the true residual within
+    1e-10), and each kernel is deterministic."""
+    A = make()
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 1))
+    x_r, u_r = run_cg(hb, A, b, 1e-8)
+    x_r2, u_r2 = run_cg(hb, A, b, 1e-8)
+    assert u_r == u_r2 and np.array_equal(x_r, x_r2)
+    prev = hb.CGSolver.set_resident(False)
+    try:
+        x_s, u_s = run_cg(hb, A, b, 1e-8)
+    finally:
+        hb.CGSolver.set_resident(prev)
+    assert prev is True
+    assert abs(u_r - u_s) <= 1, (u_r, u_s)
+    assert abs(relres(oracle, A, b, x_r) - relres(oracle, A, b, x_s)) <= 1e-10
+    assert np.linalg.norm(x_r - x_s) <= 1e-6 * np.linalg.norm(x_s)
+
+
+def test_cg_resident_kernel_edge_cases(hb, oracle):
+    """The resident kernel (65^2: 34 blocks of 125 rows) on the loop's edges: max_iters = 0,
+    a cap that stops the loop, a zero right-hand side, a non-zero start vector, FP32."""
+    A = P.q1_poisson(65)
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 2))
+    x0 = P.uniform_vector(A.rows, 3)
+    x_g, u_g = run_cg(hb, A, b, 1e-8, max_iters=0, x0=x0)
+    assert u_g == 0 and np.array_equal(x_g, x0)
+    x_g, u_g = run_cg(hb, A, b, 1e-12, max_iters=7)
+    x_o, u_o = oracle.cg(A, b, eps=1e-12, max_iters=7)
+    assert u_g == u_o == 7 and np.linalg.norm(x_g - x_o) <= 1e-12 * np.linalg.norm(x_o)
+    x_g, u_g = run_cg(hb, A, np.zeros(A.rows), 1e-8)
+    x_o, u_o = oracle.cg(A, np.zeros(A.rows), eps=1e-8)
+    assert u_g == u_o and np.array_equal(x_g, x_o)
+    x_g, u_g = run_cg(hb, A, b, 1e-8, x0=x0)
+    x_o, u_o = oracle.cg(A, b, x0=x0, eps=1e-8)
+    assert abs(u_g - u_o) <= 1 and abs(relres(oracle, A, b, x_g) - relres(oracle, A, b, x_o)) <= 1e-10
+    A32 = P.q1_poisson(257).astype(np.float32)
+    b32 = oracle.spmv(A32, P.uniform_vector(A32.rows, 1).astype(np.float32))
+    x_o, u_o = oracle.cg(A32, b32, eps=1e-5, max_iters=20000)
+    x_g, u_g = run_cg(hb, A32, b32, 1e-5)
+    assert abs(u_g - u_o) <= 0.02 * u_o + 1, (u_g, u_o)
+    r_o = relres(oracle, A32.astype(np.float64), b32.astype(np.float64), x_o.astype(np.float64))
+    r_g = relres(oracle, A32.astype(np.float64), b32.astype(np.float64), x_g.astype(np.float64))
+    assert abs(r_g - r_o) <= 1e-5, (r_g, r_o)
