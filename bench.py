@@ -331,10 +331,17 @@ def bench_q1band(la, ctx, x, ell_s, M=M_SPMV, reps=100, cpu=True):
     return out
 
 
+MG_COARSE_ITERS = 100
+
+
 def bench_mg(la, ctx, M=2049, seed=5, cpu=True):
     """Q1 Poisson M^2 (unit coefficient, the reference's rediscretised hierarchy down to 9^2):
     MGSolver V(2,2), damped Jacobi 0.7, PROLMAT transfers, coarse CG, x0 = 0, b = A x_true.
-    FP64 to 1e-8 relative; FP32 to 1e-6 (FP32 stagnates near 1e-7).  Plus the FP64 SpMV on the
+    FP64 to 1e-8 relative; FP32 to 1e-6 (FP32 stagnates near 1e-7).  The coarse CG is capped at
+    MG_COARSE_ITERS iterations, MGUtil::configure's max_iters_coarse in the reference's own MG
+    test (honei/math/mg_TEST.cc:421); the 9^2 coarse system (identity Dirichlet rows, not
+    symmetric) stagnates well before that, and a run at a cap of 1000 (f64_banded_coarse1000)
+    takes the same cycles to the same residual.  Plus the FP64 SpMV on the
     permuted matrix (seeded symmetric row/column permutation) and, when the compiled reference
     is present, its MultiCore::SSE MG solve of the same FP64 system on the host cores."""
     import torch
@@ -342,15 +349,18 @@ def bench_mg(la, ctx, M=2049, seed=5, cpu=True):
 
     H = P.mg_hierarchy(M)
     xt = P.uniform_vector(M * M, seed)
-    out = {"workload": f"MG V(2,2) on Q1 {M}^2, {len(H.sides)} levels, coarse CG on 9^2; *_banded: banded "
-                       "levels and matrix-free transfers, the same cycle"}
+    out = {"workload": f"MG V(2,2) on Q1 {M}^2, {len(H.sides)} levels, coarse CG on 9^2 (at most "
+                       f"{MG_COARSE_ITERS} iterations); *_banded: banded levels and matrix-free transfers, the same "
+                       "cycle", "max_iters_coarse": MG_COARSE_ITERS}
     bref = None
     xs_ell = {}
-    for name, npdt, tdt, eps, banded in (("f64", np.float64, torch.float64, 1e-8, False),
-                                          ("f32", np.float32, torch.float32, 1e-6, False),
-                                          ("f64_banded", np.float64, torch.float64, 1e-8, True),
-                                          ("f32_banded", np.float32, torch.float32, 1e-6, True)):
-        data = la.MGData.from_hierarchy(H, npdt, ctx=ctx, eps=eps, max_iters=100, banded=banded)
+    for name, npdt, tdt, eps, banded, mic in (("f64", np.float64, torch.float64, 1e-8, False, MG_COARSE_ITERS),
+                                               ("f32", np.float32, torch.float32, 1e-6, False, MG_COARSE_ITERS),
+                                               ("f64_banded", np.float64, torch.float64, 1e-8, True, MG_COARSE_ITERS),
+                                               ("f32_banded", np.float32, torch.float32, 1e-6, True, MG_COARSE_ITERS),
+                                               ("f64_banded_coarse1000", np.float64, torch.float64, 1e-8, True, 1000)):
+        data = la.MGData.from_hierarchy(H, npdt, ctx=ctx, eps=eps, max_iters=100, max_iters_coarse=mic,
+                                        banded=banded)
         A = data.A[-1]
         xtd = torch.from_numpy(xt.astype(npdt)).cuda()
         b = torch.empty_like(xtd)
@@ -370,7 +380,7 @@ def bench_mg(la, ctx, M=2049, seed=5, cpu=True):
         err = float(torch.linalg.norm((x - xtd).double()) / torch.linalg.norm(xtd.double()))
         out[name] = {"ms": round(ms, 2), "cycles": cycles, "ms_per_cycle": round(ms / max(cycles, 1), 3),
                      "relres": r1 / r0 if r0 else 0.0, "eps": eps, "err_vs_x_true": err}
-        if banded:
+        if banded and mic == MG_COARSE_ITERS:
             # the banded cycle rounds as the ELL cycle: same iterate
             out[name]["same_x_as_ell"] = bool(torch.equal(x, xs_ell[name.split("_")[0]]))
         else:
@@ -381,7 +391,7 @@ def bench_mg(la, ctx, M=2049, seed=5, cpu=True):
     if cpu:
         R = _ref_cpu()
         if R is not None:
-            _, used, sec = R.mg(H, bref, eps=1e-8, tag="mc-sse")
+            _, used, sec = R.mg(H, bref, eps=1e-8, max_iters_coarse=MG_COARSE_ITERS, tag="mc-sse")
             out["cpu_reference_f64"] = {"s": round(sec, 3), "cycles": used, "cores": os.cpu_count(),
                                         "tag": "tags::CPU::MultiCore::SSE"}
             out["speedup_f64_vs_cpu"] = round(sec * 1e3 / out["f64"]["ms"], 1)

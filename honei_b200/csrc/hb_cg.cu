@@ -3,12 +3,18 @@
 //
 // The reference runs 7 launches, 2 device->host scalar round trips and 2 cudaMalloc/cudaFree
 // pairs per iteration (honei/la/*-cuda.cc).  Here the loop, its scalars and its stopping test
-// live on the device; per iteration there are two phases separated by grid barriers:
+// live on the device; per iteration there are two phases, each ending in a grid-wide reduction
+// on an arrival counter (hbd::CountExchange):
 //
 //   phase 1  p_i = r_i + beta * p_i  (computed on the fly for every gathered column, so the
 //            separate Scale+Sum passes disappear), v = A p, partial v.p
 //   phase 2  lambda = alpha / v.p;  x += lambda p;  r += (-lambda) v;  partial r.r
 //
+// The gathers of x, r and p are ordinary, L1-cacheable loads: every value they read was written
+// by another block before its release-arrival at an exchange that this block acquired (thread 0)
+// and then passed through __syncthreads, so the memory model guarantees the current value; the
+// rows of a warp then share L1 lines, where an L2-only load fetches a 32-byte sector per 8-byte
+// element (about a third less time per iteration at 1025^2).
 // p is double-buffered (phase 1 gathers the old p of neighbour rows while writing the new p
 // of its own rows).  Every elementwise formula rounds exactly as cg.hh's operator sequence
 // (ScaledSum, Scale, Sum) does on tags::CPU; the two dot products use a fixed-order tree
@@ -68,7 +74,8 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
     const int64_t gpb = (groups + G - 1) / G;
     const int64_t g_lo = (int64_t)blockIdx.x * gpb;
     const int64_t g_hi = min(groups, g_lo + gpb);
-    T *slotA = P.partials, *slotB = P.partials + G;
+    const hbd::CountExchange X{P.bar.count, P.bar.status};
+    unsigned e = 0;
     const int64_t rows = P.rows;
     bool ok = true;
 
@@ -79,7 +86,7 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
         for (int i = 0; i < 4; ++i) xv[i] = (4 * g + i < rows) ? P.x_user[4 * g + i] : T(0);
         hbd::st4(P.x + 4 * g, xv);
     }
-    ok = P.bar.sync(G, &s_flag);
+    ok = X.arrive_wait(T(0), P.partials, e, G, &s_flag);
 
     // r = b - A x (Defect), alpha = r.r (Norm<l2, false>)
     T acc = T(0);
@@ -87,7 +94,7 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
         const T *xw = P.x;
         for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
             T s[4], rv[4];
-            hbd::ell_rows4<T, KT>(P.Aj, P.Ax, P.ld, P.K, 4 * g, [&](int32_t j) { return __ldcg(xw + j); }, s);
+            hbd::ell_rows4<T, KT>(P.Aj, P.Ax, P.ld, P.K, 4 * g, [&](int32_t j) { return xw[j]; }, s);
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const T bb = (4 * g + i < rows) ? P.b_user[4 * g + i] : T(0);
@@ -97,10 +104,9 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
             hbd::st4(P.r + 4 * g, rv);
         }
         acc = hbd::block_sum(acc, red);
-        if (threadIdx.x == 0) slotB[blockIdx.x] = acc;
-        ok = P.bar.sync(G, &s_flag);
+        ok = X.arrive_wait(acc, P.partials, ++e, G, &s_flag);
     }
-    T alpha = ok ? grid_total(slotB, red, &bcast) : T(0);
+    T alpha = ok ? grid_total(P.partials + (e & 1u) * G, red, &bcast) : T(0);
     const T initial_defect = dsqrt(alpha);
     T current_defect = T(0);
     T beta = T(0);
@@ -115,8 +121,8 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
         for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
             T s[4];
             hbd::ell_rows4<T, KT>(P.Aj, P.Ax, P.ld, P.K, 4 * g, [&](int32_t j) {
-                const T rj = __ldcg(rw + j);
-                return first ? rj : add(mul(__ldcg(pw + j), beta), rj);
+                const T rj = rw[j];
+                return first ? rj : add(mul(pw[j], beta), rj);
             }, s);
             T rv[4], pv[4], pn[4];
             hbd::ld4(P.r + 4 * g, rv);
@@ -130,9 +136,8 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
             hbd::st4(P.v + 4 * g, s);
         }
         acc = hbd::block_sum(acc, red);
-        if (threadIdx.x == 0) slotA[blockIdx.x] = acc;
-        if (!P.bar.sync(G, &s_flag)) break;
-        const T temp = grid_total(slotA, red, &bcast);
+        if (!X.arrive_wait(acc, P.partials, ++e, G, &s_flag)) break;
+        const T temp = grid_total(P.partials + (e & 1u) * G, red, &bcast);
         const T lambda = alpha / (fabs(temp) > epsm ? temp : epsm);
         const T mlambda = -lambda;
 
@@ -154,10 +159,9 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
             hbd::st4(P.r + 4 * g, rv);
         }
         acc = hbd::block_sum(acc, red);
-        if (threadIdx.x == 0) slotB[blockIdx.x] = acc;
-        if (!P.bar.sync(G, &s_flag)) break;
+        if (!X.arrive_wait(acc, P.partials, ++e, G, &s_flag)) break;
         const T alpha_old = alpha;
-        alpha = grid_total(slotB, red, &bcast);
+        alpha = grid_total(P.partials + (e & 1u) * G, red, &bcast);
         beta = alpha / (fabs(alpha_old) > epsm ? alpha_old : epsm);
         T *t = pin; pin = pout; pout = t;
         ++it;
@@ -686,12 +690,16 @@ int cg_impl(hb_context *ctx, const hb_ell *A, const T *b, T *x, int64_t max_iter
 
 namespace {
 
-// One block waits at a grid barrier sized for two: the second arrival never comes, so the wait
-// runs to its limit (HB_WAIT_NS), records HB_DEV_TIMEOUT and the kernel returns.
-__global__ void wait_timeout_kernel(hbd::GridBarrier bar, hb_solve_result *res)
+// One block waits for a second block that never comes, at a grid barrier (COUNTER false) or at
+// an arrival-counter exchange (COUNTER true): the wait runs to its limit (HB_WAIT_NS), records
+// HB_DEV_TIMEOUT and the kernel returns.
+template <bool COUNTER>
+__global__ void wait_timeout_kernel(hbd::GridBarrier bar, double *slots, hb_solve_result *res)
 {
     __shared__ int s_flag;
-    const bool ok = bar.sync(2, &s_flag);
+    bool ok;
+    if (COUNTER) ok = hbd::CountExchange{bar.count, bar.status}.arrive_wait(1.0, slots, 0u, 2u, &s_flag);
+    else ok = bar.sync(2, &s_flag);
     if (threadIdx.x == 0) {
         res->used = ok ? 1 : 0;
         res->status = *(volatile int *)bar.status;
@@ -710,16 +718,22 @@ int hb_selftest_wait_timeout(hb_context *ctx)
     bar.count = w;
     bar.gen = w + 1;
     bar.status = (int *)(w + 2);
-    HB_CUDA_TRY(ctx, cudaMemsetAsync(w, 0, 4 * sizeof(unsigned), ctx->stream));
-    wait_timeout_kernel<<<1, 32, 0, ctx->stream>>>(bar, hb_result(ctx));
-    int st = hb_check_launch(ctx, "wait_timeout_kernel");
-    if (st) return st;
     hb_solve_result *h = (hb_solve_result *)ctx->pinned;
-    HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, hb_result(ctx), sizeof(hb_solve_result), cudaMemcpyDeviceToHost, ctx->stream));
-    HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    bool as_designed = true;
+    for (int counter = 0; counter < 2; ++counter) {
+        HB_CUDA_TRY(ctx, cudaMemsetAsync(w, 0, 4 * sizeof(unsigned), ctx->stream));
+        if (counter) wait_timeout_kernel<true><<<1, 32, 0, ctx->stream>>>(bar, hb_partials(ctx), hb_result(ctx));
+        else wait_timeout_kernel<false><<<1, 32, 0, ctx->stream>>>(bar, hb_partials(ctx), hb_result(ctx));
+        int st = hb_check_launch(ctx, "wait_timeout_kernel");
+        if (st) return st;
+        HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, hb_result(ctx), sizeof(hb_solve_result), cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+        HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        as_designed = as_designed && h->status == HB_DEV_TIMEOUT && h->used == 0;
+    }
     // leave the barrier words clean for the next cooperative launch
     HB_CUDA_TRY(ctx, cudaMemsetAsync(w, 0, 4 * sizeof(unsigned), ctx->stream));
-    return (h->status == HB_DEV_TIMEOUT && h->used == 0) ? HB_ERR_TIMEOUT : HB_ERR_CUDA;
+    return as_designed ? HB_ERR_TIMEOUT : HB_ERR_CUDA;
 }
 
 int hb_cg_f64(hb_context *ctx, const hb_ell *A, const double *b, double *x, int64_t max_iters,

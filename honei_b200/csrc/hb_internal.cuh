@@ -283,6 +283,8 @@ struct GridBarrier {
 // until the counter reaches (e + 1) * blocks; every block may then read all partials of e, and
 // everything the other blocks wrote before arriving.  Two slot arrays suffice: a block reaches
 // exchange e + 2 only after every block arrived at e + 1, i.e. after every block read e.
+// The barrier form (arrive) publishes whatever thread 0 of each block stored before it; a slot
+// written at exchange e may be rewritten at e + 2 at the earliest, by the same argument.
 // Waits are bounded like GridBarrier's (HB_WAIT_NS, HB_DEV_TIMEOUT in the status word; a block
 // that sees another block's failure leaves too).
 struct CountExchange {
@@ -292,10 +294,15 @@ struct CountExchange {
     template <typename T>
     __device__ __forceinline__ bool arrive_wait(T partial, T *slots, unsigned e, unsigned nblocks, int *s_flag) const
     {
+        if (threadIdx.x == 0) __stcg(slots + (e & 1u) * nblocks + blockIdx.x, partial);
+        return arrive(e, nblocks, s_flag);
+    }
+
+    __device__ __forceinline__ bool arrive(unsigned e, unsigned nblocks, int *s_flag) const
+    {
         __syncthreads();
         if (threadIdx.x == 0) {
             int ok = 1;
-            __stcg(slots + (e & 1u) * nblocks + blockIdx.x, partial);
             red_release_add(count, 1u);
             const unsigned target = (e + 1u) * nblocks;
             if ((int)(ld_acquire(count) - target) < 0) {

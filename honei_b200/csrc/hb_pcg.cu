@@ -13,7 +13,7 @@
 //            P, read for a matrix P), v = A p, partial v.p
 //   phase 2  x += lambda p; r += (-lambda) v; partial r.r (vector P: also z = P r and r.z)
 //   phase 3  (matrix P only) z = P r, partial r.z
-// separated by bounded grid barriers; every block sums the partials in one fixed order, so all
+// separated by bounded grid-wide exchanges on an arrival counter; every block sums the partials in one fixed order, so all
 // blocks hold the same scalars and take the same branches.  Elementwise formulas round as the
 // reference's operator sequence (ScaledSum, Scale, Sum, ElementProduct); the dot products use
 // the fixed-order tree of the plain CG kernel.
@@ -82,6 +82,10 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
     const int64_t g_lo = (int64_t)blockIdx.x * gpb;
     const int64_t g_hi = min(groups, g_lo + gpb);
     T *slotA = P.partials, *slotB = P.partials + G, *slotC = P.partials + 2 * G;
+    // grid-wide reductions on the arrival counter; no slot is written at two consecutive
+    // exchanges (A; B, C; A; B (C); [C;] A ...), so fixed slot arrays suffice
+    const hbd::CountExchange X{P.bar.count, P.bar.status};
+    unsigned e = 0;
     const int64_t rows = P.rows;
     bool ok = true;
 
@@ -89,7 +93,7 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
     auto precon4 = [&](int64_t g, const T (&rv)[4], T (&zv)[4]) {
         if (PMAT) {
             const T *rw = P.r;
-            hbd::ell_rows4<T, 0>(P.Pj, P.Px, P.Pld, P.PK, 4 * g, [&](int32_t j) { return __ldcg(rw + j); }, zv);
+            hbd::ell_rows4<T, 0>(P.Pj, P.Px, P.Pld, P.PK, 4 * g, [&](int32_t j) { return rw[j]; }, zv);
         } else {
             T pd[4];
             hbd::ld4(P.Pd + 4 * g, pd);
@@ -104,7 +108,7 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
         for (int i = 0; i < 4; ++i) xv[i] = (4 * g + i < rows) ? P.x_user[4 * g + i] : T(0);
         hbd::st4(P.x + 4 * g, xv);
     }
-    ok = P.bar.sync(G, &s_flag);
+    ok = X.arrive(e++, G, &s_flag);
 
     // r = b - A x (Defect)
     T rr = T(0), rp = T(0);
@@ -112,7 +116,7 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
         const T *xw = P.x;
         for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
             T s[4], rv[4];
-            hbd::ell_rows4<T, KT, 4>(P.Aj, P.Ax, P.ld, P.K, 4 * g, [&](int32_t j) { return __ldcg(xw + j); }, s);
+            hbd::ell_rows4<T, KT, 4>(P.Aj, P.Ax, P.ld, P.K, 4 * g, [&](int32_t j) { return xw[j]; }, s);
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const T bb = (4 * g + i < rows) ? P.b_user[4 * g + i] : T(0);
@@ -131,7 +135,7 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
                 }
             }
         }
-        ok = P.bar.sync(G, &s_flag);
+        ok = X.arrive(e++, G, &s_flag);
     }
     if (PMAT && ok) {
         // p = P r needs every row of r
@@ -151,7 +155,7 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
     if (threadIdx.x == 0) slotB[blockIdx.x] = rr;
     rp = hbd::block_sum(rp, red);
     if (threadIdx.x == 0) slotC[blockIdx.x] = rp;
-    if (ok) ok = P.bar.sync(G, &s_flag);
+    if (ok) ok = X.arrive(e++, G, &s_flag);
     const T initial_defect = ok ? dsqrt(grid_total(slotB, red, &bcast)) : T(0);
     T alpha_new = ok ? grid_total(slotC, red, &bcast) : T(0);
     T current_defect = T(0);
@@ -166,9 +170,9 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
         for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
             T s[4];
             hbd::ell_rows4<T, KT, 4>(P.Aj, P.Ax, P.ld, P.K, 4 * g, [&](int32_t j) {
-                const T pj = __ldcg(pw + j);
+                const T pj = pw[j];
                 if (first) return pj;
-                const T zj = PMAT ? __ldcg(zw + j) : mul(__ldcg(dw + j), __ldcg(rw + j));
+                const T zj = PMAT ? zw[j] : mul(dw[j], rw[j]);
                 return add(mul(pj, talpha), zj);
             }, s);
             T pv[4], pn[4];
@@ -195,7 +199,7 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
         }
         acc = hbd::block_sum(acc, red);
         if (threadIdx.x == 0) slotA[blockIdx.x] = acc;
-        if (!P.bar.sync(G, &s_flag)) break;
+        if (!X.arrive(e++, G, &s_flag)) break;
         const T temp = grid_total(slotA, red, &bcast);
         const T lambda = alpha_new / guard(temp);
         const T mlambda = -lambda;
@@ -230,7 +234,7 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
             rz = hbd::block_sum(rz, red);
             if (threadIdx.x == 0) slotC[blockIdx.x] = rz;
         }
-        if (!P.bar.sync(G, &s_flag)) break;
+        if (!X.arrive(e++, G, &s_flag)) break;
         ++it;
         current_defect = dsqrt(grid_total(slotB, red, &bcast));
         if (current_defect < P.eps * initial_defect) { used = it; break; }
@@ -250,7 +254,7 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
             }
             rz = hbd::block_sum(rz, red);
             if (threadIdx.x == 0) slotC[blockIdx.x] = rz;
-            if (!P.bar.sync(G, &s_flag)) break;
+            if (!X.arrive(e++, G, &s_flag)) break;
         }
         const T alpha = alpha_new;
         alpha_new = grid_total(slotC, red, &bcast);

@@ -262,10 +262,11 @@ int hb_cg_var_ell_f64(hb_context *ctx, const hb_ell *A, const hb_ell *P, const d
 int hb_cg_var_ell_f32(hb_context *ctx, const hb_ell *A, const hb_ell *P, const float *b, float *x,
                       int64_t max_iters, float eps, int64_t *used_iters, float *final_defect);
 
-/* Self-test of the bounded device waits (no reference counterpart): one block waits at a grid
- * barrier for an arrival that never comes; the wait gives up after its limit (2 s), records the
- * timeout in the context's status word and the kernel returns.  Returns HB_ERR_TIMEOUT when that
- * happened as designed; the context stays usable. */
+/* Self-test of the bounded device waits (no reference counterpart): one block waits for an
+ * arrival that never comes, first at a grid barrier, then at an arrival-counter exchange (the
+ * CG kernels' reductions); each wait gives up after its limit (2 s), records the timeout in the
+ * context's status word and the kernel returns.  Returns HB_ERR_TIMEOUT when both happened as
+ * designed; the context stays usable. */
 int hb_selftest_wait_timeout(hb_context *ctx);
 
 /* Allocation-free variant of hb_cg_f64.  This entry point has no counterpart in the reference.

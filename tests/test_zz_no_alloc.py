@@ -45,6 +45,9 @@ def test_noalloc_cg_matches_context_cg_twice_in_a_row():
     ctx = C.c_void_p()
     assert L.hb_create(C.byref(ctx), torch.cuda.current_device()) == 0
     assert L.hb_set_stream(ctx, C.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
+    # the allocation-free entry point always runs the streaming kernel; the context's CG runs
+    # the resident-operator kernel by default on systems that fit, so compare kernel to kernel
+    assert L.hb_cg_set_resident(ctx, 0) == 1
     try:
         # two different systems back to back, so the second call starts from the first
         # call's leftovers in the static array
@@ -69,6 +72,13 @@ def test_noalloc_cg_matches_context_cg_twice_in_a_row():
                 assert torch.equal(x, x_ref)
                 rel = (x - xt).norm().item() / xt.norm().item()
                 assert rel < 1e-4
+            # the resident kernel on the same system: the CG tolerance
+            L.hb_cg_set_resident(ctx, 1)
+            x_res = torch.zeros_like(xt)
+            st, u_res, d_res = _solve_ctx(L, ctx, A, b, x_res, 20000, 1e-8)
+            L.hb_cg_set_resident(ctx, 0)
+            assert st == 0 and abs(u_res - u_ref) <= 1
+            assert (x_res - x_ref).norm().item() <= 1e-6 * x_ref.norm().item()
     finally:
         L.hb_destroy(ctx)
 
