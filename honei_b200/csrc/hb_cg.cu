@@ -364,12 +364,49 @@ template <typename T> struct ResParams {
     hbd::CountExchange X;
 };
 
+constexpr int RES_MAX_BLOCKS = 256;
+
+// The block's partial, in thread 0: warp trees, then warp 0 sums the warp results.  One
+// __syncthreads; the red[] slots are free again because every caller passes another block-wide
+// barrier (the exchange) before the next call.
 template <typename T>
-__device__ __forceinline__ T res_total(const T *slots, unsigned e, unsigned G, T *red, T *bcast)
+__device__ __forceinline__ T res_partial(T v, T *red)
 {
-    T v = threadIdx.x < G ? __ldcg(slots + (e & 1u) * G + threadIdx.x) : T(0);
-    v = hbd::block_sum(v, red);
-    if (threadIdx.x == 0) *bcast = v;
+    v = hbd::warp_sum(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) v = hbd::warp_sum((int)threadIdx.x < (int)(blockDim.x >> 5) ? red[threadIdx.x] : T(0));
+    return v;
+}
+
+// The grid total of exchange e: warp 0 loads the partials (lane l: l, l + 32, ... summed in
+// order, then a warp tree) -- the same value in every block -- and broadcasts it through shared
+// memory; the other warps' loads (the halo) go out between res_total_load and res_total_sum.
+// Reading the partials in one warp per block keeps the L2 lines that hold them from being
+// hammered by every warp of the grid at once.
+template <typename T>
+__device__ __forceinline__ void res_total_load(const T *slots, unsigned e, unsigned G, T (&pv)[RES_MAX_BLOCKS / 32])
+{
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int i = 0; i < RES_MAX_BLOCKS / 32; ++i)
+            pv[i] = (lane + 32 * i < (int)G) ? __ldcg(slots + (e & 1u) * G + lane + 32 * i) : T(0);
+    }
+}
+// Ends in a __syncthreads (which also orders the halo's shared-memory writes before phase 1).
+template <typename T>
+__device__ __forceinline__ T res_total_sum(unsigned G, const T (&pv)[RES_MAX_BLOCKS / 32], T *bcast)
+{
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x < 32) {
+        T v = T(0);
+#pragma unroll
+        for (int i = 0; i < RES_MAX_BLOCKS / 32; ++i)
+            if (lane + 32 * i < (int)G) v = hbd::add(v, pv[i]);
+        v = hbd::warp_sum(v);
+        if (lane == 0) *bcast = v;
+    }
     __syncthreads();
     return *bcast;
 }
@@ -380,7 +417,7 @@ __global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<
     using hbd::add; using hbd::mul; using hbd::sub;
     extern __shared__ __align__(16) unsigned char res_smem[];
     __shared__ T red[32];
-    __shared__ T bcast;
+    __shared__ T bcast[2];
     __shared__ int s_flag, s_min, s_max;
     const CGParams<T> &P = Q.c;
     const int K = KT > 0 ? KT : P.K;
@@ -447,9 +484,10 @@ __global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<
         __stcg(P.r + lo + il, r);
         acc = add(acc, mul(r, r));
     }
-    acc = hbd::block_sum(acc, red);
+    acc = res_partial(acc, red);
     unsigned e = 0;
-    bool ok = Q.X.arrive_wait(acc, P.partials, e, G, &s_flag);
+    if (threadIdx.x == 0) __stcg(P.partials + (e & 1u) * G + blockIdx.x, acc);
+    bool ok = Q.X.arrive_synced(e, G, &s_flag);
     // the window's other rows of r (halo), loaded beside the partials
     const int64_t n_left = nr > 0 ? own : 0, n_halo = nr > 0 ? own + (wlo + W - hi) : 0;
     auto halo = [&]() {
@@ -463,10 +501,12 @@ __global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<
             if (q2 < n_halo) r_w[w2] = b;
         }
     };
+    T pv[RES_MAX_BLOCKS / 32];
     T alpha = T(0);
     if (ok) {
+        res_total_load(P.partials, e, G, pv);
         halo();
-        alpha = res_total(P.partials, e, G, red, &bcast);
+        alpha = res_total_sum(G, pv, &bcast[0]);
     }
     const T initial_defect = dsqrt(alpha);
     T current_defect = T(0);
@@ -501,9 +541,12 @@ __global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<
             __stcg(pout + lo + il, pi);
             acc = add(acc, mul(s, pi));
         }
-        acc = hbd::block_sum(acc, red);
-        if (!Q.X.arrive_wait(acc, P.partials, ++e, G, &s_flag)) break;
-        const T temp = res_total(P.partials, e, G, red, &bcast);
+        acc = res_partial(acc, red);
+        ++e;
+        if (threadIdx.x == 0) __stcg(P.partials + (e & 1u) * G + blockIdx.x, acc);
+        if (!Q.X.arrive_synced(e, G, &s_flag)) break;
+        res_total_load(P.partials, e, G, pv);
+        const T temp = res_total_sum(G, pv, &bcast[1]);
         const T lambda = alpha / (fabs(temp) > epsm ? temp : epsm);
         const T mlambda = -lambda;
 
@@ -516,11 +559,14 @@ __global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<
             __stcg(P.r + lo + il, r);
             acc = add(acc, mul(r, r));
         }
-        acc = hbd::block_sum(acc, red);
-        if (!Q.X.arrive_wait(acc, P.partials, ++e, G, &s_flag)) break;
+        acc = res_partial(acc, red);
+        ++e;
+        if (threadIdx.x == 0) __stcg(P.partials + (e & 1u) * G + blockIdx.x, acc);
+        if (!Q.X.arrive_synced(e, G, &s_flag)) break;
+        res_total_load(P.partials, e, G, pv);
         halo();
         const T alpha_old = alpha;
-        alpha = res_total(P.partials, e, G, red, &bcast);
+        alpha = res_total_sum(G, pv, &bcast[0]);
         beta = alpha / (fabs(alpha_old) > epsm ? alpha_old : epsm);
         T *t = pin; pin = pout; pout = t;
         ++it;
@@ -557,7 +603,7 @@ bool res_plan(hb_context *ctx, int64_t rows, int K, int *blocks, int64_t *rpb, i
         return false;
     }
     const size_t avail = (size_t)optin - 1024;    // static shared memory of the kernel
-    const int64_t G = std::max<int64_t>(1, std::min<int64_t>(ctx->num_sms, (rows + 127) / 128));
+    const int64_t G = std::max<int64_t>(1, std::min<int64_t>(std::min(ctx->num_sms, RES_MAX_BLOCKS), (rows + 127) / 128));
     const int64_t r = (rows + G - 1) / G;
     const size_t fixed = res_smem_bytes<T>(K, r, 0);
     if (fixed + 2 * (size_t)r * sizeof(T) > avail) return false;

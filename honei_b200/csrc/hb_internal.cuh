@@ -301,6 +301,13 @@ struct CountExchange {
     __device__ __forceinline__ bool arrive(unsigned e, unsigned nblocks, int *s_flag) const
     {
         __syncthreads();
+        return arrive_synced(e, nblocks, s_flag);
+    }
+
+    // arrive() for callers whose threads passed a __syncthreads after their last global store
+    // (a block reduction ending in one): thread 0's release then covers those stores already
+    __device__ __forceinline__ bool arrive_synced(unsigned e, unsigned nblocks, int *s_flag) const
+    {
         if (threadIdx.x == 0) {
             int ok = 1;
             red_release_add(count, 1u);
