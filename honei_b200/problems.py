@@ -100,6 +100,103 @@ def ell_from_csr(rows: int, cols: int, indptr, indices, data, threads: int = 1,
     return EllMatrix(rows, cols, stride, ncpr, T, Aj, Ax, Arl, int(len(indices)))
 
 
+@dataclasses.dataclass
+class CsrMatrix:
+    """A sparse matrix in the reference's SparseMatrixCSR layout (host arrays,
+    honei/la/sparse_matrix_csr.hh): ``Ar[rows + 1]`` block offsets, ``Aj[nblocks]`` the first
+    column of each block, ``Ax[nblocks * blocksize]`` (csr::blocksize values per block; lanes
+    without an entry hold zero)."""
+
+    rows: int
+    cols: int
+    blocksize: int
+    Ar: np.ndarray   # uint64[rows + 1]
+    Aj: np.ndarray   # uint64[nblocks]
+    Ax: np.ndarray   # float64 or float32 [nblocks * blocksize]
+    used: int = 0    # stored entries (used_elements)
+
+    @property
+    def dtype(self):
+        return self.Ax.dtype
+
+    @property
+    def nblocks(self) -> int:
+        return int(self.Ar[-1]) if len(self.Ar) else 0
+
+    def astype(self, dtype) -> "CsrMatrix":
+        return dataclasses.replace(self, Ax=self.Ax.astype(dtype))
+
+    def to_dense(self) -> np.ndarray:
+        """Dense copy (small matrices, for tests): lanes at or beyond cols are dropped."""
+        D = np.zeros((self.rows, self.cols), self.Ax.dtype)
+        bs = self.blocksize
+        for r in range(self.rows):
+            for i in range(int(self.Ar[r]), int(self.Ar[r + 1])):
+                for k in range(bs):
+                    c = int(self.Aj[i]) + k
+                    if c < self.cols:
+                        D[r, c] += self.Ax[i * bs + k]
+        return D
+
+
+def csr_blocked(rows: int, cols: int, indptr, indices, data, blocksize: int = 1, dtype=np.float64) -> CsrMatrix:
+    """The reference's SparseMatrixCSR(SparseMatrix) conversion with csr::blocksize = blocksize
+    (honei/la/sparse_matrix_csr-impl.hh:98-136): per row, walking the stored entries in column
+    order, a block starts at the entry's column rounded down to a multiple of blocksize and
+    takes the following entries that fall on its lanes; lanes without an entry hold zero.
+    ``indices`` ascending per row; every stored entry is kept, zero values included."""
+    bs = int(blocksize)
+    if bs < 1:
+        raise ValueError("blocksize must be >= 1")
+    indptr = np.asarray(indptr, np.int64)
+    indices = np.asarray(indices, np.int64)
+    data = np.asarray(data)
+    Ar = np.zeros(rows + 1, np.uint64)
+    Aj, Ax = [], []
+    for r in range(rows):
+        Ar[r] = len(Aj)
+        lo, hi = int(indptr[r]), int(indptr[r + 1])
+        i = lo
+        while i < hi:
+            start = int(indices[i]) - int(indices[i]) % bs
+            lanes = np.zeros(bs, dtype)
+            d = 0
+            for k in range(bs):
+                if i + d < hi and start + k == int(indices[i + d]):
+                    lanes[k] = data[i + d]
+                    d += 1
+            Aj.append(start)
+            Ax.append(lanes)
+            i += d
+    Ar[rows] = len(Aj)
+    Axa = np.concatenate(Ax).astype(dtype) if Ax else np.zeros(0, dtype)
+    return CsrMatrix(rows, cols, bs, Ar, np.asarray(Aj, np.uint64), Axa, int(indptr[-1]) if rows else 0)
+
+
+def csr_from_ell(A: "EllMatrix", blocksize: int = 1) -> CsrMatrix:
+    """SparseMatrixCSR(SparseMatrixELL) (sparse_matrix_csr-impl.hh:84-96): through the
+    matrix's stored entries, ascending columns per row."""
+    ip, ix, dv = A.to_csr()
+    order = np.lexsort((ix, np.repeat(np.arange(A.rows), np.diff(ip))))
+    return csr_blocked(A.rows, A.cols, ip, ix[order], dv[order], blocksize, A.Ax.dtype)
+
+
+def csr_product_test_matrix(size: int, dtype=np.float64):
+    """The matrix of the reference's CSR product test (honei/la/product_TEST.cc:936-941): size x
+    (size + 3), element with flat index i = r * (size + 3) + c set to i / 1.234 when i % 5 == 0
+    (the element at index 0 stores 0), and its x: 4 everywhere, x[0] = 1, x[1] = 2.  Returns
+    (indptr, indices, data, x)."""
+    cols = size + 3
+    flat = np.arange(0, size * cols, 5, dtype=np.int64)
+    r, c = flat // cols, flat % cols
+    data = (flat.astype(np.float64) / 1.234).astype(dtype)
+    indptr = np.zeros(size + 1, np.int64)
+    np.cumsum(np.bincount(r, minlength=size), out=indptr[1:])
+    x = np.full(cols, 4, dtype)
+    x[0], x[1] = 1, 2
+    return indptr, c, data, x
+
+
 def q1_poisson_csr(M: int, coef=None, symmetric: bool = False):
     """CSR of the Q1 Poisson matrix on an M x M node grid, Dirichlet rows = identity.
 

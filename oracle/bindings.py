@@ -45,6 +45,16 @@ class _OraMG(_c.Structure):
                 ("n_pre", _u64), ("n_post", _u64)]
 
 
+class _OraCsr(_c.Structure):
+    _fields_ = [("rows", _u64), ("cols", _u64), ("blocksize", _u64), ("Ar", _vp), ("Aj", _vp), ("Ax", _vp)]
+
+
+def _csr(A):
+    e = _OraCsr(A.rows, A.cols, A.blocksize, A.Ar.ctypes.data, A.Aj.ctypes.data, A.Ax.ctypes.data)
+    e._keep = A
+    return e
+
+
 def _ell(A):
     e = _OraEll(A.rows, A.cols, A.stride, A.ncpr, A.threads, A.Aj.ctypes.data, A.Ax.ctypes.data,
                 A.Arl.ctypes.data)
@@ -90,6 +100,24 @@ class Oracle:
         e = _ell(A)
         getattr(self.lib, f"ora_spmv_{s}")(_c.byref(e), _ptr(x), _ptr(y))
         return y
+
+    def csr_spmv(self, A, x):
+        """Product<tags::CPU>(DV, SparseMatrixCSR, DV) restated; A a problems.CsrMatrix."""
+        s = self._suffix(A.dtype)
+        x = np.ascontiguousarray(x, A.dtype)
+        y = np.zeros(A.rows, A.dtype)
+        e = _csr(A)
+        getattr(self.lib, f"ora_csr_spmv_{s}")(_c.byref(e), _ptr(x), _ptr(y))
+        return y
+
+    def csr_defect(self, A, b, x):
+        s = self._suffix(A.dtype)
+        b = np.ascontiguousarray(b, A.dtype)
+        x = np.ascontiguousarray(x, A.dtype)
+        r = np.zeros(A.rows, A.dtype)
+        e = _csr(A)
+        getattr(self.lib, f"ora_csr_defect_{s}")(_c.byref(e), _ptr(b), _ptr(x), _ptr(r))
+        return r
 
     def defect(self, A, b, x):
         s = self._suffix(A.dtype)
@@ -437,6 +465,71 @@ class Reference:
         self._check(getattr(self.lib, f"ref_spmv_{s}")(TAGS[tag], *self._args(A), _ptr(x), _ptr(y),
                                                         reps, _c.byref(sec)))
         return y, sec.value
+
+    def csr_product_test(self, size, blocksize):
+        """The reference's CSR product test case (product_TEST.cc:936-948) converted with
+        csr::blocksize: (CsrMatrix, x, y = Product<tags::CPU>(A, x))."""
+        from honei_b200.problems import CsrMatrix
+        f = self.lib.ref_csr_product_test_f64
+        f.argtypes = [_c.c_ulong, _c.c_ulong, _vp, _vp, _vp, _vp, _vp, _vp]
+        info = (_c.c_ulong * 5)()
+        self._check(f(size, blocksize, info, None, None, None, None, None))
+        rows, cols, bs, nb, used = list(info)
+        Ar = np.zeros(rows + 1, np.uint64)
+        Aj = np.zeros(max(nb, 1), np.uint64)
+        Ax = np.zeros(max(nb * bs, 1))
+        x = np.zeros(cols)
+        y = np.zeros(rows)
+        self._check(f(size, blocksize, info, _ptr(Ar), _ptr(Aj), _ptr(Ax), _ptr(x), _ptr(y)))
+        return CsrMatrix(rows, cols, bs, Ar, Aj[:nb], Ax[:nb * bs], used), x, y
+
+    def csr_from_ell(self, A, blocksize):
+        """SparseMatrixCSR(SparseMatrixELL) with csr::blocksize (FP64)."""
+        from honei_b200.problems import CsrMatrix
+        f = self.lib.ref_csr_from_ell_f64
+        f.argtypes = [_c.c_ulong] * 5 + [_vp, _vp, _c.c_ulong, _vp, _vp, _vp, _vp]
+        info = (_c.c_ulong * 5)()
+        args = self._args(A)
+        self._check(f(*args, blocksize, info, None, None, None))
+        rows, cols, bs, nb, used = list(info)
+        Ar = np.zeros(rows + 1, np.uint64)
+        Aj = np.zeros(max(nb, 1), np.uint64)
+        Ax = np.zeros(max(nb * bs, 1))
+        self._check(f(*args, blocksize, info, _ptr(Ar), _ptr(Aj), _ptr(Ax)))
+        return CsrMatrix(rows, cols, bs, Ar, Aj[:nb], Ax[:nb * bs], used)
+
+    def _csr_args(self, A, s):
+        Aj = np.ascontiguousarray(A.Aj if len(A.Aj) else np.zeros(1, np.uint64), np.uint64)
+        Ax = np.ascontiguousarray(A.Ax if len(A.Ax) else np.zeros(1, A.dtype), A.dtype)
+        self._keep_csr = (Aj, Ax)
+        return [A.rows, A.cols, A.blocksize, A.used, _ptr(np.ascontiguousarray(A.Ar, np.uint64)), _ptr(Aj), _ptr(Ax)]
+
+    def csr_spmv(self, A, x, tag="cpu", reps=0):
+        """Product<tag>(DV, SparseMatrixCSR, DV): (y, median seconds of reps timed calls)."""
+        s = "f64" if A.dtype == np.float64 else "f32"
+        f = getattr(self.lib, f"ref_csr_spmv_{s}")
+        f.argtypes = [_c.c_int] + [_c.c_ulong] * 4 + [_vp] * 5 + [_c.c_int, _c.POINTER(_c.c_double)]
+        x = np.ascontiguousarray(x, A.dtype)
+        y = np.zeros(A.rows, A.dtype)
+        Ar = np.ascontiguousarray(A.Ar, np.uint64)
+        args = self._csr_args(A, s)
+        args[4] = _ptr(Ar)
+        sec = _c.c_double(0)
+        self._check(f(TAGS[tag], *args, _ptr(x), _ptr(y), reps, _c.byref(sec)))
+        return y, sec.value
+
+    def csr_defect(self, A, b, x, tag="cpu"):
+        s = "f64" if A.dtype == np.float64 else "f32"
+        f = getattr(self.lib, f"ref_csr_defect_{s}")
+        f.argtypes = [_c.c_int] + [_c.c_ulong] * 4 + [_vp] * 6
+        b = np.ascontiguousarray(b, A.dtype)
+        x = np.ascontiguousarray(x, A.dtype)
+        r = np.zeros(A.rows, A.dtype)
+        Ar = np.ascontiguousarray(A.Ar, np.uint64)
+        args = self._csr_args(A, s)
+        args[4] = _ptr(Ar)
+        self._check(f(TAGS[tag], *args, _ptr(b), _ptr(x), _ptr(r)))
+        return r
 
     def defect(self, A, b, x, tag="cpu"):
         s = "f64" if A.dtype == np.float64 else "f32"

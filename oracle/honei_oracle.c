@@ -46,6 +46,30 @@ void ora_defect_##SUF(const ora_ell *A, const DT *b, const DT *x, DT *r)        
 ORA_SPMV(f64, double)
 ORA_SPMV(f32, float)
 
+/* Product<tags::CPU>::value(DV, SparseMatrixCSR, DV) -- honei/la/product.hh:209-242, and the
+ * CSR Defect -- honei/math/defect.hh:386-419 (the same sum, then rhs - sum in one step). */
+#define ORA_CSR(SUF, DT)                                                                    \
+static DT ora_csr_row_##SUF(const ora_csr *A, const DT *x, uint64_t row)                    \
+{                                                                                           \
+    const DT *Ax = (const DT *)A->Ax;                                                       \
+    const uint64_t bs = A->blocksize;                                                       \
+    DT sum = 0;                                                                             \
+    for (uint64_t i = A->Ar[row]; i < A->Ar[row + 1]; ++i)                                  \
+        for (uint64_t k = 0; k < bs; ++k)                                                   \
+            if (A->Aj[i] + k < A->cols) sum += Ax[i * bs + k] * x[A->Aj[i] + k];            \
+    return sum;                                                                             \
+}                                                                                           \
+void ora_csr_spmv_##SUF(const ora_csr *A, const DT *x, DT *y)                               \
+{                                                                                           \
+    for (uint64_t row = 0; row < A->rows; ++row) y[row] = ora_csr_row_##SUF(A, x, row);     \
+}                                                                                           \
+void ora_csr_defect_##SUF(const ora_csr *A, const DT *rhs, const DT *x, DT *r)              \
+{                                                                                           \
+    for (uint64_t row = 0; row < A->rows; ++row) r[row] = rhs[row] - ora_csr_row_##SUF(A, x, row); \
+}
+ORA_CSR(f64, double)
+ORA_CSR(f32, float)
+
 /* DotProduct<tags::CPU> -- honei/la/dot_product.hh:72-88: sequential, left to right.
  * Norm<vnt_l_two, false> == DotProduct(x, x) (honei/la/norm.hh:290-306). */
 #define ORA_DOT(SUF, DT)                                                                    \

@@ -27,11 +27,26 @@ typedef struct {
     const uint64_t *Arl;
 } ora_ell;
 
+/* SparseMatrixCSR<DT> (honei/la/sparse_matrix_csr.hh): Ar[rows + 1] block offsets, Aj[nblocks]
+ * the first column of each block, Ax[nblocks * blocksize] (csr::blocksize values per block). */
+typedef struct {
+    uint64_t rows, cols, blocksize;
+    const uint64_t *Ar, *Aj;
+    const void *Ax;       /* double* or float* */
+} ora_csr;
+
 /* ---- BLAS-1 and SpMV (f64 / f32) ---- */
 void   ora_spmv_f64(const ora_ell *A, const double *x, double *y);
 void   ora_spmv_f32(const ora_ell *A, const float *x, float *y);
 void   ora_defect_f64(const ora_ell *A, const double *b, const double *x, double *r);
 void   ora_defect_f32(const ora_ell *A, const float *b, const float *x, float *r);
+/* Product<tags::CPU>(DV, SparseMatrixCSR, DV) (honei/la/product.hh:209-242): per row, over its
+ * blocks and their lanes in order, sum += Ax * x for lanes whose column is < cols; Defect
+ * (honei/math/defect.hh:386-419): r = rhs - that sum. */
+void   ora_csr_spmv_f64(const ora_csr *A, const double *x, double *y);
+void   ora_csr_spmv_f32(const ora_csr *A, const float *x, float *y);
+void   ora_csr_defect_f64(const ora_csr *A, const double *rhs, const double *x, double *r);
+void   ora_csr_defect_f32(const ora_csr *A, const float *rhs, const float *x, float *r);
 /* BandedMatrixQx<Q1Type> (honei/la/banded_matrix_qx.hh): nine bands of n values in the
  * Q1BandIndex order LL, LD, LU, DL, DD, DU, UL, UD, UU (honei/la/band_type.hh); root =
  * floor(sqrt(n)).  y = A x as Product<tags::CPU> (honei/la/product.hh:371-404); r = b - A x as

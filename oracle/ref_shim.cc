@@ -22,10 +22,14 @@
 //   IRSolver<Outer, Inner, Norm>                            honei/math/ir.hh:30-78
 //   FillMatrix<POISSON, DIRICHLET_0> + SparseMatrix -> ELL  honei/math/fill_matrix.hh:37-77, honei/la/sparse_matrix_ell-impl.hh:75-122
 //   Transposition<Tag>                                      honei/math/transposition.hh:30-50
+//   SparseMatrixCSR(SparseMatrix / SparseMatrixELL)         honei/la/sparse_matrix_csr-impl.hh:73-136
+//   Product<Tag>::value(DV, SparseMatrixCSR, DV)            honei/la/product.hh:209-242 (tags::CPU)
+//   Defect<Tag>::value(DV, DV, SparseMatrixCSR, DV)         honei/math/defect.hh:386-419 (tags::CPU)
 
 #include <honei/la/dense_vector.hh>
 #include <honei/la/sparse_matrix.hh>
 #include <honei/la/sparse_matrix_ell.hh>
+#include <honei/la/sparse_matrix_csr.hh>
 #include <honei/la/banded_matrix_qx.hh>
 #include <honei/la/product.hh>
 #include <honei/la/dot_product.hh>
@@ -340,6 +344,55 @@ namespace
         });
     }
 
+
+    // SparseMatrixCSR from plain arrays (the raw-array constructor, sparse_matrix_csr.hh)
+    template <typename DT_> SparseMatrixCSR<DT_> csr_from(unsigned long rows, unsigned long cols,
+            unsigned long blocksize, unsigned long used, const uint64_t * Ar, const uint64_t * Aj, const DT_ * Ax)
+    {
+        const unsigned long nblocks(Ar[rows]);
+        DenseVector<unsigned long> ar(rows + 1), aj(nblocks ? nblocks : 1);
+        for (unsigned long i(0) ; i <= rows ; ++i) ar[i] = Ar[i];
+        for (unsigned long i(0) ; i < nblocks ; ++i) aj[i] = Aj[i];
+        DenseVector<DT_> ax(dv_from(Ax, nblocks ? nblocks * blocksize : 1));
+        return SparseMatrixCSR<DT_>(blocksize, rows, cols, aj, ax, ar, used);
+    }
+
+    // info = {rows, cols, blocksize, nblocks, used_elements}; arrays copied when non-null
+    template <typename DT_> void csr_to(const SparseMatrixCSR<DT_> & A, unsigned long * info, uint64_t * Ar,
+            uint64_t * Aj, DT_ * Ax)
+    {
+        const unsigned long nb(A.Ar()[A.rows()]);
+        info[0] = A.rows(); info[1] = A.columns(); info[2] = A.blocksize(); info[3] = nb; info[4] = A.used_elements();
+        if (Ar) for (unsigned long i(0) ; i <= A.rows() ; ++i) Ar[i] = A.Ar()[i];
+        if (Aj) for (unsigned long i(0) ; i < nb ; ++i) Aj[i] = A.Aj()[i];
+        if (Ax) for (unsigned long i(0) ; i < nb * A.blocksize() ; ++i) Ax[i] = A.Ax()[i];
+    }
+
+    struct BlocksizeScope
+    {
+        unsigned long old;
+        explicit BlocksizeScope(unsigned long bs) : old(Configuration::instance()->get_value("csr::blocksize", 1))
+        { Configuration::instance()->set_value("csr::blocksize", bs); }
+        ~BlocksizeScope() { Configuration::instance()->set_value("csr::blocksize", old); }
+    };
+
+    template <typename T_, typename DT_> void csr_spmv_reps(SparseMatrixCSR<DT_> & A, DenseVector<DT_> & y,
+            const DenseVector<DT_> & x, int reps, double * seconds)
+    {
+        Product<T_>::value(y, A, x);                      // warm-up
+        std::vector<double> t;
+        for (int r(0) ; r < reps ; ++r)
+        {
+            double t0(now_s());
+            Product<T_>::value(y, A, x);
+            t.push_back(now_s() - t0);
+        }
+        if (seconds)
+        {
+            std::sort(t.begin(), t.end());
+            *seconds = t.empty() ? 0. : t[t.size() / 2];
+        }
+    }
 }
 
 extern "C"
@@ -660,6 +713,94 @@ extern "C"
             if (seconds) *seconds = now_s() - t0;
             *used = u;
             dv_to(xv, x);
+        });
+    }
+
+    // The reference's CSR product test matrix (honei/la/product_TEST.cc:936-948) converted with
+    // csr::blocksize = blocksize: info, arrays (two-phase: call with null arrays for info), x and
+    // y = Product<tags::CPU>(A, x).
+    int ref_csr_product_test_f64(unsigned long size, unsigned long blocksize, unsigned long * info,
+            uint64_t * Ar, uint64_t * Aj, double * Ax, double * x, double * y)
+    {
+        return guarded([&]() {
+            BlocksizeScope scope(blocksize);
+            SparseMatrix<double> sms(size, size + 3);
+            for (SparseMatrix<double>::ElementIterator i(sms.begin_elements()) ; i < sms.end_elements() ; ++i)
+            {
+                if (i.index() % 5 == 0)
+                    *i = double(i.index()) / 1.234;
+            }
+            SparseMatrixCSR<double> A(sms);
+            csr_to(A, info, Ar, Aj, Ax);
+            if (x && y)
+            {
+                DenseVector<double> dv1(size + 3, double(4));
+                dv1[0] = 1;
+                dv1[1] = 2;
+                DenseVector<double> prod(size, double(4711));
+                Product<tags::CPU>::value(prod, A, dv1);
+                dv_to(dv1, x);
+                dv_to(prod, y);
+            }
+        });
+    }
+
+    // SparseMatrixCSR(SparseMatrixELL) with csr::blocksize = blocksize (two-phase like above).
+    int ref_csr_from_ell_f64(unsigned long rows, unsigned long cols, unsigned long stride, unsigned long ncpr,
+            unsigned long threads, const uint64_t * Aj_ell, const double * Ax_ell, unsigned long blocksize,
+            unsigned long * info, uint64_t * Ar, uint64_t * Aj, double * Ax)
+    {
+        return guarded([&]() {
+            BlocksizeScope scope(blocksize);
+            SparseMatrixELL<double> E(ell_from(rows, cols, stride, ncpr, threads, Aj_ell, Ax_ell));
+            SparseMatrixCSR<double> A(E);
+            csr_to(A, info, Ar, Aj, Ax);
+        });
+    }
+
+    int ref_csr_spmv_f64(int tag, unsigned long rows, unsigned long cols, unsigned long blocksize, unsigned long used,
+            const uint64_t * Ar, const uint64_t * Aj, const double * Ax, const double * x, double * y,
+            int reps, double * seconds)
+    {
+        return guarded([&]() {
+            SparseMatrixCSR<double> A(csr_from(rows, cols, blocksize, used, Ar, Aj, Ax));
+            DenseVector<double> xv(dv_from(x, cols)), yv(rows, 0.);
+            REF_DISPATCH(tag, (csr_spmv_reps<T_, double>(A, yv, xv, reps, seconds)));
+            dv_to(yv, y);
+        });
+    }
+
+    int ref_csr_spmv_f32(int tag, unsigned long rows, unsigned long cols, unsigned long blocksize, unsigned long used,
+            const uint64_t * Ar, const uint64_t * Aj, const float * Ax, const float * x, float * y,
+            int reps, double * seconds)
+    {
+        return guarded([&]() {
+            SparseMatrixCSR<float> A(csr_from(rows, cols, blocksize, used, Ar, Aj, Ax));
+            DenseVector<float> xv(dv_from(x, cols)), yv(rows, 0.f);
+            REF_DISPATCH(tag, (csr_spmv_reps<T_, float>(A, yv, xv, reps, seconds)));
+            dv_to(yv, y);
+        });
+    }
+
+    int ref_csr_defect_f64(int tag, unsigned long rows, unsigned long cols, unsigned long blocksize, unsigned long used,
+            const uint64_t * Ar, const uint64_t * Aj, const double * Ax, const double * b, const double * x, double * r)
+    {
+        return guarded([&]() {
+            SparseMatrixCSR<double> A(csr_from(rows, cols, blocksize, used, Ar, Aj, Ax));
+            DenseVector<double> xv(dv_from(x, cols)), bv(dv_from(b, rows)), rv(rows, 0.);
+            REF_DISPATCH(tag, (Defect<T_>::value(rv, bv, A, xv)));
+            dv_to(rv, r);
+        });
+    }
+
+    int ref_csr_defect_f32(int tag, unsigned long rows, unsigned long cols, unsigned long blocksize, unsigned long used,
+            const uint64_t * Ar, const uint64_t * Aj, const float * Ax, const float * b, const float * x, float * r)
+    {
+        return guarded([&]() {
+            SparseMatrixCSR<float> A(csr_from(rows, cols, blocksize, used, Ar, Aj, Ax));
+            DenseVector<float> xv(dv_from(x, cols)), bv(dv_from(b, rows)), rv(rows, 0.f);
+            REF_DISPATCH(tag, (Defect<T_>::value(rv, bv, A, xv)));
+            dv_to(rv, r);
         });
     }
 }

@@ -38,6 +38,13 @@ def load_golden(name):
     return np.load(os.path.join(GOLDEN, name + ".npz"))
 
 
+def golden_csr(d, key, dtype=np.float64):
+    """problems.CsrMatrix stored in a golden npz under key_{Ar,Aj,Ax,info}."""
+    from honei_b200 import problems as P
+    rows, cols, bs, used = (int(v) for v in d[key + "_info"])
+    return P.CsrMatrix(rows, cols, bs, d[key + "_Ar"], d[key + "_Aj"], d[key + "_Ax"].astype(dtype), used)
+
+
 def golden_matrix(d, name, dtype=np.float64):
     """EllMatrix (reference layout, T = 1) from a CSR stored in a golden npz."""
     from honei_b200 import problems as P

@@ -30,7 +30,7 @@ readers, honei/math/matrix_io.hh and honei/math/vector_io.hh):
   poisson_advanced4/sort_0 A_4 (A_4_sainv.ell, A_4_spai.ell; rhs_4, init_4), each with the
   reference's solution and iteration count (A_4, rhs_4, init_4 live in featflow_pa4.npz).
 
-    python tests/golden/make_golden.py [/path/to/honei-tree] [--only q1band|pcg]
+    python tests/golden/make_golden.py [/path/to/honei-tree] [--only q1band|pcg|csr]
 """
 from __future__ import annotations
 
@@ -125,10 +125,55 @@ def pcg(R, tree: str) -> None:
     np.savez_compressed(os.path.join(HERE, "pcg.npz"), **out)
 
 
+def csr(R) -> None:
+    """SparseMatrixCSR: the reference's own CSR product test cases (product_TEST.cc:917-958,
+    csr::blocksize 1, 2, 4, 8), the reference's ELL -> CSR conversion of Q1 33^2 with its
+    product and defect, and a rectangular random pattern with empty rows and a ragged last
+    block, each with tags::CPU results."""
+    out = {}
+    for bs in (1, 2, 4, 8):
+        for size in (11, 44, 176):
+            A, x, y = R.csr_product_test(size, bs)
+            k = f"t{bs}_{size}"
+            out[k + "_Ar"], out[k + "_Aj"], out[k + "_Ax"] = A.Ar, A.Aj, A.Ax
+            out[k + "_info"] = np.array([A.rows, A.cols, A.blocksize, A.used], np.uint64)
+            out[k + "_x"], out[k + "_y"] = x, y
+    E = R.q1_poisson(33)
+    for bs in (1, 4):
+        A = R.csr_from_ell(E, bs)
+        x = P.uniform_vector(A.cols, 7)
+        b = P.uniform_vector(A.rows, 8)
+        k = f"q1_{bs}"
+        out[k + "_Ar"], out[k + "_Aj"], out[k + "_Ax"] = A.Ar, A.Aj, A.Ax
+        out[k + "_info"] = np.array([A.rows, A.cols, A.blocksize, A.used], np.uint64)
+        out[k + "_x"], out[k + "_b"] = x, b
+        out[k + "_y"] = R.csr_spmv(A, x)[0]
+        out[k + "_r"] = R.csr_defect(A, b, x)
+    rng = np.random.default_rng(11)
+    rows, cols = 300, 257
+    mask = rng.random((rows, cols)) < 0.05
+    mask[rng.choice(rows, 20, replace=False)] = False          # empty rows
+    mask[:, cols - 1] |= rng.random(rows) < 0.3                # last column: ragged last blocks
+    ri, ci = np.nonzero(mask)
+    ip = np.zeros(rows + 1, np.int64)
+    np.cumsum(np.bincount(ri, minlength=rows), out=ip[1:])
+    dv = rng.uniform(-1, 1, len(ci))
+    for bs in (1, 3, 8):
+        A = P.csr_blocked(rows, cols, ip, ci, dv, bs)
+        x = rng.uniform(-1, 1, cols)
+        k = f"rand_{bs}"
+        out[k + "_Ar"], out[k + "_Aj"], out[k + "_Ax"] = A.Ar, A.Aj, A.Ax
+        out[k + "_info"] = np.array([A.rows, A.cols, A.blocksize, A.used], np.uint64)
+        out[k + "_x"] = x
+        out[k + "_y"] = R.csr_spmv(A, x)[0]
+        out[k + "_y32"] = R.csr_spmv(A.astype(np.float32), x.astype(np.float32))[0]
+    np.savez_compressed(os.path.join(HERE, "csr.npz"), **out)
+
+
 def main(tree: str, only: str | None = None) -> None:
     R = Reference()
     if only is not None:
-        {"q1band": lambda R: banded(R), "pcg": lambda R: pcg(R, tree)}[only](R)
+        {"q1band": lambda R: banded(R), "pcg": lambda R: pcg(R, tree), "csr": lambda R: csr(R)}[only](R)
         print("golden fixture", only, "written to", HERE)
         return
     td = os.path.join(tree, "honei", "math", "testdata")
@@ -219,6 +264,7 @@ def main(tree: str, only: str | None = None) -> None:
     np.savez_compressed(os.path.join(HERE, "q1_small.npz"), **out)
     banded(R)
     pcg(R, tree)
+    csr(R)
     print("golden fixtures written to", HERE)
 
 
