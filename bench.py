@@ -295,6 +295,43 @@ def _ref_cpu():
         return None
 
 
+def bench_csr(la, ctx, x, ell_s, M=M_SPMV, reps=100, cpu=True):
+    """Product on SparseMatrixCSR (csr::blocksize 1) of the same 2049^2 Poisson matrix and x as
+    the headline: algorithmic bytes nnz*(8 + 4) + (n + 1)*8 + 2*n*8 per product (values and
+    int32 columns once, the int64 row offsets, x once, y once).  ``ell_s`` is the ELL product's
+    measured time, for the ratio."""
+    import torch
+    from honei_b200 import problems as P
+    Ch = P.csr_from_ell(P.q1_poisson(M), 1)
+    C = la.SparseMatrixCSR.from_reference(Ch, ctx)
+    n, nnz = C.rows(), C.nblocks
+    y = torch.empty_like(x)
+    for _ in range(3):
+        la.Product.value(y, C, x, ctx=ctx)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        la.Product.value(y, C, x, ctx=ctx)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    nbytes = nnz * 12 + (n + 1) * 8 + 2 * n * 8
+    peak, _ = measured_peak()
+    out = {"workload": f"SparseMatrixCSR product (csr::blocksize 1), Poisson {M}^2, FP64", "bytes_per_product": nbytes,
+           "us_per_product": round(t * 1e6, 2), "gbs": round(nbytes / t / 1e9, 1),
+           "frac_of_peak": round(nbytes / t / 1e9 / peak, 4), "time_vs_ell_product": round(t / ell_s, 3)}
+    if cpu:
+        R = _ref_cpu()
+        if R is not None:
+            _, sec = R.csr_spmv(Ch, x.cpu().numpy(), tag="mc-sse", reps=10)
+            out["cpu_reference_gbs"] = round(nbytes / sec / 1e9, 2)
+            out["cpu_reference"] = f"tags::CPU::MultiCore::SSE, {os.cpu_count()} cores, median of 10"
+    del C
+    torch.cuda.empty_cache()
+    return out
+
+
 def bench_q1band(la, ctx, x, ell_s, M=M_SPMV, reps=100, cpu=True):
     """Product on BandedMatrixQx<Q1Type> (nine bands of n values, no index array) for the same
     2049^2 Poisson matrix and x as the headline: algorithmic bytes 11*n*8 per product (nine
@@ -582,6 +619,8 @@ def run_ours(args):
 
     # ---- banded Q1 product (BandedMatrixQx<Q1Type>) of the same grid (extra) ----
     band_extra = bench_q1band(la, ctx, x, per_launch_s, cpu=(ws == 1 and not args.no_cpu_baseline))
+    # ---- SparseMatrixCSR product of the same matrix (extra) ----
+    csr_extra = bench_csr(la, ctx, x, per_launch_s, cpu=(ws == 1 and not args.no_cpu_baseline))
 
     # ---- plain FP64 CG on 257^2: solve latency (host b -> device solve -> host x) ----
     Acg = la.SparseMatrixELL.q1_poisson(M_CG, ctx=ctx)
@@ -651,7 +690,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": n * 8, "api": "honei_b200.la.Product.value (C ABI hb_spmv_f64)"},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
-            "extra": {"spmv_f32_gbs": round(gbs32, 2), "q1band_2049": band_extra, "cg_257": cg_extra,
+            "extra": {"spmv_f32_gbs": round(gbs32, 2), "q1band_2049": band_extra, "csr_2049": csr_extra, "cg_257": cg_extra,
                       "cg_257_cluster": cg_cluster,
                       "mg_2049": mg_extra, "ir_2049": ir_extra, "batch_512": batch_extra, "serve": serve_extra},
         }

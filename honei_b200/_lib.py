@@ -33,6 +33,12 @@ class HbQ1Band(C.Structure):
                 ("pad_", C.c_int32)]
 
 
+class HbCsr(C.Structure):
+    _fields_ = [("rows", C.c_int64), ("cols", C.c_int64), ("blocksize", C.c_int64), ("nblocks", C.c_int64),
+                ("Ar", C.c_void_p), ("Aj", C.c_void_p), ("Ax", C.c_void_p), ("dtype", C.c_int32),
+                ("pad_", C.c_int32)]
+
+
 class HbMGParams(C.Structure):
     _fields_ = [("max_iters", C.c_int64), ("max_iters_coarse", C.c_int64), ("n_pre", C.c_int64),
                 ("n_post", C.c_int64), ("damping", C.c_double), ("eps", C.c_double)]
@@ -42,6 +48,7 @@ i64, vp, f64, f32, i32 = C.c_int64, C.c_void_p, C.c_double, C.c_float, C.c_int
 P_i64 = C.POINTER(C.c_int64)
 P_ell = C.POINTER(HbEll)
 P_band = C.POINTER(HbQ1Band)
+P_csr = C.POINTER(HbCsr)
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -130,6 +137,12 @@ SIGNATURES = {
     "hb_ell_write_file": (i32, [vp, P_ell, C.c_char_p]),
     # banded Q1 matrices
     "hb_q1band_root": (i64, [i64]),
+    "hb_csr_import_f64": (i32, [vp, vp, vp, vp, P_csr]),
+    "hb_csr_import_f32": (i32, [vp, vp, vp, vp, P_csr]),
+    "hb_csr_spmv_f64": (i32, [vp, P_csr, vp, vp]),
+    "hb_csr_spmv_f32": (i32, [vp, P_csr, vp, vp]),
+    "hb_csr_defect_f64": (i32, [vp, P_csr, vp, vp, vp]),
+    "hb_csr_defect_f32": (i32, [vp, P_csr, vp, vp, vp]),
     "hb_q1band_spmv_f64": (i32, [vp, P_band, vp, vp]),
     "hb_q1band_spmv_f32": (i32, [vp, P_band, vp, vp]),
     "hb_q1band_defect_f64": (i32, [vp, P_band, vp, vp, vp]),

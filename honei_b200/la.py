@@ -22,7 +22,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import HbEll, check, lib
+from ._lib import HbCsr, HbEll, check, lib
 
 
 class VectorSizeDoesNotMatch(ValueError):
@@ -308,15 +308,63 @@ class BandedMatrixQ1:
         return self.bands[k, : self.n]
 
 
+class SparseMatrixCSR:
+    """Device mirror of a HONEI SparseMatrixCSR (honei/la/sparse_matrix_csr.hh): Ar int64[rows + 1]
+    block offsets, Aj int32[nblocks] first column of each block, Ax [nblocks * blocksize]."""
+
+    def __init__(self, rows, cols, blocksize, Ar: torch.Tensor, Aj: torch.Tensor, Ax: torch.Tensor):
+        self._rows, self._cols, self._bs = int(rows), int(cols), int(blocksize)
+        self.Ar, self.Aj, self.Ax = Ar, Aj, Ax
+        self.dtype = Ax.dtype
+        self.nblocks = int(Aj.numel())
+        self._s = HbCsr(self._rows, self._cols, self._bs, self.nblocks, Ar.data_ptr(), Aj.data_ptr(),
+                        Ax.data_ptr(), _DT[Ax.dtype], 0)
+
+    def rows(self) -> int:
+        return self._rows
+
+    def columns(self) -> int:
+        return self._cols
+
+    def blocksize(self) -> int:
+        return self._bs
+
+    @property
+    def struct(self) -> HbCsr:
+        return self._s
+
+    @classmethod
+    def from_reference(cls, csr, ctx: Context | None = None, device="cuda") -> "SparseMatrixCSR":
+        """Uploads the reference-layout arrays (u64 Ar, u64 Aj, Ax; problems.CsrMatrix) and
+        imports them (hb_csr_import_*)."""
+        ctx = ctx or default_context()
+        dt = torch.float64 if csr.Ax.dtype == np.float64 else torch.float32
+        nb = int(csr.Ar[-1]) if len(csr.Ar) else 0
+        Ar_ref = torch.from_numpy(np.ascontiguousarray(csr.Ar, np.uint64).view(np.int64)).to(device)
+        Aj_ref = torch.from_numpy(np.ascontiguousarray(csr.Aj[:nb], np.uint64).view(np.int64)).to(device)
+        Ax_ref = torch.from_numpy(np.ascontiguousarray(csr.Ax[:nb * csr.blocksize])).to(device)
+        Ar = torch.empty(csr.rows + 1, dtype=torch.int64, device=device)
+        Aj = torch.empty(max(nb, 1), dtype=torch.int32, device=device)[:nb]
+        Ax = torch.empty(max(nb * csr.blocksize, 1), dtype=dt, device=device)[:nb * csr.blocksize]
+        out = HbCsr(csr.rows, csr.cols, csr.blocksize, nb, Ar.data_ptr(), Aj.data_ptr(), Ax.data_ptr(), _DT[dt], 0)
+        fn = lib().hb_csr_import_f64 if dt == torch.float64 else lib().hb_csr_import_f32
+        check(fn(ctx.handle, Ar_ref.data_ptr(), Aj_ref.data_ptr(), Ax_ref.data_ptr(), C.byref(out)),
+              "hb_csr_import", ctx.handle)
+        return cls(csr.rows, csr.cols, csr.blocksize, Ar, Aj, Ax)
+
+
 def _spmv_fn(A, kind: str):
     if isinstance(A, BandedMatrixQ1):
         return getattr(lib(), f"hb_q1band_{kind}_{_SUF[A.dtype]}")
+    if isinstance(A, SparseMatrixCSR):
+        return getattr(lib(), f"hb_csr_{kind}_{_SUF[A.dtype]}")
     return getattr(lib(), f"hb_{kind}_{_SUF[A.dtype]}")
 
 
 class Product:
     """Product<tags::GPU::CUDA>::value(y, A, x): y = A x, for a SparseMatrixELL
-    (honei/la/product.hh:1758-1760) or a BandedMatrixQ1 (honei/la/product.hh:1750-1756)."""
+    (honei/la/product.hh:1758-1760), a SparseMatrixCSR (honei/la/product.hh:1762-1764) or a
+    BandedMatrixQ1 (honei/la/product.hh:1750-1756)."""
 
     @staticmethod
     def value(y: torch.Tensor, A, x: torch.Tensor, ctx: Context | None = None):
@@ -332,14 +380,15 @@ class Product:
 
 class Defect:
     """Defect<tags::GPU::CUDA>::value(r, b, A, x): r = b - A x for a SparseMatrixELL
-    (honei/math/defect.hh:660-670) or a BandedMatrixQ1 (honei/math/defect.hh:645-658)."""
+    (honei/math/defect.hh:660-670), a SparseMatrixCSR (honei/math/defect.hh:673-676) or a
+    BandedMatrixQ1 (honei/math/defect.hh:645-658)."""
 
     @staticmethod
     def value(r: torch.Tensor, b: torch.Tensor, A, x: torch.Tensor, ctx: Context | None = None):
         if x.numel() != A.columns():
             raise VectorSizeDoesNotMatch(x.numel(), A.columns())
-        if b.numel() != A.columns():
-            raise VectorSizeDoesNotMatch(b.numel(), A.columns())
+        if b.numel() != A.rows():
+            raise VectorSizeDoesNotMatch(b.numel(), A.rows())
         if r.numel() != A.rows():
             raise VectorSizeDoesNotMatch(r.numel(), A.rows())
         ctx = ctx or default_context()

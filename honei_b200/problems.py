@@ -144,33 +144,29 @@ def csr_blocked(rows: int, cols: int, indptr, indices, data, blocksize: int = 1,
     (honei/la/sparse_matrix_csr-impl.hh:98-136): per row, walking the stored entries in column
     order, a block starts at the entry's column rounded down to a multiple of blocksize and
     takes the following entries that fall on its lanes; lanes without an entry hold zero.
-    ``indices`` ascending per row; every stored entry is kept, zero values included."""
+    ``indices`` strictly ascending per row; every stored entry is kept, zero values included."""
     bs = int(blocksize)
     if bs < 1:
         raise ValueError("blocksize must be >= 1")
     indptr = np.asarray(indptr, np.int64)
     indices = np.asarray(indices, np.int64)
     data = np.asarray(data)
+    n = int(indptr[-1]) if rows else 0
+    row_of = np.repeat(np.arange(rows, dtype=np.int64), np.diff(indptr))
+    if n and not np.all((np.diff(indices[:n]) > 0) | (np.diff(row_of) != 0)):
+        raise ValueError("column indices must ascend strictly within each row (a SparseMatrix's rows do)")
+    # a block is a run of entries sharing (row, column // blocksize): the blocks the
+    # reference's entry walk forms on strictly ascending columns
+    blk = indices[:n] // bs
+    new = np.ones(n, bool)
+    new[1:] = (row_of[1:] != row_of[:-1]) | (blk[1:] != blk[:-1])
+    bid = np.cumsum(new) - 1
+    nb = int(bid[-1]) + 1 if n else 0
+    Ax = np.zeros(nb * bs, dtype)
+    Ax[bid * bs + indices[:n] % bs] = data[:n]
     Ar = np.zeros(rows + 1, np.uint64)
-    Aj, Ax = [], []
-    for r in range(rows):
-        Ar[r] = len(Aj)
-        lo, hi = int(indptr[r]), int(indptr[r + 1])
-        i = lo
-        while i < hi:
-            start = int(indices[i]) - int(indices[i]) % bs
-            lanes = np.zeros(bs, dtype)
-            d = 0
-            for k in range(bs):
-                if i + d < hi and start + k == int(indices[i + d]):
-                    lanes[k] = data[i + d]
-                    d += 1
-            Aj.append(start)
-            Ax.append(lanes)
-            i += d
-    Ar[rows] = len(Aj)
-    Axa = np.concatenate(Ax).astype(dtype) if Ax else np.zeros(0, dtype)
-    return CsrMatrix(rows, cols, bs, Ar, np.asarray(Aj, np.uint64), Axa, int(indptr[-1]) if rows else 0)
+    np.cumsum(np.bincount(row_of[new], minlength=rows), out=Ar[1:])
+    return CsrMatrix(rows, cols, bs, Ar, (blk[new] * bs).astype(np.uint64), Ax, n)
 
 
 def csr_from_ell(A: "EllMatrix", blocksize: int = 1) -> CsrMatrix:

@@ -100,6 +100,39 @@ int hb_ell_import_f32(hb_context *ctx, int64_t rows, int64_t cols, int64_t strid
 /* Same pattern, values cast to float (for the FP32 inner solves of mixed precision). */
 int hb_ell_cast_f64_f32(hb_context *ctx, const hb_ell *src, hb_ell *dst);
 
+/* ------------------------------------------------------------------------------------------
+ * Device CSR matrix.  Replaces the device copies of SparseMatrixCSR's Ar/Aj/Ax arrays
+ * (honei/la/sparse_matrix_csr.hh) that the reference uploads for its CSR product kernel
+ * (cuda_product_csr_dv_{float,double}, honei/backends/cuda/operations.hh, product.cu:257-296).
+ *
+ * Layout: Ar int64[rows + 1] block offsets (Ar[0] = 0, non-decreasing, Ar[rows] = nblocks);
+ * Aj int32[nblocks] the first column of each block (csr::blocksize values per block); Ax
+ * dtype[nblocks * blocksize].  Block columns at or beyond cols are stored as cols: every lane of
+ * such a block lies outside the matrix, as in the reference, whose product skips lanes whose
+ * column is not below cols.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct hb_csr {
+    int64_t rows, cols;
+    int64_t blocksize;   /* csr::blocksize */
+    int64_t nblocks;
+    int64_t *Ar;         /* device */
+    int32_t *Aj;         /* device */
+    void *Ax;            /* device */
+    int32_t dtype;       /* HB_F64 / HB_F32 */
+    int32_t pad_;
+} hb_csr;
+
+/* Import a reference SparseMatrixCSR whose arrays (uint64 Ar[rows + 1], uint64 Aj[nblocks],
+ * values Ax[nblocks * blocksize]) are already on the device into out (out->Ar/Aj/Ax
+ * preallocated; out->rows, cols, blocksize, nblocks set).  Replaces the matrix half of
+ * MemoryBackend<tags::GPU::CUDA>::upload for SparseMatrixCSR plus the narrowing of the 64-bit
+ * indices.  HB_ERR_INVALID when Ar is not a valid offset array (checked on the device; the
+ * call synchronises ctx's stream); HB_ERR_UNSUPPORTED for cols or rows beyond 2^31 - 2. */
+int hb_csr_import_f64(hb_context *ctx, const uint64_t *Ar_ref, const uint64_t *Aj_ref, const double *Ax_ref,
+                      hb_csr *out);
+int hb_csr_import_f32(hb_context *ctx, const uint64_t *Ar_ref, const uint64_t *Aj_ref, const float *Ax_ref,
+                      hb_csr *out);
+
 /* Q1 Poisson assembly on the device (the FillMatrix<POISSON, DIRICHLET_0> stencil,
  * honei/math/fill_matrix.hh:37-77, built straight into hb_ell layout, K = 9): M x M nodes,
  * Dirichlet rows identity; coef = NULL (unit) or device double[(M-1)^2] cell coefficients
@@ -222,6 +255,17 @@ int hb_fill_f64(hb_context *ctx, int64_t n, double *x, double value);
 int hb_fill_f32(hb_context *ctx, int64_t n, float *x, float value);
 int hb_convert_f64_f32(hb_context *ctx, int64_t n, float *dst, const double *src);
 int hb_convert_f32_f64(hb_context *ctx, int64_t n, double *dst, const float *src);
+
+/* y = A x on SparseMatrixCSR: Product<tags::GPU::CUDA>::value(DV, SparseMatrixCSR, DV)
+ * (honei/la/product.hh:1762-1764) with the tags::CPU arithmetic (honei/la/product.hh:209-242):
+ * per row, its blocks and their lanes in order, lanes whose column is not below cols skipped;
+ * bit-identical to tags::CPU.  r = rhs - A x: Defect<tags::GPU::CUDA>::value(DV, DV,
+ * SparseMatrixCSR, DV) (honei/math/defect.hh:673-676; tags::CPU honei/math/defect.hh:386-419).
+ * x has cols entries, y / rhs / r rows; asynchronous on ctx's stream. */
+int hb_csr_spmv_f64(hb_context *ctx, const hb_csr *A, const double *x, double *y);
+int hb_csr_spmv_f32(hb_context *ctx, const hb_csr *A, const float *x, float *y);
+int hb_csr_defect_f64(hb_context *ctx, const hb_csr *A, const double *rhs, const double *x, double *r);
+int hb_csr_defect_f32(hb_context *ctx, const hb_csr *A, const float *rhs, const float *x, float *r);
 
 /* ------------------------------------------------------------------------------------------
  * Solvers.
