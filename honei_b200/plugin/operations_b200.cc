@@ -1,9 +1,9 @@
 /* operations_b200.cc -- HONEI's tags::GPU::CUDA operators on the B200 backend.
  *
  * Defines the static members HONEI declares unconditionally for the GPU tag:
- *   Product<tags::GPU::CUDA>         honei/la/product.hh:1728-1794   (ELL SpMV, banded Q1
- *                                                                     product, Jacobi apply)
- *   Defect<tags::GPU::CUDA>          honei/math/defect.hh:645-692    (ELL and banded Q1 defect)
+ *   Product<tags::GPU::CUDA>         honei/la/product.hh:1728-1794   (ELL and CSR SpMV, banded
+ *                                                                     Q1 product, Jacobi apply)
+ *   Defect<tags::GPU::CUDA>          honei/math/defect.hh:645-692    (ELL, CSR and banded Q1 defect)
  *   DotProduct<tags::GPU::CUDA>      honei/la/dot_product.hh:343-368
  *   Norm<vnt_l_two, {false,true}, tags::GPU::CUDA>  honei/la/norm.hh:538-580
  *   ScaledSum<tags::GPU::CUDA>       honei/la/scaled_sum.hh:444-488
@@ -23,6 +23,7 @@
 #include <honei/la/product.hh>
 #include <honei/la/scale.hh>
 #include <honei/la/scaled_sum.hh>
+#include <honei/la/sparse_matrix_csr.hh>
 #include <honei/la/sum.hh>
 #include <honei/la/vector_error.hh>
 #include <honei/math/defect.hh>
@@ -73,8 +74,26 @@ namespace honei
                 void * Aj_dev[3];
             };
 
+            struct CsrMirror
+            {
+                hb_csr csr;
+                std::uint64_t gen[3];
+                void * dev[3];
+            };
+
             std::mutex g_mirror_mutex;
-            std::map<void *, Mirror> g_mirrors;   // keyed by the Ax memid
+            std::map<void *, Mirror> g_mirrors;        // keyed by the Ax memid
+            std::map<void *, CsrMirror> g_csr_mirrors; // keyed by the Ax memid
+
+            void free_csr(hb_csr & c)
+            {
+                cudaFree(c.Ar);
+                cudaFree(c.Aj);
+                cudaFree(c.Ax);
+                c.Ar = nullptr;
+                c.Aj = nullptr;
+                c.Ax = nullptr;
+            }
 
             template <typename DT_> int dtype_of();
             template <> int dtype_of<double>() { return HB_F64; }
@@ -103,6 +122,66 @@ namespace honei
                 cudaFree(i->second.ell.Ax);
                 g_mirrors.erase(i);
             }
+            auto c(g_csr_mirrors.find(memid));
+            if (c != g_csr_mirrors.end())
+            {
+                free_csr(c->second.csr);
+                g_csr_mirrors.erase(c);
+            }
+        }
+
+        /// The hb_csr mirror of a SparseMatrixCSR: imported from the backend's copies of
+        /// Ar / Aj / Ax on first use, again whenever one of them was uploaded again.
+        template <typename DT_> const hb_csr & device_mirror(const SparseMatrixCSR<DT_> & a)
+        {
+            // the stored blocks (Aj may be allocated longer: the reference sizes it by entries)
+            const std::int64_t nb((std::int64_t)a.Ar()[a.rows()]);
+            void * ar(a.Ar().lock(lm_read_only, tags::GPU::CUDA::memory_value));
+            void * aj(a.Aj().lock(lm_read_only, tags::GPU::CUDA::memory_value));
+            void * ax(a.Ax().lock(lm_read_only, tags::GPU::CUDA::memory_value));
+            const std::uint64_t g0(generation(a.Ar().memid(), a.Ar().address()));
+            const std::uint64_t g1(generation(a.Aj().memid(), a.Aj().address()));
+            const std::uint64_t g2(generation(a.Ax().memid(), a.Ax().address()));
+            std::lock_guard<std::mutex> l(g_mirror_mutex);
+            CsrMirror & m(g_csr_mirrors[a.Ax().memid()]);
+            int st(HB_OK);
+            if (! m.csr.Ar || m.gen[0] != g0 || m.gen[1] != g1 || m.gen[2] != g2 || m.dev[0] != ar
+                    || m.dev[1] != aj || m.dev[2] != ax)
+            {
+                const std::int64_t bs((std::int64_t)a.blocksize());
+                if (! m.csr.Ar || m.csr.rows != (std::int64_t)a.rows() || m.csr.nblocks != nb || m.csr.blocksize != bs)
+                {
+                    free_csr(m.csr);
+                    if (cudaMalloc((void **)&m.csr.Ar, (a.rows() + 1) * sizeof(std::int64_t)) != cudaSuccess ||
+                            cudaMalloc((void **)&m.csr.Aj, (nb > 0 ? nb : 1) * sizeof(std::int32_t)) != cudaSuccess ||
+                            cudaMalloc(&m.csr.Ax, (nb > 0 ? nb * bs : 1) * sizeof(DT_)) != cudaSuccess)
+                    {
+                        cudaGetLastError();
+                        free_csr(m.csr);
+                        st = HB_ERR_ALLOC;
+                    }
+                }
+                if (! st)
+                {
+                    m.csr.rows = a.rows();
+                    m.csr.cols = a.columns();
+                    m.csr.blocksize = bs;
+                    m.csr.nblocks = nb;
+                    m.csr.dtype = dtype_of<DT_>();
+                    m.csr.pad_ = 0;
+                    st = sizeof(DT_) == 8
+                        ? hb_csr_import_f64(context(), (const uint64_t *)ar, (const uint64_t *)aj, (const double *)ax, &m.csr)
+                        : hb_csr_import_f32(context(), (const uint64_t *)ar, (const uint64_t *)aj, (const float *)ax, &m.csr);
+                }
+                m.gen[0] = g0; m.gen[1] = g1; m.gen[2] = g2;
+                m.dev[0] = ar; m.dev[1] = aj; m.dev[2] = ax;
+                if (st) m.gen[0] = 0;
+            }
+            a.Ar().unlock(lm_read_only);
+            a.Aj().unlock(lm_read_only);
+            a.Ax().unlock(lm_read_only);
+            check(st, "SparseMatrixCSR device mirror");
+            return m.csr;
         }
 
         template <typename DT_> const hb_ell & device_mirror(const SparseMatrixELL<DT_> & a)
@@ -253,6 +332,43 @@ namespace honei
                     "Defect<GPU::CUDA> (BandedMatrixQx)");
         }
 
+        int csr_spmv(const hb_csr & A, const double * x, double * y) { return hb_csr_spmv_f64(context(), &A, x, y); }
+        int csr_spmv(const hb_csr & A, const float * x, float * y) { return hb_csr_spmv_f32(context(), &A, x, y); }
+        int csr_defect(const hb_csr & A, const double * b, const double * x, double * r)
+        { return hb_csr_defect_f64(context(), &A, b, x, r); }
+        int csr_defect(const hb_csr & A, const float * b, const float * x, float * r)
+        { return hb_csr_defect_f32(context(), &A, b, x, r); }
+
+        template <typename DT_>
+        void product(DenseVectorContinuousBase<DT_> & result, const SparseMatrixCSR<DT_> & a, const DenseVectorContinuousBase<DT_> & b)
+        {
+            if (b.size() != a.columns())
+                throw VectorSizeDoesNotMatch(b.size(), a.columns());
+            if (a.rows() != result.size())
+                throw VectorSizeDoesNotMatch(a.rows(), result.size());
+            const hb_csr & A(device_mirror(a));
+            DeviceLock<DenseVectorContinuousBase<DT_> > x(b, lm_read_only);
+            DeviceLock<DenseVectorContinuousBase<DT_> > y(result, lm_write_only);
+            check(csr_spmv(A, (const DT_ *)x.ptr, (DT_ *)y.ptr), "Product<GPU::CUDA> (CSR)");
+        }
+
+        template <typename DT_>
+        void defect(DenseVectorContinuousBase<DT_> & result, const DenseVectorContinuousBase<DT_> & rhs,
+                const SparseMatrixCSR<DT_> & a, const DenseVectorContinuousBase<DT_> & x)
+        {
+            if (x.size() != a.columns())
+                throw VectorSizeDoesNotMatch(x.size(), a.columns());
+            if (rhs.size() != a.rows())
+                throw VectorSizeDoesNotMatch(rhs.size(), a.rows());
+            if (result.size() != a.rows())
+                throw VectorSizeDoesNotMatch(result.size(), a.rows());
+            const hb_csr & A(device_mirror(a));
+            DeviceLock<DenseVectorContinuousBase<DT_> > xl(x, lm_read_only);
+            DeviceLock<DenseVectorContinuousBase<DT_> > bl(rhs, lm_read_only);
+            DeviceLock<DenseVectorContinuousBase<DT_> > rl(result, lm_write_only);
+            check(csr_defect(A, (const DT_ *)bl.ptr, (const DT_ *)xl.ptr, (DT_ *)rl.ptr), "Defect<GPU::CUDA> (CSR)");
+        }
+
         template <typename DT_>
         void product(DenseVectorContinuousBase<DT_> & result, const SparseMatrixELL<DT_> & a, const DenseVectorContinuousBase<DT_> & b)
         {
@@ -299,6 +415,22 @@ namespace honei
             const DenseVector<double> & b)
     {
         CONTEXT("When multiplying SparseMatrixELL<double> with DenseVector<double> (B200):");
+        b200::product<double>(result, a, b);
+        return result;
+    }
+
+    DenseVector<float> & Product<tags::GPU::CUDA>::value(DenseVector<float> & result, const SparseMatrixCSR<float> & a,
+            const DenseVector<float> & b)
+    {
+        CONTEXT("When multiplying SparseMatrixCSR<float> with DenseVector<float> (B200):");
+        b200::product<float>(result, a, b);
+        return result;
+    }
+
+    DenseVector<double> & Product<tags::GPU::CUDA>::value(DenseVector<double> & result, const SparseMatrixCSR<double> & a,
+            const DenseVector<double> & b)
+    {
+        CONTEXT("When multiplying SparseMatrixCSR<double> with DenseVector<double> (B200):");
         b200::product<double>(result, a, b);
         return result;
     }
@@ -396,6 +528,22 @@ namespace honei
 
     DenseVectorContinuousBase<double> & Defect<tags::GPU::CUDA>::value(DenseVectorContinuousBase<double> & result,
             const DenseVectorContinuousBase<double> & rhs, const SparseMatrixELL<double> & system,
+            const DenseVectorContinuousBase<double> & x)
+    {
+        b200::defect<double>(result, rhs, system, x);
+        return result;
+    }
+
+    DenseVectorContinuousBase<float> & Defect<tags::GPU::CUDA>::value(DenseVectorContinuousBase<float> & result,
+            const DenseVectorContinuousBase<float> & rhs, const SparseMatrixCSR<float> & system,
+            const DenseVectorContinuousBase<float> & x)
+    {
+        b200::defect<float>(result, rhs, system, x);
+        return result;
+    }
+
+    DenseVectorContinuousBase<double> & Defect<tags::GPU::CUDA>::value(DenseVectorContinuousBase<double> & result,
+            const DenseVectorContinuousBase<double> & rhs, const SparseMatrixCSR<double> & system,
             const DenseVectorContinuousBase<double> & x)
     {
         b200::defect<double>(result, rhs, system, x);

@@ -14,7 +14,9 @@
 #include <honei/la/product.hh>
 #include <honei/la/scale.hh>
 #include <honei/la/scaled_sum.hh>
+#include <honei/la/sparse_matrix_csr.hh>
 #include <honei/la/sum.hh>
+#include <honei/util/configuration.hh>
 #include <honei/math/cg.hh>
 #include <honei/math/defect.hh>
 #include <honei/math/matrix_io.hh>
@@ -223,8 +225,62 @@ template <typename DT_> void banded(unsigned long M, const std::string & tag)
     report(threw, "BandedMatrixQx VectorSizeDoesNotMatch before launch " + tag);
 }
 
+// SparseMatrixCSR (csr::blocksize 1 and 4) built from the reference's Q1 ELL matrix, and the
+// reference's own CSR product test matrix (rectangular, ragged last blocks): product and defect
+// on tags::GPU::CUDA against tags::CPU.
+template <typename DT_> void csr(unsigned long M, const std::string & tag)
+{
+    SparseMatrixELL<DT_> E(q1<DT_>(M));
+    const unsigned long n(E.rows());
+    DenseVector<DT_> x(seeded<DT_>(n, 21)), b(seeded<DT_>(n, 22));
+    const unsigned long old(Configuration::instance()->get_value("csr::blocksize", 1));
+    for (unsigned long bs(1) ; bs <= 4 ; bs *= 4)
+    {
+        Configuration::instance()->set_value("csr::blocksize", bs);
+        SparseMatrixCSR<DT_> A(E);
+        const std::string what(" blocksize " + std::to_string(bs) + " " + tag);
+        DenseVector<DT_> ycpu(n), ygpu(n);
+        Product<tags::CPU>::value(ycpu, A, x);
+        Product<tags::GPU::CUDA>::value(ygpu, A, x);
+        report(equal(ycpu, ygpu), "Product<GPU::CUDA> SparseMatrixCSR bit-exact" + what);
+        DenseVector<DT_> rcpu(n), rgpu(n);
+        Defect<tags::CPU>::value(rcpu, b, A, x);
+        Defect<tags::GPU::CUDA>::value(rgpu, b, A, x);
+        report(equal(rcpu, rgpu), "Defect<GPU::CUDA> SparseMatrixCSR bit-exact" + what);
+        // the matrix of the reference's CSR product test (honei/la/product_TEST.cc:936-947)
+        const unsigned long size(176);
+        SparseMatrix<DT_> sms(size, size + 3);
+        for (typename SparseMatrix<DT_>::ElementIterator i(sms.begin_elements()) ; i < sms.end_elements() ; ++i)
+            if (i.index() % 5 == 0)
+                *i = DT_(i.index()) / 1.234;
+        SparseMatrixCSR<DT_> T(sms);
+        DenseVector<DT_> dv1(size + 3, DT_(4));
+        dv1[0] = 1;
+        dv1[1] = 2;
+        DenseVector<DT_> pc(size, DT_(4711)), pg(size, DT_(4711));
+        Product<tags::CPU>::value(pc, T, dv1);
+        Product<tags::GPU::CUDA>::value(pg, T, dv1);
+        report(equal(pc, pg), "Product<GPU::CUDA> SparseMatrixCSR (reference test matrix) bit-exact" + what);
+    }
+    Configuration::instance()->set_value("csr::blocksize", old);
+    bool threw(false);
+    try
+    {
+        SparseMatrixCSR<DT_> A(E);
+        DenseVector<DT_> wrong(n + 1), y(n);
+        Product<tags::GPU::CUDA>::value(y, A, wrong);
+    }
+    catch (VectorSizeDoesNotMatch &)
+    {
+        threw = true;
+    }
+    report(threw, "SparseMatrixCSR VectorSizeDoesNotMatch before launch " + tag);
+}
+
 int main(int argc, char ** argv)
 {
+    csr<double>(33, "f64 33^2");
+    csr<float>(65, "f32 65^2");
     banded<double>(33, "f64 33^2");
     banded<float>(129, "f32 129^2");
     operators<double>(33, "f64 33^2");

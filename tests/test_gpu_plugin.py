@@ -45,6 +45,7 @@ def test_plugin_operators_and_generic_solvers(tmp_path):
     assert "FAIL" not in out
     assert out.count("PASS") >= 54
     assert out.count("BandedMatrixQx") == 14
+    assert out.count("SparseMatrixCSR") == 14
 
 
 def test_plugin_cg_specialisation():
