@@ -458,6 +458,7 @@ int hb_batch_results(hb_context *ctx, int64_t count, void *ws, hb_batch_result *
 int hb_batch_solve(hb_context *ctx, const hb_batch_system *sys, int64_t count, void *ws, const hb_batch_config *cfg,
                    hb_batch_result *results_host)
 {
+    HB_RANGE("hb_batch_solve");
     int st = hb_batch_prepare(ctx, sys, count, ws);
     if (st) return st;
     st = hb_batch_run(ctx, count, ws, cfg);
@@ -468,6 +469,7 @@ int hb_batch_solve(hb_context *ctx, const hb_batch_system *sys, int64_t count, v
 int hb_batch_tune(hb_context *ctx, const hb_batch_system *sys, int64_t count, void *ws, hb_batch_config *best,
                   double *times_ms)
 {
+    HB_RANGE("hb_batch_tune");
     if (!ctx || !best) return HB_ERR_INVALID;
     int st = hb_batch_prepare(ctx, sys, count, ws);
     if (st) return st;

@@ -156,47 +156,49 @@ template int hb_launch_dot<float>(hb_context *, int64_t, const float *, const fl
 extern "C" {
 
 int hb_dot_f64(hb_context *ctx, int64_t n, const double *x, const double *y, double *res)
-{ return dot_impl<double, false>(ctx, n, x, y, res); }
+{ HB_RANGE("hb_dot_f64"); return dot_impl<double, false>(ctx, n, x, y, res); }
 int hb_dot_f32(hb_context *ctx, int64_t n, const float *x, const float *y, float *res)
-{ return dot_impl<float, false>(ctx, n, x, y, res); }
+{ HB_RANGE("hb_dot_f32"); return dot_impl<float, false>(ctx, n, x, y, res); }
 
 int hb_norm_l2_f64(hb_context *ctx, int64_t n, const double *x, int root, double *res)
 {
+    HB_RANGE("hb_norm_l2_f64");
     int st = dot_impl<double, true>(ctx, n, x, nullptr, res);
     if (!st && root) *res = std::sqrt(*res);
     return st;
 }
 int hb_norm_l2_f32(hb_context *ctx, int64_t n, const float *x, int root, float *res)
 {
+    HB_RANGE("hb_norm_l2_f32");
     int st = dot_impl<float, true>(ctx, n, x, nullptr, res);
     if (!st && root) *res = std::sqrt(*res);
     return st;
 }
 
 int hb_scaled_sum_f64(hb_context *c, int64_t n, double *x, const double *y, double b)
-{ if (!x || !y) return HB_ERR_INVALID; return ew_launch<double, OP_AXPY>(c, n, x, x, y, b); }
+{ HB_RANGE("hb_scaled_sum_f64"); if (!x || !y) return HB_ERR_INVALID; return ew_launch<double, OP_AXPY>(c, n, x, x, y, b); }
 int hb_scaled_sum_f32(hb_context *c, int64_t n, float *x, const float *y, float b)
-{ if (!x || !y) return HB_ERR_INVALID; return ew_launch<float, OP_AXPY>(c, n, x, x, y, b); }
+{ HB_RANGE("hb_scaled_sum_f32"); if (!x || !y) return HB_ERR_INVALID; return ew_launch<float, OP_AXPY>(c, n, x, x, y, b); }
 int hb_scaled_sum3_f64(hb_context *c, int64_t n, double *r, const double *x, const double *y, double b)
-{ if (!x || !y) return HB_ERR_INVALID; return ew_launch<double, OP_AXPY3>(c, n, r, x, y, b); }
+{ HB_RANGE("hb_scaled_sum3_f64"); if (!x || !y) return HB_ERR_INVALID; return ew_launch<double, OP_AXPY3>(c, n, r, x, y, b); }
 int hb_scaled_sum3_f32(hb_context *c, int64_t n, float *r, const float *x, const float *y, float b)
-{ if (!x || !y) return HB_ERR_INVALID; return ew_launch<float, OP_AXPY3>(c, n, r, x, y, b); }
+{ HB_RANGE("hb_scaled_sum3_f32"); if (!x || !y) return HB_ERR_INVALID; return ew_launch<float, OP_AXPY3>(c, n, r, x, y, b); }
 int hb_scale_f64(hb_context *c, int64_t n, double *x, double a)
-{ if (!x) return HB_ERR_INVALID; return ew_launch<double, OP_SCALE>(c, n, x, x, nullptr, a); }
+{ HB_RANGE("hb_scale_f64"); if (!x) return HB_ERR_INVALID; return ew_launch<double, OP_SCALE>(c, n, x, x, nullptr, a); }
 int hb_scale_f32(hb_context *c, int64_t n, float *x, float a)
-{ if (!x) return HB_ERR_INVALID; return ew_launch<float, OP_SCALE>(c, n, x, x, nullptr, a); }
+{ HB_RANGE("hb_scale_f32"); if (!x) return HB_ERR_INVALID; return ew_launch<float, OP_SCALE>(c, n, x, x, nullptr, a); }
 int hb_sum_f64(hb_context *c, int64_t n, double *x, const double *y)
-{ if (!x || !y) return HB_ERR_INVALID; return ew_launch<double, OP_SUM>(c, n, x, x, y, 0.0); }
+{ HB_RANGE("hb_sum_f64"); if (!x || !y) return HB_ERR_INVALID; return ew_launch<double, OP_SUM>(c, n, x, x, y, 0.0); }
 int hb_sum_f32(hb_context *c, int64_t n, float *x, const float *y)
-{ if (!x || !y) return HB_ERR_INVALID; return ew_launch<float, OP_SUM>(c, n, x, x, y, 0.f); }
+{ HB_RANGE("hb_sum_f32"); if (!x || !y) return HB_ERR_INVALID; return ew_launch<float, OP_SUM>(c, n, x, x, y, 0.f); }
 int hb_difference_f64(hb_context *c, int64_t n, double *r, const double *x, const double *y)
-{ if (!x || !y) return HB_ERR_INVALID; return ew_launch<double, OP_DIFF>(c, n, r, x, y, 0.0); }
+{ HB_RANGE("hb_difference_f64"); if (!x || !y) return HB_ERR_INVALID; return ew_launch<double, OP_DIFF>(c, n, r, x, y, 0.0); }
 int hb_difference_f32(hb_context *c, int64_t n, float *r, const float *x, const float *y)
-{ if (!x || !y) return HB_ERR_INVALID; return ew_launch<float, OP_DIFF>(c, n, r, x, y, 0.f); }
+{ HB_RANGE("hb_difference_f32"); if (!x || !y) return HB_ERR_INVALID; return ew_launch<float, OP_DIFF>(c, n, r, x, y, 0.f); }
 int hb_element_product_f64(hb_context *c, int64_t n, double *r, const double *x, const double *y)
-{ if (!x || !y) return HB_ERR_INVALID; return ew_launch<double, OP_EPROD>(c, n, r, x, y, 0.0); }
+{ HB_RANGE("hb_element_product_f64"); if (!x || !y) return HB_ERR_INVALID; return ew_launch<double, OP_EPROD>(c, n, r, x, y, 0.0); }
 int hb_element_product_f32(hb_context *c, int64_t n, float *r, const float *x, const float *y)
-{ if (!x || !y) return HB_ERR_INVALID; return ew_launch<float, OP_EPROD>(c, n, r, x, y, 0.f); }
+{ HB_RANGE("hb_element_product_f32"); if (!x || !y) return HB_ERR_INVALID; return ew_launch<float, OP_EPROD>(c, n, r, x, y, 0.f); }
 int hb_fill_f64(hb_context *c, int64_t n, double *x, double v)
 { return ew_launch<double, OP_FILL>(c, n, x, nullptr, nullptr, v); }
 int hb_fill_f32(hb_context *c, int64_t n, float *x, float v)
@@ -211,8 +213,8 @@ int hb_copy(hb_context *ctx, void *dst, const void *src, int64_t bytes)
 }
 
 int hb_convert_f64_f32(hb_context *ctx, int64_t n, float *dst, const double *src)
-{ return convert_impl<double, float>(ctx, n, dst, src); }
+{ HB_RANGE("hb_convert_f64_f32"); return convert_impl<double, float>(ctx, n, dst, src); }
 int hb_convert_f32_f64(hb_context *ctx, int64_t n, double *dst, const float *src)
-{ return convert_impl<float, double>(ctx, n, dst, src); }
+{ HB_RANGE("hb_convert_f32_f64"); return convert_impl<float, double>(ctx, n, dst, src); }
 
 }  // extern "C"

@@ -785,12 +785,14 @@ int hb_selftest_wait_timeout(hb_context *ctx)
 int hb_cg_f64(hb_context *ctx, const hb_ell *A, const double *b, double *x, int64_t max_iters,
               double eps, int64_t *used_iters, double *final_defect)
 {
+    HB_RANGE("hb_cg_f64");
     return cg_impl<double>(ctx, A, b, x, max_iters, eps, used_iters, final_defect, HB_F64);
 }
 
 int hb_cg_f32(hb_context *ctx, const hb_ell *A, const float *b, float *x, int64_t max_iters,
               float eps, int64_t *used_iters, float *final_defect)
 {
+    HB_RANGE("hb_cg_f32");
     return cg_impl<float>(ctx, A, b, x, max_iters, eps, used_iters, final_defect, HB_F32);
 }
 

@@ -157,32 +157,38 @@ extern "C" {
 int hb_csr_import_f64(hb_context *ctx, const uint64_t *Ar_ref, const uint64_t *Aj_ref, const double *Ax_ref,
                       hb_csr *out)
 {
+    HB_RANGE("hb_csr_import_f64");
     return import_impl<double>(ctx, Ar_ref, Aj_ref, Ax_ref, out, HB_F64);
 }
 
 int hb_csr_import_f32(hb_context *ctx, const uint64_t *Ar_ref, const uint64_t *Aj_ref, const float *Ax_ref,
                       hb_csr *out)
 {
+    HB_RANGE("hb_csr_import_f32");
     return import_impl<float>(ctx, Ar_ref, Aj_ref, Ax_ref, out, HB_F32);
 }
 
 int hb_csr_spmv_f64(hb_context *ctx, const hb_csr *A, const double *x, double *y)
 {
+    HB_RANGE("hb_csr_spmv_f64");
     return launch<double, 0>(ctx, A, x, nullptr, y, HB_F64);
 }
 
 int hb_csr_spmv_f32(hb_context *ctx, const hb_csr *A, const float *x, float *y)
 {
+    HB_RANGE("hb_csr_spmv_f32");
     return launch<float, 0>(ctx, A, x, nullptr, y, HB_F32);
 }
 
 int hb_csr_defect_f64(hb_context *ctx, const hb_csr *A, const double *rhs, const double *x, double *r)
 {
+    HB_RANGE("hb_csr_defect_f64");
     return launch<double, 1>(ctx, A, x, rhs, r, HB_F64);
 }
 
 int hb_csr_defect_f32(hb_context *ctx, const hb_csr *A, const float *rhs, const float *x, float *r)
 {
+    HB_RANGE("hb_csr_defect_f32");
     return launch<float, 1>(ctx, A, x, rhs, r, HB_F32);
 }
 

@@ -254,6 +254,18 @@ int hb_check_ell(const hb_ell *A, int dtype)
 
 namespace {
 
+// Counts the slots whose column is neither the padding mark (-1) nor inside [0, cols).
+__global__ void ell_validate_kernel(int64_t total, int64_t cols, const int32_t *__restrict__ Aj,
+                                    unsigned long long *bad)
+{
+    unsigned long long n = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t j = Aj[i];
+        if (j < -1 || (int64_t)j >= cols) ++n;
+    }
+    if (n) atomicAdd(bad, n);
+}
+
 template <typename T>
 int import_impl(hb_context *ctx, int64_t rows, int64_t cols, int64_t stride, int64_t ncpr,
                 int64_t threads, const uint64_t *Aj_ref, const T *Ax_ref, const uint64_t *Arl,
@@ -288,6 +300,25 @@ int import_impl(hb_context *ctx, int64_t rows, int64_t cols, int64_t stride, int
 
 extern "C" {
 
+int hb_ell_validate(hb_context *ctx, const hb_ell *A, int64_t *bad_slots)
+{
+    HB_RANGE("hb_ell_validate");
+    if (!ctx || !bad_slots || !A || !A->Aj) return HB_ERR_INVALID;
+    if (A->rows < 0 || A->cols < 0 || A->K < 1 || A->ld < A->rows) return HB_ERR_INVALID;
+    unsigned long long *bad = (unsigned long long *)hb_scalars(ctx);
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(bad, 0, sizeof(*bad), ctx->stream));
+    const int64_t total = A->K * A->ld;
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 32));
+    ell_validate_kernel<<<blocks, 256, 0, ctx->stream>>>(total, A->cols, A->Aj, bad);
+    int st = hb_check_launch(ctx, "ell_validate_kernel");
+    if (st) return st;
+    unsigned long long *h = (unsigned long long *)ctx->pinned;
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, bad, sizeof(*h), cudaMemcpyDeviceToHost, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    *bad_slots = (int64_t)*h;
+    return HB_OK;
+}
+
 int hb_ell_layout(int64_t rows, int64_t ncpr, int64_t threads, int64_t *K, int64_t *ld)
 {
     if (!K || !ld || rows < 0 || ncpr < 1 || threads < 1) return HB_ERR_INVALID;
@@ -300,6 +331,7 @@ int hb_ell_import_f64(hb_context *ctx, int64_t rows, int64_t cols, int64_t strid
                       int64_t threads, const uint64_t *Aj_ref, const double *Ax_ref,
                       const uint64_t *Arl_ref, hb_ell *out)
 {
+    HB_RANGE("hb_ell_import_f64");
     return import_impl<double>(ctx, rows, cols, stride, ncpr, threads, Aj_ref, Ax_ref, Arl_ref, out, HB_F64);
 }
 
@@ -307,6 +339,7 @@ int hb_ell_import_f32(hb_context *ctx, int64_t rows, int64_t cols, int64_t strid
                       int64_t threads, const uint64_t *Aj_ref, const float *Ax_ref,
                       const uint64_t *Arl_ref, hb_ell *out)
 {
+    HB_RANGE("hb_ell_import_f32");
     return import_impl<float>(ctx, rows, cols, stride, ncpr, threads, Aj_ref, Ax_ref, Arl_ref, out, HB_F32);
 }
 
@@ -349,6 +382,7 @@ int hb_q1_assemble_f64(hb_context *ctx, int64_t M, const double *coef, int symme
 
 int hb_spmv_f64(hb_context *ctx, const hb_ell *A, const double *x, double *y)
 {
+    HB_RANGE("hb_spmv_f64");
     int st = hb_check_ell(A, HB_F64);
     if (st) return st;
     return hb_launch_spmv_mode<double>(ctx, A, HB_MODE_SPMV, x, nullptr, nullptr, y);
@@ -356,6 +390,7 @@ int hb_spmv_f64(hb_context *ctx, const hb_ell *A, const double *x, double *y)
 
 int hb_spmv_f32(hb_context *ctx, const hb_ell *A, const float *x, float *y)
 {
+    HB_RANGE("hb_spmv_f32");
     int st = hb_check_ell(A, HB_F32);
     if (st) return st;
     return hb_launch_spmv_mode<float>(ctx, A, HB_MODE_SPMV, x, nullptr, nullptr, y);
@@ -363,6 +398,7 @@ int hb_spmv_f32(hb_context *ctx, const hb_ell *A, const float *x, float *y)
 
 int hb_defect_f64(hb_context *ctx, const hb_ell *A, const double *b, const double *x, double *r)
 {
+    HB_RANGE("hb_defect_f64");
     int st = hb_check_ell(A, HB_F64);
     if (st) return st;
     if (A->rows != A->cols) return HB_ERR_SIZE;
@@ -371,6 +407,7 @@ int hb_defect_f64(hb_context *ctx, const hb_ell *A, const double *b, const doubl
 
 int hb_defect_f32(hb_context *ctx, const hb_ell *A, const float *b, const float *x, float *r)
 {
+    HB_RANGE("hb_defect_f32");
     int st = hb_check_ell(A, HB_F32);
     if (st) return st;
     if (A->rows != A->cols) return HB_ERR_SIZE;

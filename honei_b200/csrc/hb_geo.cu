@@ -141,21 +141,25 @@ extern "C" {
 
 int hb_prolongate_f64(hb_context *ctx, int64_t n_fine, double *fine, const double *coarse, const uint64_t *mask)
 {
+    HB_RANGE("hb_prolongate_f64");
     return transfer<double>(ctx, n_fine, fine, coarse, mask, true);
 }
 
 int hb_prolongate_f32(hb_context *ctx, int64_t n_fine, float *fine, const float *coarse, const uint64_t *mask)
 {
+    HB_RANGE("hb_prolongate_f32");
     return transfer<float>(ctx, n_fine, fine, coarse, mask, true);
 }
 
 int hb_restrict_f64(hb_context *ctx, int64_t n_fine, double *coarse, const double *fine, const uint64_t *mask)
 {
+    HB_RANGE("hb_restrict_f64");
     return transfer<double>(ctx, n_fine, coarse, fine, mask, false);
 }
 
 int hb_restrict_f32(hb_context *ctx, int64_t n_fine, float *coarse, const float *fine, const uint64_t *mask)
 {
+    HB_RANGE("hb_restrict_f32");
     return transfer<float>(ctx, n_fine, coarse, fine, mask, false);
 }
 

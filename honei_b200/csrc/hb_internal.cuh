@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 #include <string>
 #include <mutex>
@@ -49,6 +50,17 @@ struct hb_context {
     int cg_resident = 1;
     std::string last_error;
 };
+
+// An NVTX range around each compute entry point (named after it), for nsys / ncu
+// (--nvtx --nvtx-include "hb_cg_f64/").  NVTX v3 is header-only: without a tool attached a
+// push / pop is a check of one function pointer.
+struct HbRange {
+    explicit HbRange(const char *name) { nvtxRangePushA(name); }
+    ~HbRange() { nvtxRangePop(); }
+    HbRange(const HbRange &) = delete;
+    HbRange &operator=(const HbRange &) = delete;
+};
+#define HB_RANGE(name) HbRange hb_range_guard_(name)
 
 void hb_note_error(hb_context *ctx, cudaError_t e, const char *what);
 int hb_ensure_work(hb_context *ctx, size_t bytes);

@@ -151,16 +151,19 @@ int hb_ell_file_info(const char *path, int64_t *info)
 
 int hb_ell_read_file_f64(hb_context *ctx, const char *path, hb_ell *out)
 {
+    HB_RANGE("hb_ell_read_file_f64");
     return read_impl<double>(ctx, path, out, HB_F64);
 }
 
 int hb_ell_read_file_f32(hb_context *ctx, const char *path, hb_ell *out)
 {
+    HB_RANGE("hb_ell_read_file_f32");
     return read_impl<float>(ctx, path, out, HB_F32);
 }
 
 int hb_ell_write_file(hb_context *ctx, const hb_ell *A, const char *path)
 {
+    HB_RANGE("hb_ell_write_file");
     if (!ctx || !A || !path) return HB_ERR_INVALID;
     int st = hb_check_ell(A, HB_F64);
     if (st) return st;

@@ -593,12 +593,14 @@ extern "C" {
 int hb_mg_create(hb_context *ctx, int nlevels, const hb_ell *A, const hb_ell *prol, const hb_ell *res,
                  const hb_mg_params *params, hb_mg **out)
 {
+    HB_RANGE("hb_mg_create");
     return mg_create_impl(ctx, nlevels, A, prol, res, nullptr, params, out);
 }
 
 int hb_mg_create_banded(hb_context *ctx, int nlevels, const hb_ell *A, const hb_q1band *B, const hb_mg_params *params,
                         hb_mg **out)
 {
+    HB_RANGE("hb_mg_create_banded");
     if (!B) return HB_ERR_INVALID;
     return mg_create_impl(ctx, nlevels, A, nullptr, nullptr, B, params, out);
 }
@@ -626,6 +628,7 @@ int hb_mg_set_params(hb_mg *mg, const hb_mg_params *params)
 
 int hb_mg_solve_f64(hb_mg *mg, const double *b, double *x, int64_t *used_cycles, double *rnorm_host)
 {
+    HB_RANGE("hb_mg_solve_f64");
     if (!mg || !b || !x) return HB_ERR_INVALID;
     if (mg->dtype != HB_F64) return HB_ERR_INVALID;
     return mg_solve<double>(mg, b, x, used_cycles, rnorm_host);
@@ -633,6 +636,7 @@ int hb_mg_solve_f64(hb_mg *mg, const double *b, double *x, int64_t *used_cycles,
 
 int hb_mg_solve_f32(hb_mg *mg, const float *b, float *x, int64_t *used_cycles, float *rnorm_host)
 {
+    HB_RANGE("hb_mg_solve_f32");
     if (!mg || !b || !x) return HB_ERR_INVALID;
     if (mg->dtype != HB_F32) return HB_ERR_INVALID;
     return mg_solve<float>(mg, b, x, used_cycles, rnorm_host);
@@ -642,6 +646,7 @@ int hb_mg_solve_f32(hb_mg *mg, const float *b, float *x, int64_t *used_cycles, f
 int hb_ir_mg_solve(hb_context *ctx, const hb_ell *A64, hb_mg *mg32, const double *b, double *x, double eps,
                    int64_t max_iters, int warm_start, int64_t *used_outer, double *rnorm_host)
 {
+    HB_RANGE("hb_ir_mg_solve");
     if (!ctx || !A64 || !mg32 || !b || !x || max_iters < 0) return HB_ERR_INVALID;
     HB_TRY(hb_check_ell(A64, HB_F64));
     if (mg32->dtype != HB_F32) return HB_ERR_INVALID;
@@ -692,6 +697,7 @@ int hb_ir_cg_solve(hb_context *ctx, const hb_ell *A64, const hb_ell *A32, const 
                    float inner_eps, int64_t inner_max_iters, int64_t max_iters, int64_t *used_outer,
                    int64_t *inner_total, double *rnorm_host)
 {
+    HB_RANGE("hb_ir_cg_solve");
     if (!ctx || !A64 || !A32 || !b || !x || max_iters < 0 || inner_max_iters < 0) return HB_ERR_INVALID;
     HB_TRY(hb_check_ell(A64, HB_F64));
     HB_TRY(hb_check_ell(A32, HB_F32));

@@ -355,24 +355,28 @@ extern "C" {
 int hb_cg_var_diag_f64(hb_context *ctx, const hb_ell *A, const double *P, const double *b, double *x,
                        int64_t max_iters, double eps, int64_t *used_iters, double *final_defect)
 {
+    HB_RANGE("hb_cg_var_diag_f64");
     return pcg_impl<double>(ctx, A, P, nullptr, b, x, max_iters, eps, used_iters, final_defect, HB_F64);
 }
 
 int hb_cg_var_diag_f32(hb_context *ctx, const hb_ell *A, const float *P, const float *b, float *x,
                        int64_t max_iters, float eps, int64_t *used_iters, float *final_defect)
 {
+    HB_RANGE("hb_cg_var_diag_f32");
     return pcg_impl<float>(ctx, A, P, nullptr, b, x, max_iters, eps, used_iters, final_defect, HB_F32);
 }
 
 int hb_cg_var_ell_f64(hb_context *ctx, const hb_ell *A, const hb_ell *P, const double *b, double *x,
                       int64_t max_iters, double eps, int64_t *used_iters, double *final_defect)
 {
+    HB_RANGE("hb_cg_var_ell_f64");
     return pcg_impl<double>(ctx, A, nullptr, P, b, x, max_iters, eps, used_iters, final_defect, HB_F64);
 }
 
 int hb_cg_var_ell_f32(hb_context *ctx, const hb_ell *A, const hb_ell *P, const float *b, float *x,
                       int64_t max_iters, float eps, int64_t *used_iters, float *final_defect)
 {
+    HB_RANGE("hb_cg_var_ell_f32");
     return pcg_impl<float>(ctx, A, nullptr, P, b, x, max_iters, eps, used_iters, final_defect, HB_F32);
 }
 

@@ -461,6 +461,7 @@ extern "C" {
 
 int hb_q1_create(hb_context *ctx, int64_t M, const double *coef, hb_q1 **out)
 {
+    HB_RANGE("hb_q1_create");
     if (!ctx || !out || M < 2) return HB_ERR_INVALID;
     if (M * M > INT32_MAX) return HB_ERR_UNSUPPORTED;
     *out = nullptr;
@@ -570,6 +571,7 @@ int hb_q1_set_fused_tail(hb_q1 *q, int64_t max_rows)
 int hb_q1_solve(hb_q1 *q, const double *b, double *x, double eps, double inner_eps, int64_t max_outer,
                 int64_t max_inner, hb_batch_result *info)
 {
+    HB_RANGE("hb_q1_solve");
     if (!q || !b || !x || max_outer < 0 || max_inner < 0) return HB_ERR_INVALID;
     hb_context *ctx = q->ctx;
     const hb_ell &A = q->A64[q->L - 1];

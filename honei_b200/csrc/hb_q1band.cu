@@ -275,21 +275,25 @@ int64_t hb_q1band_root(int64_t n) { return n > 0 ? q1band_root(n) : 0; }
 
 int hb_q1band_spmv_f64(hb_context *ctx, const hb_q1band *A, const double *x, double *y)
 {
+    HB_RANGE("hb_q1band_spmv_f64");
     return q1band_apply<double>(ctx, A, nullptr, x, y, 0, HB_F64);
 }
 
 int hb_q1band_spmv_f32(hb_context *ctx, const hb_q1band *A, const float *x, float *y)
 {
+    HB_RANGE("hb_q1band_spmv_f32");
     return q1band_apply<float>(ctx, A, nullptr, x, y, 0, HB_F32);
 }
 
 int hb_q1band_defect_f64(hb_context *ctx, const hb_q1band *A, const double *b, const double *x, double *r)
 {
+    HB_RANGE("hb_q1band_defect_f64");
     return q1band_apply<double>(ctx, A, b, x, r, 1, HB_F64);
 }
 
 int hb_q1band_defect_f32(hb_context *ctx, const hb_q1band *A, const float *b, const float *x, float *r)
 {
+    HB_RANGE("hb_q1band_defect_f32");
     return q1band_apply<float>(ctx, A, b, x, r, 1, HB_F32);
 }
 

@@ -673,6 +673,7 @@ int hb_q1_batch_solve(hb_context *ctx, hb_q1 *const *systems, const double *cons
                       double eps, double inner_eps, int64_t max_outer, int64_t max_inner, const hb_batch_config *cfg,
                       hb_batch_result *results)
 {
+    HB_RANGE("hb_q1_batch_solve");
     if (!ctx || count < 0 || (count > 0 && (!systems || !b || !x || !results))) return HB_ERR_INVALID;
     if (max_outer < 0 || max_inner < 0) return HB_ERR_INVALID;
     if (count == 0) return HB_OK;

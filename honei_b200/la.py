@@ -162,6 +162,14 @@ class SparseMatrixELL:
                  Ax_ref.data_ptr(), Arl.data_ptr(), C.byref(out)), "hb_ell_import", ctx.handle)
         return cls(ell.rows, ell.cols, K, ld, Aj, Ax)
 
+    def validate(self, ctx: Context | None = None) -> int:
+        """Number of slots whose column is neither padding (-1) nor inside [0, cols)
+        (hb_ell_validate); 0 for every matrix the import and the assemblers build."""
+        ctx = ctx or default_context()
+        n = C.c_int64(0)
+        check(lib().hb_ell_validate(ctx.handle, C.byref(self.struct), C.byref(n)), "hb_ell_validate", ctx.handle)
+        return n.value
+
     @classmethod
     def q1_poisson(cls, M: int, coef: torch.Tensor | None = None, ctx: Context | None = None,
                    device="cuda", symmetric: bool = False) -> "SparseMatrixELL":

@@ -97,6 +97,12 @@ int hb_ell_import_f64(hb_context *ctx, int64_t rows, int64_t cols, int64_t strid
 int hb_ell_import_f32(hb_context *ctx, int64_t rows, int64_t cols, int64_t stride, int64_t ncpr,
                       int64_t threads, const uint64_t *Aj_ref, const float *Ax_ref,
                       const uint64_t *Arl_ref, hb_ell *out);
+/* Debug check of a device ELL matrix (no reference counterpart: the reference's kernels trust
+ * their indices): *bad_slots receives the number of slots whose column is neither the padding
+ * mark -1 nor inside [0, cols).  The product kernels assume 0 (hb_ell_import and the
+ * assemblers guarantee it); run this once on a matrix built by hand before using it.
+ * Synchronises ctx's stream. */
+int hb_ell_validate(hb_context *ctx, const hb_ell *A, int64_t *bad_slots);
 /* Same pattern, values cast to float (for the FP32 inner solves of mixed precision). */
 int hb_ell_cast_f64_f32(hb_context *ctx, const hb_ell *src, hb_ell *dst);
 

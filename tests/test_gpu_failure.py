@@ -59,3 +59,19 @@ def test_invalid_inputs_are_refused_before_launch(hb):
     x = torch.zeros(81, dtype=torch.float64, device="cuda")
     assert lib().hb_spmv_f64(ctx.handle, C.byref(bad), x.data_ptr(), x.data_ptr()) == 1
     assert ctx.launches() == launches
+
+
+def test_ell_validate_counts_bad_columns(hb):
+    """The debug check of a hand-built matrix: 0 for imported and assembled matrices; every slot
+    whose column is neither the padding mark nor inside [0, cols) is counted (no product runs on
+    the corrupted copy)."""
+    A = hb.SparseMatrixELL.from_reference(P.q1_poisson(33))
+    assert A.validate() == 0
+    assert hb.SparseMatrixELL.q1_poisson(65).validate() == 0
+    Aj = A.Aj.clone()
+    Aj[5] = A.columns()            # one past the end
+    Aj[17] = -2                    # below the padding mark
+    Aj[100] = 2 ** 31 - 1
+    Aj[200] = -1                   # padding: fine
+    bad = hb.SparseMatrixELL(A.rows(), A.columns(), A.K, A.ld, Aj, A.Ax)
+    assert bad.validate() == 3
