@@ -20,7 +20,7 @@
 // (ScaledSum, Scale, Sum) does on tags::CPU; the two dot products use a fixed-order tree
 // (block partials, then every block sums all partials in the same order), so each block
 // computes bit-identical scalars and takes the same branch at the stopping test.
-#include "hb_spmv_core.cuh"
+#include "hb_resident.cuh"
 
 #include <cfloat>
 #include <mutex>
@@ -355,8 +355,6 @@ int launch_cg_small(hb_context *ctx, const CGParams<T> &P, int64_t groups)
 // thread over its rows, a block tree and a tree over the block partials -- deterministic, the
 // same in every block.
 // ---------------------------------------------------------------------------------------
-constexpr int RES_THREADS = 512;
-
 template <typename T> struct ResParams {
     CGParams<T> c;
     int64_t rpb;     // rows per block
@@ -364,55 +362,8 @@ template <typename T> struct ResParams {
     hbd::CountExchange X;
 };
 
-constexpr int RES_MAX_BLOCKS = 256;
-
-// The block's partial, in thread 0: warp trees, then warp 0 sums the warp results.  One
-// __syncthreads; the red[] slots are free again because every caller passes another block-wide
-// barrier (the exchange) before the next call.
-template <typename T>
-__device__ __forceinline__ T res_partial(T v, T *red)
-{
-    v = hbd::warp_sum(v);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x < 32) v = hbd::warp_sum((int)threadIdx.x < (int)(blockDim.x >> 5) ? red[threadIdx.x] : T(0));
-    return v;
-}
-
-// The grid total of exchange e: warp 0 loads the partials (lane l: l, l + 32, ... summed in
-// order, then a warp tree) -- the same value in every block -- and broadcasts it through shared
-// memory; the other warps' loads (the halo) go out between res_total_load and res_total_sum.
-// Reading the partials in one warp per block keeps the L2 lines that hold them from being
-// hammered by every warp of the grid at once.
-template <typename T>
-__device__ __forceinline__ void res_total_load(const T *slots, unsigned e, unsigned G, T (&pv)[RES_MAX_BLOCKS / 32])
-{
-    const int lane = threadIdx.x & 31;
-    if (threadIdx.x < 32) {
-#pragma unroll
-        for (int i = 0; i < RES_MAX_BLOCKS / 32; ++i)
-            pv[i] = (lane + 32 * i < (int)G) ? __ldcg(slots + (e & 1u) * G + lane + 32 * i) : T(0);
-    }
-}
-// Ends in a __syncthreads (which also orders the halo's shared-memory writes before phase 1).
-template <typename T>
-__device__ __forceinline__ T res_total_sum(unsigned G, const T (&pv)[RES_MAX_BLOCKS / 32], T *bcast)
-{
-    const int lane = threadIdx.x & 31;
-    if (threadIdx.x < 32) {
-        T v = T(0);
-#pragma unroll
-        for (int i = 0; i < RES_MAX_BLOCKS / 32; ++i)
-            if (lane + 32 * i < (int)G) v = hbd::add(v, pv[i]);
-        v = hbd::warp_sum(v);
-        if (lane == 0) *bcast = v;
-    }
-    __syncthreads();
-    return *bcast;
-}
-
 template <typename T, int KT>
-__global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<T> Q)
+__global__ void __launch_bounds__(hbr::RES_THREADS, 1) cg_res_kernel(const ResParams<T> Q)
 {
     using hbd::add; using hbd::mul; using hbd::sub;
     extern __shared__ __align__(16) unsigned char res_smem[];
@@ -423,49 +374,15 @@ __global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<
     const int K = KT > 0 ? KT : P.K;
     const int64_t rpb = Q.rpb, wcap = Q.wcap;
     const unsigned G = gridDim.x;
-    const int64_t lo = (int64_t)blockIdx.x * rpb;
-    const int64_t hi = min(P.rows, lo + rpb);
-    const int nr = hi > lo ? (int)(hi - lo) : 0;
     T *Ax_s = (T *)res_smem;                    // [K][rpb]
     T *r_w = Ax_s + (int64_t)K * rpb;           // [wcap]
     T *p_w = r_w + wcap;                        // [wcap]
     T *x_s = p_w + wcap;                        // [rpb]
     T *v_s = x_s + rpb;                         // [rpb]
-    int32_t *Aj_s = (int32_t *)(v_s + rpb);     // [K][rpb]: window offset, -1 padding, -(j + 2) outside
-
-    // column span of the block's rows (own rows included)
-    if (threadIdx.x == 0) { s_min = INT_MAX; s_max = -1; }
-    __syncthreads();
-    {
-        int cmin = INT_MAX, cmax = -1;
-        for (int64_t q = threadIdx.x; q < (int64_t)K * nr; q += blockDim.x) {
-            const int k = (int)(q / nr), il = (int)(q - (int64_t)k * nr);
-            const int32_t j = P.Aj[(int64_t)k * P.ld + lo + il];
-            if (j >= 0) { cmin = min(cmin, (int)j); cmax = max(cmax, (int)j); }
-        }
-        if (nr > 0) { cmin = min(cmin, (int)lo); cmax = max(cmax, (int)(hi - 1)); }
-        atomicMin(&s_min, cmin);
-        atomicMax(&s_max, cmax);
-    }
-    __syncthreads();
-    int64_t wlo = 0, W = 0;
-    if (nr > 0) {
-        if ((int64_t)s_max - s_min + 1 <= wcap) { wlo = s_min; W = (int64_t)s_max - s_min + 1; }
-        else {
-            wlo = lo - (wcap - nr) / 2;
-            if (wlo < 0) wlo = 0;
-            W = wcap < P.rows - wlo ? wcap : P.rows - wlo;
-        }
-    }
-    const int64_t own = lo - wlo;    // window offset of the block's first row
-    for (int64_t q = threadIdx.x; q < (int64_t)K * nr; q += blockDim.x) {
-        const int k = (int)(q / nr), il = (int)(q - (int64_t)k * nr);
-        const int64_t gi = (int64_t)k * P.ld + lo + il;
-        const int32_t j = P.Aj[gi];
-        Ax_s[(int64_t)k * rpb + il] = P.Ax[gi];
-        Aj_s[(int64_t)k * rpb + il] = j < 0 ? -1 : ((j >= wlo && j < wlo + W) ? (int32_t)(j - wlo) : -(j + 2));
-    }
-    __syncthreads();
+    int32_t *Aj_s = (int32_t *)(v_s + rpb);     // [K][rpb]
+    const hbr::ResWindow win = hbr::res_stage<T, KT>(P.Aj, P.Ax, P.ld, P.K, P.rows, rpb, wcap, Ax_s, Aj_s, &s_min, &s_max);
+    const int64_t lo = win.lo, wlo = win.wlo, W = win.W, own = win.own();
+    const int nr = win.nr;
 
     // r = b - A x (Defect), alpha = r.r
     T acc = T(0);
@@ -475,8 +392,7 @@ __global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<
         for (int k = 0; k < K; ++k) {
             const int32_t c = Aj_s[(int64_t)k * rpb + il];
             if (c == -1) continue;
-            const int64_t j = c >= 0 ? (int64_t)c + wlo : -(int64_t)c - 2;
-            s = add(s, mul(Ax_s[(int64_t)k * rpb + il], P.x_user[j]));
+            s = add(s, mul(Ax_s[(int64_t)k * rpb + il], P.x_user[hbr::res_column(c, wlo)]));
         }
         const T r = sub(P.b_user[lo + il], s);
         r_w[own + il] = r;
@@ -484,29 +400,16 @@ __global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<
         __stcg(P.r + lo + il, r);
         acc = add(acc, mul(r, r));
     }
-    acc = res_partial(acc, red);
+    acc = hbr::res_partial(acc, red);
     unsigned e = 0;
     if (threadIdx.x == 0) __stcg(P.partials + (e & 1u) * G + blockIdx.x, acc);
     bool ok = Q.X.arrive_synced(e, G, &s_flag);
-    // the window's other rows of r (halo), loaded beside the partials
-    const int64_t n_left = nr > 0 ? own : 0, n_halo = nr > 0 ? own + (wlo + W - hi) : 0;
-    auto halo = [&]() {
-        for (int64_t q = threadIdx.x; q < n_halo; q += 2 * (int64_t)blockDim.x) {
-            const int64_t q2 = q + blockDim.x;
-            const int64_t w1 = q < n_left ? q : q - n_left + (hi - wlo);
-            const int64_t w2 = q2 < n_left ? q2 : q2 - n_left + (hi - wlo);
-            const T a = __ldcg(P.r + wlo + w1);
-            const T b = q2 < n_halo ? __ldcg(P.r + wlo + w2) : T(0);
-            r_w[w1] = a;
-            if (q2 < n_halo) r_w[w2] = b;
-        }
-    };
-    T pv[RES_MAX_BLOCKS / 32];
+    T pv[hbr::RES_MAX_BLOCKS / 32];
     T alpha = T(0);
     if (ok) {
-        res_total_load(P.partials, e, G, pv);
-        halo();
-        alpha = res_total_sum(G, pv, &bcast[0]);
+        hbr::res_total_load(P.partials + (e & 1u) * G, G, pv);
+        hbr::res_halo(P.r, r_w, win);
+        alpha = hbr::res_total_sum(G, pv, &bcast[0]);
     }
     const T initial_defect = dsqrt(alpha);
     T current_defect = T(0);
@@ -530,7 +433,7 @@ __global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<
                 if (c >= 0) {
                     pj = p_w[c];
                 } else {
-                    const int64_t j = -(int64_t)c - 2;
+                    const int64_t j = hbr::res_column(c, wlo);
                     const T rj = __ldcg(P.r + j);
                     pj = first ? rj : add(mul(__ldcg(pin + j), beta), rj);
                 }
@@ -541,12 +444,12 @@ __global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<
             __stcg(pout + lo + il, pi);
             acc = add(acc, mul(s, pi));
         }
-        acc = res_partial(acc, red);
+        acc = hbr::res_partial(acc, red);
         ++e;
         if (threadIdx.x == 0) __stcg(P.partials + (e & 1u) * G + blockIdx.x, acc);
         if (!Q.X.arrive_synced(e, G, &s_flag)) break;
-        res_total_load(P.partials, e, G, pv);
-        const T temp = res_total_sum(G, pv, &bcast[1]);
+        hbr::res_total_load(P.partials + (e & 1u) * G, G, pv);
+        const T temp = hbr::res_total_sum(G, pv, &bcast[1]);
         const T lambda = alpha / (fabs(temp) > epsm ? temp : epsm);
         const T mlambda = -lambda;
 
@@ -559,14 +462,14 @@ __global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<
             __stcg(P.r + lo + il, r);
             acc = add(acc, mul(r, r));
         }
-        acc = res_partial(acc, red);
+        acc = hbr::res_partial(acc, red);
         ++e;
         if (threadIdx.x == 0) __stcg(P.partials + (e & 1u) * G + blockIdx.x, acc);
         if (!Q.X.arrive_synced(e, G, &s_flag)) break;
-        res_total_load(P.partials, e, G, pv);
-        halo();
+        hbr::res_total_load(P.partials + (e & 1u) * G, G, pv);
+        hbr::res_halo(P.r, r_w, win);
         const T alpha_old = alpha;
-        alpha = res_total_sum(G, pv, &bcast[0]);
+        alpha = hbr::res_total_sum(G, pv, &bcast[0]);
         beta = alpha / (fabs(alpha_old) > epsm ? alpha_old : epsm);
         T *t = pin; pin = pout; pout = t;
         ++it;
@@ -584,62 +487,21 @@ __global__ void __launch_bounds__(RES_THREADS, 1) cg_res_kernel(const ResParams<
     }
 }
 
-// Shared memory of cg_res_kernel for rpb rows per block and a window of wcap entries.
-template <typename T> size_t res_smem_bytes(int K, int64_t rpb, int64_t wcap)
-{
-    return (size_t)((int64_t)K * rpb + 2 * wcap + 2 * rpb) * sizeof(T) + (size_t)K * rpb * sizeof(int32_t);
-}
-
-// Plans the resident form: one block per SM (fewer for small systems, about 128 rows each),
-// the window as large as the shared memory left over allows.  Returns false when the rows of a
-// block do not fit.
-template <typename T, int KT>
-bool res_plan(hb_context *ctx, int64_t rows, int K, int *blocks, int64_t *rpb, int64_t *wcap, size_t *smem)
-{
-    int dev = 0, optin = 0, occ = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    const size_t avail = (size_t)optin - 1024;    // static shared memory of the kernel
-    const int64_t G = std::max<int64_t>(1, std::min<int64_t>(std::min(ctx->num_sms, RES_MAX_BLOCKS), (rows + 127) / 128));
-    const int64_t r = (rows + G - 1) / G;
-    const size_t fixed = res_smem_bytes<T>(K, r, 0);
-    if (fixed + 2 * (size_t)r * sizeof(T) > avail) return false;
-    const int64_t w = std::min<int64_t>(rows, (int64_t)((avail - fixed) / (2 * sizeof(T))));
-    const size_t bytes = res_smem_bytes<T>(K, r, w);
-    if (cudaFuncSetAttribute((const void *)cg_res_kernel<T, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)bytes) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, cg_res_kernel<T, KT>, RES_THREADS, bytes) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    if ((int64_t)occ * ctx->num_sms < G) return false;
-    *blocks = (int)G;
-    *rpb = r;
-    *wcap = w;
-    *smem = bytes;
-    return true;
-}
-
 template <typename T, int KT>
 int launch_cg_res(hb_context *ctx, CGParams<T> &P, bool *launched)
 {
     *launched = false;
-    int blocks = 0;
-    int64_t rpb = 0, wcap = 0;
-    size_t smem = 0;
-    if (!res_plan<T, KT>(ctx, P.rows, P.K, &blocks, &rpb, &wcap, &smem)) return HB_OK;
+    hbr::ResPlan plan;
+    if (!hbr::res_plan<T>(ctx, P.rows, KT > 0 ? KT : P.K, 2, 2, (const void *)cg_res_kernel<T, KT>, &plan)) return HB_OK;
     ResParams<T> Q;
     Q.c = P;
-    Q.rpb = rpb;
-    Q.wcap = wcap;
+    Q.rpb = plan.rpb;
+    Q.wcap = plan.wcap;
     Q.X.count = P.bar.count;
     Q.X.status = P.bar.status;
     void *args[] = {&Q};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void *)cg_res_kernel<T, KT>, dim3(blocks), dim3(RES_THREADS),
-                                                args, smem, ctx->stream);
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *)cg_res_kernel<T, KT>, dim3(plan.blocks),
+                                                dim3(hbr::RES_THREADS), args, plan.smem, ctx->stream);
     if (e != cudaSuccess) { hb_note_error(ctx, e, "cudaLaunchCooperativeKernel(cg_res_kernel)"); return HB_ERR_CUDA; }
     *launched = true;
     return hb_check_launch(ctx, "cg_res_kernel");

@@ -17,7 +17,7 @@
 // blocks hold the same scalars and take the same branches.  Elementwise formulas round as the
 // reference's operator sequence (ScaledSum, Scale, Sum, ElementProduct); the dot products use
 // the fixed-order tree of the plain CG kernel.
-#include "hb_spmv_core.cuh"
+#include "hb_resident.cuh"
 
 #include <cfloat>
 
@@ -273,6 +273,188 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Resident-operator form for a vector (Jacobi) preconditioner, on systems whose rows fit the
+// shared memory of one block per SM (hb_resident.cuh): the block's ELL rows, x and v of its rows,
+// and r, p and the preconditioner's diagonal on its column window stay in shared memory for the
+// whole solve.  p = p * t + P r is formed redundantly on the window (bit for bit what its owner
+// forms), so only r crosses blocks, through its halo.  Per iteration two arrival-counter
+// exchanges: v.p, then (r.r, r.z) together.  The arithmetic per element is the streaming
+// kernel's; the dot products use the resident reduction tree.
+// ---------------------------------------------------------------------------------------
+template <typename T> struct PCGResParams {
+    PCGParams<T> c;
+    int64_t rpb, wcap;
+    hbd::CountExchange X;
+};
+
+template <typename T, int KT>
+__global__ void __launch_bounds__(hbr::RES_THREADS, 1) pcg_res_kernel(const PCGResParams<T> Q)
+{
+    using hbd::add; using hbd::mul; using hbd::sub;
+    extern __shared__ __align__(16) unsigned char res_smem[];
+    __shared__ T red[32];
+    __shared__ T bcast[3];
+    __shared__ int s_flag, s_min, s_max;
+    const PCGParams<T> &P = Q.c;
+    const int K = KT > 0 ? KT : P.K;
+    const int64_t rpb = Q.rpb, wcap = Q.wcap;
+    const unsigned G = gridDim.x;
+    T *Ax_s = (T *)res_smem;                    // [K][rpb]
+    T *r_w = Ax_s + (int64_t)K * rpb;           // [wcap]
+    T *p_w = r_w + wcap;                        // [wcap]
+    T *d_w = p_w + wcap;                        // [wcap] preconditioner diagonal
+    T *x_s = d_w + wcap;                        // [rpb]
+    T *v_s = x_s + rpb;                         // [rpb]
+    int32_t *Aj_s = (int32_t *)(v_s + rpb);     // [K][rpb]
+    const hbr::ResWindow win = hbr::res_stage<T, KT>(P.Aj, P.Ax, P.ld, P.K, P.rows, rpb, wcap, Ax_s, Aj_s, &s_min, &s_max);
+    const int64_t lo = win.lo, wlo = win.wlo, W = win.W, own = win.own();
+    const int nr = win.nr;
+    for (int64_t w = threadIdx.x; w < W; w += blockDim.x) d_w[w] = P.Pd[wlo + w];
+    __syncthreads();
+    auto slots = [&](unsigned e) { return P.partials + (e & 1u) * 2u * G; };
+
+    // r = b - A x (Defect); p = P r; ||r||^2 and r.p
+    T rr = T(0), rp = T(0);
+    for (int il = threadIdx.x; il < nr; il += blockDim.x) {
+        T s = T(0);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int32_t c = Aj_s[(int64_t)k * rpb + il];
+            if (c == -1) continue;
+            s = add(s, mul(Ax_s[(int64_t)k * rpb + il], P.x_user[hbr::res_column(c, wlo)]));
+        }
+        const T r = sub(P.b_user[lo + il], s);
+        const T z = mul(d_w[own + il], r);
+        r_w[own + il] = r;
+        x_s[il] = P.x_user[lo + il];
+        __stcg(P.r + lo + il, r);
+        __stcg(P.p0 + lo + il, z);
+        rr = add(rr, mul(r, r));
+        rp = add(rp, mul(r, z));
+    }
+    rr = hbr::res_partial(rr, red);
+    if (threadIdx.x == 0) __stcg(slots(0) + blockIdx.x, rr);
+    __syncthreads();
+    rp = hbr::res_partial(rp, red);
+    unsigned e = 0;
+    if (threadIdx.x == 0) __stcg(slots(0) + G + blockIdx.x, rp);
+    bool ok = Q.X.arrive_synced(e, G, &s_flag);
+    T pv[hbr::RES_MAX_BLOCKS / 32], pz[hbr::RES_MAX_BLOCKS / 32];
+    T initial_defect = T(0), alpha_new = T(0);
+    if (ok) {
+        hbr::res_total_load(slots(e), G, pv);
+        hbr::res_total_load(slots(e) + G, G, pz);
+        hbr::res_halo(P.r, r_w, win);
+        initial_defect = dsqrt(hbr::res_total_sum(G, pv, &bcast[0]));
+        alpha_new = hbr::res_total_sum(G, pz, &bcast[1]);
+        for (int64_t w = threadIdx.x; w < W; w += blockDim.x) p_w[w] = mul(d_w[w], r_w[w]);
+        __syncthreads();
+    }
+    T current_defect = T(0);
+    T talpha = T(0);
+    T *pin = P.p0, *pout = P.p1;
+    int64_t it = 0, used = 0;
+    while (ok && it < P.max_iters) {
+        // ---- phase 1: p = p * talpha + P r on the window (after the first iteration), v = A p, v.p
+        const bool first = (it == 0);
+        if (!first) {
+            for (int64_t w = threadIdx.x; w < W; w += blockDim.x) p_w[w] = add(mul(p_w[w], talpha), mul(d_w[w], r_w[w]));
+            __syncthreads();
+        }
+        T acc = T(0);
+        for (int il = threadIdx.x; il < nr; il += blockDim.x) {
+            T s = T(0);
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const int32_t c = Aj_s[(int64_t)k * rpb + il];
+                if (c == -1) continue;
+                T pj;
+                if (c >= 0) {
+                    pj = p_w[c];
+                } else {
+                    const int64_t j = hbr::res_column(c, wlo);
+                    pj = __ldcg(pin + j);
+                    if (!first) pj = add(mul(pj, talpha), mul(__ldcg(P.Pd + j), __ldcg(P.r + j)));
+                }
+                s = add(s, mul(Ax_s[(int64_t)k * rpb + il], pj));
+            }
+            v_s[il] = s;
+            const T pi = p_w[own + il];
+            __stcg(pout + lo + il, pi);
+            acc = add(acc, mul(s, pi));
+        }
+        acc = hbr::res_partial(acc, red);
+        ++e;
+        if (threadIdx.x == 0) __stcg(slots(e) + blockIdx.x, acc);
+        if (!Q.X.arrive_synced(e, G, &s_flag)) break;
+        hbr::res_total_load(slots(e), G, pv);
+        const T temp = hbr::res_total_sum(G, pv, &bcast[2]);
+        const T lambda = alpha_new / guard(temp);
+        const T mlambda = -lambda;
+
+        // ---- phase 2: x += p lambda; r += v (-lambda); r.r and r.z (z = P r)
+        rr = T(0);
+        T rz = T(0);
+        for (int il = threadIdx.x; il < nr; il += blockDim.x) {
+            x_s[il] = add(x_s[il], mul(p_w[own + il], lambda));
+            const T r = add(r_w[own + il], mul(v_s[il], mlambda));
+            r_w[own + il] = r;
+            __stcg(P.r + lo + il, r);
+            rr = add(rr, mul(r, r));
+            rz = add(rz, mul(r, mul(d_w[own + il], r)));
+        }
+        rr = hbr::res_partial(rr, red);
+        ++e;
+        if (threadIdx.x == 0) __stcg(slots(e) + blockIdx.x, rr);
+        __syncthreads();
+        rz = hbr::res_partial(rz, red);
+        if (threadIdx.x == 0) __stcg(slots(e) + G + blockIdx.x, rz);
+        if (!Q.X.arrive_synced(e, G, &s_flag)) break;
+        hbr::res_total_load(slots(e), G, pv);
+        hbr::res_total_load(slots(e) + G, G, pz);
+        hbr::res_halo(P.r, r_w, win);
+        ++it;
+        current_defect = dsqrt(hbr::res_total_sum(G, pv, &bcast[0]));
+        const T rz_total = hbr::res_total_sum(G, pz, &bcast[1]);
+        if (current_defect < P.eps * initial_defect) { used = it; break; }
+        if (current_defect < P.eps) { used = it; break; }
+        if (it == P.max_iters) { used = it; break; }
+        const T alpha = alpha_new;
+        alpha_new = rz_total;
+        talpha = alpha_new / guard(alpha);
+        T *t = pin; pin = pout; pout = t;
+    }
+    for (int il = threadIdx.x; il < nr; il += blockDim.x) P.x_user[lo + il] = x_s[il];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        P.res->used = used;
+        P.res->defect0 = (double)initial_defect;
+        P.res->defect = (double)current_defect;
+        P.res->status = *(volatile int *)Q.X.status;
+    }
+}
+
+template <typename T, int KT>
+int launch_pcg_res(hb_context *ctx, PCGParams<T> &P, bool *launched)
+{
+    *launched = false;
+    hbr::ResPlan plan;
+    if (!hbr::res_plan<T>(ctx, P.rows, KT > 0 ? KT : P.K, 3, 2, (const void *)pcg_res_kernel<T, KT>, &plan))
+        return HB_OK;
+    PCGResParams<T> Q;
+    Q.c = P;
+    Q.rpb = plan.rpb;
+    Q.wcap = plan.wcap;
+    Q.X.count = P.bar.count;
+    Q.X.status = P.bar.status;
+    void *args[] = {&Q};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *)pcg_res_kernel<T, KT>, dim3(plan.blocks),
+                                                dim3(hbr::RES_THREADS), args, plan.smem, ctx->stream);
+    if (e != cudaSuccess) { hb_note_error(ctx, e, "cudaLaunchCooperativeKernel(pcg_res_kernel)"); return HB_ERR_CUDA; }
+    *launched = true;
+    return hb_check_launch(ctx, "pcg_res_kernel");
+}
+
 template <typename T, int KT, bool PMAT>
 int launch_pcg(hb_context *ctx, PCGParams<T> &P, int64_t groups)
 {
@@ -335,7 +517,11 @@ int pcg_impl(hb_context *ctx, const hb_ell *A, const T *Pd, const hb_ell *Pm, co
     HB_CUDA_TRY(ctx, cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), ctx->stream));
     const int64_t groups = ld / 4;
     const bool k9 = (A->K == 9);
-    if (Pd) st = k9 ? launch_pcg<T, 9, false>(ctx, P, groups) : launch_pcg<T, 0, false>(ctx, P, groups);
+    if (Pd && ctx->cg_resident && groups > 0) {
+        bool launched = false;
+        st = k9 ? launch_pcg_res<T, 9>(ctx, P, &launched) : launch_pcg_res<T, 0>(ctx, P, &launched);
+        if (!st && !launched) st = k9 ? launch_pcg<T, 9, false>(ctx, P, groups) : launch_pcg<T, 0, false>(ctx, P, groups);
+    } else if (Pd) st = k9 ? launch_pcg<T, 9, false>(ctx, P, groups) : launch_pcg<T, 0, false>(ctx, P, groups);
     else st = k9 ? launch_pcg<T, 9, true>(ctx, P, groups) : launch_pcg<T, 0, true>(ctx, P, groups);
     if (st) return st;
     hb_solve_result *h = (hb_solve_result *)ctx->pinned;

@@ -595,8 +595,9 @@ class CGSolver:
 
     @staticmethod
     def set_resident(enable: bool, ctx: Context | None = None) -> bool:
-        """Whether CG on ctx uses the resident-operator kernel where the system fits (the
-        default) or always the streaming kernel; returns the previous setting."""
+        """Whether CG (and CGSolverVAR with a vector preconditioner) on ctx uses the
+        resident-operator kernel where the system fits (the default) or always the streaming
+        kernel; returns the previous setting."""
         ctx = ctx or default_context()
         return bool(lib().hb_cg_set_resident(ctx.handle, 1 if enable else 0))
 

@@ -290,8 +290,9 @@ int hb_cg_f64(hb_context *ctx, const hb_ell *A, const double *b, double *x, int6
 int hb_cg_f32(hb_context *ctx, const hb_ell *A, const float *b, float *x, int64_t max_iters,
               float eps, int64_t *used_iters, float *final_defect);
 
-/* Selects whether hb_cg_f64 / hb_cg_f32 on this context use the resident-operator kernel
- * where it applies (enable != 0, the default) or always the streaming kernel.  Both give
+/* Selects whether hb_cg_f64 / hb_cg_f32 and hb_cg_var_diag_f64 / _f32 on this context use the
+ * resident-operator kernels where they apply (enable != 0, the default) or always the
+ * streaming kernels.  Both give
  * results within rounding of each other (their dot products use different summation trees);
  * each is deterministic.  Returns the previous setting. */
 int hb_cg_set_resident(hb_context *ctx, int enable);

@@ -84,15 +84,47 @@ def test_jacobi_random_q1_parity(hb, oracle, M, dt, eps):
 
 def test_vector_and_diagonal_matrix_preconditioner_agree_bitwise(hb, oracle):
     """The same Jacobi preconditioner as a vector and as a diagonal ELL matrix: z = P r rounds
-    identically (0 + P r), so both kernels produce the same iterates bit for bit."""
+    identically (0 + P r), so the two streaming kernels produce the same iterates bit for bit
+    (the vector case forced off the resident kernel, whose reduction tree differs)."""
     M = 65
     A = P.q1_poisson(M, P.log_uniform_coef(M, 1e-2, 1e2, 3))
     Pd = jacobi(A)
     Pm = P.ell_from_csr(A.rows, A.rows, np.arange(A.rows + 1), np.arange(A.rows), Pd)
     b = oracle.spmv(A, P.uniform_vector(A.rows, 4))
-    x1, u1 = solve(hb, A, Pd, b, np.zeros(A.rows), 3000, 1e-8)
+    prev = hb.CGSolver.set_resident(False)
+    try:
+        x1, u1 = solve(hb, A, Pd, b, np.zeros(A.rows), 3000, 1e-8)
+    finally:
+        hb.CGSolver.set_resident(prev)
     x2, u2 = solve(hb, A, Pm, b, np.zeros(A.rows), 3000, 1e-8)
     assert u1 == u2 and np.array_equal(x1, x2)
+
+
+@pytest.mark.parametrize("name,make", [
+    ("q1_257_coef", lambda: P.q1_poisson(257, P.log_uniform_coef(257, 1e-2, 1e2, 6))),
+    ("q1_257_permuted", lambda: P.q1_poisson_permuted(257, 8)[0]),
+    ("q1_9", lambda: P.q1_poisson(9)),
+], ids=["q1_257_coef", "q1_257_permuted", "q1_9"])
+def test_resident_and_streaming_jacobi_kernels_agree(hb, oracle, name, make):
+    """With a vector preconditioner, systems that fit run in the resident-operator kernel; the
+    streaming kernel solves them to the same bar (iterations within 1, true residual within
+    1e-10) and each kernel is deterministic.  The permuted matrix takes the out-of-window
+    gathers."""
+    A = make()
+    Pd = jacobi(A)
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 3))
+    x_r, u_r = solve(hb, A, Pd, b, np.zeros(A.rows), 20000, 1e-8)
+    x_r2, u_r2 = solve(hb, A, Pd, b, np.zeros(A.rows), 20000, 1e-8)
+    assert u_r == u_r2 and np.array_equal(x_r, x_r2)
+    prev = hb.CGSolver.set_resident(False)
+    try:
+        x_s, u_s = solve(hb, A, Pd, b, np.zeros(A.rows), 20000, 1e-8)
+    finally:
+        hb.CGSolver.set_resident(prev)
+    assert abs(u_r - u_s) <= 1, (u_r, u_s)
+    assert abs(relres(oracle, A, b, x_r) - relres(oracle, A, b, x_s)) <= 1e-10
+    x_o, u_o = oracle.cg_var(A, Pd, b, max_iters=20000, eps=1e-8)
+    assert abs(u_r - u_o) <= 1, (u_r, u_o)
 
 
 def test_edge_cases(hb, oracle):
