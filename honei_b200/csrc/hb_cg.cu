@@ -10,6 +10,12 @@
 //            separate Scale+Sum passes disappear), v = A p, partial v.p
 //   phase 2  lambda = alpha / v.p;  x += lambda p;  r += (-lambda) v;  partial r.r
 //
+// Rows are dealt to threads in lane-strided quads (hbd::quad_rows: lane l of a 128-row tile
+// owns rows l, l + 32, l + 64, l + 96), so each gather instruction of a warp reads 32
+// neighbouring rows' columns -- about two cache lines instead of eight for four consecutive rows
+// per thread; with three ELL slots' loads in flight per step this took the 1025^2 iteration from
+// 45 to 32 us.  The one-block kernel for small systems deals its rows the same way, so the two
+// give bit-identical iterates.
 // The gathers of x, r and p are ordinary, L1-cacheable loads: every value they read was written
 // by another block before its release-arrival at an exchange that this block acquired (thread 0)
 // and then passed through __syncthreads, so the memory model guarantees the current value; the
@@ -81,10 +87,10 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
 
     // x (padded with zeros) from the caller's x0
     for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
-        T xv[4];
+        uint32_t row[4];
+        hbd::quad_rows(g, groups, row);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) xv[i] = (4 * g + i < rows) ? P.x_user[4 * g + i] : T(0);
-        hbd::st4(P.x + 4 * g, xv);
+        for (int i = 0; i < 4; ++i) P.x[row[i]] = (row[i] < rows) ? P.x_user[row[i]] : T(0);
     }
     ok = X.arrive_wait(T(0), P.partials, e, G, &s_flag);
 
@@ -93,15 +99,17 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
     if (ok) {
         const T *xw = P.x;
         for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
-            T s[4], rv[4];
-            hbd::ell_rows4<T, KT>(P.Aj, P.Ax, P.ld, P.K, 4 * g, [&](int32_t j) { return xw[j]; }, s);
+            uint32_t row[4];
+            hbd::quad_rows(g, groups, row);
+            T s[4];
+            hbd::ell_rows4s<T, KT, (KT > 0 ? 3 : 4)>(P.Aj, P.Ax, P.ld, P.K, row, [&](int32_t j) { return xw[j]; }, s);
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                const T bb = (4 * g + i < rows) ? P.b_user[4 * g + i] : T(0);
-                rv[i] = sub(bb, s[i]);
-                acc = add(acc, mul(rv[i], rv[i]));
+                const T bb = (row[i] < rows) ? P.b_user[row[i]] : T(0);
+                const T rv = sub(bb, s[i]);
+                acc = add(acc, mul(rv, rv));
+                P.r[row[i]] = rv;
             }
-            hbd::st4(P.r + 4 * g, rv);
         }
         acc = hbd::block_sum(acc, red);
         ok = X.arrive_wait(acc, P.partials, ++e, G, &s_flag);
@@ -119,21 +127,21 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
         const bool first = (it == 0);
         acc = T(0);
         for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+            uint32_t row[4];
+            hbd::quad_rows(g, groups, row);
             T s[4];
-            hbd::ell_rows4<T, KT>(P.Aj, P.Ax, P.ld, P.K, 4 * g, [&](int32_t j) {
+            hbd::ell_rows4s<T, KT, (KT > 0 ? 3 : 4)>(P.Aj, P.Ax, P.ld, P.K, row, [&](int32_t j) {
                 const T rj = rw[j];
                 return first ? rj : add(mul(pw[j], beta), rj);
             }, s);
-            T rv[4], pv[4], pn[4];
-            hbd::ld4(P.r + 4 * g, rv);
-            hbd::ld4(pin + 4 * g, pv);
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                pn[i] = first ? rv[i] : add(mul(pv[i], beta), rv[i]);
-                acc = add(acc, mul(s[i], pn[i]));
+                const T rv = P.r[row[i]];
+                const T pn = first ? rv : add(mul(pin[row[i]], beta), rv);
+                acc = add(acc, mul(s[i], pn));
+                pout[row[i]] = pn;
+                P.v[row[i]] = s[i];
             }
-            hbd::st4(pout + 4 * g, pn);
-            hbd::st4(P.v + 4 * g, s);
         }
         acc = hbd::block_sum(acc, red);
         if (!X.arrive_wait(acc, P.partials, ++e, G, &s_flag)) break;
@@ -144,19 +152,24 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
         // ---- phase 2: x += lambda p; r += (-lambda) v; alpha = r.r
         acc = T(0);
         for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+            uint32_t row[4];
+            hbd::quad_rows(g, groups, row);
             T xv[4], pv[4], rv[4], vv[4];
-            hbd::ld4(P.x + 4 * g, xv);
-            hbd::ld4(pout + 4 * g, pv);
-            hbd::ld4(P.r + 4 * g, rv);
-            hbd::ld4(P.v + 4 * g, vv);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                xv[i] = P.x[row[i]];
+                pv[i] = pout[row[i]];
+                rv[i] = P.r[row[i]];
+                vv[i] = P.v[row[i]];
+            }
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 xv[i] = add(xv[i], mul(lambda, pv[i]));
                 rv[i] = add(rv[i], mul(mlambda, vv[i]));
                 acc = add(acc, mul(rv[i], rv[i]));
+                P.x[row[i]] = xv[i];
+                P.r[row[i]] = rv[i];
             }
-            hbd::st4(P.x + 4 * g, xv);
-            hbd::st4(P.r + 4 * g, rv);
         }
         acc = hbd::block_sum(acc, red);
         if (!X.arrive_wait(acc, P.partials, ++e, G, &s_flag)) break;
@@ -171,10 +184,13 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
         if (it == P.max_iters) used = it;
     }
     // x back to the caller (own rows)
-    for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x)
+    for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+        uint32_t row[4];
+        hbd::quad_rows(g, groups, row);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-            if (4 * g + i < rows) P.x_user[4 * g + i] = P.x[4 * g + i];
+            if (row[i] < rows) P.x_user[row[i]] = P.x[row[i]];
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         P.res->used = used;
         P.res->defect0 = (double)initial_defect;
@@ -227,7 +243,9 @@ __global__ void __launch_bounds__(SMALL_GROUPS) cg_small_kernel(CGParams<T> P)
     const int64_t groups = P.ld / 4;
     const int64_t g = threadIdx.x;
     const bool own = g < groups;
-    const int64_t r0 = 4 * g;
+    // the rows of this thread's quad, lane-strided exactly as in cg_kernel
+    uint32_t row[4] = {0, 0, 0, 0};
+    if (own) hbd::quad_rows(g, groups, row);
 
     int32_t aj[KR][4];
     T ax[KR][4];
@@ -235,8 +253,11 @@ __global__ void __launch_bounds__(SMALL_GROUPS) cg_small_kernel(CGParams<T> P)
 #pragma unroll
         for (int k = 0; k < KR; ++k) {
             if (own) {
-                hbd::ld4_stream(P.Aj + (int64_t)k * P.ld + r0, aj[k]);
-                hbd::ld4_stream(P.Ax + (int64_t)k * P.ld + r0, ax[k]);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    aj[k][i] = __ldcs(P.Aj + (int64_t)k * P.ld + row[i]);
+                    ax[k][i] = __ldcs(P.Ax + (int64_t)k * P.ld + row[i]);
+                }
             } else {
 #pragma unroll
                 for (int i = 0; i < 4; ++i) { aj[k][i] = -1; ax[k][i] = T(0); }
@@ -258,8 +279,8 @@ __global__ void __launch_bounds__(SMALL_GROUPS) cg_small_kernel(CGParams<T> P)
             for (int k = 0; k < P.K; ++k)
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
-                    const int32_t j = __ldg(P.Aj + (int64_t)k * P.ld + r0 + i);
-                    if (j >= 0) s[i] = add(s[i], mul(__ldg(P.Ax + (int64_t)k * P.ld + r0 + i), sp[j]));
+                    const int32_t j = __ldg(P.Aj + (int64_t)k * P.ld + row[i]);
+                    if (j >= 0) s[i] = add(s[i], mul(__ldg(P.Ax + (int64_t)k * P.ld + row[i]), sp[j]));
                 }
         }
     };
@@ -267,8 +288,8 @@ __global__ void __launch_bounds__(SMALL_GROUPS) cg_small_kernel(CGParams<T> P)
     T x[4], r[4], p[4], v[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        x[i] = (own && r0 + i < rows) ? P.x_user[r0 + i] : T(0);
-        if (own) sp[r0 + i] = x[i];
+        x[i] = (own && row[i] < rows) ? P.x_user[row[i]] : T(0);
+        if (own) sp[row[i]] = x[i];
     }
     block_sync();
     // r = b - A x, alpha = r.r
@@ -276,7 +297,7 @@ __global__ void __launch_bounds__(SMALL_GROUPS) cg_small_kernel(CGParams<T> P)
     product(v);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const T bb = (own && r0 + i < rows) ? P.b_user[r0 + i] : T(0);
+        const T bb = (own && row[i] < rows) ? P.b_user[row[i]] : T(0);
         r[i] = sub(bb, v[i]);
         acc = add(acc, mul(r[i], r[i]));
         p[i] = T(0);
@@ -295,7 +316,7 @@ __global__ void __launch_bounds__(SMALL_GROUPS) cg_small_kernel(CGParams<T> P)
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             p[i] = first ? r[i] : add(mul(p[i], beta), r[i]);
-            if (own) sp[r0 + i] = p[i];
+            if (own) sp[row[i]] = p[i];
         }
         block_sync();
         product(v);
@@ -323,7 +344,7 @@ __global__ void __launch_bounds__(SMALL_GROUPS) cg_small_kernel(CGParams<T> P)
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i)
-        if (own && r0 + i < rows) P.x_user[r0 + i] = x[i];
+        if (own && row[i] < rows) P.x_user[row[i]] = x[i];
     if (threadIdx.x == 0) {
         P.res->used = used;
         P.res->defect0 = (double)initial_defect;

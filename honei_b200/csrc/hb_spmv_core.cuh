@@ -62,4 +62,47 @@ __device__ __forceinline__ void ell_rows4(const int32_t *__restrict__ Aj, const 
     }
 }
 
+
+// Lane-strided quads: quad q holds rows tile*128 + lane + w*i (i = 0..3) of its 128-row tile
+// (tile = q / 32, lane = q % 32, w = quads in that tile, 32 except in a last partial tile), so a
+// warp's 32 lanes read 32 consecutive rows per instruction.
+__device__ __forceinline__ void quad_rows(int64_t q, int64_t groups, uint32_t (&row)[4])
+{
+    const int64_t tile = q >> 5;
+    const int64_t left = groups - (tile << 5);
+    const uint32_t w = (uint32_t)(left < 32 ? left : 32);
+    const uint32_t base = (uint32_t)((tile << 7) + (q & 31));
+#pragma unroll
+    for (int i = 0; i < 4; ++i) row[i] = base + w * (uint32_t)i;
+}
+
+// ell_rows4 on the rows of a lane-strided quad: the loads of CH slots at a time (all of them for
+// CH >= KT), then their gathers, in slot order.
+template <typename T, int KT, int CH = (KT > 0 ? KT : 4), typename Gather>
+__device__ __forceinline__ void ell_rows4s(const int32_t *__restrict__ Aj, const T *__restrict__ Ax, int64_t ld,
+                                           int K, const uint32_t (&row)[4], Gather gather, T (&sum)[4])
+{
+#pragma unroll
+    for (int i = 0; i < 4; ++i) sum[i] = T(0);
+    const int kend = KT > 0 ? KT : K;
+#pragma unroll
+    for (int k0 = 0; k0 < kend; k0 += CH) {
+        int32_t j[CH][4];
+        T a[CH][4];
+#pragma unroll
+        for (int c = 0; c < CH; ++c)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const bool in = k0 + c < kend;
+                j[c][i] = in ? __ldcs(Aj + (int64_t)(k0 + c) * ld + row[i]) : -1;
+                a[c][i] = in ? __ldcs(Ax + (int64_t)(k0 + c) * ld + row[i]) : T(0);
+            }
+#pragma unroll
+        for (int c = 0; c < CH; ++c)
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (j[c][i] >= 0) sum[i] = add(sum[i], mul(a[c][i], gather(j[c][i])));
+    }
+}
+
 }  // namespace hbd
