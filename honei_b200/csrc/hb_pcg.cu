@@ -90,23 +90,23 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
     bool ok = true;
 
     // z = P r on the thread's own rows (matrix P: a gathered product of the current r)
-    auto precon4 = [&](int64_t g, const T (&rv)[4], T (&zv)[4]) {
+    auto precon4 = [&](const uint32_t (&row)[4], const T (&rv)[4], T (&zv)[4]) {
         if (PMAT) {
             const T *rw = P.r;
-            hbd::ell_rows4<T, 0>(P.Pj, P.Px, P.Pld, P.PK, 4 * g, [&](int32_t j) { return rw[j]; }, zv);
+            hbd::ell_rows4s<T, 0>(P.Pj, P.Px, P.Pld, P.PK, row, [&](int32_t j) { return rw[j]; }, zv);
         } else {
-            T pd[4];
-            hbd::ld4(P.Pd + 4 * g, pd);
 #pragma unroll
-            for (int i = 0; i < 4; ++i) zv[i] = mul(pd[i], rv[i]);
+            for (int i = 0; i < 4; ++i) zv[i] = mul(P.Pd[row[i]], rv[i]);
         }
     };
 
     for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+            uint32_t row[4];
+            hbd::quad_rows(g, groups, row);
         T xv[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) xv[i] = (4 * g + i < rows) ? P.x_user[4 * g + i] : T(0);
-        hbd::st4(P.x + 4 * g, xv);
+        for (int i = 0; i < 4; ++i) xv[i] = (row[i] < rows) ? P.x_user[row[i]] : T(0);
+        for (int i = 0; i < 4; ++i) P.x[row[i]] = xv[i];
     }
     ok = X.arrive(e++, G, &s_flag);
 
@@ -115,19 +115,21 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
     if (ok) {
         const T *xw = P.x;
         for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+            uint32_t row[4];
+            hbd::quad_rows(g, groups, row);
             T s[4], rv[4];
-            hbd::ell_rows4<T, KT, 4>(P.Aj, P.Ax, P.ld, P.K, 4 * g, [&](int32_t j) { return xw[j]; }, s);
+            hbd::ell_rows4s<T, KT, (KT > 0 ? 3 : 4)>(P.Aj, P.Ax, P.ld, P.K, row, [&](int32_t j) { return xw[j]; }, s);
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                const T bb = (4 * g + i < rows) ? P.b_user[4 * g + i] : T(0);
+                const T bb = (row[i] < rows) ? P.b_user[row[i]] : T(0);
                 rv[i] = sub(bb, s[i]);
             }
-            hbd::st4(P.r + 4 * g, rv);
+            for (int i = 0; i < 4; ++i) P.r[row[i]] = rv[i];
             if (!PMAT) {
                 // p = P r, ||r||^2, r.p
                 T pv[4];
-                precon4(g, rv, pv);
-                hbd::st4(P.p0 + 4 * g, pv);
+                precon4(row, rv, pv);
+                for (int i = 0; i < 4; ++i) P.p0[row[i]] = pv[i];
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     rr = add(rr, mul(rv[i], rv[i]));
@@ -140,10 +142,12 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
     if (PMAT && ok) {
         // p = P r needs every row of r
         for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+            uint32_t row[4];
+            hbd::quad_rows(g, groups, row);
             T rv[4], pv[4];
-            hbd::ld4(P.r + 4 * g, rv);
-            precon4(g, rv, pv);
-            hbd::st4(P.p0 + 4 * g, pv);
+            for (int i = 0; i < 4; ++i) rv[i] = P.r[row[i]];
+            precon4(row, rv, pv);
+            for (int i = 0; i < 4; ++i) P.p0[row[i]] = pv[i];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 rr = add(rr, mul(rv[i], rv[i]));
@@ -168,34 +172,36 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
         const T *pw = pin, *rw = P.r, *zw = P.z, *dw = P.Pd;
         T acc = T(0);
         for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+            uint32_t row[4];
+            hbd::quad_rows(g, groups, row);
             T s[4];
-            hbd::ell_rows4<T, KT, 4>(P.Aj, P.Ax, P.ld, P.K, 4 * g, [&](int32_t j) {
+            hbd::ell_rows4s<T, KT, (KT > 0 ? 3 : 4)>(P.Aj, P.Ax, P.ld, P.K, row, [&](int32_t j) {
                 const T pj = pw[j];
                 if (first) return pj;
                 const T zj = PMAT ? zw[j] : mul(dw[j], rw[j]);
                 return add(mul(pj, talpha), zj);
             }, s);
             T pv[4], pn[4];
-            hbd::ld4(pin + 4 * g, pv);
+            for (int i = 0; i < 4; ++i) pv[i] = pin[row[i]];
             if (first) {
 #pragma unroll
                 for (int i = 0; i < 4; ++i) pn[i] = pv[i];
             } else {
                 T zv[4];
                 if (PMAT) {
-                    hbd::ld4(P.z + 4 * g, zv);
+                    for (int i = 0; i < 4; ++i) zv[i] = P.z[row[i]];
                 } else {
                     T rv[4];
-                    hbd::ld4(P.r + 4 * g, rv);
-                    precon4(g, rv, zv);
+                    for (int i = 0; i < 4; ++i) rv[i] = P.r[row[i]];
+                    precon4(row, rv, zv);
                 }
 #pragma unroll
                 for (int i = 0; i < 4; ++i) pn[i] = add(mul(pv[i], talpha), zv[i]);
             }
 #pragma unroll
             for (int i = 0; i < 4; ++i) acc = add(acc, mul(s[i], pn[i]));
-            hbd::st4(pout + 4 * g, pn);
-            hbd::st4(P.v + 4 * g, s);
+            for (int i = 0; i < 4; ++i) pout[row[i]] = pn[i];
+            for (int i = 0; i < 4; ++i) P.v[row[i]] = s[i];
         }
         acc = hbd::block_sum(acc, red);
         if (threadIdx.x == 0) slotA[blockIdx.x] = acc;
@@ -208,22 +214,24 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
         rr = T(0);
         T rz = T(0);
         for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+            uint32_t row[4];
+            hbd::quad_rows(g, groups, row);
             T xv[4], pv[4], rv[4], vv[4];
-            hbd::ld4(P.x + 4 * g, xv);
-            hbd::ld4(pout + 4 * g, pv);
-            hbd::ld4(P.r + 4 * g, rv);
-            hbd::ld4(P.v + 4 * g, vv);
+            for (int i = 0; i < 4; ++i) xv[i] = P.x[row[i]];
+            for (int i = 0; i < 4; ++i) pv[i] = pout[row[i]];
+            for (int i = 0; i < 4; ++i) rv[i] = P.r[row[i]];
+            for (int i = 0; i < 4; ++i) vv[i] = P.v[row[i]];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 xv[i] = add(xv[i], mul(pv[i], lambda));
                 rv[i] = add(rv[i], mul(vv[i], mlambda));
                 rr = add(rr, mul(rv[i], rv[i]));
             }
-            hbd::st4(P.x + 4 * g, xv);
-            hbd::st4(P.r + 4 * g, rv);
+            for (int i = 0; i < 4; ++i) P.x[row[i]] = xv[i];
+            for (int i = 0; i < 4; ++i) P.r[row[i]] = rv[i];
             if (!PMAT) {
                 T zv[4];
-                precon4(g, rv, zv);
+                precon4(row, rv, zv);
 #pragma unroll
                 for (int i = 0; i < 4; ++i) rz = add(rz, mul(rv[i], zv[i]));
             }
@@ -245,10 +253,12 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
         if (PMAT) {
             rz = T(0);
             for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+            uint32_t row[4];
+            hbd::quad_rows(g, groups, row);
                 T rv[4], zv[4];
-                hbd::ld4(P.r + 4 * g, rv);
-                precon4(g, rv, zv);
-                hbd::st4(P.z + 4 * g, zv);
+                for (int i = 0; i < 4; ++i) rv[i] = P.r[row[i]];
+                precon4(row, rv, zv);
+                for (int i = 0; i < 4; ++i) P.z[row[i]] = zv[i];
 #pragma unroll
                 for (int i = 0; i < 4; ++i) rz = add(rz, mul(rv[i], zv[i]));
             }
@@ -261,10 +271,13 @@ __global__ void __launch_bounds__(PCG_THREADS) pcg_var_kernel(PCGParams<T> P)
         talpha = alpha_new / guard(alpha);
         T *t = pin; pin = pout; pout = t;
     }
-    for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x)
+    for (int64_t g = g_lo + threadIdx.x; g < g_hi; g += blockDim.x) {
+        uint32_t row[4];
+        hbd::quad_rows(g, groups, row);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-            if (4 * g + i < rows) P.x_user[4 * g + i] = P.x[4 * g + i];
+            if (row[i] < rows) P.x_user[row[i]] = P.x[row[i]];
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         P.res->used = used;
         P.res->defect0 = (double)initial_defect;
