@@ -255,6 +255,56 @@ def bench_batch(la, ctx, n_systems=512, seed=2024):
     return out
 
 
+def bench_cg_large(la, ctx, sizes=(1025, 2049), cpu=True, cpu_iters=10):
+    """Plain FP64 CG (config 2's CG) on the Q1 Poisson grids of 1025^2 and 2049^2: b = A x_true
+    with x_true ~ U[-1, 1], x0 = 0, 1e-8 relative; the streaming persistent kernel.  Algorithmic
+    bytes per iteration nnz*(8 + 4) + 10*n*8 (the matrix once, the vectors of both phases).  With
+    the compiled reference present, its MultiCore::SSE CGSolver on the host cores over a bounded
+    sample of cpu_iters iterations of the same system (seconds per iteration)."""
+    import torch
+    from honei_b200 import problems as P
+    peak, _ = measured_peak()
+    out = {}
+    for M in sizes:
+        A = la.SparseMatrixELL.q1_poisson(M, ctx=ctx)
+        n = A.rows()
+        xt = torch.from_numpy(P.uniform_vector(n, 1)).cuda()
+        b = torch.empty_like(xt)
+        la.Product.value(b, A, xt, ctx=ctx)
+        x = torch.zeros_like(xt)
+        la.CGSolver.value(A, None, b, x, 20, 1e-8, ctx=ctx)          # warm-up
+        x.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        used = la.CGSolver.value(A, None, b, x, 100000, 1e-8, ctx=ctx)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        r = torch.empty_like(xt)
+        la.Defect.value(r, b, A, x, ctx=ctx)
+        nnz = int((A.Aj >= 0).sum())
+        per_it = nnz * 12 + 10 * n * 8
+        us = 1e3 * ms / max(used, 1)
+        row = {"iterations": used, "ms": round(ms, 2), "us_per_iteration": round(us, 2),
+               "bytes_per_iteration": per_it, "gbs": round(per_it / (us * 1e3), 1),
+               "frac_of_peak": round(per_it / (us * 1e3) / peak, 4),
+               "relres": float(torch.linalg.norm(r) / torch.linalg.norm(b))}
+        del A, x, r, b, xt
+        torch.cuda.empty_cache()
+        if cpu:
+            R = _ref_cpu()
+            if R is not None:
+                Ah = P.q1_poisson(M)
+                bh, _ = R.spmv(Ah, P.uniform_vector(Ah.rows, 1), tag="mc-sse")
+                _, u, sec = R.cg(Ah, bh, max_iters=cpu_iters, eps=1e-30, tag="mc-sse")
+                row["cpu_reference"] = {"s_per_iteration": round(sec / max(u, 1), 5), "sample_iterations": u,
+                                        "cores": os.cpu_count(), "tag": "tags::CPU::MultiCore::SSE"}
+                row["speedup_per_iteration_vs_cpu"] = round(sec / max(u, 1) / (us / 1e6), 1)
+        out[f"{M}"] = row
+    return {"workload": "plain FP64 CG on Q1 Poisson, 1e-8 relative, x0 = 0 (streaming kernel)", **out}
+
+
 def bench_cg_cluster(ctx, M=M_CG, n_solves=30):
     """The 257^2 plain FP64 CG solve on one thread-block cluster (batched kernel, batch of 1)."""
     import torch
@@ -698,6 +748,7 @@ def run_ours(args):
             cg_extra["speedup_vs_cpu_reference"] = round(1e3 * statistics.median(secs) / cg_extra["p50_ms"], 1)
 
     cg_cluster = bench_cg_cluster(ctx)
+    cg_large = bench_cg_large(la, ctx, cpu=(ws == 1 and not args.no_cpu_baseline)) if not args.no_mg else None
     batch_extra = None if args.no_batch else bench_batch(la, ctx, n_systems=args.batch_systems)
     # the serving sample before the multi-second 2049^2 solves (their heat lowers the clocks)
     serve_extra = None if (args.no_serve or rank != 0 and ws > 1) else bench_serve(args.serve_requests, device=local)
@@ -731,7 +782,7 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "extra": {"spmv_f32_gbs": round(gbs32, 2), "q1band_2049": band_extra, "csr_2049": csr_extra, "cg_257": cg_extra,
-                      "cg_257_cluster": cg_cluster,
+                      "cg_257_cluster": cg_cluster, "cg_large": cg_large,
                       "mg_2049": mg_extra, "ir_2049": ir_extra, "batch_512": batch_extra, "serve": serve_extra},
         }
         print(json.dumps(line), flush=True)
