@@ -46,7 +46,23 @@ struct hb_mg {
     // run as one single-cluster launch; tail_desc is its device descriptor
     int tail_level = -1, tail_top = -1;
     void *tail_desc = nullptr;
+    // one cycle of hb_mg_solve_* (V-cycle, finest defect, its squared norm) captured as a CUDA
+    // graph for the (x, b) it was captured with; replayed once per cycle
+    cudaGraphExec_t cycle_graph = nullptr;
+    const void *graph_x = nullptr, *graph_b = nullptr;
+    uint64_t graph_kernels = 0;
+    bool graph_failed = false;
 };
+
+// Drops the captured cycle (its kernels' parameters changed); waits for replays in flight.
+static void drop_cycle_graph(hb_mg *mg)
+{
+    if (!mg->cycle_graph) return;
+    cudaStreamSynchronize(mg->ctx->stream);
+    cudaGraphExecDestroy(mg->cycle_graph);
+    mg->cycle_graph = nullptr;
+    mg->graph_x = mg->graph_b = nullptr;
+}
 
 namespace {
 
@@ -191,7 +207,65 @@ template <typename T> int vcycle(hb_mg *mg, int l, T *X, const T *B)
     return smooth<T>(mg, l, X, B, mg->prm.n_post);
 }
 
+// One cycle of mg_solve as enqueued work: the V-cycle, the finest defect and its squared norm
+// into mg->norm.
+template <typename T> int solve_cycle(hb_mg *mg, T *x, const T *b)
+{
+    const int top = mg->L - 1;
+    T *r = tp<T>(mg->r);
+    HB_TRY(vcycle<T>(mg, top, x, b));
+    HB_TRY(level_mode<T>(mg, top, HB_MODE_DEFECT, x, b, nullptr, r));
+    return hb_launch_dot<T>(mg->ctx, mg->A[top].rows, r, r, tp<T>(mg->norm));
+}
+
+// Captures solve_cycle into mg->cycle_graph on a private stream (the context's stream may be
+// the legacy default stream, which cannot be captured).  Only hierarchies whose coarse solve is
+// one plain launch qualify (the dense inverse, the fused tail, or the one-block CG).
+template <typename T> int capture_cycle(hb_mg *mg, T *x, const T *b)
+{
+    hb_context *ctx = mg->ctx;
+    const bool coarse_plain = mg->coarse_inv || mg->tail_level >= 0 || mg->A[0].ld / 4 <= 256;
+    if (!coarse_plain || mg->graph_failed) return HB_ERR_UNSUPPORTED;
+    cudaStream_t cs = nullptr;
+    cudaEvent_t ev = nullptr;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (cs) cudaStreamDestroy(cs);
+        mg->graph_failed = true;
+        return HB_ERR_CUDA;
+    }
+    cudaEventRecord(ev, ctx->stream);
+    cudaStreamWaitEvent(cs, ev, 0);
+    cudaStream_t saved = ctx->stream;
+    const uint64_t l0 = ctx->launches;
+    ctx->stream = cs;
+    cudaGraph_t g = nullptr;
+    int st = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess ? HB_OK : HB_ERR_CUDA;
+    if (!st) st = solve_cycle<T>(mg, x, b);
+    const cudaError_t e = cudaStreamEndCapture(cs, &g);
+    ctx->stream = saved;
+    mg->graph_kernels = ctx->launches - l0;
+    ctx->launches = l0;
+    if (!st && e != cudaSuccess) st = HB_ERR_CUDA;
+    if (!st && cudaGraphInstantiate(&mg->cycle_graph, g, 0) != cudaSuccess) st = HB_ERR_CUDA;
+    if (g) cudaGraphDestroy(g);
+    cudaEventDestroy(ev);
+    cudaStreamDestroy(cs);
+    if (st) {
+        cudaGetLastError();
+        mg->cycle_graph = nullptr;
+        mg->graph_failed = true;
+        return st;
+    }
+    mg->graph_x = x;
+    mg->graph_b = b;
+    return HB_OK;
+}
+
 // MGSolver::value (mg.hh:1098-1126): r = b - A x; rnorm0 = |r|; cycles until |r| < eps rnorm0.
+// Each cycle is one replay of the captured cycle graph where it applies (the same kernels in
+// the same order, so the same iterates), then the norm's read-back for the stopping test.
 template <typename T> int mg_solve(hb_mg *mg, const T *b, T *x, int64_t *used, T *rnorm)
 {
     hb_context *ctx = mg->ctx;
@@ -201,11 +275,19 @@ template <typename T> int mg_solve(hb_mg *mg, const T *b, T *x, int64_t *used, T
     HB_TRY(level_mode<T>(mg, top, HB_MODE_DEFECT, x, b, nullptr, r));
     T r0, rc = T(1e16);
     HB_TRY(norm_host<T>(mg, r, n, &r0));
+    if (mg->cycle_graph && (mg->graph_x != x || mg->graph_b != b)) drop_cycle_graph(mg);
+    if (!mg->cycle_graph && mg->prm.max_iters > 1) capture_cycle<T>(mg, x, b);
     int64_t u = 0;
     for (int64_t i = 0; i < mg->prm.max_iters; ++i) {
-        HB_TRY(vcycle<T>(mg, top, x, b));
-        HB_TRY(level_mode<T>(mg, top, HB_MODE_DEFECT, x, b, nullptr, r));
-        HB_TRY(norm_host<T>(mg, r, n, &rc));
+        if (mg->cycle_graph) {
+            HB_CUDA_TRY(ctx, cudaGraphLaunch(mg->cycle_graph, ctx->stream));
+            ctx->launches += mg->graph_kernels;
+        } else {
+            HB_TRY(solve_cycle<T>(mg, x, b));
+        }
+        HB_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->pinned, mg->norm, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+        HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        rc = std::sqrt(*static_cast<T *>(ctx->pinned));
         u = i + 1;
         if (rc < (T)mg->prm.eps * r0) break;
     }
@@ -309,6 +391,7 @@ int hb_mg_finest(hb_mg *mg, hb_ell *A)
 
 int hb_mg_set_dense_coarse(hb_mg *mg, void *inv)
 {
+    drop_cycle_graph(mg);
     mg->coarse_inv = inv;
     return HB_OK;
 }
@@ -316,6 +399,7 @@ int hb_mg_set_dense_coarse(hb_mg *mg, void *inv)
 int hb_mg_enable_tail(hb_mg *mg, int64_t max_rows)
 {
     if (!mg || max_rows < 0) return HB_ERR_INVALID;
+    drop_cycle_graph(mg);
     mg->tail_level = -1;
     if (max_rows == 0) return HB_OK;
     if (mg->dtype != HB_F32 || mg->B.empty() || !mg->coarse_inv) return HB_ERR_UNSUPPORTED;
@@ -608,6 +692,7 @@ int hb_mg_create_banded(hb_context *ctx, int nlevels, const hb_ell *A, const hb_
 int hb_mg_destroy(hb_mg *mg)
 {
     if (!mg) return HB_ERR_INVALID;
+    drop_cycle_graph(mg);
     // stream-ordered: the memory returns to the pool once the stream's queued work is done
     if (mg->tail_desc) cudaFreeAsync(mg->tail_desc, mg->ctx->stream);
     cudaFreeAsync(mg->mem, mg->ctx->stream);
@@ -621,6 +706,7 @@ int hb_mg_set_params(hb_mg *mg, const hb_mg_params *params)
     if (params->max_iters < 0 || params->max_iters_coarse < 0 || params->n_pre < 0 || params->n_post < 0)
         return HB_ERR_INVALID;
     const bool redo = params->damping != mg->prm.damping;
+    drop_cycle_graph(mg);
     mg->prm = *params;
     if (redo) return mg->dtype == HB_F64 ? jacobi_init<double>(mg) : jacobi_init<float>(mg);
     return HB_OK;
