@@ -263,8 +263,9 @@ struct hb_q1 {
 
 namespace {
 
+template <bool SMEM>
 __global__ void dense_inverse_kernel(int64_t n, const int32_t *__restrict__ Aj, const double *__restrict__ Ax,
-                                     int64_t ld, int K, double *__restrict__ W, float *__restrict__ inv, int *singular);
+                                     int64_t ld, int K, double *__restrict__ Wg, float *__restrict__ inv, int *singular);
 
 int q1_alloc(hb_q1 *q, void **p, size_t bytes)
 {
@@ -360,8 +361,19 @@ int q1_build(hb_q1 *q, const double *coef)
     q->coarse_inv = (float *)p;
     int *singular = (int *)hb_scalars(ctx) + 65;
     HB_CUDA_TRY(ctx, cudaMemsetAsync(singular, 0, sizeof(int), ctx->stream));
-    dense_inverse_kernel<<<1, 256, 0, ctx->stream>>>(nc, q->A64[0].Aj, (const double *)q->A64[0].Ax, q->A64[0].ld,
-                                                     (int)q->A64[0].K, q->gj, q->coarse_inv, singular);
+    const size_t wbytes = (size_t)nc * 2 * nc * sizeof(double);
+    if (nc <= 128 && wbytes <= 200 * 1024 &&
+        cudaFuncSetAttribute(dense_inverse_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wbytes) ==
+            cudaSuccess) {
+        dense_inverse_kernel<true><<<1, 256, wbytes, ctx->stream>>>(nc, q->A64[0].Aj, (const double *)q->A64[0].Ax,
+                                                                    q->A64[0].ld, (int)q->A64[0].K, q->gj,
+                                                                    q->coarse_inv, singular);
+    } else {
+        cudaGetLastError();
+        dense_inverse_kernel<false><<<1, 256, 0, ctx->stream>>>(nc, q->A64[0].Aj, (const double *)q->A64[0].Ax,
+                                                                q->A64[0].ld, (int)q->A64[0].K, q->gj, q->coarse_inv,
+                                                                singular);
+    }
     if ((st = hb_check_launch(ctx, "dense_inverse_kernel"))) return st;
     hb_mg_set_dense_coarse(q->mg, q->coarse_inv);
     // the coarse levels of the cycle as one single-cluster launch (same arithmetic)
@@ -381,10 +393,17 @@ int q1_build(hb_q1 *q, const double *coef)
 }
 
 // Gauss-Jordan inverse of a small SPD matrix (one block): W = [A | I] in FP64 with partial
-// pivoting; the inverse is stored row-major as FP32.  n <= 81 (the coarsest level).
+// pivoting (the first row of largest magnitude in the column, the row itself first); the inverse
+// is stored row-major as FP32.  SMEM: W lives in dynamic shared memory (n <= 81, the coarsest
+// level: 105 KB) instead of the global workspace.  The pivot is found by warp 0 (lane l scans
+// rows c + l, c + l + 32, ... in order, then a shuffle reduction that keeps the lowest row among
+// equal magnitudes), the same row the sequential scan picks.
+template <bool SMEM>
 __global__ void dense_inverse_kernel(int64_t n, const int32_t *__restrict__ Aj, const double *__restrict__ Ax,
-                                     int64_t ld, int K, double *__restrict__ W, float *__restrict__ inv, int *singular)
+                                     int64_t ld, int K, double *__restrict__ Wg, float *__restrict__ inv, int *singular)
 {
+    extern __shared__ double Ws[];
+    double *W = SMEM ? Ws : Wg;
     __shared__ double fac[128];
     __shared__ int piv;
     const int64_t w = 2 * n;
@@ -399,13 +418,27 @@ __global__ void dense_inverse_kernel(int64_t n, const int32_t *__restrict__ Aj, 
     }
     __syncthreads();
     for (int64_t c = 0; c < n; ++c) {
-        if (threadIdx.x == 0) {
-            int64_t p = c;
-            double best = fabs(W[c * w + c]);
-            for (int64_t r = c + 1; r < n; ++r)
-                if (fabs(W[r * w + c]) > best) { best = fabs(W[r * w + c]); p = r; }
-            if (best == 0.0) *singular = 1;
-            piv = (int)p;
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            double best = -1.0;
+            int64_t p = n;
+            for (int64_t r = c + lane; r < n; r += 32) {
+                double v = fabs(W[r * w + c]);
+                if (v != v) v = -1.0;                  // a NaN below the diagonal is never chosen
+                if (v > best) { best = v; p = r; }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_down_sync(0xffffffffu, best, o);
+                const int64_t op = __shfl_down_sync(0xffffffffu, p, o);
+                if (ob > best || (ob == best && op < p)) { best = ob; p = op; }
+            }
+            if (lane == 0) {
+                const double dc = fabs(W[c * w + c]);
+                if (dc != dc || best <= dc) p = c;       // the diagonal wins ties (and a NaN there)
+                if (dc == dc && (p == c ? dc : best) == 0.0) *singular = 1;
+                piv = (int)p;
+            }
         }
         __syncthreads();
         if (piv != c)
