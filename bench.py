@@ -564,7 +564,11 @@ def bench_serve(n_requests=120, rate=150.0, seed=11, device=0):
     timed = S.poisson_trace(n_requests, rate=rate, seed=seed)
     out = {"workload": f"{n_requests} requests of the serving stream (side log-U[33,1025], coef log-U[1e-2,1e2], "
                        f"1e-8 FP64), burst and Poisson {rate:g}/s", "rows_total": burst.rows}
-    with S.Server(mode="mixed") as srv:  # warm-up: module load, memory pool
+    # warm-up, untimed: the whole burst once through a mixed server (every path's kernels loaded,
+    # the stream-ordered memory pool grown to the stream's peak), a few requests through plain CG
+    with S.Server(mode="mixed") as srv:
+        S.replay(srv, burst, realtime=False)
+    with S.Server(mode="plain") as srv:
         S.replay(srv, S.poisson_trace(8, 0.0, seed=seed + 1000), realtime=False)
     for mode in ("mixed", "plain"):
         res = {}
