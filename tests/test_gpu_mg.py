@@ -219,3 +219,37 @@ def test_banded_mg_general_sides_bitwise(hb, M):
         data.close()
     assert out[0][:3] == out[1][:3]
     assert np.array_equal(out[0][3], out[1][3])
+
+
+def test_mg_cycle_graph_recapture_and_parameter_changes(hb, oracle):
+    """A solve replays its cycle as a captured CUDA graph: solving into another x buffer or with
+    another b re-captures it (same results as the first buffers), and changing the parameters
+    drops it (the new coarse iteration cap takes effect; the old one back gives the old x)."""
+    M = 65
+    H = P.mg_hierarchy(M)
+    A = H.A[-1]
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 2))
+    data = hb.MGData.from_hierarchy(H, eps=1e-8)
+    bd = dev(b)
+    xs = []
+    for _ in range(2):                       # x1, x2, then x1 again
+        for k in range(2):
+            x = dev(np.zeros(A.rows))
+            used, _, _ = hb.MGSolver.value(data, bd, x)
+            xs.append((host(x), used))
+    assert all(np.array_equal(xs[0][0], x) and xs[0][1] == u for x, u in xs)
+    bd2 = dev(b * 2.0)
+    x = dev(np.zeros(A.rows))
+    hb.MGSolver.value(data, bd2, x)
+    assert np.allclose(host(x), 2.0 * xs[0][0], rtol=0, atol=1e-7 * np.abs(xs[0][0]).max())
+    x_o, u_o = oracle.mg(H, b, eps=1e-8, max_iters_coarse=1)
+    data.configure(max_iters_coarse=1)
+    x = dev(np.zeros(A.rows))
+    used1, _, _ = hb.MGSolver.value(data, bd, x)
+    assert abs(used1 - u_o) <= 1
+    assert not np.array_equal(host(x), xs[0][0])
+    data.configure(max_iters_coarse=1000)
+    x = dev(np.zeros(A.rows))
+    hb.MGSolver.value(data, bd, x)
+    assert np.array_equal(host(x), xs[0][0])
+    data.close()
