@@ -10,6 +10,10 @@
 
 void hb_note_error(hb_context *ctx, cudaError_t e, const char *what)
 {
+    // clear the runtime's last error (a failed launch or API call that is not sticky), so the
+    // failure is reported once, through the status this library returns, and not again by the
+    // caller's next unrelated CUDA call
+    cudaGetLastError();
     if (!ctx) return;
     ctx->last_error = std::string(what) + ": " + cudaGetErrorString(e);
 }

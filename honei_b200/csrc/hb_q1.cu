@@ -362,8 +362,9 @@ int q1_build(hb_q1 *q, const double *coef)
     int *singular = (int *)hb_scalars(ctx) + 65;
     HB_CUDA_TRY(ctx, cudaMemsetAsync(singular, 0, sizeof(int), ctx->stream));
     const size_t wbytes = (size_t)nc * 2 * nc * sizeof(double);
+    // the cap is process-wide (concurrent builds): one value for every launch
     if (nc <= 128 && wbytes <= 200 * 1024 &&
-        cudaFuncSetAttribute(dense_inverse_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wbytes) ==
+        cudaFuncSetAttribute(dense_inverse_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) ==
             cudaSuccess) {
         dense_inverse_kernel<true><<<1, 256, wbytes, ctx->stream>>>(nc, q->A64[0].Aj, (const double *)q->A64[0].Ax,
                                                                     q->A64[0].ld, (int)q->A64[0].K, q->gj,

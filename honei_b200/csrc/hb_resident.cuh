@@ -175,7 +175,14 @@ bool res_plan(hb_context *ctx, int64_t rows, int K, int nwin, int nown, const vo
     if (fixed + nwin * (size_t)r * sizeof(T) > avail) return false;
     const int64_t w = std::min<int64_t>(rows, (int64_t)((avail - fixed) / (nwin * sizeof(T))));
     const size_t bytes = res_smem_bytes<T>(K, r, w, nwin, nown);
-    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess ||
+    // The kernel's dynamic shared memory cap is process-wide: always the largest value, so that
+    // plans of concurrent solves (other threads, other contexts) never lower it under each
+    // other's launches; each launch passes its own size.
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess ||
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             optin - (int)fa.sharedSizeBytes) != cudaSuccess ||
+        bytes + fa.sharedSizeBytes > (size_t)optin ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, RES_THREADS, bytes) != cudaSuccess) {
         cudaGetLastError();
         return false;

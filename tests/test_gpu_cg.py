@@ -231,3 +231,45 @@ def test_cg_resident_kernel_edge_cases(hb, oracle):
     r_o = relres(oracle, A32.astype(np.float64), b32.astype(np.float64), x_o.astype(np.float64))
     r_g = relres(oracle, A32.astype(np.float64), b32.astype(np.float64), x_g.astype(np.float64))
     assert abs(r_g - r_o) <= 1e-5, (r_g, r_o)
+
+
+def test_cg_concurrent_solves_on_separate_contexts(hb):
+    """Four host threads, each with its own context and stream, solve systems of different sizes
+    (and so different resident-kernel plans) at the same time.  Every solve succeeds and is
+    bit-identical to the same solve run alone; no failure leaks into the caller's CUDA state."""
+    import threading
+    sizes = (257, 129, 257, 513)
+
+    def solve(M, seed, ctx=None, stream=None):
+        A = hb.SparseMatrixELL.q1_poisson(M, ctx=ctx)
+        xt = dev(P.uniform_vector(M * M, seed))
+        b = torch.empty_like(xt)
+        hb.Product.value(b, A, xt, ctx=ctx)
+        x = torch.zeros_like(xt)
+        used = hb.CGSolver.value(A, None, b, x, 100000, 1e-8, ctx=ctx)
+        (stream or torch.cuda.current_stream()).synchronize()
+        return used, x.cpu().numpy()
+
+    alone = [solve(M, k + 1) for k, M in enumerate(sizes)]
+    results, errors = {}, []
+
+    def worker(k, M):
+        try:
+            ctx = hb.Context(0)
+            s = torch.cuda.Stream()
+            ctx.bind_stream(s)
+            with torch.cuda.stream(s):
+                results[k] = [solve(M, k + 1, ctx, s) for _ in range(3)]
+        except Exception as e:    # reported below, in the test's thread
+            errors.append((k, repr(e)))
+
+    threads = [threading.Thread(target=worker, args=(k, M)) for k, M in enumerate(sizes)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    torch.cuda.synchronize()
+    for k in range(len(sizes)):
+        for used, x in results[k]:
+            assert used == alone[k][0] and np.array_equal(x, alone[k][1]), k
