@@ -66,6 +66,8 @@ SIGNATURES = {
     "hb_ell_import_f64": (i32, [vp, i64, i64, i64, i64, i64, vp, vp, vp, P_ell]),
     "hb_ell_import_f32": (i32, [vp, i64, i64, i64, i64, i64, vp, vp, vp, P_ell]),
     "hb_ell_cast_f64_f32": (i32, [vp, P_ell, P_ell]),
+    "hb_spai2_f64": (i32, [vp, P_ell, P_ell]),
+    "hb_spai2_f32": (i32, [vp, P_ell, P_ell]),
     "hb_q1_assemble_f64": (i32, [vp, i64, vp, i32, P_ell]),
     "hb_spmv_f64": (i32, [vp, P_ell, vp, vp]),
     "hb_spmv_f32": (i32, [vp, P_ell, vp, vp]),

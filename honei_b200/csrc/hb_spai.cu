@@ -1,0 +1,312 @@
+// hb_spai.cu -- SPAI2<tags::GPU::CUDA>::value(M, A) (honei/math/spai2.hh:294-298, wrapper
+// honei/math/spai2-cuda.cc:180-228): the sparse approximate inverse M of a square matrix A with
+// A's sparsity pattern, column by column (Grote and Huckle's least-squares SPAI restricted to
+// the pattern of A), with the arithmetic of SPAI2<tags::CPU::SSE> (honei/math/spai2.hh:129-260)
+// so that M is bit-identical to it:
+//   J  = the rows of A's column idx (ascending), n2 of them;
+//   I  = the rows of A's columns J[0], J[1], ... concatenated (each ascending), n1 of them;
+//   At(k, j) = A(I[k], J[j]), et(k) = (I[k] == idx);
+//   product(i, j) = sum_k At(k, i) At(k, j), pro_v(i) = sum_k At(k, i) et(k), sequential in k;
+//   LUDecomposition<tags::CPU::SSE> (honei/math/ludecomposition.hh:254-320): elimination
+//   without pivoting, then forward and backward substitution with sequential sums;
+//   M(J[i], idx) = res[i].
+// The entries of A are what SparseMatrix(const SparseMatrixELL &) takes (honei/la/sparse_matrix.hh:
+// 157-185): slots whose value is not 0.  Columns with n2 == 0 or n1 == 0 keep A's values (M
+// starts as a copy of A, spai2-cuda.cc:187).
+//
+// Device plan:
+//   1. the column structure of A: per-column counts (atomics), an exclusive scan, a fill by
+//      atomics and a per-column insertion sort by row -- CSC rows ascending plus, per entry, its
+//      ELL slot (where M's value goes);
+//   2. one warp per column (grid-stride): At is built 32 rows at a time in shared memory (lane k
+//      reads row I[k]'s ELL slots and places each value by a binary search in J), the n2 (n2 + 1)
+//      / 2 distinct product entries (product is symmetric: the two multiplication orders give
+//      the same products) and pro_v accumulate across the chunks in k order, one lane per entry;
+//      the elimination runs in place on the warp's product (rows in parallel, columns in
+//      parallel within a step), the two substitutions in lane 0.
+// A row that stores one column twice is outside the supported input (the reference's
+// conversion keeps the later slot; here both would enter the column lists).
+#include "hb_internal.cuh"
+
+#include <cub/device/device_scan.cuh>
+
+namespace {
+
+constexpr int SPAI_MAX_WARPS = 8;
+
+template <typename T>
+__device__ __forceinline__ bool spai_entry(int32_t c, T v, int64_t n)
+{
+    return c >= 0 && (int64_t)c < n && v != T(0);
+}
+
+template <typename T>
+__global__ void spai_count_kernel(const int32_t *__restrict__ Aj, const T *__restrict__ Ax, int64_t n, int64_t ld,
+                                  int64_t K, unsigned long long *__restrict__ cnt)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < K * n; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = q / n, r = q - s * n;
+        const int32_t c = Aj[s * ld + r];
+        if (spai_entry(c, Ax[s * ld + r], n)) atomicAdd(cnt + c, 1ull);
+    }
+}
+
+template <typename T>
+__global__ void spai_fill_kernel(const int32_t *__restrict__ Aj, const T *__restrict__ Ax, int64_t n, int64_t ld,
+                                 int64_t K, unsigned long long *__restrict__ cursor, int32_t *__restrict__ crow,
+                                 int32_t *__restrict__ cslot)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < K * n; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = q / n, r = q - s * n;
+        const int32_t c = Aj[s * ld + r];
+        if (!spai_entry(c, Ax[s * ld + r], n)) continue;
+        const unsigned long long p = atomicAdd(cursor + c, 1ull);
+        crow[p] = (int32_t)r;
+        cslot[p] = (int32_t)s;
+    }
+}
+
+// Sorts each column's (row, slot) pairs by row and records the longest column.
+__global__ void spai_sort_kernel(int64_t n, const unsigned long long *__restrict__ cp, int32_t *__restrict__ crow,
+                                 int32_t *__restrict__ cslot, unsigned *__restrict__ maxlen)
+{
+    unsigned longest = 0;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t lo = (int64_t)cp[c], hi = (int64_t)cp[c + 1];
+        for (int64_t a = lo + 1; a < hi; ++a) {
+            const int32_t r = crow[a], s = cslot[a];
+            int64_t b = a - 1;
+            while (b >= lo && crow[b] > r) {
+                crow[b + 1] = crow[b];
+                cslot[b + 1] = cslot[b];
+                --b;
+            }
+            crow[b + 1] = r;
+            cslot[b + 1] = s;
+        }
+        longest = max(longest, (unsigned)(hi - lo));
+    }
+    for (int o = 16; o > 0; o >>= 1) longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(maxlen, longest);
+}
+
+// Shared memory of one warp for columns of up to cap entries.
+template <typename T> size_t spai_warp_bytes(int cap)
+{
+    const size_t b = ((size_t)32 * cap + (size_t)cap * cap + cap + 32) * sizeof(T) + (size_t)(2 * cap + 1) * sizeof(int32_t);
+    return (b + 15) & ~(size_t)15;
+}
+
+template <typename T>
+__global__ void spai2_kernel(const int32_t *__restrict__ Aj, const T *__restrict__ Ax, int64_t ld, int64_t K,
+                             int64_t n, const unsigned long long *__restrict__ cp, const int32_t *__restrict__ crow,
+                             const int32_t *__restrict__ cslot, T *__restrict__ Mx, int cap, unsigned warp_bytes)
+{
+    using hbd::add; using hbd::div; using hbd::mul; using hbd::sub;
+    extern __shared__ __align__(16) unsigned char spai_smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    T *At = (T *)(spai_smem + (size_t)w * warp_bytes);    // [32][cap]: chunk rows of At
+    T *prod = At + 32 * cap;                               // [n2][n2]: product, then its L\U
+    T *pv = prod + cap * cap;                              // [n2]: pro_v, then the solution
+    T *et = pv + cap;                                      // [32]
+    int32_t *J = (int32_t *)(et + 32);                     // [n2]
+    int32_t *seg = J + cap;                                // [n2 + 1]: start of column J[i]'s rows in I
+
+    for (int64_t col = (int64_t)blockIdx.x * wpb + w; col < n; col += (int64_t)gridDim.x * wpb) {
+        const int64_t c0 = (int64_t)cp[col];
+        const int n2 = (int)((int64_t)cp[col + 1] - c0);
+        if (n2 == 0) continue;
+        for (int i = lane; i < n2; i += 32) J[i] = crow[c0 + i];
+        __syncwarp();
+        if (lane == 0) {
+            int s = 0;
+            seg[0] = 0;
+            for (int i = 0; i < n2; ++i) {
+                s += (int)(cp[J[i] + 1] - cp[J[i]]);
+                seg[i + 1] = s;
+            }
+        }
+        __syncwarp();
+        const int n1 = seg[n2];
+        if (n1 == 0) {
+            __syncwarp();
+            continue;
+        }
+        for (int q = lane; q < n2 * n2; q += 32) prod[q] = T(0);
+        for (int i = lane; i < n2; i += 32) pv[i] = T(0);
+        const int npairs = n2 * (n2 + 1) / 2;
+        for (int k0 = 0; k0 < n1; k0 += 32) {
+            const int kc = min(32, n1 - k0);
+            if (lane < kc) {
+                const int k = k0 + lane;
+                int i = 0;
+                while (seg[i + 1] <= k) ++i;
+                const int32_t r = crow[(int64_t)cp[J[i]] + (k - seg[i])];
+                T *row = At + lane * cap;
+                for (int j = 0; j < n2; ++j) row[j] = T(0);
+                for (int64_t s = 0; s < K; ++s) {
+                    const int32_t c = Aj[s * ld + r];
+                    if (c < 0) continue;
+                    const T v = Ax[s * ld + r];
+                    if (!spai_entry(c, v, n)) continue;
+                    int lo = 0, hi = n2;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (J[mid] < c) lo = mid + 1; else hi = mid;
+                    }
+                    if (lo < n2 && J[lo] == c) row[lo] = v;
+                }
+                et[lane] = (int64_t)r == col ? T(1) : T(0);
+            }
+            __syncwarp();
+            for (int q = lane; q < npairs; q += 32) {
+                int i = 0, rem = q;
+                while (rem >= n2 - i) { rem -= n2 - i; ++i; }
+                const int j = i + rem;
+                T acc = prod[i * n2 + j];
+                for (int kk = 0; kk < kc; ++kk) acc = add(acc, mul(At[kk * cap + i], At[kk * cap + j]));
+                prod[i * n2 + j] = acc;
+            }
+            for (int i = lane; i < n2; i += 32) {
+                T acc = pv[i];
+                for (int kk = 0; kk < kc; ++kk) acc = add(acc, mul(At[kk * cap + i], et[kk]));
+                pv[i] = acc;
+            }
+            __syncwarp();
+        }
+        for (int q = lane; q < n2 * n2; q += 32) {
+            const int i = q / n2, j = q - i * n2;
+            if (i > j) prod[q] = prod[j * n2 + i];
+        }
+        __syncwarp();
+        // elimination step k: l(j, k) = u(j, k) / u(k, k), stored at (j, k) (u's column k below
+        // the diagonal is not read again); u(j, i) -= l(j, k) u(k, i) for i > k
+        for (int k = 0; k + 1 < n2; ++k) {
+            const T ukk = prod[k * n2 + k];
+            for (int j = k + 1 + lane; j < n2; j += 32) prod[j * n2 + k] = div(prod[j * n2 + k], ukk);
+            __syncwarp();
+            const int m = n2 - k - 1;
+            for (int q = lane; q < m * m; q += 32) {
+                const int j = k + 1 + q / m, i = k + 1 + q % m;
+                prod[j * n2 + i] = sub(prod[j * n2 + i], mul(prod[j * n2 + k], prod[k * n2 + i]));
+            }
+            __syncwarp();
+        }
+        if (lane == 0) {
+            // forward: x_i = 1 / l(i, i) * (b_i - sum), l(i, i) = 1 and 1 / 1 * v == v
+            for (int i = 0; i < n2; ++i) {
+                T s = T(0);
+                for (int j = 0; j < i; ++j) s = add(s, mul(prod[i * n2 + j], pv[j]));
+                pv[i] = sub(pv[i], s);
+            }
+            // backward: x_i = 1 / u(i, i) * (x_i - sum)
+            for (int i = n2 - 1; i >= 0; --i) {
+                T s = T(0);
+                for (int j = i + 1; j < n2; ++j) s = add(s, mul(prod[i * n2 + j], pv[j]));
+                pv[i] = mul(div(T(1), prod[i * n2 + i]), sub(pv[i], s));
+            }
+        }
+        __syncwarp();
+        for (int i = lane; i < n2; i += 32) Mx[(int64_t)cslot[c0 + i] * ld + J[i]] = pv[i];
+        __syncwarp();
+    }
+}
+
+unsigned grid_of(hb_context *ctx, int64_t work)
+{
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, (int64_t)ctx->num_sms * 16));
+}
+
+template <typename T>
+int spai2_impl(hb_context *ctx, const hb_ell *A, hb_ell *M, int dtype)
+{
+    if (!ctx) return HB_ERR_INVALID;
+    int st = hb_check_ell(A, dtype);
+    if (st) return st;
+    st = hb_check_ell(M, dtype);
+    if (st) return st;
+    if (A->rows != A->cols || M->rows != A->rows || M->cols != A->cols || M->K != A->K || M->ld != A->ld)
+        return HB_ERR_INVALID;
+    if (M->Ax == A->Ax) return HB_ERR_INVALID;
+    const int64_t n = A->rows, K = A->K, ld = A->ld;
+    if (n == 0) return HB_OK;
+    if (K * n > INT32_MAX) return HB_ERR_UNSUPPORTED;
+    cudaStream_t s = ctx->stream;
+    // M = A.copy()
+    if (M->Aj != A->Aj) HB_CUDA_TRY(ctx, cudaMemcpyAsync(M->Aj, A->Aj, (size_t)K * ld * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(M->Ax, A->Ax, (size_t)K * ld * sizeof(T), cudaMemcpyDeviceToDevice, s));
+
+    // workspace: counts / cursor, column offsets, rows and slots of the column lists, scan scratch
+    size_t scan_bytes = 0;
+    if (cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (unsigned long long *)nullptr,
+                                      (unsigned long long *)nullptr, (int)(n + 1), s) != cudaSuccess) {
+        cudaGetLastError();
+        return HB_ERR_CUDA;
+    }
+    const size_t off_cp = (size_t)(n + 1) * 8, off_rows = off_cp + (size_t)(n + 1) * 8;
+    const size_t off_slots = off_rows + (((size_t)K * n * 4 + 15) & ~(size_t)15);
+    const size_t off_scan = off_slots + (((size_t)K * n * 4 + 15) & ~(size_t)15);
+    st = hb_ensure_work(ctx, off_scan + scan_bytes + 16);
+    if (st) return st;
+    char *w = (char *)ctx->work;
+    auto *cnt = (unsigned long long *)w;
+    auto *cp = (unsigned long long *)(w + off_cp);
+    auto *crow = (int32_t *)(w + off_rows);
+    auto *cslot = (int32_t *)(w + off_slots);
+    unsigned *maxlen = (unsigned *)hb_scalars(ctx) + 96;
+
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(cnt, 0, (size_t)(n + 1) * 8, s));
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(maxlen, 0, sizeof(unsigned), s));
+    spai_count_kernel<T><<<grid_of(ctx, K * n), 256, 0, s>>>(A->Aj, (const T *)A->Ax, n, ld, K, cnt);
+    if ((st = hb_check_launch(ctx, "spai_count_kernel"))) return st;
+    size_t sb = scan_bytes;
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(w + off_scan, sb, cnt, cp, (int)(n + 1), s);
+    if (e != cudaSuccess) { hb_note_error(ctx, e, "DeviceScan::ExclusiveSum"); return HB_ERR_CUDA; }
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(cnt, cp, (size_t)(n + 1) * 8, cudaMemcpyDeviceToDevice, s));
+    spai_fill_kernel<T><<<grid_of(ctx, K * n), 256, 0, s>>>(A->Aj, (const T *)A->Ax, n, ld, K, cnt, crow, cslot);
+    if ((st = hb_check_launch(ctx, "spai_fill_kernel"))) return st;
+    spai_sort_kernel<<<grid_of(ctx, n), 256, 0, s>>>(n, cp, crow, cslot, maxlen);
+    if ((st = hb_check_launch(ctx, "spai_sort_kernel"))) return st;
+    unsigned *h = (unsigned *)ctx->pinned;
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, maxlen, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    HB_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    const int cap = (int)*h;
+    if (cap == 0) return HB_OK;
+
+    int dev = 0, optin = 0;
+    HB_CUDA_TRY(ctx, cudaGetDevice(&dev));
+    HB_CUDA_TRY(ctx, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa;
+    HB_CUDA_TRY(ctx, cudaFuncGetAttributes(&fa, spai2_kernel<T>));
+    const size_t avail = (size_t)optin - fa.sharedSizeBytes;
+    const size_t wb = spai_warp_bytes<T>(cap);
+    const int wpb = (int)std::min<size_t>(SPAI_MAX_WARPS, avail / wb);
+    if (wpb < 1) return HB_ERR_UNSUPPORTED;    // one column's least-squares system does not fit
+    // the attribute is process-wide: always the largest value, so that concurrent calls with
+    // other sizes never lower it under each other's launches
+    HB_CUDA_TRY(ctx, cudaFuncSetAttribute(spai2_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)avail));
+    int occ = 0;
+    HB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, spai2_kernel<T>, 32 * wpb, wb * wpb));
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->num_sms * std::max(occ, 1), (n + wpb - 1) / wpb));
+    spai2_kernel<T><<<(unsigned)blocks, 32 * wpb, wb * wpb, s>>>(A->Aj, (const T *)A->Ax, ld, K, n, cp, crow, cslot,
+                                                                 (T *)M->Ax, cap, (unsigned)wb);
+    return hb_check_launch(ctx, "spai2_kernel");
+}
+
+}  // namespace
+
+extern "C" {
+
+int hb_spai2_f64(hb_context *ctx, const hb_ell *A, hb_ell *M)
+{
+    HB_RANGE("hb_spai2_f64");
+    return spai2_impl<double>(ctx, A, M, HB_F64);
+}
+
+int hb_spai2_f32(hb_context *ctx, const hb_ell *A, hb_ell *M)
+{
+    HB_RANGE("hb_spai2_f32");
+    return spai2_impl<float>(ctx, A, M, HB_F32);
+}
+
+}  // extern "C"

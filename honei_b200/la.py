@@ -639,6 +639,30 @@ class CGSolverVAR:
         return used.value
 
 
+class SPAI2:
+    """SPAI2<tags::GPU::CUDA>::value(M, A) (honei/math/spai2.hh:294-298, hb_spai2_*): the sparse
+    approximate inverse of the square matrix A on A's pattern, bit-identical to
+    SPAI2<tags::CPU::SSE> (honei/math/spai2.hh:129-260).  The result is the matrix preconditioner
+    CGSolverVAR takes.
+
+    ``value(A)`` returns a new SparseMatrixELL M; ``value(A, M)`` fills a caller-provided M of
+    A's layout and returns it.
+    """
+
+    @staticmethod
+    def value(A: SparseMatrixELL, M: SparseMatrixELL | None = None, ctx: Context | None = None) -> SparseMatrixELL:
+        if A.rows() != A.columns():
+            raise MatrixRowsDoNotMatch(A.rows(), A.columns())
+        ctx = ctx or default_context()
+        if M is None:
+            M = SparseMatrixELL(A.rows(), A.columns(), A.K, A.ld, torch.empty_like(A.Aj), torch.empty_like(A.Ax))
+        elif (M.rows(), M.columns(), M.K, M.ld, M.dtype) != (A.rows(), A.columns(), A.K, A.ld, A.dtype):
+            raise MatrixRowsDoNotMatch(M.rows(), A.rows())
+        fn = getattr(lib(), f"hb_spai2_{_SUF[A.dtype]}")
+        check(fn(ctx.handle, C.byref(A.struct), C.byref(M.struct)), "SPAI2", ctx.handle)
+        return M
+
+
 class MGData:
     """Device MG hierarchy (MGData + the V(n_pre, n_post) cycle; honei/math/mg.hh:57-243, 567-662).
 

@@ -106,6 +106,19 @@ int hb_ell_validate(hb_context *ctx, const hb_ell *A, int64_t *bad_slots);
 /* Same pattern, values cast to float (for the FP32 inner solves of mixed precision). */
 int hb_ell_cast_f64_f32(hb_context *ctx, const hb_ell *src, hb_ell *dst);
 
+/* SPAI2<tags::GPU::CUDA>::value(M, A) (honei/math/spai2.hh:294-298; wrapper
+ * honei/math/spai2-cuda.cc:180-228): the sparse approximate inverse of the square matrix A with
+ * A's pattern, bit-identical to SPAI2<tags::CPU::SSE> (honei/math/spai2.hh:129-260): for every
+ * column the normal equations of the least-squares problem on the rows A's pattern reaches,
+ * solved by LU without pivoting.  M is caller-allocated with A's rows, cols, K and ld (M->Aj
+ * may be A->Aj; M->Ax must not be A->Ax); it receives A's pattern and the SPAI values, the
+ * columns whose system is empty keeping A's values (M = A.copy() first, as the reference).
+ * Entries are the slots whose value is not 0.  HB_ERR_UNSUPPORTED when one column's system
+ * does not fit in shared memory (columns of more than about 150 entries in FP64).  Uses the
+ * context workspace (about 8 * (K + 2) bytes per row) and synchronizes the stream once. */
+int hb_spai2_f64(hb_context *ctx, const hb_ell *A, hb_ell *M);
+int hb_spai2_f32(hb_context *ctx, const hb_ell *A, hb_ell *M);
+
 /* ------------------------------------------------------------------------------------------
  * Device CSR matrix.  Replaces the device copies of SparseMatrixCSR's Ar/Aj/Ax arrays
  * (honei/la/sparse_matrix_csr.hh) that the reference uploads for its CSR product kernel

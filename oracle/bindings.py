@@ -276,6 +276,19 @@ class Oracle:
         return x, used.value, inner.value, hist[: used.value + 1]
 
 
+    def spai2(self, A, col_start=0, col_end=0, Mx=None):
+        """SPAI2<tags::CPU::SSE> restated (ora_spai2.inc): M's values in A's ELL layout.  Columns
+        outside [col_start, col_end) keep Mx's values (A's when Mx is None); col_end 0 = all."""
+        s = self._suffix(A.dtype)
+        Mx = np.array(A.Ax if Mx is None else Mx, A.dtype)
+        f = getattr(self.lib, f"ora_spai2_{s}")
+        f.argtypes = [_vp, _vp, _u64, _u64]
+        e = _ell(A)
+        if f(_c.byref(e), _ptr(Mx), col_start, col_end) != 0:
+            raise RuntimeError("oracle SPAI2: matrix not square or out of memory")
+        return Mx
+
+
 class Reference:
     """The reference's own CPU path (unmodified HONEI sources + ref_shim.cc)."""
 
@@ -362,6 +375,18 @@ class Reference:
                    _ptr(b), _ptr(x), max_iters, eps, _c.byref(used), _c.byref(sec))
         self._check(rc)
         return x, used.value, sec.value
+
+    def spai2(self, A, tag="sse"):
+        """SPAI2<tag>::value(M, A) with M = A.copy() (tag "sse" or "mc-sse"): M's values in A's
+        ELL layout (0 in empty slots), and the seconds the call took."""
+        s = "f64" if A.dtype == np.float64 else "f32"
+        ainfo = np.array([A.rows, A.cols, A.stride, A.ncpr, A.threads], np.uint64)
+        Mx = np.zeros_like(A.Ax)
+        sec = _c.c_double(0)
+        f = getattr(self.lib, f"ref_spai2_{s}")
+        f.argtypes = [_c.c_int, _vp, _vp, _vp, _vp, _c.POINTER(_c.c_double)]
+        self._check(f(TAGS[tag], _ptr(ainfo), _ptr(A.Aj), _ptr(A.Ax), _ptr(Mx), _c.byref(sec)))
+        return Mx, sec.value
 
     def q1band_spmv(self, bands, x, tag="cpu", reps=0):
         """Product<tag> on BandedMatrixQx<Q1Type>: (y, median seconds of `reps` timed calls);

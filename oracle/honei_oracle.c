@@ -621,3 +621,17 @@ void ora_restrict_##SUF(uint64_t n_fine, DT *coarse, const DT *fine, const uint6
 }
 ORA_TRANSFER(f64, double)
 ORA_TRANSFER(f32, float)
+
+/* ---- SPAI2 (honei/math/spai2.hh:129-260) ---- */
+#define ORA_CAT2(a, b) a##b
+#define ORA_CAT(a, b) ORA_CAT2(a, b)
+#define DT double
+#define SUF f64
+#include "ora_spai2.inc"
+#undef DT
+#undef SUF
+#define DT float
+#define SUF f32
+#include "ora_spai2.inc"
+#undef DT
+#undef SUF

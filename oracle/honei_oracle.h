@@ -77,6 +77,15 @@ void   ora_sum_f64(uint64_t n, double *x, const double *y);
 void   ora_difference_f64(uint64_t n, double *r, const double *x, const double *y);
 void   ora_element_product_f64(uint64_t n, double *r, const double *x, const double *y);
 
+/* ---- Preconditioner construction ----
+ * SPAI2<tags::CPU::SSE>::value(M, A, col_start, col_end) (honei/math/spai2.hh:129-260) on the
+ * SparseMatrix made of A (honei/la/sparse_matrix.hh:157-185).  Mx is in A's ELL layout and must
+ * hold A's values on entry (M = A.copy()); the entries of columns [col_start, col_end) are
+ * overwritten (col_end == 0: every column).  Returns 0, or 1 when A is not square or memory runs
+ * out.  The algorithm is restated in ora_spai2.inc. */
+int    ora_spai2_f64(const ora_ell *A, double *Mx, uint64_t col_start, uint64_t col_end);
+int    ora_spai2_f32(const ora_ell *A, float *Mx, uint64_t col_start, uint64_t col_end);
+
 /* ---- Solvers ----
  * CG returns the number of iterations in *used; hist (optional, max_iters+1 entries) gets
  * sqrt(alpha) after every iteration, hist[0] = initial defect. */

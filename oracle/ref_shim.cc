@@ -25,6 +25,7 @@
 //   SparseMatrixCSR(SparseMatrix / SparseMatrixELL)         honei/la/sparse_matrix_csr-impl.hh:73-136
 //   Product<Tag>::value(DV, SparseMatrixCSR, DV)            honei/la/product.hh:209-242 (tags::CPU)
 //   Defect<Tag>::value(DV, DV, SparseMatrixCSR, DV)         honei/math/defect.hh:386-419 (tags::CPU)
+//   SPAI2<tags::CPU::SSE / MultiCore::SSE>::value(SM, SM)   honei/math/spai2.hh:129-296
 
 #include <honei/la/dense_vector.hh>
 #include <honei/la/sparse_matrix.hh>
@@ -47,6 +48,7 @@
 #include <honei/math/prolongation.hh>
 #include <honei/math/transposition.hh>
 #include <honei/math/fill_matrix.hh>
+#include <honei/math/spai2.hh>
 #include <honei/math/matrix_io.hh>
 #include <honei/math/vector_io.hh>
 #include <honei/util/configuration.hh>
@@ -393,6 +395,34 @@ namespace
             *seconds = t.empty() ? 0. : t[t.size() / 2];
         }
     }
+
+    // SPAI2 on the SparseMatrix made of the ELL matrix (sparse_matrix.hh:157-185), M starting as
+    // a copy of it (the test's and spai2-cuda.cc's M = A.copy()); Mx returns M's value at every
+    // ELL slot of A that holds an entry (0 elsewhere).  tag 2: SSE, 4: MultiCore::SSE.
+    template <typename DT_> int spai2_impl(int tag, const unsigned long * ainfo, const uint64_t * Aj,
+            const DT_ * Ax, DT_ * Mx, double * seconds)
+    {
+        return guarded([&]() {
+            SparseMatrixELL<DT_> A(ell_from(ainfo[0], ainfo[1], ainfo[2], ainfo[3], ainfo[4], Aj, Ax));
+            SparseMatrix<DT_> sm(A);
+            SparseMatrix<DT_> m(sm.copy());
+            double t0(now_s());
+            switch (tag)
+            {
+                case 2: SPAI2<tags::CPU::SSE>::value(m, sm); break;
+                case 4: SPAI2<tags::CPU::MultiCore::SSE>::value(m, sm); break;
+                default: throw InternalError("ref_shim: SPAI2 tag not available");
+            }
+            if (seconds) *seconds = now_s() - t0;
+            const SparseMatrix<DT_> & cm(m);
+            const unsigned long size(ainfo[2] * ainfo[3]), T(ainfo[4]), stride(ainfo[2]);
+            for (unsigned long i(0) ; i < size ; ++i)
+            {
+                const unsigned long row((i % stride) / T);
+                Mx[i] = Ax[i] != DT_(0) ? cm[row][Aj[i]] : DT_(0);
+            }
+        });
+    }
 }
 
 extern "C"
@@ -408,6 +438,14 @@ extern "C"
             const unsigned long * pinfo, const uint64_t * Pj, const float * Px, const float * b, float * x,
             unsigned long max_iters, float eps, unsigned long * used, double * seconds)
     { return cg_var_impl<float>(tag, ainfo, Aj, Ax, Pd, pinfo, Pj, Px, b, x, max_iters, eps, used, seconds); }
+
+    int ref_spai2_f64(int tag, const unsigned long * ainfo, const uint64_t * Aj, const double * Ax, double * Mx,
+            double * seconds)
+    { return spai2_impl<double>(tag, ainfo, Aj, Ax, Mx, seconds); }
+
+    int ref_spai2_f32(int tag, const unsigned long * ainfo, const uint64_t * Aj, const float * Ax, float * Mx,
+            double * seconds)
+    { return spai2_impl<float>(tag, ainfo, Aj, Ax, Mx, seconds); }
 
     int ref_q1band_spmv_f64(int tag, unsigned long n, const double * const * band, const double * x, double * y,
             int reps, double * seconds)

@@ -30,7 +30,13 @@ readers, honei/math/matrix_io.hh and honei/math/vector_io.hh):
   poisson_advanced4/sort_0 A_4 (A_4_sainv.ell, A_4_spai.ell; rhs_4, init_4), each with the
   reference's solution and iteration count (A_4, rhs_4, init_4 live in featflow_pa4.npz).
 
-    python tests/golden/make_golden.py [/path/to/honei-tree] [--only q1band|pcg|csr]
+* spai2.npz -- SPAI2<tags::CPU::SSE> (honei/math/spai2.hh:129-260, the tag the reference's
+  spai2_TEST.cc runs) of poisson_advanced/q2_sort_0/A_2 (Q2, 25 entries per row),
+  poisson_advanced/sort_0/A_4 and poisson_advanced4/sort_0/A_4 (matrix in featflow_pa4.npz),
+  FP64 and FP32, each with the reference's stored A_*_spai.ell beside it (pcg.npz for the
+  last), and of the reference's Q1 33^2 construction.
+
+    python tests/golden/make_golden.py [/path/to/honei-tree] [--only q1band|pcg|csr|spai2]
 """
 from __future__ import annotations
 
@@ -125,6 +131,31 @@ def pcg(R, tree: str) -> None:
     np.savez_compressed(os.path.join(HERE, "pcg.npz"), **out)
 
 
+def spai2(R, tree: str) -> None:
+    """SPAI2 of the FEATFLOW matrices and of Q1 33^2: M's values in the CSR order of A (M has
+    A's pattern), FP64 and FP32, plus the reference's stored SPAI matrix of each file."""
+    import dataclasses
+    td = os.path.join(tree, "honei", "math", "testdata")
+    out = {}
+    for name, path in (("q2a2", "poisson_advanced/q2_sort_0/A_2"), ("pa_a4", "poisson_advanced/sort_0/A_4"),
+                       ("pa4_a4", "poisson_advanced4/sort_0/A_4")):
+        A = R.read_ell(os.path.join(td, path + ".ell"))
+        if name != "pa4_a4":    # A_4 is in featflow_pa4.npz, its A_4_spai.ell in pcg.npz
+            put_matrix(out, name, A)
+            put_matrix(out, name + "_file", R.read_ell(os.path.join(td, path + "_spai.ell")))
+        for dt, suf in ((np.float64, "64"), (np.float32, "32")):
+            B = A.astype(dt)
+            Mx, _ = R.spai2(B, "sse")
+            out[f"{name}_M{suf}"] = dataclasses.replace(B, Ax=Mx).to_csr()[2]
+    Aq = R.q1_poisson(33)
+    put_matrix(out, "q1", Aq)
+    for dt, suf in ((np.float64, "64"), (np.float32, "32")):
+        B = Aq.astype(dt)
+        Mx, _ = R.spai2(B, "sse")
+        out[f"q1_M{suf}"] = dataclasses.replace(B, Ax=Mx).to_csr()[2]
+    np.savez_compressed(os.path.join(HERE, "spai2.npz"), **out)
+
+
 def csr(R) -> None:
     """SparseMatrixCSR: the reference's own CSR product test cases (product_TEST.cc:917-958,
     csr::blocksize 1, 2, 4, 8), the reference's ELL -> CSR conversion of Q1 33^2 with its
@@ -173,7 +204,8 @@ def csr(R) -> None:
 def main(tree: str, only: str | None = None) -> None:
     R = Reference()
     if only is not None:
-        {"q1band": lambda R: banded(R), "pcg": lambda R: pcg(R, tree), "csr": lambda R: csr(R)}[only](R)
+        {"q1band": lambda R: banded(R), "pcg": lambda R: pcg(R, tree), "csr": lambda R: csr(R),
+         "spai2": lambda R: spai2(R, tree)}[only](R)
         print("golden fixture", only, "written to", HERE)
         return
     td = os.path.join(tree, "honei", "math", "testdata")
@@ -265,6 +297,7 @@ def main(tree: str, only: str | None = None) -> None:
     banded(R)
     pcg(R, tree)
     csr(R)
+    spai2(R, tree)
     print("golden fixtures written to", HERE)
 
 

@@ -5,6 +5,8 @@
 * Where oracle/_ref/libhonei_ref.so exists: live, against the reference's CPU path.
 Bit-exact comparisons throughout: the oracle restates tags::CPU's arithmetic order.
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -333,3 +335,66 @@ def test_oracle_csr_live_against_reference(oracle, reference):
             A = reference.csr_from_ell(E, bs)
             C = P.csr_from_ell(E, bs)
             assert np.array_equal(C.Ar, A.Ar) and np.array_equal(C.Aj, A.Aj) and np.array_equal(C.Ax, A.Ax)
+
+
+# ---- SPAI2 (honei/math/spai2.hh:129-260) --------------------------------------------------
+def spai2_cases():
+    """(name, A, stored SPAI matrix of the reference's testdata or None) of spai2.npz."""
+    g, f, p = load_golden("spai2"), load_golden("featflow_pa4"), load_golden("pcg")
+    return g, [("q2a2", golden_matrix(g, "q2a2"), golden_matrix(g, "q2a2_file")),
+               ("pa_a4", golden_matrix(g, "pa_a4"), golden_matrix(g, "pa_a4_file")),
+               ("pa4_a4", golden_matrix(f, "A_4"), golden_matrix(p, "a4_spai")),
+               ("q1", golden_matrix(g, "q1"), None)]
+
+
+def test_oracle_spai2_matches_reference_fixture(oracle):
+    """The restatement equals SPAI2<tags::CPU::SSE> bit for bit on the FEATFLOW matrices (Q2 with
+    25 entries per row, Q1 levels) and Q1 33^2, FP64 and FP32; and the reference's own stored
+    A_*_spai.ell files are SPAI2 of their matrices: same pattern, values within 1e-13."""
+    g, cases = spai2_cases()
+    for name, A, stored in cases:
+        for dt, suf in ((np.float64, "64"), (np.float32, "32")):
+            B = A.astype(dt)
+            M = dataclasses.replace(B, Ax=oracle.spai2(B))
+            assert np.array_equal(M.to_csr()[2], g[f"{name}_M{suf}"]), (name, suf)
+        if stored is not None:
+            ip, ix, dv = dataclasses.replace(A, Ax=oracle.spai2(A)).to_csr()
+            sp, sx, sv = stored.to_csr()
+            assert np.array_equal(ip, sp) and np.array_equal(ix, sx), name
+            assert np.abs(dv - sv).max() <= 1e-13, name
+
+
+def test_oracle_spai2_is_a_better_inverse_than_jacobi(oracle):
+    """The reference's own SPAI2 test property (honei/math/spai2_TEST.cc:47-77):
+    ||I - A M||_1 (entrywise) below ||I - A diag(A)^-1||_1, on its Q2 matrix."""
+    _, cases = spai2_cases()
+    A = cases[0][1]
+    ip, ix, dv = A.to_csr()
+    Ad = np.zeros((A.rows, A.cols))
+    Ad[np.repeat(np.arange(A.rows), np.diff(ip)), ix] = dv
+    _, mx, mv = dataclasses.replace(A, Ax=oracle.spai2(A)).to_csr()
+    Md = np.zeros_like(Ad)
+    Md[np.repeat(np.arange(A.rows), np.diff(ip)), mx] = mv
+    eye = np.eye(A.rows)
+    assert np.abs(eye - Ad @ Md).sum() < np.abs(eye - Ad @ np.diag(1 / np.diag(Ad))).sum()
+
+
+def test_oracle_spai2_live_against_reference(oracle, reference):
+    """Live, against the compiled reference: natural, permuted, variable-coefficient and
+    threads = 4 layouts, FP64 and FP32, the SSE and MultiCore::SSE tags; and a column range
+    (the col_start / col_end arguments) changes only its own columns."""
+    cases = [P.q1_poisson(17), P.q1_poisson_permuted(17, 2)[0], P.q1_poisson(17, P.log_uniform_coef(17, 1e-2, 1e2, 3)),
+             P.ell_from_csr(289, 289, *P.q1_poisson_csr(17), threads=4)]
+    for A in cases:
+        for dt in (np.float64, np.float32):
+            B = A.astype(dt)
+            Mr, _ = reference.spai2(B, "sse")
+            assert np.array_equal(oracle.spai2(B), Mr)
+    Mr, _ = reference.spai2(cases[1], "mc-sse")
+    assert np.array_equal(oracle.spai2(cases[1]), Mr)
+    A = cases[0]
+    full = oracle.spai2(A)
+    part = oracle.spai2(A, 40, 90)
+    inside = np.isin(A.Aj.astype(np.int64), np.arange(40, 90)) & (A.Ax != 0)
+    assert np.array_equal(part[inside], full[inside]) and np.array_equal(part[~inside], A.Ax[~inside])
+    assert not np.array_equal(part[inside], A.Ax[inside])
