@@ -382,6 +382,52 @@ def bench_csr(la, ctx, x, ell_s, M=M_SPMV, reps=100, cpu=True):
     return out
 
 
+def bench_spai2(la, ctx, M=M_SPMV, reps=5, cpu=True, cpu_side=257):
+    """SPAI2<tags::GPU::CUDA> of the Q1 Poisson matrix of side M (M^2 columns, each a
+    least-squares system of up to 81 rows and 9 unknowns), FP64 and FP32: whole-call time
+    (column structure, normal equations, LU, one stream synchronization) per call.  The CPU
+    reference is the faster of SPAI2<tags::CPU::SSE> and SPAI2<tags::CPU::MultiCore::SSE> on the
+    side-cpu_side matrix, compared per column."""
+    import torch
+    from honei_b200 import problems as P
+    A = la.SparseMatrixELL.q1_poisson(M, ctx=ctx)
+    out = {"workload": f"SPAI2 of Q1 Poisson {M}^2 (pattern of A), whole call", "columns": A.rows()}
+    for name, A_ in (("f64", A), ("f32", A.to_float(ctx=ctx))):
+        Mm = la.SPAI2.value(A_, ctx=ctx)
+        la.SPAI2.value(A_, Mm, ctx=ctx)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            la.SPAI2.value(A_, Mm, ctx=ctx)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        t = statistics.median(ts)
+        out[name] = {"ms": round(t * 1e3, 3), "columns_per_s": round(A.rows() / t, 1)}
+        del Mm
+    if cpu:
+        R = _ref_cpu()
+        if R is not None:
+            # both CPU tags the reference has; the faster one is the baseline (the ten-thread
+            # MultiCore::SSE is held back by its per-column allocations)
+            Ah = P.q1_poisson(cpu_side)
+            best = None
+            for tag, threads in (("sse", 1), ("mc-sse", 10)):
+                sec = statistics.median(R.spai2(Ah, tag)[1] for _ in range(3))
+                cps = Ah.rows / sec
+                out[f"cpu_reference_{tag}"] = {"columns_per_s": round(cps, 1), "threads": threads}
+                if best is None or cps > best[0]:
+                    best = (cps, tag)
+            out["cpu_reference"] = {"columns_per_s": round(best[0], 1), "tag": best[1],
+                                    "sample": f"Q1 {cpu_side}^2 FP64, median of 3"}
+            out["speedup_f64_vs_cpu_reference"] = round(out["f64"]["columns_per_s"] / best[0], 1)
+    del A
+    torch.cuda.empty_cache()
+    return out
+
+
 def bench_q1band(la, ctx, x, ell_s, M=M_SPMV, reps=100, cpu=True):
     """Product on BandedMatrixQx<Q1Type> (nine bands of n values, no index array) for the same
     2049^2 Poisson matrix and x as the headline: algorithmic bytes 11*n*8 per product (nine
@@ -712,6 +758,8 @@ def run_ours(args):
     band_extra = bench_q1band(la, ctx, x, per_launch_s, cpu=(ws == 1 and not args.no_cpu_baseline))
     # ---- SparseMatrixCSR product of the same matrix (extra) ----
     csr_extra = bench_csr(la, ctx, x, per_launch_s, cpu=(ws == 1 and not args.no_cpu_baseline))
+    # ---- SPAI2 preconditioner construction on the same grid (extra) ----
+    spai_extra = bench_spai2(la, ctx, cpu=(ws == 1 and not args.no_cpu_baseline))
 
     # ---- plain FP64 CG on 257^2: solve latency (host b -> device solve -> host x) ----
     Acg = la.SparseMatrixELL.q1_poisson(M_CG, ctx=ctx)
@@ -785,7 +833,8 @@ def run_ours(args):
                     "serial_value": round(e2e_serial_value, 2)},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
-            "extra": {"spmv_f32_gbs": round(gbs32, 2), "q1band_2049": band_extra, "csr_2049": csr_extra, "cg_257": cg_extra,
+            "extra": {"spmv_f32_gbs": round(gbs32, 2), "q1band_2049": band_extra, "csr_2049": csr_extra, "spai2_2049": spai_extra,
+                      "cg_257": cg_extra,
                       "cg_257_cluster": cg_cluster, "cg_large": cg_large,
                       "mg_2049": mg_extra, "ir_2049": ir_extra, "batch_512": batch_extra, "serve": serve_extra},
         }

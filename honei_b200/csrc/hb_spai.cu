@@ -18,8 +18,9 @@
 //   1. the column structure of A: per-column counts (atomics), an exclusive scan, a fill by
 //      atomics and a per-column insertion sort by row -- CSC rows ascending plus, per entry, its
 //      ELL slot (where M's value goes);
-//   2. one warp per column (grid-stride): At is built 32 rows at a time in shared memory (lane k
-//      reads row I[k]'s ELL slots and places each value by a binary search in J), the n2 (n2 + 1)
+//   2. one warp per column (grid-stride): J's column lengths are scanned across the warp; At is
+//      built 32 rows at a time in shared memory (lane k loads row I[k]'s ELL slots together and
+//      places each value by a binary search in J), the n2 (n2 + 1)
 //      / 2 distinct product entries (product is symmetric: the two multiplication orders give
 //      the same products) and pro_v accumulate across the chunks in k order, one lane per entry;
 //      the elimination runs in place on the warp's product (rows in parallel, columns in
@@ -33,6 +34,7 @@
 namespace {
 
 constexpr int SPAI_MAX_WARPS = 8;
+constexpr int SLOTS = 9;           // ELL slots of a row whose loads are in flight together (Q1: all)
 
 template <typename T>
 __device__ __forceinline__ bool spai_entry(int32_t c, T v, int64_t n)
@@ -93,12 +95,12 @@ __global__ void spai_sort_kernel(int64_t n, const unsigned long long *__restrict
 // Shared memory of one warp for columns of up to cap entries.
 template <typename T> size_t spai_warp_bytes(int cap)
 {
-    const size_t b = ((size_t)32 * cap + (size_t)cap * cap + cap + 32) * sizeof(T) + (size_t)(2 * cap + 1) * sizeof(int32_t);
+    const size_t b = ((size_t)32 * cap + (size_t)cap * cap + cap + 32) * sizeof(T) + (size_t)(3 * cap + 1) * sizeof(int32_t);
     return (b + 15) & ~(size_t)15;
 }
 
 template <typename T>
-__global__ void spai2_kernel(const int32_t *__restrict__ Aj, const T *__restrict__ Ax, int64_t ld, int64_t K,
+__global__ void __launch_bounds__(SPAI_MAX_WARPS * 32, 4) spai2_kernel(const int32_t *__restrict__ Aj, const T *__restrict__ Ax, int64_t ld, int64_t K,
                              int64_t n, const unsigned long long *__restrict__ cp, const int32_t *__restrict__ crow,
                              const int32_t *__restrict__ cslot, T *__restrict__ Mx, int cap, unsigned warp_bytes)
 {
@@ -111,23 +113,36 @@ __global__ void spai2_kernel(const int32_t *__restrict__ Aj, const T *__restrict
     T *et = pv + cap;                                      // [32]
     int32_t *J = (int32_t *)(et + 32);                     // [n2]
     int32_t *seg = J + cap;                                // [n2 + 1]: start of column J[i]'s rows in I
+    int32_t *cstart = seg + cap + 1;                       // [n2]: column J[i]'s first entry (CSC)
 
     for (int64_t col = (int64_t)blockIdx.x * wpb + w; col < n; col += (int64_t)gridDim.x * wpb) {
         const int64_t c0 = (int64_t)cp[col];
         const int n2 = (int)((int64_t)cp[col + 1] - c0);
         if (n2 == 0) continue;
-        for (int i = lane; i < n2; i += 32) J[i] = crow[c0 + i];
-        __syncwarp();
-        if (lane == 0) {
-            int s = 0;
-            seg[0] = 0;
-            for (int i = 0; i < n2; ++i) {
-                s += (int)(cp[J[i] + 1] - cp[J[i]]);
-                seg[i + 1] = s;
+        // J, the CSC start of each column J[i], and the offsets of their row lists in I (an
+        // inclusive warp scan of the column lengths, 32 columns at a time)
+        int carry = 0;
+        if (lane == 0) seg[0] = 0;
+        for (int i0 = 0; i0 < n2; i0 += 32) {
+            const int i = i0 + lane;
+            int len = 0;
+            if (i < n2) {
+                const int32_t j = crow[c0 + i];
+                const int64_t a = (int64_t)cp[j];
+                len = (int)((int64_t)cp[j + 1] - a);
+                J[i] = j;
+                cstart[i] = (int32_t)a;
             }
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, len, o);
+                if (lane >= o) len += t;
+            }
+            if (i < n2) seg[i + 1] = carry + len;
+            carry += __shfl_sync(0xffffffffu, len, 31);
         }
         __syncwarp();
-        const int n1 = seg[n2];
+        const int n1 = carry;
         if (n1 == 0) {
             __syncwarp();
             continue;
@@ -141,20 +156,30 @@ __global__ void spai2_kernel(const int32_t *__restrict__ Aj, const T *__restrict
                 const int k = k0 + lane;
                 int i = 0;
                 while (seg[i + 1] <= k) ++i;
-                const int32_t r = crow[(int64_t)cp[J[i]] + (k - seg[i])];
+                const int32_t r = crow[(int64_t)cstart[i] + (k - seg[i])];
                 T *row = At + lane * cap;
                 for (int j = 0; j < n2; ++j) row[j] = T(0);
-                for (int64_t s = 0; s < K; ++s) {
-                    const int32_t c = Aj[s * ld + r];
-                    if (c < 0) continue;
-                    const T v = Ax[s * ld + r];
-                    if (!spai_entry(c, v, n)) continue;
-                    int lo = 0, hi = n2;
-                    while (lo < hi) {
-                        const int mid = (lo + hi) >> 1;
-                        if (J[mid] < c) lo = mid + 1; else hi = mid;
+                // the row's slots, SLOTS at a time with all loads in flight, then placed by a
+                // binary search in J (slots in order: a later slot of the same column would win)
+                for (int64_t s0 = 0; s0 < K; s0 += SLOTS) {
+                    int32_t cc[SLOTS];
+                    T vv[SLOTS];
+#pragma unroll
+                    for (int u = 0; u < SLOTS; ++u) {
+                        const bool in = s0 + u < K;
+                        cc[u] = in ? Aj[(s0 + u) * ld + r] : -1;
+                        vv[u] = in ? Ax[(s0 + u) * ld + r] : T(0);
                     }
-                    if (lo < n2 && J[lo] == c) row[lo] = v;
+#pragma unroll
+                    for (int u = 0; u < SLOTS; ++u) {
+                        if (!spai_entry(cc[u], vv[u], n)) continue;
+                        int lo = 0, hi = n2;
+                        while (lo < hi) {
+                            const int mid = (lo + hi) >> 1;
+                            if (J[mid] < cc[u]) lo = mid + 1; else hi = mid;
+                        }
+                        if (lo < n2 && J[lo] == cc[u]) row[lo] = vv[u];
+                    }
                 }
                 et[lane] = (int64_t)r == col ? T(1) : T(0);
             }

@@ -8,6 +8,7 @@
  *   Norm<vnt_l_two, {false,true}, tags::GPU::CUDA>  honei/la/norm.hh:538-580
  *   ScaledSum<tags::GPU::CUDA>       honei/la/scaled_sum.hh:444-488
  *   Scale, Sum, Difference, ElementProduct <tags::GPU::CUDA>
+ *   SPAI2<tags::GPU::CUDA>           honei/math/spai2.hh:294-298     (SparseMatrix in and out)
  * Every operator checks sizes first and throws VectorSizeDoesNotMatch as the CPU tags do, locks
  * its vectors for tags::GPU::CUDA (the MemoryArbiter uploads lazily through
  * MemoryBackend<tags::GPU::CUDA>), calls one entry point of the C ABI, and unlocks.  Results
@@ -26,7 +27,9 @@
 #include <honei/la/sparse_matrix_csr.hh>
 #include <honei/la/sum.hh>
 #include <honei/la/vector_error.hh>
+#include <honei/la/matrix_error.hh>
 #include <honei/math/defect.hh>
+#include <honei/math/spai2.hh>
 #include <honei/util/memory_arbiter.hh>
 
 #include <cuda_runtime.h>
@@ -34,6 +37,7 @@
 #include <cmath>
 #include <map>
 #include <mutex>
+#include <vector>
 
 namespace honei
 {
@@ -398,6 +402,55 @@ namespace honei
             DeviceLock<DenseVectorContinuousBase<DT_> > rl(result, lm_write_only);
             check(b200::defect(A, (const DT_ *)bl.ptr, (const DT_ *)xl.ptr, (DT_ *)rl.ptr), "Defect<GPU::CUDA> (ELL)");
         }
+        int spai2_call(const hb_ell & A, hb_ell & M, double) { return hb_spai2_f64(context(), &A, &M); }
+        int spai2_call(const hb_ell & A, hb_ell & M, float) { return hb_spai2_f32(context(), &A, &M); }
+
+        /// SPAI2<tags::GPU::CUDA> on host SparseMatrix containers, as the reference's wrapper
+        /// (honei/math/spai2-cuda.cc:180-228): M = A.copy(), the values computed on the device
+        /// from A's ELL form (SparseMatrixELL(SparseMatrix), whose device mirror the arbiter
+        /// uploads), then written into M entry by entry.
+        template <typename DT_> SparseMatrix<DT_> & spai2(SparseMatrix<DT_> & M, const SparseMatrix<DT_> & a)
+        {
+            if (a.rows() != a.columns())
+                throw MatrixIsNotSquare(a.rows(), a.columns());
+            M = a.copy();
+            SparseMatrixELL<DT_> e(a);
+            const hb_ell & A(device_mirror(e));
+            const std::size_t slots(A.K * A.ld);
+            hb_ell Md(A);
+            Md.Aj = nullptr;
+            Md.Ax = nullptr;
+            std::vector<int32_t> aj(slots);
+            std::vector<DT_> ax(slots);
+            int st(HB_OK);
+            if (cudaMalloc((void **)&Md.Aj, slots * sizeof(int32_t)) != cudaSuccess ||
+                    cudaMalloc(&Md.Ax, slots * sizeof(DT_)) != cudaSuccess)
+            {
+                cudaGetLastError();
+                st = HB_ERR_ALLOC;
+            }
+            if (! st)
+                st = spai2_call(A, Md, DT_(0));
+            if (! st)
+                st = hb_synchronize(context());
+            if (! st && (cudaMemcpy(aj.data(), Md.Aj, slots * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess ||
+                        cudaMemcpy(ax.data(), Md.Ax, slots * sizeof(DT_), cudaMemcpyDeviceToHost) != cudaSuccess))
+            {
+                cudaGetLastError();
+                st = HB_ERR_CUDA;
+            }
+            cudaFree(Md.Aj);
+            cudaFree(Md.Ax);
+            check(st, "SPAI2<GPU::CUDA>");
+            for (int64_t r(0) ; r < A.rows ; ++r)
+                for (int64_t k(0) ; k < A.K ; ++k)
+                {
+                    const int32_t c(aj[k * A.ld + r]);
+                    if (c >= 0)
+                        M(r, c, ax[k * A.ld + r]);
+                }
+            return M;
+        }
     }
 
     using namespace b200;
@@ -703,4 +756,20 @@ namespace honei
     DenseVectorContinuousBase<double> & ElementProduct<tags::GPU::CUDA>::value(DenseVectorContinuousBase<double> & r,
             const DenseVectorContinuousBase<double> & a, const DenseVectorContinuousBase<double> & b)
     { b200_eprod<double>(r, a, b); return r; }
+}
+
+namespace honei
+{
+    // ---- SPAI2 ---------------------------------------------------------------------------
+    SparseMatrix<float> & SPAI2<tags::GPU::CUDA>::value(SparseMatrix<float> & M, const SparseMatrix<float> & A)
+    {
+        CONTEXT("When calculating SPAI2<float> (B200):");
+        return b200::spai2<float>(M, A);
+    }
+
+    SparseMatrix<double> & SPAI2<tags::GPU::CUDA>::value(SparseMatrix<double> & M, const SparseMatrix<double> & A)
+    {
+        CONTEXT("When calculating SPAI2<double> (B200):");
+        return b200::spai2<double>(M, A);
+    }
 }

@@ -25,8 +25,10 @@
 #include <honei/math/prolongation.hh>
 #include <honei/math/restriction.hh>
 #include <honei/math/ri.hh>
+#include <honei/math/spai2.hh>
 #include <honei/math/vector_io.hh>
 
+#include <cstring>
 #include <iostream>
 #include <sstream>
 
@@ -277,8 +279,42 @@ template <typename DT_> void csr(unsigned long M, const std::string & tag)
     report(threw, "SparseMatrixCSR VectorSizeDoesNotMatch before launch " + tag);
 }
 
+// SPAI2<tags::GPU::CUDA> against SPAI2<tags::CPU::SSE> (the tag honei/math/spai2_TEST.cc runs):
+// every entry of M bit-identical, the pattern that of A.
+template <typename DT_> void spai(unsigned long M, const std::string & tag)
+{
+    SparseMatrix<DT_> A(q1<DT_>(M));
+    SparseMatrix<DT_> mc(A.copy()), mg(A.rows(), A.columns());
+    SPAI2<tags::CPU::SSE>::value(mc, A);
+    SPAI2<tags::GPU::CUDA>::value(mg, A);
+    bool ok(true);
+    for (unsigned long r(0) ; ok && r < A.rows() ; ++r)
+    {
+        const SparseVector<DT_> & c(mc[r]), & g(mg[r]), & a(A[r]);
+        ok = c.used_elements() == g.used_elements() && g.used_elements() == a.used_elements();
+        for (unsigned long i(0) ; ok && i < c.used_elements() ; ++i)
+            ok = c.indices()[i] == g.indices()[i] && g.indices()[i] == a.indices()[i] &&
+                std::memcmp(c.elements() + i, g.elements() + i, sizeof(DT_)) == 0;
+    }
+    report(ok, "SPAI2<GPU::CUDA> bit-exact to SPAI2<CPU::SSE> " + tag);
+    bool threw(false);
+    try
+    {
+        SparseMatrix<DT_> R(4, 6), out(4, 6);
+        R(0, 0, DT_(1));
+        SPAI2<tags::GPU::CUDA>::value(out, R);
+    }
+    catch (MatrixIsNotSquare &)
+    {
+        threw = true;
+    }
+    report(threw, "SPAI2<GPU::CUDA> MatrixIsNotSquare " + tag);
+}
+
 int main(int argc, char ** argv)
 {
+    spai<double>(33, "f64 33^2");
+    spai<float>(65, "f32 65^2");
     csr<double>(33, "f64 33^2");
     csr<float>(65, "f32 65^2");
     banded<double>(33, "f64 33^2");

@@ -46,6 +46,7 @@ def test_plugin_operators_and_generic_solvers(tmp_path):
     assert out.count("PASS") >= 54
     assert out.count("BandedMatrixQx") == 14
     assert out.count("SparseMatrixCSR") == 14
+    assert out.count("PASS SPAI2<GPU::CUDA>") == 4
 
 
 def test_plugin_cg_specialisation():
