@@ -18,7 +18,9 @@
 //   1. the column structure of A: per-column counts (atomics), an exclusive scan, a fill by
 //      atomics and a per-column insertion sort by row -- CSC rows ascending plus, per entry, its
 //      ELL slot (where M's value goes);
-//   2. one warp per column (grid-stride): J's column lengths are scanned across the warp; At is
+//   2. columns of at most 9 entries (every Q1 matrix): one thread per column with the normal
+//      equations, the LU and the substitutions in registers (spai2_col_kernel);
+//   3. wider columns: one warp per column (grid-stride): J's column lengths are scanned across the warp; At is
 //      built 32 rows at a time in shared memory (lane k loads row I[k]'s ELL slots together and
 //      places each value by a binary search in J), the n2 (n2 + 1)
 //      / 2 distinct product entries (product is symmetric: the two multiplication orders give
@@ -237,6 +239,145 @@ __global__ void __launch_bounds__(SPAI_MAX_WARPS * 32, 4) spai2_kernel(const int
     }
 }
 
+// Thread per column for columns of at most N entries (N = 9 covers every Q1 matrix): J, the
+// normal-equation sums (their N (N + 1) / 2 distinct entries), the LU and both substitutions in
+// registers with compile-time indices.  A column with n2 < N entries is padded: J's padding
+// matches no column, so its At entries are 0 and only the leading n2 x n2 block is eliminated
+// and substituted (the operations on it, and their order, are the warp kernel's and the
+// reference's).  Rows of I are visited in I's order: column J[0]'s rows, then J[1]'s, ...
+template <typename T, int N>
+__global__ void __launch_bounds__(128) spai2_col_kernel(const int32_t *__restrict__ Aj, const T *__restrict__ Ax,
+                                                         int64_t ld, int64_t K, int64_t n,
+                                                         const unsigned long long *__restrict__ cp,
+                                                         const int32_t *__restrict__ crow,
+                                                         const int32_t *__restrict__ cslot, T *__restrict__ Mx)
+{
+    using hbd::add; using hbd::div; using hbd::mul; using hbd::sub;
+    constexpr int NP = N * (N + 1) / 2;
+    for (int64_t col = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; col < n; col += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c0 = (int64_t)cp[col];
+        const int n2 = (int)((int64_t)cp[col + 1] - c0);
+        if (n2 == 0) continue;
+        // J in registers; the CSC start and length of each column J[i] in shared memory, so the
+        // loop over the rows of I is one loop (not one copy per segment: the loop body stays
+        // small in the instruction cache)
+        __shared__ int64_t sh_cst[N][128];
+        __shared__ int sh_len[N][128];
+        const int t = threadIdx.x;
+        int32_t J[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) J[i] = i < n2 ? crow[c0 + i] : -2;
+        int n1 = 0;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            int64_t a = 0;
+            int l = 0;
+            if (i < n2) {
+                a = (int64_t)cp[J[i]];
+                l = (int)((int64_t)cp[J[i] + 1] - a);
+            }
+            sh_cst[i][t] = a;
+            sh_len[i][t] = l;
+            n1 += l;
+        }
+        if (n1 == 0) continue;    // M keeps A's values
+        T acc[NP], pv[N];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) acc[q] = T(0);
+#pragma unroll
+        for (int i = 0; i < N; ++i) pv[i] = T(0);
+        int seg = 0, q = 0;
+        for (int k = 0; k < n1; ++k) {
+            while (q == sh_len[seg][t]) { ++seg; q = 0; }
+            const int32_t r = crow[sh_cst[seg][t] + q];
+            ++q;
+            T a[N];
+#pragma unroll
+            for (int j = 0; j < N; ++j) a[j] = T(0);
+            for (int64_t s0 = 0; s0 < K; s0 += SLOTS) {
+                int32_t cc[SLOTS];
+                T vv[SLOTS];
+#pragma unroll
+                for (int u = 0; u < SLOTS; ++u) {
+                    const bool in = s0 + u < K;
+                    cc[u] = in ? Aj[(s0 + u) * ld + r] : -1;
+                    vv[u] = in ? Ax[(s0 + u) * ld + r] : T(0);
+                }
+#pragma unroll
+                for (int u = 0; u < SLOTS; ++u) {
+                    if (!spai_entry(cc[u], vv[u], n)) continue;
+#pragma unroll
+                    for (int j = 0; j < N; ++j)
+                        if (J[j] == cc[u]) a[j] = vv[u];
+                }
+            }
+            const T e = (int64_t)r == col ? T(1) : T(0);
+            int p = 0;
+#pragma unroll
+            for (int i2 = 0; i2 < N; ++i2)
+#pragma unroll
+                for (int j2 = i2; j2 < N; ++j2) {
+                    acc[p] = add(acc[p], mul(a[i2], a[j2]));
+                    ++p;
+                }
+#pragma unroll
+            for (int i2 = 0; i2 < N; ++i2) pv[i2] = add(pv[i2], mul(a[i2], e));
+        }
+        T u[N][N];
+        {
+            int p = 0;
+#pragma unroll
+            for (int i2 = 0; i2 < N; ++i2)
+#pragma unroll
+                for (int j2 = i2; j2 < N; ++j2) {
+                    u[i2][j2] = acc[p];
+                    u[j2][i2] = acc[p];
+                    ++p;
+                }
+        }
+        // elimination without pivoting on the leading n2 x n2 block; l(j, k) kept at (j, k)
+#pragma unroll
+        for (int k = 0; k + 1 < N; ++k) {
+#pragma unroll
+            for (int j = k + 1; j < N; ++j) {
+                if (j < n2) {
+                    const T l = div(u[j][k], u[k][k]);
+                    u[j][k] = l;
+#pragma unroll
+                    for (int i = k + 1; i < N; ++i)
+                        if (i < n2) u[j][i] = sub(u[j][i], mul(l, u[k][i]));
+                }
+            }
+        }
+        T x[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            x[i] = T(0);
+            if (i < n2) {
+                T sum = T(0);
+#pragma unroll
+                for (int j = 0; j < i; ++j) sum = add(sum, mul(u[i][j], x[j]));
+                x[i] = sub(pv[i], sum);
+            }
+        }
+#pragma unroll
+        for (int i = N - 1; i >= 0; --i) {
+            if (i < n2) {
+                T sum = T(0);
+#pragma unroll
+                for (int j = i + 1; j < N; ++j)
+                    if (j < n2) sum = add(sum, mul(u[i][j], x[j]));
+                x[i] = mul(div(T(1), u[i][i]), sub(x[i], sum));
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+            if (i < n2) Mx[(int64_t)cslot[c0 + i] * ld + J[i]] = x[i];
+    }
+}
+
+constexpr int SPAI_COL_N = 9;
+
 unsigned grid_of(hb_context *ctx, int64_t work)
 {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, (int64_t)ctx->num_sms * 16));
@@ -298,6 +439,14 @@ int spai2_impl(hb_context *ctx, const hb_ell *A, hb_ell *M, int dtype)
     const int cap = (int)*h;
     if (cap == 0) return HB_OK;
 
+    if (cap <= SPAI_COL_N) {
+        int occ = 0;
+        HB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, spai2_col_kernel<T, SPAI_COL_N>, 128, 0));
+        const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->num_sms * std::max(occ, 1), (n + 127) / 128));
+        spai2_col_kernel<T, SPAI_COL_N><<<(unsigned)blocks, 128, 0, s>>>(A->Aj, (const T *)A->Ax, ld, K, n, cp, crow,
+                                                                        cslot, (T *)M->Ax);
+        return hb_check_launch(ctx, "spai2_col_kernel");
+    }
     int dev = 0, optin = 0;
     HB_CUDA_TRY(ctx, cudaGetDevice(&dev));
     HB_CUDA_TRY(ctx, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
