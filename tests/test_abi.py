@@ -39,3 +39,18 @@ def test_status_strings():
     from honei_b200 import _lib
     assert _lib.status_string(0) == "ok"
     assert "sizes" in _lib.status_string(2)
+
+
+def test_entry_points_refuse_invalid_arguments_before_any_device_call():
+    """A null context or matrix is HB_ERR_INVALID, returned before any CUDA call (so this runs
+    without a GPU)."""
+    from honei_b200 import _lib
+    lib = _lib.lib()
+    invalid = 1
+    for name, args in (("hb_spai2_f64", [None] * 3), ("hb_spai2_f32", [None] * 3), ("hb_csr_spmv_f64", [None] * 4),
+                       ("hb_csr_defect_f32", [None] * 5), ("hb_spmv_f64", [None] * 4), ("hb_defect_f64", [None] * 5),
+                       ("hb_cg_f64", [None] * 4 + [10, 1e-8, None, None])):
+        st = getattr(lib, name)(*args)
+        assert st == invalid, (name, st)
+    e = _lib.HbEll(9, 9, 1, 64, 0, 0, 0, 0)
+    assert lib.hb_spai2_f64(None, ctypes.byref(e), ctypes.byref(e)) == invalid
