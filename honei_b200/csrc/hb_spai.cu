@@ -33,9 +33,12 @@
 
 #include <cub/device/device_scan.cuh>
 
+#include <climits>
+
 namespace {
 
 constexpr int SPAI_MAX_WARPS = 8;
+constexpr int SPAI_MAX_COLUMN = 256;   // longest column any SPAI kernel here can solve (shared memory)
 constexpr int SLOTS = 9;           // ELL slots of a row whose loads are in flight together (Q1: all)
 
 template <typename T>
@@ -70,13 +73,18 @@ __global__ void spai_fill_kernel(const int32_t *__restrict__ Aj, const T *__rest
     }
 }
 
-// Sorts each column's (row, slot) pairs by row and records the longest column.
+// Sorts each column's (row, slot) pairs by row and records the longest column.  A column longer
+// than SPAI_MAX_COLUMN is left unsorted (the call is refused once the longest length is known), so
+// the quadratic insertion sort stays bounded for any input.
 __global__ void spai_sort_kernel(int64_t n, const unsigned long long *__restrict__ cp, int32_t *__restrict__ crow,
                                  int32_t *__restrict__ cslot, unsigned *__restrict__ maxlen)
 {
     unsigned longest = 0;
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
         const int64_t lo = (int64_t)cp[c], hi = (int64_t)cp[c + 1];
+        const int64_t len = hi - lo;
+        longest = max(longest, len > (int64_t)UINT_MAX ? UINT_MAX : (unsigned)len);
+        if (len > SPAI_MAX_COLUMN) continue;
         for (int64_t a = lo + 1; a < hi; ++a) {
             const int32_t r = crow[a], s = cslot[a];
             int64_t b = a - 1;
@@ -88,7 +96,6 @@ __global__ void spai_sort_kernel(int64_t n, const unsigned long long *__restrict
             crow[b + 1] = r;
             cslot[b + 1] = s;
         }
-        longest = max(longest, (unsigned)(hi - lo));
     }
     for (int o = 16; o > 0; o >>= 1) longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));
     if ((threadIdx.x & 31) == 0) atomicMax(maxlen, longest);
@@ -436,6 +443,7 @@ int spai2_impl(hb_context *ctx, const hb_ell *A, hb_ell *M, int dtype)
     unsigned *h = (unsigned *)ctx->pinned;
     HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, maxlen, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     HB_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    if (*h > (unsigned)SPAI_MAX_COLUMN) return HB_ERR_UNSUPPORTED;    // column lists left unsorted
     const int cap = (int)*h;
     if (cap == 0) return HB_OK;
 

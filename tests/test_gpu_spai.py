@@ -112,8 +112,8 @@ def test_spai2_random_patterns_and_wide_columns(hb, oracle):
 
 def test_spai2_edge_cases(hb, oracle):
     """An empty row and column, a column whose system is empty (n1 == 0: M keeps A's value), a
-    1 x 1 matrix; a non-square matrix and a column system too large for shared memory are
-    refused before any launch."""
+    1 x 1 matrix; a non-square matrix, a column system too large for shared memory and a column
+    longer than any kernel solves are refused."""
     # column 0 holds row 1 only, and column 1 is empty: n1 == 0, M(1, 0) stays 5
     A = P.ell_from_csr(3, 3, np.array([0, 0, 1, 2]), np.array([0, 2]), np.array([5.0, 2.0]))
     keys, vals = gpu_spai2(hb, A)
@@ -130,6 +130,15 @@ def test_spai2_edge_cases(hb, oracle):
     dense = random_square(np.random.default_rng(3), 200, 1.0)
     with pytest.raises(HBError):
         hb.SPAI2.value(hb.SparseMatrixELL.from_reference(dense))
+    # a column of 300 entries (every row couples to row 0): longer than any kernel solves, refused
+    # after the column lists are built (and left unsorted)
+    n = 300
+    ip = np.concatenate([[0], np.arange(1, 2 * n, 2)])
+    ix = np.concatenate([[0]] + [[0, r] for r in range(1, n)])
+    vals = np.where(ix == 0, -1.0, 4.0)
+    vals[0] = 4.0
+    with pytest.raises(HBError):
+        hb.SPAI2.value(hb.SparseMatrixELL.from_reference(P.ell_from_csr(n, n, ip, ix, vals)))
 
 
 def test_spai2_2049_column_ranges(hb, oracle):
