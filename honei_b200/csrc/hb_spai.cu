@@ -252,8 +252,11 @@ __global__ void __launch_bounds__(SPAI_MAX_WARPS * 32, 4) spai2_kernel(const int
 // matches no column, so its At entries are 0 and only the leading n2 x n2 block is eliminated
 // and substituted (the operations on it, and their order, are the warp kernel's and the
 // reference's).  Rows of I are visited in I's order: column J[0]'s rows, then J[1]'s, ...
+// Launch bounds: FP64 at 3 blocks per SM (168 registers; the few spills fall in the LU, once per
+// column) measured 14.0 ms against 15.2 ms at 2 blocks (223 registers) for Q1 2049^2; FP32 fits 4
+// blocks per SM in 128 registers.
 template <typename T, int N>
-__global__ void __launch_bounds__(128) spai2_col_kernel(const int32_t *__restrict__ Aj, const T *__restrict__ Ax,
+__global__ void __launch_bounds__(128, sizeof(T) == 8 ? 3 : 4) spai2_col_kernel(const int32_t *__restrict__ Aj, const T *__restrict__ Ax,
                                                          int64_t ld, int64_t K, int64_t n,
                                                          const unsigned long long *__restrict__ cp,
                                                          const int32_t *__restrict__ crow,
