@@ -39,6 +39,7 @@ namespace {
 
 constexpr int SPAI_MAX_WARPS = 8;
 constexpr int SPAI_MAX_COLUMN = 256;   // longest column any SPAI kernel here can solve (shared memory)
+constexpr int SORT_REG = 16;           // columns up to this length are sorted in registers
 constexpr int SLOTS = 9;           // ELL slots of a row whose loads are in flight together (Q1: all)
 
 template <typename T>
@@ -85,6 +86,34 @@ __global__ void spai_sort_kernel(int64_t n, const unsigned long long *__restrict
         const int64_t len = hi - lo;
         longest = max(longest, len > (int64_t)UINT_MAX ? UINT_MAX : (unsigned)len);
         if (len > SPAI_MAX_COLUMN) continue;
+        if (len <= SORT_REG) {
+            // in registers: one load and one store per entry, an odd-even transposition network
+            // (rows within a column are distinct, so any correct sort gives the same order)
+            int32_t rr[SORT_REG], ss[SORT_REG];
+#pragma unroll
+            for (int u = 0; u < SORT_REG; ++u) {
+                rr[u] = u < len ? crow[lo + u] : INT_MAX;
+                ss[u] = u < len ? cslot[lo + u] : 0;
+            }
+#pragma unroll
+            for (int round = 0; round < SORT_REG; ++round)
+#pragma unroll
+                for (int u = round & 1; u + 1 < SORT_REG; u += 2)
+                    if (rr[u] > rr[u + 1]) {
+                        const int32_t tr = rr[u], ts = ss[u];
+                        rr[u] = rr[u + 1];
+                        ss[u] = ss[u + 1];
+                        rr[u + 1] = tr;
+                        ss[u + 1] = ts;
+                    }
+#pragma unroll
+            for (int u = 0; u < SORT_REG; ++u)
+                if (u < len) {
+                    crow[lo + u] = rr[u];
+                    cslot[lo + u] = ss[u];
+                }
+            continue;
+        }
         for (int64_t a = lo + 1; a < hi; ++a) {
             const int32_t r = crow[a], s = cslot[a];
             int64_t b = a - 1;
