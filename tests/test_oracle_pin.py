@@ -392,6 +392,11 @@ def test_oracle_spai2_live_against_reference(oracle, reference):
             assert np.array_equal(oracle.spai2(B), Mr)
     Mr, _ = reference.spai2(cases[1], "mc-sse")
     assert np.array_equal(oracle.spai2(cases[1]), Mr)
+    # an empty row and column, a column whose system is empty (n1 == 0: M keeps A's value), 1 x 1
+    for E in (P.ell_from_csr(3, 3, np.array([0, 0, 1, 2]), np.array([0, 2]), np.array([5.0, 2.0])),
+              P.ell_from_csr(1, 1, np.array([0, 1]), np.array([0]), np.array([4.0]))):
+        Mr, _ = reference.spai2(E, "sse")
+        assert np.array_equal(oracle.spai2(E), Mr)
     A = cases[0]
     full = oracle.spai2(A)
     part = oracle.spai2(A, 40, 90)
