@@ -4,6 +4,7 @@ device path:
     python -m honei_b200.io_tools mtxtoell  matrix.mtx  matrix.ell   # clients/io_tools/mtxtoell.cc
     python -m honei_b200.io_tools elltomtx  matrix.ell  matrix.mtx   # clients/io_tools/elltomtx.cc
     python -m honei_b200.io_tools ellinfo   matrix.ell               # clients/io_tools/ellinfo.cc
+    python -m honei_b200.io_tools elltospai matrix.ell  spai.ell     # clients/io_tools/elltospai.cc
 
 MatrixMarket reading follows MatrixIO<io_formats::MTX>::read_matrix
 (honei/math/matrix_io.hh:234-338): any line containing '%' is a comment (one that also contains
@@ -14,7 +15,10 @@ every off-diagonal entry; a later entry of the same position overwrites an earli
 getline/eof loop skips it.  Entries of value 0 are dropped when the ELL matrix is built, as
 SparseMatrixELL(SparseMatrix) does.  Writing follows write_matrix (matrix_io.hh:400-430): a
 "coordinate real general" header, "rows columns nnz", then "row column value" with the value
-printed as a C++ stream prints a double (six significant digits).
+printed as a C++ stream prints a double (six significant digits).  elltospai reads the file
+straight to the device, builds SPAI2 there (bit-identical to the reference's
+SPAI2<tags::CPU::MultiCore::SSE>, which computes what SPAI2<tags::CPU::SSE> does) and writes M in
+the same one-lane layout; it needs a GPU.
 """
 from __future__ import annotations
 
@@ -100,9 +104,18 @@ def ellinfo(ell: str) -> str:
             f"NumColsPerRow: {A.ncpr}, Stride: {A.stride}, Threads: {A.threads}\n")
 
 
+def elltospai(ell: str, spai: str) -> None:
+    """clients/io_tools/elltospai.cc: SPAI2 of the file's matrix (pattern of A), written as an
+    ELL file (FP64)."""
+    from . import la
+    A = la.SparseMatrixELL.read_file(ell)
+    la.SPAI2.value(A).write_file(spai)
+
+
 def main(argv=None) -> int:
     argv = list(sys.argv[1:] if argv is None else argv)
-    usage = "usage: python -m honei_b200.io_tools {mtxtoell MTX ELL | elltomtx ELL MTX | ellinfo ELL}"
+    usage = ("usage: python -m honei_b200.io_tools {mtxtoell MTX ELL | elltomtx ELL MTX | ellinfo ELL | "
+             "elltospai ELL SPAI_ELL}")
     if not argv:
         print(usage)
         return 1
@@ -113,6 +126,8 @@ def main(argv=None) -> int:
         elltomtx(*args)
     elif cmd == "ellinfo" and len(args) == 1:
         sys.stdout.write(ellinfo(args[0]))
+    elif cmd == "elltospai" and len(args) == 2:
+        elltospai(*args)
     else:
         print(usage)
         return 1

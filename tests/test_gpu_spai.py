@@ -187,3 +187,17 @@ def test_spai2_preconditioned_cg(hb, oracle):
     Mdn[rows[order], ix[order]] = mv
     eye = np.eye(B.rows)
     assert np.abs(eye - Adn @ Mdn).sum() < np.abs(eye - Adn @ np.diag(1 / np.diag(Adn))).sum()
+
+
+def test_elltospai_client(hb, tmp_path):
+    """clients/io_tools/elltospai.cc on the device: the file's SPAI2 written in the same one-lane
+    ELL layout, values bit-identical to the reference's."""
+    from honei_b200 import io_tools
+    g = load_golden("spai2")
+    A = golden_matrix(g, "pa_a4")
+    P.write_ell(str(tmp_path / "A.ell"), A)
+    assert io_tools.main(["elltospai", str(tmp_path / "A.ell"), str(tmp_path / "M.ell")]) == 0
+    M = P.read_ell(str(tmp_path / "M.ell"))
+    assert (M.rows, M.cols, M.stride, M.ncpr) == (A.rows, A.cols, A.stride, A.ncpr)
+    assert np.array_equal(M.Aj, A.Aj)
+    assert same_bits(M.to_csr()[2], g["pa_a4_M64"])

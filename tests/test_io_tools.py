@@ -63,3 +63,4 @@ def test_elltomtx_and_ellinfo_round_trip(tmp_path):
     info = T.ellinfo(ell)
     assert f"Rows: {A.rows}" in info and f"Non Zero Elements: {A.nnz}" in info
     assert T.main(["ellinfo", ell]) == 0 and T.main(["bogus"]) == 1
+    assert T.main(["elltospai", ell]) == 1          # usage error, before any device work
