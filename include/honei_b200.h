@@ -114,8 +114,9 @@ int hb_ell_cast_f64_f32(hb_context *ctx, const hb_ell *src, hb_ell *dst);
  * may be A->Aj; M->Ax must not be A->Ax); it receives A's pattern and the SPAI values, the
  * columns whose system is empty keeping A's values (M = A.copy() first, as the reference).
  * Entries are the slots whose value is not 0.  HB_ERR_UNSUPPORTED when one column's system
- * does not fit in shared memory (columns of more than about 150 entries in FP64).  Uses the
- * context workspace (about 8 * (K + 2) bytes per row) and synchronizes the stream once. */
+ * does not fit in shared memory (columns of more than about 150 entries in FP64, 220 in FP32)
+ * or a column holds more than 256 entries.  Uses the context workspace (about 8 * (K + 2) bytes
+ * per row) and synchronizes the stream once. */
 int hb_spai2_f64(hb_context *ctx, const hb_ell *A, hb_ell *M);
 int hb_spai2_f32(hb_context *ctx, const hb_ell *A, hb_ell *M);
 
