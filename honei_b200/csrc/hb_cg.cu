@@ -684,13 +684,14 @@ int hb_cg_f32(hb_context *ctx, const hb_ell *A, const float *b, float *x, int64_
 // ---------------------------------------------------------------------------------------
 // Allocation-free CG: hb_cg_f64_noalloc.
 //
-// For callers that cannot allocate device memory at solve time: code that runs while a
-// stream is being captured into a CUDA graph (cudaMalloc is not allowed there), real-time
-// or embedded hosts that forbid allocation after start-up, and processes whose device memory
-// is entirely reserved by another framework's caching allocator.  The work vectors, the
+// For callers that cannot allocate device memory at solve time: real-time or embedded hosts
+// that forbid allocation after start-up (an allocation can block for an unbounded time), and
+// processes whose device memory is entirely reserved by another framework's caching
+// allocator (a cudaMalloc there fails although the memory is idle).  The work vectors, the
 // reduction partials, the barrier words and the result record live in one file-scope
 // __device__ array instead of a context's cudaMalloc'd workspace.  Every GPU that loads this
-// library holds the array (NOALLOC_BYTES, about 5.3 MB) until the process exits.
+// library in a process holds its own copy of the array (NOALLOC_BYTES, about 5.3 MB) until the
+// process exits.  Each call copies its result record to the host and synchronises its stream.
 // ---------------------------------------------------------------------------------------
 namespace {
 
@@ -709,33 +710,33 @@ static __device__ __align__(256) unsigned char hb_cg_noalloc_scratch[NOALLOC_BYT
 
 namespace {
 
-// The symbol's device address, looked up once per device with that device current.  The
-// name hb_cg_noalloc_scratch is only a host-side stand-in in host code; kernels must be given
-// this address.
+// The symbol's device address, looked up per device with that device current.  In host code
+// the name hb_cg_noalloc_scratch is only a host-side stand-in; kernels must be given this
+// address.  A lookup that fails is not cached: the next call on that device tries again.
 struct NoAllocDevice {
-    std::once_flag once;
     void *base = nullptr;
     int num_sms = 0;
-    int status = HB_OK;
 };
 NoAllocDevice g_noalloc[NOALLOC_MAX_DEVICES];
+std::mutex g_noalloc_mutex;
 
-int noalloc_setup(int device, NoAllocDevice **out)
+int noalloc_setup(int device, NoAllocDevice *out)
 {
     if (device < 0 || device >= NOALLOC_MAX_DEVICES) return HB_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     NoAllocDevice &d = g_noalloc[device];
-    std::call_once(d.once, [&d, device]() {
+    if (!d.base) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, hb_cg_noalloc_scratch);
-        if (e != cudaSuccess) { cudaGetLastError(); d.status = HB_ERR_CUDA; return; }
+        if (e != cudaSuccess || !p) { cudaGetLastError(); return HB_ERR_CUDA; }
         int sms = 0;
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        if (e != cudaSuccess) { cudaGetLastError(); d.status = HB_ERR_CUDA; return; }
-        d.base = p;
+        if (e != cudaSuccess || sms <= 0) { cudaGetLastError(); return HB_ERR_CUDA; }
         d.num_sms = sms;
-    });
-    *out = &d;
-    return d.status;
+        d.base = p;
+    }
+    *out = d;
+    return HB_OK;
 }
 
 template <int KT>
@@ -770,11 +771,18 @@ extern "C" int hb_cg_f64_noalloc(const hb_ell *A, const double *b, double *x, in
     if (A->rows > NOALLOC_MAX_ROWS || A->ld > NOALLOC_MAX_ROWS) return HB_ERR_UNSUPPORTED;
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return HB_ERR_CUDA; }
-    NoAllocDevice *d = nullptr;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    if (stream) {
+        // the scratch address belongs to the current device: a stream of another device
+        // would run the kernel against a foreign device's address
+        int sdev = -1;
+        if (cudaStreamGetDevice(stream, &sdev) != cudaSuccess) { cudaGetLastError(); return HB_ERR_INVALID; }
+        if (sdev != device) return HB_ERR_INVALID;
+    }
+    NoAllocDevice d;
     st = noalloc_setup(device, &d);
     if (st) return st;
-    cudaStream_t stream = (cudaStream_t)stream_;
-    char *base = (char *)d->base;
+    char *base = (char *)d.base;
     double *work = (double *)base;
     double *partials = (double *)(base + NOALLOC_WORK_BYTES);
     unsigned *bar = (unsigned *)(base + NOALLOC_WORK_BYTES + NOALLOC_PART_BYTES);
@@ -799,7 +807,7 @@ extern "C" int hb_cg_f64_noalloc(const hb_ell *A, const double *b, double *x, in
     P.bar.status = (int *)(bar + 2);
     P.res = res;
     const int64_t groups = ld / 4;
-    st = (A->K == 9) ? noalloc_launch<9>(stream, d->num_sms, P, groups) : noalloc_launch<0>(stream, d->num_sms, P, groups);
+    st = (A->K == 9) ? noalloc_launch<9>(stream, d.num_sms, P, groups) : noalloc_launch<0>(stream, d.num_sms, P, groups);
     if (st) return st;
     hb_solve_result h;
     if (cudaMemcpyAsync(&h, res, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||

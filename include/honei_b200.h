@@ -335,20 +335,23 @@ int hb_cg_var_ell_f32(hb_context *ctx, const hb_ell *A, const hb_ell *P, const f
 int hb_selftest_wait_timeout(hb_context *ctx);
 
 /* Allocation-free variant of hb_cg_f64.  This entry point has no counterpart in the reference.
- * It is for callers that cannot allocate device memory when they solve: code issuing work
- * while a stream is captured into a CUDA graph (cudaMalloc is not allowed there), real-time
- * or embedded hosts that forbid allocation after start-up, and processes whose device memory
- * is held entirely by another framework's caching allocator.  It needs no hb_context: its
- * work vectors, reduction partials, barrier words and result record live in one static
- * __device__ array of about 5.3 MB that every GPU loading this library keeps until exit.
+ * It is for callers that cannot allocate device memory when they solve: real-time or embedded
+ * hosts that forbid allocation after start-up (an allocation may block for an unbounded
+ * time), and processes whose device memory is held entirely by another framework's caching
+ * allocator (a cudaMalloc there fails although that memory is idle).  It needs no hb_context:
+ * its work vectors, reduction partials, barrier words and result record live in one static
+ * __device__ array of about 5.3 MB, which every GPU that loads this library in a process keeps
+ * until the process exits.
  * Limit: A->rows <= 131072 (FP64; e.g. the 257 x 257 Q1 grid); larger systems return
  * HB_ERR_UNSUPPORTED without launching.  The caller passes A, b, x (device) and the stream
- * (cudaStream_t, NULL = legacy stream); results as for hb_cg_f64.  It calls no cudaMalloc,
- * cudaFree or other allocating routine.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress) with that device current: make that first call
- * before any stream capture.  All calls on a device share the one array, so calls that
- * overlap on the GPU (different streams, threads or processes' streams at once) race and
- * must be serialised by the caller; the barrier words are re-zeroed by every call. */
+ * (cudaStream_t, NULL = legacy stream); `stream` must belong to the current device
+ * (HB_ERR_INVALID otherwise).  Results as for hb_cg_f64: the call copies its result record to
+ * the host and synchronises `stream` before it returns.  It calls no cudaMalloc, cudaFree or
+ * other allocating routine.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; a lookup that fails is retried by the next
+ * call.  The array is per process and per device: all calls in one process on one device share
+ * it, so such calls that overlap on the GPU (different streams or host threads at once) race
+ * and must be serialised by the caller.  The barrier words are re-zeroed by every call. */
 int hb_cg_f64_noalloc(const hb_ell *A, const double *b, double *x, int64_t max_iters, double eps,
                       int64_t *used_iters, double *final_defect, void *stream);
 
