@@ -132,67 +132,111 @@ def dist_setup():
 _CPU_CASE = {}
 
 
-def cpu_spmv_gbs(reps=None, budget_s=10.0):
+def spmv_config(ws):
+    """The workload's config dict, the same in both arms."""
+    return {"workload": "ell_spmv_q1_2049_f64", "rows": M_SPMV ** 2, "nnz": q1_nnz(M_SPMV),
+            "spmv_per_step": SPMV_PER_STEP, "bytes_per_spmv": spmv_bytes(q1_nnz(M_SPMV), M_SPMV ** 2, 8),
+            "parallelism": f"replicas{ws}",
+            "l2": "matrix 453 MB > L2 each application; no flush (x stays L2-resident by design)"}
+
+
+def _cpu_case():
     from honei_b200 import problems as P
     if not _CPU_CASE:
         _CPU_CASE["A"] = P.q1_poisson(M_SPMV)
         _CPU_CASE["x"] = P.uniform_vector(_CPU_CASE["A"].rows, 1)
-    A, x = _CPU_CASE["A"], _CPU_CASE["x"]
-    nbytes = spmv_bytes(A.nnz, A.rows, 8)
-    cores = os.cpu_count() or 1
+    return _CPU_CASE["A"], _CPU_CASE["x"]
+
+
+def _ref_handle():
+    """The reference's SparseMatrixELL<double> of the workload, built once, with every host
+    core given to its MultiCore tags; None without the compiled reference."""
+    if "h" in _CPU_CASE:
+        return _CPU_CASE["h"]
+    h = None
     try:
         from oracle.bindings import REF_SO, Reference
-        if not os.path.exists(REF_SO):
-            raise OSError
-        R = Reference()
-        R.set_threads(cores)
-        _, t1 = R.spmv(A, x, tag="mc-sse", reps=1)
-        if reps is None:
-            reps = int(max(3, min(200, budget_s / max(t1, 1e-4))))
-        _, t = R.spmv(A, x, tag="mc-sse", reps=reps)
-        kind, used_cores = "reference", cores
-        desc = f"tags::CPU::MultiCore::SSE, {reps} SpMVs of the 2049^2 FP64 matrix, median"
+        if os.path.exists(REF_SO):
+            R = Reference()
+            R.set_threads(os.cpu_count() or 1)
+            A, x = _cpu_case()
+            h = R.ell_handle(A, x)
     except OSError:
-        from oracle.bindings import Oracle
-        O = Oracle()
+        h = None
+    _CPU_CASE["h"] = h
+    return h
+
+
+def cpu_spmv_gbs(budget_s=10.0):
+    """The reference's Product<tags::CPU::MultiCore::SSE> on the workload's matrix, built once,
+    over a bounded sample (about budget_s of products; median), plus tags::CPU (the oracle's
+    order) and tags::CPU::SSE on one core (5 products each).  Without the compiled reference,
+    the C restatement of tags::CPU on one core."""
+    A, x = _cpu_case()
+    nbytes = spmv_bytes(A.nnz, A.rows, 8)
+    cores = os.cpu_count() or 1
+    h = _ref_handle()
+    if h is not None:
+        t1 = float(h.spmv("mc-sse", 2)[-1])
+        reps = int(max(3, min(200, budget_s / max(t1, 1e-4))))
+        t = statistics.median(h.spmv("mc-sse", reps))
+        single = {tag: round(nbytes / statistics.median(h.spmv(tag, 5)) / 1e9, 3) for tag in ("cpu", "sse")}
+        return {"value": round(nbytes / t / 1e9, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
+                "sample": f"tags::CPU::MultiCore::SSE on {cores} threads, {reps} products of the 2049^2 FP64 "
+                          "matrix (built once), median",
+                "single_core_gbs": {"tags::CPU": single["cpu"], "tags::CPU::SSE": single["sse"]}}
+    from oracle.bindings import Oracle
+    O = Oracle()
+    ts = []
+    for _ in range(5):
         t0 = time.perf_counter()
         O.spmv(A, x)
-        t1 = time.perf_counter() - t0
-        if reps is None:
-            reps = int(max(3, min(100, budget_s / max(t1, 1e-4))))
-        ts = []
-        for _ in range(reps):
-            t0 = time.perf_counter()
-            O.spmv(A, x)
-            ts.append(time.perf_counter() - t0)
-        t = statistics.median(ts)
-        kind, used_cores = "port", 1
-        desc = f"C restatement of tags::CPU, {reps} SpMVs of the 2049^2 FP64 matrix, median"
-    return nbytes / t / 1e9, used_cores, kind, desc, reps
+        ts.append(time.perf_counter() - t0)
+    return {"value": round(nbytes / statistics.median(ts) / 1e9, 3), "unit": "GB/s", "cores": 1, "kind": "port",
+            "sample": "C restatement of tags::CPU, 5 products of the 2049^2 FP64 matrix, median"}
 
 
 def run_reference_arm(args):
+    """The reference's own CPU path on the same workload: Product<tags::CPU::MultiCore::SSE> on
+    all host cores (oracle/_ref, the reference compiled from its sources), the matrix built once;
+    one step = SPMV_PER_STEP products, wall-clocked.  Rank 0 only."""
     ws, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    gbs_list = []
+    A, x = _cpu_case()
+    nbytes = spmv_bytes(A.nnz, A.rows, 8)
+    h = _ref_handle()
+    cores = os.cpu_count() or 1
+    if h is not None:
+        def step():
+            return float(np.sum(h.spmv("mc-sse", SPMV_PER_STEP)))
+        kind, used = "reference", cores
+        desc = f"tags::CPU::MultiCore::SSE on {cores} threads, {SPMV_PER_STEP} products of the 2049^2 FP64 matrix per step"
+    else:
+        from oracle.bindings import Oracle
+        O = Oracle()
+
+        def step():
+            t0 = time.perf_counter()
+            for _ in range(SPMV_PER_STEP):
+                O.spmv(A, x)
+            return time.perf_counter() - t0
+        kind, used = "port", 1
+        desc = f"C restatement of tags::CPU, {SPMV_PER_STEP} products of the 2049^2 FP64 matrix per step"
     for _ in range(args.warmup):
-        cpu_spmv_gbs(reps=SPMV_PER_STEP)
+        step()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        g, cores, kind, desc, _ = cpu_spmv_gbs(reps=SPMV_PER_STEP)
-        gbs_list.append(g)
+        step()
     wall = time.perf_counter() - t0
-    value = statistics.median(gbs_list)
+    value = nbytes * SPMV_PER_STEP * args.steps / wall / 1e9
     line = {
         "impl": "reference", "metric": "ell_spmv_gbs_q1_2049_f64", "value": round(value, 3), "unit": "GB/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1000 * wall / max(args.steps, 1), 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "ell_spmv_q1_2049_f64", "rows": M_SPMV ** 2, "nnz": q1_nnz(M_SPMV),
-                   "spmv_per_step": SPMV_PER_STEP},
-        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": cores, "kind": kind,
-                         "sample": desc.replace(f"{SPMV_PER_STEP} SpMVs", f"{SPMV_PER_STEP} SpMVs per step")},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Q1 Poisson 2049^2, x ~ U[-1,1])",
+        "config": spmv_config(ws),
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": used, "kind": kind, "sample": desc},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -597,37 +641,90 @@ def bench_ir(la, ctx, M=2049, seed=3):
     return out
 
 
-def bench_serve(n_requests=120, rate=150.0, seed=11, device=0):
-    """The serving stream: Q1 requests with grid side log-uniform in [33, 1025], cellwise
-    coefficient log-uniform in [1e-2, 1e2], b = A x_true, each solved to 1e-8 relative FP64
-    residual, submitted from host buffers and returned to host buffers.  The mixed server
-    (batched small grids + concurrent MG-PCG workers) against plain FP64 CG one request at a
-    time, on the same trace: once as a burst (every request queued at t = 0: capacity in
-    solves/s) and once with Poisson arrivals at ``rate`` per second (latency under load)."""
+SERVE_RATE = 40.0
+
+
+def _cpu_serve_baseline(trace, budget_s=20.0):
+    """The reference's CGSolver<tags::CPU::MultiCore::SSE> (plain FP64 CG, 1e-8 relative) on the
+    stream's requests in order, on every host core, until about budget_s have passed: solves/s
+    of that sample (host-side assembly excluded from the timing)."""
+    try:
+        from oracle.bindings import REF_SO, Reference
+        if not os.path.exists(REF_SO):
+            return None
+        R = Reference()
+        R.set_threads(os.cpu_count() or 1)
+    except OSError:
+        return None
+    from honei_b200 import problems as P
+    spent, solved, rows = 0.0, 0, 0
+    for i in range(len(trace)):
+        req = trace.request(i)
+        A = P.q1_poisson(req.M, req.coef.reshape(req.M - 1, req.M - 1), symmetric=True)
+        b, _ = R.spmv(A, req.x_true, tag="mc-sse")
+        _, used, sec = R.cg(A, b, eps=1e-8, max_iters=1000000, tag="mc-sse")
+        spent += sec
+        solved += 1
+        rows += req.M * req.M
+        if spent > budget_s:
+            break
+    return {"solves_per_s": round(solved / spent, 3), "requests": solved, "rows": rows, "seconds": round(spent, 2),
+            "cores": os.cpu_count(), "tag": "CGSolver<tags::CPU::MultiCore::SSE> (plain FP64 CG), the stream's "
+                                              "first requests in order"}
+
+
+def bench_serve(n_requests=20000, prefix=2000, rate=SERVE_RATE, seed=11, device=0, window=512, cpu=True):
+    """The serving configuration: a stream of Q1 requests, side log-uniform in [33, 1025],
+    cellwise coefficient log-uniform in [1e-2, 1e2], b = A x_true, each solved to 1e-8 relative
+    FP64 residual, submitted from host buffers and returned to host buffers.
+
+    Capacity (solves/s): the stream served closed-loop (at most `window` requests outstanding,
+    each submitted as soon as the server takes it) -- the mixed server on all n_requests, the two
+    plain FP64 CG baselines on the first `prefix` requests (and the mixed server on that prefix
+    too, for the like-for-like ratio).  Latency (p50/p99, arrival to result): the prefix with
+    Poisson arrivals at `rate` per second, a rate both the mixed server and the batched plain
+    baseline sustain, so p99 is service time rather than queue growth."""
     from honei_b200 import serve as S
 
-    burst = S.poisson_trace(n_requests, rate=0.0, seed=seed)
-    timed = S.poisson_trace(n_requests, rate=rate, seed=seed)
-    out = {"workload": f"{n_requests} requests of the serving stream (side log-U[33,1025], coef log-U[1e-2,1e2], "
-                       f"1e-8 FP64), burst and Poisson {rate:g}/s", "rows_total": burst.rows}
-    # warm-up, untimed: the whole burst once through a mixed server (every path's kernels loaded,
-    # the stream-ordered memory pool grown to the stream's peak), a few requests through plain CG
-    with S.Server(mode="mixed") as srv:
-        S.replay(srv, burst, realtime=False)
-    with S.Server(mode="plain") as srv:
-        S.replay(srv, S.poisson_trace(8, 0.0, seed=seed + 1000), realtime=False)
-    for mode in ("mixed", "plain"):
-        res = {}
-        for name, tr, rt in (("burst", burst, False), ("poisson", timed, True)):
-            with S.Server(mode=mode) as srv, ClockSampler(device) as clk:
-                rep = S.replay(srv, tr, realtime=rt)
-                peak = srv.stats()["bytes_peak"]
-            res[name] = {"solves_per_s": round(rep["solves_per_s"], 2), "p50_ms": round(rep["p50_ms"], 2),
-                         "p99_ms": round(rep["p99_ms"], 2), "ok": rep["ok"], "paths": rep["paths"],
-                         "max_true_relres": rep["max_true_relres"], "hbm_peak_bytes": peak,
-                         "clocks": clk.summary()}
-        out[mode] = res
-    out["speedup_solves_per_s"] = round(out["mixed"]["burst"]["solves_per_s"] / out["plain"]["burst"]["solves_per_s"], 2)
+    full = S.stream_trace(n_requests, rate=0.0, seed=seed)
+    pre = full.prefix(prefix)
+    timed = S.stream_trace(prefix, rate=rate, seed=seed)
+    out = {"workload": f"serving stream: {n_requests} requests (side log-U[33,1025], coef log-U[1e-2,1e2], "
+                       f"1e-8 FP64); baselines on its first {prefix} requests; latency on those {prefix} with "
+                       f"Poisson arrivals at {rate:g}/s",
+           "n_requests": n_requests, "prefix": prefix, "rows_total": full.rows, "rows_prefix": pre.rows,
+           "rate_per_s": rate}
+    # warm-up, untimed: kernels of every path loaded, the stream-ordered pool grown
+    warm = S.stream_trace(400, rate=0.0, seed=seed + 1000)
+    for mode in ("mixed", "plain_batched"):
+        with S.Server(mode=mode) as srv:
+            S.replay_stream(srv, warm, realtime=False, window=window)
+
+    def run(mode, trace, realtime):
+        with S.Server(mode=mode) as srv, ClockSampler(device) as clk:
+            rep = S.replay_stream(srv, trace, realtime=realtime, window=window)
+            st = srv.stats()
+        return {"requests": rep["completed"], "solves_per_s": round(rep["solves_per_s"], 2),
+                "p50_ms": round(rep["p50_ms"], 2), "p99_ms": round(rep["p99_ms"], 2),
+                "service_p50_ms": round(rep["service_p50_ms"], 2), "service_p99_ms": round(rep["service_p99_ms"], 2),
+                "ok": rep["ok"], "paths": rep["paths"], "max_true_relres": rep["max_true_relres"],
+                "makespan_s": round(rep["makespan_s"], 2), "submit_lag_max_ms": round(rep["submit_lag_max_ms"], 2),
+                "admitted_bytes_peak": st["bytes_peak"], "pool_used_high": st.get("pool_used_high"),
+                "pool_reserved_high": st.get("pool_reserved_high"), "clocks": clk.summary()}
+
+    out["mixed_full"] = run("mixed", full, False)
+    out["mixed_prefix"] = run("mixed", pre, False)
+    out["plain_batched_prefix"] = run("plain_batched", pre, False)
+    out["plain_prefix"] = run("plain", pre, False)
+    out["mixed_poisson"] = run("mixed", timed, True)
+    out["plain_batched_poisson"] = run("plain_batched", timed, True)
+    mp = out["mixed_prefix"]["solves_per_s"]
+    out["speedup_vs_plain_batched"] = round(mp / max(out["plain_batched_prefix"]["solves_per_s"], 1e-9), 2)
+    out["speedup_vs_plain_one_at_a_time"] = round(mp / max(out["plain_prefix"]["solves_per_s"], 1e-9), 2)
+    if cpu:
+        cb = _cpu_serve_baseline(full)
+        if cb is not None:
+            out["cpu_reference"] = cb
     return out
 
 
@@ -803,7 +900,9 @@ def run_ours(args):
     cg_large = bench_cg_large(la, ctx, cpu=(ws == 1 and not args.no_cpu_baseline)) if not args.no_mg else None
     batch_extra = None if args.no_batch else bench_batch(la, ctx, n_systems=args.batch_systems)
     # the serving sample before the multi-second 2049^2 solves (their heat lowers the clocks)
-    serve_extra = None if (args.no_serve or rank != 0 and ws > 1) else bench_serve(args.serve_requests, device=local)
+    serve_extra = None if (args.no_serve or rank != 0 and ws > 1) else bench_serve(
+        args.serve_requests, args.serve_prefix, args.serve_rate, device=local,
+        cpu=(ws == 1 and not args.no_cpu_baseline))
     mg_extra = None if args.no_mg else bench_mg(la, ctx, cpu=(ws == 1 and not args.no_cpu_baseline))
     ir_extra = None if args.no_mg else bench_ir(la, ctx)
 
@@ -811,16 +910,13 @@ def run_ours(args):
     if rank == 0:
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
-            g, cores, kind, desc, reps = cpu_spmv_gbs()
-            cpu = {"value": round(g, 3), "unit": "GB/s", "cores": cores, "kind": kind, "sample": desc}
+            cpu = cpu_spmv_gbs()
         line = {
             "metric": "ell_spmv_gbs_q1_2049_f64", "value": round(value, 2), "unit": "GB/s", "n_gpus": ws,
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": round(ms_max / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Q1 Poisson 2049^2, x ~ U[-1,1])",
-            "config": {"workload": "ell_spmv_q1_2049_f64", "rows": n, "nnz": nnz, "spmv_per_step": SPMV_PER_STEP,
-                       "bytes_per_spmv": nbytes, "parallelism": f"replicas{ws}",
-                       "l2": "matrix 453 MB > L2 each application; no flush (x stays L2-resident by design)"},
+            "config": spmv_config(ws),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_src,
                          "traffic": profile_traffic("ell_spmv_q1_2049_f64"),
@@ -855,7 +951,10 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream workload")
     ap.add_argument("--batch-systems", type=int, default=512, help="systems in the batched workload")
     ap.add_argument("--no-mg", action="store_true", help="skip the 2049^2 MG and mixed-precision workloads")
-    ap.add_argument("--serve-requests", type=int, default=120, help="requests in the serving sample")
+    ap.add_argument("--serve-requests", type=int, default=20000, help="requests in the serving stream")
+    ap.add_argument("--serve-prefix", type=int, default=2000,
+                    help="first requests of the stream served by the plain FP64 CG baselines")
+    ap.add_argument("--serve-rate", type=float, default=SERVE_RATE, help="Poisson arrivals per second (latency)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -66,6 +66,13 @@ SIGNATURES = {
     "hb_ell_import_f64": (i32, [vp, i64, i64, i64, i64, i64, vp, vp, vp, P_ell]),
     "hb_ell_import_f32": (i32, [vp, i64, i64, i64, i64, i64, vp, vp, vp, P_ell]),
     "hb_ell_cast_f64_f32": (i32, [vp, P_ell, P_ell]),
+    "hb_ell_cm_order": (i32, [vp, P_ell, vp, vp, P_i64]),
+    "hb_ell_bandwidth": (i32, [vp, P_ell, vp, P_i64]),
+    "hb_ell_permute": (i32, [vp, P_ell, vp, vp, P_ell]),
+    "hb_spmv_rows_f64": (i32, [vp, P_ell, vp, vp, vp]),
+    "hb_spmv_rows_f32": (i32, [vp, P_ell, vp, vp, vp]),
+    "hb_gather_f64": (i32, [vp, i64, vp, vp, vp]),
+    "hb_gather_f32": (i32, [vp, i64, vp, vp, vp]),
     "hb_spai2_f64": (i32, [vp, P_ell, P_ell]),
     "hb_spai2_f32": (i32, [vp, P_ell, P_ell]),
     "hb_q1_assemble_f64": (i32, [vp, i64, vp, i32, P_ell]),
@@ -73,6 +80,8 @@ SIGNATURES = {
     "hb_spmv_f32": (i32, [vp, P_ell, vp, vp]),
     "hb_defect_f64": (i32, [vp, P_ell, vp, vp, vp]),
     "hb_defect_f32": (i32, [vp, P_ell, vp, vp, vp]),
+    "hb_jacobi_sweeps_f64": (i32, [vp, P_ell, vp, vp, vp, vp, i64]),
+    "hb_jacobi_sweeps_f32": (i32, [vp, P_ell, vp, vp, vp, vp, i64]),
     "hb_dot_f64": (i32, [vp, i64, vp, vp, C.POINTER(f64)]),
     "hb_dot_f32": (i32, [vp, i64, vp, vp, C.POINTER(f32)]),
     "hb_norm_l2_f64": (i32, [vp, i64, vp, i32, C.POINTER(f64)]),
@@ -108,6 +117,9 @@ SIGNATURES = {
     "hb_mg_set_params": (i32, [vp, C.POINTER(HbMGParams)]),
     "hb_mg_solve_f64": (i32, [vp, vp, vp, P_i64, C.POINTER(f64)]),
     "hb_mg_solve_f32": (i32, [vp, vp, vp, P_i64, C.POINTER(f32)]),
+    "hb_mg_cycle_f64": (i32, [vp, vp, vp]),
+    "hb_mg_cycle_f32": (i32, [vp, vp, vp]),
+    "hb_mg_set_smoother": (i32, [vp, i32, vp]),
     "hb_ir_mg_solve": (i32, [vp, P_ell, vp, vp, vp, f64, i64, i32, P_i64, C.POINTER(f64)]),
     "hb_ir_cg_solve": (i32, [vp, P_ell, P_ell, vp, vp, f64, f32, i64, i64, P_i64, P_i64, C.POINTER(f64)]),
     # batched solves (struct pointers passed as void*; honei_b200.batch declares the structs)
@@ -159,6 +171,7 @@ SIGNATURES = {
     "hb_server_drain": (i32, [vp]),
     "hb_server_clock": (f64, [vp]),
     "hb_server_stats": (i32, [vp, P_i64, P_i64, P_i64, P_i64]),
+    "hb_server_pool_stats": (i32, [vp, P_i64, P_i64]),
     "hb_server_destroy": (i32, [vp]),
 }
 

@@ -298,6 +298,29 @@ int import_impl(hb_context *ctx, int64_t rows, int64_t cols, int64_t stride, int
 
 }  // namespace
 
+template <typename T>
+static int jacobi_sweeps(hb_context *ctx, const hb_ell *A, int dtype, const T *P, const T *b, T *x, T *tmp,
+                         int64_t sweeps)
+{
+    if (!ctx) return HB_ERR_INVALID;
+    int st = hb_check_ell(A, dtype);
+    if (st) return st;
+    if (A->rows != A->cols) return HB_ERR_SIZE;
+    if (sweeps < 0) return HB_ERR_INVALID;
+    if (sweeps == 0 || A->rows == 0) return HB_OK;
+    if (!P || !b || !x || !tmp || tmp == x) return HB_ERR_INVALID;
+    // x' = x + P (b - A x) reads every x it gathers while it writes: ping-pong through tmp
+    T *cur = x, *other = tmp;
+    for (int64_t k = 0; k < sweeps; ++k) {
+        st = hb_launch_spmv_mode<T>(ctx, A, HB_MODE_JACOBI, cur, b, P, other);
+        if (st) return st;
+        T *t = cur; cur = other; other = t;
+    }
+    if (cur != x)
+        HB_CUDA_TRY(ctx, cudaMemcpyAsync(x, cur, sizeof(T) * A->rows, cudaMemcpyDeviceToDevice, ctx->stream));
+    return HB_OK;
+}
+
 extern "C" {
 
 int hb_ell_validate(hb_context *ctx, const hb_ell *A, int64_t *bad_slots)
@@ -394,6 +417,20 @@ int hb_spmv_f32(hb_context *ctx, const hb_ell *A, const float *x, float *y)
     int st = hb_check_ell(A, HB_F32);
     if (st) return st;
     return hb_launch_spmv_mode<float>(ctx, A, HB_MODE_SPMV, x, nullptr, nullptr, y);
+}
+
+int hb_jacobi_sweeps_f64(hb_context *ctx, const hb_ell *A, const double *P, const double *b, double *x, double *tmp,
+                         int64_t sweeps)
+{
+    HB_RANGE("hb_jacobi_sweeps_f64");
+    return jacobi_sweeps<double>(ctx, A, HB_F64, P, b, x, tmp, sweeps);
+}
+
+int hb_jacobi_sweeps_f32(hb_context *ctx, const hb_ell *A, const float *P, const float *b, float *x, float *tmp,
+                         int64_t sweeps)
+{
+    HB_RANGE("hb_jacobi_sweeps_f32");
+    return jacobi_sweeps<float>(ctx, A, HB_F32, P, b, x, tmp, sweeps);
 }
 
 int hb_defect_f64(hb_context *ctx, const hb_ell *A, const double *b, const double *x, double *r)

@@ -579,6 +579,15 @@ int hb_mg_pcg_f32_graph(hb_mg *mg, cudaStream_t capture_stream, const float *b, 
 
 namespace {
 
+// One V-cycle on the finest level (the OperatorList that MGCycleCreation<V::STATIC> builds,
+// honei/math/mg.hh:567-662, run once): asynchronous on the context stream.
+template <typename T> int mg_cycle(hb_mg *mg, const T *b, T *x)
+{
+    if (!b || !x) return HB_ERR_INVALID;
+    if (mg->dtype != (sizeof(T) == 8 ? HB_F64 : HB_F32)) return HB_ERR_INVALID;
+    return vcycle<T>(mg, mg->L - 1, x, b);
+}
+
 template <typename T> int jacobi_init(hb_mg *mg)
 {
     for (int l = 0; l < mg->L; ++l)
@@ -726,6 +735,29 @@ int hb_mg_solve_f32(hb_mg *mg, const float *b, float *x, int64_t *used_cycles, f
     if (!mg || !b || !x) return HB_ERR_INVALID;
     if (mg->dtype != HB_F32) return HB_ERR_INVALID;
     return mg_solve<float>(mg, b, x, used_cycles, rnorm_host);
+}
+
+int hb_mg_cycle_f64(hb_mg *mg, const double *b, double *x)
+{
+    HB_RANGE("hb_mg_cycle_f64");
+    if (!mg) return HB_ERR_INVALID;
+    return mg_cycle<double>(mg, b, x);
+}
+
+int hb_mg_cycle_f32(hb_mg *mg, const float *b, float *x)
+{
+    HB_RANGE("hb_mg_cycle_f32");
+    if (!mg) return HB_ERR_INVALID;
+    return mg_cycle<float>(mg, b, x);
+}
+
+int hb_mg_set_smoother(hb_mg *mg, int level, const void *P)
+{
+    if (!mg || !P || level < 0 || level >= mg->L) return HB_ERR_INVALID;
+    const size_t es = mg->dtype == HB_F64 ? 8 : 4;
+    HB_CUDA_TRY(mg->ctx, cudaMemcpyAsync(mg->P[level], P, es * mg->A[level].rows, cudaMemcpyDeviceToDevice,
+                                         mg->ctx->stream));
+    return HB_OK;
 }
 
 // IRSolver<double outer, float inner, Norm<l2, true>> (honei/math/ir.hh:30-78).

@@ -1,0 +1,379 @@
+// hb_order.cu -- locality order of a device ELL matrix and the product through a reordered copy.
+//
+// A matrix whose rows and columns were numbered at random (the permuted Q1 workload) makes
+// every x gather of the product a separate 32-byte sector from L2: 37.7 M of them per product
+// at 2049^2, where the natural numbering needs about a third of a sector per entry.  The fix
+// does not change a single rounding: the rows are stored in a Cuthill-McKee breadth-first
+// order of the matrix graph (row -> its columns), each row keeping its slots in their order,
+// and the product writes row order[k]'s sum to y[order[k]].  With the columns renumbered as
+// well (B = P A P^T) the gathers become local; x then goes through the same permutation first
+// (xw[k] = x[order[k]]).  Either way each y entry is the same sum of the same products in the
+// same order as the product on A, so y is bit-identical to Product<tags::CPU>
+// (honei/la/product.hh:148-204).
+#include "hb_spmv_core.cuh"
+
+#include <algorithm>
+
+namespace {
+
+constexpr int ORD_THREADS = 1024;
+constexpr int ORD_ITEMS = 16;                                  // (row, slot) items per thread and tile
+constexpr int64_t ORD_TILE = (int64_t)ORD_THREADS * ORD_ITEMS;
+constexpr unsigned long long ORD_NONE = ~0ull;
+constexpr int ROWS_THREADS = 256;
+
+// Exclusive scan of one value per thread over the block, in thread order; *total = the sum.
+// smem: 33 entries.  Every thread of the block must call it.
+__device__ int64_t block_exclusive_scan(int64_t v, int64_t *smem, int64_t *total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int64_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    __syncthreads();
+    if (lane == 31) smem[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const int64_t w = lane < nw ? smem[lane] : 0;
+        int64_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        if (lane < nw) smem[lane] = wi - w;
+        if (lane == 31) smem[32] = wi;
+    }
+    __syncthreads();
+    const int64_t excl = smem[warp] + inc - v;
+    *total = smem[32];
+    return excl;
+}
+
+// Cuthill-McKee order in one block (the levels depend on each other; one block keeps every
+// level's hand-over inside __syncthreads).  Start: the row with the fewest off-diagonal
+// entries among rows that have one, lowest index on ties.  Level l + 1 = the rows first
+// reached from level l, ordered by the position of the first row of level l that reaches
+// them and, within that row, by slot -- the sequential breadth-first order, obtained in
+// parallel: every (row, slot) item of the level claims its column with atomicMin on its item
+// index, and the winning items are compacted in item order.  Rows the search never reaches
+// follow in ascending order.  info: levels, rows reached, start row.
+__global__ void __launch_bounds__(ORD_THREADS)
+cm_order_kernel(int64_t n, int64_t ld, int K, const int32_t *__restrict__ Aj, int32_t *__restrict__ order,
+                int32_t *__restrict__ pos, unsigned long long *__restrict__ key, int64_t *__restrict__ info)
+{
+    __shared__ int64_t s_scan[33];
+    __shared__ unsigned long long s_best;
+    const int tid = threadIdx.x;
+    for (int64_t r = tid; r < n; r += blockDim.x) {
+        pos[r] = -1;
+        key[r] = ORD_NONE;
+    }
+    if (tid == 0) s_best = ORD_NONE;
+    __syncthreads();
+    unsigned long long best = ORD_NONE;
+    for (int64_t r = tid; r < n; r += blockDim.x) {
+        unsigned long long deg = 0;
+        for (int k = 0; k < K; ++k) {
+            const int32_t c = Aj[(int64_t)k * ld + r];
+            if (c >= 0 && c != r) ++deg;
+        }
+        if (deg) best = min(best, (deg << 32) | (unsigned long long)r);
+    }
+    atomicMin(&s_best, best);
+    __syncthreads();
+    int64_t s = 0, e = 0, levels = 0;
+    const unsigned long long start = s_best;
+    if (start != ORD_NONE) {
+        const int32_t r0 = (int32_t)(start & 0xffffffffull);
+        if (tid == 0) { order[0] = r0; pos[r0] = 0; }
+        e = 1;
+    }
+    __syncthreads();
+    while (e > s) {
+        const int64_t items = (e - s) * K;
+        for (int64_t i = tid; i < items; i += blockDim.x) {
+            const int64_t k = i / K;
+            const int slot = (int)(i - k * K);
+            const int32_t v = order[s + k];
+            const int32_t c = Aj[(int64_t)slot * ld + v];
+            if (c >= 0 && c != v && pos[c] < 0) atomicMin(&key[c], (unsigned long long)i);
+        }
+        __syncthreads();
+        int64_t placed = e;
+        for (int64_t t0 = 0; t0 < items; t0 += ORD_TILE) {
+            int32_t cs[ORD_ITEMS];
+            int cnt = 0;
+#pragma unroll
+            for (int j = 0; j < ORD_ITEMS; ++j) {
+                const int64_t i = t0 + (int64_t)tid * ORD_ITEMS + j;
+                cs[j] = -1;
+                if (i < items) {
+                    const int64_t k = i / K;
+                    const int slot = (int)(i - k * K);
+                    const int32_t v = order[s + k];
+                    const int32_t c = Aj[(int64_t)slot * ld + v];
+                    if (c >= 0 && c != v && pos[c] < 0 && __ldcg(key + c) == (unsigned long long)i) {
+                        cs[j] = c;
+                        ++cnt;
+                    }
+                }
+            }
+            int64_t total;
+            int64_t at = placed + block_exclusive_scan(cnt, s_scan, &total);
+#pragma unroll
+            for (int j = 0; j < ORD_ITEMS; ++j) {
+                if (cs[j] >= 0) {
+                    order[at] = cs[j];
+                    pos[cs[j]] = (int32_t)at;
+                    ++at;
+                }
+            }
+            placed += total;
+            __syncthreads();
+        }
+        s = e;
+        e = placed;
+        ++levels;
+    }
+    const int64_t reached = e;
+    int64_t placed = e;
+    for (int64_t t0 = 0; t0 < n; t0 += ORD_TILE) {
+        int cnt = 0;
+        for (int j = 0; j < ORD_ITEMS; ++j) {
+            const int64_t r = t0 + (int64_t)tid * ORD_ITEMS + j;
+            if (r < n && pos[r] < 0) ++cnt;
+        }
+        int64_t total;
+        int64_t at = placed + block_exclusive_scan(cnt, s_scan, &total);
+        for (int j = 0; j < ORD_ITEMS; ++j) {
+            const int64_t r = t0 + (int64_t)tid * ORD_ITEMS + j;
+            if (r < n && pos[r] < 0) {
+                order[at] = (int32_t)r;
+                pos[r] = (int32_t)at;
+                ++at;
+            }
+        }
+        placed += total;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        info[0] = levels;
+        info[1] = reached;
+        info[2] = start == ORD_NONE ? -1 : (int64_t)(start & 0xffffffffull);
+    }
+}
+
+// max |pos(c) - pos(r)| over the stored entries (identity numbering when pos is null).
+__global__ void ell_bandwidth_kernel(int64_t rows, int64_t ld, int K, const int32_t *__restrict__ Aj,
+                                     const int32_t *__restrict__ pos, unsigned long long *out)
+{
+    unsigned long long m = 0;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < (int64_t)K * ld;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = idx / ld, r = idx - k * ld;
+        if (r >= rows) continue;
+        const int32_t c = Aj[idx];
+        if (c < 0) continue;
+        const int64_t a = pos ? pos[r] : r, b = pos ? pos[c] : c;
+        const unsigned long long d = (unsigned long long)(a > b ? a - b : b - a);
+        m = d > m ? d : m;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long t = __shfl_down_sync(0xffffffffu, m, o);
+        m = t > m ? t : m;
+    }
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+// B row kk = A row order[kk], slots unchanged; columns renumbered through pos when given.
+template <typename T>
+__global__ void ell_permute_kernel(int64_t rows, int64_t ld, int K, const int32_t *__restrict__ Aj,
+                                   const T *__restrict__ Ax, const int32_t *__restrict__ order,
+                                   const int32_t *__restrict__ pos, int32_t *__restrict__ Bj, T *__restrict__ Bx)
+{
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < (int64_t)K * ld;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = idx / ld, kk = idx - k * ld;
+        int32_t c = -1;
+        T a = T(0);
+        if (kk < rows) {
+            const int64_t src = k * ld + order[kk];
+            c = Aj[src];
+            a = Ax[src];
+            if (pos && c >= 0) c = pos[c];
+        }
+        Bj[idx] = c;
+        Bx[idx] = a;
+    }
+}
+
+// y[order[r]] = sum over B's row r (the rows4 loop of the plain product; x gathered with B's
+// column indices).
+template <typename T, int KT>
+__global__ void __launch_bounds__(ROWS_THREADS)
+ell_spmv_rows_kernel(int64_t rows, int64_t ld, int K, const int32_t *__restrict__ Aj, const T *__restrict__ Ax,
+                     const T *__restrict__ x, const int32_t *__restrict__ order, T *__restrict__ y)
+{
+    const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t r0 = g * 4;
+    if (r0 >= rows) return;
+    T sum[4];
+    hbd::ell_rows4<T, KT>(Aj, Ax, ld, K, r0, [&](int32_t j) { return __ldg(x + j); }, sum);
+    if (r0 + 3 < rows) {
+        const int4 o = __ldg(reinterpret_cast<const int4 *>(order + r0));
+        y[o.x] = sum[0];
+        y[o.y] = sum[1];
+        y[o.z] = sum[2];
+        y[o.w] = sum[3];
+    } else {
+        for (int i = 0; i < 4 && r0 + i < rows; ++i) y[order[r0 + i]] = sum[i];
+    }
+}
+
+// xw[k] = x[order[k]]
+template <typename T>
+__global__ void gather_kernel(int64_t n, const int32_t *__restrict__ order, const T *__restrict__ x, T *__restrict__ xw)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        xw[k] = __ldg(x + __ldg(order + k));
+}
+
+template <typename T>
+int spmv_rows_impl(hb_context *ctx, const hb_ell *B, int dtype, const int32_t *order, const T *x, T *y)
+{
+    if (!ctx) return HB_ERR_INVALID;
+    int st = hb_check_ell(B, dtype);
+    if (st) return st;
+    if (B->rows == 0) return HB_OK;
+    if (!order || !x || !y || ((uintptr_t)order % 16)) return HB_ERR_INVALID;
+    const int64_t groups = (B->rows + 3) / 4;
+    const unsigned blocks = (unsigned)((groups + ROWS_THREADS - 1) / ROWS_THREADS);
+    const T *Bx = (const T *)B->Ax;
+    if (B->K == 9)
+        ell_spmv_rows_kernel<T, 9><<<blocks, ROWS_THREADS, 0, ctx->stream>>>(B->rows, B->ld, 9, B->Aj, Bx, x, order, y);
+    else if (B->K == 4)
+        ell_spmv_rows_kernel<T, 4><<<blocks, ROWS_THREADS, 0, ctx->stream>>>(B->rows, B->ld, 4, B->Aj, Bx, x, order, y);
+    else
+        ell_spmv_rows_kernel<T, 0><<<blocks, ROWS_THREADS, 0, ctx->stream>>>(B->rows, B->ld, (int)B->K, B->Aj, Bx, x,
+                                                                             order, y);
+    return hb_check_launch(ctx, "ell_spmv_rows_kernel");
+}
+
+template <typename T>
+int gather_impl(hb_context *ctx, int64_t n, const int32_t *order, const T *x, T *xw)
+{
+    if (!ctx || n < 0) return HB_ERR_INVALID;
+    if (n == 0) return HB_OK;
+    if (!order || !x || !xw) return HB_ERR_INVALID;
+    const unsigned blocks = (unsigned)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 16);
+    gather_kernel<T><<<blocks, 256, 0, ctx->stream>>>(n, order, x, xw);
+    return hb_check_launch(ctx, "gather_kernel");
+}
+
+}  // namespace
+
+extern "C" {
+
+int hb_ell_cm_order(hb_context *ctx, const hb_ell *A, int32_t *order, int32_t *pos, int64_t *info)
+{
+    HB_RANGE("hb_ell_cm_order");
+    if (!ctx || !A || !order) return HB_ERR_INVALID;
+    if (!A->Aj || A->rows < 0 || A->K < 1 || A->ld < A->rows) return HB_ERR_INVALID;
+    if (A->rows != A->cols) return HB_ERR_SIZE;
+    if (A->rows > INT32_MAX) return HB_ERR_UNSUPPORTED;
+    const int64_t n = A->rows;
+    if (n == 0) {
+        if (info) info[0] = info[1] = 0, info[2] = -1;
+        return HB_OK;
+    }
+    // workspace: key (u64) and, without a caller array, pos (int32)
+    const size_t key_bytes = (size_t)n * 8;
+    const size_t pos_bytes = pos ? 0 : hb_round_up(n * 4, 256);
+    int st = hb_ensure_work(ctx, key_bytes + pos_bytes);
+    if (st) return st;
+    unsigned long long *key = (unsigned long long *)ctx->work;
+    int32_t *p = pos ? pos : (int32_t *)((char *)ctx->work + key_bytes);
+    int64_t *dinfo = (int64_t *)hb_scalars(ctx);
+    cm_order_kernel<<<1, ORD_THREADS, 0, ctx->stream>>>(n, A->ld, (int)A->K, A->Aj, order, p, key, dinfo);
+    st = hb_check_launch(ctx, "cm_order_kernel");
+    if (st) return st;
+    int64_t *h = (int64_t *)ctx->pinned;
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, dinfo, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (info) { info[0] = h[0]; info[1] = h[1]; info[2] = h[2]; }
+    return HB_OK;
+}
+
+int hb_ell_bandwidth(hb_context *ctx, const hb_ell *A, const int32_t *pos, int64_t *bandwidth)
+{
+    HB_RANGE("hb_ell_bandwidth");
+    if (!ctx || !A || !A->Aj || !bandwidth || A->rows < 0 || A->K < 1 || A->ld < A->rows) return HB_ERR_INVALID;
+    unsigned long long *d = (unsigned long long *)hb_scalars(ctx);
+    HB_CUDA_TRY(ctx, cudaMemsetAsync(d, 0, sizeof(*d), ctx->stream));
+    const int64_t total = A->K * A->ld;
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 16));
+    ell_bandwidth_kernel<<<blocks, 256, 0, ctx->stream>>>(A->rows, A->ld, (int)A->K, A->Aj, pos, d);
+    int st = hb_check_launch(ctx, "ell_bandwidth_kernel");
+    if (st) return st;
+    unsigned long long *h = (unsigned long long *)ctx->pinned;
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, d, sizeof(*h), cudaMemcpyDeviceToHost, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    *bandwidth = (int64_t)*h;
+    return HB_OK;
+}
+
+int hb_ell_permute(hb_context *ctx, const hb_ell *A, const int32_t *order, const int32_t *pos, hb_ell *B)
+{
+    HB_RANGE("hb_ell_permute");
+    if (!ctx || !B || !order) return HB_ERR_INVALID;
+    int st = hb_check_ell(A, A ? A->dtype : 0);
+    if (st) return st;
+    if (pos && A->rows != A->cols) return HB_ERR_SIZE;
+    if (B->K != A->K || B->ld != A->ld || B->Aj == A->Aj || B->Ax == A->Ax) return HB_ERR_SIZE;
+    B->rows = A->rows;
+    B->cols = A->cols;
+    B->dtype = A->dtype;
+    st = hb_check_ell(B, A->dtype);
+    if (st) return st;
+    const int64_t total = A->K * A->ld;
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 32));
+    if (A->dtype == HB_F64)
+        ell_permute_kernel<double><<<blocks, 256, 0, ctx->stream>>>(A->rows, A->ld, (int)A->K, A->Aj,
+                                                                    (const double *)A->Ax, order, pos, B->Aj,
+                                                                    (double *)B->Ax);
+    else
+        ell_permute_kernel<float><<<blocks, 256, 0, ctx->stream>>>(A->rows, A->ld, (int)A->K, A->Aj,
+                                                                   (const float *)A->Ax, order, pos, B->Aj,
+                                                                   (float *)B->Ax);
+    return hb_check_launch(ctx, "ell_permute_kernel");
+}
+
+int hb_spmv_rows_f64(hb_context *ctx, const hb_ell *B, const int32_t *order, const double *x, double *y)
+{
+    HB_RANGE("hb_spmv_rows_f64");
+    return spmv_rows_impl<double>(ctx, B, HB_F64, order, x, y);
+}
+
+int hb_spmv_rows_f32(hb_context *ctx, const hb_ell *B, const int32_t *order, const float *x, float *y)
+{
+    HB_RANGE("hb_spmv_rows_f32");
+    return spmv_rows_impl<float>(ctx, B, HB_F32, order, x, y);
+}
+
+int hb_gather_f64(hb_context *ctx, int64_t n, const int32_t *order, const double *x, double *xw)
+{
+    HB_RANGE("hb_gather_f64");
+    return gather_impl<double>(ctx, n, order, x, xw);
+}
+
+int hb_gather_f32(hb_context *ctx, int64_t n, const int32_t *order, const float *x, float *xw)
+{
+    HB_RANGE("hb_gather_f32");
+    return gather_impl<float>(ctx, n, order, x, xw);
+}
+
+}  // extern "C"

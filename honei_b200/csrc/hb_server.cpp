@@ -10,7 +10,10 @@
 //                   cluster launch (HB_BATCH_IR32);
 //   large workers   each owns a context + stream; builds the request's hb_q1 (device-assembled
 //                   matrix + Galerkin hierarchy) and runs the mixed-precision MG-PCG solve;
-//   plain worker    (HB_SERVE_PLAIN_CG64) one request at a time with hb_cg_f64.
+//   plain worker    (HB_SERVE_PLAIN_CG64) one request at a time with hb_cg_f64;
+//   plain batched   (HB_SERVE_PLAIN_CG64_BATCHED) the baseline with the mixed server's
+//                   concurrency: grids up to mid_max_side in batched HB_BATCH_CG64 cluster
+//                   launches, larger ones on large_workers concurrent hb_cg_f64 workers.
 // Requests that arrive while others are on the GPU are admitted as soon as memory frees up, and
 // their work overlaps with the in-flight work on the other streams.  All device memory of a
 // request is stream-ordered (cudaMallocAsync / cudaFreeAsync), so nothing synchronises the
@@ -55,6 +58,7 @@ struct hb_server {
     bool stop = false;
     std::thread admitter;
     std::vector<std::thread> workers;
+    cudaMemPool_t pool = nullptr;
 
     double now() const
     {
@@ -207,6 +211,9 @@ void admit_loop(hb_server *s)
         if (s->p.mode == HB_SERVE_PLAIN_CG64) {
             it->path = HB_PATH_CG64;
             s->large_q.push_back(it);
+        } else if (s->p.mode == HB_SERVE_PLAIN_CG64_BATCHED) {
+            it->path = it->r.M <= s->p.mid_max_side ? HB_PATH_BATCH_CG64 : HB_PATH_CG64;
+            (it->path == HB_PATH_CG64 ? s->large_q : s->small_q).push_back(it);
         } else if (it->r.M <= s->p.small_max_side) {
             it->path = HB_PATH_BATCH;
             s->small_q.push_back(it);
@@ -304,12 +311,13 @@ void small_loop(hb_server *s)
             continue;
         }
         const int64_t count = (int64_t)batch.size();
+        const bool plain = s->p.mode == HB_SERVE_PLAIN_CG64_BATCHED;
         std::vector<DeviceSystem> ds(count, DeviceSystem{w.ctx});
         std::vector<hb_batch_system> sys(count);
         std::vector<int> st(count, HB_OK);
         for (int64_t i = 0; i < count; ++i) {
             const hb_request &r = batch[i]->r;
-            st[i] = ds[i].inputs(r, true, true);
+            st[i] = ds[i].inputs(r, true, !plain);
             if (!st[i]) st[i] = ds[i].rhs(r, ds[i].A64);
             if (!st[i] && cudaMemsetAsync(ds[i].x, 0, r.M * r.M * 8, w.stream) != cudaSuccess) st[i] = HB_ERR_CUDA;
             hb_batch_system &b = sys[i];
@@ -318,7 +326,7 @@ void small_loop(hb_server *s)
             b.A32 = ds[i].A32;
             b.b = ds[i].b;
             b.x = ds[i].x;
-            b.mode = HB_BATCH_IR32;
+            b.mode = plain ? HB_BATCH_CG64 : HB_BATCH_IR32;
             b.max_iters = 1000000;
             b.max_outer = 50;
             b.eps = s->p.eps;
@@ -353,7 +361,7 @@ void small_loop(hb_server *s)
         for (int64_t i = 0; i < count; ++i) {
             hb_completion c{};
             c.tag = batch[i]->r.tag;
-            c.path = HB_PATH_BATCH;
+            c.path = plain ? HB_PATH_BATCH_CG64 : HB_PATH_BATCH;
             c.t_submit = batch[i]->t_submit;
             c.t_admit = batch[i]->t_admit;
             c.bytes = batch[i]->bytes;
@@ -466,7 +474,9 @@ int hb_server_create(const hb_server_params *params, hb_server **out)
 {
     if (!params || !out) return HB_ERR_INVALID;
     *out = nullptr;
-    if (params->mode != HB_SERVE_MIXED && params->mode != HB_SERVE_PLAIN_CG64) return HB_ERR_INVALID;
+    if (params->mode != HB_SERVE_MIXED && params->mode != HB_SERVE_PLAIN_CG64 &&
+        params->mode != HB_SERVE_PLAIN_CG64_BATCHED)
+        return HB_ERR_INVALID;
     if (params->hbm_budget_bytes <= 0) return HB_ERR_INVALID;
     hb_server *s = new hb_server();
     s->p = *params;
@@ -477,8 +487,20 @@ int hb_server_create(const hb_server_params *params, hb_server **out)
     if (s->p.mid_cfg.cluster == 0) s->p.mid_cfg = hb_batch_config{16, 512, 0};
     s->t0 = std::chrono::steady_clock::now();
     s->admitter = std::thread(admit_loop, s);
+    // the pool's high-water marks from here on (hb_server_pool_stats)
+    if (cudaDeviceGetDefaultMemPool(&s->pool, s->p.device) == cudaSuccess) {
+        unsigned long long zero = 0;
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrUsedMemHigh, &zero);
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReservedMemHigh, &zero);
+    } else {
+        cudaGetLastError();
+        s->pool = nullptr;
+    }
     if (s->p.mode == HB_SERVE_PLAIN_CG64) {
         s->workers.emplace_back(large_loop, s);   // one request at a time
+    } else if (s->p.mode == HB_SERVE_PLAIN_CG64_BATCHED) {
+        for (int i = 0; i < s->p.large_workers; ++i) s->workers.emplace_back(large_loop, s);
+        for (int i = 0; i < s->p.small_workers; ++i) s->workers.emplace_back(small_loop, s);
     } else {
         for (int i = 0; i < s->p.large_workers; ++i) s->workers.emplace_back(large_loop, s);
         for (int i = 0; i < s->p.small_workers; ++i) s->workers.emplace_back(small_loop, s);
@@ -539,6 +561,21 @@ int hb_server_stats(hb_server *s, int64_t *in_use, int64_t *peak, int64_t *submi
     if (peak) *peak = s->peak;
     if (submitted) *submitted = s->submitted;
     if (completed) *completed = s->completed;
+    return HB_OK;
+}
+
+int hb_server_pool_stats(hb_server *s, int64_t *used_high, int64_t *reserved_high)
+{
+    if (!s) return HB_ERR_INVALID;
+    if (!s->pool) return HB_ERR_UNSUPPORTED;
+    unsigned long long u = 0, r = 0;
+    if (cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrUsedMemHigh, &u) != cudaSuccess ||
+        cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReservedMemHigh, &r) != cudaSuccess) {
+        cudaGetLastError();
+        return HB_ERR_CUDA;
+    }
+    if (used_high) *used_high = (int64_t)u;
+    if (reserved_high) *reserved_high = (int64_t)r;
     return HB_OK;
 }
 

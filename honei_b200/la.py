@@ -243,6 +243,74 @@ class SparseMatrixELL:
         check(lib().hb_ell_cast_f64_f32(ctx.handle, C.byref(self._s), C.byref(dst)), "hb_ell_cast", ctx.handle)
         return SparseMatrixELL(self._rows, self._cols, self.K, self.ld, Aj, Ax)
 
+    def cm_order(self, ctx: Context | None = None):
+        """(order, pos, info): the Cuthill-McKee locality order of the matrix graph
+        (hb_ell_cm_order); order[k] = the row placed at position k, pos its inverse, info =
+        (levels, rows reached, start row)."""
+        ctx = ctx or default_context()
+        n = self._rows
+        order = torch.empty(max(n, 4), dtype=torch.int32, device=self.Aj.device)
+        pos = torch.empty(max(n, 4), dtype=torch.int32, device=self.Aj.device)
+        info = (C.c_int64 * 3)()
+        check(lib().hb_ell_cm_order(ctx.handle, C.byref(self._s), order.data_ptr(), pos.data_ptr(), info),
+              "hb_ell_cm_order", ctx.handle)
+        return order[:n], pos[:n], tuple(info)
+
+    def bandwidth(self, pos: torch.Tensor | None = None, ctx: Context | None = None) -> int:
+        """max |pos[c] - pos[r]| over the stored entries (the matrix's own numbering by default)."""
+        ctx = ctx or default_context()
+        bw = C.c_int64(0)
+        check(lib().hb_ell_bandwidth(ctx.handle, C.byref(self._s), None if pos is None else pos.data_ptr(),
+                                     C.byref(bw)), "hb_ell_bandwidth", ctx.handle)
+        return bw.value
+
+    def ordered(self, columns: bool = True, ctx: Context | None = None) -> "OrderedMatrixELL":
+        """A copy stored in the Cuthill-McKee locality order, for products with a badly numbered
+        matrix (e.g. a randomly permuted grid).  Product.value on the copy gives y = A x bit for
+        bit.  columns=True renumbers the columns too (local gathers; x is permuted into a work
+        vector first); columns=False keeps A's columns (no work vector; gathers stay scattered,
+        rows that share columns run together)."""
+        ctx = ctx or default_context()
+        order, pos, info = self.cm_order(ctx)
+        Aj = torch.empty_like(self.Aj)
+        Ax = torch.empty_like(self.Ax)
+        B = HbEll(self._rows, self._cols, self.K, self.ld, Aj.data_ptr(), Ax.data_ptr(), _DT[self.dtype], 0)
+        check(lib().hb_ell_permute(ctx.handle, C.byref(self._s), order.data_ptr(),
+                                   pos.data_ptr() if columns else None, C.byref(B)), "hb_ell_permute", ctx.handle)
+        return OrderedMatrixELL(SparseMatrixELL(self._rows, self._cols, self.K, self.ld, Aj, Ax), order, pos,
+                                columns, info)
+
+
+class OrderedMatrixELL:
+    """A SparseMatrixELL stored in a locality order (SparseMatrixELL.ordered): B = the rows of
+    A in `order`, with its columns renumbered through `pos` when `columns`.  Products through it
+    equal A's bit for bit."""
+
+    def __init__(self, B: SparseMatrixELL, order: torch.Tensor, pos: torch.Tensor, columns: bool, info=None):
+        self.B, self.order, self.pos, self.columns_renumbered = B, order, pos, columns
+        self.info = info
+        self.dtype = B.dtype
+        self._xw = None
+
+    def rows(self) -> int:
+        return self.B.rows()
+
+    def columns(self) -> int:
+        return self.B.columns()
+
+    def product(self, y: torch.Tensor, x: torch.Tensor, ctx: Context):
+        suf = _SUF[self.dtype]
+        xp = _vec(x, self.dtype, "x")
+        if self.columns_renumbered:
+            if self._xw is None or self._xw.device != x.device:
+                self._xw = torch.empty(self.B.ld, dtype=self.dtype, device=x.device)
+            check(getattr(lib(), f"hb_gather_{suf}")(ctx.handle, self.B.rows(), self.order.data_ptr(), xp,
+                                                     self._xw.data_ptr()), "hb_gather", ctx.handle)
+            xp = self._xw.data_ptr()
+        check(getattr(lib(), f"hb_spmv_rows_{suf}")(ctx.handle, C.byref(self.B.struct), self.order.data_ptr(), xp,
+                                                    _vec(y, self.dtype, "y")), "Product", ctx.handle)
+        return y
+
 
 class BandedMatrixQ1:
     """BandedMatrixQx<Q1Type, DT> (honei/la/banded_matrix_qx.hh): nine bands of n values in the
@@ -381,6 +449,8 @@ class Product:
         if A.rows() != y.numel():
             raise VectorSizeDoesNotMatch(A.rows(), y.numel())
         ctx = ctx or default_context()
+        if isinstance(A, OrderedMatrixELL):
+            return A.product(y, x, ctx)
         fn = _spmv_fn(A, "spmv")
         check(fn(ctx.handle, C.byref(A.struct), _vec(x, A.dtype, "x"), _vec(y, A.dtype, "y")), "Product", ctx.handle)
         return y

@@ -11,7 +11,13 @@ with a cellwise coefficient and b = A x_true; the server assembles it on the dev
 ``eps`` relative FP64 residual and copies x back into the request's host array.  ``mode="mixed"``
 serves small grids in batched cluster launches (FP32 CG inside FP64 refinement) and large grids on
 MG-preconditioned mixed-precision workers; ``mode="plain"`` is the baseline on the same queue:
-plain FP64 CG, one request at a time.  No reference counterpart: HONEI solves one system per call.
+plain FP64 CG, one request at a time; ``mode="plain_batched"`` is plain FP64 CG with the mixed
+server's concurrency (batched cluster launches up to ``mid_max_side``, concurrent whole-GPU CG
+workers above).  No reference counterpart: HONEI solves one system per call.
+
+Long streams (the 20,000-request configuration) are generated on demand: ``stream_trace`` holds
+only sides, arrival times and seeds, and ``replay_stream`` stages each request's host buffers
+shortly before it is submitted and lets them go once it completes.
 """
 from __future__ import annotations
 
@@ -24,8 +30,9 @@ from . import problems as P
 from ._lib import HBError, lib, status_string
 from .batch import HbBatchConfig
 
-HB_SERVE_MIXED, HB_SERVE_PLAIN_CG64 = 0, 1
-PATHS = {0: "batch", 1: "mgpcg", 2: "cg64", 3: "mgbatch"}
+HB_SERVE_MIXED, HB_SERVE_PLAIN_CG64, HB_SERVE_PLAIN_CG64_BATCHED = 0, 1, 2
+MODES = {"mixed": HB_SERVE_MIXED, "plain": HB_SERVE_PLAIN_CG64, "plain_batched": HB_SERVE_PLAIN_CG64_BATCHED}
+PATHS = {0: "batch", 1: "mgpcg", 2: "cg64", 3: "mgbatch", 4: "batch_cg64"}
 
 
 class HbServerParams(C.Structure):
@@ -57,9 +64,10 @@ def _register():
     L.hb_server_clock.argtypes = [vp]
     L.hb_server_clock.restype = C.c_double
     L.hb_server_stats.argtypes = [vp, P_i64, P_i64, P_i64, P_i64]
+    L.hb_server_pool_stats.argtypes = [vp, P_i64, P_i64]
     L.hb_server_destroy.argtypes = [vp]
     for n in ("hb_server_create", "hb_server_submit", "hb_server_poll", "hb_server_drain", "hb_server_stats",
-              "hb_server_destroy"):
+              "hb_server_pool_stats", "hb_server_destroy"):
         getattr(L, n).restype = C.c_int
     return L
 
@@ -111,25 +119,60 @@ class Trace:
         return int(sum(r.M * r.M for r in self.requests))
 
 
+class StreamTrace:
+    """A serving stream whose requests are generated on demand.  Request i's side, arrival time,
+    coefficient and x_true depend only on (seed, i) and the ranges, so the first k requests of a
+    long stream are the k-request stream of the same seed, and ``request(i)`` always returns the
+    same data."""
+
+    def __init__(self, count: int, rate: float, side_range=(33, 1025), coef_range=(1e-2, 1e2), seed: int = 0,
+                 arrival_seed: int | None = None):
+        rng = np.random.default_rng(seed)
+        lo, hi = side_range
+        sides = np.rint(np.exp(rng.uniform(np.log(lo), np.log(hi), size=count))).astype(np.int64)
+        self.sides = np.clip(sides, lo, hi)
+        arng = np.random.default_rng(seed + 1 if arrival_seed is None else arrival_seed)
+        gaps = arng.exponential(1.0 / rate, size=count) if rate > 0 else np.zeros(count)
+        self.arrivals = np.cumsum(gaps) - (gaps[0] if count else 0.0)
+        self.rate, self.seed = rate, seed
+        self.side_range, self.coef_range = tuple(side_range), tuple(coef_range)
+        self.arrival_seed = arrival_seed
+
+    def __len__(self) -> int:
+        return len(self.sides)
+
+    @property
+    def rows(self) -> int:
+        return int(np.sum(self.sides.astype(np.int64) ** 2))
+
+    def request(self, i: int) -> Request:
+        M = int(self.sides[i])
+        lo, hi = self.coef_range
+        coef = P.log_uniform_coef(M, lo, hi, self.seed * 1000003 + i).ravel()
+        xt = P.uniform_vector(M * M, self.seed * 1000003 + i + 7)
+        return Request(M=M, coef=coef, x_true=xt, arrival=float(self.arrivals[i]), tag=i)
+
+    def prefix(self, k: int) -> "StreamTrace":
+        t = StreamTrace.__new__(StreamTrace)
+        t.__dict__.update(self.__dict__)
+        t.sides, t.arrivals = self.sides[:k], self.arrivals[:k]
+        return t
+
+
+def stream_trace(count: int, rate: float, side_range=(33, 1025), coef_range=(1e-2, 1e2), seed: int = 0,
+                 arrival_seed: int | None = None) -> StreamTrace:
+    """``count`` requests with Poisson-process arrivals of ``rate`` per second (exponential gaps;
+    rate 0: all at once), grid side log-uniform in ``side_range`` (rounded to an integer), a
+    log-uniform cellwise coefficient in ``coef_range`` and x_true uniform in [-1, 1], all from
+    ``seed``; generated on demand."""
+    return StreamTrace(count, rate, side_range, coef_range, seed, arrival_seed)
+
+
 def poisson_trace(count: int, rate: float, side_range=(33, 1025), coef_range=(1e-2, 1e2), seed: int = 0,
                   arrival_seed: int | None = None) -> Trace:
-    """``count`` requests with Poisson-process arrivals of ``rate`` per second (exponential gaps),
-    grid side log-uniform in ``side_range`` (rounded to an integer), a log-uniform cellwise
-    coefficient in ``coef_range`` and x_true uniform in [-1, 1], all from ``seed``."""
-    rng = np.random.default_rng(seed)
-    lo, hi = side_range
-    sides = np.rint(np.exp(rng.uniform(np.log(lo), np.log(hi), size=count))).astype(np.int64)
-    sides = np.clip(sides, lo, hi)
-    arng = np.random.default_rng(seed + 1 if arrival_seed is None else arrival_seed)
-    gaps = arng.exponential(1.0 / rate, size=count) if rate > 0 else np.zeros(count)
-    arrivals = np.cumsum(gaps) - (gaps[0] if count else 0.0)
-    reqs = []
-    for i, M in enumerate(sides):
-        M = int(M)
-        coef = P.log_uniform_coef(M, coef_range[0], coef_range[1], seed * 1000003 + i).ravel()
-        xt = P.uniform_vector(M * M, seed * 1000003 + i + 7)
-        reqs.append(Request(M=M, coef=coef, x_true=xt, arrival=float(arrivals[i]), tag=i))
-    return Trace(reqs, rate, seed, tuple(side_range), tuple(coef_range))
+    """The requests of ``stream_trace(count, rate, ...)``, all generated now."""
+    st = StreamTrace(count, rate, side_range, coef_range, seed, arrival_seed)
+    return Trace([st.request(i) for i in range(count)], rate, seed, tuple(side_range), tuple(coef_range))
 
 
 @dataclass
@@ -165,7 +208,7 @@ class Server:
                  mid_cluster: int = 16, mid_threads: int = 512, mid_max_clusters: int = 0):
         self._lib = _register()
         prm = HbServerParams()
-        prm.mode = {"mixed": HB_SERVE_MIXED, "plain": HB_SERVE_PLAIN_CG64}[mode]
+        prm.mode = MODES[mode]
         prm.device = device
         prm.hbm_budget_bytes = int(budget_bytes)
         prm.large_workers = large_workers
@@ -238,7 +281,11 @@ class Server:
     def stats(self) -> dict:
         v = [C.c_int64() for _ in range(4)]
         self._lib.hb_server_stats(self.handle, *[C.byref(x) for x in v])
-        return dict(zip(("bytes_in_use", "bytes_peak", "submitted", "completed"), (x.value for x in v)))
+        out = dict(zip(("bytes_in_use", "bytes_peak", "submitted", "completed"), (x.value for x in v)))
+        u, r = C.c_int64(), C.c_int64()
+        if self._lib.hb_server_pool_stats(self.handle, C.byref(u), C.byref(r)) == 0:
+            out["pool_used_high"], out["pool_reserved_high"] = u.value, r.value
+        return out
 
     def close(self):
         if self.handle:
@@ -282,6 +329,113 @@ def replay(server: Server, trace: Trace, realtime: bool = True) -> dict:
         server.submit(req, st)
     done += server.drain()
     return summarise(done)
+
+
+def replay_stream(server: Server, trace: StreamTrace, realtime: bool = True, window: int = 512,
+                  lookahead: int = 256, producers: int = 4, keep_x: bool = False) -> dict:
+    """Serves a stream that is generated while it runs.  Producer threads build and stage request
+    i (its host buffers, page-locked when the server is) ahead of its turn, at most
+    ``lookahead`` requests ahead.  With ``realtime`` the requests are submitted at their arrival
+    times (open loop; a request staged late is submitted late, and its latency counts from its
+    scheduled arrival); without it, as fast as the server takes them with at most ``window``
+    requests outstanding (closed loop: the server's capacity).  A request's host buffers are
+    released when its completion is collected (its solution too, unless ``keep_x``)."""
+    import threading
+
+    n = len(trace)
+    ready: dict = {}
+    cv = threading.Condition()
+    state = {"next": 0, "submitted": 0, "stop": False, "error": None}
+
+    def produce():
+        try:
+            while True:
+                with cv:
+                    cv.wait_for(lambda: state["stop"] or state["next"] >= n
+                                or state["next"] < state["submitted"] + lookahead)
+                    if state["stop"] or state["next"] >= n:
+                        return
+                    i = state["next"]
+                    state["next"] += 1
+                req = trace.request(i)
+                staged = server.stage(req)
+                req.coef = req.x_true = None          # the staged copies are what the server reads
+                with cv:
+                    ready[i] = (req, staged)
+                    cv.notify_all()
+        except BaseException as e:  # reported by the submitting thread
+            with cv:
+                state["error"] = e
+                state["stop"] = True
+                cv.notify_all()
+
+    threads = [threading.Thread(target=produce, daemon=True) for _ in range(max(1, producers))]
+    for t in threads:
+        t.start()
+    done, lag_max = [], 0.0
+    outstanding = 0
+
+    def collect(wait_ms):
+        nonlocal outstanding
+        got = server.poll(256, wait_ms=wait_ms)
+        for c in got:
+            if not keep_x:
+                c.x = None
+        outstanding -= len(got)
+        done.extend(got)
+
+    t_base = server.clock()
+    sched = {}
+    try:
+        for i in range(n):
+            with cv:
+                cv.wait_for(lambda: i in ready or state["stop"])
+                if state["error"] is not None:
+                    raise state["error"]
+                req, staged = ready.pop(i)
+            if realtime:
+                target = t_base + float(trace.arrivals[i])
+                while True:
+                    lag = target - server.clock()
+                    if lag <= 0:
+                        break
+                    collect(max(0, min(int(lag * 1000), 20)))
+                    if lag < 0.001:
+                        while server.clock() < target:
+                            pass
+                        break
+                sched[req.tag] = target
+            else:
+                while outstanding >= window:
+                    collect(20)
+            server.submit(req, staged)
+            outstanding += 1
+            if realtime:
+                lag_max = max(lag_max, server.clock() - sched[req.tag])
+            with cv:
+                state["submitted"] = i + 1
+                cv.notify_all()
+            if outstanding and i % 16 == 0:
+                collect(0)
+    finally:
+        with cv:
+            state["stop"] = True
+            cv.notify_all()
+        for t in threads:
+            t.join()
+    rest = server.drain()
+    for c in rest:
+        if not keep_x:
+            c.x = None
+    done.extend(rest)
+    if realtime:
+        # latency from the scheduled arrival (covers a late submission)
+        for c in done:
+            c.t_submit = min(c.t_submit, sched.get(c.tag, c.t_submit))
+    out = summarise(done)
+    out["submit_lag_max_ms"] = lag_max * 1e3
+    out["mode"] = "open loop (arrival times)" if realtime else f"closed loop, {window} outstanding"
+    return out
 
 
 def summarise(done: list) -> dict:

@@ -106,6 +106,34 @@ int hb_ell_validate(hb_context *ctx, const hb_ell *A, int64_t *bad_slots);
 /* Same pattern, values cast to float (for the FP32 inner solves of mixed precision). */
 int hb_ell_cast_f64_f32(hb_context *ctx, const hb_ell *src, hb_ell *dst);
 
+/* Locality order of a square device ELL matrix.  No reference counterpart: the reference
+ * multiplies in the row order the matrix has (Product<Tag> on SparseMatrixELL,
+ * honei/la/product.hh:148-204).  A Cuthill-McKee breadth-first order of the matrix graph (row ->
+ * its columns): from the row with the fewest off-diagonal entries (lowest index on ties), each
+ * level's newly reached rows in the order of the first row reaching them, then by slot; rows
+ * never reached follow in ascending order.  order: device int32[rows], order[k] = the row at
+ * position k; pos: device int32[rows] or NULL, pos[order[k]] = k.  info (host int64[3], may be
+ * NULL): levels, rows reached, start row.  Uses the context workspace (8 bytes per row, 12
+ * without pos) and synchronises the stream.  Deterministic. */
+int hb_ell_cm_order(hb_context *ctx, const hb_ell *A, int32_t *order, int32_t *pos, int64_t *info);
+/* max |pos[c] - pos[r]| over A's stored entries (r, c); pos NULL = A's own numbering.
+ * Synchronises the stream. */
+int hb_ell_bandwidth(hb_context *ctx, const hb_ell *A, const int32_t *pos, int64_t *bandwidth);
+/* B = A's rows in `order` (B row k = A row order[k], its slots in their order): with pos NULL
+ * the columns stay A's; with pos the columns are renumbered (B = P A P^T, square A).  B has A's
+ * K and ld and its own arrays (caller-allocated). */
+int hb_ell_permute(hb_context *ctx, const hb_ell *A, const int32_t *order, const int32_t *pos, hb_ell *B);
+/* Product through a row-reordered copy B (hb_ell_permute): y[order[k]] = sum over B's row k of
+ * B(k, j) x[j].  With B's columns A's own (pos NULL above), x is A's x and y = A x bit for bit
+ * (each row's sum is the same as Product<tags::CPU>'s).  With renumbered columns, x must be
+ * gathered first (hb_gather: xw[k] = x[order[k]]); y is then again A x, bit for bit.  order
+ * must be 16-byte aligned.  Asynchronous. */
+int hb_spmv_rows_f64(hb_context *ctx, const hb_ell *B, const int32_t *order, const double *x, double *y);
+int hb_spmv_rows_f32(hb_context *ctx, const hb_ell *B, const int32_t *order, const float *x, float *y);
+/* xw[k] = x[order[k]], k < n.  Asynchronous. */
+int hb_gather_f64(hb_context *ctx, int64_t n, const int32_t *order, const double *x, double *xw);
+int hb_gather_f32(hb_context *ctx, int64_t n, const int32_t *order, const float *x, float *xw);
+
 /* SPAI2<tags::GPU::CUDA>::value(M, A) (honei/math/spai2.hh:294-298; wrapper
  * honei/math/spai2-cuda.cc:180-228): the sparse approximate inverse of the square matrix A with
  * A's pattern, bit-identical to SPAI2<tags::CPU::SSE> (honei/math/spai2.hh:129-260): for every
@@ -193,6 +221,14 @@ int hb_spmv_f32(hb_context *ctx, const hb_ell *A, const float *x, float *y);
  * cuda_defect_smell_dv_{float,double} (honei/backends/cuda/defect.cu:367-416).
  * Bit-identical to Defect<tags::CPU> (honei/math/defect.hh:357-383). */
 int hb_defect_f64(hb_context *ctx, const hb_ell *A, const double *b, const double *x, double *r);
+/* RISmoother<tags::GPU::CUDA>::value(A, P, b, x, temp_vecs, sweeps) (honei/math/ri.hh:97-133)
+ * with a vector P: `sweeps` times x = x + P (b - A x), each sweep one fused kernel rounding as
+ * Defect, Product(P, .) and Sum do (bit-identical to tags::CPU).  tmp: a device vector of rows
+ * entries other than x (the sweep reads x while it writes).  Asynchronous. */
+int hb_jacobi_sweeps_f64(hb_context *ctx, const hb_ell *A, const double *P, const double *b, double *x, double *tmp,
+                         int64_t sweeps);
+int hb_jacobi_sweeps_f32(hb_context *ctx, const hb_ell *A, const float *P, const float *b, float *x, float *tmp,
+                         int64_t sweeps);
 int hb_defect_f32(hb_context *ctx, const hb_ell *A, const float *b, const float *x, float *r);
 
 /* BandedMatrixQx<Q1Type, DT> (honei/la/banded_matrix_qx.hh:44-129): the nine-band matrix of a
@@ -386,6 +422,16 @@ int hb_mg_set_params(hb_mg *mg, const hb_mg_params *params);
  * rnorm_host[2] = {initial, final} defect norms (may be NULL). */
 int hb_mg_solve_f64(hb_mg *mg, const double *b, double *x, int64_t *used_cycles, double *rnorm_host);
 int hb_mg_solve_f32(hb_mg *mg, const float *b, float *x, int64_t *used_cycles, float *rnorm_host);
+/* One V-cycle on the finest level, x updated in place: what one OperatorList::value() call of
+ * the cycle MGCycleCreation<Tag, V::STATIC, CGSolver<NONE>, RISmoother, Restriction<PROLMAT>,
+ * Prolongation<PROLMAT>> builds does (honei/math/mg.hh:567-662).  Asynchronous. */
+int hb_mg_cycle_f64(hb_mg *mg, const double *b, double *x);
+int hb_mg_cycle_f32(hb_mg *mg, const float *b, float *x);
+/* The smoother vector of one level (0 = coarsest) taken from the caller (device, rows entries,
+ * the hierarchy's dtype), in place of damping / diag(A): MGData's P[l] as PreconFill built it
+ * (honei/math/mg.hh:255-286).  A later hb_mg_set_params that changes the damping recomputes
+ * damping / diag(A). */
+int hb_mg_set_smoother(hb_mg *mg, int level, const void *P);
 
 /* Mixed precision iterative refinement, IRSolver<Outer=double, Inner=float>,
  * honei/math/ir.hh:30-78: FP64 defect b - A x, convergence norm and solution update on the
@@ -526,14 +572,16 @@ int hb_q1_batch_solve(hb_context *ctx, hb_q1 *const *systems, const double *cons
  * grids in batched MG-preconditioned cluster launches (hb_q1_batch_solve), large grids on
  * MG-preconditioned mixed-precision workers (hb_q1_solve), each on its own stream --
  * while new requests keep arriving (continuous batching).  A request's result does not depend
- * on what it was served with.  HB_SERVE_PLAIN_CG64 is the baseline on the same queue: one
- * request at a time, plain FP64 CG (hb_cg_f64) on the whole GPU.
+ * on what it was served with.  Two baselines run on the same queue: HB_SERVE_PLAIN_CG64, one
+ * request at a time, plain FP64 CG (hb_cg_f64) on the whole GPU; and HB_SERVE_PLAIN_CG64_BATCHED,
+ * plain FP64 CG with the mixed server's concurrency -- grids up to mid_max_side in batched
+ * cluster launches (HB_BATCH_CG64), larger grids on large_workers concurrent hb_cg_f64 streams.
  * ---------------------------------------------------------------------------------------- */
-enum { HB_SERVE_MIXED = 0, HB_SERVE_PLAIN_CG64 = 1 };
-enum { HB_PATH_BATCH = 0, HB_PATH_MGPCG = 1, HB_PATH_CG64 = 2, HB_PATH_MGBATCH = 3 };
+enum { HB_SERVE_MIXED = 0, HB_SERVE_PLAIN_CG64 = 1, HB_SERVE_PLAIN_CG64_BATCHED = 2 };
+enum { HB_PATH_BATCH = 0, HB_PATH_MGPCG = 1, HB_PATH_CG64 = 2, HB_PATH_MGBATCH = 3, HB_PATH_BATCH_CG64 = 4 };
 
 typedef struct {
-    int32_t mode;               /* HB_SERVE_MIXED or HB_SERVE_PLAIN_CG64                      */
+    int32_t mode;               /* HB_SERVE_MIXED, HB_SERVE_PLAIN_CG64 or _PLAIN_CG64_BATCHED  */
     int32_t device;
     int64_t hbm_budget_bytes;   /* admission limit for resident request state                  */
     int32_t large_workers;      /* concurrent MG-PCG solves (one stream each)                  */
@@ -584,6 +632,10 @@ int hb_server_drain(hb_server *s);
 double hb_server_clock(hb_server *s);
 /* in_use / peak resident bytes, requests submitted / completed. */
 int hb_server_stats(hb_server *s, int64_t *bytes_in_use, int64_t *bytes_peak, int64_t *submitted, int64_t *completed);
+/* What the device's stream-ordered memory pool (which holds every request's device memory)
+ * actually used and reserved at its highest since the server started, against the admission
+ * charges above.  Counts every stream-ordered allocation of the process on that device. */
+int hb_server_pool_stats(hb_server *s, int64_t *used_high, int64_t *reserved_high);
 int hb_server_destroy(hb_server *s);
 
 #if defined(__GNUC__)

@@ -289,6 +289,43 @@ class Oracle:
         return Mx
 
 
+class RefEllHandle:
+    """The reference's SparseMatrixELL<double> and input vector, built once (ref_ell_create_f64);
+    ``spmv(tag, reps)`` runs Product<tag> reps times and returns the per-product seconds."""
+
+    def __init__(self, R, A, x):
+        self.R = R
+        L = R.lib
+        ul = _c.c_ulong
+        L.ref_ell_create_f64.argtypes = [ul] * 5 + [_vp, _vp, _vp, _c.POINTER(_vp)]
+        L.ref_ell_spmv_f64.argtypes = [_c.c_int, _vp, _c.c_int, _vp, _vp]
+        L.ref_ell_destroy.argtypes = [_vp]
+        self.rows = A.rows
+        h = _vp()
+        x = np.ascontiguousarray(x, np.float64)
+        R._check(L.ref_ell_create_f64(A.rows, A.cols, A.stride, A.ncpr, A.threads, _ptr(A.Aj), _ptr(A.Ax),
+                                      _ptr(x), _c.byref(h)))
+        self.h = h
+
+    def spmv(self, tag="mc-sse", reps=1, want_y=False):
+        sec = np.zeros(max(reps, 1))
+        y = np.zeros(self.rows) if want_y else None
+        self.R._check(self.R.lib.ref_ell_spmv_f64(TAGS[tag], self.h, reps, _ptr(sec),
+                                                  _ptr(y) if want_y else None))
+        return (sec[:reps], y) if want_y else sec[:reps]
+
+    def close(self):
+        if self.h:
+            self.R.lib.ref_ell_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Reference:
     """The reference's own CPU path (unmodified HONEI sources + ref_shim.cc)."""
 
@@ -319,17 +356,22 @@ class Reference:
         L.ref_set_threads.argtypes = [_c.c_int]
         mg_args = [_c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
         L.ref_mg_f64.argtypes = mg_args + [_c.c_double, ul, ul, ul, ul, _c.c_double,
-                                           _c.POINTER(ul), _c.POINTER(_c.c_double)]
+                                           _c.POINTER(ul), _c.POINTER(_c.c_double), _vp, _vp, _vp]
         L.ref_mg_f32.argtypes = mg_args + [_c.c_float, ul, ul, ul, ul, _c.c_float,
-                                           _c.POINTER(ul), _c.POINTER(_c.c_double)]
+                                           _c.POINTER(ul), _c.POINTER(_c.c_double), _vp, _vp, _vp]
         L.ref_q1band_spmv_f64.argtypes = [_c.c_int, ul, _vp, _vp, _vp, _c.c_int, _c.POINTER(_c.c_double)]
         L.ref_q1band_spmv_f32.argtypes = L.ref_q1band_spmv_f64.argtypes
         L.ref_q1band_defect_f64.argtypes = [ul, _vp, _vp, _vp, _vp]
         L.ref_q1band_poisson_f64.argtypes = [ul, _vp]
         L.ref_q1band_from_ell_f64.argtypes = [_vp, _vp, _vp, _vp]
-        L.ref_ir_mg.argtypes = [_c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+        L.ref_ir_mg.argtypes = [_c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                 _c.c_float, ul, ul, ul, ul, _c.c_float, _c.c_double, ul,
-                                _c.POINTER(ul), _c.POINTER(_c.c_double)]
+                                _c.POINTER(ul), _c.POINTER(_c.c_double), _vp, _vp, _vp]
+
+    def ell_handle(self, A, x):
+        """A SparseMatrixELL<double> built once from A with the input vector x, for timing
+        products alone: returns a RefEllHandle."""
+        return RefEllHandle(self, A, x)
 
     def _check(self, rc):
         if self._mask is not None:
@@ -583,6 +625,16 @@ class Reference:
                                                       max_iters, eps, _c.byref(used), _c.byref(sec)))
         return x, used.value, sec.value
 
+    @staticmethod
+    def _res_arrays(H):
+        """The restriction matrices H.res (Res_l = Prol_l^T, the entries of each row in
+        ascending column order, as the reference's Transposition gives them)."""
+        n = max(len(H.res), 1)
+        rinfo = np.array([r.info() for r in H.res] or [[0] * 5], np.uint64).ravel()
+        Rj = (_vp * n)(*[r.Aj.ctypes.data for r in H.res])
+        Rx = (_vp * n)(*[r.Ax.ctypes.data for r in H.res])
+        return rinfo, Rj, Rx
+
     def _mg_arrays(self, H):
         L = len(H.A)
         ainfo = np.array([a.info() for a in H.A], np.uint64).ravel()
@@ -602,13 +654,15 @@ class Reference:
         x = np.zeros(H.A[-1].rows, dt) if x0 is None else np.array(x0, dt)
         used = _c.c_ulong(0)
         sec = _c.c_double(0)
+        rinfo, Rj, Rx = self._res_arrays(H)
         self._check(getattr(self.lib, f"ref_mg_{s}")(TAGS[tag], L, _ptr(ainfo), Aj, Ax, _ptr(pinfo), Pj, Px,
                                                       _ptr(b), _ptr(x), damping, max_iters, max_iters_coarse,
-                                                      n_pre, n_post, eps, _c.byref(used), _c.byref(sec)))
+                                                      n_pre, n_post, eps, _c.byref(used), _c.byref(sec),
+                                                      _ptr(rinfo) if len(H.res) else None, Rj, Rx))
         return x, used.value, sec.value
 
     def ir_mg(self, H64, H32, b, x0=None, damping=0.7, eps=1e-10, inner_eps=1e-3, max_iters=100,
-              inner_max_iters=100, max_iters_coarse=1000, n_pre=2, n_post=2):
+              inner_max_iters=100, max_iters_coarse=1000, n_pre=2, n_post=2, tag="cpu"):
         L, ainfo, pinfo, Aj, Ax64, Pj, _ = self._mg_arrays(H64)
         Ax32 = (_vp * L)(*[a.Ax.ctypes.data for a in H32.A])
         Px32 = (_vp * max(L - 1, 1))(*[p.Ax.ctypes.data for p in H32.prol])
@@ -616,7 +670,10 @@ class Reference:
         x = np.zeros(H64.A[-1].rows) if x0 is None else np.array(x0, np.float64)
         used = _c.c_ulong(0)
         sec = _c.c_double(0)
-        self._check(self.lib.ref_ir_mg(L, _ptr(ainfo), Aj, Ax64, Ax32, _ptr(pinfo), Pj, Px32, _ptr(b),
+        rinfo, Rj, _ = self._res_arrays(H64)
+        Rx32 = (_vp * max(len(H32.res), 1))(*[r.Ax.ctypes.data for r in H32.res])
+        self._check(self.lib.ref_ir_mg(TAGS[tag], L, _ptr(ainfo), Aj, Ax64, Ax32, _ptr(pinfo), Pj, Px32, _ptr(b),
                                        _ptr(x), damping, inner_max_iters, max_iters_coarse, n_pre, n_post,
-                                       inner_eps, eps, max_iters, _c.byref(used), _c.byref(sec)))
+                                       inner_eps, eps, max_iters, _c.byref(used), _c.byref(sec),
+                                       _ptr(rinfo) if len(H64.res) else None, Rj, Rx32))
         return x, used.value, sec.value

@@ -198,11 +198,14 @@ namespace
 
     // Builds MGData exactly as MGUtil::load_data (mg.hh:442-547) does from files, but from
     // arrays: A_l, Prol_l from the caller; P_l = PreconFill "jac" = damping / diag(A_l)
-    // (mg.hh:255-286); Res_l = Transposition(Prol_l) (mg.hh:496).
+    // (mg.hh:255-286); Res_l = Transposition(Prol_l) (mg.hh:496), or -- when the caller passes
+    // them (rinfo non-null) -- the transposes it computed already (the same entries in the same
+    // row order; HONEI's Transposition of a 2049^2 prolongation takes tens of seconds).
     template <typename DT_> MGData<SparseMatrixELL<DT_>, DenseVector<DT_>, SparseMatrixELL<DT_>, DenseVector<DT_>, DT_>
     mg_data_from(int nlevels, const unsigned long * ainfo, const uint64_t * const * Aj, const DT_ * const * Ax,
             const unsigned long * pinfo, const uint64_t * const * Pj, const DT_ * const * Px,
-            const DT_ * b, const DT_ * x0, DT_ damping)
+            const DT_ * b, const DT_ * x0, DT_ damping, const unsigned long * rinfo = nullptr,
+            const uint64_t * const * Rj = nullptr, const DT_ * const * Rx = nullptr)
     {
         MGLevels<DT_> L;
         for (int i(0) ; i < nlevels ; ++i)
@@ -216,7 +219,13 @@ namespace
                 const unsigned long * pi(pinfo + 5 * i);
                 SparseMatrixELL<DT_> p(ell_from(pi[0], pi[1], pi[2], pi[3], pi[4], Pj[i], Px[i]));
                 L.prol.push_back(p);
-                L.res.push_back(Transposition<tags::CPU>::value(p.copy()));
+                if (rinfo)
+                {
+                    const unsigned long * ri(rinfo + 5 * i);
+                    L.res.push_back(ell_from(ri[0], ri[1], ri[2], ri[3], ri[4], Rj[i], Rx[i]));
+                }
+                else
+                    L.res.push_back(Transposition<tags::CPU>::value(p.copy()));
             }
             const unsigned long n(ai[0]);
             DenseVector<DT_> zero(n, DT_(0));
@@ -245,6 +254,17 @@ namespace
         OperatorList cycle(MGCycleCreation<T_, methods::CYCLE::V::STATIC, CGSolver<T_, methods::NONE>, RISmoother<T_>,
                 Restriction<T_, methods::PROLMAT>, Prolongation<T_, methods::PROLMAT>, DT_>::value(data));
         MGSolver<T_, Norm<vnt_l_two, true, T_> >::value(data, cycle);
+    }
+
+    // IRSolver<T_, T_> (honei/math/ir.hh:30-78): FP64 outer loop around the FP32 V-cycle of data.
+    template <typename T_> void ir_mg_run(SparseMatrixELL<double> & A, DenseVector<double> & b,
+            DenseVector<double> & x,
+            MGData<SparseMatrixELL<float>, DenseVector<float>, SparseMatrixELL<float>, DenseVector<float>, float> & data,
+            double eps, unsigned long max_iters, unsigned long & used)
+    {
+        OperatorList cycle(MGCycleCreation<T_, methods::CYCLE::V::STATIC, CGSolver<T_, methods::NONE>, RISmoother<T_>,
+                Restriction<T_, methods::PROLMAT>, Prolongation<T_, methods::PROLMAT>, float>::value(data));
+        IRSolver<T_, T_, Norm<vnt_l_two, true, T_> >::value(A, b, x, data, cycle, eps, max_iters, used);
     }
 
     // MGSolver prints its initial and final norm to stdout (mg.hh:1107,1125); keep the
@@ -634,6 +654,43 @@ extern "C"
             int reps, double * seconds)
     { return spmv_impl<float>(tag, rows, cols, stride, ncpr, threads, Aj, Ax, x, y, reps, seconds); }
 
+    // A reference SparseMatrixELL<double> built once and kept (the product benchmark's set-up,
+    // honei/benchmark/product_ell_file_BENCHMARK.cc:57-92), then Product<tag> on it `reps`
+    // times: the wall time of every product into seconds[0..reps).
+    struct RefEll
+    {
+        SparseMatrixELL<double> A;
+        DenseVector<double> x, y;
+        RefEll(SparseMatrixELL<double> a, DenseVector<double> xv) : A(a), x(xv), y(a.rows(), 0.) {}
+    };
+
+    int ref_ell_create_f64(unsigned long rows, unsigned long cols, unsigned long stride, unsigned long ncpr,
+            unsigned long threads, const uint64_t * Aj, const double * Ax, const double * x, void ** out)
+    {
+        return guarded([&]() {
+            *out = new RefEll(ell_from<double>(rows, cols, stride, ncpr, threads, Aj, Ax), dv_from(x, cols));
+        });
+    }
+
+    int ref_ell_spmv_f64(int tag, void * h, int reps, double * seconds, double * y)
+    {
+        return guarded([&]() {
+            RefEll & e(*static_cast<RefEll *>(h));
+            for (int r(0) ; r < reps ; ++r)
+            {
+                double t0(now_s());
+                REF_DISPATCH(tag, (Product<T_>::value(e.y, e.A, e.x)));
+                if (seconds) seconds[r] = now_s() - t0;
+            }
+            if (y) dv_to(e.y, y);
+        });
+    }
+
+    int ref_ell_destroy(void * h)
+    {
+        return guarded([&]() { delete static_cast<RefEll *>(h); });
+    }
+
     int ref_defect_f64(int tag, unsigned long rows, unsigned long cols, unsigned long stride, unsigned long ncpr,
             unsigned long threads, const uint64_t * Aj, const double * Ax, const double * b, const double * x, double * r)
     { return defect_impl<double>(tag, rows, cols, stride, ncpr, threads, Aj, Ax, b, x, r); }
@@ -683,12 +740,13 @@ extern "C"
             const double * const * Ax, const unsigned long * pinfo, const uint64_t * const * Pj,
             const double * const * Px, const double * b, double * x, double damping,
             unsigned long max_iters, unsigned long max_iters_coarse, unsigned long n_pre, unsigned long n_post,
-            double eps, unsigned long * used, double * seconds)
+            double eps, unsigned long * used, double * seconds, const unsigned long * rinfo,
+            const uint64_t * const * Rj, const double * const * Rx)
     {
         return guarded([&]() {
             MuteCout mute;
             MGData<SparseMatrixELL<double>, DenseVector<double>, SparseMatrixELL<double>, DenseVector<double>, double>
-                data(mg_data_from<double>(nlevels, ainfo, Aj, Ax, pinfo, Pj, Px, b, x, damping));
+                data(mg_data_from<double>(nlevels, ainfo, Aj, Ax, pinfo, Pj, Px, b, x, damping, rinfo, Rj, Rx));
             MGUtil<tags::CPU, SparseMatrixELL<double>, DenseVector<double>, SparseMatrixELL<double>, DenseVector<double>,
                 MatrixIO<io_formats::ELL>, VectorIO<io_formats::EXP>, double>::configure(
                         data, max_iters, max_iters_coarse, n_pre, n_post, 1, eps);
@@ -704,12 +762,13 @@ extern "C"
             const float * const * Ax, const unsigned long * pinfo, const uint64_t * const * Pj,
             const float * const * Px, const float * b, float * x, float damping,
             unsigned long max_iters, unsigned long max_iters_coarse, unsigned long n_pre, unsigned long n_post,
-            float eps, unsigned long * used, double * seconds)
+            float eps, unsigned long * used, double * seconds, const unsigned long * rinfo,
+            const uint64_t * const * Rj, const float * const * Rx)
     {
         return guarded([&]() {
             MuteCout mute;
             MGData<SparseMatrixELL<float>, DenseVector<float>, SparseMatrixELL<float>, DenseVector<float>, float>
-                data(mg_data_from<float>(nlevels, ainfo, Aj, Ax, pinfo, Pj, Px, b, x, damping));
+                data(mg_data_from<float>(nlevels, ainfo, Aj, Ax, pinfo, Pj, Px, b, x, damping, rinfo, Rj, Rx));
             MGUtil<tags::CPU, SparseMatrixELL<float>, DenseVector<float>, SparseMatrixELL<float>, DenseVector<float>,
                 MatrixIO<io_formats::ELL>, VectorIO<io_formats::EXP>, float>::configure(
                         data, max_iters, max_iters_coarse, n_pre, n_post, 1, eps);
@@ -723,31 +782,30 @@ extern "C"
 
     // IRSolver<tags::CPU, tags::CPU, Norm<l2, true>> (ir.hh:30-78): FP64 outer defect/update
     // around the FP32 MG above.  The inner data keeps its x between outer steps, as ir.hh does.
-    int ref_ir_mg(int nlevels, const unsigned long * ainfo, const uint64_t * const * Aj,
+    int ref_ir_mg(int tag, int nlevels, const unsigned long * ainfo, const uint64_t * const * Aj,
             const double * const * Ax64, const float * const * Ax32, const unsigned long * pinfo,
             const uint64_t * const * Pj, const float * const * Px32, const double * b, double * x,
             float damping, unsigned long inner_max_iters, unsigned long max_iters_coarse,
             unsigned long n_pre, unsigned long n_post, float inner_eps, double eps,
-            unsigned long max_iters, unsigned long * used, double * seconds)
+            unsigned long max_iters, unsigned long * used, double * seconds, const unsigned long * rinfo,
+            const uint64_t * const * Rj, const float * const * Rx32)
     {
         return guarded([&]() {
             MuteCout mute;
             const unsigned long n(ainfo[5 * (nlevels - 1)]);
             std::vector<float> zero(n, 0.f);
             MGData<SparseMatrixELL<float>, DenseVector<float>, SparseMatrixELL<float>, DenseVector<float>, float>
-                data(mg_data_from<float>(nlevels, ainfo, Aj, Ax32, pinfo, Pj, Px32, zero.data(), zero.data(), damping));
+                data(mg_data_from<float>(nlevels, ainfo, Aj, Ax32, pinfo, Pj, Px32, zero.data(), zero.data(), damping,
+                        rinfo, Rj, Rx32));
             MGUtil<tags::CPU, SparseMatrixELL<float>, DenseVector<float>, SparseMatrixELL<float>, DenseVector<float>,
                 MatrixIO<io_formats::ELL>, VectorIO<io_formats::EXP>, float>::configure(
                         data, inner_max_iters, max_iters_coarse, n_pre, n_post, 1, inner_eps);
-            OperatorList cycle(MGCycleCreation<tags::CPU, methods::CYCLE::V::STATIC, CGSolver<tags::CPU, methods::NONE>,
-                    RISmoother<tags::CPU>, Restriction<tags::CPU, methods::PROLMAT>, Prolongation<tags::CPU, methods::PROLMAT>,
-                    float>::value(data));
             const unsigned long * ai(ainfo + 5 * (nlevels - 1));
             SparseMatrixELL<double> A(ell_from(ai[0], ai[1], ai[2], ai[3], ai[4], Aj[nlevels - 1], Ax64[nlevels - 1]));
             DenseVector<double> bv(dv_from(b, n)), xv(dv_from(x, n));
             unsigned long u(0);
             double t0(now_s());
-            IRSolver<tags::CPU, tags::CPU, Norm<vnt_l_two, true, tags::CPU> >::value(A, bv, xv, data, cycle, eps, max_iters, u);
+            REF_DISPATCH(tag, (ir_mg_run<T_>(A, bv, xv, data, eps, max_iters, u)));
             if (seconds) *seconds = now_s() - t0;
             *used = u;
             dv_to(xv, x);

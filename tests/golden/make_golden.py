@@ -36,7 +36,14 @@ readers, honei/math/matrix_io.hh and honei/math/vector_io.hh):
   FP64 and FP32, each with the reference's stored A_*_spai.ell beside it (pcg.npz for the
   last), and of the reference's Q1 33^2 construction.
 
-    python tests/golden/make_golden.py [/path/to/honei-tree] [--only q1band|pcg|csr|spai2]
+* batch512.npz -- the 512-system batch workload (SPD Q1 systems, side U{17..257} from seed 2024,
+  cellwise coefficient 10^U(-1,1) with seed 2024 + i, x_true U[-1,1] with seed 2024 + i + 1,
+  b = A x_true): for every system, the iteration count and final true relative residual of
+  CGSolver<tags::CPU, NONE> and of CGSolver<tags::CPU::SSE, NONE> (eps 1e-8, x0 = 0).  The two
+  tags differ only in the summation order of their dot products; their spread is the measured
+  sensitivity of these solves to that order.  Needs only oracle/_ref (no HONEI tree).
+
+    python tests/golden/make_golden.py [/path/to/honei-tree] [--only q1band|pcg|csr|spai2|batch512]
 """
 from __future__ import annotations
 
@@ -205,7 +212,7 @@ def main(tree: str, only: str | None = None) -> None:
     R = Reference()
     if only is not None:
         {"q1band": lambda R: banded(R), "pcg": lambda R: pcg(R, tree), "csr": lambda R: csr(R),
-         "spai2": lambda R: spai2(R, tree)}[only](R)
+         "spai2": lambda R: spai2(R, tree), "batch512": lambda R: batch512(R)}[only](R)
         print("golden fixture", only, "written to", HERE)
         return
     td = os.path.join(tree, "honei", "math", "testdata")
@@ -299,6 +306,36 @@ def main(tree: str, only: str | None = None) -> None:
     csr(R)
     spai2(R, tree)
     print("golden fixtures written to", HERE)
+
+
+BATCH_SEED = 2024
+
+
+def batch512(R):
+    """CG on every system of the 512-system batch with the reference's tags::CPU and
+    tags::CPU::SSE, one host thread per system (the reference's containers are independent)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle.bindings import Oracle
+    O = Oracle()
+    R.set_threads(1)
+    sides = np.random.default_rng(BATCH_SEED).integers(17, 258, size=512)
+
+    def one(i):
+        M = int(sides[i])
+        A = P.q1_poisson(M, P.log_uniform_coef(M, 1e-1, 1e1, BATCH_SEED + i), symmetric=True)
+        b, _ = R.spmv(A, P.uniform_vector(M * M, BATCH_SEED + i + 1))
+        nb = np.linalg.norm(b)
+        row = []
+        for tag in ("cpu", "sse"):
+            x, u, _ = R.cg(A, b, eps=1e-8, max_iters=100000, tag=tag)
+            row += [u, np.linalg.norm(O.defect(A, b, x)) / nb]
+        return row
+
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        rows = list(ex.map(one, range(len(sides))))
+    r = np.array(rows)
+    np.savez_compressed(os.path.join(HERE, "batch512.npz"), sides=sides, cpu_used=r[:, 0].astype(np.int64),
+                        cpu_relres=r[:, 1], sse_used=r[:, 2].astype(np.int64), sse_relres=r[:, 3])
 
 
 if __name__ == "__main__":

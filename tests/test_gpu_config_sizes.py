@@ -1,0 +1,225 @@
+"""Parity at the workloads' own sizes, against the reference compiled from its sources.
+
+The small-size tests pin every solver against the oracle; these run the same comparisons on
+the systems the benchmark quotes its figures on:
+
+- plain FP64 CG on the Q1 Poisson grids of 1025^2 and 2049^2 (x0 = 0, relative residual 1e-8);
+- V(2,2) MG on the 2049^2 grid, FP64 and FP32 (coarse CG capped at 100 iterations);
+- FP64 iterative refinement around FP32 V-cycles on the 2049^2 grid with a cellwise
+  coefficient 10^U(-2,2) (contrast 10^4, Galerkin coarse levels), to 1e-10;
+- every system of the 512-system batch (side U{17..257}, coefficient 10^U(-1,1)), FP64 CG and
+  FP32-inner refinement.
+
+The reference side is HONEI's own solver templates (honei/math/cg.hh:68-132,
+honei/math/mg.hh:1098-1126, honei/math/ir.hh:30-78) on tags::CPU::MultiCore::SSE over all host
+cores (tests/test_oracle_pin.py pins that tag's iteration counts to tags::CPU's); the batch
+systems go through the plain-C oracle, one host thread per system.
+
+Bar (north star): iterations / cycles / outer steps within +-1 of the reference's, and the
+final true relative residual ||b - A x|| / ||b|| within 1e-10 of the reference's.  Where the
+counts differ by one, the residuals differ by one step's contraction, which is stated and
+checked per case (FP32 solves: the FP32 bar of the test).  The batch's FP64 CG is held to the
+reference's own spread between two of its tags on the same systems (the test says why).
+"""
+import os
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+import pytest
+
+from honei_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+CORES = os.cpu_count() or 1
+
+
+@pytest.fixture(scope="module")
+def hb():
+    from honei_b200 import la
+    assert torch.cuda.is_available()
+    return la
+
+
+@pytest.fixture(scope="module")
+def ref(reference):
+    reference.set_threads(CORES)
+    return reference
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def relres(oracle, A, b, x):
+    return float(np.linalg.norm(oracle.defect(A, b, np.asarray(x, A.dtype))) / np.linalg.norm(b))
+
+
+def contraction(hist_len, rel):
+    """Mean residual reduction per step of a solve that reached `rel` in `hist_len` steps."""
+    return rel ** (1.0 / max(hist_len, 1))
+
+
+@pytest.mark.parametrize("M", [1025, 2049])
+def test_cg_f64_at_size_matches_reference(hb, oracle, ref, M):
+    A = P.q1_poisson(M)
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 1))
+    x_r, u_r, _ = ref.cg(A, b, eps=1e-8, max_iters=100000, tag="mc-sse")
+    Ad = hb.SparseMatrixELL.from_reference(A)
+    x = torch.zeros(A.rows, dtype=torch.float64, device="cuda")
+    u_g = hb.CGSolver.value(Ad, None, dev(b), x, 100000, 1e-8)
+    x_g = host(x)
+    rg, rr = relres(oracle, A, b, x_g), relres(oracle, A, b, x_r)
+    print(f"CG {M}^2: GPU {u_g} iterations, relres {rg:.6e}; reference {u_r}, {rr:.6e}")
+    assert abs(u_g - u_r) <= 1, (M, u_g, u_r)
+    if u_g == u_r:
+        assert abs(rg - rr) <= 1e-10, (M, rg, rr)
+    else:
+        # one CG step apart: the residuals differ by about one step's reduction
+        q = contraction(u_r, rr)
+        assert abs(rg - rr) <= 2 * (1 - q) * rr + 1e-10, (M, rg, rr, q)
+    assert np.linalg.norm(x_g - x_r) <= 1e-5 * np.linalg.norm(x_r)
+
+
+@pytest.fixture(scope="module")
+def h2049():
+    return P.mg_hierarchy(2049)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["f64", "f32"])
+def test_mg_2049_matches_reference(hb, oracle, ref, h2049, dt):
+    """V(2,2) MG, damped Jacobi 0.7, PROLMAT transfers, 9^2 coarse CG capped at 100 iterations
+    (max_iters_coarse of honei/math/mg_TEST.cc:421).  FP64 to 1e-8; FP32 to 1e-6 (FP32 V-cycles
+    stagnate near 1e-7)."""
+    H = h2049 if dt == np.float64 else h2049.astype(np.float32)
+    A64 = h2049.A[-1]
+    eps = 1e-8 if dt == np.float64 else 1e-6
+    b64 = oracle.spmv(A64, P.uniform_vector(A64.rows, 5))
+    b = b64.astype(dt)
+    x_r, u_r, _ = ref.mg(H, b, eps=eps, max_iters=100, max_iters_coarse=100, tag="mc-sse")
+    data = hb.MGData.from_hierarchy(H, dt, eps=eps, max_iters=100, max_iters_coarse=100)
+    x = torch.zeros(A64.rows, dtype=torch.float64 if dt == np.float64 else torch.float32, device="cuda")
+    u_g, r0, r1 = hb.MGSolver.value(data, dev(b), x)
+    x_g = host(x)
+    data.close()
+    # residuals of both solutions in FP64 against the FP64 system
+    rg = relres(oracle, A64, b64, x_g.astype(np.float64))
+    rr = relres(oracle, A64, b64, x_r.astype(np.float64))
+    print(f"MG 2049^2 {np.dtype(dt).name}: GPU {u_g} cycles, relres {rg:.6e}; reference {u_r}, {rr:.6e}")
+    assert abs(u_g - u_r) <= 1, (u_g, u_r)
+    if dt == np.float64:
+        tol = 1e-10 if u_g == u_r else 2 * (1 - contraction(u_r, rr)) * rr + 1e-10
+    else:
+        # FP32: the V-cycle's own rounding (~1e-7 relative) bounds the agreement
+        tol = 1e-7 if u_g == u_r else 2 * (1 - contraction(u_r, rr)) * rr + 1e-7
+    assert abs(rg - rr) <= tol, (rg, rr, u_g, u_r)
+
+
+def test_ir_2049_contrast_1e4_matches_reference(hb, oracle, ref):
+    """IRSolver (honei/math/ir.hh:30-78, warm-started inner MG as the reference runs it): FP64
+    defect / norm / update around FP32 V(2,2) cycles to 1e-3, outer target 1e-10, on the 2049^2
+    grid with a cellwise coefficient 10^U(-2,2) and Galerkin coarse levels."""
+    M = 2049
+    coef = P.log_uniform_coef(M, 1e-2, 1e2, 3)
+    H = P.mg_hierarchy(M, coef=coef)
+    H32 = H.astype(np.float32)
+    A = H.A[-1]
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 4))
+    x_r, u_r, _ = ref.ir_mg(H, H32, b, eps=1e-10, inner_eps=1e-3, max_iters=100, inner_max_iters=100,
+                            max_iters_coarse=100, tag="mc-sse")
+    A64 = hb.SparseMatrixELL.from_reference(A)
+    mg32 = hb.MGData.from_hierarchy(H, dtype=np.float32, eps=1e-3, max_iters=100, max_iters_coarse=100)
+    x = torch.zeros(A.rows, dtype=torch.float64, device="cuda")
+    u_g, r0, r1 = hb.IRSolver.value(A64, dev(b), x, mg32, eps=1e-10, max_iters=100, warm_start=True)
+    x_g = host(x)
+    mg32.close()
+    rg, rr = relres(oracle, A, b, x_g), relres(oracle, A, b, x_r)
+    print(f"IR 2049^2: GPU {u_g} outer steps, relres {rg:.6e}; reference {u_r}, {rr:.6e}; "
+          f"|x_g - x_r| / |x_r| = {np.linalg.norm(x_g - x_r) / np.linalg.norm(x_r):.3e}")
+    assert abs(u_g - u_r) <= 1, (u_g, u_r)
+    assert rg < 1e-10 and rr < 1e-10, (rg, rr)
+    assert abs(rg - rr) <= 1e-10
+    # the two solutions agree to the accuracy the 1e-10 residual target gives
+    assert np.linalg.norm(x_g - x_r) <= 1e-6 * np.linalg.norm(x_r), np.linalg.norm(x_g - x_r) / np.linalg.norm(x_r)
+
+
+BATCH_SEED = 2024
+
+
+def _batch_sides(n=512, seed=BATCH_SEED):
+    return np.random.default_rng(seed).integers(17, 258, size=n)
+
+
+def test_batch_512_cg64_within_the_references_own_spread(hb, oracle):
+    """The 512-system batch of the benchmark, FP64 CG, solved in one launch at the tuned shape
+    (2-CTA clusters of 512 threads), against the reference's CGSolver<tags::CPU> on every
+    system (tests/golden/batch512.npz, written by the compiled reference).
+
+    On these systems (contrast 10^2, up to 872 iterations) the iteration count at which the
+    1e-8 test fires depends on the summation order of the dot products: the reference's own
+    tags::CPU::SSE, which differs from tags::CPU only in that order, lands on tags::CPU's count
+    for 239 of the 512 systems, one apart for 192 and up to 6 apart for the rest (the same
+    fixture).  The bar is therefore the reference's own spread: per system, the GPU count
+    within the largest tags::CPU / tags::CPU::SSE difference of the batch (and within 1 where
+    that is smaller), the final true residual below the target, and its distance from
+    tags::CPU's within the largest such distance between the two reference tags."""
+    from conftest import load_golden
+    from honei_b200 import batch as B
+    g = load_golden("batch512")
+    sides = _batch_sides()
+    assert np.array_equal(sides, g["sides"])
+    systems = B.q1_batch(sides, coef_range=(1e-1, 1e1), seed=BATCH_SEED, mode="cg64", eps=1e-8)
+    res = B.BatchSolver(systems).solve(B.HbBatchConfig(2, 512))
+    du_ref = np.abs(g["sse_used"] - g["cpu_used"])
+    dr_ref = np.abs(g["sse_relres"] - g["cpu_relres"])
+    D, Rr = max(1, int(du_ref.max())), float(dr_ref.max())
+    u_g = np.array([r["iterations"] for r in res])
+    r_g = np.array([r["true_relres"] for r in res])
+    st = np.array([r["status"] for r in res])
+    du = np.abs(u_g - g["cpu_used"])
+    dr = np.abs(r_g - g["cpu_relres"])
+    print(f"batch 512 cg64: |GPU - tags::CPU| iterations: {np.sum(du == 0)} equal, {np.sum(du == 1)} one apart, "
+          f"max {du.max()}, mean {du.mean():.2f}; tags::CPU::SSE: {np.sum(du_ref == 0)} equal, "
+          f"{np.sum(du_ref == 1)} one apart, max {du_ref.max()}, mean {du_ref.mean():.2f}; residual gap max "
+          f"{dr.max():.3e} (SSE {Rr:.3e})")
+    assert np.all(st == 0)
+    assert np.all(r_g < 1e-8 * (1 + 1e-6)), r_g.max()
+    assert du.max() <= D, (du.max(), D)
+    assert dr.max() <= Rr, (dr.max(), Rr)
+    # spot check: the device-reported true residual is the host's on a few systems
+    for i in (0, 17, 255):
+        A = systems[i].A64.to_host()
+        b, x = host(systems[i].b), host(systems[i].x)
+        assert abs(relres(oracle, A, b, x) - r_g[i]) <= 1e-6 * r_g[i]
+
+
+def test_batch_512_ir32_every_system_matches_oracle(hb, oracle):
+    """The same batch in mixed precision (FP64 refinement around FP32 CG to 1e-3 per step, to a
+    1e-8 FP64 residual): every system's outer step count against the oracle's scaled
+    refinement around FP32 CG on the same matrix and right-hand side."""
+    from honei_b200 import batch as B
+    sides = _batch_sides()
+    systems = B.q1_batch(sides, coef_range=(1e-1, 1e1), seed=BATCH_SEED, mode="ir32", eps=1e-8, inner_eps=1e-3)
+    res = B.BatchSolver(systems).solve(B.HbBatchConfig(2, 512))
+    mats = [s.A64.to_host() for s in systems]
+    bs = [host(s.b) for s in systems]
+    xs = [host(s.x) for s in systems]
+
+    def ref_solve(i):
+        A, b = mats[i], bs[i]
+        _, u_o, _, _ = oracle.ir_cg(A, A.astype(np.float32), b, eps=1e-8, inner_eps=1e-3)
+        return u_o, relres(oracle, A, b, xs[i])
+
+    with ThreadPoolExecutor(CORES) as pool:
+        out = list(pool.map(ref_solve, range(len(systems))))
+    bad = [(i, int(sides[i]), r["outer"], u_o, rg) for i, (r, (u_o, rg)) in enumerate(zip(res, out))
+           if r["status"] != 0 or abs(r["outer"] - u_o) > 1 or rg >= 1e-8]
+    d = [abs(r["outer"] - o[0]) for r, o in zip(res, out)]
+    print(f"batch 512 ir32: {d.count(0)} systems with the oracle's outer step count, {d.count(1)} one apart")
+    assert not bad, f"{len(bad)} of {len(systems)} systems outside the bar: {bad[:8]}"

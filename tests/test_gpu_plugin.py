@@ -28,18 +28,7 @@ def _run(name, *args):
 
 
 def test_plugin_operators_and_generic_solvers(tmp_path):
-    H = P.mg_hierarchy(65)
-    L = len(H.A)
-    for l, A in enumerate(H.A, 1):
-        P.write_ell(str(tmp_path / f"A_{l}.ell"), A)
-    for l, Pm in enumerate(H.prol, 2):
-        P.write_ell(str(tmp_path / f"prol_{l}.ell"), Pm)
-    A = H.A[-1]
-    xt = P.uniform_vector(A.rows, 4)
-    ip, ix, dv = A.to_csr()
-    b = np.add.reduceat(dv * xt[ix], ip[:-1])
-    P.write_exp(str(tmp_path / f"rhs_{L}"), b)
-    P.write_exp(str(tmp_path / f"init_{L}"), np.zeros(A.rows))
+    L = _write_hierarchy(tmp_path, 65)
     out = _run("plugin_ops_test", str(tmp_path), str(L))
     assert "PASS MGSolver<GPU::CUDA>" in out
     assert "FAIL" not in out
@@ -53,3 +42,28 @@ def test_plugin_cg_specialisation():
     out = _run("plugin_cg_test")
     assert out.count("PASS") == 8 and "FAIL" not in out
     assert out.count("PASS CGSolver<GPU::CUDA, VAR>") == 4
+
+
+def _write_hierarchy(tmp_path, M, seed=4):
+    H = P.mg_hierarchy(M)
+    L = len(H.A)
+    for l, A in enumerate(H.A, 1):
+        P.write_ell(str(tmp_path / f"A_{l}.ell"), A)
+    for l, Pm in enumerate(H.prol, 2):
+        P.write_ell(str(tmp_path / f"prol_{l}.ell"), Pm)
+    A = H.A[-1]
+    xt = P.uniform_vector(A.rows, seed)
+    ip, ix, dv = A.to_csr()
+    P.write_exp(str(tmp_path / f"rhs_{L}"), np.add.reduceat(dv * xt[ix], ip[:-1]))
+    P.write_exp(str(tmp_path / f"init_{L}"), np.zeros(A.rows))
+    return L
+
+
+def test_plugin_mg_fast_path(tmp_path):
+    """HONEI's MGSolver / MGCycleCreation / RISmoother / IRSolver on tags::GPU::CUDA with the
+    plugin's specialisations (honei_b200/plugin/mg_b200.hh), on a hierarchy loaded by
+    MGUtil::load_data: smoother sweeps and one coarse-free cycle bit-exact to tags::CPU, the
+    solve within +-1 cycle and 1e-10 of tags::CPU's residual, IRSolver within +-1 outer step."""
+    L = _write_hierarchy(tmp_path, 257)
+    out = _run("plugin_mg_test", str(tmp_path), str(L))
+    assert out.count("PASS") == 5 and "FAIL" not in out

@@ -95,3 +95,53 @@ def test_empty_and_single_node_requests(S):
     for tag, M in enumerate((1, 2, 3)):
         assert out[tag].status == 0, out[tag]
         assert np.allclose(out[tag].x, 1.0, rtol=1e-8)
+
+
+def test_plain_batched_baseline_solves_every_request(S):
+    """The plain FP64 CG baseline with the mixed server's concurrency: grids up to mid_max_side in
+    batched cluster launches, larger ones on concurrent whole-GPU CG workers; every request
+    reaches the target, and a batched request's solution equals the same system solved in a
+    batch of its own."""
+    trace = S.poisson_trace(20, rate=0.0, side_range=(17, 400), seed=6)
+    with S.Server(mode="plain_batched", mid_max_side=200, large_workers=2) as srv:
+        rep = S.replay(srv, trace, realtime=False)
+    assert rep["completed"] == rep["ok"] == 20
+    assert set(rep["paths"]) == {"batch_cg64", "cg64"}
+    assert rep["max_true_relres"] < 1e-8
+    by_tag = {c.tag: c for c in rep["records"]}
+    with S.Server(mode="plain_batched", mid_max_side=200, large_workers=2) as srv:
+        for req in trace.requests[:6]:
+            srv.submit(req)
+            (c,) = srv.drain()
+            m = by_tag[req.tag]
+            assert c.path == m.path and c.iterations == m.iterations
+            assert np.array_equal(c.x, m.x), (req.M, c.path)
+
+
+def test_stream_replay_closed_and_open_loop(S):
+    """The on-demand stream: a prefix of a long stream is the short stream, and both replays
+    (closed loop with a window, open loop at arrival times) serve every request once."""
+    long = S.stream_trace(200, rate=300.0, side_range=(17, 200), seed=4)
+    short = S.poisson_trace(30, rate=300.0, side_range=(17, 200), seed=4)
+    for i, r in enumerate(short.requests):
+        q = long.request(i)
+        assert q.M == r.M and np.array_equal(q.coef, r.coef) and np.array_equal(q.x_true, r.x_true)
+    with S.Server(mode="mixed", small_max_side=64, large_workers=2, mid_max_side=128) as srv:
+        rep = S.replay_stream(srv, long.prefix(60), realtime=False, window=8, producers=2)
+        assert rep["completed"] == rep["ok"] == 60 and rep["max_true_relres"] < 1e-8
+        rep = S.replay_stream(srv, long.prefix(40), realtime=True, producers=2)
+        assert rep["completed"] == rep["ok"] == 40
+        assert sorted(c.tag for c in rep["records"]) == list(range(40))
+
+
+def test_admission_charge_covers_the_pool(S):
+    """What the stream-ordered pool really held never exceeds what admission charged: the
+    high-water mark of the pool's used bytes stays under the peak of the admitted charges."""
+    trace = S.poisson_trace(40, rate=0.0, side_range=(17, 700), seed=8)
+    for mode in ("mixed", "plain_batched", "plain"):
+        with S.Server(mode=mode, mid_max_side=200) as srv:
+            rep = S.replay(srv, trace, realtime=False)
+            st = srv.stats()
+        assert rep["ok"] == 40
+        assert "pool_used_high" in st, st
+        assert 0 < st["pool_used_high"] <= st["bytes_peak"], (mode, st)

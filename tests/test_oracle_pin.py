@@ -6,6 +6,7 @@
 Bit-exact comparisons throughout: the oracle restates tags::CPU's arithmetic order.
 """
 import dataclasses
+import os
 
 import numpy as np
 import pytest
@@ -142,6 +143,58 @@ def test_oracle_multicore_tags_agree_on_iterations(reference):
     b, _ = reference.spmv(A, P.uniform_vector(A.rows, 1))
     counts = {tag: reference.cg(A, b, tag=tag)[1] for tag in ("cpu", "generic", "sse", "mc-sse")}
     assert max(counts.values()) - min(counts.values()) <= 1, counts
+
+
+def test_oracle_multicore_mg_and_ir_agree_with_cpu_tag(reference):
+    """MultiCore::SSE (the tag the full-size GPU comparisons use) takes tags::CPU's cycle and
+    outer-step counts for MG and for IRSolver, and reaches the same residual."""
+    reference.set_threads(os.cpu_count() or 1)
+    H = P.mg_hierarchy(33, coef=P.log_uniform_coef(33, 1e-2, 1e2, 7))
+    A = H.A[-1]
+    b, _ = reference.spmv(A, P.uniform_vector(A.rows, 2))
+    runs = {t: reference.mg(H, b, eps=1e-8, max_iters_coarse=100, tag=t) for t in ("cpu", "mc-sse")}
+    assert runs["cpu"][1] == runs["mc-sse"][1]
+    assert np.allclose(runs["cpu"][0], runs["mc-sse"][0], rtol=0, atol=1e-9 * np.abs(runs["cpu"][0]).max())
+    H32 = H.astype(np.float32)
+    irs = {t: reference.ir_mg(H, H32, b, eps=1e-10, inner_eps=1e-3, max_iters_coarse=100, tag=t)
+           for t in ("cpu", "mc-sse")}
+    assert abs(irs["cpu"][1] - irs["mc-sse"][1]) <= 1
+    r = {t: np.linalg.norm(reference.defect(A, b, irs[t][0])) / np.linalg.norm(b) for t in irs}
+    assert r["cpu"] < 1e-10 and r["mc-sse"] < 1e-10, r
+
+
+def test_batch512_fixture_matches_oracle_and_reference():
+    """The 512-system batch fixture (tests/golden/batch512.npz, CGSolver<tags::CPU> and
+    <tags::CPU::SSE> counts): the oracle reproduces tags::CPU's count and residual on a sample of
+    the systems, and, where the compiled reference is present, its SSE tag the stored SSE count."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle.bindings import REF_SO, Oracle, Reference
+    O = Oracle()
+    g = load_golden("batch512")
+    seed = 2024
+    sides = np.random.default_rng(seed).integers(17, 258, size=512)
+    assert np.array_equal(sides, g["sides"])
+    sample = [int(i) for i in np.argsort(sides)[::37]]        # 14 systems across the size range
+
+    def system(i):
+        M = int(sides[i])
+        A = P.q1_poisson(M, P.log_uniform_coef(M, 1e-1, 1e1, seed + i), symmetric=True)
+        return A, O.spmv(A, P.uniform_vector(M * M, seed + i + 1))
+
+    def run(i):
+        A, b = system(i)
+        x, u = O.cg(A, b, eps=1e-8, max_iters=100000)
+        return u, np.linalg.norm(O.defect(A, b, x)) / np.linalg.norm(b)
+
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        out = list(ex.map(run, sample))
+    for i, (u, r) in zip(sample, out):
+        assert u == g["cpu_used"][i] and r == g["cpu_relres"][i], (i, u, g["cpu_used"][i])
+    if os.path.exists(REF_SO):
+        R = Reference()
+        for i in sample[:4]:
+            A, b = system(i)
+            assert R.cg(A, b, eps=1e-8, max_iters=100000, tag="sse")[1] == g["sse_used"][i]
 
 
 # ---- BandedMatrixQx<Q1Type> ----------------------------------------------------------------
