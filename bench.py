@@ -246,6 +246,120 @@ def run_reference_arm(args):
 # ---------------------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------------------
+def _time_us(fn, reps, flush=None):
+    """Median CUDA-event time of fn() in microseconds, after 3 warm-up calls; with `flush`
+    (a device buffer larger than L2) zeroed between the timed calls, outside the events."""
+    import torch
+    for _ in range(3):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1) * 1e3)
+    return statistics.median(ts)
+
+
+def bench_spmv_variants(la, ctx, M=M_SPMV, seed=5, cpu=True, reps=50):
+    """The other SpMV lines of the SpMV configuration: the FP32 product of the 2049^2 matrix; the
+    randomly permuted 2049^2 matrix (seeded symmetric row/column permutation) in FP64 and FP32,
+    as given and through its Cuthill-McKee ordered copy (SparseMatrixELL.ordered: rows stored
+    in the locality order, columns renumbered, x permuted into a work vector inside the timed
+    product, y scattered back -- bit-identical to the product on the permuted matrix); the
+    1025^2 FP64 product with L2 flushed between products (its 130 MB would otherwise stay
+    partly in L2).  GB/s are the algorithmic bytes of the product on the given matrix
+    (nnz*(s+4) + 2*n*s)."""
+    import torch
+    from honei_b200 import problems as P
+    peak, _ = measured_peak()
+    n = M * M
+    nnz = q1_nnz(M)
+    out = {"workload": f"ELL SpMV variants: Q1 {M}^2 FP32; Q1 {M}^2 randomly permuted (seed {seed}), FP64 and "
+                       "FP32, as given and through the Cuthill-McKee ordered copy; Q1 1025^2 FP64 with L2 flushed"}
+
+    def line(us, s, nn=n, nz=nnz):
+        g = spmv_bytes(nz, nn, s) / (us * 1e3)
+        return {"us": round(us, 2), "gbs": round(g, 1), "frac_of_peak": round(g / peak, 4)}
+
+    A = la.SparseMatrixELL.q1_poisson(M, ctx=ctx)
+    A32 = A.to_float(ctx=ctx)
+    x32 = torch.from_numpy(P.uniform_vector(n, 1).astype(np.float32)).cuda()
+    y32 = torch.empty_like(x32)
+    out["natural_f32"] = line(_time_us(lambda: la.Product.value(y32, A32, x32, ctx=ctx), reps), 4)
+    del A, A32
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    Ap, _ = P.q1_poisson_permuted(M, seed=seed)
+    out["host_permuted_matrix_s"] = round(time.perf_counter() - t0, 2)
+    for name, dt, s in (("f64", np.float64, 8), ("f32", np.float32, 4)):
+        Ad = la.SparseMatrixELL.from_reference(Ap.astype(dt) if dt != np.float64 else Ap, ctx)
+        x = torch.from_numpy(P.uniform_vector(n, seed + 1).astype(dt)).cuda()
+        y = torch.empty_like(x)
+        out[f"permuted_{name}"] = line(_time_us(lambda: la.Product.value(y, Ad, x, ctx=ctx), reps), s)
+        y0 = y.clone()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        B = Ad.ordered(columns=True, ctx=ctx)
+        torch.cuda.synchronize()
+        t_order = time.perf_counter() - t0
+        r = line(_time_us(lambda: la.Product.value(y, B, x, ctx=ctx), reps), s)
+        r["same_y_as_permuted"] = bool(torch.equal(y, y0))
+        r["ordering_ms"] = round(t_order * 1e3, 1)
+        r["levels"], r["bandwidth_before"], r["bandwidth_after"] = int(B.info[0]), Ad.bandwidth(), B.B.bandwidth()
+        out[f"permuted_ordered_{name}"] = r
+        del Ad, B, x, y, y0
+        torch.cuda.empty_cache()
+    if cpu:
+        h = None
+        try:
+            from oracle.bindings import REF_SO, Reference
+            if os.path.exists(REF_SO):
+                R = Reference()
+                R.set_threads(os.cpu_count() or 1)
+                h = R.ell_handle(Ap, P.uniform_vector(n, seed + 1))
+        except OSError:
+            h = None
+        if h is not None:
+            t = statistics.median(h.spmv("mc-sse", 10))
+            out["permuted_f64_cpu_reference_gbs"] = round(spmv_bytes(nnz, n, 8) / t / 1e9, 2)
+            h.close()
+    del Ap
+    M2 = 1025
+    n2, nz2 = M2 * M2, q1_nnz(M2)
+    A = la.SparseMatrixELL.q1_poisson(M2, ctx=ctx)
+    x = torch.from_numpy(P.uniform_vector(n2, 1)).cuda()
+    y = torch.empty_like(x)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    out["natural_1025_f64_l2_flushed"] = line(_time_us(lambda: la.Product.value(y, A, x, ctx=ctx), reps, flush),
+                                              8, n2, nz2)
+    out["natural_1025_f64_warm_l2"] = line(_time_us(lambda: la.Product.value(y, A, x, ctx=ctx), reps), 8, n2, nz2)
+    del A, flush
+    torch.cuda.empty_cache()
+    return out
+
+
+def plugin_e2e(M=M_SPMV, steps=20):
+    """The product through HONEI's own API with host DenseVectors (tests/plugin: Product<tags::
+    GPU::CUDA>::value through MemoryArbiter and MemoryBackend<tags::GPU::CUDA>, one upload of x
+    and one download of y per step): one product per step and ten per step.  None where the
+    plugin programs are not built."""
+    import subprocess
+    exe = os.path.join(ROOT, "tests", "plugin", "_build", "plugin_product_bench")
+    if not os.path.exists(exe):
+        return None
+    try:
+        p = subprocess.run([exe, str(M), str(steps)], capture_output=True, text=True, timeout=600)
+        return json.loads(p.stdout.strip().splitlines()[-1]) if p.returncode == 0 else {"error": p.stderr[-300:]}
+    except (OSError, ValueError, subprocess.SubprocessError, IndexError) as e:
+        return {"error": repr(e)}
+
+
 def bench_batch(la, ctx, n_systems=512, seed=2024):
     """512 independent SPD Q1 systems, side ~ U{17..257}, cell coefficient 10^U(-1,1), b = A x_true:
     one persistent batched launch (FP64 CG, and FP32-inner IR to a 1e-8 FP64 residual) against
@@ -426,52 +540,6 @@ def bench_csr(la, ctx, x, ell_s, M=M_SPMV, reps=100, cpu=True):
     return out
 
 
-def bench_spai2(la, ctx, M=M_SPMV, reps=5, cpu=True, cpu_side=257):
-    """SPAI2<tags::GPU::CUDA> of the Q1 Poisson matrix of side M (M^2 columns, each a
-    least-squares system of up to 81 rows and 9 unknowns), FP64 and FP32: whole-call time
-    (column structure, normal equations, LU, one stream synchronization) per call.  The CPU
-    reference is the faster of SPAI2<tags::CPU::SSE> and SPAI2<tags::CPU::MultiCore::SSE> on the
-    side-cpu_side matrix, compared per column."""
-    import torch
-    from honei_b200 import problems as P
-    A = la.SparseMatrixELL.q1_poisson(M, ctx=ctx)
-    out = {"workload": f"SPAI2 of Q1 Poisson {M}^2 (pattern of A), whole call", "columns": A.rows()}
-    for name, A_ in (("f64", A), ("f32", A.to_float(ctx=ctx))):
-        Mm = la.SPAI2.value(A_, ctx=ctx)
-        la.SPAI2.value(A_, Mm, ctx=ctx)
-        torch.cuda.synchronize()
-        ts = []
-        for _ in range(reps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            la.SPAI2.value(A_, Mm, ctx=ctx)
-            e1.record()
-            torch.cuda.synchronize()
-            ts.append(e0.elapsed_time(e1) / 1e3)
-        t = statistics.median(ts)
-        out[name] = {"ms": round(t * 1e3, 3), "columns_per_s": round(A.rows() / t, 1)}
-        del Mm
-    if cpu:
-        R = _ref_cpu()
-        if R is not None:
-            # both CPU tags the reference has; the faster one is the baseline (the ten-thread
-            # MultiCore::SSE is held back by its per-column allocations)
-            Ah = P.q1_poisson(cpu_side)
-            best = None
-            for tag, threads in (("sse", 1), ("mc-sse", 10)):
-                sec = statistics.median(R.spai2(Ah, tag)[1] for _ in range(3))
-                cps = Ah.rows / sec
-                out[f"cpu_reference_{tag}"] = {"columns_per_s": round(cps, 1), "threads": threads}
-                if best is None or cps > best[0]:
-                    best = (cps, tag)
-            out["cpu_reference"] = {"columns_per_s": round(best[0], 1), "tag": best[1],
-                                    "sample": f"Q1 {cpu_side}^2 FP64, median of 3"}
-            out["speedup_f64_vs_cpu_reference"] = round(out["f64"]["columns_per_s"] / best[0], 1)
-    del A
-    torch.cuda.empty_cache()
-    return out
-
-
 def bench_q1band(la, ctx, x, ell_s, M=M_SPMV, reps=100, cpu=True):
     """Product on BandedMatrixQx<Q1Type> (nine bands of n values, no index array) for the same
     2049^2 Poisson matrix and x as the headline: algorithmic bytes 11*n*8 per product (nine
@@ -511,6 +579,30 @@ def bench_q1band(la, ctx, x, ell_s, M=M_SPMV, reps=100, cpu=True):
 MG_COARSE_ITERS = 100
 
 
+def mg_cycle_bytes(H, s, banded):
+    """Algorithmic bytes of one MGSolver cycle (V(2,2) plus the finest defect and its norm) on
+    hierarchy H with s-byte values.  Per level above the coarsest (n rows, n_c coarse rows): four
+    Jacobi sweeps x' = x + P (b - A x) (matrix, x, b, P read, x' written), the defect (matrix, x,
+    b read, store written), the restriction (store read, d_c written; the ELL cycle also reads
+    Res), the zero fill of c_c, prolongation + sum (c_c, x read, x written; ELL also reads Prol).
+    Matrix per application: 9 n s banded (nine bands), nnz (s + 4) ELL.  The coarsest level's CG
+    (81 rows) is latency, not bytes, and is left out."""
+    total = 0
+    L = len(H.A)
+    for l in range(1, L):
+        A = H.A[l]
+        n, nc = A.rows, H.A[l - 1].rows
+        mat = 9 * n * s if banded else A.nnz * (s + 4)
+        sweep = mat + 4 * n * s
+        defect = mat + 3 * n * s
+        restrict = n * s + nc * s + (0 if banded else H.res[l - 1].nnz * (s + 4))
+        prolong = nc * s + 2 * n * s + (0 if banded else H.prol[l - 1].nnz * (s + 4))
+        total += 4 * sweep + defect + restrict + nc * s + prolong
+    n = H.A[-1].rows
+    total += (9 * n * s if banded else H.A[-1].nnz * (s + 4)) + 3 * n * s + n * s
+    return int(total)
+
+
 def bench_mg(la, ctx, M=2049, seed=5, cpu=True):
     """Q1 Poisson M^2 (unit coefficient, the reference's rediscretised hierarchy down to 9^2):
     MGSolver V(2,2), damped Jacobi 0.7, PROLMAT transfers, coarse CG, x0 = 0, b = A x_true.
@@ -518,9 +610,9 @@ def bench_mg(la, ctx, M=2049, seed=5, cpu=True):
     MG_COARSE_ITERS iterations, MGUtil::configure's max_iters_coarse in the reference's own MG
     test (honei/math/mg_TEST.cc:421); the 9^2 coarse system (identity Dirichlet rows, not
     symmetric) stagnates well before that, and a run at a cap of 1000 (f64_banded_coarse1000)
-    takes the same cycles to the same residual.  Plus the FP64 SpMV on the
-    permuted matrix (seeded symmetric row/column permutation) and, when the compiled reference
-    is present, its MultiCore::SSE MG solve of the same FP64 system on the host cores."""
+    takes the same cycles to the same residual.  When the compiled reference is present, its
+    MultiCore::SSE MG solve of the same FP64 system on the host cores.  Each variant reports its
+    algorithmic bytes per cycle (mg_cycle_bytes) and the fraction of the HBM peak that gives."""
     import torch
     from honei_b200 import problems as P
 
@@ -555,8 +647,12 @@ def bench_mg(la, ctx, M=2049, seed=5, cpu=True):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         err = float(torch.linalg.norm((x - xtd).double()) / torch.linalg.norm(xtd.double()))
+        peak, _ = measured_peak()
+        cb = mg_cycle_bytes(H, np.dtype(npdt).itemsize, banded)
+        gbs = cb / (ms / max(cycles, 1) * 1e6)
         out[name] = {"ms": round(ms, 2), "cycles": cycles, "ms_per_cycle": round(ms / max(cycles, 1), 3),
-                     "relres": r1 / r0 if r0 else 0.0, "eps": eps, "err_vs_x_true": err}
+                     "relres": r1 / r0 if r0 else 0.0, "eps": eps, "err_vs_x_true": err,
+                     "bytes_per_cycle": cb, "gbs": round(gbs, 1), "frac_of_peak": round(gbs / peak, 4)}
         if banded and mic == MG_COARSE_ITERS:
             # the banded cycle rounds as the ELL cycle: same iterate
             out[name]["same_x_as_ell"] = bool(torch.equal(x, xs_ell[name.split("_")[0]]))
@@ -572,21 +668,6 @@ def bench_mg(la, ctx, M=2049, seed=5, cpu=True):
             out["cpu_reference_f64"] = {"s": round(sec, 3), "cycles": used, "cores": os.cpu_count(),
                                         "tag": "tags::CPU::MultiCore::SSE"}
             out["speedup_f64_vs_cpu"] = round(sec * 1e3 / out["f64"]["ms"], 1)
-    # permuted SpMV (stresses the gathers of x)
-    Ap, _ = P.q1_poisson_permuted(M, seed=seed)
-    Ad = la.SparseMatrixELL.from_reference(Ap, ctx)
-    x = torch.from_numpy(P.uniform_vector(M * M, seed + 1)).cuda()
-    y = torch.empty_like(x)
-    for _ in range(3):
-        la.Product.value(y, Ad, x, ctx=ctx)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(50):
-        la.Product.value(y, Ad, x, ctx=ctx)
-    e1.record()
-    torch.cuda.synchronize()
-    out["spmv_permuted_f64_gbs"] = round(spmv_bytes(Ap.nnz, Ap.rows, 8) * 50 / (e0.elapsed_time(e1) / 1e3) / 1e9, 1)
     return out
 
 
@@ -641,7 +722,8 @@ def bench_ir(la, ctx, M=2049, seed=3):
     return out
 
 
-SERVE_RATE = 40.0
+SERVE_RATE = 20.0           # Poisson arrivals per second: about half the plain baselines' capacity
+SERVE_LATENCY_REQUESTS = 600
 
 
 def _cpu_serve_baseline(trace, budget_s=20.0):
@@ -673,29 +755,35 @@ def _cpu_serve_baseline(trace, budget_s=20.0):
                                               "first requests in order"}
 
 
-def bench_serve(n_requests=20000, prefix=2000, rate=SERVE_RATE, seed=11, device=0, window=512, cpu=True):
+def bench_serve(n_requests=20000, prefix=2000, rate=SERVE_RATE, seed=11, device=0, window=256, cpu=True,
+                latency_requests=SERVE_LATENCY_REQUESTS):
     """The serving configuration: a stream of Q1 requests, side log-uniform in [33, 1025],
     cellwise coefficient log-uniform in [1e-2, 1e2], b = A x_true, each solved to 1e-8 relative
     FP64 residual, submitted from host buffers and returned to host buffers.
 
     Capacity (solves/s): the stream served closed-loop (at most `window` requests outstanding,
-    each submitted as soon as the server takes it) -- the mixed server on all n_requests, the two
-    plain FP64 CG baselines on the first `prefix` requests (and the mixed server on that prefix
-    too, for the like-for-like ratio).  Latency (p50/p99, arrival to result): the prefix with
-    Poisson arrivals at `rate` per second, a rate both the mixed server and the batched plain
-    baseline sustain, so p99 is service time rather than queue growth."""
+    each submitted as soon as the server takes one) -- the mixed server on all n_requests; the
+    two plain FP64 CG baselines (one request at a time; and with the mixed server's concurrency:
+    batched cluster launches for small grids, concurrent whole-GPU CG for the rest) and the mixed
+    server again on the first `prefix` requests, for the like-for-like ratios.  Latency (p50/p99,
+    arrival to result): the first `latency_requests` requests with Poisson arrivals at `rate` per
+    second, a rate every server sustains (about half the plain baselines' capacity), so p99 is
+    service time rather than queue growth; the mixed server also at 7.5x that rate."""
     from honei_b200 import serve as S
 
     full = S.stream_trace(n_requests, rate=0.0, seed=seed)
     pre = full.prefix(prefix)
-    timed = S.stream_trace(prefix, rate=rate, seed=seed)
+    timed = S.stream_trace(latency_requests, rate=rate, seed=seed)
+    fast = S.stream_trace(latency_requests, rate=7.5 * rate, seed=seed)
     out = {"workload": f"serving stream: {n_requests} requests (side log-U[33,1025], coef log-U[1e-2,1e2], "
-                       f"1e-8 FP64); baselines on its first {prefix} requests; latency on those {prefix} with "
-                       f"Poisson arrivals at {rate:g}/s",
+                       f"1e-8 FP64); capacity closed-loop ({window} outstanding): the mixed server on all "
+                       f"{n_requests}, both plain FP64 CG baselines and the mixed server on the first {prefix}; "
+                       f"latency: the first {latency_requests} with Poisson arrivals at {rate:g}/s "
+                       f"(mixed also at {7.5 * rate:g}/s)",
            "n_requests": n_requests, "prefix": prefix, "rows_total": full.rows, "rows_prefix": pre.rows,
-           "rate_per_s": rate}
+           "rate_per_s": rate, "window": window}
     # warm-up, untimed: kernels of every path loaded, the stream-ordered pool grown
-    warm = S.stream_trace(400, rate=0.0, seed=seed + 1000)
+    warm = S.stream_trace(300, rate=0.0, seed=seed + 1000)
     for mode in ("mixed", "plain_batched"):
         with S.Server(mode=mode) as srv:
             S.replay_stream(srv, warm, realtime=False, window=window)
@@ -718,6 +806,8 @@ def bench_serve(n_requests=20000, prefix=2000, rate=SERVE_RATE, seed=11, device=
     out["plain_prefix"] = run("plain", pre, False)
     out["mixed_poisson"] = run("mixed", timed, True)
     out["plain_batched_poisson"] = run("plain_batched", timed, True)
+    out["plain_poisson"] = run("plain", timed, True)
+    out["mixed_poisson_fast"] = run("mixed", fast, True)
     mp = out["mixed_prefix"]["solves_per_s"]
     out["speedup_vs_plain_batched"] = round(mp / max(out["plain_batched_prefix"]["solves_per_s"], 1e-9), 2)
     out["speedup_vs_plain_one_at_a_time"] = round(mp / max(out["plain_prefix"]["solves_per_s"], 1e-9), 2)
@@ -726,6 +816,52 @@ def bench_serve(n_requests=20000, prefix=2000, rate=SERVE_RATE, seed=11, device=
         if cb is not None:
             out["cpu_reference"] = cb
     return out
+
+
+def bench_cg_257(la, ctx, cpu=True):
+    """Plain FP64 CG on the 257^2 Q1 system (the CG configuration): solve latency from host b to
+    host x (pinned copies inside each timed solve), 30 solves after 3 warm-ups; with the compiled
+    reference, its CGSolver<MultiCore::SSE> on the same system on every host core."""
+    import torch
+    from honei_b200 import problems as P
+    Acg = la.SparseMatrixELL.q1_poisson(M_CG, ctx=ctx)
+    ncg = Acg.rows()
+    xt = torch.from_numpy(P.uniform_vector(ncg, 1)).cuda()
+    bcg = torch.empty_like(xt)
+    la.Product.value(bcg, Acg, xt, ctx=ctx)
+    bh = bcg.cpu().pin_memory()
+    xh_cg = torch.empty(ncg, dtype=torch.float64).pin_memory()
+    bd, xd_cg = torch.empty_like(bcg), torch.empty_like(bcg)
+    lat, iters = [], None
+    n_solves = 30
+    for i in range(n_solves + 3):
+        t0 = time.perf_counter()
+        bd.copy_(bh, non_blocking=True)
+        xd_cg.zero_()
+        iters = la.CGSolver.value(Acg, None, bd, xd_cg, 20000, 1e-8, ctx=ctx)
+        xh_cg.copy_(xd_cg, non_blocking=True)
+        torch.cuda.synchronize()
+        if i >= 3:
+            lat.append(time.perf_counter() - t0)
+    lat_ms = sorted(1e3 * v for v in lat)
+    cg_extra = {"workload": "plain FP64 CG, Q1 257^2, 1e-8 relative, x0 = 0", "iterations": iters,
+                "solves_per_s": round(len(lat) / sum(lat), 2),
+                "p50_ms": round(statistics.median(lat_ms), 3),
+                "p99_ms": round(lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))], 3)}
+    if cpu:
+        # the reference's own CGSolver<MultiCore::SSE> on the host cores, same system
+        R = _ref_cpu()
+        if R is not None:
+            Ah = P.q1_poisson(M_CG)
+            secs = []
+            for _ in range(3):
+                _, used_ref, sec = R.cg(Ah, bh.numpy(), eps=1e-8, max_iters=20000, tag="mc-sse")
+                secs.append(sec)
+            cg_extra["cpu_reference"] = {"ms": round(1e3 * statistics.median(secs), 2), "iterations": used_ref,
+                                         "cores": os.cpu_count(), "tag": "tags::CPU::MultiCore::SSE"}
+            cg_extra["speedup_vs_cpu_reference"] = round(1e3 * statistics.median(secs) / cg_extra["p50_ms"], 1)
+
+    return cg_extra
 
 
 def run_ours(args):
@@ -831,80 +967,36 @@ def run_ours(args):
         torch.cuda.synchronize()
         return replicas.max_over_ranks(e0.elapsed_time(e1))
 
+    def e2e_one_step():
+        xd[0].copy_(xh[0], non_blocking=True)
+        la.Product.value(yd[0], A, xd[0], ctx=ctx)
+        yh[0].copy_(yd[0], non_blocking=True)
+
+    e2e_one_ms = timed_e2e(lambda k: e2e_one_step())
+    e2e_one_value = ws * nbytes * args.steps / (e2e_one_ms / 1e3) / 1e9
     e2e_serial_ms = timed_e2e(lambda k: e2e_serial_step())
     ems = timed_e2e(e2e_step)
     e2e_value = ws * nbytes * apps / (ems / 1e3) / 1e9
     e2e_serial_value = ws * nbytes * apps / (e2e_serial_ms / 1e3) / 1e9
 
-    # ---- FP32 SpMV on the same matrix (extra) ----
-    A32 = A.to_float(ctx=ctx)
-    x32, y32 = x.float(), torch.empty(n, dtype=torch.float32, device="cuda")
-    for _ in range(3):
-        la.Product.value(y32, A32, x32, ctx=ctx)
-    torch.cuda.synchronize()
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(100):
-        la.Product.value(y32, A32, x32, ctx=ctx)
-    f1.record(stream)
-    torch.cuda.synchronize()
-    gbs32 = spmv_bytes(nnz, n, 4) * 100 / (f0.elapsed_time(f1) / 1e3) / 1e9
-    del A32, x32, y32
-
-    # ---- banded Q1 product (BandedMatrixQx<Q1Type>) of the same grid (extra) ----
-    band_extra = bench_q1band(la, ctx, x, per_launch_s, cpu=(ws == 1 and not args.no_cpu_baseline))
-    # ---- SparseMatrixCSR product of the same matrix (extra) ----
-    csr_extra = bench_csr(la, ctx, x, per_launch_s, cpu=(ws == 1 and not args.no_cpu_baseline))
-    # ---- SPAI2 preconditioner construction on the same grid (extra) ----
-    spai_extra = bench_spai2(la, ctx, cpu=(ws == 1 and not args.no_cpu_baseline))
-
-    # ---- plain FP64 CG on 257^2: solve latency (host b -> device solve -> host x) ----
-    Acg = la.SparseMatrixELL.q1_poisson(M_CG, ctx=ctx)
-    ncg = Acg.rows()
-    xt = torch.from_numpy(P.uniform_vector(ncg, 1)).cuda()
-    bcg = torch.empty_like(xt)
-    la.Product.value(bcg, Acg, xt, ctx=ctx)
-    bh = bcg.cpu().pin_memory()
-    xh_cg = torch.empty(ncg, dtype=torch.float64).pin_memory()
-    bd, xd_cg = torch.empty_like(bcg), torch.empty_like(bcg)
-    lat, iters = [], None
-    n_solves = 30
-    for i in range(n_solves + 3):
-        t0 = time.perf_counter()
-        bd.copy_(bh, non_blocking=True)
-        xd_cg.zero_()
-        iters = la.CGSolver.value(Acg, None, bd, xd_cg, 20000, 1e-8, ctx=ctx)
-        xh_cg.copy_(xd_cg, non_blocking=True)
-        torch.cuda.synchronize()
-        if i >= 3:
-            lat.append(time.perf_counter() - t0)
-    lat_ms = sorted(1e3 * v for v in lat)
-    cg_extra = {"workload": "plain FP64 CG, Q1 257^2, 1e-8 relative, x0 = 0", "iterations": iters,
-                "solves_per_s": round(len(lat) / sum(lat), 2),
-                "p50_ms": round(statistics.median(lat_ms), 3),
-                "p99_ms": round(lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))], 3)}
-    if ws == 1 and not args.no_cpu_baseline:
-        # the reference's own CGSolver<MultiCore::SSE> on the host cores, same system
-        R = _ref_cpu()
-        if R is not None:
-            Ah = P.q1_poisson(M_CG)
-            secs = []
-            for _ in range(3):
-                _, used_ref, sec = R.cg(Ah, bh.numpy(), eps=1e-8, max_iters=20000, tag="mc-sse")
-                secs.append(sec)
-            cg_extra["cpu_reference"] = {"ms": round(1e3 * statistics.median(secs), 2), "iterations": used_ref,
-                                         "cores": os.cpu_count(), "tag": "tags::CPU::MultiCore::SSE"}
-            cg_extra["speedup_vs_cpu_reference"] = round(1e3 * statistics.median(secs) / cg_extra["p50_ms"], 1)
-
-    cg_cluster = bench_cg_cluster(ctx)
-    cg_large = bench_cg_large(la, ctx, cpu=(ws == 1 and not args.no_cpu_baseline)) if not args.no_mg else None
-    batch_extra = None if args.no_batch else bench_batch(la, ctx, n_systems=args.batch_systems)
-    # the serving sample before the multi-second 2049^2 solves (their heat lowers the clocks)
-    serve_extra = None if (args.no_serve or rank != 0 and ws > 1) else bench_serve(
-        args.serve_requests, args.serve_prefix, args.serve_rate, device=local,
-        cpu=(ws == 1 and not args.no_cpu_baseline))
-    mg_extra = None if args.no_mg else bench_mg(la, ctx, cpu=(ws == 1 and not args.no_cpu_baseline))
-    ir_extra = None if args.no_mg else bench_ir(la, ctx)
+    # ---- extras: every other workload of the configurations, on one GPU only (the scaling runs
+    # time the headline product alone) ----
+    spmv_extra = band_extra = csr_extra = cg_extra = cg_cluster = cg_large = None
+    batch_extra = serve_extra = mg_extra = ir_extra = None
+    if ws == 1 and not args.no_extras:
+        cpu_on = not args.no_cpu_baseline
+        spmv_extra = bench_spmv_variants(la, ctx, cpu=cpu_on)
+        band_extra = bench_q1band(la, ctx, x, per_launch_s, cpu=cpu_on)
+        csr_extra = bench_csr(la, ctx, x, per_launch_s, cpu=cpu_on)
+        cg_extra = bench_cg_257(la, ctx, cpu=cpu_on)
+        cg_cluster = bench_cg_cluster(ctx)
+        cg_large = bench_cg_large(la, ctx, cpu=cpu_on) if not args.no_mg else None
+        batch_extra = None if args.no_batch else bench_batch(la, ctx, n_systems=args.batch_systems)
+        # the serving stream before the multi-second 2049^2 solves (their heat lowers the clocks)
+        serve_extra = None if args.no_serve else bench_serve(args.serve_requests, args.serve_prefix, args.serve_rate,
+                                                              device=local, cpu=cpu_on)
+        mg_extra = None if args.no_mg else bench_mg(la, ctx, cpu=cpu_on)
+        ir_extra = None if args.no_mg else bench_ir(la, ctx)
 
     line = None
     if rank == 0:
@@ -926,10 +1018,12 @@ def run_ours(args):
                     "d2h_bytes_per_step": n * 8, "api": "honei_b200.la.Product.value (C ABI hb_spmv_f64)",
                     "pipeline": "steps on three streams, double-buffered: upload of step k+1 and download of "
                                 "step k-1 overlap the products of step k",
-                    "serial_value": round(e2e_serial_value, 2)},
+                    "serial_value": round(e2e_serial_value, 2),
+                    "one_product_per_step": round(e2e_one_value, 2),
+                    "honei_plugin": plugin_e2e() if ws == 1 else None},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
-            "extra": {"spmv_f32_gbs": round(gbs32, 2), "q1band_2049": band_extra, "csr_2049": csr_extra, "spai2_2049": spai_extra,
+            "extra": {"spmv": spmv_extra, "q1band_2049": band_extra, "csr_2049": csr_extra,
                       "cg_257": cg_extra,
                       "cg_257_cluster": cg_cluster, "cg_large": cg_large,
                       "mg_2049": mg_extra, "ir_2049": ir_extra, "batch_512": batch_extra, "serve": serve_extra},
@@ -940,6 +1034,65 @@ def run_ours(args):
     return 0
 
 
+def run_case(name):
+    """One small workload for a profiler capture (ncu -k <kernel> ... python bench.py --case NAME):
+    spmv / spmv_permuted / spmv_ordered (2049^2 FP64 products), cg_2049 (the streaming CG kernel,
+    200 iterations), mg_2049 (one banded FP64 V(2,2) solve), batch_512 / batch_128 (the
+    512-system batch or its first 128 systems, tuned shape), q1batch (48 mid-size served systems in one batched MG-PCG launch), blas1 (dot,
+    norm and axpy on 2049^2 vectors).  Prints 'ok' and the case's own figure."""
+    import torch
+    from honei_b200 import la, problems as P
+    torch.cuda.set_device(0)
+    ctx = la.Context(0)
+    if name in ("spmv", "spmv_permuted", "spmv_ordered"):
+        if name == "spmv":
+            A = la.SparseMatrixELL.q1_poisson(M_SPMV, ctx=ctx)
+        else:
+            A = la.SparseMatrixELL.from_reference(P.q1_poisson_permuted(M_SPMV, 5)[0], ctx)
+            if name == "spmv_ordered":
+                A = A.ordered(columns=True, ctx=ctx)
+        x = torch.from_numpy(P.uniform_vector(M_SPMV ** 2, 6)).cuda()
+        y = torch.empty_like(x)
+        for _ in range(4):
+            la.Product.value(y, A, x, ctx=ctx)
+    elif name == "cg_2049":
+        A = la.SparseMatrixELL.q1_poisson(M_SPMV, ctx=ctx)
+        xt = torch.from_numpy(P.uniform_vector(A.rows(), 1)).cuda()
+        b = torch.empty_like(xt)
+        la.Product.value(b, A, xt, ctx=ctx)
+        print([la.CGSolver.value(A, None, b, torch.zeros_like(xt), 200, 1e-8, ctx=ctx) for _ in range(2)])
+    elif name == "mg_2049":
+        H = P.mg_hierarchy(M_SPMV)
+        data = la.MGData.from_hierarchy(H, np.float64, ctx=ctx, eps=1e-8, max_iters=100,
+                                        max_iters_coarse=MG_COARSE_ITERS, banded=True)
+        b = torch.from_numpy(P.uniform_vector(M_SPMV ** 2, 5)).cuda()
+        print(la.MGSolver.value(data, b, torch.zeros_like(b)))
+    elif name in ("batch_512", "batch_128"):
+        from honei_b200 import batch as B
+        sides = np.random.default_rng(2024).integers(17, 258, size=512)[:int(name.split("_")[1])]
+        systems = B.q1_batch(sides, coef_range=(1e-1, 1e1), seed=2024, mode="cg64", eps=1e-8)
+        res = B.BatchSolver(systems, ctx=ctx).solve(B.HbBatchConfig(2, 512))
+        print(sum(r["iterations"] for r in res))
+    elif name == "q1batch":
+        from honei_b200 import serve as S
+        tr = S.poisson_trace(48, rate=0.0, side_range=(97, 300), seed=3)
+        with S.Server(mode="mixed", small_max_side=96, mid_max_side=300) as srv:
+            print(S.replay(srv, tr, realtime=False)["paths"])
+    elif name == "blas1":
+        n = M_SPMV ** 2
+        x = torch.from_numpy(P.uniform_vector(n, 1)).cuda()
+        y = torch.from_numpy(P.uniform_vector(n, 2)).cuda()
+        for _ in range(3):
+            la.DotProduct.value(x, y, ctx=ctx)
+            la.Norm.value(x, root=True, ctx=ctx)
+            la.ScaledSum.value(x, y, 0.5, ctx=ctx)
+    else:
+        raise SystemExit(f"unknown case {name}")
+    torch.cuda.synchronize()
+    print("ok")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -947,6 +1100,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="the headline product only")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-system batched workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream workload")
     ap.add_argument("--batch-systems", type=int, default=512, help="systems in the batched workload")
@@ -955,7 +1109,10 @@ def main():
     ap.add_argument("--serve-prefix", type=int, default=2000,
                     help="first requests of the stream served by the plain FP64 CG baselines")
     ap.add_argument("--serve-rate", type=float, default=SERVE_RATE, help="Poisson arrivals per second (latency)")
+    ap.add_argument("--case", default=None, help="run one small workload for a profiler capture and exit")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args.case)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)

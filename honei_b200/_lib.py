@@ -69,6 +69,9 @@ SIGNATURES = {
     "hb_ell_cm_order": (i32, [vp, P_ell, vp, vp, P_i64]),
     "hb_ell_bandwidth": (i32, [vp, P_ell, vp, P_i64]),
     "hb_ell_permute": (i32, [vp, P_ell, vp, vp, P_ell]),
+    "hb_ell_permute_sorted": (i32, [vp, P_ell, vp, vp, P_ell, vp]),
+    "hb_spmv_ranked_f64": (i32, [vp, P_ell, vp, vp, vp, vp]),
+    "hb_spmv_ranked_f32": (i32, [vp, P_ell, vp, vp, vp, vp]),
     "hb_spmv_rows_f64": (i32, [vp, P_ell, vp, vp, vp]),
     "hb_spmv_rows_f32": (i32, [vp, P_ell, vp, vp, vp]),
     "hb_gather_f64": (i32, [vp, i64, vp, vp, vp]),

@@ -189,6 +189,53 @@ __global__ void ell_bandwidth_kernel(int64_t rows, int64_t ld, int K, const int3
     if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
 }
 
+// B row kk = A row order[kk] with its columns renumbered through pos and its valid slots sorted
+// by the new column (one thread per row; import-time work).  ranks[kk] packs, 4 bits per
+// physical slot k, the rank of that slot in A's row (its place in the reference's summation
+// order); padding slots (Aj = -1) follow the valid ones.
+template <typename T, int KMAX>
+__global__ void ell_permute_sorted_kernel(int64_t rows, int64_t ld, int K, const int32_t *__restrict__ Aj,
+                                          const T *__restrict__ Ax, const int32_t *__restrict__ order,
+                                          const int32_t *__restrict__ pos, int32_t *__restrict__ Bj,
+                                          T *__restrict__ Bx, unsigned long long *__restrict__ ranks)
+{
+    for (int64_t kk = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; kk < ld; kk += (int64_t)gridDim.x * blockDim.x) {
+        int32_t c[KMAX];
+        T a[KMAX];
+        int rk[KMAX];
+        int n = 0;
+        if (kk < rows) {
+            const int64_t r = order[kk];
+            for (int k = 0; k < K; ++k) {
+                const int32_t j = Aj[(int64_t)k * ld + r];
+                if (j < 0) continue;
+                // insertion by new column; equal columns keep their original order
+                const int32_t cj = pos[j];
+                const T aj = Ax[(int64_t)k * ld + r];
+                int at = n;
+                while (at > 0 && c[at - 1] > cj) {
+                    c[at] = c[at - 1];
+                    a[at] = a[at - 1];
+                    rk[at] = rk[at - 1];
+                    --at;
+                }
+                c[at] = cj;
+                a[at] = aj;
+                rk[at] = n;
+                ++n;
+            }
+        }
+        unsigned long long packed = 0;
+        for (int k = 0; k < K; ++k) {
+            const bool v = k < n;
+            Bj[(int64_t)k * ld + kk] = v ? c[k] : -1;
+            Bx[(int64_t)k * ld + kk] = v ? a[k] : T(0);
+            packed |= (unsigned long long)(v ? rk[k] : 15) << (4 * k);
+        }
+        if (kk < rows) ranks[kk] = packed;
+    }
+}
+
 // B row kk = A row order[kk], slots unchanged; columns renumbered through pos when given.
 template <typename T>
 __global__ void ell_permute_kernel(int64_t rows, int64_t ld, int K, const int32_t *__restrict__ Aj,
@@ -234,6 +281,40 @@ ell_spmv_rows_kernel(int64_t rows, int64_t ld, int K, const int32_t *__restrict_
     }
 }
 
+// The product through a sorted, ranked copy (ell_permute_sorted_kernel): one row per thread,
+// the products of its slots (physical order, so a warp's gathers for one slot are neighbours)
+// parked in shared memory at their ranks, then summed in rank order -- the order the
+// reference sums the row in.  y[order[r]] = the sum.
+constexpr int RANKED_THREADS = 256;
+template <typename T, int KT>
+__global__ void __launch_bounds__(RANKED_THREADS)
+ell_spmv_ranked_kernel(int64_t rows, int64_t ld, int K, const int32_t *__restrict__ Aj, const T *__restrict__ Ax,
+                       const unsigned long long *__restrict__ ranks, const T *__restrict__ x,
+                       const int32_t *__restrict__ order, T *__restrict__ y)
+{
+    constexpr int KS = KT > 0 ? KT : 16;
+    __shared__ T park[KS * RANKED_THREADS];
+    const int K_ = KT > 0 ? KT : K;
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    const unsigned long long rk = __ldg(ranks + r);
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < KS; ++k) {
+        if (k >= K_) break;
+        const int32_t j = __ldcs(Aj + (int64_t)k * ld + r);
+        const T a = __ldcs(Ax + (int64_t)k * ld + r);
+        if (j >= 0) {
+            const int at = (int)((rk >> (4 * k)) & 15ull);
+            park[at * RANKED_THREADS + threadIdx.x] = hbd::mul(a, __ldg(x + j));
+            ++cnt;
+        }
+    }
+    T sum = T(0);
+    for (int k = 0; k < cnt; ++k) sum = hbd::add(sum, park[k * RANKED_THREADS + threadIdx.x]);
+    y[__ldg(order + r)] = sum;
+}
+
 // xw[k] = x[order[k]]
 template <typename T>
 __global__ void gather_kernel(int64_t n, const int32_t *__restrict__ order, const T *__restrict__ x, T *__restrict__ xw)
@@ -261,6 +342,27 @@ int spmv_rows_impl(hb_context *ctx, const hb_ell *B, int dtype, const int32_t *o
         ell_spmv_rows_kernel<T, 0><<<blocks, ROWS_THREADS, 0, ctx->stream>>>(B->rows, B->ld, (int)B->K, B->Aj, Bx, x,
                                                                              order, y);
     return hb_check_launch(ctx, "ell_spmv_rows_kernel");
+}
+
+template <typename T>
+int spmv_ranked_impl(hb_context *ctx, const hb_ell *B, int dtype, const int32_t *order,
+                     const unsigned long long *ranks, const T *x, T *y)
+{
+    if (!ctx) return HB_ERR_INVALID;
+    int st = hb_check_ell(B, dtype);
+    if (st) return st;
+    if (B->K > 16) return HB_ERR_UNSUPPORTED;
+    if (B->rows == 0) return HB_OK;
+    if (!order || !ranks || !x || !y) return HB_ERR_INVALID;
+    const unsigned blocks = (unsigned)((B->rows + RANKED_THREADS - 1) / RANKED_THREADS);
+    const T *Bx = (const T *)B->Ax;
+    if (B->K == 9)
+        ell_spmv_ranked_kernel<T, 9><<<blocks, RANKED_THREADS, 0, ctx->stream>>>(B->rows, B->ld, 9, B->Aj, Bx, ranks, x,
+                                                                                 order, y);
+    else
+        ell_spmv_ranked_kernel<T, 0><<<blocks, RANKED_THREADS, 0, ctx->stream>>>(B->rows, B->ld, (int)B->K, B->Aj, Bx,
+                                                                                 ranks, x, order, y);
+    return hb_check_launch(ctx, "ell_spmv_ranked_kernel");
 }
 
 template <typename T>
@@ -350,6 +452,46 @@ int hb_ell_permute(hb_context *ctx, const hb_ell *A, const int32_t *order, const
                                                                    (const float *)A->Ax, order, pos, B->Aj,
                                                                    (float *)B->Ax);
     return hb_check_launch(ctx, "ell_permute_kernel");
+}
+
+int hb_ell_permute_sorted(hb_context *ctx, const hb_ell *A, const int32_t *order, const int32_t *pos, hb_ell *B,
+                          uint64_t *ranks)
+{
+    HB_RANGE("hb_ell_permute_sorted");
+    if (!ctx || !B || !order || !pos || !ranks) return HB_ERR_INVALID;
+    int st = hb_check_ell(A, A ? A->dtype : 0);
+    if (st) return st;
+    if (A->rows != A->cols) return HB_ERR_SIZE;
+    if (A->K > 16) return HB_ERR_UNSUPPORTED;
+    if (B->K != A->K || B->ld != A->ld || B->Aj == A->Aj || B->Ax == A->Ax) return HB_ERR_SIZE;
+    B->rows = A->rows;
+    B->cols = A->cols;
+    B->dtype = A->dtype;
+    st = hb_check_ell(B, A->dtype);
+    if (st) return st;
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((A->ld + 255) / 256, (int64_t)ctx->num_sms * 32));
+    unsigned long long *rk = (unsigned long long *)ranks;
+    if (A->dtype == HB_F64)
+        ell_permute_sorted_kernel<double, 16><<<blocks, 256, 0, ctx->stream>>>(
+            A->rows, A->ld, (int)A->K, A->Aj, (const double *)A->Ax, order, pos, B->Aj, (double *)B->Ax, rk);
+    else
+        ell_permute_sorted_kernel<float, 16><<<blocks, 256, 0, ctx->stream>>>(
+            A->rows, A->ld, (int)A->K, A->Aj, (const float *)A->Ax, order, pos, B->Aj, (float *)B->Ax, rk);
+    return hb_check_launch(ctx, "ell_permute_sorted_kernel");
+}
+
+int hb_spmv_ranked_f64(hb_context *ctx, const hb_ell *B, const int32_t *order, const uint64_t *ranks, const double *x,
+                       double *y)
+{
+    HB_RANGE("hb_spmv_ranked_f64");
+    return spmv_ranked_impl<double>(ctx, B, HB_F64, order, (const unsigned long long *)ranks, x, y);
+}
+
+int hb_spmv_ranked_f32(hb_context *ctx, const hb_ell *B, const int32_t *order, const uint64_t *ranks, const float *x,
+                       float *y)
+{
+    HB_RANGE("hb_spmv_ranked_f32");
+    return spmv_ranked_impl<float>(ctx, B, HB_F32, order, (const unsigned long long *)ranks, x, y);
 }
 
 int hb_spmv_rows_f64(hb_context *ctx, const hb_ell *B, const int32_t *order, const double *x, double *y)

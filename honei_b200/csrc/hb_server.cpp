@@ -37,15 +37,27 @@ struct Item {
     int path = 0;
 };
 
-int64_t estimate_bytes(int64_t M)
+// Device bytes a request of side M holds while resident on a path: a fixed 1 MiB (launch
+// workspaces, descriptors, pool granularity) plus a per-row charge 15-25 % above what the
+// stream-ordered pool was measured to hold per row on a B200 (one request at a time, sides 33 to
+// 1025): batched FP32-inner refinement 204-215 B (FP64 + FP32 matrix values, int32 columns,
+// coefficients, b, x, the batch work vectors); the MG-preconditioned paths 414-428 B (the
+// device-built Galerkin hierarchy in FP64 and FP32, its banded copies and the refinement and PCG
+// vectors); plain CG 140-146 B; batched plain CG 172-181 B.
+int64_t estimate_bytes(int path, int64_t M)
 {
-    // matrix (FP64 + FP32 values, int32 indices, 9 slots) + MG levels + vectors + work,
-    // generously rounded; the same estimate for every path keeps admission comparable
     const int64_t n = M * M;
-    return (int64_t(1) << 20) + 320 * n;
+    int64_t per_row = 256;
+    if (path == HB_PATH_MGPCG || path == HB_PATH_MGBATCH) per_row = 512;
+    else if (path == HB_PATH_CG64) per_row = 176;
+    else if (path == HB_PATH_BATCH_CG64) per_row = 224;
+    return (int64_t(1) << 20) + per_row * n;
 }
 
 }  // namespace
+
+struct hb_server;
+static int route(const hb_server *s, int64_t M);
 
 struct hb_server {
     hb_server_params p{};
@@ -194,6 +206,20 @@ int true_relres(hb_context *ctx, const hb_ell &A, const double *b, const double 
     return st;
 }
 
+}  // namespace
+
+// The path a request of side M takes on this server.
+static int route(const hb_server *s, int64_t M)
+{
+    if (s->p.mode == HB_SERVE_PLAIN_CG64) return HB_PATH_CG64;
+    if (s->p.mode == HB_SERVE_PLAIN_CG64_BATCHED) return M <= s->p.mid_max_side ? HB_PATH_BATCH_CG64 : HB_PATH_CG64;
+    if (M <= s->p.small_max_side) return HB_PATH_BATCH;
+    if (M <= s->p.mid_max_side) return HB_PATH_MGBATCH;
+    return HB_PATH_MGPCG;
+}
+
+namespace {
+
 void admit_loop(hb_server *s)
 {
     std::unique_lock<std::mutex> l(s->mu);
@@ -208,22 +234,9 @@ void admit_loop(hb_server *s)
         s->in_use += it->bytes;
         s->peak = std::max(s->peak, s->in_use);
         it->t_admit = s->now();
-        if (s->p.mode == HB_SERVE_PLAIN_CG64) {
-            it->path = HB_PATH_CG64;
-            s->large_q.push_back(it);
-        } else if (s->p.mode == HB_SERVE_PLAIN_CG64_BATCHED) {
-            it->path = it->r.M <= s->p.mid_max_side ? HB_PATH_BATCH_CG64 : HB_PATH_CG64;
-            (it->path == HB_PATH_CG64 ? s->large_q : s->small_q).push_back(it);
-        } else if (it->r.M <= s->p.small_max_side) {
-            it->path = HB_PATH_BATCH;
-            s->small_q.push_back(it);
-        } else if (it->r.M <= s->p.mid_max_side) {
-            it->path = HB_PATH_MGBATCH;
-            s->mid_q.push_back(it);
-        } else {
-            it->path = HB_PATH_MGPCG;
-            s->large_q.push_back(it);
-        }
+        if (it->path == HB_PATH_BATCH || it->path == HB_PATH_BATCH_CG64) s->small_q.push_back(it);
+        else if (it->path == HB_PATH_MGBATCH) s->mid_q.push_back(it);
+        else s->large_q.push_back(it);
         s->cv_work.notify_all();
     }
 }
@@ -517,7 +530,8 @@ int hb_server_submit(hb_server *s, const hb_request *req)
     if (req->M * req->M > INT32_MAX) return HB_ERR_UNSUPPORTED;
     Item *it = new Item();
     it->r = *req;
-    it->bytes = estimate_bytes(req->M);
+    it->path = route(s, req->M);
+    it->bytes = estimate_bytes(it->path, req->M);
     std::lock_guard<std::mutex> l(s->mu);
     if (it->bytes > s->p.hbm_budget_bytes) {
         delete it;

@@ -267,18 +267,25 @@ class SparseMatrixELL:
     def ordered(self, columns: bool = True, ctx: Context | None = None) -> "OrderedMatrixELL":
         """A copy stored in the Cuthill-McKee locality order, for products with a badly numbered
         matrix (e.g. a randomly permuted grid).  Product.value on the copy gives y = A x bit for
-        bit.  columns=True renumbers the columns too (local gathers; x is permuted into a work
-        vector first); columns=False keeps A's columns (no work vector; gathers stay scattered,
-        rows that share columns run together)."""
+        bit.  columns=True renumbers the columns too and stores each row's slots by new column
+        with their summation ranks (local gathers; x is permuted into a work vector first);
+        columns=False keeps A's columns (no work vector; gathers stay scattered, rows that share
+        columns run together)."""
         ctx = ctx or default_context()
         order, pos, info = self.cm_order(ctx)
         Aj = torch.empty_like(self.Aj)
         Ax = torch.empty_like(self.Ax)
         B = HbEll(self._rows, self._cols, self.K, self.ld, Aj.data_ptr(), Ax.data_ptr(), _DT[self.dtype], 0)
-        check(lib().hb_ell_permute(ctx.handle, C.byref(self._s), order.data_ptr(),
-                                   pos.data_ptr() if columns else None, C.byref(B)), "hb_ell_permute", ctx.handle)
+        ranks = None
+        if columns:
+            ranks = torch.empty(max(self._rows, 1), dtype=torch.int64, device=self.Aj.device)
+            check(lib().hb_ell_permute_sorted(ctx.handle, C.byref(self._s), order.data_ptr(), pos.data_ptr(),
+                                              C.byref(B), ranks.data_ptr()), "hb_ell_permute_sorted", ctx.handle)
+        else:
+            check(lib().hb_ell_permute(ctx.handle, C.byref(self._s), order.data_ptr(), None, C.byref(B)),
+                  "hb_ell_permute", ctx.handle)
         return OrderedMatrixELL(SparseMatrixELL(self._rows, self._cols, self.K, self.ld, Aj, Ax), order, pos,
-                                columns, info)
+                                columns, info, ranks)
 
 
 class OrderedMatrixELL:
@@ -286,9 +293,11 @@ class OrderedMatrixELL:
     A in `order`, with its columns renumbered through `pos` when `columns`.  Products through it
     equal A's bit for bit."""
 
-    def __init__(self, B: SparseMatrixELL, order: torch.Tensor, pos: torch.Tensor, columns: bool, info=None):
+    def __init__(self, B: SparseMatrixELL, order: torch.Tensor, pos: torch.Tensor, columns: bool, info=None,
+                 ranks: torch.Tensor | None = None):
         self.B, self.order, self.pos, self.columns_renumbered = B, order, pos, columns
         self.info = info
+        self.ranks = ranks
         self.dtype = B.dtype
         self._xw = None
 
@@ -307,6 +316,10 @@ class OrderedMatrixELL:
             check(getattr(lib(), f"hb_gather_{suf}")(ctx.handle, self.B.rows(), self.order.data_ptr(), xp,
                                                      self._xw.data_ptr()), "hb_gather", ctx.handle)
             xp = self._xw.data_ptr()
+            check(getattr(lib(), f"hb_spmv_ranked_{suf}")(ctx.handle, C.byref(self.B.struct), self.order.data_ptr(),
+                                                          self.ranks.data_ptr(), xp, _vec(y, self.dtype, "y")),
+                  "Product", ctx.handle)
+            return y
         check(getattr(lib(), f"hb_spmv_rows_{suf}")(ctx.handle, C.byref(self.B.struct), self.order.data_ptr(), xp,
                                                     _vec(y, self.dtype, "y")), "Product", ctx.handle)
         return y

@@ -201,10 +201,10 @@ class Server:
     device bytes of the admitted requests; a request above the budget alone is refused at
     submit with HB_ERR_CAPACITY."""
 
-    def __init__(self, mode: str = "mixed", budget_bytes: int = 64 << 30, large_workers: int = 12,
-                 small_workers: int = 1, small_max_side: int = 96, max_batch: int = 256, cluster: int = 2,
+    def __init__(self, mode: str = "mixed", budget_bytes: int = 64 << 30, large_workers: int = 16,
+                 small_workers: int = 2, small_max_side: int = 96, max_batch: int = 32, cluster: int = 2,
                  threads: int = 512, max_clusters: int = 0, eps: float = 1e-8, inner_eps: float = 1e-3,
-                 device: int = 0, pinned: bool = True, mid_max_side: int = 300, mid_workers: int = 1,
+                 device: int = 0, pinned: bool = True, mid_max_side: int = 300, mid_workers: int = 3,
                  mid_cluster: int = 16, mid_threads: int = 512, mid_max_clusters: int = 0):
         self._lib = _register()
         prm = HbServerParams()

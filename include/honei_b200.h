@@ -130,6 +130,21 @@ int hb_ell_permute(hb_context *ctx, const hb_ell *A, const int32_t *order, const
  * must be 16-byte aligned.  Asynchronous. */
 int hb_spmv_rows_f64(hb_context *ctx, const hb_ell *B, const int32_t *order, const double *x, double *y);
 int hb_spmv_rows_f32(hb_context *ctx, const hb_ell *B, const int32_t *order, const float *x, float *y);
+/* The copy whose gathers are local: B row k = A row order[k] with its columns renumbered through
+ * pos (B = P A P^T, square A) and its stored slots sorted by the new column, so the slots of
+ * neighbouring rows point at neighbouring entries of the permuted x.  ranks (device uint64[rows])
+ * records, 4 bits per stored slot, that slot's place in A's row -- the reference's summation
+ * order -- so the product can still add in that order.  K <= 16 (HB_ERR_UNSUPPORTED above).
+ * B has A's K and ld and its own arrays (caller-allocated).  Asynchronous. */
+int hb_ell_permute_sorted(hb_context *ctx, const hb_ell *A, const int32_t *order, const int32_t *pos, hb_ell *B,
+                          uint64_t *ranks);
+/* The product through such a sorted copy: y[order[k]] = B's row k summed in the ranks' order,
+ * with x already permuted (hb_gather: xw[k] = x[order[k]]); y = A x bit for bit (one row per
+ * thread; each row's products wait in shared memory for their turn).  Asynchronous. */
+int hb_spmv_ranked_f64(hb_context *ctx, const hb_ell *B, const int32_t *order, const uint64_t *ranks, const double *x,
+                       double *y);
+int hb_spmv_ranked_f32(hb_context *ctx, const hb_ell *B, const int32_t *order, const uint64_t *ranks, const float *x,
+                       float *y);
 /* xw[k] = x[order[k]], k < n.  Asynchronous. */
 int hb_gather_f64(hb_context *ctx, int64_t n, const int32_t *order, const double *x, double *xw);
 int hb_gather_f32(hb_context *ctx, int64_t n, const int32_t *order, const float *x, float *xw);

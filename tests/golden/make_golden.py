@@ -39,9 +39,11 @@ readers, honei/math/matrix_io.hh and honei/math/vector_io.hh):
 * batch512.npz -- the 512-system batch workload (SPD Q1 systems, side U{17..257} from seed 2024,
   cellwise coefficient 10^U(-1,1) with seed 2024 + i, x_true U[-1,1] with seed 2024 + i + 1,
   b = A x_true): for every system, the iteration count and final true relative residual of
-  CGSolver<tags::CPU, NONE> and of CGSolver<tags::CPU::SSE, NONE> (eps 1e-8, x0 = 0).  The two
-  tags differ only in the summation order of their dot products; their spread is the measured
-  sensitivity of these solves to that order.  Needs only oracle/_ref (no HONEI tree).
+  CGSolver<tags::CPU, NONE>, of CGSolver<tags::CPU::SSE, NONE> and of
+  CGSolver<tags::CPU::MultiCore::SSE, NONE> on 4 and on 16 threads (eps 1e-8, x0 = 0).  The tags
+  differ only in the summation order of their dot products; their spread is the measured
+  sensitivity of these solves to that order.  Needs only oracle/_ref (no HONEI tree).  An
+  existing file keeps the columns it has; missing ones are added.
 
     python tests/golden/make_golden.py [/path/to/honei-tree] [--only q1band|pcg|csr|spai2|batch512]
 """
@@ -331,11 +333,31 @@ def batch512(R):
             row += [u, np.linalg.norm(O.defect(A, b, x)) / nb]
         return row
 
-    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
-        rows = list(ex.map(one, range(len(sides))))
-    r = np.array(rows)
-    np.savez_compressed(os.path.join(HERE, "batch512.npz"), sides=sides, cpu_used=r[:, 0].astype(np.int64),
-                        cpu_relres=r[:, 1], sse_used=r[:, 2].astype(np.int64), sse_relres=r[:, 3])
+    path = os.path.join(HERE, "batch512.npz")
+    out = dict(np.load(path)) if os.path.exists(path) else {}
+    if "cpu_used" not in out:
+        with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+            r = np.array(list(ex.map(one, range(len(sides)))))
+        out.update(sides=sides, cpu_used=r[:, 0].astype(np.int64), cpu_relres=r[:, 1],
+                   sse_used=r[:, 2].astype(np.int64), sse_relres=r[:, 3])
+    # the MultiCore tag runs its own thread pool: one system at a time, on 4 threads (the
+    # honeirc default) and on 16; every dot product is split into that many partial sums
+    for threads in (4, 16):
+        if f"mc{threads}_used" in out:
+            continue
+        R.set_threads(threads)
+        used, rel = [], []
+        for i in range(len(sides)):
+            M = int(sides[i])
+            A = P.q1_poisson(M, P.log_uniform_coef(M, 1e-1, 1e1, BATCH_SEED + i), symmetric=True)
+            b, _ = R.spmv(A, P.uniform_vector(M * M, BATCH_SEED + i + 1))
+            x, u, _ = R.cg(A, b, eps=1e-8, max_iters=100000, tag="mc-sse")
+            used.append(u)
+            rel.append(np.linalg.norm(O.defect(A, b, x)) / np.linalg.norm(b))
+        out[f"mc{threads}_used"] = np.array(used, np.int64)
+        out[f"mc{threads}_relres"] = np.array(rel)
+        np.savez_compressed(path, **out)
+    np.savez_compressed(path, **out)
 
 
 if __name__ == "__main__":

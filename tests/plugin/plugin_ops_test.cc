@@ -28,6 +28,7 @@
 #include <honei/math/spai2.hh>
 #include <honei/math/vector_io.hh>
 
+#include <chrono>
 #include <cstring>
 #include <iostream>
 #include <sstream>
@@ -150,7 +151,7 @@ void generic_cg()
     report((uc > ug ? uc - ug : ug - uc) <= 1 && rel < 1.5e-8, "generic CGSolver<GPU::CUDA, NONE> vs tags::CPU", d.str());
 }
 
-template <typename Tag_> void run_mg(const std::string & dir, unsigned long L, DenseVector<double> & x_out,
+template <typename Tag_> double run_mg(const std::string & dir, unsigned long L, DenseVector<double> & x_out,
         unsigned long & cycles)
 {
     typedef MGUtil<Tag_, SparseMatrixELL<double>, DenseVector<double>, SparseMatrixELL<double>, DenseVector<double>,
@@ -160,17 +161,23 @@ template <typename Tag_> void run_mg(const std::string & dir, unsigned long L, D
     Util::configure(data, 100, 1000, 2, 2, 1, 1e-8);
     OperatorList ol(MGCycleCreation<Tag_, methods::CYCLE::V::STATIC, CGSolver<Tag_, methods::NONE>, RISmoother<Tag_>,
             Restriction<Tag_, methods::PROLMAT>, Prolongation<Tag_, methods::PROLMAT>, double>::value(data));
+    const auto t0(std::chrono::steady_clock::now());
     MGSolver<Tag_, Norm<vnt_l_two, true, Tag_> >::value(data, ol);
+    data.x.back().lock(lm_read_only);
+    data.x.back().unlock(lm_read_only);
+    const double ms(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
     cycles = data.used_iters;
     x_out = data.x.back().copy();
+    return ms;
 }
 
 void generic_mg(const std::string & dir, unsigned long L)
 {
     DenseVector<double> xc(1), xg(1);
     unsigned long cc(0), cg(0);
-    run_mg<tags::CPU>(dir, L, xc, cc);
-    run_mg<tags::GPU::CUDA>(dir, L, xg, cg);
+    const double msc(run_mg<tags::CPU>(dir, L, xc, cc));
+    run_mg<tags::GPU::CUDA>(dir, L, xg, cg);                 // first solve: uploads and mirrors
+    const double msg(run_mg<tags::GPU::CUDA>(dir, L, xg, cg));
     double err(0), nrm(0);
     xc.lock(lm_read_only);
     xg.lock(lm_read_only);
@@ -182,7 +189,8 @@ void generic_mg(const std::string & dir, unsigned long L)
     xc.unlock(lm_read_only);
     xg.unlock(lm_read_only);
     std::ostringstream d;
-    d << "cycles cpu " << cc << " gpu " << cg << ", max |x_gpu - x_cpu| / max |x| = " << err / nrm;
+    d << "cycles cpu " << cc << " gpu " << cg << ", max |x_gpu - x_cpu| / max |x| = " << err / nrm << ", ms cpu "
+      << msc << " gpu " << msg;
     report((cc > cg ? cc - cg : cg - cc) <= 1 && err <= 1e-6 * nrm, "MGSolver<GPU::CUDA> (MGUtil::load_data, V(2,2), jac)",
             d.str());
 }

@@ -162,13 +162,14 @@ def test_batch_512_cg64_within_the_references_own_spread(hb, oracle):
     system (tests/golden/batch512.npz, written by the compiled reference).
 
     On these systems (contrast 10^2, up to 872 iterations) the iteration count at which the
-    1e-8 test fires depends on the summation order of the dot products: the reference's own
-    tags::CPU::SSE, which differs from tags::CPU only in that order, lands on tags::CPU's count
-    for 239 of the 512 systems, one apart for 192 and up to 6 apart for the rest (the same
-    fixture).  The bar is therefore the reference's own spread: per system, the GPU count
-    within the largest tags::CPU / tags::CPU::SSE difference of the batch (and within 1 where
-    that is smaller), the final true residual below the target, and its distance from
-    tags::CPU's within the largest such distance between the two reference tags."""
+    1e-8 test fires depends on the summation order of the dot products.  The reference's own
+    tags show it: tags::CPU::SSE, tags::CPU::MultiCore::SSE on 4 and on 16 threads differ from
+    tags::CPU only in that order, and land on tags::CPU's count for 180 to 239 of the 512
+    systems, up to 6 or 7 iterations apart on others (the same fixture).  The GPU sums each dot
+    product as a tree over the cluster's 1024 threads.  The bar is therefore the reference's own
+    spread: the largest and the mean |iterations - tags::CPU's| over the batch within the largest
+    such figures of the reference's tags, every final true residual below the target, and its
+    distance from tags::CPU's within the largest such distance between the reference's tags."""
     from conftest import load_golden
     from honei_b200 import batch as B
     g = load_golden("batch512")
@@ -176,21 +177,25 @@ def test_batch_512_cg64_within_the_references_own_spread(hb, oracle):
     assert np.array_equal(sides, g["sides"])
     systems = B.q1_batch(sides, coef_range=(1e-1, 1e1), seed=BATCH_SEED, mode="cg64", eps=1e-8)
     res = B.BatchSolver(systems).solve(B.HbBatchConfig(2, 512))
-    du_ref = np.abs(g["sse_used"] - g["cpu_used"])
-    dr_ref = np.abs(g["sse_relres"] - g["cpu_relres"])
-    D, Rr = max(1, int(du_ref.max())), float(dr_ref.max())
+    tags = [t for t in ("sse", "mc4", "mc16") if f"{t}_used" in g]
+    d_ref = {t: np.abs(g[f"{t}_used"] - g["cpu_used"]) for t in tags}
+    r_ref = {t: np.abs(g[f"{t}_relres"] - g["cpu_relres"]) for t in tags}
+    D = max(1, max(int(d.max()) for d in d_ref.values()))
+    Dmean = max(float(d.mean()) for d in d_ref.values())
+    Rr = max(float(r.max()) for r in r_ref.values())
     u_g = np.array([r["iterations"] for r in res])
     r_g = np.array([r["true_relres"] for r in res])
     st = np.array([r["status"] for r in res])
     du = np.abs(u_g - g["cpu_used"])
     dr = np.abs(r_g - g["cpu_relres"])
-    print(f"batch 512 cg64: |GPU - tags::CPU| iterations: {np.sum(du == 0)} equal, {np.sum(du == 1)} one apart, "
-          f"max {du.max()}, mean {du.mean():.2f}; tags::CPU::SSE: {np.sum(du_ref == 0)} equal, "
-          f"{np.sum(du_ref == 1)} one apart, max {du_ref.max()}, mean {du_ref.mean():.2f}; residual gap max "
-          f"{dr.max():.3e} (SSE {Rr:.3e})")
+    ref_txt = "; ".join(f"{t}: {int(np.sum(d == 0))} equal, max {int(d.max())}, mean {d.mean():.2f}"
+                        for t, d in d_ref.items())
+    print(f"batch 512 cg64: |GPU - tags::CPU| iterations: {int(np.sum(du == 0))} equal, {int(np.sum(du == 1))} "
+          f"one apart, max {int(du.max())}, mean {du.mean():.2f}; reference tags: {ref_txt}; residual gap max "
+          f"{dr.max():.3e} (reference tags {Rr:.3e})")
     assert np.all(st == 0)
     assert np.all(r_g < 1e-8 * (1 + 1e-6)), r_g.max()
-    assert du.max() <= D, (du.max(), D)
+    assert du.max() <= D and du.mean() <= Dmean, (int(du.max()), D, du.mean(), Dmean)
     assert dr.max() <= Rr, (dr.max(), Rr)
     # spot check: the device-reported true residual is the host's on a few systems
     for i in (0, 17, 255):

@@ -64,6 +64,14 @@ def test_plugin_mg_fast_path(tmp_path):
     plugin's specialisations (honei_b200/plugin/mg_b200.hh), on a hierarchy loaded by
     MGUtil::load_data: smoother sweeps and one coarse-free cycle bit-exact to tags::CPU, the
     solve within +-1 cycle and 1e-10 of tags::CPU's residual, IRSolver within +-1 outer step."""
+    import re
     L = _write_hierarchy(tmp_path, 257)
     out = _run("plugin_mg_test", str(tmp_path), str(L))
     assert out.count("PASS") == 5 and "FAIL" not in out
+    # the same solve through HONEI's generic templates on the GPU tag (one operator call per
+    # step of the cycle, tests/plugin/plugin_ops_test.cc): same cycles, slower
+    gen = _run("plugin_ops_test", str(tmp_path), str(L))
+    fast_ms = float(re.search(r"fast path vs tags::CPU.*ms cpu \S+ gpu (\S+)", out).group(1))
+    gen_ms = float(re.search(r"MGSolver<GPU::CUDA> \(MGUtil.*ms cpu \S+ gpu (\S+)", gen).group(1))
+    print(f"MGSolver<GPU::CUDA> 257^2: fast path {fast_ms:.1f} ms, generic operator path {gen_ms:.1f} ms")
+    assert fast_ms < gen_ms
