@@ -386,7 +386,7 @@ def bench_batch(la, ctx, n_systems=512, seed=2024):
         ms = e0.elapsed_time(e1)
         res = solver.results()
         out[mode] = {"ms": round(ms, 2), "systems_per_s": round(n_systems / (ms / 1e3), 1),
-                     "config": {"cluster": cfg.cluster, "threads": cfg.threads},
+                     "config": {"cluster": cfg.cluster, "threads": cfg.threads, "rows_per_thread": cfg.rows_per_thread},
                      "iterations_mean": round(float(np.mean([r["iterations"] for r in res])), 1),
                      "max_true_relres": float(max(r["true_relres"] for r in res)),
                      "tune_ms": getattr(solver, "tune_times", None)}

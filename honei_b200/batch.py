@@ -26,6 +26,7 @@ from .la import SparseMatrixELL, default_context
 HB_BATCH_CG64, HB_BATCH_IR32 = 0, 1
 CLUSTERS = (1, 2, 4, 8, 16)
 THREADS = (256, 512)
+ROWS_PER_THREAD = (4, 1)
 
 
 class HbBatchSystem(C.Structure):
@@ -40,7 +41,8 @@ class HbBatchResult(C.Structure):
 
 
 class HbBatchConfig(C.Structure):
-    _fields_ = [("cluster", C.c_int32), ("threads", C.c_int32), ("max_clusters", C.c_int32)]
+    _fields_ = [("cluster", C.c_int32), ("threads", C.c_int32), ("max_clusters", C.c_int32),
+                ("rows_per_thread", C.c_int32)]
 
 
 def _register():
@@ -162,7 +164,8 @@ class BatchSolver:
         return self.results()
 
     def tune(self, use_cache=True) -> HbBatchConfig:
-        """Autotuner: times every (cluster, threads) shape, keeps the fastest, caches it."""
+        """Autotuner: times every (rows per thread, cluster, threads) shape, keeps the fastest,
+        caches it."""
         key = self.signature()
         path = _cache_path()
         cache = {}
@@ -173,15 +176,18 @@ class BatchSolver:
                 cache = {}
         if use_cache and key in cache:
             c = cache[key]
-            return HbBatchConfig(int(c["cluster"]), int(c["threads"]))
-        best = HbBatchConfig(4, 512)
-        times = (C.c_double * (len(CLUSTERS) * len(THREADS)))()
+            return HbBatchConfig(int(c["cluster"]), int(c["threads"]), 0, int(c.get("rows_per_thread", 4)))
+        best = HbBatchConfig(4, 512, 0, 4)
+        n = len(ROWS_PER_THREAD) * len(CLUSTERS) * len(THREADS)
+        times = (C.c_double * n)()
         check(self.L.hb_batch_tune(self.ctx.handle, self._arr, self.count, C.c_void_p(self._ws), C.byref(best), times),
               "hb_batch_tune", self.ctx.handle)
         self.prepared = True
-        self.tune_times = {f"c{c}_t{t}": round(times[i * len(THREADS) + j], 4)
-                           for i, c in enumerate(CLUSTERS) for j, t in enumerate(THREADS)}
-        cache[key] = {"cluster": best.cluster, "threads": best.threads, "times_ms": self.tune_times}
+        self.tune_times = {f"r{r}_c{c}_t{t}": round(times[(k * len(CLUSTERS) + i) * len(THREADS) + j], 4)
+                           for k, r in enumerate(ROWS_PER_THREAD) for i, c in enumerate(CLUSTERS)
+                           for j, t in enumerate(THREADS)}
+        cache[key] = {"cluster": best.cluster, "threads": best.threads, "rows_per_thread": best.rows_per_thread,
+                      "times_ms": self.tune_times}
         try:
             os.makedirs(os.path.dirname(path), exist_ok=True)
             json.dump(cache, open(path, "w"), indent=1)

@@ -166,6 +166,85 @@ __device__ void cluster_cg(const int32_t *__restrict__ Aj, const T *__restrict__
     d_out = current_defect;
 }
 
+// The same CG loop with one row per thread instead of a group of four: every slot's Aj / Ax load
+// of the row is in flight at once, then every gather, with fewer registers per thread (so more
+// threads per SM).  Same formulas, same per-row summation order; the dot products' partial sums
+// group the rows differently, so its iterates differ from the four-row layout's at round-off.
+template <typename T, int KT>
+__device__ void cluster_cg1(const int32_t *__restrict__ Aj, const T *__restrict__ Ax, int64_t ld, int K, Range rg,
+                            T *x, T *r, T *p0, T *p1, T *v, T alpha, T eps, int64_t max_iters, Smem &s, int &phase,
+                            int64_t &used_out, T &d0_out, T &d_out)
+{
+    using hbd::add; using hbd::mul;
+    constexpr int KS = KT > 0 ? KT : 4;
+    const T initial_defect = dsqrt(alpha);
+    T current_defect = T(0);
+    T beta = T(0);
+    const T epsm = eps_mach<T>();
+    T *pin = p0, *pout = p1;
+    int64_t it = 0, used = 0;
+    const int64_t lo = 4 * rg.lo, hi = 4 * rg.hi;
+    const int kend = KT > 0 ? KT : K;
+    while (it < max_iters) {
+        const bool first = (it == 0);
+        T acc = T(0);
+        for (int64_t row = lo + threadIdx.x; row < hi; row += blockDim.x) {
+            T sm = T(0);
+            for (int k0 = 0; k0 < kend; k0 += KS) {
+                int32_t j[KS];
+                T a[KS];
+#pragma unroll
+                for (int c = 0; c < KS; ++c) {
+                    const bool in = k0 + c < kend;
+                    j[c] = in ? __ldcs(Aj + (int64_t)(k0 + c) * ld + row) : -1;
+                    a[c] = in ? __ldcs(Ax + (int64_t)(k0 + c) * ld + row) : T(0);
+                }
+                T g[KS];
+#pragma unroll
+                for (int c = 0; c < KS; ++c) {
+                    if (j[c] >= 0) {
+                        const T rj = __ldcg(r + j[c]);
+                        g[c] = first ? rj : add(mul(__ldcg(pin + j[c]), beta), rj);
+                    } else {
+                        g[c] = T(0);
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < KS; ++c)
+                    if (j[c] >= 0) sm = add(sm, mul(a[c], g[c]));
+            }
+            const T rv = r[row];
+            const T pn = first ? rv : add(mul(pin[row], beta), rv);
+            acc = add(acc, mul(sm, pn));
+            pout[row] = pn;
+            v[row] = sm;
+        }
+        const T temp = cluster_total<T>(acc, s, phase);
+        const T lambda = alpha / (fabs(temp) > epsm ? temp : epsm);
+        const T mlambda = -lambda;
+        acc = T(0);
+        for (int64_t row = lo + threadIdx.x; row < hi; row += blockDim.x) {
+            const T xv = add(x[row], mul(lambda, pout[row]));
+            const T rv = add(r[row], mul(mlambda, v[row]));
+            acc = add(acc, mul(rv, rv));
+            x[row] = xv;
+            r[row] = rv;
+        }
+        const T alpha_old = alpha;
+        alpha = cluster_total<T>(acc, s, phase);
+        beta = alpha / (fabs(alpha_old) > epsm ? alpha_old : epsm);
+        T *t = pin; pin = pout; pout = t;
+        ++it;
+        current_defect = dsqrt(alpha);
+        if (current_defect < eps * initial_defect) { used = it; break; }
+        if (current_defect < eps) { used = it; break; }
+        if (it == max_iters) used = it;
+    }
+    used_out = used;
+    d0_out = initial_defect;
+    d_out = current_defect;
+}
+
 // rv = b - A x over the owned groups (FP64), returns the thread's partial r.r.
 template <int KT>
 __device__ double defect64(const BatchDesc &d, Range rg, const double *xw, double *rw)
@@ -187,7 +266,48 @@ __device__ double defect64(const BatchDesc &d, Range rg, const double *xw, doubl
     return acc;
 }
 
+// defect64 with one row per thread (the layout of cluster_cg1): rv = b - A x, the thread's r.r.
 template <int KT>
+__device__ double defect64_1(const BatchDesc &d, Range rg, const double *xw, double *rw)
+{
+    using hbd::add; using hbd::mul; using hbd::sub;
+    constexpr int KS = KT > 0 ? KT : 4;
+    const int kend = KT > 0 ? KT : d.K;
+    double acc = 0.0;
+    for (int64_t row = 4 * rg.lo + threadIdx.x; row < 4 * rg.hi; row += blockDim.x) {
+        double sm = 0.0;
+        for (int k0 = 0; k0 < kend; k0 += KS) {
+            int32_t j[KS];
+            double a[KS];
+#pragma unroll
+            for (int c = 0; c < KS; ++c) {
+                const bool in = k0 + c < kend;
+                j[c] = in ? __ldcs(d.Aj + (int64_t)(k0 + c) * d.ld + row) : -1;
+                a[c] = in ? __ldcs(d.Ax64 + (int64_t)(k0 + c) * d.ld + row) : 0.0;
+            }
+            double g[KS];
+#pragma unroll
+            for (int c = 0; c < KS; ++c) g[c] = j[c] >= 0 ? __ldcg(xw + j[c]) : 0.0;
+#pragma unroll
+            for (int c = 0; c < KS; ++c)
+                if (j[c] >= 0) sm = add(sm, mul(a[c], g[c]));
+        }
+        const double bb = row < d.n ? d.b[row] : 0.0;
+        const double rv = sub(bb, sm);
+        acc = add(acc, mul(rv, rv));
+        rw[row] = rv;
+    }
+    return acc;
+}
+
+template <int KT, int RPT>
+__device__ double defect_any(const BatchDesc &d, Range rg, const double *xw, double *rw)
+{
+    if (RPT == 1) return defect64_1<KT>(d, rg, xw, rw);
+    return defect64<KT>(d, rg, xw, rw);
+}
+
+template <int KT, int RPT>
 __device__ void solve_system(const BatchDesc &d, Smem &s, int &phase)
 {
     cgx::cluster_group cl = cgx::this_cluster();
@@ -215,11 +335,15 @@ __device__ void solve_system(const BatchDesc &d, Smem &s, int &phase)
     hb_batch_result res{};
     if (d.mode == HB_BATCH_CG64) {
         double *p0 = xw + 2 * ld, *p1 = xw + 3 * ld, *v = xw + 4 * ld;
-        const double alpha = cluster_total<double>(defect64<KT>(d, rg, xw, r64), s, phase);
+        const double alpha = cluster_total<double>(defect_any<KT, RPT>(d, rg, xw, r64), s, phase);
         int64_t used;
         double d0, d1;
-        cluster_cg<double, KT>(d.Aj, d.Ax64, ld, d.K, rg, xw, r64, p0, p1, v, alpha, d.eps, d.max_iters, s, phase,
-                               used, d0, d1);
+        if (RPT == 1)
+            cluster_cg1<double, KT>(d.Aj, d.Ax64, ld, d.K, rg, xw, r64, p0, p1, v, alpha, d.eps, d.max_iters, s, phase,
+                                    used, d0, d1);
+        else
+            cluster_cg<double, KT>(d.Aj, d.Ax64, ld, d.K, rg, xw, r64, p0, p1, v, alpha, d.eps, d.max_iters, s, phase,
+                                   used, d0, d1);
         res.iterations = used;
         res.defect0 = d0;
         res.defect = d1;
@@ -229,7 +353,7 @@ __device__ void solve_system(const BatchDesc &d, Smem &s, int &phase)
         double nrm0 = 0.0, nrm = 0.0;
         int64_t outer = 0, total = 0;
         while (true) {
-            nrm = dsqrt(cluster_total<double>(defect64<KT>(d, rg, xw, r64), s, phase));
+            nrm = dsqrt(cluster_total<double>(defect_any<KT, RPT>(d, rg, xw, r64), s, phase));
             if (outer == 0) nrm0 = nrm;
             else if (nrm < d.eps * nrm0) break;
             if (nrm == 0.0 || outer >= d.max_outer) break;
@@ -250,8 +374,12 @@ __device__ void solve_system(const BatchDesc &d, Smem &s, int &phase)
             const float alpha32 = cluster_total<float>(acc, s, phase);
             int64_t used;
             float d0, d1;
-            cluster_cg<float, KT>(d.Aj, d.Ax32, ld, d.K, rg, x32, r32, q0, q1, v32, alpha32, (float)d.inner_eps,
-                                  d.max_iters, s, phase, used, d0, d1);
+            if (RPT == 1)
+                cluster_cg1<float, KT>(d.Aj, d.Ax32, ld, d.K, rg, x32, r32, q0, q1, v32, alpha32, (float)d.inner_eps,
+                                       d.max_iters, s, phase, used, d0, d1);
+            else
+                cluster_cg<float, KT>(d.Aj, d.Ax32, ld, d.K, rg, x32, r32, q0, q1, v32, alpha32, (float)d.inner_eps,
+                                      d.max_iters, s, phase, used, d0, d1);
             total += used;
             for (int64_t g = rg.lo + threadIdx.x; g < rg.hi; g += blockDim.x) {
                 double xv[4];
@@ -272,7 +400,7 @@ __device__ void solve_system(const BatchDesc &d, Smem &s, int &phase)
     }
     // x back to the caller and the true FP64 relative residual
     cl.sync();
-    const double rr = cluster_total<double>(defect64<KT>(d, rg, xw, r64), s, phase);
+    const double rr = cluster_total<double>(defect_any<KT, RPT>(d, rg, xw, r64), s, phase);
     for (int64_t g = rg.lo + threadIdx.x; g < rg.hi; g += blockDim.x)
 #pragma unroll
         for (int i = 0; i < 4; ++i)
@@ -284,8 +412,8 @@ __device__ void solve_system(const BatchDesc &d, Smem &s, int &phase)
     }
 }
 
-template <int THREADS>
-__global__ void __launch_bounds__(THREADS) batch_kernel(const BatchDesc *__restrict__ descs, int64_t count,
+template <int THREADS, int RPT>
+__global__ void __launch_bounds__(THREADS, RPT == 1 && THREADS == 256 ? 3 : 0) batch_kernel(const BatchDesc *__restrict__ descs, int64_t count,
                                                         unsigned long long *counter)
 {
     __shared__ Smem s;
@@ -298,8 +426,8 @@ __global__ void __launch_bounds__(THREADS) batch_kernel(const BatchDesc *__restr
         cl.sync();
         if (item >= count) break;
         const BatchDesc d = descs[item];
-        if (d.K == 9) solve_system<9>(d, s, phase);
-        else solve_system<0>(d, s, phase);
+        if (d.K == 9) solve_system<9, RPT>(d, s, phase);
+        else solve_system<0, RPT>(d, s, phase);
     }
 }
 
@@ -330,9 +458,9 @@ int check_system(const hb_batch_system &s)
     return HB_OK;
 }
 
-template <int THREADS> int launch_batch(hb_context *ctx, int cluster, int max_clusters, int64_t count, void *ws)
+template <int THREADS, int RPT> int launch_batch(hb_context *ctx, int cluster, int max_clusters, int64_t count, void *ws)
 {
-    auto kern = batch_kernel<THREADS>;
+    auto kern = batch_kernel<THREADS, RPT>;
     if (cluster > 8) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (e != cudaSuccess) { hb_note_error(ctx, e, "cudaFuncSetAttribute(non-portable cluster)"); return HB_ERR_CUDA; }
@@ -437,10 +565,14 @@ int hb_batch_run(hb_context *ctx, int64_t count, void *ws, const hb_batch_config
     const int cluster = cfg ? cfg->cluster : 4;
     const int threads = cfg ? cfg->threads : 512;
     const int max_clusters = cfg ? cfg->max_clusters : 0;
+    const int rpt = cfg && cfg->rows_per_thread ? cfg->rows_per_thread : 4;
     if (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8 && cluster != 16) return HB_ERR_INVALID;
+    if (rpt != 1 && rpt != 4) return HB_ERR_INVALID;
     HB_CUDA_TRY(ctx, cudaMemsetAsync(ws, 0, 256, ctx->stream));
-    if (threads == 256) return launch_batch<256>(ctx, cluster, max_clusters, count, ws);
-    if (threads == 512) return launch_batch<512>(ctx, cluster, max_clusters, count, ws);
+    if (threads == 256) return rpt == 1 ? launch_batch<256, 1>(ctx, cluster, max_clusters, count, ws)
+                                        : launch_batch<256, 4>(ctx, cluster, max_clusters, count, ws);
+    if (threads == 512) return rpt == 1 ? launch_batch<512, 1>(ctx, cluster, max_clusters, count, ws)
+                                        : launch_batch<512, 4>(ctx, cluster, max_clusters, count, ws);
     return HB_ERR_INVALID;
 }
 
@@ -475,14 +607,16 @@ int hb_batch_tune(hb_context *ctx, const hb_batch_system *sys, int64_t count, vo
     if (st) return st;
     const int clusters[5] = {1, 2, 4, 8, 16};
     const int threads[2] = {256, 512};
+    const int rows[2] = {4, 1};
     cudaEvent_t e0, e1;
     HB_CUDA_TRY(ctx, cudaEventCreate(&e0));
     HB_CUDA_TRY(ctx, cudaEventCreate(&e1));
     double best_ms = 1e300;
     int k = 0;
+    for (int rpt : rows)
     for (int c : clusters)
         for (int t : threads) {
-            hb_batch_config cfg{c, t, 0};
+            hb_batch_config cfg{c, t, 0, rpt};
             float ms = -1.f;
             // warm-up then one timed run, every run from x = 0
             st = zero_x(ctx, sys, count);

@@ -496,8 +496,8 @@ int hb_server_create(const hb_server_params *params, hb_server **out)
     if (s->p.large_workers < 1) s->p.large_workers = 1;
     if (s->p.small_workers < 1) s->p.small_workers = 1;
     if (s->p.max_batch < 1) s->p.max_batch = 256;
-    if (s->p.batch_cfg.cluster == 0) s->p.batch_cfg = hb_batch_config{2, 512, 0};
-    if (s->p.mid_cfg.cluster == 0) s->p.mid_cfg = hb_batch_config{16, 512, 0};
+    if (s->p.batch_cfg.cluster == 0) s->p.batch_cfg = hb_batch_config{2, 512, 0, 0};
+    if (s->p.mid_cfg.cluster == 0) s->p.mid_cfg = hb_batch_config{16, 512, 0, 0};
     s->t0 = std::chrono::steady_clock::now();
     s->admitter = std::thread(admit_loop, s);
     // the pool's high-water marks from here on (hb_server_pool_stats)

@@ -509,6 +509,8 @@ typedef struct {
     int32_t threads;           /* threads per CTA: 256 or 512                              */
     int32_t max_clusters;      /* cap on resident clusters (0 = all that fit): leaves SMs
                                   to concurrent work on other streams                      */
+    int32_t rows_per_thread;   /* CG rows per thread: 4 (a group of four rows, 16-byte
+                                  loads; 0 means 4) or 1 (one row, every slot in flight)   */
 } hb_batch_config;
 
 /* Device workspace bytes for these systems (work vectors, descriptors, results, counter). */
@@ -525,10 +527,11 @@ int hb_batch_solve(hb_context *ctx, const hb_batch_system *sys, int64_t count, v
 int hb_batch_prepare(hb_context *ctx, const hb_batch_system *sys, int64_t count, void *workspace);
 int hb_batch_run(hb_context *ctx, int64_t count, void *workspace, const hb_batch_config *cfg);
 int hb_batch_results(hb_context *ctx, int64_t count, void *workspace, hb_batch_result *results_host);
-/* Autotuner core: times every (cluster, threads) candidate on this batch (each run once after a
- * warm-up) and returns the fastest in *best; times_ms (may be NULL) receives one time per
- * candidate in the order cluster {1,2,4,8,16} x threads {256,512} (-1 = shape not launchable).
- * Every run starts from x = 0 (the systems' x are zeroed and overwritten). */
+/* Autotuner core: times every (rows per thread, cluster, threads) candidate on this batch (each
+ * run once after a warm-up) and returns the fastest in *best; times_ms (may be NULL, else 20
+ * entries) receives one time per candidate in the order rows per thread {4,1} x cluster
+ * {1,2,4,8,16} x threads {256,512} (-1 = shape not launchable).  Every run starts from x = 0 (the
+ * systems' x are zeroed and overwritten). */
 int hb_batch_tune(hb_context *ctx, const hb_batch_system *sys, int64_t count, void *workspace,
                   hb_batch_config *best, double *times_ms);
 

@@ -25,9 +25,10 @@ def host(t):
 SIDES = [5, 9, 17, 33, 65, 129, 3, 21, 47]
 
 
-def test_batch_cg64_parity_with_oracle(B, oracle):
+@pytest.mark.parametrize("rows", [4, 1])
+def test_batch_cg64_parity_with_oracle(B, oracle, rows):
     systems = B.q1_batch(SIDES, coef_range=(1e-1, 1e1), seed=3, mode="cg64", eps=1e-8)
-    res = B.BatchSolver(systems).solve(B.HbBatchConfig(4, 256))
+    res = B.BatchSolver(systems).solve(B.HbBatchConfig(4, 256, 0, rows))
     for s, r, M in zip(systems, res, SIDES):
         A = P.q1_poisson(M, P.log_uniform_coef(M, 1e-1, 1e1, s_seed(systems, s)), symmetric=True)
         b = host(s.b)
@@ -65,9 +66,10 @@ def test_batch_ir32_reaches_fp64_target(B, oracle):
         assert abs(r["outer"] - u_o) <= 1, (M, r["outer"], u_o)
 
 
-@pytest.mark.parametrize("cluster,threads", [(1, 256), (2, 512), (4, 256), (8, 512), (16, 256)])
-def test_batch_alone_equals_in_the_mix(B, cluster, threads):
-    cfg = B.HbBatchConfig(cluster, threads)
+@pytest.mark.parametrize("cluster,threads,rows", [(1, 256, 4), (2, 512, 4), (4, 256, 4), (8, 512, 4), (16, 256, 4),
+                                                  (1, 512, 1), (2, 256, 1), (8, 256, 1)])
+def test_batch_alone_equals_in_the_mix(B, cluster, threads, rows):
+    cfg = B.HbBatchConfig(cluster, threads, 0, rows)
     mix = B.q1_batch(SIDES, coef_range=(1e-1, 1e1), seed=5, mode="ir32")
     mix[1].mode = B.HB_BATCH_CG64
     res_mix = B.BatchSolver(mix).solve(cfg)
@@ -85,13 +87,14 @@ def test_batch_tuner_and_every_shape_solves(B, tmp_path, monkeypatch):
     systems = B.q1_batch([17, 33, 65, 9, 129, 33, 17, 65], coef_range=(1e-1, 1e1), seed=1, mode="ir32")
     solver = B.BatchSolver(systems)
     cfg = solver.tune()
-    assert cfg.cluster in B.CLUSTERS and cfg.threads in B.THREADS
+    assert cfg.cluster in B.CLUSTERS and cfg.threads in B.THREADS and cfg.rows_per_thread in B.ROWS_PER_THREAD
+    assert len(solver.tune_times) == 20
     assert (tmp_path / "tune.json").exists()
     assert all(v > 0 for v in solver.tune_times.values())
     res = solver.solve(cfg)
     assert all(r["true_relres"] < 1e-8 for r in res)
     cfg2 = B.BatchSolver(systems).tune()            # cache hit
-    assert (cfg2.cluster, cfg2.threads) == (cfg.cluster, cfg.threads)
+    assert (cfg2.cluster, cfg2.threads, cfg2.rows_per_thread) == (cfg.cluster, cfg.threads, cfg.rows_per_thread)
 
 
 def test_batch_empty_and_single_row(B):
