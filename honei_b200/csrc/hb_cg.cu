@@ -200,6 +200,132 @@ __global__ void __launch_bounds__(CG_THREADS) cg_kernel(CGParams<T> P)
 }
 
 // ---------------------------------------------------------------------------------------
+// The same persistent CG with one row per thread: each block owns the same contiguous rows as
+// in cg_kernel (whole groups of four), its threads walk them one row at a time with every
+// slot's Aj / Ax load of the row in flight together, then every gather.  Fewer registers per
+// thread than the four-row groups, so three 256-thread blocks share an SM (24 warps against 16)
+// and more loads are in flight per SM.  Same formulas, same per-row summation order and the
+// same exchanges; the dot products' partial sums group the rows differently, so its iterates
+// differ from cg_kernel's at round-off (same bar against the reference).
+// ---------------------------------------------------------------------------------------
+constexpr int CG_ROW_THREADS = 256;
+
+template <typename T, int KT>
+__global__ void __launch_bounds__(CG_ROW_THREADS, 3) cg_row_kernel(CGParams<T> P)
+{
+    using hbd::add; using hbd::mul; using hbd::sub;
+    constexpr int KS = KT > 0 ? KT : 4;
+    __shared__ T red[32];
+    __shared__ T bcast;
+    __shared__ int s_flag;
+    const unsigned G = gridDim.x;
+    const int64_t groups = P.ld / 4;
+    const int64_t gpb = (groups + G - 1) / G;
+    const int64_t lo = 4 * min(groups, (int64_t)blockIdx.x * gpb);
+    const int64_t hi = 4 * min(groups, (int64_t)blockIdx.x * gpb + gpb);
+    const int kend = KT > 0 ? KT : P.K;
+    const hbd::CountExchange X{P.bar.count, P.bar.status};
+    unsigned e = 0;
+    const int64_t rows = P.rows;
+    bool ok = true;
+
+    // the row's sum over its slots in slot order, gathering g(j) for column j
+    auto row_sum = [&](int64_t row, auto g) {
+        T sm = T(0);
+        for (int k0 = 0; k0 < kend; k0 += KS) {
+            int32_t j[KS];
+            T a[KS];
+#pragma unroll
+            for (int c = 0; c < KS; ++c) {
+                const bool in = k0 + c < kend;
+                j[c] = in ? __ldcs(P.Aj + (int64_t)(k0 + c) * P.ld + row) : -1;
+                a[c] = in ? __ldcs(P.Ax + (int64_t)(k0 + c) * P.ld + row) : T(0);
+            }
+            T v[KS];
+#pragma unroll
+            for (int c = 0; c < KS; ++c) v[c] = j[c] >= 0 ? g(j[c]) : T(0);
+#pragma unroll
+            for (int c = 0; c < KS; ++c)
+                if (j[c] >= 0) sm = add(sm, mul(a[c], v[c]));
+        }
+        return sm;
+    };
+
+    for (int64_t row = lo + threadIdx.x; row < hi; row += blockDim.x)
+        P.x[row] = row < rows ? P.x_user[row] : T(0);
+    ok = X.arrive_wait(T(0), P.partials, e, G, &s_flag);
+
+    T acc = T(0);
+    if (ok) {
+        const T *xw = P.x;
+        for (int64_t row = lo + threadIdx.x; row < hi; row += blockDim.x) {
+            const T s = row_sum(row, [&](int32_t j) { return xw[j]; });
+            const T bb = row < rows ? P.b_user[row] : T(0);
+            const T rv = sub(bb, s);
+            acc = add(acc, mul(rv, rv));
+            P.r[row] = rv;
+        }
+        acc = hbd::block_sum(acc, red);
+        ok = X.arrive_wait(acc, P.partials, ++e, G, &s_flag);
+    }
+    T alpha = ok ? grid_total(P.partials + (e & 1u) * G, red, &bcast) : T(0);
+    const T initial_defect = dsqrt(alpha);
+    T current_defect = T(0);
+    T beta = T(0);
+    const T epsm = eps_mach<T>();
+    T *pin = P.p0, *pout = P.p1;
+    int64_t it = 0, used = 0;
+    while (ok && it < P.max_iters) {
+        const T *rw = P.r, *pw = pin;
+        const bool first = (it == 0);
+        acc = T(0);
+        for (int64_t row = lo + threadIdx.x; row < hi; row += blockDim.x) {
+            const T s = row_sum(row, [&](int32_t j) {
+                const T rj = rw[j];
+                return first ? rj : add(mul(pw[j], beta), rj);
+            });
+            const T rv = P.r[row];
+            const T pn = first ? rv : add(mul(pin[row], beta), rv);
+            acc = add(acc, mul(s, pn));
+            pout[row] = pn;
+            P.v[row] = s;
+        }
+        acc = hbd::block_sum(acc, red);
+        if (!X.arrive_wait(acc, P.partials, ++e, G, &s_flag)) break;
+        const T temp = grid_total(P.partials + (e & 1u) * G, red, &bcast);
+        const T lambda = alpha / (fabs(temp) > epsm ? temp : epsm);
+        const T mlambda = -lambda;
+        acc = T(0);
+        for (int64_t row = lo + threadIdx.x; row < hi; row += blockDim.x) {
+            const T xv = add(P.x[row], mul(lambda, pout[row]));
+            const T rv = add(P.r[row], mul(mlambda, P.v[row]));
+            acc = add(acc, mul(rv, rv));
+            P.x[row] = xv;
+            P.r[row] = rv;
+        }
+        acc = hbd::block_sum(acc, red);
+        if (!X.arrive_wait(acc, P.partials, ++e, G, &s_flag)) break;
+        const T alpha_old = alpha;
+        alpha = grid_total(P.partials + (e & 1u) * G, red, &bcast);
+        beta = alpha / (fabs(alpha_old) > epsm ? alpha_old : epsm);
+        T *t = pin; pin = pout; pout = t;
+        ++it;
+        current_defect = dsqrt(alpha);
+        if (current_defect < P.eps * initial_defect) { used = it; break; }
+        if (current_defect < P.eps) { used = it; break; }
+        if (it == P.max_iters) used = it;
+    }
+    for (int64_t row = lo + threadIdx.x; row < hi; row += blockDim.x)
+        if (row < rows) P.x_user[row] = P.x[row];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        P.res->used = used;
+        P.res->defect0 = (double)initial_defect;
+        P.res->defect = (double)current_defect;
+        P.res->status = *(volatile int *)P.bar.status;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // Small systems (at most SMALL_GROUPS row groups, e.g. the coarsest MG level): the same
 // iteration in one block, thread t owning row group t, p exchanged through shared memory and
 // the matrix slots held in registers, so an iteration is two block reductions and no global
@@ -546,6 +672,26 @@ int cg_max_blocks(hb_context *ctx)
     return std::max(1, occ) * ctx->num_sms;
 }
 
+// The one-row-per-thread kernel: every co-resident block (for systems large enough to fill
+// them), else about one row per thread.
+template <typename T, int KT>
+int launch_cg_row(hb_context *ctx, CGParams<T> &P)
+{
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, cg_row_kernel<T, KT>, CG_ROW_THREADS, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return HB_ERR_CUDA;
+    }
+    const int64_t maxb = (int64_t)std::max(1, occ) * ctx->num_sms;
+    const int64_t want = (P.ld + CG_ROW_THREADS - 1) / CG_ROW_THREADS;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(maxb, 4096)));
+    void *args[] = {&P};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *)cg_row_kernel<T, KT>, dim3(blocks),
+                                                dim3(CG_ROW_THREADS), args, 0, ctx->stream);
+    if (e != cudaSuccess) { hb_note_error(ctx, e, "cudaLaunchCooperativeKernel(cg_row_kernel)"); return HB_ERR_CUDA; }
+    return hb_check_launch(ctx, "cg_row_kernel");
+}
+
 }  // namespace
 
 template <typename T>
@@ -584,6 +730,7 @@ int hb_launch_cg(hb_context *ctx, const hb_ell *A, const T *b, T *x, int64_t max
         const int st = k9 ? launch_cg_res<T, 9>(ctx, P, &launched) : launch_cg_res<T, 0>(ctx, P, &launched);
         if (st || launched) return st;
     }
+    if (ctx->cg_row_layout) return k9 ? launch_cg_row<T, 9>(ctx, P) : launch_cg_row<T, 0>(ctx, P);
     return k9 ? launch_cg_kt<T, 9>(ctx, P, blocks) : launch_cg_kt<T, 0>(ctx, P, blocks);
 }
 template int hb_launch_cg<double>(hb_context *, const hb_ell *, const double *, double *, int64_t, double,

@@ -147,6 +147,14 @@ int hb_cg_set_resident(hb_context *ctx, int enable)
     return prev;
 }
 
+int hb_cg_set_layout(hb_context *ctx, int rows_per_thread)
+{
+    if (!ctx || (rows_per_thread != 1 && rows_per_thread != 4)) return -1;
+    const int prev = ctx->cg_row_layout ? 1 : 4;
+    ctx->cg_row_layout = rows_per_thread == 1;
+    return prev;
+}
+
 int hb_reserve(hb_context *ctx, int64_t n)
 {
     if (!ctx || n < 0) return HB_ERR_INVALID;

@@ -48,6 +48,8 @@ struct hb_context {
     uint64_t launches = 0;
     // CG on systems that fit: the resident-operator kernel (hb_cg_set_resident)
     int cg_resident = 1;
+    // streaming CG: one row per thread (cg_row_kernel) or groups of four rows (hb_cg_set_layout)
+    int cg_row_layout = 0;
     std::string last_error;
 };
 

@@ -684,6 +684,16 @@ class CGSolver:
         ctx = ctx or default_context()
         return bool(lib().hb_cg_set_resident(ctx.handle, 1 if enable else 0))
 
+    @staticmethod
+    def set_layout(rows_per_thread: int, ctx: Context | None = None) -> int:
+        """The streaming CG kernel's layout on ctx: 4 rows per thread (groups of four) or 1 (one
+        row per thread); returns the previous setting."""
+        ctx = ctx or default_context()
+        prev = lib().hb_cg_set_layout(ctx.handle, int(rows_per_thread))
+        if prev < 0:
+            raise ValueError("rows_per_thread must be 1 or 4")
+        return prev
+
 
 class CGSolverVAR:
     """CGSolver<tags::GPU::CUDA, methods::VAR>::value (honei/math/cg.hh:140-219): CG with the

@@ -361,6 +361,12 @@ int hb_cg_f32(hb_context *ctx, const hb_ell *A, const float *b, float *x, int64_
  * results within rounding of each other (their dot products use different summation trees);
  * each is deterministic.  Returns the previous setting. */
 int hb_cg_set_resident(hb_context *ctx, int enable);
+/* Selects the streaming CG kernel's layout on this context: rows_per_thread 4 (groups of four
+ * rows per thread, 16-byte loads; the default) or 1 (one row per thread, every slot of the row in
+ * flight, more threads per SM).  Same formulas and per-row sums; the dot products' partial sums
+ * group the rows differently, so the iterates agree to rounding.  Returns the previous setting,
+ * or -1 for an invalid argument. */
+int hb_cg_set_layout(hb_context *ctx, int rows_per_thread);
 
 /* Preconditioned CG, CGSolver<Tag, methods::VAR>::value(A, P, b, x, max_iters, used_iters,
  * eps), honei/math/cg.hh:140-219, with the preconditioner container P either a vector (the

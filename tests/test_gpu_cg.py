@@ -273,3 +273,31 @@ def test_cg_concurrent_solves_on_separate_contexts(hb):
     for k in range(len(sizes)):
         for used, x in results[k]:
             assert used == alone[k][0] and np.array_equal(x, alone[k][1]), k
+
+
+@pytest.mark.parametrize("name,make", RESIDENT_CASES[:2] + [("q1_513", lambda: P.q1_poisson(513))],
+                         ids=[c[0] for c in RESIDENT_CASES[:2]] + ["q1_513"])
+def test_cg_row_layout_matches_group_layout(hb, oracle, name, make):
+    """The streaming kernel with one row per thread solves the same systems to the CG bar
+    (iterations within 1 of the four-row layout's and of the oracle's, true residual within
+    1e-10), deterministically."""
+    A = make()
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 1))
+    prev_res = hb.CGSolver.set_resident(False)
+    try:
+        prev = hb.CGSolver.set_layout(4)
+        x4, u4 = run_cg(hb, A, b, 1e-8)
+        hb.CGSolver.set_layout(1)
+        x1, u1 = run_cg(hb, A, b, 1e-8)
+        x1b, u1b = run_cg(hb, A, b, 1e-8)
+        hb.CGSolver.set_layout(prev)
+    finally:
+        hb.CGSolver.set_resident(prev_res)
+    assert u1 == u1b and np.array_equal(x1, x1b)
+    assert abs(u1 - u4) <= 1, (u1, u4)
+    assert abs(relres(oracle, A, b, x1) - relres(oracle, A, b, x4)) <= 1e-10
+    if A.rows <= 129 * 129:
+        x_o, u_o = oracle.cg(A, b, eps=1e-8, max_iters=20000)
+        assert abs(u1 - u_o) <= 1 and abs(relres(oracle, A, b, x1) - relres(oracle, A, b, x_o)) <= 1e-10
+    with pytest.raises(ValueError):
+        hb.CGSolver.set_layout(3)

@@ -156,9 +156,10 @@ def _batch_sides(n=512, seed=BATCH_SEED):
     return np.random.default_rng(seed).integers(17, 258, size=n)
 
 
-def test_batch_512_cg64_within_the_references_own_spread(hb, oracle):
-    """The 512-system batch of the benchmark, FP64 CG, solved in one launch at the tuned shape
-    (2-CTA clusters of 512 threads), against the reference's CGSolver<tags::CPU> on every
+@pytest.mark.parametrize("shape", [(2, 512, 4), (4, 256, 1), (8, 256, 1)], ids=lambda t: "c%d_t%d_r%d" % t)
+def test_batch_512_cg64_within_the_references_own_spread(hb, oracle, shape):
+    """The 512-system batch of the benchmark, FP64 CG, solved in one launch at the shapes the
+    tuner picks (4-CTA clusters of 256 threads, one row per thread) and two others, against the reference's CGSolver<tags::CPU> on every
     system (tests/golden/batch512.npz, written by the compiled reference).
 
     On these systems (contrast 10^2, up to 872 iterations) the iteration count at which the
@@ -178,7 +179,7 @@ def test_batch_512_cg64_within_the_references_own_spread(hb, oracle):
     sides = _batch_sides()
     assert np.array_equal(sides, g["sides"])
     systems = B.q1_batch(sides, coef_range=(1e-1, 1e1), seed=BATCH_SEED, mode="cg64", eps=1e-8)
-    res = B.BatchSolver(systems).solve(B.HbBatchConfig(2, 512))
+    res = B.BatchSolver(systems).solve(B.HbBatchConfig(shape[0], shape[1], 0, shape[2]))
     tags = [t for t in ("sse", "mc4", "mc16") if f"{t}_used" in g]
     d_ref = {t: np.abs(g[f"{t}_used"] - g["cpu_used"]) for t in tags}
     r_ref = {t: np.abs(g[f"{t}_relres"] - g["cpu_relres"]) for t in tags}
@@ -192,7 +193,7 @@ def test_batch_512_cg64_within_the_references_own_spread(hb, oracle):
     dr = np.abs(r_g - g["cpu_relres"])
     ref_txt = "; ".join(f"{t}: {int(np.sum(d == 0))} equal, max {int(d.max())}, mean {d.mean():.2f}"
                         for t, d in d_ref.items())
-    print(f"batch 512 cg64: |GPU - tags::CPU| iterations: {int(np.sum(du == 0))} equal, {int(np.sum(du == 1))} "
+    print(f"batch 512 cg64 {shape}: |GPU - tags::CPU| iterations: {int(np.sum(du == 0))} equal, {int(np.sum(du == 1))} "
           f"one apart, max {int(du.max())}, mean {du.mean():.2f}; reference tags: {ref_txt}; residual gap max "
           f"{dr.max():.3e} (reference tags {Rr:.3e})")
     assert np.all(st == 0)
@@ -208,12 +209,12 @@ def test_batch_512_cg64_within_the_references_own_spread(hb, oracle):
 
 def test_batch_512_ir32_every_system_matches_oracle(hb, oracle):
     """The same batch in mixed precision (FP64 refinement around FP32 CG to 1e-3 per step, to a
-    1e-8 FP64 residual): every system's outer step count against the oracle's scaled
+    1e-8 FP64 residual), at the tuned shape (4-CTA clusters of 256 threads, one row per thread): every system's outer step count against the oracle's scaled
     refinement around FP32 CG on the same matrix and right-hand side."""
     from honei_b200 import batch as B
     sides = _batch_sides()
     systems = B.q1_batch(sides, coef_range=(1e-1, 1e1), seed=BATCH_SEED, mode="ir32", eps=1e-8, inner_eps=1e-3)
-    res = B.BatchSolver(systems).solve(B.HbBatchConfig(2, 512))
+    res = B.BatchSolver(systems).solve(B.HbBatchConfig(4, 256, 0, 1))
     mats = [s.A64.to_host() for s in systems]
     bs = [host(s.b) for s in systems]
     xs = [host(s.x) for s in systems]
