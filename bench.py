@@ -270,8 +270,9 @@ def bench_spmv_variants(la, ctx, M=M_SPMV, seed=5, cpu=True, reps=50):
     """The other SpMV lines of the SpMV configuration: the FP32 product of the 2049^2 matrix; the
     randomly permuted 2049^2 matrix (seeded symmetric row/column permutation) in FP64 and FP32,
     as given and through its Cuthill-McKee ordered copy (SparseMatrixELL.ordered: rows stored
-    in the locality order, columns renumbered, x permuted into a work vector inside the timed
-    product, y scattered back -- bit-identical to the product on the permuted matrix); the
+    in the locality order, columns renumbered and packed as 16-bit offsets, x permuted into a
+    work vector inside the timed product, y scattered back -- bit-identical to the product on
+    the permuted matrix; the unpacked ranked form beside it); the
     1025^2 FP64 product with L2 flushed between products (its 130 MB would otherwise stay
     partly in L2).  GB/s are the algorithmic bytes of the product on the given matrix
     (nnz*(s+4) + 2*n*s)."""
@@ -312,8 +313,21 @@ def bench_spmv_variants(la, ctx, M=M_SPMV, seed=5, cpu=True, reps=50):
         r["same_y_as_permuted"] = bool(torch.equal(y, y0))
         r["ordering_ms"] = round(t_order * 1e3, 1)
         r["levels"], r["bandwidth_before"], r["bandwidth_after"] = int(B.info[0]), Ad.bandwidth(), B.B.bandwidth()
+        r["form"] = "packed (16-bit column offsets, 32-bit ranks)" if B.Bd is not None else "ranked"
+        # the bytes this form moves: x gathered (order, x, xw) and the product's own arrays
+        # (every slot of the K x ld value and offset arrays, rank words, order, xw, y)
+        idx = 2 if B.Bd is not None else 4
+        rk = 4 if B.Bd is not None else 8
+        own = (4 + 2 * s) * n + B.B.K * B.B.ld * (s + idx) + (rk + 4 + 2 * s) * n
+        r["own_bytes"] = own
+        r["own_gbs"] = round(own / (r["us"] * 1e3), 1)
+        y.fill_(0)
+        R = Ad.ordered(columns=True, packed=False, ctx=ctx)
+        r2 = line(_time_us(lambda: la.Product.value(y, R, x, ctx=ctx), reps), s)
+        r2["same_y_as_permuted"] = bool(torch.equal(y, y0))
+        r["ranked_form"] = r2
         out[f"permuted_ordered_{name}"] = r
-        del Ad, B, x, y, y0
+        del Ad, B, R, x, y, y0
         torch.cuda.empty_cache()
     if cpu:
         h = None

@@ -24,6 +24,8 @@ import torch
 from . import _lib
 from ._lib import HbCsr, HbEll, check, lib
 
+HB_ERR_UNSUPPORTED = 6                 # hb_status: shape outside what a kernel supports
+
 
 class VectorSizeDoesNotMatch(ValueError):
     """honei/la/vector_error.hh: VectorSizeDoesNotMatch(size, expected)."""
@@ -264,13 +266,15 @@ class SparseMatrixELL:
                                      C.byref(bw)), "hb_ell_bandwidth", ctx.handle)
         return bw.value
 
-    def ordered(self, columns: bool = True, ctx: Context | None = None) -> "OrderedMatrixELL":
+    def ordered(self, columns: bool = True, packed: bool = True, ctx: Context | None = None) -> "OrderedMatrixELL":
         """A copy stored in the Cuthill-McKee locality order, for products with a badly numbered
         matrix (e.g. a randomly permuted grid).  Product.value on the copy gives y = A x bit for
         bit.  columns=True renumbers the columns too and stores each row's slots by new column
         with their summation ranks (local gathers; x is permuted into a work vector first);
-        columns=False keeps A's columns (no work vector; gathers stay scattered, rows that share
-        columns run together)."""
+        packed=True then also keeps the columns as 16-bit offsets from the row and the ranks in
+        32 bits when K <= 9 and the reordered bandwidth allows (hb_ell_pack_ordered), and the
+        product reads those.  columns=False keeps A's columns (no work vector; gathers stay
+        scattered, rows that share columns run together)."""
         ctx = ctx or default_context()
         order, pos, info = self.cm_order(ctx)
         Aj = torch.empty_like(self.Aj)
@@ -284,8 +288,18 @@ class SparseMatrixELL:
         else:
             check(lib().hb_ell_permute(ctx.handle, C.byref(self._s), order.data_ptr(), None, C.byref(B)),
                   "hb_ell_permute", ctx.handle)
-        return OrderedMatrixELL(SparseMatrixELL(self._rows, self._cols, self.K, self.ld, Aj, Ax), order, pos,
-                                columns, info, ranks)
+        O = OrderedMatrixELL(SparseMatrixELL(self._rows, self._cols, self.K, self.ld, Aj, Ax), order, pos,
+                             columns, info, ranks)
+        if columns and packed and self.K <= 9 and self._rows > 0:
+            Bd = torch.empty((self.K, self.ld), dtype=torch.int16, device=self.Aj.device)
+            r32 = torch.empty(self._rows, dtype=torch.int32, device=self.Aj.device)
+            st = lib().hb_ell_pack_ordered(ctx.handle, C.byref(O.B.struct), ranks.data_ptr(), Bd.data_ptr(),
+                                           r32.data_ptr())
+            if st == 0:
+                O.Bd, O.ranks32 = Bd, r32
+            elif st != HB_ERR_UNSUPPORTED:
+                check(st, "hb_ell_pack_ordered", ctx.handle)
+        return O
 
 
 class OrderedMatrixELL:
@@ -298,6 +312,7 @@ class OrderedMatrixELL:
         self.B, self.order, self.pos, self.columns_renumbered = B, order, pos, columns
         self.info = info
         self.ranks = ranks
+        self.Bd = self.ranks32 = None                   # the packed form, when it was made
         self.dtype = B.dtype
         self._xw = None
 
@@ -316,9 +331,14 @@ class OrderedMatrixELL:
             check(getattr(lib(), f"hb_gather_{suf}")(ctx.handle, self.B.rows(), self.order.data_ptr(), xp,
                                                      self._xw.data_ptr()), "hb_gather", ctx.handle)
             xp = self._xw.data_ptr()
-            check(getattr(lib(), f"hb_spmv_ranked_{suf}")(ctx.handle, C.byref(self.B.struct), self.order.data_ptr(),
-                                                          self.ranks.data_ptr(), xp, _vec(y, self.dtype, "y")),
-                  "Product", ctx.handle)
+            if self.Bd is not None:
+                check(getattr(lib(), f"hb_spmv_packed_{suf}")(ctx.handle, C.byref(self.B.struct), self.Bd.data_ptr(),
+                                                              self.order.data_ptr(), self.ranks32.data_ptr(), xp,
+                                                              _vec(y, self.dtype, "y")), "Product", ctx.handle)
+            else:
+                check(getattr(lib(), f"hb_spmv_ranked_{suf}")(ctx.handle, C.byref(self.B.struct),
+                                                              self.order.data_ptr(), self.ranks.data_ptr(), xp,
+                                                              _vec(y, self.dtype, "y")), "Product", ctx.handle)
             return y
         check(getattr(lib(), f"hb_spmv_rows_{suf}")(ctx.handle, C.byref(self.B.struct), self.order.data_ptr(), xp,
                                                     _vec(y, self.dtype, "y")), "Product", ctx.handle)

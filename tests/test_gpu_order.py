@@ -1,5 +1,6 @@
 """Locality order (hb_ell_cm_order) and the product through a reordered copy (hb_ell_permute,
-hb_spmv_rows, hb_gather).
+hb_spmv_rows, hb_gather; the sorted copy with hb_spmv_ranked; its packed form with
+hb_spmv_packed).
 
 The order has no reference counterpart; the product through the reordered copy must equal the
 product on the matrix as given (Product<tags::CPU>, honei/la/product.hh:148-204) bit for bit,
@@ -85,17 +86,45 @@ def test_cm_order_matches_sequential_definition(hb, name, make):
     assert torch.equal(order, order2) and info == info2
 
 
+FORMS = ["rows", "ranked", "packed"]
+
+
+def ordered_form(Ad, form):
+    """The ordered copy in one of its forms: rows (A's columns), ranked (renumbered, sorted,
+    64-bit ranks) and packed (16-bit offsets, 32-bit ranks)."""
+    B = Ad.ordered(columns=form != "rows", packed=form == "packed")
+    if form == "packed":
+        assert B.Bd is not None and B.Bd.dtype == torch.int16 and B.ranks32.dtype == torch.int32
+    else:
+        assert B.Bd is None
+    return B
+
+
 @pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
-@pytest.mark.parametrize("columns", [True, False])
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("dt", [np.float64, np.float32])
-def test_product_through_ordered_copy_bit_exact(hb, oracle, name, make, columns, dt):
+def test_product_through_ordered_copy_bit_exact(hb, oracle, name, make, form, dt):
     A = make().astype(dt)
     Ad = hb.SparseMatrixELL.from_reference(A)
-    Bd = Ad.ordered(columns=columns)
+    Bd = ordered_form(Ad, form)
     x = P.uniform_vector(A.cols, 5).astype(dt)
     y = torch.full((A.rows,), float("nan"), dtype=Ad.dtype, device="cuda")
     hb.Product.value(y, Bd, torch.from_numpy(x).cuda())
     assert np.array_equal(y.cpu().numpy(), oracle.spmv(A, x))
+
+
+def test_packed_form_declined_falls_back_to_ranks(hb, oracle):
+    """The packed form needs K <= 9 and every reordered column within +-32767 of its row: a
+    random pattern over 120,000 rows (offsets up to n after ordering) and one with 12 entries per
+    row are left in the 64-bit ranked form, and their products stay bit-exact."""
+    for A in (random_pattern(120000, 7, max_per_row=3), random_pattern(800, 9, max_per_row=12)):
+        Ad = hb.SparseMatrixELL.from_reference(A)
+        B = Ad.ordered(columns=True, packed=True)
+        assert B.Bd is None and B.ranks is not None
+        x = P.uniform_vector(A.cols, 2)
+        y = torch.empty(A.rows, dtype=torch.float64, device="cuda")
+        hb.Product.value(y, B, torch.from_numpy(x).cuda())
+        assert np.array_equal(y.cpu().numpy(), oracle.spmv(A, x))
 
 
 def test_ordered_copy_of_permuted_grid_is_banded(hb):
@@ -113,18 +142,18 @@ def test_ordered_copy_of_permuted_grid_is_banded(hb):
 
 
 def test_product_through_ordered_copy_2049_permuted_bit_exact(hb, oracle):
-    """The permuted 2049^2 workload: both forms of the ordered copy give the product on the
+    """The permuted 2049^2 workload: every form of the ordered copy gives the product on the
     permuted matrix bit for bit."""
     Ap, _ = P.q1_poisson_permuted(2049, 5)
     Ad = hb.SparseMatrixELL.from_reference(Ap)
     x = torch.from_numpy(P.uniform_vector(Ap.rows, 6)).cuda()
     y0 = torch.empty_like(x)
     hb.Product.value(y0, Ad, x)
-    for columns in (True, False):
-        B = Ad.ordered(columns=columns)
+    for form in FORMS:
+        B = ordered_form(Ad, form)
         y = torch.full_like(x, float("nan"))
         hb.Product.value(y, B, x)
-        assert torch.equal(y, y0), columns
+        assert torch.equal(y, y0), form
     # and the product on the permuted matrix against the oracle
     assert np.array_equal(y0.cpu().numpy(), oracle.spmv(Ap, x.cpu().numpy()))
 
@@ -145,9 +174,10 @@ def test_ordered_copy_edge_cases(hb, oracle):
         A = P.q1_poisson_permuted(M, M)[0]
         Ad = hb.SparseMatrixELL.from_reference(A)
         xh = P.uniform_vector(A.rows, M)
-        y = torch.empty(A.rows, dtype=torch.float64, device="cuda")
-        hb.Product.value(y, Ad.ordered(), torch.from_numpy(xh).cuda())
-        assert np.array_equal(y.cpu().numpy(), oracle.spmv(A, xh))
+        for form in FORMS:
+            y = torch.empty(A.rows, dtype=torch.float64, device="cuda")
+            hb.Product.value(y, ordered_form(Ad, form), torch.from_numpy(xh).cuda())
+            assert np.array_equal(y.cpu().numpy(), oracle.spmv(A, xh)), (M, form)
     # a rectangular matrix (a prolongation) has no order
     nf, nc, ip, ix, dv = P.prolongation_csr(Mc=5)
     R = hb.SparseMatrixELL.from_reference(P.ell_from_csr(nf, nc, ip, ix, dv))
