@@ -118,8 +118,8 @@ __device__ void cluster_cg(const int32_t *__restrict__ Aj, const T *__restrict__
             T sm[4];
             const T *rw = r, *pw = pin;
             hbd::ell_rows4<T, KT, 4>(Aj, Ax, ld, K, 4 * g, [&](int32_t j) {
-                const T rj = __ldcg(rw + j);
-                return first ? rj : add(mul(__ldcg(pw + j), beta), rj);
+                const T rj = __ldca(rw + j);
+                return first ? rj : add(mul(__ldca(pw + j), beta), rj);
             }, sm);
             T rv[4], pv[4], pn[4];
             hbd::ld4(r + 4 * g, rv);
@@ -203,8 +203,8 @@ __device__ void cluster_cg1(const int32_t *__restrict__ Aj, const T *__restrict_
 #pragma unroll
                 for (int c = 0; c < KS; ++c) {
                     if (j[c] >= 0) {
-                        const T rj = __ldcg(r + j[c]);
-                        g[c] = first ? rj : add(mul(__ldcg(pin + j[c]), beta), rj);
+                        const T rj = __ldca(r + j[c]);
+                        g[c] = first ? rj : add(mul(__ldca(pin + j[c]), beta), rj);
                     } else {
                         g[c] = T(0);
                     }
@@ -253,7 +253,7 @@ __device__ double defect64(const BatchDesc &d, Range rg, const double *xw, doubl
     double acc = 0.0;
     for (int64_t g = rg.lo + threadIdx.x; g < rg.hi; g += blockDim.x) {
         double sm[4], rv[4];
-        hbd::ell_rows4<double, KT, 4>(d.Aj, d.Ax64, d.ld, d.K, 4 * g, [&](int32_t j) { return __ldcg(xw + j); }, sm);
+        hbd::ell_rows4<double, KT, 4>(d.Aj, d.Ax64, d.ld, d.K, 4 * g, [&](int32_t j) { return __ldca(xw + j); }, sm);
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int64_t row = 4 * g + i;
@@ -287,7 +287,7 @@ __device__ double defect64_1(const BatchDesc &d, Range rg, const double *xw, dou
             }
             double g[KS];
 #pragma unroll
-            for (int c = 0; c < KS; ++c) g[c] = j[c] >= 0 ? __ldcg(xw + j[c]) : 0.0;
+            for (int c = 0; c < KS; ++c) g[c] = j[c] >= 0 ? __ldca(xw + j[c]) : 0.0;
 #pragma unroll
             for (int c = 0; c < KS; ++c)
                 if (j[c] >= 0) sm = add(sm, mul(a[c], g[c]));

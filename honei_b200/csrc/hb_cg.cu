@@ -581,8 +581,8 @@ __global__ void __launch_bounds__(hbr::RES_THREADS, 1) cg_res_kernel(const ResPa
                     pj = p_w[c];
                 } else {
                     const int64_t j = hbr::res_column(c, wlo);
-                    const T rj = __ldcg(P.r + j);
-                    pj = first ? rj : add(mul(__ldcg(pin + j), beta), rj);
+                    const T rj = __ldca(P.r + j);
+                    pj = first ? rj : add(mul(__ldca(pin + j), beta), rj);
                 }
                 s = add(s, mul(Ax_s[(int64_t)k * rpb + il], pj));
             }

@@ -387,8 +387,8 @@ __global__ void __launch_bounds__(hbr::RES_THREADS, 1) pcg_res_kernel(const PCGR
                     pj = p_w[c];
                 } else {
                     const int64_t j = hbr::res_column(c, wlo);
-                    pj = __ldcg(pin + j);
-                    if (!first) pj = add(mul(pj, talpha), mul(__ldcg(P.Pd + j), __ldcg(P.r + j)));
+                    pj = __ldca(pin + j);
+                    if (!first) pj = add(mul(pj, talpha), mul(__ldca(P.Pd + j), __ldca(P.r + j)));
                 }
                 s = add(s, mul(Ax_s[(int64_t)k * rpb + il], pj));
             }

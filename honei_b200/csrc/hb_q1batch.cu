@@ -146,9 +146,9 @@ __device__ __forceinline__ void band_rows4(const QBand &B, int64_t r0, const flo
 #pragma unroll
     for (int t = 0; t < 6; ++t) {
         const int64_t jl = r0 - root - 1 + t, jm = r0 - 1 + t, jh = r0 + root - 1 + t;
-        lo[t] = (jl >= 0 && jl < n) ? __ldcg(x + jl) : 0.f;
-        mid[t] = (jm >= 0 && jm < n) ? __ldcg(x + jm) : 0.f;
-        hi[t] = (jh >= 0 && jh < n) ? __ldcg(x + jh) : 0.f;
+        lo[t] = (jl >= 0 && jl < n) ? __ldca(x + jl) : 0.f;
+        mid[t] = (jm >= 0 && jm < n) ? __ldca(x + jm) : 0.f;
+        hi[t] = (jh >= 0 && jh < n) ? __ldca(x + jh) : 0.f;
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -190,7 +190,7 @@ __device__ __forceinline__ float prolong_row(int64_t k, int64_t Mf, int64_t Mc, 
     if (C & 1) { ci[0] = (C - 1) / 2; ci[1] = (C + 1) / 2; wc[0] = wc[1] = 0.5f; nc = 2; }
     else { ci[0] = C / 2; wc[0] = 1.f; nc = 1; }
     for (int a = 0; a < nr; ++a)
-        for (int q = 0; q < nc; ++q) s = add(s, mul(wr[a] * wc[q], __ldcg(c + ri[a] * Mc + ci[q])));
+        for (int q = 0; q < nc; ++q) s = add(s, mul(wr[a] * wc[q], __ldca(c + ri[a] * Mc + ci[q])));
     return s;
 }
 
@@ -206,7 +206,7 @@ __device__ __forceinline__ float restrict_row(int64_t k, int64_t Mf, int64_t Mc,
         for (int64_t C = 2 * c - 1; C <= 2 * c + 1; ++C) {
             if (C < 0 || C >= Mf || fine_boundary(R, C, Mf)) continue;
             const float wc = (C == 2 * c) ? 1.f : 0.5f;
-            s = add(s, mul(wr * wc, __ldcg(f + R * Mf + C)));
+            s = add(s, mul(wr * wc, __ldca(f + R * Mf + C)));
         }
     }
     return s;
@@ -423,7 +423,7 @@ __device__ __forceinline__ double defect64(const QSys &S, Range rg)
     const double *xw = S.x;
     for (int64_t g = rg.lo + threadIdx.x; g < rg.hi; g += blockDim.x) {
         double s[4], rv[4];
-        hbd::ell_rows4<double, 0, 4>(S.Aj, S.Ax64, S.ld, S.K, 4 * g, [&](int32_t j) { return __ldcg(xw + j); }, s);
+        hbd::ell_rows4<double, 0, 4>(S.Aj, S.Ax64, S.ld, S.K, 4 * g, [&](int32_t j) { return __ldca(xw + j); }, s);
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int64_t row = 4 * g + i;

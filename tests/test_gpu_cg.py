@@ -74,15 +74,20 @@ def test_cg_257_matches_reference_fixture(hb, oracle):
 
 
 def test_cg_f32_parity(hb, oracle):
+    """FP32 CG against the oracle's FP32 CG (tags::CPU order): iterations within +-1 (measured on
+    B200: equal at 33^2, 65^2, 129^2 and 257^2, as are the reference's own tags::CPU::SSE and
+    MultiCore::SSE); the final true residual, evaluated in FP64 from the FP32 iterates, within
+    2 % of the oracle's -- the FP32 iterates themselves differ at FP32 rounding."""
     for M in (33, 129):
         A = P.q1_poisson(M).astype(np.float32)
         b = oracle.spmv(A, P.uniform_vector(A.rows, 1).astype(np.float32))
         x_o, u_o = oracle.cg(A, b, eps=1e-5, max_iters=20000)
         x_g, u_g = run_cg(hb, A, b, 1e-5)
-        assert abs(u_g - u_o) <= 0.02 * u_o + 1, (u_g, u_o)
+        assert abs(u_g - u_o) <= 1, (u_g, u_o)
         r_o = relres(oracle, A.astype(np.float64), b.astype(np.float64), x_o.astype(np.float64))
         r_g = relres(oracle, A.astype(np.float64), b.astype(np.float64), x_g.astype(np.float64))
-        assert abs(r_g - r_o) <= 1e-5, (r_g, r_o)
+        print(M, u_g, u_o, r_g, r_o)
+        assert abs(r_g - r_o) <= 0.02 * r_o, (r_g, r_o)
 
 
 def test_cg_edge_cases(hb, oracle):
@@ -227,10 +232,11 @@ def test_cg_resident_kernel_edge_cases(hb, oracle):
     b32 = oracle.spmv(A32, P.uniform_vector(A32.rows, 1).astype(np.float32))
     x_o, u_o = oracle.cg(A32, b32, eps=1e-5, max_iters=20000)
     x_g, u_g = run_cg(hb, A32, b32, 1e-5)
-    assert abs(u_g - u_o) <= 0.02 * u_o + 1, (u_g, u_o)
+    assert abs(u_g - u_o) <= 1, (u_g, u_o)
     r_o = relres(oracle, A32.astype(np.float64), b32.astype(np.float64), x_o.astype(np.float64))
     r_g = relres(oracle, A32.astype(np.float64), b32.astype(np.float64), x_g.astype(np.float64))
-    assert abs(r_g - r_o) <= 1e-5, (r_g, r_o)
+    print(u_g, u_o, r_g, r_o)
+    assert abs(r_g - r_o) <= 0.02 * r_o, (r_g, r_o)
 
 
 def test_cg_concurrent_solves_on_separate_contexts(hb):
