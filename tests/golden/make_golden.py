@@ -366,4 +366,7 @@ if __name__ == "__main__":
     if "--only" in sys.argv:
         only = sys.argv[sys.argv.index("--only") + 1]
         args = [a for a in args if a != only]
-    main(args[0] if args else "/root/reference", only)
+    tree = args[0] if args else os.environ.get("HONEI_REF")
+    if not tree:
+        sys.exit("usage: make_golden.py <HONEI source tree> [--only NAME]  (or set HONEI_REF)")
+    main(tree, only)
