@@ -1085,7 +1085,7 @@ def run_case(name):
         from honei_b200 import batch as B
         sides = np.random.default_rng(2024).integers(17, 258, size=512)[:int(name.split("_")[1])]
         systems = B.q1_batch(sides, coef_range=(1e-1, 1e1), seed=2024, mode="cg64", eps=1e-8)
-        res = B.BatchSolver(systems, ctx=ctx).solve(B.HbBatchConfig(4, 256, 0, 1))
+        res = B.BatchSolver(systems, ctx=ctx).solve(B.HbBatchConfig(8, 256, 0, 1))
         print(sum(r["iterations"] for r in res))
     elif name == "q1batch":
         from honei_b200 import serve as S
