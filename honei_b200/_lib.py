@@ -62,6 +62,7 @@ SIGNATURES = {
     "hb_reserve": (i32, [vp, i64]),
     "hb_cg_set_resident": (i32, [vp, i32]),
     "hb_cg_set_layout": (i32, [vp, i32]),
+    "hb_set_block_size": (i32, [vp, i32, i32]),
     "hb_ell_validate": (i32, [vp, P_ell, P_i64]),
     "hb_ell_layout": (i32, [i64, i64, i64, P_i64, P_i64]),
     "hb_ell_import_f64": (i32, [vp, i64, i64, i64, i64, i64, vp, vp, vp, P_ell]),

@@ -118,8 +118,9 @@ int ew_launch(hb_context *ctx, int64_t n, T *r, const T *x, const T *y, T a)
 {
     if (!ctx || n < 0 || !r) return HB_ERR_INVALID;
     if (n == 0) return HB_OK;
-    const int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)ctx->num_sms * 16);
-    ew_kernel<T, OP><<<(unsigned)blocks, 256, 0, ctx->stream>>>(n, r, x, y, a);
+    const int th = ctx->block[HB_BLOCK_VECTOR] ? ctx->block[HB_BLOCK_VECTOR] : 256;
+    const int64_t blocks = std::min<int64_t>((n + th - 1) / th, (int64_t)ctx->num_sms * 16 * (256 / th > 0 ? 256 / th : 1));
+    ew_kernel<T, OP><<<(unsigned)blocks, th, 0, ctx->stream>>>(n, r, x, y, a);
     return hb_check_launch(ctx, "ew_kernel");
 }
 

@@ -155,6 +155,16 @@ int hb_cg_set_layout(hb_context *ctx, int rows_per_thread)
     return prev;
 }
 
+int hb_set_block_size(hb_context *ctx, int family, int threads)
+{
+    if (!ctx || family < HB_BLOCK_ELL || family > HB_BLOCK_VECTOR) return -1;
+    const int max = family == HB_BLOCK_VECTOR ? 1024 : 256;
+    if (threads != 0 && (threads < 32 || threads > max || threads % 32)) return -1;
+    const int prev = ctx->block[family];
+    ctx->block[family] = threads;
+    return prev;
+}
+
 int hb_reserve(hb_context *ctx, int64_t n)
 {
     if (!ctx || n < 0) return HB_ERR_INVALID;

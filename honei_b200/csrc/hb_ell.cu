@@ -199,14 +199,15 @@ int hb_launch_spmv_mode(hb_context *ctx, const hb_ell *A, int mode, const T *x, 
     if ((mode == HB_MODE_DEFECT || mode == HB_MODE_JACOBI) && !b) return HB_ERR_INVALID;
     if (mode == HB_MODE_JACOBI && !P) return HB_ERR_INVALID;
     const int64_t groups = (A->rows + 3) / 4;
-    const int64_t blocks = (groups + SPMV_THREADS - 1) / SPMV_THREADS;
+    const int threads = ctx->block[HB_BLOCK_ELL] ? ctx->block[HB_BLOCK_ELL] : SPMV_THREADS;
+    const int64_t blocks = (groups + threads - 1) / threads;
     const int vec = (((uintptr_t)y | (uintptr_t)b | (uintptr_t)P |
                       (mode == HB_MODE_JACOBI ? (uintptr_t)x : 0)) % 16) == 0;
     const int K = (int)A->K;
     const int32_t *Aj = A->Aj;
     const T *Ax = (const T *)A->Ax;
 #define HB_SPMV_CASE(KC, MD)                                                                    \
-    ell_spmv_kernel<T, KC, MD><<<(unsigned)blocks, SPMV_THREADS, 0, ctx->stream>>>(              \
+    ell_spmv_kernel<T, KC, MD><<<(unsigned)blocks, threads, 0, ctx->stream>>>(                   \
         A->rows, A->ld, K, Aj, Ax, x, b, P, y, vec)
 #define HB_SPMV_K(MD)                                                                           \
     switch (K) {                                                                                \

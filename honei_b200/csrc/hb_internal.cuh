@@ -50,6 +50,8 @@ struct hb_context {
     int cg_resident = 1;
     // streaming CG: one row per thread (cg_row_kernel) or groups of four rows (hb_cg_set_layout)
     int cg_row_layout = 0;
+    // threads per block chosen by the caller for a kernel family (hb_set_block_size); 0 = default
+    int block[3] = {0, 0, 0};
     std::string last_error;
 };
 

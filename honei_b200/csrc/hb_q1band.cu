@@ -212,10 +212,14 @@ int check_q1band(const hb_q1band *A, int dtype)
 
 inline bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 
+// threads per block of the banded kernels on this context (hb_set_block_size), and their grid
+int band_threads(hb_context *ctx) { return ctx->block[HB_BLOCK_Q1BAND] ? ctx->block[HB_BLOCK_Q1BAND] : 256; }
+
 int grid_for(hb_context *ctx, int64_t work)
 {
-    const int64_t blocks = (work + 255) / 256;
-    return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)ctx->num_sms * 64));
+    const int th = band_threads(ctx);
+    const int64_t blocks = (work + th - 1) / th;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)ctx->num_sms * 64 * (256 / th)));
 }
 
 template <typename T>
@@ -232,11 +236,11 @@ int q1band_apply(hb_context *ctx, const hb_q1band *A, const T *b, const T *x, T 
     const Bands<T> B = bands_of<T>(A);
     const int grid = grid_for(ctx, (n + Rows<T>::R - 1) / Rows<T>::R);
     if (mode == 0) {
-        if (vec) q1band_kernel<T, 0, true><<<grid, 256, 0, ctx->stream>>>(n, A->root, B, x, b, y);
-        else q1band_kernel<T, 0, false><<<grid, 256, 0, ctx->stream>>>(n, A->root, B, x, b, y);
+        if (vec) q1band_kernel<T, 0, true><<<grid, band_threads(ctx), 0, ctx->stream>>>(n, A->root, B, x, b, y);
+        else q1band_kernel<T, 0, false><<<grid, band_threads(ctx), 0, ctx->stream>>>(n, A->root, B, x, b, y);
     } else {
-        if (vec) q1band_kernel<T, 1, true><<<grid, 256, 0, ctx->stream>>>(n, A->root, B, x, b, y);
-        else q1band_kernel<T, 1, false><<<grid, 256, 0, ctx->stream>>>(n, A->root, B, x, b, y);
+        if (vec) q1band_kernel<T, 1, true><<<grid, band_threads(ctx), 0, ctx->stream>>>(n, A->root, B, x, b, y);
+        else q1band_kernel<T, 1, false><<<grid, band_threads(ctx), 0, ctx->stream>>>(n, A->root, B, x, b, y);
     }
     return hb_check_launch(ctx, "q1band_kernel");
 }
@@ -253,8 +257,8 @@ int hb_launch_band_mode(hb_context *ctx, const hb_q1band *A, int mode, const T *
     const Bands<T> B = bands_of<T>(A);
     const int grid = grid_for(ctx, (n + Rows<T>::R - 1) / Rows<T>::R);
 #define HB_BAND_LAUNCH(MD)                                                                                     \
-    if (vec) q1band_kernel<T, MD, true, true><<<grid, 256, 0, ctx->stream>>>(n, A->root, B, x, b, y, P);       \
-    else q1band_kernel<T, MD, false, true><<<grid, 256, 0, ctx->stream>>>(n, A->root, B, x, b, y, P)
+    if (vec) q1band_kernel<T, MD, true, true><<<grid, band_threads(ctx), 0, ctx->stream>>>(n, A->root, B, x, b, y, P);       \
+    else q1band_kernel<T, MD, false, true><<<grid, band_threads(ctx), 0, ctx->stream>>>(n, A->root, B, x, b, y, P)
     switch (mode) {
         case HB_MODE_SPMV: HB_BAND_LAUNCH(0); break;
         case HB_MODE_DEFECT: HB_BAND_LAUNCH(1); break;
@@ -307,9 +311,9 @@ int hb_q1band_fill_poisson(hb_context *ctx, int64_t M, hb_q1band *A)
         if (!A->band[k]) return HB_ERR_INVALID;
     const int grid = grid_for(ctx, A->n);
     if (A->dtype == HB_F64)
-        q1band_poisson_kernel<double><<<grid, 256, 0, ctx->stream>>>(A->n, M, bands_of<double>(A));
+        q1band_poisson_kernel<double><<<grid, band_threads(ctx), 0, ctx->stream>>>(A->n, M, bands_of<double>(A));
     else
-        q1band_poisson_kernel<float><<<grid, 256, 0, ctx->stream>>>(A->n, M, bands_of<float>(A));
+        q1band_poisson_kernel<float><<<grid, band_threads(ctx), 0, ctx->stream>>>(A->n, M, bands_of<float>(A));
     return hb_check_launch(ctx, "q1band_poisson_kernel");
 }
 
@@ -327,10 +331,10 @@ int hb_q1band_from_ell(hb_context *ctx, const hb_ell *E, hb_q1band *A)
     int *flag = (int *)hb_scalars(ctx);
     HB_CUDA_TRY(ctx, cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream));
     if (A->dtype == HB_F64)
-        q1band_from_ell_kernel<double><<<grid, 256, 0, ctx->stream>>>(n, A->root, E->ld, (int)E->K, E->Aj,
+        q1band_from_ell_kernel<double><<<grid, band_threads(ctx), 0, ctx->stream>>>(n, A->root, E->ld, (int)E->K, E->Aj,
                                                                       (const double *)E->Ax, bands_of<double>(A), flag);
     else
-        q1band_from_ell_kernel<float><<<grid, 256, 0, ctx->stream>>>(n, A->root, E->ld, (int)E->K, E->Aj,
+        q1band_from_ell_kernel<float><<<grid, band_threads(ctx), 0, ctx->stream>>>(n, A->root, E->ld, (int)E->K, E->Aj,
                                                                      (const float *)E->Ax, bands_of<float>(A), flag);
     int st = hb_check_launch(ctx, "q1band_from_ell_kernel");
     if (st) return st;

@@ -104,6 +104,21 @@ def _vec(t: torch.Tensor, dtype, name: str) -> int:
     return t.data_ptr()
 
 
+BLOCK_FAMILIES = {"ell": 0, "q1band": 1, "vector": 2}
+
+
+def set_block_size(family: str, threads: int, ctx: Context | None = None) -> int:
+    """Threads per block of a kernel family on ctx (hb_set_block_size): "ell" (ELL product,
+    defect, Jacobi sweep; 32..256), "q1band" (banded Q1 kernels; 32..256) or "vector"
+    (elementwise kernels; 32..1024), a multiple of 32, or 0 for the default.  The knob HONEI's
+    honeirc block-size keys set; results do not depend on it.  Returns the previous value."""
+    ctx = ctx or default_context()
+    prev = lib().hb_set_block_size(ctx.handle, BLOCK_FAMILIES[family], int(threads))
+    if prev < 0:
+        raise ValueError(f"block size {threads} is not valid for {family}")
+    return prev
+
+
 class _DeviceArray:
     """__cuda_array_interface__ view of device memory owned elsewhere (zero copy)."""
 

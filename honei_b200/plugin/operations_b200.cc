@@ -13,6 +13,17 @@
  * its vectors for tags::GPU::CUDA (the MemoryArbiter uploads lazily through
  * MemoryBackend<tags::GPU::CUDA>), calls one entry point of the C ABI, and unlocks.  Results
  * stay on the device until a host lock reads them back.
+ *
+ * Block sizes come from HONEI's Configuration, as the reference's CUDA wrappers take them (e.g.
+ * honei/la/product-cuda.cc:594-625, honei/la/scaled_sum-cuda.cc:210-236): before each call the
+ * operator reads its honeirc key (cuda::product_smell_dv_{float,double} for the ELL product and
+ * defect, cuda::product_bmdv_q1_* for the banded ones, cuda::scaled_sum_two_*,
+ * cuda::scaled_sum_three_*, cuda::scale_one_*, cuda::sum_two_*, cuda::difference_two_*,
+ * cuda::element_product_two_* for the vector operators; default 128 as there) and sets it on
+ * the context (hb_set_block_size), clamped to the kernel's range and rounded down to a multiple
+ * of 32.  The results do not depend on it.  The dot-product and norm keys are not used: those
+ * kernels keep one fixed reduction tree.  ell::threads is honoured by the matrices themselves:
+ * a SparseMatrixELL built with T lanes per row is imported with its T.
  */
 #include "b200_backend.hh"
 
@@ -30,6 +41,7 @@
 #include <honei/la/matrix_error.hh>
 #include <honei/math/defect.hh>
 #include <honei/math/spai2.hh>
+#include <honei/util/configuration.hh>
 #include <honei/util/memory_arbiter.hh>
 
 #include <cuda_runtime.h>
@@ -255,33 +267,48 @@ namespace honei
                 throw VectorSizeDoesNotMatch(b.size(), a.size());
         }
 
-        int spmv(const hb_ell & A, const double * x, double * y) { return hb_spmv_f64(context(), &A, x, y); }
-        int spmv(const hb_ell & A, const float * x, float * y) { return hb_spmv_f32(context(), &A, x, y); }
-        int defect(const hb_ell & A, const double * b, const double * x, double * r) { return hb_defect_f64(context(), &A, b, x, r); }
-        int defect(const hb_ell & A, const float * b, const float * x, float * r) { return hb_defect_f32(context(), &A, b, x, r); }
+        /// Sets the block size of a kernel family on this thread's context from a honeirc key.
+        hb_context * configured(int family, const char * key)
+        {
+            hb_context * ctx(context());
+            int v(Configuration::instance()->get_value(key, 128));
+            const int max(family == HB_BLOCK_VECTOR ? 1024 : 256);
+            v = v < 32 ? 32 : (v > max ? max : v);
+            hb_set_block_size(ctx, family, v - v % 32);
+            return ctx;
+        }
+
+        int spmv(const hb_ell & A, const double * x, double * y)
+        { return hb_spmv_f64(configured(HB_BLOCK_ELL, "cuda::product_smell_dv_double"), &A, x, y); }
+        int spmv(const hb_ell & A, const float * x, float * y)
+        { return hb_spmv_f32(configured(HB_BLOCK_ELL, "cuda::product_smell_dv_float"), &A, x, y); }
+        int defect(const hb_ell & A, const double * b, const double * x, double * r)
+        { return hb_defect_f64(configured(HB_BLOCK_ELL, "cuda::product_smell_dv_double"), &A, b, x, r); }
+        int defect(const hb_ell & A, const float * b, const float * x, float * r)
+        { return hb_defect_f32(configured(HB_BLOCK_ELL, "cuda::product_smell_dv_float"), &A, b, x, r); }
         int dot(int64_t n, const double * x, const double * y, double * out) { return hb_dot_f64(context(), n, x, y, out); }
         int dot(int64_t n, const float * x, const float * y, float * out) { return hb_dot_f32(context(), n, x, y, out); }
         int norm(int64_t n, const double * x, int root, double * out) { return hb_norm_l2_f64(context(), n, x, root, out); }
         int norm(int64_t n, const float * x, int root, float * out) { return hb_norm_l2_f32(context(), n, x, root, out); }
-        int axpy(int64_t n, double * x, const double * y, double b) { return hb_scaled_sum_f64(context(), n, x, y, b); }
-        int axpy(int64_t n, float * x, const float * y, float b) { return hb_scaled_sum_f32(context(), n, x, y, b); }
-        int axpy3(int64_t n, double * r, const double * x, const double * y, double b) { return hb_scaled_sum3_f64(context(), n, r, x, y, b); }
-        int axpy3(int64_t n, float * r, const float * x, const float * y, float b) { return hb_scaled_sum3_f32(context(), n, r, x, y, b); }
-        int scale(int64_t n, double * x, double a) { return hb_scale_f64(context(), n, x, a); }
-        int scale(int64_t n, float * x, float a) { return hb_scale_f32(context(), n, x, a); }
-        int sum(int64_t n, double * x, const double * y) { return hb_sum_f64(context(), n, x, y); }
-        int sum(int64_t n, float * x, const float * y) { return hb_sum_f32(context(), n, x, y); }
-        int diff(int64_t n, double * r, const double * x, const double * y) { return hb_difference_f64(context(), n, r, x, y); }
-        int diff(int64_t n, float * r, const float * x, const float * y) { return hb_difference_f32(context(), n, r, x, y); }
-        int eprod(int64_t n, double * r, const double * x, const double * y) { return hb_element_product_f64(context(), n, r, x, y); }
-        int eprod(int64_t n, float * r, const float * x, const float * y) { return hb_element_product_f32(context(), n, r, x, y); }
+        int axpy(int64_t n, double * x, const double * y, double b) { return hb_scaled_sum_f64(configured(HB_BLOCK_VECTOR, "cuda::scaled_sum_two_double"), n, x, y, b); }
+        int axpy(int64_t n, float * x, const float * y, float b) { return hb_scaled_sum_f32(configured(HB_BLOCK_VECTOR, "cuda::scaled_sum_two_float"), n, x, y, b); }
+        int axpy3(int64_t n, double * r, const double * x, const double * y, double b) { return hb_scaled_sum3_f64(configured(HB_BLOCK_VECTOR, "cuda::scaled_sum_three_double"), n, r, x, y, b); }
+        int axpy3(int64_t n, float * r, const float * x, const float * y, float b) { return hb_scaled_sum3_f32(configured(HB_BLOCK_VECTOR, "cuda::scaled_sum_three_float"), n, r, x, y, b); }
+        int scale(int64_t n, double * x, double a) { return hb_scale_f64(configured(HB_BLOCK_VECTOR, "cuda::scale_one_double"), n, x, a); }
+        int scale(int64_t n, float * x, float a) { return hb_scale_f32(configured(HB_BLOCK_VECTOR, "cuda::scale_one_float"), n, x, a); }
+        int sum(int64_t n, double * x, const double * y) { return hb_sum_f64(configured(HB_BLOCK_VECTOR, "cuda::sum_two_double"), n, x, y); }
+        int sum(int64_t n, float * x, const float * y) { return hb_sum_f32(configured(HB_BLOCK_VECTOR, "cuda::sum_two_float"), n, x, y); }
+        int diff(int64_t n, double * r, const double * x, const double * y) { return hb_difference_f64(configured(HB_BLOCK_VECTOR, "cuda::difference_two_double"), n, r, x, y); }
+        int diff(int64_t n, float * r, const float * x, const float * y) { return hb_difference_f32(configured(HB_BLOCK_VECTOR, "cuda::difference_two_float"), n, r, x, y); }
+        int eprod(int64_t n, double * r, const double * x, const double * y) { return hb_element_product_f64(configured(HB_BLOCK_VECTOR, "cuda::element_product_two_double"), n, r, x, y); }
+        int eprod(int64_t n, float * r, const float * x, const float * y) { return hb_element_product_f32(configured(HB_BLOCK_VECTOR, "cuda::element_product_two_float"), n, r, x, y); }
 
-        int q1_spmv(const hb_q1band & A, const double * x, double * y) { return hb_q1band_spmv_f64(context(), &A, x, y); }
-        int q1_spmv(const hb_q1band & A, const float * x, float * y) { return hb_q1band_spmv_f32(context(), &A, x, y); }
+        int q1_spmv(const hb_q1band & A, const double * x, double * y) { return hb_q1band_spmv_f64(configured(HB_BLOCK_Q1BAND, "cuda::product_bmdv_q1_double"), &A, x, y); }
+        int q1_spmv(const hb_q1band & A, const float * x, float * y) { return hb_q1band_spmv_f32(configured(HB_BLOCK_Q1BAND, "cuda::product_bmdv_q1_float"), &A, x, y); }
         int q1_defect(const hb_q1band & A, const double * b, const double * x, double * r)
-        { return hb_q1band_defect_f64(context(), &A, b, x, r); }
+        { return hb_q1band_defect_f64(configured(HB_BLOCK_Q1BAND, "cuda::product_bmdv_q1_double"), &A, b, x, r); }
         int q1_defect(const hb_q1band & A, const float * b, const float * x, float * r)
-        { return hb_q1band_defect_f32(context(), &A, b, x, r); }
+        { return hb_q1band_defect_f32(configured(HB_BLOCK_Q1BAND, "cuda::product_bmdv_q1_float"), &A, b, x, r); }
 
         /// The nine bands of a BandedMatrixQx locked for the GPU tag (the MemoryArbiter uploads
         /// them on first use and keeps them resident), as an hb_q1band.

@@ -380,6 +380,20 @@ int hb_cg_set_resident(hb_context *ctx, int enable);
  * group the rows differently, so the iterates agree to rounding.  Returns the previous setting,
  * or -1 for an invalid argument. */
 int hb_cg_set_layout(hb_context *ctx, int rows_per_thread);
+/* Threads per block of a kernel family on this context, the knob HONEI's honeirc keys set for
+ * its CUDA kernels (honei/honeirc: cuda::product_smell_dv_*, cuda::product_bmdv_q1_*,
+ * cuda::scaled_sum_two_* and the other vector keys; read at honei/la/product-cuda.cc:594-625,
+ * honei/la/scaled_sum-cuda.cc:210-236, honei/la/difference-cuda.cc:184-210):
+ *   HB_BLOCK_ELL     the ELL product / defect / Jacobi-sweep kernel (4 rows per thread): 32..256
+ *   HB_BLOCK_Q1BAND  the banded Q1 kernels: 32..256
+ *   HB_BLOCK_VECTOR  the elementwise vector kernels (scaled sums, scale, sum, difference,
+ *                    element product, fill): 32..1024
+ * in multiples of 32; 0 restores the library's default (256).  Results do not depend on it (each
+ * output element is computed by one thread in a fixed order).  The dot-product and norm kernels
+ * keep their fixed reduction tree (and so their bits) and have no such knob.  Returns the
+ * previous setting (0 = default), or -1 for an invalid family or size. */
+enum { HB_BLOCK_ELL = 0, HB_BLOCK_Q1BAND = 1, HB_BLOCK_VECTOR = 2 };
+int hb_set_block_size(hb_context *ctx, int family, int threads);
 
 /* Preconditioned CG, CGSolver<Tag, methods::VAR>::value(A, P, b, x, max_iters, used_iters,
  * eps), honei/math/cg.hh:140-219, with the preconditioner container P either a vector (the

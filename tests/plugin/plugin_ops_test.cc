@@ -6,6 +6,7 @@
 // This translation unit does NOT include solvers_b200.hh: CGSolver<tags::GPU::CUDA, NONE> here
 // is HONEI's generic template (honei/math/cg.hh:63-133) running on the plugin's operators.
 #include "plugin_common.hh"
+#include "honei_b200/plugin/b200_backend.hh"
 
 #include <honei/la/difference.hh>
 #include <honei/la/dot_product.hh>
@@ -319,8 +320,55 @@ template <typename DT_> void spai(unsigned long M, const std::string & tag)
     report(threw, "SPAI2<GPU::CUDA> MatrixIsNotSquare " + tag);
 }
 
+// The honeirc block-size keys (honei/honeirc: cuda::product_smell_dv_*, cuda::product_bmdv_q1_*,
+// cuda::scaled_sum_two_*): each value set through Configuration reaches the plugin's context
+// (clamped to the kernel's range, a multiple of 32), and the results stay bit-exact to tags::CPU.
+template <typename DT_> void honeirc_blocks(unsigned long M, const std::string & tag)
+{
+    const bool dbl(sizeof(DT_) == 8);
+    const std::string ell(dbl ? "cuda::product_smell_dv_double" : "cuda::product_smell_dv_float");
+    const std::string band(dbl ? "cuda::product_bmdv_q1_double" : "cuda::product_bmdv_q1_float");
+    const std::string axpy(dbl ? "cuda::scaled_sum_two_double" : "cuda::scaled_sum_two_float");
+    SparseMatrixELL<DT_> A(q1<DT_>(M));
+    const unsigned long n(A.rows());
+    DenseVector<DT_> z(n, DT_(0));
+    BandedMatrixQx<Q1Type, DT_> Q(n, z.copy(), z.copy(), z.copy(), z.copy(), z.copy(), z.copy(), z.copy(),
+            z.copy(), z.copy());
+    FillMatrix<tags::CPU, applications::POISSON, boundary_types::DIRICHLET::DIRICHLET_0>::value(Q);
+    DenseVector<DT_> x(seeded<DT_>(n, 31)), w(seeded<DT_>(n, 32));
+    DenseVector<DT_> ycpu(n), qcpu(n), acpu(x.copy());
+    Product<tags::CPU>::value(ycpu, A, x);
+    Product<tags::CPU>::value(qcpu, Q, x);
+    ScaledSum<tags::CPU>::value(acpu, w, DT_(0.5));
+    const int sizes[] = {32, 96, 128, 200, 256, 1000};
+    for (int bs : sizes)
+    {
+        Configuration::instance()->set_value(ell, bs);
+        Configuration::instance()->set_value(band, bs);
+        Configuration::instance()->set_value(axpy, bs);
+        DenseVector<DT_> y(n), q(n), a(x.copy());
+        Product<tags::GPU::CUDA>::value(y, A, x);
+        const int got_ell(hb_set_block_size(b200::context(), HB_BLOCK_ELL, 0));
+        Product<tags::GPU::CUDA>::value(q, Q, x);
+        const int got_band(hb_set_block_size(b200::context(), HB_BLOCK_Q1BAND, 0));
+        ScaledSum<tags::GPU::CUDA>::value(a, w, DT_(0.5));
+        const int got_vec(hb_set_block_size(b200::context(), HB_BLOCK_VECTOR, 0));
+        const int want(bs > 256 ? 256 : bs - bs % 32), want_vec(bs - bs % 32);
+        std::ostringstream d;
+        d << "context blocks " << got_ell << " / " << got_band << " / " << got_vec;
+        report(got_ell == want && got_band == want && got_vec == want_vec && equal(ycpu, y) && equal(qcpu, q)
+                && equal(acpu, a), "honeirc block size " + std::to_string(bs) + " applied, results bit-exact " + tag,
+                d.str());
+    }
+    Configuration::instance()->set_value(ell, 128);
+    Configuration::instance()->set_value(band, 128);
+    Configuration::instance()->set_value(axpy, 128);
+}
+
 int main(int argc, char ** argv)
 {
+    honeirc_blocks<double>(33, "f64 33^2");
+    honeirc_blocks<float>(65, "f32 65^2");
     spai<double>(33, "f64 33^2");
     spai<float>(65, "f32 65^2");
     csr<double>(33, "f64 33^2");

@@ -10,6 +10,7 @@
 #include "plugin_common.hh"
 
 #include <honei/la/product.hh>
+#include <honei/util/configuration.hh>
 #include <honei/util/memory_arbiter.hh>
 
 #include <algorithm>
@@ -68,6 +69,8 @@ int main(int argc, char ** argv)
     y.unlock(lm_read_only);
     double out[2] = {0., 0.}, ms[2] = {0., 0.};
     const unsigned long ks[2] = {1, 10};
+    // the product kernel's block size, as honeirc gives it (cuda::product_smell_dv_double)
+    const int configured(Configuration::instance()->get_value("cuda::product_smell_dv_double", 128));
     for (int c(0) ; c < 2 ; ++c)
     {
         std::vector<double> t;
@@ -94,7 +97,7 @@ int main(int argc, char ** argv)
             " with host DenseVectors through MemoryArbiter / MemoryBackend<tags::GPU::CUDA>\", \"rows\": %lu, \"nnz\": %lu, "
             "\"bytes_per_product\": %.0f, \"one_product_per_upload_gbs\": %.2f, \"ms_per_product_one_per_upload\": %.4f, "
             "\"ten_products_per_upload_gbs\": %.2f, \"ms_per_step_ten_products\": %.4f, \"h2d_bytes_per_step\": %lu, "
-            "\"d2h_bytes_per_step\": %lu, \"steps\": %lu, \"y_equals_tags_cpu\": %s}\n",
-            n, nnz, bytes, out[0], ms[0], out[1], ms[1], n * 8, n * 8, steps, same ? "true" : "false");
+            "\"d2h_bytes_per_step\": %lu, \"steps\": %lu, \"y_equals_tags_cpu\": %s, \"honeirc_block\": %d}\n",
+            n, nnz, bytes, out[0], ms[0], out[1], ms[1], n * 8, n * 8, steps, same ? "true" : "false", configured);
     return same ? 0 : 1;
 }
