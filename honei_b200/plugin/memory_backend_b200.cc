@@ -8,6 +8,14 @@
  * Blocks are keyed by (memid, address) so ranges of one vector get their own device copies.
  * Every (re)upload bumps a generation counter, which the SparseMatrixELL mirror cache uses to
  * notice that a matrix changed on the host.
+ *
+ * Device buffers are recycled: free() (which the arbiter calls whenever the host writes a vector,
+ * so every step of a host-side loop) returns a block's buffer to a size-keyed cache instead of
+ * cudaFree, and the next block of a fitting size takes it instead of cudaMalloc.  cudaFree
+ * synchronises the whole device and a large cudaMalloc costs milliseconds, once per step each.
+ * The cache holds at most a quarter of the device's memory; a cudaMalloc that fails empties it
+ * and tries again.  Reuse is ordered: every kernel of this backend runs on the legacy default
+ * stream, as do the synchronous copies that refill a recycled buffer.
  */
 #include "b200_backend.hh"
 
@@ -34,6 +42,9 @@ namespace honei
         };
 
         std::map<std::pair<void *, void *>, Block> blocks;
+        std::multimap<unsigned long, void *> cache;     // recycled buffers by size
+        unsigned long cached_bytes = 0;
+        unsigned long cache_limit = 0;
         std::recursive_mutex mutex;
         std::uint64_t next_generation = 1;
 
@@ -43,6 +54,57 @@ namespace honei
             return i == blocks.end() ? nullptr : &i->second;
         }
 
+        void release(void * device, unsigned long bytes)
+        {
+            if (! cache_limit)
+            {
+                std::size_t free_b(0), total_b(0);
+                cudaMemGetInfo(&free_b, &total_b);
+                cache_limit = total_b / 4 ? total_b / 4 : 1;
+            }
+            if (cached_bytes + bytes <= cache_limit)
+            {
+                cache.insert(std::make_pair(bytes, device));
+                cached_bytes += bytes;
+            }
+            else
+                cudaFree(device);
+        }
+
+        void drop_cache()
+        {
+            for (auto & kv : cache)
+                cudaFree(kv.second);
+            cache.clear();
+            cached_bytes = 0;
+        }
+
+        /// A buffer of at least bytes: a recycled one of up to 5/4 of the size, else a new one.
+        std::pair<void *, unsigned long> take(unsigned long bytes)
+        {
+            const unsigned long want(bytes ? bytes : 1);
+            auto i(cache.lower_bound(want));
+            if (i != cache.end() && i->first <= want + want / 4)
+            {
+                std::pair<void *, unsigned long> r(i->second, i->first);
+                cached_bytes -= i->first;
+                cache.erase(i);
+                return r;
+            }
+            void * d(nullptr);
+            if (cudaMalloc(&d, want) != cudaSuccess)
+            {
+                cudaGetLastError();
+                drop_cache();
+                if (cudaMalloc(&d, want) != cudaSuccess)
+                {
+                    cudaGetLastError();
+                    throw InternalError("MemoryBackend<GPU::CUDA>: cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+                }
+            }
+            return std::make_pair(d, want);
+        }
+
         Block & get(void * memid, void * address, unsigned long bytes)
         {
             Block * b(find(memid, address));
@@ -50,18 +112,13 @@ namespace honei
                 return *b;
             if (b)
             {
-                cudaFree(b->device);
+                release(b->device, b->bytes);
                 blocks.erase(std::make_pair(memid, address));
             }
-            void * d(nullptr);
-            if (cudaMalloc(&d, bytes ? bytes : 1) != cudaSuccess)
-            {
-                cudaGetLastError();
-                throw InternalError("MemoryBackend<GPU::CUDA>: cudaMalloc of " + std::to_string(bytes) + " bytes failed");
-            }
+            const std::pair<void *, unsigned long> d(take(bytes));
             Block & nb(blocks[std::make_pair(memid, address)]);
-            nb.device = d;
-            nb.bytes = bytes;
+            nb.device = d.first;
+            nb.bytes = d.second;
             nb.generation = next_generation++;
             return nb;
         }
@@ -85,6 +142,7 @@ namespace honei
     {
         for (auto & kv : _imp->blocks)
             cudaFree(kv.second.device);
+        _imp->drop_cache();
         g_backend_imp = nullptr;
     }
 
@@ -133,7 +191,7 @@ namespace honei
         {
             if (i->first.first == memid)
             {
-                cudaFree(i->second.device);
+                _imp->release(i->second.device, i->second.bytes);
                 i = _imp->blocks.erase(i);
             }
             else

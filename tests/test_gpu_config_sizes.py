@@ -159,8 +159,9 @@ def _batch_sides(n=512, seed=BATCH_SEED):
 @pytest.mark.parametrize("shape", [(2, 512, 4), (4, 256, 1), (8, 256, 1)], ids=lambda t: "c%d_t%d_r%d" % t)
 def test_batch_512_cg64_within_the_references_own_spread(hb, oracle, shape):
     """The 512-system batch of the benchmark, FP64 CG, solved in one launch at the shapes the
-    tuner picks (4-CTA clusters of 256 threads, one row per thread) and two others, against the reference's CGSolver<tags::CPU> on every
-    system (tests/golden/batch512.npz, written by the compiled reference).
+    tuner picks (clusters of 4 or 8 CTAs of 256 threads, one row per thread) and at the
+    four-row layout, against the reference's CGSolver<tags::CPU> on every system
+    (tests/golden/batch512.npz, written by the compiled reference).
 
     On these systems (contrast 10^2, up to 872 iterations) the iteration count at which the
     1e-8 test fires depends on the summation order of the dot products.  The reference's own
@@ -209,8 +210,9 @@ def test_batch_512_cg64_within_the_references_own_spread(hb, oracle, shape):
 
 def test_batch_512_ir32_every_system_matches_oracle(hb, oracle):
     """The same batch in mixed precision (FP64 refinement around FP32 CG to 1e-3 per step, to a
-    1e-8 FP64 residual), at the tuned shape (4-CTA clusters of 256 threads, one row per thread): every system's outer step count against the oracle's scaled
-    refinement around FP32 CG on the same matrix and right-hand side."""
+    1e-8 FP64 residual), one row per thread on 4-CTA clusters of 256 threads: every system's
+    outer step count against the oracle's scaled refinement around FP32 CG on the same matrix
+    and right-hand side."""
     from honei_b200 import batch as B
     sides = _batch_sides()
     systems = B.q1_batch(sides, coef_range=(1e-1, 1e1), seed=BATCH_SEED, mode="ir32", eps=1e-8, inner_eps=1e-3)
