@@ -1050,7 +1050,7 @@ def run_ours(args):
 
 def run_case(name):
     """One small workload for a profiler capture (ncu -k <kernel> ... python bench.py --case NAME):
-    spmv / spmv_permuted / spmv_ordered (2049^2 FP64 products), cg_2049 (the streaming CG kernel,
+    spmv / spmv_permuted / spmv_ordered (2049^2 FP64 products), spmv_f32 (the FP32 product), cg_2049 (the streaming CG kernel,
     200 iterations), mg_2049 (one banded FP64 V(2,2) solve), batch_512 / batch_128 (the
     512-system batch or its first 128 systems, tuned shape), q1batch (48 mid-size served systems in one batched MG-PCG launch), blas1 (dot,
     norm and axpy on 2049^2 vectors).  Prints 'ok' and the case's own figure."""
@@ -1058,7 +1058,13 @@ def run_case(name):
     from honei_b200 import la, problems as P
     torch.cuda.set_device(0)
     ctx = la.Context(0)
-    if name in ("spmv", "spmv_permuted", "spmv_ordered"):
+    if name == "spmv_f32":
+        A = la.SparseMatrixELL.q1_poisson(M_SPMV, ctx=ctx).to_float(ctx=ctx)
+        x = torch.from_numpy(P.uniform_vector(M_SPMV ** 2, 6).astype(np.float32)).cuda()
+        y = torch.empty_like(x)
+        for _ in range(4):
+            la.Product.value(y, A, x, ctx=ctx)
+    elif name in ("spmv", "spmv_permuted", "spmv_ordered"):
         if name == "spmv":
             A = la.SparseMatrixELL.q1_poisson(M_SPMV, ctx=ctx)
         else:
