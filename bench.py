@@ -427,6 +427,44 @@ def bench_batch(la, ctx, n_systems=512, seed=2024):
     return out
 
 
+def bench_cg_permuted(la, ctx, M=M_SPMV, seed=5):
+    """Config 2's CG on the randomly permuted 2049^2 matrix: as given (every gather a random
+    sector) and through its Cuthill-McKee ordered copy (CGSolver on an OrderedMatrixELL: b and x
+    permuted once per solve, the iterations in the copy's numbering)."""
+    import torch
+    from honei_b200 import problems as P
+    Ap, _ = P.q1_poisson_permuted(M, seed=seed)
+    Ad = la.SparseMatrixELL.from_reference(Ap, ctx)
+    n = Ap.rows
+    xt = torch.from_numpy(P.uniform_vector(n, 1)).cuda()
+    b = torch.empty_like(xt)
+    la.Product.value(b, Ad, xt, ctx=ctx)
+    r = torch.empty_like(xt)
+    out = {"workload": f"plain FP64 CG, Q1 {M}^2 randomly permuted (seed {seed}), 1e-8 relative, x0 = 0"}
+    t0 = time.perf_counter()
+    O = Ad.ordered(columns=True, ctx=ctx)
+    torch.cuda.synchronize()
+    out["ordering_ms"] = round((time.perf_counter() - t0) * 1e3, 1)
+    for name, A in (("as_given", Ad), ("ordered_copy", O)):
+        x = torch.zeros_like(xt)
+        la.CGSolver.value(A, None, b, x, 20, 1e-8, ctx=ctx)          # warm-up
+        x.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        used = la.CGSolver.value(A, None, b, x, 100000, 1e-8, ctx=ctx)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        la.Defect.value(r, b, Ad, x, ctx=ctx)
+        out[name] = {"iterations": used, "ms": round(ms, 2), "us_per_iteration": round(1e3 * ms / max(used, 1), 2),
+                     "relres": float(torch.linalg.norm(r) / torch.linalg.norm(b))}
+    out["speedup_ordered"] = round(out["as_given"]["ms"] / out["ordered_copy"]["ms"], 2)
+    del Ap, Ad, O
+    torch.cuda.empty_cache()
+    return out
+
+
 def bench_cg_large(la, ctx, sizes=(1025, 2049), cpu=True, cpu_iters=10):
     """Plain FP64 CG (config 2's CG) on the Q1 Poisson grids of 1025^2 and 2049^2: b = A x_true
     with x_true ~ U[-1, 1], x0 = 0, 1e-8 relative; the streaming persistent kernel.  Algorithmic
@@ -995,7 +1033,7 @@ def run_ours(args):
 
     # ---- extras: every other workload of the configurations, on one GPU only (the scaling runs
     # time the headline product alone) ----
-    spmv_extra = band_extra = csr_extra = cg_extra = cg_cluster = cg_large = None
+    spmv_extra = band_extra = csr_extra = cg_extra = cg_cluster = cg_large = cg_perm = None
     batch_extra = serve_extra = mg_extra = ir_extra = None
     if ws == 1 and not args.no_extras:
         cpu_on = not args.no_cpu_baseline
@@ -1005,6 +1043,7 @@ def run_ours(args):
         cg_extra = bench_cg_257(la, ctx, cpu=cpu_on)
         cg_cluster = bench_cg_cluster(ctx)
         cg_large = bench_cg_large(la, ctx, cpu=cpu_on) if not args.no_mg else None
+        cg_perm = bench_cg_permuted(la, ctx) if not args.no_mg else None
         batch_extra = None if args.no_batch else bench_batch(la, ctx, n_systems=args.batch_systems)
         # the serving stream before the multi-second 2049^2 solves (their heat lowers the clocks)
         serve_extra = None if args.no_serve else bench_serve(args.serve_requests, args.serve_prefix, args.serve_rate,
@@ -1039,7 +1078,7 @@ def run_ours(args):
             "clocks": clk.summary(),
             "extra": {"spmv": spmv_extra, "q1band_2049": band_extra, "csr_2049": csr_extra,
                       "cg_257": cg_extra,
-                      "cg_257_cluster": cg_cluster, "cg_large": cg_large,
+                      "cg_257_cluster": cg_cluster, "cg_large": cg_large, "cg_permuted_2049": cg_perm,
                       "mg_2049": mg_extra, "ir_2049": ir_extra, "batch_512": batch_extra, "serve": serve_extra},
         }
         print(json.dumps(line), flush=True)

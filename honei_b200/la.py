@@ -703,6 +703,8 @@ class CGSolver:
         if x.numel() != A.columns():
             raise VectorSizeDoesNotMatch(x.numel(), A.columns())
         ctx = ctx or default_context()
+        if isinstance(A, OrderedMatrixELL):
+            return CGSolver._value_ordered(A, b, x, max_iters, eps_relative, ctx)
         used = C.c_int64(0)
         d = C.c_double() if A.dtype == torch.float64 else C.c_float()
         fn = getattr(lib(), f"hb_cg_{_SUF[A.dtype]}")
@@ -710,6 +712,27 @@ class CGSolver:
                  eps_relative, C.byref(used), C.byref(d)), "CGSolver", ctx.handle)
         CGSolver.last_defect = d.value
         return used.value
+
+    @staticmethod
+    def _value_ordered(O: "OrderedMatrixELL", b, x, max_iters, eps_relative, ctx) -> int:
+        """CG on a matrix through its ordered copy (columns renumbered): b and x0 are permuted
+        into the copy's numbering once (hb_gather with order), the solve runs on the copy B =
+        P A P^T, whose gathers are local, and x is permuted back (hb_gather with pos: x[i] =
+        xw[pos[i]]).  The same CG; its dot products add the entries in the copy's order and
+        each row of B sums its slots in ascending new column, so the iterates agree with CG on A
+        to rounding (the parity bar of any reordered reduction)."""
+        if not O.columns_renumbered:
+            raise ValueError("CG through an ordered copy needs its columns renumbered (ordered(columns=True))")
+        n = O.rows()
+        suf = _SUF[O.dtype]
+        gather = getattr(lib(), f"hb_gather_{suf}")
+        bw = torch.empty(n, dtype=O.dtype, device=b.device)
+        xw = torch.empty(n, dtype=O.dtype, device=b.device)
+        check(gather(ctx.handle, n, O.order.data_ptr(), _vec(b, O.dtype, "b"), bw.data_ptr()), "hb_gather", ctx.handle)
+        check(gather(ctx.handle, n, O.order.data_ptr(), _vec(x, O.dtype, "x"), xw.data_ptr()), "hb_gather", ctx.handle)
+        used = CGSolver.value(O.B, None, bw, xw, max_iters, eps_relative, ctx=ctx)
+        check(gather(ctx.handle, n, O.pos.data_ptr(), xw.data_ptr(), x.data_ptr()), "hb_gather", ctx.handle)
+        return used
 
     @staticmethod
     def set_resident(enable: bool, ctx: Context | None = None) -> bool:
@@ -749,6 +772,8 @@ class CGSolverVAR:
         if x.numel() != A.columns():
             raise VectorSizeDoesNotMatch(x.numel(), A.columns())
         ctx = ctx or default_context()
+        if isinstance(A, OrderedMatrixELL):
+            return CGSolver._value_ordered(A, b, x, max_iters, eps_relative, ctx)
         used = C.c_int64(0)
         d = C.c_double() if A.dtype == torch.float64 else C.c_float()
         if isinstance(P, SparseMatrixELL):

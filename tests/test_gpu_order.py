@@ -184,3 +184,26 @@ def test_ordered_copy_edge_cases(hb, oracle):
     with pytest.raises(HBError) as e:
         R.cm_order()
     assert e.value.status == 2
+
+
+@pytest.mark.parametrize("M", [65, 257])
+def test_cg_through_ordered_copy_matches_oracle_on_the_permuted_system(hb, oracle, M):
+    """CGSolver on a randomly permuted Q1 system through its ordered copy (b and x permuted in
+    once, the solve in the copy's numbering, x permuted back) against the oracle's CG on the
+    permuted matrix: iterations within +-1, final true residual within 1e-10."""
+    Ap, _ = P.q1_poisson_permuted(M, 3)
+    b = oracle.spmv(Ap, P.uniform_vector(Ap.rows, 1))
+    x_o, u_o = oracle.cg(Ap, b, eps=1e-8, max_iters=20000)
+    O = hb.SparseMatrixELL.from_reference(Ap).ordered(columns=True)
+    x = torch.zeros(Ap.rows, dtype=torch.float64, device="cuda")
+    u = hb.CGSolver.value(O, None, torch.from_numpy(b).cuda(), x, 20000, 1e-8)
+    xg = x.cpu().numpy()
+    nb = np.linalg.norm(b)
+    rg = np.linalg.norm(oracle.defect(Ap, b, xg)) / nb
+    ro = np.linalg.norm(oracle.defect(Ap, b, x_o)) / nb
+    print(M, u, u_o, rg, ro)
+    assert abs(u - u_o) <= 1, (u, u_o)
+    assert abs(rg - ro) <= 1e-10, (rg, ro)
+    with pytest.raises(ValueError):
+        hb.CGSolver.value(hb.SparseMatrixELL.from_reference(Ap).ordered(columns=False), None,
+                          torch.from_numpy(b).cuda(), x, 10, 1e-8)
