@@ -48,10 +48,8 @@ struct BatchDesc {
 struct Smem {
     double red64[32];
     float red32[32];
-    double slot64[2];
-    float slot32[2];
-    double bc64;
-    float bc32;
+    double slot64[2 * 16];      // [phase][rank]: every CTA's partial, pushed by its owner
+    float slot32[2 * 16];
     long long item;
 };
 
@@ -61,9 +59,6 @@ template <> __device__ __forceinline__ float *red_of<float>(Smem &s) { return s.
 template <typename T> __device__ __forceinline__ T *slot_of(Smem &s);
 template <> __device__ __forceinline__ double *slot_of<double>(Smem &s) { return s.slot64; }
 template <> __device__ __forceinline__ float *slot_of<float>(Smem &s) { return s.slot32; }
-template <typename T> __device__ __forceinline__ T *bc_of(Smem &s);
-template <> __device__ __forceinline__ double *bc_of<double>(Smem &s) { return &s.bc64; }
-template <> __device__ __forceinline__ float *bc_of<float>(Smem &s) { return &s.bc32; }
 
 __device__ __forceinline__ double dsqrt(double v) { return __dsqrt_rn(v); }
 __device__ __forceinline__ float dsqrt(float v) { return __fsqrt_rn(v); }
@@ -72,24 +67,26 @@ template <> __device__ __forceinline__ double eps_mach<double>() { return DBL_EP
 template <> __device__ __forceinline__ float eps_mach<float>() { return FLT_EPSILON; }
 
 // Cluster-wide sum in a fixed order (thread partials -> CTA tree -> CTA partials in rank
-// order), identical in every CTA.  The two slots alternate so a slot is never rewritten
-// before every CTA has read it (the next reduction's barrier separates them).
+// order), identical in every CTA.  Each CTA pushes its total into every CTA's slot for its
+// rank (DSMEM stores before the cluster barrier), so after the barrier each CTA sums local
+// shared memory.  The two slot sets alternate: a set is rewritten only two barriers later,
+// after every CTA has read it.
 template <typename T> __device__ T cluster_total(T v, Smem &s, int &phase)
 {
     v = hbd::block_sum(v, red_of<T>(s));
-    T *slot = slot_of<T>(s);
-    if (threadIdx.x == 0) slot[phase] = v;
     cgx::cluster_group cl = cgx::this_cluster();
-    cl.sync();
-    if (threadIdx.x == 0) {
-        T t = T(0);
-        const unsigned nb = cl.num_blocks();
-        for (unsigned r = 0; r < nb; ++r) t = hbd::add(t, *cl.map_shared_rank(slot + phase, r));
-        *bc_of<T>(s) = t;
+    const unsigned nb = cl.num_blocks();
+    T *slot = slot_of<T>(s) + 16 * phase;
+    if (threadIdx.x < 32) {
+        // warp 0: the CTA total to every lane; lane q stores it into CTA q's slot of this rank
+        v = __shfl_sync(0xffffffffu, v, 0);
+        if (threadIdx.x < nb) *cl.map_shared_rank(slot + cl.block_rank(), threadIdx.x) = v;
     }
-    __syncthreads();
+    cl.sync();
+    T t = T(0);
+    for (unsigned r = 0; r < nb; ++r) t = hbd::add(t, slot[r]);
     phase ^= 1;
-    return *bc_of<T>(s);
+    return t;
 }
 
 struct Range {
