@@ -15,11 +15,11 @@ honei/math/mg.hh:1098-1126, honei/math/ir.hh:30-78) on tags::CPU::MultiCore::SSE
 cores (tests/test_oracle_pin.py pins that tag's iteration counts to tags::CPU's); the batch
 systems go through the plain-C oracle, one host thread per system.
 
-Bar (north star): iterations / cycles / outer steps within +-1 of the reference's, and the
+Bar: iterations / cycles / outer steps within +-1 of the reference's, and the
 final true relative residual ||b - A x|| / ||b|| within 1e-10 of the reference's.  Where the
 counts differ by one, the residuals differ by one step's contraction, which is stated and
 checked per case (FP32 solves: the FP32 bar of the test).  The batch's FP64 CG is held to the
-reference's own spread between two of its tags on the same systems (the test says why).
+reference's own spread between its tags on the same systems (the test says why).
 """
 import os
 from concurrent.futures import ThreadPoolExecutor
