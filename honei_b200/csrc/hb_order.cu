@@ -167,6 +167,186 @@ cm_order_kernel(int64_t n, int64_t ld, int K, const int32_t *__restrict__ Aj, in
     }
 }
 
+// The same Cuthill-McKee order on the whole GPU (cooperative launch, every block resident):
+// each level's (row, slot) items are split into one contiguous chunk per block; three
+// grid-wide exchanges per level separate the claims (atomicMin on the item index, as above),
+// the per-block winner counts and the placement, which scans each chunk in item order and
+// offsets it by the counts of the chunks before it -- so the order is item for item the one the
+// single-block kernel produces.  Unreached rows follow in ascending order (a fourth pass of the
+// same kind over the rows).  Every exchange is bounded (CountExchange); on a timeout the blocks
+// return and the status word holds HB_DEV_TIMEOUT.
+constexpr int ORDG_THREADS = 512;
+constexpr int64_t CM_GRID_MIN_ROWS = 4096;     // smaller matrices: the single-block kernel
+constexpr int ORDG_ITEMS = 4;
+constexpr int64_t ORDG_TILE = (int64_t)ORDG_THREADS * ORDG_ITEMS;
+
+struct OrdGrid {
+    int64_t n, ld;
+    int K;
+    const int32_t *Aj;
+    int32_t *order, *pos;
+    unsigned long long *key, *best;
+    int64_t *cnt, *info;
+    hbd::CountExchange X;
+};
+
+// winner of item i of the level starting at s: its column c, or -1
+__device__ __forceinline__ int32_t ord_item(const OrdGrid &Q, int64_t s, int64_t i, bool need_key)
+{
+    const int64_t k = i / Q.K;
+    const int slot = (int)(i - k * Q.K);
+    const int32_t v = __ldcg(Q.order + s + k);
+    const int32_t c = __ldg(Q.Aj + (int64_t)slot * Q.ld + v);
+    if (c < 0 || c == v || __ldcg(Q.pos + c) >= 0) return -1;
+    if (need_key && __ldcg(Q.key + c) != (unsigned long long)i) return -1;
+    return c;
+}
+
+__global__ void __launch_bounds__(ORDG_THREADS) cm_order_grid_kernel(OrdGrid Q)
+{
+    __shared__ int64_t s_scan[33];
+    __shared__ int64_t s_off[2];
+    __shared__ unsigned long long s_best;
+    __shared__ int s_flag;
+    const int tid = threadIdx.x;
+    const unsigned G = gridDim.x;
+    const int64_t b = blockIdx.x;
+    const int64_t gstride = (int64_t)G * blockDim.x, gtid = b * blockDim.x + tid;
+    const int64_t n = Q.n;
+    unsigned e = 0;
+    for (int64_t r = gtid; r < n; r += gstride) {
+        Q.pos[r] = -1;
+        Q.key[r] = ORD_NONE;
+    }
+    if (tid == 0) s_best = ORD_NONE;
+    __syncthreads();
+    unsigned long long best = ORD_NONE;
+    for (int64_t r = gtid; r < n; r += gstride) {
+        unsigned long long deg = 0;
+        for (int k = 0; k < Q.K; ++k) {
+            const int32_t c = __ldg(Q.Aj + (int64_t)k * Q.ld + r);
+            if (c >= 0 && c != r) ++deg;
+        }
+        if (deg) best = min(best, (deg << 32) | (unsigned long long)r);
+    }
+    atomicMin(&s_best, best);
+    __syncthreads();
+    if (tid == 0 && s_best != ORD_NONE) atomicMin(Q.best, s_best);
+    if (!Q.X.arrive(e++, G, &s_flag)) return;
+    const unsigned long long start = __ldcg(Q.best);
+    int64_t lo = 0, hi = 0, levels = 0;
+    if (start != ORD_NONE) {
+        const int32_t r0 = (int32_t)(start & 0xffffffffull);
+        if (gtid == 0) { Q.order[0] = r0; Q.pos[r0] = 0; }
+        hi = 1;
+    }
+    if (!Q.X.arrive(e++, G, &s_flag)) return;
+    while (hi > lo) {
+        const int64_t items = (hi - lo) * Q.K;
+        const int64_t cs = (items + G - 1) / G;
+        const int64_t i_lo = min(items, b * cs), i_hi = min(items, i_lo + cs);
+        // claims
+        for (int64_t i = i_lo + tid; i < i_hi; i += blockDim.x) {
+            const int32_t c = ord_item(Q, lo, i, false);
+            if (c >= 0) atomicMin(Q.key + c, (unsigned long long)i);
+        }
+        if (!Q.X.arrive(e++, G, &s_flag)) return;
+        // winners of this block's chunk
+        int64_t mine = 0;
+        for (int64_t i = i_lo + tid; i < i_hi; i += blockDim.x) mine += ord_item(Q, lo, i, true) >= 0;
+        int64_t total;
+        block_exclusive_scan(mine, s_scan, &total);
+        if (tid == 0) __stcg(Q.cnt + b, total);
+        if (!Q.X.arrive(e++, G, &s_flag)) return;
+        // offsets: the winners of the chunks before this one, and the level's total
+        if (tid == 0) {
+            int64_t before = 0, all = 0;
+            for (unsigned q = 0; q < G; ++q) {
+                const int64_t c = __ldcg(Q.cnt + q);
+                if (q < b) before += c;
+                all += c;
+            }
+            s_off[0] = before;
+            s_off[1] = all;
+        }
+        __syncthreads();
+        int64_t at0 = hi + s_off[0];
+        const int64_t all = s_off[1];
+        for (int64_t t0 = i_lo; t0 < i_hi; t0 += ORDG_TILE) {
+            int32_t cs_[ORDG_ITEMS];
+            int cnt = 0;
+#pragma unroll
+            for (int j = 0; j < ORDG_ITEMS; ++j) {
+                const int64_t i = t0 + (int64_t)tid * ORDG_ITEMS + j;
+                cs_[j] = i < i_hi ? ord_item(Q, lo, i, true) : -1;
+                cnt += cs_[j] >= 0;
+            }
+            int64_t tile_total;
+            int64_t at = at0 + block_exclusive_scan(cnt, s_scan, &tile_total);
+#pragma unroll
+            for (int j = 0; j < ORDG_ITEMS; ++j) {
+                if (cs_[j] >= 0) {
+                    Q.order[at] = cs_[j];
+                    Q.pos[cs_[j]] = (int32_t)at;
+                    ++at;
+                }
+            }
+            at0 += tile_total;
+            __syncthreads();
+        }
+        if (!Q.X.arrive(e++, G, &s_flag)) return;
+        lo = hi;
+        hi += all;
+        ++levels;
+    }
+    // rows never reached, ascending: one contiguous chunk of rows per block
+    const int64_t reached = hi;
+    const int64_t rs = (n + G - 1) / G;
+    const int64_t r_lo = min(n, b * rs), r_hi = min(n, r_lo + rs);
+    int64_t mine = 0;
+    for (int64_t r = r_lo + tid; r < r_hi; r += blockDim.x) mine += __ldcg(Q.pos + r) < 0;
+    int64_t total;
+    block_exclusive_scan(mine, s_scan, &total);
+    if (tid == 0) __stcg(Q.cnt + b, total);
+    if (!Q.X.arrive(e++, G, &s_flag)) return;
+    if (tid == 0) {
+        int64_t before = 0;
+        for (unsigned q = 0; q < b; ++q) before += __ldcg(Q.cnt + q);
+        s_off[0] = before;
+    }
+    __syncthreads();
+    int64_t at0 = reached + s_off[0];
+    for (int64_t t0 = r_lo; t0 < r_hi; t0 += ORDG_TILE) {
+        int cnt = 0;
+        bool un[ORDG_ITEMS];
+#pragma unroll
+        for (int j = 0; j < ORDG_ITEMS; ++j) {
+            const int64_t r = t0 + (int64_t)tid * ORDG_ITEMS + j;
+            un[j] = r < r_hi && __ldcg(Q.pos + r) < 0;
+            cnt += un[j];
+        }
+        int64_t tile_total;
+        int64_t at = at0 + block_exclusive_scan(cnt, s_scan, &tile_total);
+        __syncthreads();   // every thread read pos for its rows before any placement below
+#pragma unroll
+        for (int j = 0; j < ORDG_ITEMS; ++j) {
+            if (un[j]) {
+                const int64_t r = t0 + (int64_t)tid * ORDG_ITEMS + j;
+                Q.order[at] = (int32_t)r;
+                Q.pos[r] = (int32_t)at;
+                ++at;
+            }
+        }
+        at0 += tile_total;
+        __syncthreads();
+    }
+    if (gtid == 0) {
+        Q.info[0] = levels;
+        Q.info[1] = reached;
+        Q.info[2] = start == ORD_NONE ? -1 : (int64_t)(start & 0xffffffffull);
+    }
+}
+
 // max |pos(c) - pos(r)| over the stored entries (identity numbering when pos is null).
 __global__ void ell_bandwidth_kernel(int64_t rows, int64_t ld, int K, const int32_t *__restrict__ Aj,
                                      const int32_t *__restrict__ pos, unsigned long long *out)
@@ -491,20 +671,58 @@ int hb_ell_cm_order(hb_context *ctx, const hb_ell *A, int32_t *order, int32_t *p
         if (info) info[0] = info[1] = 0, info[2] = -1;
         return HB_OK;
     }
-    // workspace: key (u64) and, without a caller array, pos (int32)
+    // workspace: key (u64), without a caller array pos (int32), and for the grid form the start
+    // candidate (u64) and one count per block (int64)
     const size_t key_bytes = (size_t)n * 8;
     const size_t pos_bytes = pos ? 0 : hb_round_up(n * 4, 256);
-    int st = hb_ensure_work(ctx, key_bytes + pos_bytes);
+    int grid = 0;
+    if (n >= CM_GRID_MIN_ROWS) {
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, cm_order_grid_kernel, ORDG_THREADS, 0) != cudaSuccess)
+            cudaGetLastError();
+        grid = std::min(std::max(occ, 0), 2) * ctx->num_sms;
+    }
+    const size_t grid_bytes = grid ? 256 + hb_round_up((int64_t)grid * 8, 256) : 0;
+    int st = hb_ensure_work(ctx, key_bytes + pos_bytes + grid_bytes);
     if (st) return st;
     unsigned long long *key = (unsigned long long *)ctx->work;
     int32_t *p = pos ? pos : (int32_t *)((char *)ctx->work + key_bytes);
     int64_t *dinfo = (int64_t *)hb_scalars(ctx);
-    cm_order_kernel<<<1, ORD_THREADS, 0, ctx->stream>>>(n, A->ld, (int)A->K, A->Aj, order, p, key, dinfo);
-    st = hb_check_launch(ctx, "cm_order_kernel");
+    unsigned *bar = hb_bar(ctx);
+    if (grid) {
+        OrdGrid Q;
+        Q.n = n;
+        Q.ld = A->ld;
+        Q.K = (int)A->K;
+        Q.Aj = A->Aj;
+        Q.order = order;
+        Q.pos = p;
+        Q.key = key;
+        Q.best = (unsigned long long *)((char *)ctx->work + key_bytes + pos_bytes);
+        Q.cnt = (int64_t *)((char *)Q.best + 256);
+        Q.info = dinfo;
+        Q.X.count = bar;
+        Q.X.status = (int *)(bar + 2);
+        HB_CUDA_TRY(ctx, cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), ctx->stream));
+        HB_CUDA_TRY(ctx, cudaMemsetAsync(Q.best, 0xff, sizeof(unsigned long long), ctx->stream));
+        void *args[] = {&Q};
+        HB_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void *)cm_order_grid_kernel, dim3(grid), dim3(ORDG_THREADS),
+                                                     args, 0, ctx->stream));
+        st = hb_check_launch(ctx, "cm_order_grid_kernel");
+    } else {
+        cm_order_kernel<<<1, ORD_THREADS, 0, ctx->stream>>>(n, A->ld, (int)A->K, A->Aj, order, p, key, dinfo);
+        st = hb_check_launch(ctx, "cm_order_kernel");
+    }
     if (st) return st;
     int64_t *h = (int64_t *)ctx->pinned;
     HB_CUDA_TRY(ctx, cudaMemcpyAsync(h, dinfo, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    HB_CUDA_TRY(ctx, cudaMemcpyAsync(h + 3, bar + 2, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     HB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (grid) {
+        const int dev_status = *(const int *)(h + 3);
+        HB_CUDA_TRY(ctx, cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned), ctx->stream));
+        if (dev_status == HB_DEV_TIMEOUT) return HB_ERR_TIMEOUT;
+    }
     if (info) { info[0] = h[0]; info[1] = h[1]; info[2] = h[2]; }
     return HB_OK;
 }

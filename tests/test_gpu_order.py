@@ -70,6 +70,9 @@ CASES = [
     ("q1_65_spd_varcoef", lambda: P.q1_poisson(65, P.log_uniform_coef(65, 1e-1, 1e1, 3), symmetric=True)),
     ("q1_17_threads3", lambda: P.ell_from_csr(289, 289, *P.q1_poisson_csr(17), threads=3)),
     ("random_pattern_500", lambda: random_pattern(500, 11)),
+    # 4096 rows and more take the grid-wide kernel
+    ("q1_129_permuted", lambda: P.q1_poisson_permuted(129, 6)[0]),
+    ("random_pattern_6000", lambda: random_pattern(6000, 12)),
 ]
 
 
