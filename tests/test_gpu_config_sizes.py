@@ -87,6 +87,44 @@ def test_cg_f64_at_size_matches_reference(hb, oracle, ref, M):
     assert np.linalg.norm(x_g - x_r) <= 1e-5 * np.linalg.norm(x_r)
 
 
+def test_cg_f64_permuted_2049_matches_reference(hb, oracle, ref):
+    """Config 2's CG on the randomly permuted 2049^2 matrix, against the reference's CG on the
+    same permuted matrix: the GPU as given (its product on the permuted ELL) and through the
+    Cuthill-McKee ordered copy (CGSolver on an OrderedMatrixELL), each within +-1 iteration and
+    1e-10 of the reference's final true residual."""
+    Ap, _ = P.q1_poisson_permuted(2049, 5)
+    b = oracle.spmv(Ap, P.uniform_vector(Ap.rows, 1))
+    x_r, u_r, _ = ref.cg(Ap, b, eps=1e-8, max_iters=100000, tag="mc-sse")
+    rr = relres(oracle, Ap, b, x_r)
+    Ad = hb.SparseMatrixELL.from_reference(Ap)
+    for name, A in (("as given", Ad), ("ordered copy", Ad.ordered(columns=True))):
+        x = torch.zeros(Ap.rows, dtype=torch.float64, device="cuda")
+        u_g = hb.CGSolver.value(A, None, dev(b), x, 100000, 1e-8)
+        rg = relres(oracle, Ap, b, host(x))
+        print(f"CG permuted 2049^2 {name}: GPU {u_g} iterations, relres {rg:.6e}; reference {u_r}, {rr:.6e}")
+        assert abs(u_g - u_r) <= 1, (name, u_g, u_r)
+        tol = 1e-10 if u_g == u_r else 2 * (1 - contraction(u_r, rr)) * rr + 1e-10
+        assert abs(rg - rr) <= tol, (name, rg, rr)
+
+
+def test_cg_f32_1025_matches_reference(hb, oracle, ref):
+    """Config 2's CG in FP32 at 1025^2 (to 1e-5, where FP32 CG still converges steadily) against
+    the reference's FP32 CGSolver: iterations within +-1, the final true residual (in FP64 from
+    the FP32 iterates) within 2 % of the reference's."""
+    A = P.q1_poisson(1025).astype(np.float32)
+    b = oracle.spmv(A, P.uniform_vector(A.rows, 1).astype(np.float32))
+    x_r, u_r, _ = ref.cg(A, b, eps=1e-5, max_iters=100000, tag="mc-sse")
+    Ad = hb.SparseMatrixELL.from_reference(A)
+    x = torch.zeros(A.rows, dtype=torch.float32, device="cuda")
+    u_g = hb.CGSolver.value(Ad, None, dev(b), x, 100000, 1e-5)
+    A64, b64 = A.astype(np.float64), b.astype(np.float64)
+    rg = relres(oracle, A64, b64, host(x).astype(np.float64))
+    rr = relres(oracle, A64, b64, x_r.astype(np.float64))
+    print(f"CG FP32 1025^2: GPU {u_g} iterations, relres {rg:.6e}; reference {u_r}, {rr:.6e}")
+    assert abs(u_g - u_r) <= 1, (u_g, u_r)
+    assert abs(rg - rr) <= 0.02 * rr, (rg, rr)
+
+
 @pytest.fixture(scope="module")
 def h2049():
     return P.mg_hierarchy(2049)
