@@ -114,7 +114,10 @@ int hb_ell_cast_f64_f32(hb_context *ctx, const hb_ell *src, hb_ell *dst);
  * never reached follow in ascending order.  order: device int32[rows], order[k] = the row at
  * position k; pos: device int32[rows] or NULL, pos[order[k]] = k.  info (host int64[3], may be
  * NULL): levels, rows reached, start row.  Uses the context workspace (8 bytes per row, 12
- * without pos) and synchronises the stream.  Deterministic. */
+ * without pos, plus 8 bytes per block of the grid-wide form) and synchronises the stream.
+ * Deterministic: from 4096 rows on the whole GPU computes it (one cooperative launch, three
+ * bounded grid-wide exchanges per level; HB_ERR_TIMEOUT if one gives up), the same order as the
+ * one-block form below that size. */
 int hb_ell_cm_order(hb_context *ctx, const hb_ell *A, int32_t *order, int32_t *pos, int64_t *info);
 /* max |pos[c] - pos[r]| over A's stored entries (r, c); pos NULL = A's own numbering.
  * Synchronises the stream. */
