@@ -272,7 +272,7 @@ def bench_spmv_variants(la, ctx, M=M_SPMV, seed=5, cpu=True, reps=50):
     as given and through its Cuthill-McKee ordered copy (SparseMatrixELL.ordered: rows stored
     in the locality order, columns renumbered and packed as 16-bit offsets, x permuted into a
     work vector inside the timed product, y scattered back -- bit-identical to the product on
-    the permuted matrix; the unpacked ranked form beside it); the
+    the permuted matrix; the sorted, ranked form beside it); the
     1025^2 FP64 product with L2 flushed between products (its 130 MB would otherwise stay
     partly in L2).  GB/s are the algorithmic bytes of the product on the given matrix
     (nnz*(s+4) + 2*n*s)."""
@@ -313,11 +313,12 @@ def bench_spmv_variants(la, ctx, M=M_SPMV, seed=5, cpu=True, reps=50):
         r["same_y_as_permuted"] = bool(torch.equal(y, y0))
         r["ordering_ms"] = round(t_order * 1e3, 1)
         r["levels"], r["bandwidth_before"], r["bandwidth_after"] = int(B.info[0]), Ad.bandwidth(), B.B.bandwidth()
-        r["form"] = "packed (16-bit column offsets, 32-bit ranks)" if B.Bd is not None else "ranked"
+        r["form"] = "packed (16-bit column offsets, slots in their order)" if B.Bd is not None else "ranked"
         # the bytes this form moves: x gathered (order, x, xw) and the product's own arrays
-        # (every slot of the K x ld value and offset arrays, rank words, order, xw, y)
+        # (every slot of the K x ld value and index arrays, rank words for the ranked form, order,
+        # xw, y)
         idx = 2 if B.Bd is not None else 4
-        rk = 4 if B.Bd is not None else 8
+        rk = 0 if B.Bd is not None else 8
         own = (4 + 2 * s) * n + B.B.K * B.B.ld * (s + idx) + (rk + 4 + 2 * s) * n
         r["own_bytes"] = own
         r["own_gbs"] = round(own / (r["us"] * 1e3), 1)

@@ -76,9 +76,9 @@ SIGNATURES = {
     "hb_spmv_ranked_f32": (i32, [vp, P_ell, vp, vp, vp, vp]),
     "hb_spmv_rows_f64": (i32, [vp, P_ell, vp, vp, vp]),
     "hb_spmv_rows_f32": (i32, [vp, P_ell, vp, vp, vp]),
-    "hb_ell_pack_ordered": (i32, [vp, P_ell, vp, vp, vp]),
-    "hb_spmv_packed_f64": (i32, [vp, P_ell, vp, vp, vp, vp, vp]),
-    "hb_spmv_packed_f32": (i32, [vp, P_ell, vp, vp, vp, vp, vp]),
+    "hb_ell_pack_offsets": (i32, [vp, P_ell, vp]),
+    "hb_spmv_packed_f64": (i32, [vp, P_ell, vp, vp, vp, vp]),
+    "hb_spmv_packed_f32": (i32, [vp, P_ell, vp, vp, vp, vp]),
     "hb_gather_f64": (i32, [vp, i64, vp, vp, vp]),
     "hb_gather_f32": (i32, [vp, i64, vp, vp, vp]),
     "hb_spai2_f64": (i32, [vp, P_ell, P_ell]),

@@ -503,16 +503,14 @@ __global__ void gather_kernel(int64_t n, const int32_t *__restrict__ order, cons
         xw[k] = __ldg(x + __ldg(order + k));
 }
 
-// The packed form of a sorted copy (K <= 9, offsets within +-32767): slot k of row r stores
-// its new column as the 16-bit offset c - r (PACK_NONE for padding), and the ranks keep their
-// first eight 4-bit fields (32 bits).  A ninth slot is valid only when all nine are (valid
-// slots come first), and then its rank is the one of 0..8 left over: 36 minus the other eight.
+// The packed form of a renumbered copy (hb_ell_permute with pos: rows in the locality order,
+// columns renumbered, each row's slots in their own order): slot k of row r keeps its column as
+// the 16-bit offset c - r (PACK_NONE for padding).  Bandwidths within +-32767 only.
 constexpr int16_t PACK_NONE = INT16_MIN;
 constexpr int PACKED_THREADS = 256;
 
 __global__ void ell_pack_kernel(int64_t rows, int64_t ld, int K, const int32_t *__restrict__ Bj,
-                                const unsigned long long *__restrict__ ranks, int16_t *__restrict__ Bd,
-                                uint32_t *__restrict__ ranks32, unsigned long long *__restrict__ overflow)
+                                int16_t *__restrict__ Bd, unsigned long long *__restrict__ overflow)
 {
     for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < (int64_t)K * ld;
          idx += (int64_t)gridDim.x * blockDim.x) {
@@ -525,27 +523,21 @@ __global__ void ell_pack_kernel(int64_t rows, int64_t ld, int K, const int32_t *
                 if (off < -32767 || off > 32767) atomicAdd(overflow, 1ull);
                 else d = (int16_t)off;
             }
-            if (k == 0) ranks32[r] = (uint32_t)(ranks[r] & 0xffffffffull);
         }
         Bd[idx] = d;
     }
 }
 
-// y[order[r]] = B's row r summed in rank order, from the packed form: one row per thread, in
-// two phases -- every streaming load of the row (offsets, values, rank word, order) issued
-// first, then every gather of x -- so each thread keeps all its memory requests in flight at
-// once; the products are parked in shared memory at their ranks as in ell_spmv_ranked_kernel.
-// Blocks per SM: 4 in FP64 (64 registers hold the nine values and gathers), 8 in FP32.
-template <typename T> constexpr int packed_min_blocks() { return sizeof(T) == 8 ? 4 : 8; }
-
+// y[order[r]] = B's row r from the packed form, summed in slot order (the reference's order: the
+// copy keeps each row's slots as they were): one row per thread, every streaming load of the
+// row (offsets, values, order) issued before every gather of x, 8 blocks of 256 per SM (32
+// registers).
 template <typename T, int KT>
-__global__ void __launch_bounds__(PACKED_THREADS, packed_min_blocks<T>())
+__global__ void __launch_bounds__(PACKED_THREADS, 8)
 ell_spmv_packed_kernel(int64_t rows, int64_t ld, int K, const int16_t *__restrict__ Bd, const T *__restrict__ Ax,
-                       const uint32_t *__restrict__ ranks, const T *__restrict__ x,
-                       const int32_t *__restrict__ order, T *__restrict__ y)
+                       const T *__restrict__ x, const int32_t *__restrict__ order, T *__restrict__ y)
 {
     constexpr int KS = KT > 0 ? KT : 9;
-    __shared__ T park[KS * PACKED_THREADS];
     const int K_ = KT > 0 ? KT : K;
     const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (r >= rows) return;
@@ -561,44 +553,34 @@ ell_spmv_packed_kernel(int64_t rows, int64_t ld, int K, const int16_t *__restric
             a[k] = __ldcs(Ax + (int64_t)k * ld + r);
         }
     }
-    const uint32_t rk = __ldg(ranks + r);
     const int32_t o = __ldg(order + r);
     T v[KS];
 #pragma unroll
     for (int k = 0; k < KS; ++k) v[k] = c[k] >= 0 ? __ldg(x + c[k]) : T(0);
-    int cnt = 0, used = 0;
-#pragma unroll
-    for (int k = 0; k < KS; ++k) {
-        if (c[k] >= 0) {
-            const int at = k < 8 ? (int)((rk >> (4 * k)) & 15u) : 36 - used;
-            used += at;
-            park[at * PACKED_THREADS + threadIdx.x] = hbd::mul(a[k], v[k]);
-            ++cnt;
-        }
-    }
     T sum = T(0);
-    for (int k = 0; k < cnt; ++k) sum = hbd::add(sum, park[k * PACKED_THREADS + threadIdx.x]);
+#pragma unroll
+    for (int k = 0; k < KS; ++k)
+        if (c[k] >= 0) sum = hbd::add(sum, hbd::mul(a[k], v[k]));
     y[o] = sum;
 }
 
 template <typename T>
 int spmv_packed_impl(hb_context *ctx, const hb_ell *B, int dtype, const int16_t *Bd, const int32_t *order,
-                     const uint32_t *ranks, const T *x, T *y)
+                     const T *x, T *y)
 {
     if (!ctx) return HB_ERR_INVALID;
     int st = hb_check_ell(B, dtype);
     if (st) return st;
     if (B->K > 9) return HB_ERR_UNSUPPORTED;
     if (B->rows == 0) return HB_OK;
-    if (!Bd || !order || !ranks || !x || !y) return HB_ERR_INVALID;
+    if (!Bd || !order || !x || !y) return HB_ERR_INVALID;
     const unsigned blocks = (unsigned)((B->rows + PACKED_THREADS - 1) / PACKED_THREADS);
     const T *Bx = (const T *)B->Ax;
     if (B->K == 9)
-        ell_spmv_packed_kernel<T, 9><<<blocks, PACKED_THREADS, 0, ctx->stream>>>(B->rows, B->ld, 9, Bd, Bx, ranks, x,
-                                                                                 order, y);
+        ell_spmv_packed_kernel<T, 9><<<blocks, PACKED_THREADS, 0, ctx->stream>>>(B->rows, B->ld, 9, Bd, Bx, x, order, y);
     else
-        ell_spmv_packed_kernel<T, 0><<<blocks, PACKED_THREADS, 0, ctx->stream>>>(B->rows, B->ld, (int)B->K, Bd, Bx,
-                                                                                 ranks, x, order, y);
+        ell_spmv_packed_kernel<T, 0><<<blocks, PACKED_THREADS, 0, ctx->stream>>>(B->rows, B->ld, (int)B->K, Bd, Bx, x,
+                                                                                 order, y);
     return hb_check_launch(ctx, "ell_spmv_packed_kernel");
 }
 
@@ -823,10 +805,10 @@ int hb_spmv_rows_f32(hb_context *ctx, const hb_ell *B, const int32_t *order, con
     return spmv_rows_impl<float>(ctx, B, HB_F32, order, x, y);
 }
 
-int hb_ell_pack_ordered(hb_context *ctx, const hb_ell *B, const uint64_t *ranks, int16_t *Bd, uint32_t *ranks32)
+int hb_ell_pack_offsets(hb_context *ctx, const hb_ell *B, int16_t *Bd)
 {
-    HB_RANGE("hb_ell_pack_ordered");
-    if (!ctx || !ranks || !Bd || !ranks32) return HB_ERR_INVALID;
+    HB_RANGE("hb_ell_pack_offsets");
+    if (!ctx || !Bd) return HB_ERR_INVALID;
     int st = hb_check_ell(B, B ? B->dtype : 0);
     if (st) return st;
     if (B->K > 9) return HB_ERR_UNSUPPORTED;
@@ -835,8 +817,7 @@ int hb_ell_pack_ordered(hb_context *ctx, const hb_ell *B, const uint64_t *ranks,
     HB_CUDA_TRY(ctx, cudaMemsetAsync(d, 0, sizeof(*d), ctx->stream));
     const int64_t total = B->K * B->ld;
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 32));
-    ell_pack_kernel<<<blocks, 256, 0, ctx->stream>>>(B->rows, B->ld, (int)B->K, B->Aj,
-                                                     (const unsigned long long *)ranks, Bd, ranks32, d);
+    ell_pack_kernel<<<blocks, 256, 0, ctx->stream>>>(B->rows, B->ld, (int)B->K, B->Aj, Bd, d);
     st = hb_check_launch(ctx, "ell_pack_kernel");
     if (st) return st;
     unsigned long long *h = (unsigned long long *)ctx->pinned;
@@ -845,18 +826,18 @@ int hb_ell_pack_ordered(hb_context *ctx, const hb_ell *B, const uint64_t *ranks,
     return *h ? HB_ERR_UNSUPPORTED : HB_OK;
 }
 
-int hb_spmv_packed_f64(hb_context *ctx, const hb_ell *B, const int16_t *Bd, const int32_t *order,
-                       const uint32_t *ranks, const double *x, double *y)
+int hb_spmv_packed_f64(hb_context *ctx, const hb_ell *B, const int16_t *Bd, const int32_t *order, const double *x,
+                       double *y)
 {
     HB_RANGE("hb_spmv_packed_f64");
-    return spmv_packed_impl<double>(ctx, B, HB_F64, Bd, order, ranks, x, y);
+    return spmv_packed_impl<double>(ctx, B, HB_F64, Bd, order, x, y);
 }
 
-int hb_spmv_packed_f32(hb_context *ctx, const hb_ell *B, const int16_t *Bd, const int32_t *order,
-                       const uint32_t *ranks, const float *x, float *y)
+int hb_spmv_packed_f32(hb_context *ctx, const hb_ell *B, const int16_t *Bd, const int32_t *order, const float *x,
+                       float *y)
 {
     HB_RANGE("hb_spmv_packed_f32");
-    return spmv_packed_impl<float>(ctx, B, HB_F32, Bd, order, ranks, x, y);
+    return spmv_packed_impl<float>(ctx, B, HB_F32, Bd, order, x, y);
 }
 
 int hb_gather_f64(hb_context *ctx, int64_t n, const int32_t *order, const double *x, double *xw)

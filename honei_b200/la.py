@@ -284,50 +284,53 @@ class SparseMatrixELL:
     def ordered(self, columns: bool = True, packed: bool = True, ctx: Context | None = None) -> "OrderedMatrixELL":
         """A copy stored in the Cuthill-McKee locality order, for products with a badly numbered
         matrix (e.g. a randomly permuted grid).  Product.value on the copy gives y = A x bit for
-        bit.  columns=True renumbers the columns too and stores each row's slots by new column
-        with their summation ranks (local gathers; x is permuted into a work vector first);
-        packed=True then also keeps the columns as 16-bit offsets from the row and the ranks in
-        32 bits when K <= 9 and the reordered bandwidth allows (hb_ell_pack_ordered), and the
-        product reads those.  columns=False keeps A's columns (no work vector; gathers stay
-        scattered, rows that share columns run together)."""
+        bit.  columns=True renumbers the columns too (local gathers; x is permuted into a work
+        vector first): packed=True keeps each row's slots in their order with the columns as
+        16-bit offsets from the row (hb_ell_pack_offsets; K <= 9 and a reordered bandwidth within
+        +-32767), otherwise -- or where that does not fit -- the slots are sorted by new column
+        with their summation ranks (hb_ell_permute_sorted).  columns=False keeps A's columns (no
+        work vector; gathers stay scattered, rows that share columns run together)."""
         ctx = ctx or default_context()
         order, pos, info = self.cm_order(ctx)
         Aj = torch.empty_like(self.Aj)
         Ax = torch.empty_like(self.Ax)
         B = HbEll(self._rows, self._cols, self.K, self.ld, Aj.data_ptr(), Ax.data_ptr(), _DT[self.dtype], 0)
-        ranks = None
-        if columns:
-            ranks = torch.empty(max(self._rows, 1), dtype=torch.int64, device=self.Aj.device)
-            check(lib().hb_ell_permute_sorted(ctx.handle, C.byref(self._s), order.data_ptr(), pos.data_ptr(),
-                                              C.byref(B), ranks.data_ptr()), "hb_ell_permute_sorted", ctx.handle)
-        else:
+        if not columns:
             check(lib().hb_ell_permute(ctx.handle, C.byref(self._s), order.data_ptr(), None, C.byref(B)),
                   "hb_ell_permute", ctx.handle)
-        O = OrderedMatrixELL(SparseMatrixELL(self._rows, self._cols, self.K, self.ld, Aj, Ax), order, pos,
-                             columns, info, ranks)
-        if columns and packed and self.K <= 9 and self._rows > 0:
+            return OrderedMatrixELL(SparseMatrixELL(self._rows, self._cols, self.K, self.ld, Aj, Ax), order, pos,
+                                    False, info)
+        if packed and self.K <= 9 and self._rows > 0:
+            check(lib().hb_ell_permute(ctx.handle, C.byref(self._s), order.data_ptr(), pos.data_ptr(), C.byref(B)),
+                  "hb_ell_permute", ctx.handle)
+            O = OrderedMatrixELL(SparseMatrixELL(self._rows, self._cols, self.K, self.ld, Aj, Ax), order, pos,
+                                 True, info)
             Bd = torch.empty((self.K, self.ld), dtype=torch.int16, device=self.Aj.device)
-            r32 = torch.empty(self._rows, dtype=torch.int32, device=self.Aj.device)
-            st = lib().hb_ell_pack_ordered(ctx.handle, C.byref(O.B.struct), ranks.data_ptr(), Bd.data_ptr(),
-                                           r32.data_ptr())
+            st = lib().hb_ell_pack_offsets(ctx.handle, C.byref(O.B.struct), Bd.data_ptr())
             if st == 0:
-                O.Bd, O.ranks32 = Bd, r32
-            elif st != HB_ERR_UNSUPPORTED:
-                check(st, "hb_ell_pack_ordered", ctx.handle)
-        return O
+                O.Bd = Bd
+                return O
+            if st != HB_ERR_UNSUPPORTED:
+                check(st, "hb_ell_pack_offsets", ctx.handle)
+        ranks = torch.empty(max(self._rows, 1), dtype=torch.int64, device=self.Aj.device)
+        check(lib().hb_ell_permute_sorted(ctx.handle, C.byref(self._s), order.data_ptr(), pos.data_ptr(),
+                                          C.byref(B), ranks.data_ptr()), "hb_ell_permute_sorted", ctx.handle)
+        return OrderedMatrixELL(SparseMatrixELL(self._rows, self._cols, self.K, self.ld, Aj, Ax), order, pos,
+                                True, info, ranks)
 
 
 class OrderedMatrixELL:
     """A SparseMatrixELL stored in a locality order (SparseMatrixELL.ordered): B = the rows of
-    A in `order`, with its columns renumbered through `pos` when `columns`.  Products through it
-    equal A's bit for bit."""
+    A in `order`, with its columns renumbered through `pos` when `columns` (packed: Bd holds the
+    columns as 16-bit offsets; ranked: the slots sorted by new column, ranks their summation
+    order).  Products through it equal A's bit for bit."""
 
     def __init__(self, B: SparseMatrixELL, order: torch.Tensor, pos: torch.Tensor, columns: bool, info=None,
                  ranks: torch.Tensor | None = None):
         self.B, self.order, self.pos, self.columns_renumbered = B, order, pos, columns
         self.info = info
-        self.ranks = ranks
-        self.Bd = self.ranks32 = None                   # the packed form, when it was made
+        self.ranks = ranks                              # the sorted, ranked form
+        self.Bd = None                                  # the packed form: 16-bit column offsets
         self.dtype = B.dtype
         self._xw = None
 
@@ -348,8 +351,8 @@ class OrderedMatrixELL:
             xp = self._xw.data_ptr()
             if self.Bd is not None:
                 check(getattr(lib(), f"hb_spmv_packed_{suf}")(ctx.handle, C.byref(self.B.struct), self.Bd.data_ptr(),
-                                                              self.order.data_ptr(), self.ranks32.data_ptr(), xp,
-                                                              _vec(y, self.dtype, "y")), "Product", ctx.handle)
+                                                              self.order.data_ptr(), xp, _vec(y, self.dtype, "y")),
+                      "Product", ctx.handle)
             else:
                 check(getattr(lib(), f"hb_spmv_ranked_{suf}")(ctx.handle, C.byref(self.B.struct),
                                                               self.order.data_ptr(), self.ranks.data_ptr(), xp,

@@ -151,19 +151,19 @@ int hb_spmv_ranked_f32(hb_context *ctx, const hb_ell *B, const int32_t *order, c
 /* xw[k] = x[order[k]], k < n.  Asynchronous. */
 int hb_gather_f64(hb_context *ctx, int64_t n, const int32_t *order, const double *x, double *xw);
 int hb_gather_f32(hb_context *ctx, int64_t n, const int32_t *order, const float *x, float *xw);
-/* The packed form of a sorted copy (no reference counterpart; it only shrinks the index
- * traffic of the product): Bd (device int16[K * ld]) = each stored column as its offset from
- * the row, INT16_MIN for padding; ranks32 (device uint32[rows]) = the first eight 4-bit fields
- * of ranks (a ninth slot's rank follows from the other eight).  K <= 9; HB_ERR_UNSUPPORTED when
- * an offset is outside +-32767 (the copy's bandwidth is too large; use the ranked product).
- * Synchronises the stream. */
-int hb_ell_pack_ordered(hb_context *ctx, const hb_ell *B, const uint64_t *ranks, int16_t *Bd, uint32_t *ranks32);
-/* hb_spmv_ranked_* through the packed form: B supplies rows, K, ld and the values (its Aj is
- * not read).  Same sums in the same order; y = A x bit for bit.  Asynchronous. */
-int hb_spmv_packed_f64(hb_context *ctx, const hb_ell *B, const int16_t *Bd, const int32_t *order,
-                       const uint32_t *ranks32, const double *x, double *y);
-int hb_spmv_packed_f32(hb_context *ctx, const hb_ell *B, const int16_t *Bd, const int32_t *order,
-                       const uint32_t *ranks32, const float *x, float *y);
+/* The packed form of a renumbered copy (hb_ell_permute with pos; no reference counterpart, it
+ * only shrinks the index traffic of the product): Bd (device int16[K * ld]) = each stored column
+ * as its offset from the row, INT16_MIN for padding.  K <= 9; HB_ERR_UNSUPPORTED when an offset
+ * is outside +-32767 (the copy's bandwidth is too large; use the ranked product).  Synchronises
+ * the stream. */
+int hb_ell_pack_offsets(hb_context *ctx, const hb_ell *B, int16_t *Bd);
+/* The product through the packed form: y[order[k]] = B's row k, x already permuted (hb_gather);
+ * B supplies rows, K, ld and the values (its Aj is not read).  Each row sums its slots in their
+ * order, which the renumbered copy keeps: y = A x bit for bit.  Asynchronous. */
+int hb_spmv_packed_f64(hb_context *ctx, const hb_ell *B, const int16_t *Bd, const int32_t *order, const double *x,
+                       double *y);
+int hb_spmv_packed_f32(hb_context *ctx, const hb_ell *B, const int16_t *Bd, const int32_t *order, const float *x,
+                       float *y);
 
 /* SPAI2<tags::GPU::CUDA>::value(M, A) (honei/math/spai2.hh:294-298; wrapper
  * honei/math/spai2-cuda.cc:180-228): the sparse approximate inverse of the square matrix A with

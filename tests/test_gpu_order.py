@@ -1,6 +1,6 @@
 """Locality order (hb_ell_cm_order) and the product through a reordered copy (hb_ell_permute,
-hb_spmv_rows, hb_gather; the sorted copy with hb_spmv_ranked; its packed form with
-hb_spmv_packed).
+hb_spmv_rows, hb_gather; the sorted copy with hb_spmv_ranked; the packed form with
+hb_ell_pack_offsets and hb_spmv_packed).
 
 The order has no reference counterpart; the product through the reordered copy must equal the
 product on the matrix as given (Product<tags::CPU>, honei/la/product.hh:148-204) bit for bit,
@@ -93,11 +93,12 @@ FORMS = ["rows", "ranked", "packed"]
 
 
 def ordered_form(Ad, form):
-    """The ordered copy in one of its forms: rows (A's columns), ranked (renumbered, sorted,
-    64-bit ranks) and packed (16-bit offsets, 32-bit ranks)."""
+    """The ordered copy in one of its forms: rows (A's columns), ranked (renumbered, slots sorted
+    by new column, 64-bit summation ranks) and packed (renumbered, slots in their order, 16-bit
+    column offsets)."""
     B = Ad.ordered(columns=form != "rows", packed=form == "packed")
     if form == "packed":
-        assert B.Bd is not None and B.Bd.dtype == torch.int16 and B.ranks32.dtype == torch.int32
+        assert B.Bd is not None and B.Bd.dtype == torch.int16 and B.ranks is None
     else:
         assert B.Bd is None
     return B
@@ -119,7 +120,7 @@ def test_product_through_ordered_copy_bit_exact(hb, oracle, name, make, form, dt
 def test_packed_form_declined_falls_back_to_ranks(hb, oracle):
     """The packed form needs K <= 9 and every reordered column within +-32767 of its row: a
     random pattern over 120,000 rows (offsets up to n after ordering) and one with 12 entries per
-    row are left in the 64-bit ranked form, and their products stay bit-exact."""
+    row fall back to the sorted, ranked form, and their products stay bit-exact."""
     for A in (random_pattern(120000, 7, max_per_row=3), random_pattern(800, 9, max_per_row=12)):
         Ad = hb.SparseMatrixELL.from_reference(A)
         B = Ad.ordered(columns=True, packed=True)
