@@ -721,9 +721,9 @@ class CGSolver:
         """CG on a matrix through its ordered copy (columns renumbered): b and x0 are permuted
         into the copy's numbering once (hb_gather with order), the solve runs on the copy B =
         P A P^T, whose gathers are local, and x is permuted back (hb_gather with pos: x[i] =
-        xw[pos[i]]).  The same CG; its dot products add the entries in the copy's order and
-        each row of B sums its slots in ascending new column, so the iterates agree with CG on A
-        to rounding (the parity bar of any reordered reduction)."""
+        xw[pos[i]]).  The same CG; its dot products add the entries in the copy's order (and in
+        the sorted, ranked form each row of B sums its slots in ascending new column), so the
+        iterates agree with CG on A to rounding (the parity bar of any reordered reduction)."""
         if not O.columns_renumbered:
             raise ValueError("CG through an ordered copy needs its columns renumbered (ordered(columns=True))")
         n = O.rows()
